@@ -1,0 +1,263 @@
+"""empanada_b200 -- B200-native drop-in for empanada's read-overlap path.
+
+The product is the native library (``libempanada_b200.so``, C ABI in
+``include/empanada.h``) and the ``empanada`` command built beside it.  This
+module is the host-side mirror of the reference's interface for that path:
+
+* :func:`parse_args` / :class:`Config` -- the reference's option parser
+  (config.h:10-140): ``input.fastq output.bin -o -m -r -b -c``;
+* :func:`run_file` -- the reference program (main.cu:9-77): FASTQ file in,
+  ``output.bin`` out;
+* :func:`run_bytes` / :class:`Engine` -- the same on in-memory or
+  device-resident FASTQ bytes;
+* :func:`decode_output` -- the ``output.bin`` record format
+  (overlap.cu:148-161): ``u64 n | i32 ovlp_len | u32 from[n] | u32 to[n]``.
+
+Every entry point calls the CUDA path; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import struct
+from typing import Iterable
+
+import numpy as np
+
+from . import _native
+from ._native import EmpError, check
+
+__all__ = ["Config", "parse_args", "parse_size", "Engine", "Job", "run_bytes", "run_file", "decode_output",
+           "EmpError", "UsageExit"]
+
+DEFAULTS = {"o": "31", "m": "1g", "r": "1g", "b": "32m", "c": "64m"}
+_OPTIONS = [  # (shortname, longname, description, default) as in config.h:282-290
+    ("o", "min-overlap", "minimum overlap length", "31"),
+    ("m", "map-mem", "device memory during the fingerprint generation phase", "1g"),
+    ("r", "reduce-mem", "device memory during the overlap-detection phase", "1g"),
+    ("b", "base-blocksz", "block size (count) of transposed bases", "32m"),
+    ("c", "kv-chunksz", "block size (count) of key-value pairs", "64m"),
+]
+
+
+class UsageExit(SystemExit):
+    """The reference prints its usage and exits 0 (config.h:21-35)."""
+
+    def __init__(self, message: str):
+        super().__init__(0)
+        self.message = message
+
+
+def usage_text() -> str:
+    lines = ["Usage: assembly_v3 [input fastq] [output gfa] [options]", "Options:"]
+    for s, l, d, dv in _OPTIONS:
+        lines.append(f"  -{s} or --{l}, {d}, default = {dv}")
+    return "\n".join(lines) + "\n"
+
+
+def parse_size(s: str) -> int:
+    """hmsize2bytes (config.h:75-100) through the native parser."""
+    v = ctypes.c_uint64(0)
+    rc = _native.lib().emp_parse_size(s.encode(), ctypes.byref(v))
+    if rc == _native.EMP_E_INVAL and s and not s[-1].isdigit():
+        inner = ctypes.c_uint64(0)
+        if _native.lib().emp_parse_size(s[:-1].encode(), ctypes.byref(inner)) == _native.EMP_OK:
+            return int(inner.value)  # unknown unit: logged and ignored by the reference
+    check(rc, f"size {s!r}")
+    return int(v.value)
+
+
+@dataclasses.dataclass
+class Config:
+    """Config::init (config.h:120-140)."""
+    input: str
+    output: str
+    min_ovlp: int = 31
+    map_mem: int = 1 << 30
+    reduce_mem: int = 1 << 30
+    base_blocksz: int = 32 << 20
+    kv_chunksz: int = 64 << 20
+
+    def params(self) -> _native.Params:
+        return _native.Params(self.min_ovlp, self.map_mem, self.reduce_mem, self.base_blocksz, self.kv_chunksz)
+
+
+def parse_args(argv: Iterable[str]) -> Config:
+    """parse_args (config.h:37-73) with the reference's quirks: options are
+    matched on their second character, long options are rejected, and a
+    missing positional or an unknown option raises :class:`UsageExit`."""
+    args = list(argv)
+    positional: list[str] = []
+    values: dict[str, str] = {}
+    i = 0
+    while i < len(args):
+        arg = args[i]
+        if len(positional) < 2:
+            positional.append(arg)
+            i += 1
+            continue
+        second = arg[1] if len(arg) > 1 else ""
+        found = False
+        for s, _l, _d, _dv in _OPTIONS:
+            if second == s:
+                if i + 1 >= len(args):
+                    raise ValueError(f"option {arg} needs a value")
+                values[s] = args[i + 1]
+                i += 2
+                found = True
+                break
+        if not found:
+            raise UsageExit(f"Invalid option {arg}\n" + usage_text())
+    if len(positional) < 2:
+        raise UsageExit(usage_text())
+    get = lambda k: parse_size(values.get(k, DEFAULTS[k]))
+    o = get("o")
+    o = ((o + 2**31) % 2**32) - 2**31  # int conversion of config.h:127
+    return Config(positional[0], positional[1], o, get("m"), get("r"), get("b"), get("c"))
+
+
+def _params(min_ovlp=31, map_mem="1g", reduce_mem="1g", base_blocksz="32m", kv_chunksz="64m") -> _native.Params:
+    conv = lambda v: parse_size(v) if isinstance(v, str) else int(v)
+    return _native.Params(int(min_ovlp), conv(map_mem), conv(reduce_mem), conv(base_blocksz), conv(kv_chunksz))
+
+
+class Engine:
+    """An emp_ctx: one device, its stream and hash tables."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self._lib = _native.lib()
+        h = ctypes.c_void_p()
+        check(self._lib.emp_ctx_create(device, hbm_budget_bytes, ctypes.byref(h)), "emp_ctx_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self._lib.emp_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def job(self, **params) -> "Job":
+        return Job(self, _params(**params))
+
+    def sort_pairs(self, keys_ptr: int, vals_ptr: int, n: int, stream: int = 0) -> None:
+        """Stable device sort of (u64 fingerprint, u32 value) pairs in place."""
+        check(self._lib.emp_sort_pairs(self.handle, keys_ptr, vals_ptr, n, stream or None), "emp_sort_pairs")
+
+
+class Job:
+    def __init__(self, engine: Engine, params: _native.Params):
+        self.engine = engine
+        self._lib = engine._lib
+        h = ctypes.c_void_p()
+        check(self._lib.emp_job_create(engine.handle, ctypes.byref(params), ctypes.byref(h)), "emp_job_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self._lib.emp_job_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def reserve(self, nbytes: int) -> None:
+        check(self._lib.emp_job_reserve(self.handle, nbytes), "emp_job_reserve")
+
+    def feed(self, data, last: bool = True) -> None:
+        """Append host FASTQ bytes (bytes, bytearray or a uint8 numpy array)."""
+        if isinstance(data, np.ndarray):
+            arr = np.ascontiguousarray(data, dtype=np.uint8)
+            check(self._lib.emp_job_feed_fastq(self.handle, arr.ctypes.data, arr.size, int(last)), "feed")
+        else:
+            buf = bytes(data)
+            check(self._lib.emp_job_feed_fastq(self.handle, ctypes.c_char_p(buf), len(buf), int(last)), "feed")
+
+    def feed_device(self, ptr: int, nbytes: int, last: bool = True) -> None:
+        check(self._lib.emp_job_feed_fastq_device(self.handle, ptr, nbytes, int(last)), "feed_device")
+
+    def run(self, stream: int = 0) -> None:
+        check(self._lib.emp_job_run(self.handle, stream or None), "emp_job_run")
+
+    def output(self) -> bytes:
+        n = ctypes.c_uint64()
+        check(self._lib.emp_job_output_size(self.handle, ctypes.byref(n)), "output_size")
+        buf = ctypes.create_string_buffer(max(1, n.value))
+        check(self._lib.emp_job_output_copy(self.handle, buf, n.value), "output_copy")
+        return buf.raw[: n.value]
+
+    def output_into(self, arr: np.ndarray) -> int:
+        n = ctypes.c_uint64()
+        check(self._lib.emp_job_output_size(self.handle, ctypes.byref(n)), "output_size")
+        if arr.nbytes < n.value:
+            raise ValueError("output array too small")
+        check(self._lib.emp_job_output_copy(self.handle, arr.ctypes.data, arr.nbytes), "output_copy")
+        return int(n.value)
+
+    def stats(self) -> dict:
+        st = _native.Stats()
+        check(self._lib.emp_job_stats(self.handle, ctypes.byref(st)), "stats")
+        return st.to_dict()
+
+    def fingerprints(self) -> np.ndarray:
+        n = ctypes.c_uint64()
+        check(self._lib.emp_job_fingerprints(self.handle, None, 0, ctypes.byref(n)), "fingerprints")
+        out = np.empty(n.value, dtype=np.uint64)
+        if n.value:
+            check(self._lib.emp_job_fingerprints(self.handle, out.ctypes.data, out.size, ctypes.byref(n)),
+                  "fingerprints")
+        return out
+
+
+def run_bytes(fastq, device: int = 0, engine: Engine | None = None, **params) -> tuple[bytes, dict]:
+    """FASTQ bytes in host memory -> (output.bin bytes, stats)."""
+    eng = engine or Engine(device)
+    try:
+        with eng.job(**params) as job:
+            job.feed(fastq, last=True)
+            job.run()
+            return job.output(), job.stats()
+    finally:
+        if engine is None:
+            eng.close()
+
+
+def run_file(input_path: str, output_path: str, device: int = -1, **params) -> dict:
+    """The reference program: read input_path, write output_path (main.cu:9-77)."""
+    p = _params(**params)
+    st = _native.Stats()
+    check(_native.lib().emp_run_file(input_path.encode(), output_path.encode(), ctypes.byref(p), device,
+                                     ctypes.byref(st)), "emp_run_file")
+    return st.to_dict()
+
+
+def decode_output(data: bytes) -> list[tuple[int, np.ndarray, np.ndarray]]:
+    """output.bin -> [(ovlp_len, from, to), ...] in file order."""
+    recs = []
+    off = 0
+    mv = memoryview(data)
+    while off < len(data):
+        if off + 12 > len(data):
+            raise ValueError("truncated record header")
+        n, ovlp = struct.unpack_from("<Qi", data, off)
+        off += 12
+        if off + 8 * n > len(data):
+            raise ValueError("truncated record body")
+        frm = np.frombuffer(mv[off: off + 4 * n], dtype=np.uint32)
+        to = np.frombuffer(mv[off + 4 * n: off + 8 * n], dtype=np.uint32)
+        off += 8 * n
+        recs.append((ovlp, frm, to))
+    return recs

@@ -1,0 +1,124 @@
+"""ctypes binding of libempanada_b200.so (the C ABI declared in include/empanada.h).
+
+Loading fails loudly when the library has not been built: there is no
+fallback implementation of the overlap path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libempanada_b200.so")
+
+EMP_OK = 0
+EMP_E_INVAL = -1
+EMP_E_NOMEM = -2
+EMP_E_CUDA = -3
+EMP_E_TIMEOUT = -4
+EMP_E_FORMAT = -5
+EMP_E_STATE = -6
+EMP_E_IO = -7
+EMP_E_UNSUPPORTED = -8
+EMP_E_HANG = -9
+MAX_ROUNDS = 256
+
+# every function include/empanada.h declares, with its ctypes signature
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_vp = ctypes.c_void_p
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("min_ovlp", ctypes.c_int32),
+        ("map_mem", ctypes.c_uint64),
+        ("reduce_mem", ctypes.c_uint64),
+        ("base_blocksz", ctypes.c_uint64),
+        ("kv_chunksz", ctypes.c_uint64),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("n_reads", ctypes.c_uint64),
+        ("read_len", ctypes.c_int32),
+        ("n_rounds", ctypes.c_int32),
+        ("n_unique", ctypes.c_uint64),
+        ("n_edges", ctypes.c_uint64),
+        ("n_records", ctypes.c_uint64),
+        ("fastq_bytes", ctypes.c_uint64),
+        ("output_bytes", ctypes.c_uint64),
+        ("gpu_launches", ctypes.c_uint64),
+        ("ms_h2d", ctypes.c_double),
+        ("ms_map", ctypes.c_double),
+        ("ms_dedup", ctypes.c_double),
+        ("ms_rounds", ctypes.c_double),
+        ("ms_total", ctypes.c_double),
+        ("sfx_live", ctypes.c_uint64 * MAX_ROUNDS),
+        ("pfx_live", ctypes.c_uint64 * MAX_ROUNDS),
+        ("edges", ctypes.c_uint64 * MAX_ROUNDS),
+    ]
+
+    def to_dict(self) -> dict:
+        d = {f: getattr(self, f) for f, _ in self._fields_[:14]}
+        r = self.n_rounds
+        d["sfx_live"] = list(self.sfx_live[:r])
+        d["pfx_live"] = list(self.pfx_live[:r])
+        d["edges"] = list(self.edges[:r])
+        return d
+
+
+SIGNATURES = {
+    "emp_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "emp_abi_version": (ctypes.c_int, []),
+    "emp_params_default": (ctypes.c_int, [ctypes.POINTER(Params)]),
+    "emp_parse_size": (ctypes.c_int, [ctypes.c_char_p, _u64p]),
+    "emp_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(_vp)]),
+    "emp_ctx_destroy": (ctypes.c_int, [_vp]),
+    "emp_job_create": (ctypes.c_int, [_vp, ctypes.POINTER(Params), ctypes.POINTER(_vp)]),
+    "emp_job_destroy": (ctypes.c_int, [_vp]),
+    "emp_job_feed_fastq": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int]),
+    "emp_job_feed_fastq_device": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int]),
+    "emp_job_reserve": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "emp_job_run": (ctypes.c_int, [_vp, _vp]),
+    "emp_job_output_size": (ctypes.c_int, [_vp, _u64p]),
+    "emp_job_output_copy": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64]),
+    "emp_job_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats)]),
+    "emp_job_fingerprints": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, _u64p]),
+    "emp_run_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Params), ctypes.c_int,
+                                    ctypes.POINTER(Stats)]),
+    "emp_sort_pairs": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp]),
+}
+
+_lib = None
+
+
+class EmpError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        msg = status_string(code) if _lib is not None else str(code)
+        super().__init__(f"{what}: {msg} ({code})" if what else f"{msg} ({code})")
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"native library {LIB_PATH} is missing: run __graft_entry__.build() "
+                               "(the overlap path has no CPU fallback)")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(l, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def status_string(code: int) -> str:
+    return lib().emp_status_string(code).decode()
+
+
+def check(code: int, what: str = "") -> None:
+    if code != EMP_OK:
+        raise EmpError(code, what)

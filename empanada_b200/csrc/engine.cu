@@ -1,0 +1,763 @@
+// engine.cu -- job orchestration and the C ABI (include/empanada.h).
+//
+// One job runs the reference program's two phases on the device:
+//   map     main.cu:42-58  -> nl_count/scan/nl_locate, classify/scan/scatter,
+//                             fingerprint_pack (k_map.cu)
+//   reduce  overlap.cu:206-293 -> fingerprint sort + dedup_mark + init_list,
+//                             then per round update_compact, sort, join
+//                             (k_round.cu, k_sort.cu)
+// All tables stay in HBM; the only host traffic is the FASTQ in and the
+// edge list out.  output.bin records are assembled on the host exactly as
+// write_edges_binary (overlap.cu:148-161) writes them.
+#include <cerrno>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/empanada.h"
+#include "kernels.h"
+
+namespace emp {
+std::atomic<uint64_t> g_launches{0};
+}
+
+using namespace emp;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct PinnedBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~PinnedBuf() { if (p) cudaFreeHost(p); }
+    bool ensure(size_t b) {
+        if (b <= bytes) return true;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        size_t nb = b < 4096 ? 4096 : b + b / 2;
+        if (cudaHostAlloc(&p, nb, cudaHostAllocDefault) != cudaSuccess) { p = nullptr; return false; }
+        bytes = nb;
+        return true;
+    }
+    template <class T>
+    T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+}  // namespace
+
+struct emp_ctx {
+    int device = 0;
+    uint64_t budget = 0;
+    uint64_t in_use = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf tables;  // HashTables
+};
+
+struct emp_job {
+    emp_ctx *ctx = nullptr;
+    emp_params p{};
+    // input
+    DevBuf fq;
+    uint64_t F = 0;
+    bool fed_last = false;
+    double ms_h2d = 0.0;
+    // work buffers
+    DevBuf tile_counts, tile_excl, status, misc, seq_start, seq_end, hq, idx, rec_of, keys0, cols;
+    DevBuf sk0, sv0, sk1, sv1, alive, lk0, lv0, lk1, lv1, used_s, used_p, cnt, offs, efrom, eto, sort_scratch;
+    DevBuf akeys, apos, bkeys, parts;  // record splitting
+    PinnedBuf h_parts;
+    PinnedBuf h_misc, h_hist, h_from, h_to;
+    uint64_t n_ends = 0;
+    // results
+    std::vector<uint8_t> out;
+    emp_stats st{};
+    bool have_result = false;
+};
+
+namespace {
+
+// misc device words (u64 slots)
+enum MiscSlot { kMiscErr = 0, kMiscTotal = 1, kMiscLen = 2, kMiscN = 3, kMiscU = 4, kMiscNout = 5, kMiscSout = 6,
+                kMiscE = 7, kMiscCtr = 8, kMiscParts = 9, kMiscSlots = 16 };
+
+emp_status cuda_status(cudaError_t e) { return e == cudaSuccess ? EMP_OK : (e == cudaErrorMemoryAllocation ? EMP_E_NOMEM : EMP_E_CUDA); }
+
+emp_status ensure(emp_job *j, DevBuf &b, size_t bytes) {
+    if (bytes <= b.bytes) return EMP_OK;
+    emp_ctx *c = j->ctx;
+    const size_t old = b.bytes;
+    if (c->budget && c->in_use - old + bytes > c->budget) return EMP_E_NOMEM;
+    b.release();
+    c->in_use -= old;
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return EMP_E_NOMEM;
+    }
+    b.p = p;
+    b.bytes = bytes;
+    c->in_use += bytes;
+    return EMP_OK;
+}
+
+void free_buf(emp_job *j, DevBuf &b) {
+    j->ctx->in_use -= b.bytes;
+    b.release();
+}
+
+uint32_t host_modpow(uint64_t a, uint32_t e, uint32_t p) {
+    uint64_t r = 1;
+    while (e) {
+        if (e & 1) r = (r * a) % p;
+        a = (a * a) % p;
+        e >>= 1;
+    }
+    return (uint32_t)r;
+}
+
+void host_tables(HashTables &t) {
+    t.pow1[0] = t.pow2[0] = 1;
+    for (int i = 1; i <= kMaxReadLen; ++i) {
+        t.pow1[i] = (uint32_t)(((uint64_t)t.pow1[i - 1] * kR1) % kP1);
+        t.pow2[i] = (uint32_t)(((uint64_t)t.pow2[i - 1] * kR2) % kP2);
+    }
+    t.inv1 = host_modpow(kR1, kP1 - 2, kP1);
+    t.inv2 = host_modpow(kR2, kP2 - 2, kP2);
+}
+
+#define EMP_TRY(x)                         \
+    do {                                   \
+        emp_status _s = (x);               \
+        if (_s != EMP_OK) return _s;       \
+    } while (0)
+#define EMP_CUDA(x) EMP_TRY(cuda_status(x))
+
+struct Events {
+    cudaEvent_t e[5] = {};
+    Events() { for (auto &x : e) cudaEventCreate(&x); }
+    ~Events() { for (auto &x : e) cudaEventDestroy(x); }
+};
+
+float ms_between(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) { cudaGetLastError(); return 0.f; }
+    return ms;
+}
+
+emp_status sync_and_check(emp_job *j, cudaStream_t s) {
+    EMP_CUDA(cudaMemcpyAsync(j->h_misc.p, j->misc.p, kMiscSlots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    EMP_CUDA(cudaStreamSynchronize(s));
+    const uint64_t err = j->h_misc.as<uint64_t>()[kMiscErr];
+    if (err & kErrSpin) return EMP_E_TIMEOUT;
+    return EMP_OK;
+}
+
+void append_bytes(std::vector<uint8_t> &o, const void *p, size_t n) {
+    const uint8_t *b = reinterpret_cast<const uint8_t *>(p);
+    o.insert(o.end(), b, b + n);
+}
+
+// reset look-back status words + tile counter for a chained scan over `tiles`
+emp_status reset_chain(emp_job *j, uint64_t tiles, cudaStream_t s) {
+    EMP_TRY(ensure(j, j->status, tiles * sizeof(uint64_t) + 64));
+    EMP_CUDA(cudaMemsetAsync(j->status.p, 0, tiles * sizeof(uint64_t), s));
+    EMP_CUDA(cudaMemsetAsync(j->misc.as<uint64_t>() + kMiscCtr, 0, sizeof(uint64_t), s));
+    return EMP_OK;
+}
+uint32_t *chain_ctr(emp_job *j) { return reinterpret_cast<uint32_t *>(j->misc.as<uint64_t>() + kMiscCtr); }
+uint32_t *err_word(emp_job *j) { return reinterpret_cast<uint32_t *>(j->misc.as<uint64_t>() + kMiscErr); }
+
+emp_status run_job(emp_job *j, cudaStream_t s) {
+    emp_stats &st = j->st;
+    std::memset(&st, 0, sizeof st);
+    j->out.clear();
+    j->have_result = false;
+    j->n_ends = 0;
+    st.fastq_bytes = j->F;
+    st.ms_h2d = j->ms_h2d;
+    const uint64_t launches0 = g_launches.load();
+    const uint64_t M = j->p.reduce_mem / 16;
+    if (M < 2) return EMP_E_INVAL;
+    const uint64_t F = j->F;
+    const HashTables *tables = j->ctx->tables.as<HashTables>();
+    Events ev;
+    cudaEventRecord(ev.e[0], s);
+
+    EMP_TRY(ensure(j, j->misc, kMiscSlots * sizeof(uint64_t)));
+    if (!j->h_misc.ensure(kMiscSlots * sizeof(uint64_t)) || !j->h_hist.ensure(kSortPasses * kSortRadix * 4))
+        return EMP_E_NOMEM;
+    uint64_t *hm = j->h_misc.as<uint64_t>();
+    uint64_t *dm = j->misc.as<uint64_t>();
+    EMP_CUDA(cudaMemsetAsync(j->misc.p, 0, kMiscSlots * sizeof(uint64_t), s));
+
+    uint64_t n = 0, n_rec = 0;
+    int L = 0;
+    if (F) {
+        // ---- K1: newline index
+        const uint64_t T = parse_tiles(F);
+        EMP_TRY(ensure(j, j->tile_counts, T * 4));
+        EMP_TRY(ensure(j, j->tile_excl, T * 8));
+        launch_nl_count(j->fq.as<uint8_t>(), F, j->tile_counts.as<uint32_t>(), s);
+        EMP_TRY(reset_chain(j, scan_tiles(T), s));
+        launch_scan_u32_u64(j->tile_counts.as<uint32_t>(), j->tile_excl.as<uint64_t>(), T, j->status.as<uint64_t>(),
+                            chain_ctr(j), dm + kMiscTotal, err_word(j), s);
+        EMP_TRY(sync_and_check(j, s));
+        const uint64_t total_nl = hm[kMiscTotal];
+        n_rec = total_nl ? (total_nl + 3) / 4 : 0;
+        if (n_rec) {
+            EMP_TRY(ensure(j, j->seq_start, n_rec * 8));
+            EMP_TRY(ensure(j, j->seq_end, n_rec * 8));
+            launch_nl_locate(j->fq.as<uint8_t>(), F, j->tile_excl.as<uint64_t>(), j->seq_start.as<uint64_t>(),
+                             j->seq_end.as<uint64_t>(), s);
+            if ((total_nl - 1) % 4 == 0) {  // last sequence line ends at end of input
+                hm[kMiscSlots - 1] = F;
+                EMP_CUDA(cudaMemcpyAsync(j->seq_end.as<uint64_t>() + n_rec - 1, hm + kMiscSlots - 1, 8,
+                                         cudaMemcpyHostToDevice, s));
+            }
+            // ---- K2a: classify records
+            EMP_TRY(ensure(j, j->hq, n_rec * 4));
+            EMP_TRY(ensure(j, j->idx, n_rec * 4));
+            const uint32_t mm[2] = {0xffffffffu, 0u};
+            std::memcpy(hm + kMiscLen, mm, 8);
+            EMP_CUDA(cudaMemcpyAsync(dm + kMiscLen, hm + kMiscLen, 8, cudaMemcpyHostToDevice, s));
+            launch_classify(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->seq_end.as<uint64_t>(), n_rec,
+                            j->hq.as<uint32_t>(), reinterpret_cast<uint32_t *>(dm + kMiscLen), err_word(j), s);
+            EMP_TRY(reset_chain(j, scan_tiles(n_rec), s));
+            launch_scan_u32_u32(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), n_rec, j->status.as<uint64_t>(),
+                                chain_ctr(j), dm + kMiscN, err_word(j), s);
+            EMP_TRY(sync_and_check(j, s));
+            if (hm[kMiscErr] & kErrBadBase) return EMP_E_FORMAT;
+            n = hm[kMiscN];
+            uint32_t mm2[2];
+            std::memcpy(mm2, hm + kMiscLen, 8);
+            if (n) {
+                if (mm2[0] != mm2[1]) return EMP_E_FORMAT;
+                L = (int)mm2[0];
+                if (mm2[0] > (uint32_t)kMaxReadLen) return EMP_E_UNSUPPORTED;
+            }
+        }
+    }
+    st.n_reads = n;
+    st.read_len = L;
+    if (n == 0) {
+        cudaEventRecord(ev.e[4], s);
+        EMP_CUDA(cudaStreamSynchronize(s));
+        st.ms_total = ms_between(ev.e[0], ev.e[4]);
+        st.gpu_launches = g_launches.load() - launches0;
+        j->have_result = true;
+        return EMP_OK;
+    }
+    if (j->p.min_ovlp < 0) return EMP_E_INVAL;
+    const uint64_t n2 = 2 * n;
+    if (n2 >= (1ull << 31)) return EMP_E_UNSUPPORTED;
+    if (n2 > M) return EMP_E_UNSUPPORTED;  // out-of-core merge-tree order not emulated yet
+
+    // ---- K2b: fingerprints + 2-bit column store
+    const uint64_t wpc = (n + 15) / 16;
+    EMP_TRY(ensure(j, j->rec_of, n * 4));
+    EMP_TRY(ensure(j, j->cols, (uint64_t)L * wpc * 4));
+    EMP_TRY(ensure(j, j->keys0, n2 * 8));
+    launch_scatter_hq(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), n_rec, j->rec_of.as<uint32_t>(), s);
+    launch_fingerprint_pack(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->rec_of.as<uint32_t>(), n, L, tables,
+                            j->keys0.as<uint64_t>(), j->cols.as<uint32_t>(), wpc, s);
+    j->n_ends = n2;
+    cudaEventRecord(ev.e[1], s);
+
+    // ---- fingerprint sort + duplicate removal (overlap.cu:212-225)
+    const uint64_t cap = 2 * n2;  // both tables, each at most n2 entries
+    EMP_TRY(ensure(j, j->sk0, cap * 8));
+    EMP_TRY(ensure(j, j->sk1, cap * 8));
+    EMP_TRY(ensure(j, j->sv0, cap * 4));
+    EMP_TRY(ensure(j, j->sv1, cap * 4));
+    EMP_TRY(ensure(j, j->lk0, cap * 8));
+    EMP_TRY(ensure(j, j->lk1, cap * 8));
+    EMP_TRY(ensure(j, j->lv0, cap * 4));
+    EMP_TRY(ensure(j, j->lv1, cap * 4));
+    EMP_TRY(ensure(j, j->alive, n2));
+    EMP_TRY(ensure(j, j->used_s, n2));
+    EMP_TRY(ensure(j, j->used_p, n2));
+    EMP_TRY(ensure(j, j->sort_scratch, sort_scratch_bytes(cap)));
+    EMP_CUDA(cudaMemcpyAsync(j->sk0.p, j->keys0.p, n2 * 8, cudaMemcpyDeviceToDevice, s));
+    launch_iota(j->sv0.as<uint32_t>(), n2, s);
+    int res = sort_pairs(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), j->sk1.as<uint64_t>(), j->sv1.as<uint32_t>(), n2,
+                         j->sort_scratch.p, j->h_hist.as<uint32_t>(), err_word(j), s);
+    const uint64_t *sk = res ? j->sk1.as<uint64_t>() : j->sk0.as<uint64_t>();
+    const uint32_t *sv = res ? j->sv1.as<uint32_t>() : j->sv0.as<uint32_t>();
+    launch_dedup_mark(sk, sv, n2, j->alive.as<uint8_t>(), s);
+    EMP_TRY(reset_chain(j, upd_tiles(n2), s));
+    launch_init_list(j->keys0.as<uint64_t>(), j->alive.as<uint8_t>(), n, j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(),
+                     j->status.as<uint64_t>(), chain_ctr(j), dm + kMiscU, err_word(j), s);
+    EMP_TRY(sync_and_check(j, s));
+    const uint64_t U = hm[kMiscU];
+    st.n_unique = U;
+    launch_dup_prefix_half(j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(), U, s);
+    EMP_CUDA(cudaMemsetAsync(j->used_s.p, 0, n2, s));
+    EMP_CUDA(cudaMemsetAsync(j->used_p.p, 0, n2, s));
+    cudaEventRecord(ev.e[2], s);
+
+    // ---- overlap rounds (overlap.cu:258-290)
+    uint64_t *lk[2] = {j->lk0.as<uint64_t>(), j->lk1.as<uint64_t>()};
+    uint32_t *lv[2] = {j->lv0.as<uint32_t>(), j->lv1.as<uint32_t>()};
+    int cur = 0;
+    uint64_t n_in = 2 * U;
+    const int rounds = L - j->p.min_ovlp;
+    for (int r = 0; r < rounds; ++r) {
+        EMP_TRY(reset_chain(j, upd_tiles(n_in), s));
+        EMP_CUDA(cudaMemsetAsync(dm + kMiscNout, 0, 2 * sizeof(uint64_t), s));
+        RoundArgs a{};
+        a.kin = lk[cur];
+        a.vin = lv[cur];
+        a.n_in = n_in;
+        a.kout = lk[cur ^ 1];
+        a.vout = lv[cur ^ 1];
+        a.used_s = j->used_s.as<uint8_t>();
+        a.used_p = j->used_p.as<uint8_t>();
+        a.cols = j->cols.as<uint32_t>();
+        a.wpc = wpc;
+        a.tables = tables;
+        a.L = L;
+        a.round = r;
+        a.status = j->status.as<uint64_t>();
+        a.tile_ctr = chain_ctr(j);
+        a.n_out = dm + kMiscNout;
+        a.s_out = dm + kMiscSout;
+        a.err = err_word(j);
+        launch_update_compact(a, s);
+        EMP_TRY(sync_and_check(j, s));
+        const uint64_t N = hm[kMiscNout], S = hm[kMiscSout], P = N - S;
+        if (S == 0) break;  // loop condition of build_graph (overlap.cu:258)
+        cur ^= 1;
+        n_in = N;
+        if (r < EMP_MAX_ROUNDS) {
+            st.sfx_live[r] = S;
+            st.pfx_live[r] = P;
+        }
+        st.n_rounds = r + 1;
+        if (P == 0) continue;  // one-sided search partition: no record
+        // both windows below M/2: one search partition, one record (cqutils.cuh:117-121)
+        const bool split = S >= M / 2 || P >= M / 2;
+        // sort a copy of the merged list (the list itself carries over)
+        EMP_CUDA(cudaMemcpyAsync(j->sk0.p, lk[cur], N * 8, cudaMemcpyDeviceToDevice, s));
+        EMP_CUDA(cudaMemcpyAsync(j->sv0.p, lv[cur], N * 4, cudaMemcpyDeviceToDevice, s));
+        res = sort_pairs(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), j->sk1.as<uint64_t>(), j->sv1.as<uint32_t>(), N,
+                         j->sort_scratch.p, j->h_hist.as<uint32_t>(), err_word(j), s);
+        sk = res ? j->sk1.as<uint64_t>() : j->sk0.as<uint64_t>();
+        sv = res ? j->sv1.as<uint32_t>() : j->sv0.as<uint32_t>();
+        EMP_TRY(ensure(j, j->cnt, N * 4));
+        EMP_TRY(ensure(j, j->offs, N * 8));
+        launch_join_count(sk, sv, N, j->cnt.as<uint32_t>(), s);
+        EMP_TRY(reset_chain(j, scan_tiles(N), s));
+        launch_scan_u32_u64(j->cnt.as<uint32_t>(), j->offs.as<uint64_t>(), N, j->status.as<uint64_t>(), chain_ctr(j),
+                            dm + kMiscE, err_word(j), s);
+        EMP_TRY(sync_and_check(j, s));
+        const uint64_t E = hm[kMiscE];
+        if (E) {
+            EMP_TRY(ensure(j, j->efrom, E * 4));
+            EMP_TRY(ensure(j, j->eto, E * 4));
+            if (!j->h_from.ensure(E * 4) || !j->h_to.ensure(E * 4)) return EMP_E_NOMEM;
+            launch_join_write(sk, sv, N, j->cnt.as<uint32_t>(), j->offs.as<uint64_t>(), j->efrom.as<uint32_t>(),
+                              j->eto.as<uint32_t>(), j->used_s.as<uint8_t>(), j->used_p.as<uint8_t>(), s);
+            EMP_CUDA(cudaMemcpyAsync(j->h_from.p, j->efrom.p, E * 4, cudaMemcpyDeviceToHost, s));
+            EMP_CUDA(cudaMemcpyAsync(j->h_to.p, j->eto.p, E * 4, cudaMemcpyDeviceToHost, s));
+            EMP_CUDA(cudaStreamSynchronize(s));
+        }
+        const int32_t ovlp = L - 1 - r;
+        auto record = [&](uint64_t e0, uint64_t e1) {
+            const uint64_t ne = e1 - e0;
+            append_bytes(j->out, &ne, 8);
+            append_bytes(j->out, &ovlp, 4);
+            if (ne) {
+                append_bytes(j->out, j->h_from.as<uint32_t>() + e0, ne * 4);
+                append_bytes(j->out, j->h_to.as<uint32_t>() + e0, ne * 4);
+            }
+            st.n_records += 1;
+        };
+        if (!split) {
+            record(0, E);
+        } else {
+            // search partitions of windows M/2; each two-sided one is a record
+            EMP_TRY(ensure(j, j->akeys, S * 8));
+            EMP_TRY(ensure(j, j->apos, S * 4));
+            EMP_TRY(ensure(j, j->bkeys, P * 8));
+            const uint64_t pcap = 4 * (N / (M / 2) + 1) + 1024;
+            EMP_TRY(ensure(j, j->parts, pcap * sizeof(SearchPart)));
+            EMP_TRY(reset_chain(j, upd_tiles(N), s));
+            launch_split_tables(sk, sv, N, j->akeys.as<uint64_t>(), j->apos.as<uint32_t>(), j->bkeys.as<uint64_t>(),
+                                j->status.as<uint64_t>(), chain_ctr(j), err_word(j), s);
+            launch_search_partitions(j->akeys.as<uint64_t>(), S, j->bkeys.as<uint64_t>(), P, M / 2,
+                                     j->apos.as<uint32_t>(), j->offs.as<uint64_t>(), E, j->parts.as<SearchPart>(),
+                                     pcap, dm + kMiscParts, err_word(j), s);
+            EMP_TRY(sync_and_check(j, s));
+            if (hm[kMiscErr] & kErrHang) return EMP_E_HANG;
+            if (hm[kMiscErr] & kErrCapacity) return EMP_E_UNSUPPORTED;
+            const uint64_t np = hm[kMiscParts];
+            if (!j->h_parts.ensure(np * sizeof(SearchPart) + 16)) return EMP_E_NOMEM;
+            EMP_CUDA(cudaMemcpyAsync(j->h_parts.p, j->parts.p, np * sizeof(SearchPart), cudaMemcpyDeviceToHost, s));
+            EMP_CUDA(cudaStreamSynchronize(s));
+            const SearchPart *ps = j->h_parts.as<SearchPart>();
+            for (uint64_t q = 0; q < np; ++q)
+                if (ps[q].pa && ps[q].pb) record(ps[q].e0, ps[q].e1);
+        }
+        st.n_edges += E;
+        if (r < EMP_MAX_ROUNDS) st.edges[r] = E;
+    }
+    cudaEventRecord(ev.e[3], s);
+    cudaEventRecord(ev.e[4], s);
+    EMP_TRY(sync_and_check(j, s));
+    EMP_CUDA(cudaGetLastError());
+    st.ms_map = ms_between(ev.e[0], ev.e[1]);
+    st.ms_dedup = ms_between(ev.e[1], ev.e[2]);
+    st.ms_rounds = ms_between(ev.e[2], ev.e[3]);
+    st.ms_total = ms_between(ev.e[0], ev.e[4]);
+    st.output_bytes = j->out.size();
+    st.gpu_launches = g_launches.load() - launches0;
+    j->have_result = true;
+    return EMP_OK;
+}
+
+}  // namespace
+
+// =========================================================================
+// C ABI
+// =========================================================================
+extern "C" {
+
+const char *emp_status_string(emp_status st) {
+    switch (st) {
+    case EMP_OK: return "ok";
+    case EMP_E_INVAL: return "invalid argument";
+    case EMP_E_NOMEM: return "out of memory or over the HBM budget";
+    case EMP_E_CUDA: return "CUDA error";
+    case EMP_E_TIMEOUT: return "bounded device wait timed out";
+    case EMP_E_FORMAT: return "reads of unequal length or a base outside ACGTacgt";
+    case EMP_E_STATE: return "call out of order";
+    case EMP_E_IO: return "file could not be read or written";
+    case EMP_E_UNSUPPORTED: return "unsupported input";
+    case EMP_E_HANG: return "input on which the reference never terminates";
+    default: return "unknown status";
+    }
+}
+
+int emp_abi_version(void) { return EMP_ABI_VERSION; }
+
+emp_status emp_params_default(emp_params *p) {
+    if (!p) return EMP_E_INVAL;
+    p->min_ovlp = 31;
+    p->map_mem = 1ull << 30;
+    p->reduce_mem = 1ull << 30;
+    p->base_blocksz = 32ull << 20;
+    p->kv_chunksz = 64ull << 20;
+    return EMP_OK;
+}
+
+emp_status emp_parse_size(const char *s, uint64_t *bytes) {
+    if (!s || !bytes || !*s) return EMP_E_INVAL;
+    std::string h(s);
+    const char unit = h.back();
+    int shift = 0;
+    emp_status st = EMP_OK;
+    if (!(unit >= '0' && unit <= '9')) {
+        h.pop_back();
+        switch (unit) {
+        case 'k': case 'K': shift = 10; break;
+        case 'm': case 'M': shift = 20; break;
+        case 'g': case 'G': shift = 30; break;
+        default: st = EMP_E_INVAL; break;  // reference: LOG_ERR, value without the suffix
+        }
+    }
+    if (h.empty() || !(h[0] >= '0' && h[0] <= '9') ) {
+        // std::stoul accepts leading blanks and a sign; anything else throws
+        size_t k = 0;
+        while (k < h.size() && (h[k] == ' ' || h[k] == '\t')) ++k;
+        if (k >= h.size() || !((h[k] >= '0' && h[k] <= '9') || h[k] == '+' || h[k] == '-')) return EMP_E_INVAL;
+    }
+    errno = 0;
+    char *end = nullptr;
+    unsigned long long v = std::strtoull(h.c_str(), &end, 10);
+    if (end == h.c_str() || errno == ERANGE) return EMP_E_INVAL;
+    *bytes = (uint64_t)v << shift;
+    return st;
+}
+
+emp_status emp_ctx_create(int device, uint64_t hbm_budget_bytes, emp_ctx **out) {
+    if (!out) return EMP_E_INVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return EMP_E_CUDA;
+    }
+    if (device < 0) {
+        if (cudaGetDevice(&device) != cudaSuccess) return EMP_E_CUDA;
+    }
+    if (device >= ndev) return EMP_E_INVAL;
+    if (cudaSetDevice(device) != cudaSuccess) return EMP_E_CUDA;
+    emp_ctx *c = new (std::nothrow) emp_ctx();
+    if (!c) return EMP_E_NOMEM;
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return EMP_E_CUDA;
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, sizeof(HashTables)) != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return EMP_E_NOMEM;
+    }
+    c->tables.p = p;
+    c->tables.bytes = sizeof(HashTables);
+    HashTables h;
+    host_tables(h);
+    if (cudaMemcpy(p, &h, sizeof h, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return EMP_E_CUDA;
+    }
+    *out = c;
+    return EMP_OK;
+}
+
+emp_status emp_ctx_destroy(emp_ctx *ctx) {
+    if (!ctx) return EMP_E_INVAL;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return EMP_OK;
+}
+
+emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out) {
+    if (!ctx || !out) return EMP_E_INVAL;
+    emp_job *j = new (std::nothrow) emp_job();
+    if (!j) return EMP_E_NOMEM;
+    j->ctx = ctx;
+    if (p) j->p = *p;
+    else emp_params_default(&j->p);
+    *out = j;
+    return EMP_OK;
+}
+
+emp_status emp_job_destroy(emp_job *job) {
+    if (!job) return EMP_E_INVAL;
+    cudaSetDevice(job->ctx->device);
+    cudaStreamSynchronize(job->ctx->stream);
+    DevBuf *bufs[] = {&job->fq, &job->tile_counts, &job->tile_excl, &job->status, &job->misc, &job->seq_start,
+                      &job->seq_end, &job->hq, &job->idx, &job->rec_of, &job->keys0, &job->cols, &job->sk0,
+                      &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
+                      &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
+                      &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts};
+    for (DevBuf *b : bufs) free_buf(job, *b);
+    delete job;
+    return EMP_OK;
+}
+
+emp_status emp_job_reserve(emp_job *job, uint64_t bytes) {
+    if (!job) return EMP_E_INVAL;
+    if (bytes <= job->fq.bytes) return EMP_OK;
+    cudaSetDevice(job->ctx->device);
+    DevBuf nb;
+    emp_ctx *c = job->ctx;
+    if (c->budget && c->in_use + bytes > c->budget) return EMP_E_NOMEM;
+    if (cudaMalloc(&nb.p, bytes + 16) != cudaSuccess) {
+        cudaGetLastError();
+        return EMP_E_NOMEM;
+    }
+    nb.bytes = bytes + 16;
+    c->in_use += nb.bytes;
+    if (job->F) {
+        if (cudaMemcpyAsync(nb.p, job->fq.p, job->F, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess ||
+            cudaStreamSynchronize(c->stream) != cudaSuccess)
+            return EMP_E_CUDA;
+    }
+    free_buf(job, job->fq);
+    job->fq.p = nb.p;
+    job->fq.bytes = nb.bytes;
+    nb.p = nullptr;
+    nb.bytes = 0;
+    return EMP_OK;
+}
+
+static emp_status feed(emp_job *job, const void *src, uint64_t n, int last, cudaMemcpyKind kind) {
+    if (!job || (n && !src)) return EMP_E_INVAL;
+    if (job->fed_last) return EMP_E_STATE;
+    cudaSetDevice(job->ctx->device);
+    if (job->F + n > job->fq.bytes) {
+        uint64_t want = job->F + n;
+        if (!last) want += want / 2;
+        EMP_TRY(emp_job_reserve(job, want));
+    }
+    if (n) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, job->ctx->stream);
+        cudaError_t e = cudaMemcpyAsync(job->fq.as<uint8_t>() + job->F, src, n, kind, job->ctx->stream);
+        cudaEventRecord(b, job->ctx->stream);
+        cudaError_t e2 = cudaStreamSynchronize(job->ctx->stream);
+        if (kind == cudaMemcpyHostToDevice) job->ms_h2d += ms_between(a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (e != cudaSuccess || e2 != cudaSuccess) return EMP_E_CUDA;
+        job->F += n;
+    }
+    if (last) job->fed_last = true;
+    return EMP_OK;
+}
+
+emp_status emp_job_feed_fastq(emp_job *job, const char *bytes, uint64_t n, int last) {
+    return feed(job, bytes, n, last, cudaMemcpyHostToDevice);
+}
+
+emp_status emp_job_feed_fastq_device(emp_job *job, const void *dev_bytes, uint64_t n, int last) {
+    return feed(job, dev_bytes, n, last, cudaMemcpyDeviceToDevice);
+}
+
+emp_status emp_job_run(emp_job *job, void *stream) {
+    if (!job) return EMP_E_INVAL;
+    if (cudaSetDevice(job->ctx->device) != cudaSuccess) return EMP_E_CUDA;
+    cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : job->ctx->stream;
+    emp_status st = run_job(job, s);
+    if (st != EMP_OK) {
+        cudaStreamSynchronize(s);
+        cudaGetLastError();
+        job->have_result = false;
+    }
+    return st;
+}
+
+emp_status emp_job_output_size(emp_job *job, uint64_t *bytes) {
+    if (!job || !bytes) return EMP_E_INVAL;
+    if (!job->have_result) return EMP_E_STATE;
+    *bytes = job->out.size();
+    return EMP_OK;
+}
+
+emp_status emp_job_output_copy(emp_job *job, void *dst, uint64_t cap) {
+    if (!job || (!dst && job->out.size())) return EMP_E_INVAL;
+    if (!job->have_result) return EMP_E_STATE;
+    if (cap < job->out.size()) return EMP_E_INVAL;
+    if (job->out.size()) std::memcpy(dst, job->out.data(), job->out.size());
+    return EMP_OK;
+}
+
+emp_status emp_job_stats(emp_job *job, emp_stats *st) {
+    if (!job || !st) return EMP_E_INVAL;
+    if (!job->have_result) return EMP_E_STATE;
+    *st = job->st;
+    return EMP_OK;
+}
+
+emp_status emp_job_fingerprints(emp_job *job, uint64_t *keys, uint64_t cap, uint64_t *n_ends) {
+    if (!job || !n_ends) return EMP_E_INVAL;
+    if (!job->have_result) return EMP_E_STATE;
+    *n_ends = job->n_ends;
+    if (!job->n_ends || (!keys && cap == 0)) return EMP_OK;  // size query
+    if (!keys || cap < job->n_ends) return EMP_E_INVAL;
+    cudaSetDevice(job->ctx->device);
+    if (cudaMemcpy(keys, job->keys0.p, job->n_ends * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return EMP_E_CUDA;
+    return EMP_OK;
+}
+
+emp_status emp_run_file(const char *input_path, const char *output_path, const emp_params *p, int device,
+                        emp_stats *stats) {
+    if (!input_path || !output_path) return EMP_E_INVAL;
+    emp_ctx *ctx = nullptr;
+    EMP_TRY(emp_ctx_create(device, 0, &ctx));
+    emp_job *job = nullptr;
+    emp_status st = emp_job_create(ctx, p, &job);
+    if (st != EMP_OK) {
+        emp_ctx_destroy(ctx);
+        return st;
+    }
+    // read the input (a missing file reads as empty, like the reference's ifstream)
+    FILE *f = std::fopen(input_path, "rb");
+    if (f) {
+        std::fseek(f, 0, SEEK_END);
+        long sz = std::ftell(f);
+        std::fseek(f, 0, SEEK_SET);
+        if (sz > 0) {
+            PinnedBuf hb;
+            const size_t chunk = 256ull << 20;
+            if (!hb.ensure(chunk)) st = EMP_E_NOMEM;
+            if (st == EMP_OK) st = emp_job_reserve(job, (uint64_t)sz);
+            uint64_t left = (uint64_t)sz;
+            while (st == EMP_OK && left) {
+                size_t want = left < chunk ? (size_t)left : chunk;
+                size_t got = std::fread(hb.p, 1, want, f);
+                if (got != want) { st = EMP_E_IO; break; }
+                left -= got;
+                st = emp_job_feed_fastq(job, hb.as<char>(), got, left == 0);
+            }
+        }
+        std::fclose(f);
+    }
+    if (st == EMP_OK) st = emp_job_run(job, nullptr);
+    if (st == EMP_OK) {
+        FILE *g = std::fopen(output_path, "wb");
+        if (!g) st = EMP_E_IO;
+        else {
+            if (!job->out.empty() && std::fwrite(job->out.data(), 1, job->out.size(), g) != job->out.size())
+                st = EMP_E_IO;
+            if (std::fclose(g) != 0) st = EMP_E_IO;
+        }
+        if (stats) *stats = job->st;
+    }
+    emp_job_destroy(job);
+    emp_ctx_destroy(ctx);
+    return st;
+}
+
+emp_status emp_sort_pairs(emp_ctx *ctx, uint64_t *d_keys, uint32_t *d_vals, uint64_t n, void *stream) {
+    if (!ctx || (n && (!d_keys || !d_vals))) return EMP_E_INVAL;
+    if (n < 2) return EMP_OK;
+    if (n >= (1ull << 30)) return EMP_E_UNSUPPORTED;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
+    void *k1 = nullptr, *v1 = nullptr, *scr = nullptr, *err = nullptr;
+    emp_status st = EMP_OK;
+    if (cudaMalloc(&k1, n * 8) != cudaSuccess || cudaMalloc(&v1, n * 4) != cudaSuccess ||
+        cudaMalloc(&scr, sort_scratch_bytes(n)) != cudaSuccess || cudaMalloc(&err, 8) != cudaSuccess) {
+        cudaGetLastError();
+        st = EMP_E_NOMEM;
+    }
+    if (st == EMP_OK) {
+        cudaMemsetAsync(err, 0, 8, s);
+        int res = sort_pairs(d_keys, d_vals, (uint64_t *)k1, (uint32_t *)v1, n, scr, nullptr, (uint32_t *)err, s);
+        if (res) {
+            cudaMemcpyAsync(d_keys, k1, n * 8, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(d_vals, v1, n * 4, cudaMemcpyDeviceToDevice, s);
+        }
+        uint32_t herr = 0;
+        cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) st = EMP_E_CUDA;
+        else if (herr & kErrSpin) st = EMP_E_TIMEOUT;
+    }
+    if (k1) cudaFree(k1);
+    if (v1) cudaFree(v1);
+    if (scr) cudaFree(scr);
+    if (err) cudaFree(err);
+    return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+// kernels.h -- host-side launchers of the overlap-path kernels (internal).
+#pragma once
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace emp {
+
+// Kernels launched by this library since load (every launcher adds its count).
+extern std::atomic<uint64_t> g_launches;
+inline void count_launch(uint64_t k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+// ---- generic single-pass exclusive scan (k_scan.cu) ----------------------
+constexpr uint32_t kScanTile = 4096;  // u32 inputs per tile
+__host__ __device__ inline uint64_t scan_tiles(uint64_t n) { return (n + kScanTile - 1) / kScanTile; }
+// out[i] = sum(in[0..i)); *total = sum(in).  status: scan_tiles(n) u64,
+// tile_ctr: one u32; both must be zero.  out may alias in.
+void launch_scan_u32_u64(const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *status, uint32_t *tile_ctr,
+                         uint64_t *total, uint32_t *err, cudaStream_t s);
+void launch_scan_u32_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint64_t *status, uint32_t *tile_ctr,
+                         uint64_t *total, uint32_t *err, cudaStream_t s);
+
+// ---- map phase (k_map.cu) -------------------------------------------------
+constexpr uint64_t kParseTile = 16384;  // FASTQ bytes per tile
+__host__ __device__ inline uint64_t parse_tiles(uint64_t F) { return (F + kParseTile - 1) / kParseTile; }
+void launch_nl_count(const uint8_t *fq, uint64_t F, uint32_t *tile_counts, cudaStream_t s);
+void launch_nl_locate(const uint8_t *fq, uint64_t F, const uint64_t *tile_excl, uint64_t *seq_start,
+                      uint64_t *seq_end, cudaStream_t s);
+void launch_classify(const uint8_t *fq, const uint64_t *seq_start, const uint64_t *seq_end, uint64_t n_rec,
+                     uint32_t *hq, uint32_t *len_minmax, uint32_t *err, cudaStream_t s);
+void launch_scatter_hq(const uint32_t *hq, const uint32_t *idx, uint64_t n_rec, uint32_t *rec_of, cudaStream_t s);
+// keys[2i] / keys[2i+1] = fingerprint of read i / of its reverse complement;
+// cols[c * wpc + i/16] holds base c of read i at bits 2*(i%16).
+void launch_fingerprint_pack(const uint8_t *fq, const uint64_t *seq_start, const uint32_t *rec_of, uint64_t n,
+                             int L, const HashTables *tables, uint64_t *keys, uint32_t *cols, uint64_t wpc,
+                             cudaStream_t s);
+
+// ---- radix sort (k_sort.cu) ---------------------------------------------
+constexpr int kSortBits = 8;
+constexpr int kSortRadix = 1 << kSortBits;
+constexpr int kSortPasses = 8;           // 59-bit sort keys
+constexpr uint32_t kSortTile = 4096;
+__host__ __device__ inline uint64_t sort_tiles(uint64_t n) { return (n + kSortTile - 1) / kSortTile; }
+// bytes of zero-initialised scratch a sort of n pairs needs (look-back words,
+// tile counters, histograms)
+size_t sort_scratch_bytes(uint64_t n);
+// Stable sort of (keys, vals) by sort_key(key, val).  Ping-pongs between
+// (k0,v0) and (k1,v1); returns 0 if the result is in (k0,v0), 1 otherwise.
+// hist_host (optional, kSortPasses*kSortRadix u32 pinned) enables skipping
+// passes whose digit is constant (costs one stream synchronisation).
+int sort_pairs(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, uint64_t n, void *scratch,
+               uint32_t *hist_host, uint32_t *err, cudaStream_t s);
+
+// ---- rounds (k_round.cu) --------------------------------------------------
+void launch_dedup_mark(const uint64_t *skeys, const uint32_t *svals, uint64_t n2, uint8_t *alive, cudaStream_t s);
+// rid order (evens ascending, then odds ascending) of the alive read-ends
+void launch_init_list(const uint64_t *keys0, const uint8_t *alive, uint64_t n, uint64_t *lkeys, uint32_t *lvals,
+                      uint64_t *status, uint32_t *tile_ctr, uint64_t *count, uint32_t *err, cudaStream_t s);
+void launch_dup_prefix_half(uint64_t *lkeys, uint32_t *lvals, uint64_t u, cudaStream_t s);
+void launch_iota(uint32_t *v, uint64_t n, cudaStream_t s);
+constexpr uint32_t kUpdTile = 2048;
+__host__ __device__ inline uint64_t upd_tiles(uint64_t n) { return (n + kUpdTile - 1) / kUpdTile; }
+struct RoundArgs {
+    const uint64_t *kin;
+    const uint32_t *vin;
+    uint64_t n_in;
+    uint64_t *kout;
+    uint32_t *vout;
+    const uint8_t *used_s;
+    const uint8_t *used_p;
+    const uint32_t *cols;
+    uint64_t wpc;
+    const HashTables *tables;
+    int L;
+    int round;
+    uint64_t *status;
+    uint32_t *tile_ctr;
+    uint64_t *n_out;   // total survivors
+    uint64_t *s_out;   // survivors of the suffix table (must be zero)
+    uint32_t *err;
+};
+void launch_update_compact(const RoundArgs &a, cudaStream_t s);
+// Record splitting (cq_get_search_partitions, cqutils.cuh:108-137).
+// split_tables: sorted merged list -> sorted suffix keys (+ their merged
+// positions) and sorted prefix keys.
+void launch_split_tables(const uint64_t *skeys, const uint32_t *svals, uint64_t n, uint64_t *akeys, uint32_t *apos,
+                         uint64_t *bkeys, uint64_t *status, uint32_t *tile_ctr, uint32_t *err, cudaStream_t s);
+struct SearchPart {
+    uint64_t pa, pb;  // suffixes / prefixes in the partition
+    uint64_t e0, e1;  // its edges in the round's edge list
+};
+// One thread walks the reference's partition loop with windows of h = M/2.
+void launch_search_partitions(const uint64_t *akeys, uint64_t S, const uint64_t *bkeys, uint64_t P, uint64_t h,
+                              const uint32_t *apos, const uint64_t *offs, uint64_t E, SearchPart *parts,
+                              uint64_t cap, uint64_t *count, uint32_t *err, cudaStream_t s);
+void launch_join_count(const uint64_t *skeys, const uint32_t *svals, uint64_t n, uint32_t *cnt, cudaStream_t s);
+void launch_join_write(const uint64_t *skeys, const uint32_t *svals, uint64_t n, const uint32_t *cnt,
+                       const uint64_t *offs, uint32_t *from, uint32_t *to, uint8_t *used_s, uint8_t *used_p,
+                       cudaStream_t s);
+
+}  // namespace emp

@@ -1,0 +1,142 @@
+/*
+ * empanada.h -- C ABI of the B200 read-overlap engine (libempanada_b200.so).
+ *
+ * Drop-in for empanada's read-overlap path: FASTQ -> 2-bit bases ->
+ * Rabin-Karp fingerprints of every read-end -> sort -> per-round
+ * suffix/prefix join -> output.bin.  The reference has no FFI; its seams are
+ * the process CLI (config.h:120-140, main.cu:9-77), the output.bin format
+ * (overlap.cu:148-161) and the internal C++ functions of assembly.cuh:67-82.
+ * Each entry point below names the reference code it replaces.
+ *
+ * Conventions: plain pointers and sizes, no exceptions and no exit() across
+ * the ABI; every call returns an emp_status (0 = OK, < 0 = error).  A context
+ * or job is driven by one host thread at a time; distinct jobs may be driven
+ * from distinct threads.  Every device wait inside the engine is bounded and
+ * reports EMP_E_TIMEOUT instead of hanging.
+ *
+ * output.bin: a sequence of records, little-endian, no header:
+ *     u64 n | i32 ovlp_len | u32 from[n] | u32 to[n]
+ * one record per (round, search partition) that has both suffixes and
+ * prefixes, ovlp_len = L-1-round, ids rid = 2i (read i) / 2i+1 (its reverse
+ * complement), i counting reads without N in file order.
+ */
+#ifndef EMPANADA_H
+#define EMPANADA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EMP_ABI_VERSION 1
+
+typedef int emp_status;
+#define EMP_OK 0
+#define EMP_E_INVAL (-1)       /* bad argument (reference: usage / LOG_ERR) */
+#define EMP_E_NOMEM (-2)       /* device or host allocation failed, or over the HBM budget */
+#define EMP_E_CUDA (-3)        /* CUDA runtime error (reference: CUDA_SAFE -> exit(1)) */
+#define EMP_E_TIMEOUT (-4)     /* a bounded device wait ran out */
+#define EMP_E_FORMAT (-5)      /* kept reads of unequal length, or a base outside ACGTacgt */
+#define EMP_E_STATE (-6)       /* call out of order (e.g. feed after run) */
+#define EMP_E_IO (-7)          /* file could not be read or written */
+#define EMP_E_UNSUPPORTED (-8) /* read length above 255 (reference: undefined) */
+#define EMP_E_HANG (-9)        /* input on which the reference never terminates */
+
+typedef struct emp_ctx emp_ctx;
+typedef struct emp_job emp_job;
+
+/* The reference's command-line options (config.h:282-290). */
+typedef struct emp_params {
+    int32_t min_ovlp;      /* -o, minimum overlap length (default 31) */
+    uint64_t map_mem;      /* -m, bytes (default 1g); FASTQ block = map_mem/16 (main.cu:16) */
+    uint64_t reduce_mem;   /* -r, bytes (default 1g); M = reduce_mem/16 pairs (main.cu:69) */
+    uint64_t base_blocksz; /* -b, bytes (default 32m) */
+    uint64_t kv_chunksz;   /* -c, count (default 64m) */
+} emp_params;
+
+#define EMP_MAX_ROUNDS 256
+
+typedef struct emp_stats {
+    uint64_t n_reads;      /* reads kept after the N filter */
+    int32_t read_len;      /* L */
+    int32_t n_rounds;      /* rounds executed */
+    uint64_t n_unique;     /* read-ends after duplicate removal */
+    uint64_t n_edges;      /* edges written */
+    uint64_t n_records;    /* output.bin records */
+    uint64_t fastq_bytes;  /* input size */
+    uint64_t output_bytes; /* output.bin size */
+    uint64_t gpu_launches; /* engine kernels launched by the last run */
+    double ms_h2d;         /* FASTQ host->device copy (0 for device input) */
+    double ms_map;         /* parse + fingerprint + column store (device time) */
+    double ms_dedup;       /* fingerprint sort + duplicate removal (device time) */
+    double ms_rounds;      /* overlap rounds (device time, incl. edge copies) */
+    double ms_total;       /* whole run (device time) */
+    uint64_t sfx_live[EMP_MAX_ROUNDS]; /* suffix-table size in round r */
+    uint64_t pfx_live[EMP_MAX_ROUNDS]; /* prefix-table size in round r */
+    uint64_t edges[EMP_MAX_ROUNDS];    /* edges written in round r */
+} emp_stats;
+
+/* Human-readable name of a status code. */
+const char *emp_status_string(emp_status st);
+int emp_abi_version(void);
+
+/* Defaults of config.h:285-289 (o=31, m=1g, r=1g, b=32m, c=64m). */
+emp_status emp_params_default(emp_params *p);
+
+/* hmsize2bytes (config.h:75-100): digits with an optional k/K/m/M/g/G
+ * binary suffix.  An unknown suffix is reported and ignored, like the
+ * reference (value returned without the suffix, status EMP_E_INVAL). */
+emp_status emp_parse_size(const char *s, uint64_t *bytes);
+
+/* A context owns one device (cudaSetDevice), its stream and hash tables.
+ * hbm_budget_bytes = 0: no budget.  Replaces the process-wide singletons and
+ * precomputeModulos/init_match (fingerprint.cu:26-34, overlap.cu:117-127). */
+emp_status emp_ctx_create(int device, uint64_t hbm_budget_bytes, emp_ctx **out);
+emp_status emp_ctx_destroy(emp_ctx *ctx);
+
+/* One job = one read set with the reference's options. */
+emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out);
+emp_status emp_job_destroy(emp_job *job);
+
+/* Append FASTQ bytes (host memory, any split, records may straddle calls);
+ * replaces read_block's file reads (preprocess.cu:195-237).  `last` marks
+ * the final piece. */
+emp_status emp_job_feed_fastq(emp_job *job, const char *bytes, uint64_t n, int last);
+/* Same for bytes already in device memory on the context's device. */
+emp_status emp_job_feed_fastq_device(emp_job *job, const void *dev_bytes, uint64_t n, int last);
+/* Reserve device room for `bytes` of FASTQ (optional; avoids regrowth). */
+emp_status emp_job_reserve(emp_job *job, uint64_t bytes);
+
+/* Map + reduce phases: main.cu:42-71 (read_block, transpose_reads,
+ * get_reverse_complements, generate_fingerprint_read_pairs) and build_graph
+ * (overlap.cu:206-293).  stream: a cudaStream_t, or NULL for the context's. */
+emp_status emp_job_run(emp_job *job, void *stream);
+
+/* output.bin bytes of the last run (write_edges_binary, overlap.cu:148-161). */
+emp_status emp_job_output_size(emp_job *job, uint64_t *bytes);
+emp_status emp_job_output_copy(emp_job *job, void *dst, uint64_t cap);
+emp_status emp_job_stats(emp_job *job, emp_stats *st);
+
+/* Full-length fingerprints of every read-end of the last run, indexed by
+ * read-end id (generate_fingerprint_read_pairs, fingerprint.cu:75-115).
+ * keys = NULL with cap = 0 only reports *n_ends. */
+emp_status emp_job_fingerprints(emp_job *job, uint64_t *keys, uint64_t cap, uint64_t *n_ends);
+
+/* The whole reference program (main.cu:9-77): read input_path, write
+ * output_path.  A missing input file gives an empty output.bin, as in the
+ * reference.  device < 0: current device. */
+emp_status emp_run_file(const char *input_path, const char *output_path, const emp_params *p, int device,
+                        emp_stats *st);
+
+/* Stable sort of n (key, value) pairs in device memory by
+ * (fp1, fp2, value>>31) -- the key order of thrust::sort_by_key on the
+ * reference's fingerprints (cqutils.cuh:195).  Allocates its scratch.
+ * stream: a cudaStream_t or NULL. */
+emp_status emp_sort_pairs(emp_ctx *ctx, uint64_t *d_keys, uint32_t *d_vals, uint64_t n, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -158,7 +158,6 @@ int emp_oracle_parse(const char *fq, size_t len, char **reads_out, uint64_t *n_o
                     if (!is_acgt(fq[j])) { free(reads); return EMP_ORACLE_E_FORMAT; }
                 if (L < 0) L = (int32_t)(sl > (size_t)INT32_MAX ? INT32_MAX : sl);
                 if ((size_t)L != sl) { free(reads); return EMP_ORACLE_E_FORMAT; }
-                if (L > MAX_RD_LEN) { free(reads); return EMP_ORACLE_E_UNSUPPORTED; }
                 if (used + sl > cap) {
                     while (used + sl > cap) cap *= 2;
                     char *nr = (char *)realloc(reads, cap);
@@ -173,6 +172,8 @@ int emp_oracle_parse(const char *fq, size_t len, char **reads_out, uint64_t *n_o
         ++line;
         pos = e + 1;
     }
+    /* format errors anywhere in the file take precedence over the length limit */
+    if (n && L > MAX_RD_LEN) { free(reads); return EMP_ORACLE_E_UNSUPPORTED; }
     *reads_out = reads;
     *n_out = n;
     *L_out = n ? L : 0;

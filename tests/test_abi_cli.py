@@ -1,0 +1,112 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports every
+function include/empanada.h declares, the size parser and defaults follow
+config.h, and the `empanada` command reproduces the reference's argument
+handling (config.h:10-140)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+import empanada_b200
+from empanada_b200 import _native, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "empanada.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(emp_[a-z_0-9]+)\s*\(", text, flags=re.M)))
+
+
+def test_header_declarations_are_exported():
+    names = declared_functions()
+    assert len(names) >= 18
+    lib = ctypes.CDLL(_native.LIB_PATH)
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_native.SIGNATURES), "binding table out of sync with the header"
+
+
+def test_abi_version_and_status_strings():
+    lib = _native.lib()
+    assert lib.emp_abi_version() == 1
+    for code in range(0, -10, -1):
+        assert lib.emp_status_string(code)
+    assert _native.status_string(_native.EMP_E_FORMAT).startswith("reads of unequal length")
+
+
+def test_params_default_matches_config_h():
+    p = _native.Params()
+    assert _native.lib().emp_params_default(ctypes.byref(p)) == 0
+    assert (p.min_ovlp, p.map_mem, p.reduce_mem, p.base_blocksz, p.kv_chunksz) == (31, 1 << 30, 1 << 30, 32 << 20,
+                                                                                   64 << 20)
+
+
+@pytest.mark.parametrize("s,v", [("31", 31), ("0", 0), ("1k", 1024), ("1K", 1024), ("16m", 16 << 20),
+                                 ("12g", 12 << 30), ("8G", 8 << 30), ("5x", 5)])
+def test_parse_size(s, v):
+    assert empanada_b200.parse_size(s) == v
+
+
+def test_parse_size_rejects_garbage():
+    with pytest.raises(empanada_b200.EmpError):
+        empanada_b200.parse_size("abc")
+
+
+def test_python_parse_args_quirks():
+    c = empanada_b200.parse_args(["in.fq", "out.bin"])
+    assert (c.min_ovlp, c.reduce_mem, c.base_blocksz) == (31, 1 << 30, 32 << 20)
+    c = empanada_b200.parse_args(["in.fq", "out.bin", "-o", "75", "-m", "8g", "-r", "12g", "-b", "16m", "-c", "64m"])
+    assert (c.min_ovlp, c.map_mem, c.reduce_mem, c.base_blocksz, c.kv_chunksz) == (75, 8 << 30, 12 << 30, 16 << 20,
+                                                                                   64 << 20)
+    c = empanada_b200.parse_args(["in.fq", "out.bin", "xo", "40"])  # matched on the 2nd character
+    assert c.min_ovlp == 40
+    with pytest.raises(empanada_b200.UsageExit):
+        empanada_b200.parse_args(["in.fq"])
+    with pytest.raises(empanada_b200.UsageExit):
+        empanada_b200.parse_args(["in.fq", "out.bin", "-z", "1"])
+    with pytest.raises(empanada_b200.UsageExit):
+        empanada_b200.parse_args(["in.fq", "out.bin", "--min-overlap", "1"])
+
+
+def _cli(args, cwd=None):
+    return subprocess.run([build.CLI] + args, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, cwd=cwd,
+                          timeout=60)
+
+
+def test_cli_usage_exits_zero():
+    for args in ([], ["in.fq"], ["in.fq", "out.bin", "-z", "3"], ["in.fq", "out.bin", "--min-overlap", "3"]):
+        p = _cli(args)
+        assert p.returncode == 0, args
+        assert p.stdout.strip().endswith("default = 64m")
+        assert "Usage: assembly_v3 [input fastq] [output gfa] [options]" in p.stdout
+    p = _cli(["in.fq", "out.bin", "-z", "3"])
+    assert p.stdout.startswith("Invalid option -z")
+    p = _cli(["in.fq", "out.bin", "--min-overlap", "3"])
+    assert "Not implemented yet. Use short forms instead." in p.stderr
+
+
+def test_cli_option_without_value_fails():
+    p = _cli(["in.fq", "out.bin", "-o"])
+    assert p.returncode == 1
+
+
+@pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES") is None and os.path.exists("/dev/nvidia0"),
+                    reason="GPU present: covered by the GPU tests")
+def test_cli_without_gpu_fails_cleanly(tmp_path):
+    fq = tmp_path / "in.fq"
+    fq.write_bytes(b"@r0\nACGT\n+\nIIII\n")
+    p = _cli([str(fq), str(tmp_path / "out.bin")], cwd=str(tmp_path))
+    assert p.returncode == 1
+    assert "CUDA error" in p.stderr
+
+
+def test_engine_without_gpu_raises():
+    if os.path.exists("/dev/nvidia0"):
+        pytest.skip("GPU present")
+    with pytest.raises(empanada_b200.EmpError):
+        empanada_b200.Engine(0)

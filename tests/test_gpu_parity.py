@@ -1,0 +1,76 @@
+"""CUDA path vs the reference's own output (golden digests) and the oracle.
+
+Every case of tests/golden/cases.py runs through the C ABI (emp_job_*); the
+output.bin bytes must equal the reference's (sha256 from golden.json, and the
+verbatim fixture where committed) and the oracle's.
+"""
+import hashlib
+import json
+import os
+
+import pytest
+
+import empanada_b200
+from cases import BY_NAME, CASES
+from oracle import bind
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GOLDEN = json.load(open(os.path.join(HERE, "golden.json")))
+
+FAST_CASES = [c.name for c in CASES if not c.big and c.name != "out_of_core_r16k"]
+
+
+def _run(engine, case):
+    data = case.fastq()
+    a = list(case.args)
+    opts = dict(zip(a[::2], a[1::2]))
+    out, st = empanada_b200.run_bytes(
+        data, engine=engine, min_ovlp=int(opts.get("-o", 31)), map_mem=opts.get("-m", "1g"),
+        reduce_mem=opts.get("-r", "1g"), base_blocksz=opts.get("-b", "32m"), kv_chunksz=opts.get("-c", "64m"))
+    return data, out, st
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", FAST_CASES)
+def test_case_matches_reference(engine, name):
+    case = BY_NAME[name]
+    g = GOLDEN[name]
+    data, out, st = _run(engine, case)
+    assert hashlib.sha256(data).hexdigest() == g["fastq_sha256"], "input generator drifted"
+    assert len(out) == g["size"]
+    assert hashlib.sha256(out).hexdigest() == g["sha256"]
+    if g.get("inline"):
+        assert out == open(os.path.join(HERE, f"{name}.bin"), "rb").read()
+    ref, rst = bind.run(data, case.min_ovlp(), case.reduce_mem())
+    assert out == ref
+    assert st["n_edges"] == rst["n_edges"]
+    assert st["n_records"] == rst["n_records"]
+    assert st["n_unique"] == rst["n_unique"]
+    assert st["gpu_launches"] > 0 or st["n_reads"] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["small", "larger"])
+def test_full_size_workload_matches_reference(engine, name):
+    """Configs 1 and 2 at full size: byte-identical to the reference's output.bin."""
+    case = BY_NAME[name]
+    g = GOLDEN[name]
+    data, out, st = _run(engine, case)
+    assert hashlib.sha256(data).hexdigest() == g["fastq_sha256"]
+    assert st["n_edges"] == g["edges"]
+    assert st["n_records"] == g["records"]
+    assert len(out) == g["size"]
+    assert hashlib.sha256(out).hexdigest() == g["sha256"]
+
+
+@pytest.mark.gpu
+def test_fingerprints_match_oracle(engine):
+    for name in ["tiny", "odd_len", "lowercase", "read_len_255", "read_len_1", "dups_palindromes"]:
+        data = BY_NAME[name].fastq()
+        with engine.job(min_ovlp=BY_NAME[name].min_ovlp()) as job:
+            job.feed(data)
+            job.run()
+            got = job.fingerprints()
+        want, n, L = bind.fingerprints(data)
+        assert got.size == 2 * n
+        assert (got == want).all(), name
