@@ -1,0 +1,400 @@
+#!/usr/bin/env python
+"""Throughput of empanada's read-overlap path (fingerprint + sort + overlap) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: the "larger" read set (5 Mbp seeded genome, 1.2M reads x 250 bp,
+0.1 % substitutions, -o 75 -m 8g -r 12g -b 16m -c 64m), generated on the host
+by the seeded C generator.  A step is one complete job over that read set.
+
+impl b200 (default), one process per GPU (torchrun for N > 1; replicas only,
+each rank runs its own job, no data-path collective):
+  value     reads/s with the FASTQ already in HBM: device time of emp_job_run
+            (CUDA events on the launching stream), L2 flushed before each step
+  e2e       reads/s through the C ABI with host buffers: emp_job_reset +
+            emp_job_feed_fastq (pinned host -> HBM) + emp_job_run + copy of
+            output.bin to host, wall clock per step
+  roofline  the radix-sort digit pass (dominant kernel): algorithmic bytes
+            (24 per pair: 12 read + 12 written) / its event-timed launch time,
+            against the measured HBM copy bandwidth
+  cpu_baseline  rank 0 at N=1: the reference's own sources built as a CPU
+            program (oracle/_ref, Thrust on OpenMP) on a bounded sample
+impl reference: that CPU build alone, timed per step on the bounded sample
+(rank 0 only under torchrun).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "reads/s (fingerprint+sort+overlap) on 1 B200; served-mix p50/p99 latency vs plain"
+CPU_SAMPLE_READS = 200_000
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(
+        os.environ.get("WORLD_SIZE", "1"))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_elem():
+    """DRAM bytes per pair of one digit pass from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "onesweep_traffic.json")
+    if os.path.exists(p):
+        try:
+            return float(json.load(open(p))["dram_bytes_per_pair"])
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(rows), "reasons": reasons}
+
+
+def cpu_reference_run(fastq_path: str, args: list[str], threads: int, cwd: str):
+    """One run of the reference CPU build; -> (compute seconds, wall seconds).
+    compute = wall minus the reference's own read_input rows of timings.csv."""
+    from oracle import bind
+
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    t0 = time.perf_counter()
+    p = subprocess.run([bind.REF_CPU, fastq_path, os.path.join(cwd, "out.bin")] + args, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL, env=env, cwd=cwd)
+    wall = time.perf_counter() - t0
+    if p.returncode != 0:
+        raise RuntimeError(f"reference CPU build exited {p.returncode}")
+    read_us = 0
+    tpath = os.path.join(cwd, "timings.csv")
+    if os.path.exists(tpath):
+        for line in open(tpath):
+            if line.startswith("read_input,"):
+                read_us += int(line.split(",")[1])
+    return max(wall - read_us / 1e6, 1e-9), wall
+
+
+def cpu_baseline_block(workload, steps: int = 1):
+    """Bounded sample of the workload through the reference CPU build (or the oracle port)."""
+    from empanada_b200 import synth
+    from oracle import bind
+
+    sample = workload.scaled(min(CPU_SAMPLE_READS, workload.n_reads))
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as td:
+        fq = os.path.join(td, "sample.fq")
+        synth.write_fastq(sample, fq)
+        if os.path.exists(bind.REF_CPU):
+            times = [cpu_reference_run(fq, workload.cli_args(), threads, td)[0] for _ in range(steps)]
+            kind, cores = "reference", threads
+        else:
+            data = open(fq, "rb").read()
+            times = []
+            for _ in range(steps):
+                t0 = time.perf_counter()
+                bind.run(data, workload.min_ovlp, 12 << 30)
+                times.append(time.perf_counter() - t0)
+            kind, cores = "port", 1
+    v = sample.n_reads / statistics.median(times)
+    return {"value": v, "unit": "reads/s", "cores": cores, "kind": kind,
+            "sample": f"first {sample.n_reads} reads of the workload (same genome and error model), "
+                      f"{'reference sources built with Thrust on OpenMP' if kind == 'reference' else 'oracle C port'}; "
+                      f"compute time = wall minus the reference's read_input; median of {len(times)}"}, times
+
+
+def run_reference_arm(args, workload):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return
+    from oracle import bind
+    from empanada_b200 import synth
+
+    sample = workload.scaled(min(CPU_SAMPLE_READS, workload.n_reads))
+    threads = os.cpu_count() or 1
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        fq = os.path.join(td, "sample.fq")
+        synth.write_fastq(sample, fq)
+        have_ref = os.path.exists(bind.REF_CPU)
+        data = None if have_ref else open(fq, "rb").read()
+        for i in range(args.warmup + args.steps):
+            if have_ref:
+                t = cpu_reference_run(fq, workload.cli_args(), threads, td)[0]
+            else:
+                t0 = time.perf_counter()
+                bind.run(data, workload.min_ovlp, 12 << 30)
+                t = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(t)
+    total = sum(times)
+    v = sample.n_reads * len(times) / total
+    kind = "reference" if have_ref else "port"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "reads/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded generator empanada_b200/csrc/synth_reads.c)",
+            "config": {"workload": workload.name, "sample_reads": sample.n_reads, "read_len": workload.read_len,
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": "reads/s", "cores": threads if have_ref else 1, "kind": kind,
+                             "sample": f"first {sample.n_reads} reads of the workload per step"},
+            "e2e": {"value": v, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def sort_microbench(args):
+    """The radix sort alone (emp_sort_pairs) on N random (fingerprint, id) pairs."""
+    import numpy as np
+    import torch
+
+    import empanada_b200
+
+    n = args.pairs
+    rng = np.random.default_rng(0)
+    f1 = rng.integers(0, 536870909, size=n, dtype=np.uint64)
+    f2 = rng.integers(0, 536870879, size=n, dtype=np.uint64)
+    keys = torch.from_numpy(((f1 << np.uint64(32)) | f2).view(np.int64)).cuda()
+    vals = torch.arange(n, dtype=torch.int32).cuda()
+    wk, wv = keys.clone(), vals.clone()
+    eng = empanada_b200.Engine(0)
+    stream = torch.cuda.current_stream()
+    ms = []
+    for i in range(args.warmup + args.steps):
+        wk.copy_(keys)
+        wv.copy_(vals)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.sort_pairs(wk.data_ptr(), wv.data_ptr(), n, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    peak, kind = measured_peaks()
+    med = statistics.median(ms)
+    print(json.dumps({"kernel": "emp_sort_pairs", "pairs": n, "ms_median": med, "pairs_per_s": n / med * 1e3,
+                      "bytes_per_pair_algorithmic": 12 + 8 * 24, "achieved_GBps": (12 + 8 * 24) * n / med / 1e6,
+                      "peak_GBps": peak, "peak_source": kind}), flush=True)
+    eng.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="larger")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", default=None, choices=[None, "sort"],
+                    help="microbenchmark one kernel instead of the whole path")
+    ap.add_argument("--pairs", type=int, default=1 << 24)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    from empanada_b200 import synth
+
+    workload = synth.WORKLOADS[args.workload]
+    if args.kernel == "sort":
+        sort_microbench(args)
+        return
+    if args.impl == "reference":
+        run_reference_arm(args, workload)
+        return
+
+    import numpy as np
+    import torch
+
+    import empanada_b200
+
+    rank, local_rank, world = env_rank()
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local_rank
+    torch.cuda.set_device(device)
+
+    F = synth.fastq_size(workload)
+    host = torch.empty(F, dtype=torch.uint8, pin_memory=True)
+    host_np = host.numpy()
+    synth.fastq_into(workload, host_np)
+    out_host = torch.empty(64 << 20, dtype=torch.uint8, pin_memory=True).numpy()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")  # > 126 MB L2
+
+    eng = empanada_b200.Engine(device)
+    params = dict(min_ovlp=workload.min_ovlp, map_mem=workload.map_mem, reduce_mem=workload.reduce_mem,
+                  base_blocksz=workload.base_blocksz, kv_chunksz=workload.kv_chunksz)
+    stream = torch.cuda.current_stream(device)
+    sptr = stream.cuda_stream
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if dist is not None:
+            dist.barrier()
+
+    # ---- value: FASTQ resident in HBM, device time of the whole job
+    job = eng.job(**params)
+    job.reserve(F)
+    job.feed(host_np, last=True)
+    for _ in range(args.warmup):
+        flush.zero_()
+        job.run(sptr)
+    barrier()
+    step_ms = []
+    launches = 0
+    sort_ms = 0.0
+    sort_elems = 0
+    sort_passes = 0
+    with ClockSampler(device) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            job.run(sptr)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            st = job.stats()
+            launches += st["gpu_launches"]
+            sort_ms += st["ms_sort_passes"]
+            sort_elems += st["sort_pass_elems"]
+            sort_passes += st["sort_passes"]
+    barrier()
+    clocks = clk.summary()
+    total_ms = sum(step_ms)
+    out_bytes = st["output_bytes"]
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * workload.n_reads * args.steps / (total_ms / 1000.0)
+    job.close()
+
+    # ---- e2e: host FASTQ in, output.bin out, through the C ABI
+    job = eng.job(**params)
+    job.reserve(F)
+    e2e_s = []
+    for i in range(args.warmup + args.steps):
+        barrier()
+        t0 = time.perf_counter()
+        job.reset()
+        job.feed(host_np, last=True)
+        job.run()
+        n_out = job.output_into(out_host)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_s.append(dt)
+    job.close()
+    e2e_total = sum(e2e_s)
+    if dist is not None:
+        t = torch.tensor([e2e_total], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * workload.n_reads * len(e2e_s) / e2e_total
+
+    peak, peak_kind = measured_peaks()
+    achieved = (24.0 * sort_elems) / (sort_ms / 1000.0) / 1e9 if sort_ms > 0 else 0.0
+    tpe = traffic_per_elem()
+    per_launch_elems = sort_elems / max(sort_passes, 1)
+    roofline = {"bound": "hbm", "kernel": "onesweep_kernel (radix-sort digit pass)", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} (HBM copy)",
+                "traffic": (tpe * per_launch_elems) if tpe else None,
+                "algorithmic_bytes_per_launch": 24.0 * per_launch_elems,
+                "avg_launch_us": 1000.0 * sort_ms / max(sort_passes, 1), "launches": sort_passes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu, _ = cpu_baseline_block(workload, steps=1)
+        except Exception as e:  # reported, never fatal
+            cpu = {"value": None, "unit": "reads/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                "data": "synthetic (seeded generator empanada_b200/csrc/synth_reads.c)",
+                "config": {"workload": workload.name, "reads": workload.n_reads, "read_len": workload.read_len,
+                           "fastq_bytes": F, "options": " ".join(workload.cli_args()),
+                           "l2": "input (FASTQ) larger than L2; 256 MB L2 flush before every timed step",
+                           "parallelism": f"replicas x{world}"},
+                "bases_per_s": value * workload.read_len,
+                "e2e": {"value": e2e_value, "unit": "reads/s", "h2d_bytes_per_step": F, "d2h_bytes_per_step": n_out},
+                "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+                "job": {k: st[k] for k in ("n_reads", "n_unique", "n_edges", "n_records", "n_rounds", "ms_map",
+                                           "ms_dedup", "ms_rounds")},
+                "live_entries": int(sum(st["sfx_live"]) + sum(st["pfx_live"]))}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

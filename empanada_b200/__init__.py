@@ -177,6 +177,10 @@ class Job:
     def reserve(self, nbytes: int) -> None:
         check(self._lib.emp_job_reserve(self.handle, nbytes), "emp_job_reserve")
 
+    def reset(self) -> None:
+        """Drop the fed input and last result; keep the device buffers."""
+        check(self._lib.emp_job_reset(self.handle), "emp_job_reset")
+
     def feed(self, data, last: bool = True) -> None:
         """Append host FASTQ bytes (bytes, bytearray or a uint8 numpy array)."""
         if isinstance(data, np.ndarray):

@@ -54,13 +54,16 @@ class Stats(ctypes.Structure):
         ("ms_dedup", ctypes.c_double),
         ("ms_rounds", ctypes.c_double),
         ("ms_total", ctypes.c_double),
+        ("ms_sort_passes", ctypes.c_double),
+        ("sort_passes", ctypes.c_uint64),
+        ("sort_pass_elems", ctypes.c_uint64),
         ("sfx_live", ctypes.c_uint64 * MAX_ROUNDS),
         ("pfx_live", ctypes.c_uint64 * MAX_ROUNDS),
         ("edges", ctypes.c_uint64 * MAX_ROUNDS),
     ]
 
     def to_dict(self) -> dict:
-        d = {f: getattr(self, f) for f, _ in self._fields_[:14]}
+        d = {f: getattr(self, f) for f, _ in self._fields_[:17]}
         r = self.n_rounds
         d["sfx_live"] = list(self.sfx_live[:r])
         d["pfx_live"] = list(self.pfx_live[:r])
@@ -80,6 +83,7 @@ SIGNATURES = {
     "emp_job_feed_fastq": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int]),
     "emp_job_feed_fastq_device": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int]),
     "emp_job_reserve": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "emp_job_reset": (ctypes.c_int, [_vp]),
     "emp_job_run": (ctypes.c_int, [_vp, _vp]),
     "emp_job_output_size": (ctypes.c_int, [_vp, _u64p]),
     "emp_job_output_copy": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64]),

@@ -84,6 +84,9 @@ struct emp_job {
     DevBuf sk0, sv0, sk1, sv1, alive, lk0, lv0, lk1, lv1, used_s, used_p, cnt, offs, efrom, eto, sort_scratch;
     DevBuf akeys, apos, bkeys, parts;  // record splitting
     PinnedBuf h_parts;
+    cudaEvent_t sort_ev[2 * kSortPasses] = {};
+    uint32_t sort_passes_run = 0;
+    uint64_t sort_n = 0;
     PinnedBuf h_misc, h_hist, h_from, h_to;
     uint64_t n_ends = 0;
     // results
@@ -171,6 +174,17 @@ emp_status sync_and_check(emp_job *j, cudaStream_t s) {
     return EMP_OK;
 }
 
+// fold the per-pass event times of the last sort into the stats (after a sync)
+void account_sort(emp_job *j) {
+    for (int p = 0; p < kSortPasses; ++p) {
+        if (!(j->sort_passes_run & (1u << p))) continue;
+        j->st.ms_sort_passes += ms_between(j->sort_ev[2 * p], j->sort_ev[2 * p + 1]);
+        j->st.sort_passes += 1;
+        j->st.sort_pass_elems += j->sort_n;
+    }
+    j->sort_passes_run = 0;
+}
+
 void append_bytes(std::vector<uint8_t> &o, const void *p, size_t n) {
     const uint8_t *b = reinterpret_cast<const uint8_t *>(p);
     o.insert(o.end(), b, b + n);
@@ -185,6 +199,13 @@ emp_status reset_chain(emp_job *j, uint64_t tiles, cudaStream_t s) {
 }
 uint32_t *chain_ctr(emp_job *j) { return reinterpret_cast<uint32_t *>(j->misc.as<uint64_t>() + kMiscCtr); }
 uint32_t *err_word(emp_job *j) { return reinterpret_cast<uint32_t *>(j->misc.as<uint64_t>() + kMiscErr); }
+
+// sort (sk0,sv0) in place-or-ping-pong; per-pass events for the stats
+int timed_sort(emp_job *j, uint64_t n, cudaStream_t s) {
+    j->sort_n = n;
+    return sort_pairs(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), j->sk1.as<uint64_t>(), j->sv1.as<uint32_t>(), n,
+                      j->sort_scratch.p, j->h_hist.as<uint32_t>(), err_word(j), s, j->sort_ev, &j->sort_passes_run);
+}
 
 emp_status run_job(emp_job *j, cudaStream_t s) {
     emp_stats &st = j->st;
@@ -298,8 +319,7 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
     EMP_TRY(ensure(j, j->sort_scratch, sort_scratch_bytes(cap)));
     EMP_CUDA(cudaMemcpyAsync(j->sk0.p, j->keys0.p, n2 * 8, cudaMemcpyDeviceToDevice, s));
     launch_iota(j->sv0.as<uint32_t>(), n2, s);
-    int res = sort_pairs(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), j->sk1.as<uint64_t>(), j->sv1.as<uint32_t>(), n2,
-                         j->sort_scratch.p, j->h_hist.as<uint32_t>(), err_word(j), s);
+    int res = timed_sort(j, n2, s);
     const uint64_t *sk = res ? j->sk1.as<uint64_t>() : j->sk0.as<uint64_t>();
     const uint32_t *sv = res ? j->sv1.as<uint32_t>() : j->sv0.as<uint32_t>();
     launch_dedup_mark(sk, sv, n2, j->alive.as<uint8_t>(), s);
@@ -307,6 +327,7 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
     launch_init_list(j->keys0.as<uint64_t>(), j->alive.as<uint8_t>(), n, j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(),
                      j->status.as<uint64_t>(), chain_ctr(j), dm + kMiscU, err_word(j), s);
     EMP_TRY(sync_and_check(j, s));
+    account_sort(j);
     const uint64_t U = hm[kMiscU];
     st.n_unique = U;
     launch_dup_prefix_half(j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(), U, s);
@@ -358,8 +379,7 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
         // sort a copy of the merged list (the list itself carries over)
         EMP_CUDA(cudaMemcpyAsync(j->sk0.p, lk[cur], N * 8, cudaMemcpyDeviceToDevice, s));
         EMP_CUDA(cudaMemcpyAsync(j->sv0.p, lv[cur], N * 4, cudaMemcpyDeviceToDevice, s));
-        res = sort_pairs(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), j->sk1.as<uint64_t>(), j->sv1.as<uint32_t>(), N,
-                         j->sort_scratch.p, j->h_hist.as<uint32_t>(), err_word(j), s);
+        res = timed_sort(j, N, s);
         sk = res ? j->sk1.as<uint64_t>() : j->sk0.as<uint64_t>();
         sv = res ? j->sv1.as<uint32_t>() : j->sv0.as<uint32_t>();
         EMP_TRY(ensure(j, j->cnt, N * 4));
@@ -369,6 +389,7 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
         launch_scan_u32_u64(j->cnt.as<uint32_t>(), j->offs.as<uint64_t>(), N, j->status.as<uint64_t>(), chain_ctr(j),
                             dm + kMiscE, err_word(j), s);
         EMP_TRY(sync_and_check(j, s));
+        account_sort(j);
         const uint64_t E = hm[kMiscE];
         if (E) {
             EMP_TRY(ensure(j, j->efrom, E * 4));
@@ -554,6 +575,13 @@ emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out) {
     j->ctx = ctx;
     if (p) j->p = *p;
     else emp_params_default(&j->p);
+    cudaSetDevice(ctx->device);
+    for (auto &e : j->sort_ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            emp_job_destroy(j);
+            return EMP_E_CUDA;
+        }
+    }
     *out = j;
     return EMP_OK;
 }
@@ -568,6 +596,8 @@ emp_status emp_job_destroy(emp_job *job) {
                       &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
                       &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts};
     for (DevBuf *b : bufs) free_buf(job, *b);
+    for (auto &e : job->sort_ev)
+        if (e) cudaEventDestroy(e);
     delete job;
     return EMP_OK;
 }
@@ -595,6 +625,19 @@ emp_status emp_job_reserve(emp_job *job, uint64_t bytes) {
     job->fq.bytes = nb.bytes;
     nb.p = nullptr;
     nb.bytes = 0;
+    return EMP_OK;
+}
+
+emp_status emp_job_reset(emp_job *job) {
+    if (!job) return EMP_E_INVAL;
+    cudaSetDevice(job->ctx->device);
+    cudaStreamSynchronize(job->ctx->stream);
+    job->F = 0;
+    job->fed_last = false;
+    job->ms_h2d = 0.0;
+    job->out.clear();
+    job->have_result = false;
+    job->n_ends = 0;
     return EMP_OK;
 }
 

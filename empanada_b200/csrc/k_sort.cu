@@ -186,12 +186,9 @@ static size_t onesweep_smem() {
 }
 
 int sort_pairs(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, uint64_t n, void *scratch,
-               uint32_t *hist_host, uint32_t *err, cudaStream_t s) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem());
-        attr_set = true;
-    }
+               uint32_t *hist_host, uint32_t *err, cudaStream_t s, cudaEvent_t *pass_events, uint32_t *passes_run) {
+    cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem());
+    if (passes_run) *passes_run = 0;
     if (n < 2) return 0;
     SortScratch *sc = reinterpret_cast<SortScratch *>(scratch);
     uint32_t *lookback = reinterpret_cast<uint32_t *>(sc + 1);
@@ -216,9 +213,12 @@ int sort_pairs(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, uint64_t 
     for (int p = 0; p < kSortPasses; ++p) {
         if (skip[p]) continue;
         count_launch();
+        if (pass_events) cudaEventRecord(pass_events[2 * p], s);
         onesweep_kernel<<<(unsigned)tiles, kSortThreads, onesweep_smem(), s>>>(
             kb[cur], vb[cur], kb[cur ^ 1], vb[cur ^ 1], n, p * kSortBits, sc->hist[p],
             lookback + (uint64_t)p * tiles * kSortRadix, sc->tile_ctr + p, err);
+        if (pass_events) cudaEventRecord(pass_events[2 * p + 1], s);
+        if (passes_run) *passes_run |= 1u << p;
         cur ^= 1;
     }
     return cur;

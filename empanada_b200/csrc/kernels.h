@@ -52,8 +52,11 @@ size_t sort_scratch_bytes(uint64_t n);
 // (k0,v0) and (k1,v1); returns 0 if the result is in (k0,v0), 1 otherwise.
 // hist_host (optional, kSortPasses*kSortRadix u32 pinned) enables skipping
 // passes whose digit is constant (costs one stream synchronisation).
+// pass_events (optional, 2*kSortPasses events): each digit pass is bracketed
+// by events 2p / 2p+1; *passes_run reports which passes ran (bit p).
 int sort_pairs(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, uint64_t n, void *scratch,
-               uint32_t *hist_host, uint32_t *err, cudaStream_t s);
+               uint32_t *hist_host, uint32_t *err, cudaStream_t s, cudaEvent_t *pass_events = nullptr,
+               uint32_t *passes_run = nullptr);
 
 // ---- rounds (k_round.cu) --------------------------------------------------
 void launch_dedup_mark(const uint64_t *skeys, const uint32_t *svals, uint64_t n2, uint8_t *alive, cudaStream_t s);

@@ -73,6 +73,9 @@ typedef struct emp_stats {
     double ms_dedup;       /* fingerprint sort + duplicate removal (device time) */
     double ms_rounds;      /* overlap rounds (device time, incl. edge copies) */
     double ms_total;       /* whole run (device time) */
+    double ms_sort_passes; /* device time of all radix-sort digit passes (CUDA events per launch) */
+    uint64_t sort_passes;  /* digit-pass launches */
+    uint64_t sort_pass_elems; /* sum over those launches of the pairs each one moved */
     uint64_t sfx_live[EMP_MAX_ROUNDS]; /* suffix-table size in round r */
     uint64_t pfx_live[EMP_MAX_ROUNDS]; /* prefix-table size in round r */
     uint64_t edges[EMP_MAX_ROUNDS];    /* edges written in round r */
@@ -108,6 +111,9 @@ emp_status emp_job_feed_fastq(emp_job *job, const char *bytes, uint64_t n, int l
 emp_status emp_job_feed_fastq_device(emp_job *job, const void *dev_bytes, uint64_t n, int last);
 /* Reserve device room for `bytes` of FASTQ (optional; avoids regrowth). */
 emp_status emp_job_reserve(emp_job *job, uint64_t bytes);
+/* Forget the fed input and the last result but keep every device buffer, so
+ * the job can take the next read set without new allocations. */
+emp_status emp_job_reset(emp_job *job);
 
 /* Map + reduce phases: main.cu:42-71 (read_block, transpose_reads,
  * get_reverse_complements, generate_fingerprint_read_pairs) and build_graph
