@@ -53,12 +53,13 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_elem():
-    """DRAM bytes per pair of one digit pass from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "onesweep_traffic.json")
+def traffic_summary():
+    """DRAM traffic per algorithmic byte of each profiled kernel, from the
+    committed ncu summary (profiles/traffic.json), if present."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         try:
-            return float(json.load(open(p))["dram_bytes_per_pair"])
+            return {k: float(v["dram_bytes_per_algorithmic_byte"]) for k, v in json.load(open(p)).items()}
         except Exception:
             return None
     return None
@@ -309,6 +310,9 @@ def main():
     sort_ms = 0.0
     sort_elems = 0
     sort_passes = 0
+    upd_ms = 0.0
+    upd_bytes = 0
+    upd_launches = 0
     with ClockSampler(device) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -324,6 +328,9 @@ def main():
             sort_ms += st["ms_sort_passes"]
             sort_elems += st["sort_pass_elems"]
             sort_passes += st["sort_passes"]
+            upd_ms += st["ms_update"]
+            upd_bytes += st["update_bytes"]
+            upd_launches += st["update_launches"]
     barrier()
     clocks = clk.summary()
     total_ms = sum(step_ms)
@@ -358,14 +365,22 @@ def main():
     e2e_value = world * workload.n_reads * len(e2e_s) / e2e_total
 
     peak, peak_kind = measured_peaks()
-    achieved = (24.0 * sort_elems) / (sort_ms / 1000.0) / 1e9 if sort_ms > 0 else 0.0
-    tpe = traffic_per_elem()
-    per_launch_elems = sort_elems / max(sort_passes, 1)
-    roofline = {"bound": "hbm", "kernel": "onesweep_kernel (radix-sort digit pass)", "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} (HBM copy)",
-                "traffic": (tpe * per_launch_elems) if tpe else None,
-                "algorithmic_bytes_per_launch": 24.0 * per_launch_elems,
-                "avg_launch_us": 1000.0 * sort_ms / max(sort_passes, 1), "launches": sort_passes}
+    traffic = traffic_summary()
+    if sort_ms >= upd_ms:  # the radix-sort digit pass dominates
+        per_launch = 24.0 * sort_elems / max(sort_passes, 1)
+        ms, nl, kname = sort_ms, sort_passes, "onesweep_kernel"
+        what = "radix-sort digit pass: 24 B per pair (12 read, 12 written)"
+    else:  # the per-round table update of the pipeline dominates
+        per_launch = upd_bytes / max(upd_launches, 1)
+        ms, nl, kname = upd_ms, upd_launches, "pl_update_filter_kernel"
+        what = "round update: 13 B read + 1/4 B of bases per entry in, 12 B written per entry out"
+    achieved = per_launch * nl / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
+    tb = traffic.get(kname) if traffic else None
+    roofline = {"bound": "hbm", "kernel": kname, "algorithmic": what, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} (HBM copy, burst)",
+                "traffic": (tb * per_launch) if tb else None, "algorithmic_bytes_per_launch": per_launch,
+                "avg_launch_us": 1000.0 * ms / max(nl, 1), "launches": nl,
+                "sort_pass_ms_per_step": sort_ms / args.steps, "update_ms_per_step": upd_ms / args.steps}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -140,6 +140,57 @@ EMP_DEV uint64_t lookback_exclusive(uint64_t *status, uint32_t tile, uint64_t ag
     return excl;
 }
 
+// Epoch-tagged status words: epoch in bits 44-63, flag in 42-43, value below.
+// A word whose epoch differs from the caller's is "not ready", so status
+// arrays never need clearing between uses (each use has a fresh epoch).
+constexpr uint64_t kEpAgg = 1ull << 42;
+constexpr uint64_t kEpInc = 2ull << 42;
+constexpr uint64_t kEpVal = (1ull << 42) - 1;
+EMP_DEV uint64_t ep_word(uint32_t epoch, uint64_t flag, uint64_t v) { return ((uint64_t)epoch << 44) | flag | v; }
+EMP_DEV uint32_t ep_flag(uint64_t w, uint32_t epoch) {
+    return (uint32_t)(w >> 44) == (epoch & 0xfffffu) ? (uint32_t)((w >> 42) & 3u) : 0u;
+}
+
+// lookback_exclusive with epoch-tagged words; reads up to 4 predecessors at
+// a time.  One thread; bounded waits as above.
+EMP_DEV uint64_t lookback_epoch(uint64_t *status, uint32_t tile, uint64_t aggregate, uint32_t epoch,
+                                uint32_t *err) {
+    epoch &= 0xfffffu;
+    if (tile == 0) {
+        st_status(status, ep_word(epoch, kEpInc, aggregate));
+        return 0;
+    }
+    st_status(status + tile, ep_word(epoch, kEpAgg, aggregate));
+    uint64_t excl = 0;
+    int64_t t = (int64_t)tile - 1;
+    while (t >= 0) {
+        const int k = t >= 3 ? 4 : (int)t + 1;
+        uint64_t w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (i < k) w[i] = ld_status(status + (t - i));
+        bool inc = false;
+        for (int i = 0; i < k && !inc; ++i) {
+            uint32_t f, spins = 0;
+            while ((f = ep_flag(w[i], epoch)) == 0) {
+                if (++spins > kSpinLimit) {
+                    atomicOr(err, kErrSpin);
+                    st_status(status + tile, ep_word(epoch, kEpInc, excl + aggregate));
+                    return excl;
+                }
+                if (spins > 32) __nanosleep(32);
+                w[i] = ld_status(status + (t - i));
+            }
+            excl += w[i] & kEpVal;
+            inc = f == 2;
+        }
+        if (inc) break;
+        t -= k;
+    }
+    st_status(status + tile, ep_word(epoch, kEpInc, excl + aggregate));
+    return excl;
+}
+
 // Block-wide exclusive scan of one value per thread (blockDim.x = NT).
 template <int NT, typename T>
 EMP_DEV T block_exclusive_scan(T v, T *smem_warp /* NT/32 */, T *total) {

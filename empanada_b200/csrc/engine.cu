@@ -69,6 +69,10 @@ struct emp_ctx {
     uint64_t in_use = 0;
     cudaStream_t stream = nullptr;
     DevBuf tables;  // HashTables
+    // emp_sort_pairs working set, kept for the next call
+    DevBuf sort_k1, sort_v1, sort_scr, sort_err;
+    uint64_t sort_cap = 0;
+    uint64_t sort_calls = 0;
 };
 
 struct emp_job {
@@ -84,9 +88,15 @@ struct emp_job {
     DevBuf sk0, sv0, sk1, sv1, alive, lk0, lv0, lk1, lv1, used_s, used_p, cnt, offs, efrom, eto, sort_scratch;
     DevBuf akeys, apos, bkeys, parts;  // record splitting
     PinnedBuf h_parts;
+    // device-resident round pipeline
+    DevBuf lk_init, lv_init, bloom_s, bloom_p, ck, cv, ck2, cv2, records, st_upd, st_cand, st_scan, ctl;
+    PinnedBuf h_ctl, h_records;
+    uint64_t ecap_hint = 0;
+    uint64_t sorts_since_clear = 0;
     cudaEvent_t sort_ev[2 * kSortPasses] = {};
-    uint32_t sort_passes_run = 0;
+    cudaEvent_t upd_ev[2 * EMP_MAX_ROUNDS] = {};
     uint64_t sort_n = 0;
+    bool sort_timed = false;
     PinnedBuf h_misc, h_hist, h_from, h_to;
     uint64_t n_ends = 0;
     // results
@@ -99,7 +109,10 @@ namespace {
 
 // misc device words (u64 slots)
 enum MiscSlot { kMiscErr = 0, kMiscTotal = 1, kMiscLen = 2, kMiscN = 3, kMiscU = 4, kMiscNout = 5, kMiscSout = 6,
-                kMiscE = 7, kMiscCtr = 8, kMiscParts = 9, kMiscSlots = 16 };
+                kMiscE = 7, kMiscCtr = 8, kMiscParts = 9, kMiscSortN = 10, kMiscSlots = 16 };
+
+// internal: the pipeline's edge buffer was too small (never returned by the ABI)
+constexpr emp_status kNeedEdgeRoom = -1000;
 
 emp_status cuda_status(cudaError_t e) { return e == cudaSuccess ? EMP_OK : (e == cudaErrorMemoryAllocation ? EMP_E_NOMEM : EMP_E_CUDA); }
 
@@ -176,13 +189,13 @@ emp_status sync_and_check(emp_job *j, cudaStream_t s) {
 
 // fold the per-pass event times of the last sort into the stats (after a sync)
 void account_sort(emp_job *j) {
+    if (!j->sort_timed) return;
     for (int p = 0; p < kSortPasses; ++p) {
-        if (!(j->sort_passes_run & (1u << p))) continue;
         j->st.ms_sort_passes += ms_between(j->sort_ev[2 * p], j->sort_ev[2 * p + 1]);
         j->st.sort_passes += 1;
         j->st.sort_pass_elems += j->sort_n;
     }
-    j->sort_passes_run = 0;
+    j->sort_timed = false;
 }
 
 void append_bytes(std::vector<uint8_t> &o, const void *p, size_t n) {
@@ -200,11 +213,290 @@ emp_status reset_chain(emp_job *j, uint64_t tiles, cudaStream_t s) {
 uint32_t *chain_ctr(emp_job *j) { return reinterpret_cast<uint32_t *>(j->misc.as<uint64_t>() + kMiscCtr); }
 uint32_t *err_word(emp_job *j) { return reinterpret_cast<uint32_t *>(j->misc.as<uint64_t>() + kMiscErr); }
 
-// sort (sk0,sv0) in place-or-ping-pong; per-pass events for the stats
-int timed_sort(emp_job *j, uint64_t n, cudaStream_t s) {
+// the sort scratch must start zeroed and be re-zeroed before its epoch wraps
+emp_status ensure_sort_scratch(emp_job *j, uint64_t n_max, cudaStream_t s) {
+    const size_t need = sort_scratch_bytes(n_max);
+    if (need > j->sort_scratch.bytes || j->sorts_since_clear > 100000) {
+        EMP_TRY(ensure(j, j->sort_scratch, need));
+        EMP_CUDA(cudaMemsetAsync(j->sort_scratch.p, 0, j->sort_scratch.bytes, s));
+        j->sorts_since_clear = 0;
+    }
+    return EMP_OK;
+}
+
+// stable sort of (sk0, sv0)[0..n) in place (ping-pong through sk1/sv1);
+// per-pass events for the stats
+void timed_sort(emp_job *j, uint64_t n, cudaStream_t s) {
     j->sort_n = n;
-    return sort_pairs(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), j->sk1.as<uint64_t>(), j->sv1.as<uint32_t>(), n,
-                      j->sort_scratch.p, j->h_hist.as<uint32_t>(), err_word(j), s, j->sort_ev, &j->sort_passes_run);
+    j->sort_timed = true;
+    ++j->sorts_since_clear;
+    sort_pairs(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), j->sk1.as<uint64_t>(), j->sv1.as<uint32_t>(), n,
+               j->sort_scratch.p, j->misc.as<uint64_t>() + kMiscSortN, err_word(j), s, j->sort_ev);
+}
+
+// Record `ne` edges from the host edge arrays into output.bin (overlap.cu:148-161).
+void emit_record(emp_job *j, int32_t ovlp, uint64_t e0, uint64_t e1) {
+    const uint64_t ne = e1 - e0;
+    append_bytes(j->out, &ne, 8);
+    append_bytes(j->out, &ovlp, 4);
+    if (ne) {
+        append_bytes(j->out, j->h_from.as<uint32_t>() + e0, ne * 4);
+        append_bytes(j->out, j->h_to.as<uint32_t>() + e0, ne * 4);
+    }
+    j->st.n_records += 1;
+}
+
+struct RoundEnv {
+    int L;
+    int rounds;
+    uint64_t M;
+    uint64_t wpc;
+    const HashTables *tables;
+};
+
+// One round with host synchronisation: used while the tables are large enough
+// for the reference to split a round into several search partitions
+// (cq_get_search_partitions, cqutils.cuh:108-137).  Full sort of both tables.
+emp_status sync_round(emp_job *j, cudaStream_t s, const RoundEnv &env, int r, int &cur, uint64_t &n_in,
+                      uint64_t &S_out, uint64_t &P_out, bool &stop) {
+    emp_stats &st = j->st;
+    uint64_t *hm = j->h_misc.as<uint64_t>();
+    uint64_t *dm = j->misc.as<uint64_t>();
+    uint64_t *lk[2] = {j->lk0.as<uint64_t>(), j->lk1.as<uint64_t>()};
+    uint32_t *lv[2] = {j->lv0.as<uint32_t>(), j->lv1.as<uint32_t>()};
+    const uint64_t M = env.M;
+    EMP_TRY(reset_chain(j, upd_tiles(n_in), s));
+    EMP_CUDA(cudaMemsetAsync(dm + kMiscNout, 0, 2 * sizeof(uint64_t), s));
+    RoundArgs a{};
+    a.kin = lk[cur];
+    a.vin = lv[cur];
+    a.n_in = n_in;
+    a.kout = lk[cur ^ 1];
+    a.vout = lv[cur ^ 1];
+    a.used_s = j->used_s.as<uint8_t>();
+    a.used_p = j->used_p.as<uint8_t>();
+    a.cols = j->cols.as<uint32_t>();
+    a.wpc = env.wpc;
+    a.tables = env.tables;
+    a.L = env.L;
+    a.round = r;
+    a.status = j->status.as<uint64_t>();
+    a.tile_ctr = chain_ctr(j);
+    a.n_out = dm + kMiscNout;
+    a.s_out = dm + kMiscSout;
+    a.err = err_word(j);
+    launch_update_compact(a, s);
+    EMP_TRY(sync_and_check(j, s));
+    const uint64_t N = hm[kMiscNout], S = hm[kMiscSout], P = N - S;
+    S_out = S;
+    P_out = P;
+    if (S == 0) {  // loop condition of build_graph (overlap.cu:258)
+        stop = true;
+        return EMP_OK;
+    }
+    cur ^= 1;
+    n_in = N;
+    if (r < EMP_MAX_ROUNDS) {
+        st.sfx_live[r] = S;
+        st.pfx_live[r] = P;
+    }
+    st.n_rounds = r + 1;
+    if (P == 0) return EMP_OK;  // one-sided search partition: no record
+    const bool split = S >= M / 2 || P >= M / 2;
+    // sort a copy of the merged list (the list itself carries over)
+    EMP_CUDA(cudaMemcpyAsync(j->sk0.p, lk[cur], N * 8, cudaMemcpyDeviceToDevice, s));
+    EMP_CUDA(cudaMemcpyAsync(j->sv0.p, lv[cur], N * 4, cudaMemcpyDeviceToDevice, s));
+    timed_sort(j, N, s);
+    const uint64_t *sk = j->sk0.as<uint64_t>();
+    const uint32_t *sv = j->sv0.as<uint32_t>();
+    EMP_TRY(ensure(j, j->cnt, N * 4));
+    EMP_TRY(ensure(j, j->offs, N * 8));
+    launch_join_count(sk, sv, N, j->cnt.as<uint32_t>(), s);
+    EMP_TRY(reset_chain(j, scan_tiles(N), s));
+    launch_scan_u32_u64(j->cnt.as<uint32_t>(), j->offs.as<uint64_t>(), N, j->status.as<uint64_t>(), chain_ctr(j),
+                        dm + kMiscE, err_word(j), s);
+    EMP_TRY(sync_and_check(j, s));
+    account_sort(j);
+    const uint64_t E = hm[kMiscE];
+    if (E) {
+        EMP_TRY(ensure(j, j->efrom, E * 4));
+        EMP_TRY(ensure(j, j->eto, E * 4));
+        if (!j->h_from.ensure(E * 4) || !j->h_to.ensure(E * 4)) return EMP_E_NOMEM;
+        launch_join_write(sk, sv, N, j->cnt.as<uint32_t>(), j->offs.as<uint64_t>(), j->efrom.as<uint32_t>(),
+                          j->eto.as<uint32_t>(), j->used_s.as<uint8_t>(), j->used_p.as<uint8_t>(), s);
+        EMP_CUDA(cudaMemcpyAsync(j->h_from.p, j->efrom.p, E * 4, cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaMemcpyAsync(j->h_to.p, j->eto.p, E * 4, cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaStreamSynchronize(s));
+    }
+    const int32_t ovlp = env.L - 1 - r;
+    if (!split) {
+        emit_record(j, ovlp, 0, E);
+    } else {
+        // search partitions of windows M/2; each two-sided one is a record
+        EMP_TRY(ensure(j, j->akeys, S * 8));
+        EMP_TRY(ensure(j, j->apos, S * 4));
+        EMP_TRY(ensure(j, j->bkeys, P * 8));
+        const uint64_t pcap = 4 * (N / (M / 2) + 1) + 1024;
+        EMP_TRY(ensure(j, j->parts, pcap * sizeof(SearchPart)));
+        EMP_TRY(reset_chain(j, upd_tiles(N), s));
+        launch_split_tables(sk, sv, N, j->akeys.as<uint64_t>(), j->apos.as<uint32_t>(), j->bkeys.as<uint64_t>(),
+                            j->status.as<uint64_t>(), chain_ctr(j), err_word(j), s);
+        launch_search_partitions(j->akeys.as<uint64_t>(), S, j->bkeys.as<uint64_t>(), P, M / 2,
+                                 j->apos.as<uint32_t>(), j->offs.as<uint64_t>(), E, j->parts.as<SearchPart>(), pcap,
+                                 dm + kMiscParts, err_word(j), s);
+        EMP_TRY(sync_and_check(j, s));
+        if (hm[kMiscErr] & kErrHang) return EMP_E_HANG;
+        if (hm[kMiscErr] & kErrCapacity) return EMP_E_UNSUPPORTED;
+        const uint64_t np = hm[kMiscParts];
+        if (!j->h_parts.ensure(np * sizeof(SearchPart) + 16)) return EMP_E_NOMEM;
+        EMP_CUDA(cudaMemcpyAsync(j->h_parts.p, j->parts.p, np * sizeof(SearchPart), cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaStreamSynchronize(s));
+        const SearchPart *ps = j->h_parts.as<SearchPart>();
+        for (uint64_t q = 0; q < np; ++q)
+            if (ps[q].pa && ps[q].pb) emit_record(j, ovlp, ps[q].e0, ps[q].e1);
+    }
+    st.n_edges += E;
+    if (r < EMP_MAX_ROUNDS) st.edges[r] = E;
+    return EMP_OK;
+}
+
+int bloom_bits_for(uint64_t entries) {
+    uint64_t want = entries * 32;
+    int b = 16;
+    while (b < 30 && (1ull << b) < want) ++b;
+    return b;
+}
+
+// All rounds: synchronous ones while a round could split into several search
+// partitions (sizes only shrink), then the device-resident pipeline for the
+// rest with a single synchronisation at the end.  Returns kNeedEdgeRoom with
+// *needed set when the pipeline's edge buffer (ecap edges) was too small.
+emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t U, uint64_t ecap, uint64_t *needed) {
+    emp_stats &st = j->st;
+    st.n_rounds = 0;
+    st.n_edges = 0;
+    st.n_records = 0;
+    std::memset(st.sfx_live, 0, sizeof st.sfx_live);
+    std::memset(st.pfx_live, 0, sizeof st.pfx_live);
+    std::memset(st.edges, 0, sizeof st.edges);
+    j->out.clear();
+    EMP_CUDA(cudaMemsetAsync(j->used_s.p, 0, j->used_s.bytes, s));
+    EMP_CUDA(cudaMemsetAsync(j->used_p.p, 0, j->used_p.bytes, s));
+    int cur = 0, r = 0;
+    uint64_t n_in = 2 * U, S = U, P = U;
+    const uint64_t M = env.M;
+    const bool force_sync = std::getenv("EMP_SYNC_ROUNDS") != nullptr;
+    while (r < env.rounds && (force_sync || S >= M / 2 || P >= M / 2)) {
+        bool stop = false;
+        EMP_TRY(sync_round(j, s, env, r, cur, n_in, S, P, stop));
+        if (stop) return EMP_OK;
+        ++r;
+    }
+    if (r >= env.rounds) return EMP_OK;
+
+    // ---- device-resident pipeline for rounds r .. rounds-1
+    const uint64_t nmax = n_in;
+    const int bits = bloom_bits_for(S > P ? S : P);
+    const size_t bloom_bytes = (size_t)1 << (bits - 3);
+    EMP_TRY(ensure(j, j->bloom_s, bloom_bytes));
+    EMP_TRY(ensure(j, j->bloom_p, bloom_bytes));
+    EMP_TRY(ensure(j, j->ck, nmax * 8 + 8));
+    EMP_TRY(ensure(j, j->ck2, nmax * 8 + 8));
+    EMP_TRY(ensure(j, j->cv, nmax * 4 + 4));
+    EMP_TRY(ensure(j, j->cv2, nmax * 4 + 4));
+    EMP_TRY(ensure(j, j->cnt, nmax * 4 + 4));
+    EMP_TRY(ensure(j, j->offs, nmax * 8 + 8));
+    EMP_TRY(ensure(j, j->efrom, ecap * 4));
+    EMP_TRY(ensure(j, j->eto, ecap * 4));
+    EMP_TRY(ensure(j, j->records, (size_t)env.rounds * sizeof(RoundRecord)));
+    EMP_TRY(ensure(j, j->st_upd, upd_tiles(nmax) * 8 + 8));
+    EMP_TRY(ensure(j, j->st_cand, upd_tiles(nmax) * 8 + 8));
+    EMP_TRY(ensure(j, j->st_scan, scan_tiles(nmax) * 8 + 8));
+    EMP_TRY(ensure(j, j->ctl, sizeof(RoundCtl)));
+    EMP_TRY(ensure_sort_scratch(j, nmax, s));
+    if (!j->h_ctl.ensure(sizeof(RoundCtl)) || !j->h_records.ensure((size_t)env.rounds * sizeof(RoundRecord)))
+        return EMP_E_NOMEM;
+    EMP_CUDA(cudaMemsetAsync(j->st_upd.p, 0, j->st_upd.bytes, s));
+    EMP_CUDA(cudaMemsetAsync(j->st_cand.p, 0, j->st_cand.bytes, s));
+    EMP_CUDA(cudaMemsetAsync(j->st_scan.p, 0, j->st_scan.bytes, s));
+    RoundCtl *hc = j->h_ctl.as<RoundCtl>();
+    std::memset(hc, 0, sizeof(RoundCtl));
+    hc->n = n_in;
+    hc->s = S;
+    hc->cur = (uint32_t)cur;
+    hc->round = (uint32_t)r;
+    hc->rounds = (uint32_t)env.rounds;
+    EMP_CUDA(cudaMemcpyAsync(j->ctl.p, hc, sizeof(RoundCtl), cudaMemcpyHostToDevice, s));
+    PipeArgs a{};
+    a.ctl = j->ctl.as<RoundCtl>();
+    a.records = j->records.as<RoundRecord>();
+    a.lk0 = j->lk0.as<uint64_t>();
+    a.lk1 = j->lk1.as<uint64_t>();
+    a.lv0 = j->lv0.as<uint32_t>();
+    a.lv1 = j->lv1.as<uint32_t>();
+    a.used_s = j->used_s.as<uint8_t>();
+    a.used_p = j->used_p.as<uint8_t>();
+    a.cols = j->cols.as<uint32_t>();
+    a.wpc = env.wpc;
+    a.tables = env.tables;
+    a.L = env.L;
+    a.bloom_bits = bits;
+    a.bloom_s = j->bloom_s.as<uint32_t>();
+    a.bloom_p = j->bloom_p.as<uint32_t>();
+    a.bloom_bytes = bloom_bytes;
+    a.ck = j->ck.as<uint64_t>();
+    a.ck2 = j->ck2.as<uint64_t>();
+    a.cv = j->cv.as<uint32_t>();
+    a.cv2 = j->cv2.as<uint32_t>();
+    a.cnt = j->cnt.as<uint32_t>();
+    a.offs = j->offs.as<uint64_t>();
+    a.efrom = j->efrom.as<uint32_t>();
+    a.eto = j->eto.as<uint32_t>();
+    a.ecap = ecap;
+    a.st_upd = j->st_upd.as<uint64_t>();
+    a.st_cand = j->st_cand.as<uint64_t>();
+    a.st_scan = j->st_scan.as<uint64_t>();
+    a.err = err_word(j);
+    const int r0 = r;
+    for (int q = r0; q < env.rounds; ++q) {
+        cudaEvent_t *ev = q < EMP_MAX_ROUNDS ? j->upd_ev + 2 * q : nullptr;
+        launch_pipeline_round(a, nmax, nmax, j->sort_scratch.p, s, ev);
+        ++j->sorts_since_clear;
+    }
+    EMP_CUDA(cudaMemcpyAsync(hc, j->ctl.p, sizeof(RoundCtl), cudaMemcpyDeviceToHost, s));
+    EMP_CUDA(cudaMemcpyAsync(j->h_records.p, j->records.p, (size_t)env.rounds * sizeof(RoundRecord),
+                             cudaMemcpyDeviceToHost, s));
+    EMP_TRY(sync_and_check(j, s));
+    if (hc->overflow) {
+        *needed = hc->e_total;
+        return kNeedEdgeRoom;
+    }
+    const uint64_t E_all = hc->e_total;
+    if (E_all) {
+        if (!j->h_from.ensure(E_all * 4) || !j->h_to.ensure(E_all * 4)) return EMP_E_NOMEM;
+        EMP_CUDA(cudaMemcpyAsync(j->h_from.p, j->efrom.p, E_all * 4, cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaMemcpyAsync(j->h_to.p, j->eto.p, E_all * 4, cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaStreamSynchronize(s));
+    }
+    const RoundRecord *rec = j->h_records.as<RoundRecord>();
+    const int r_end = (int)hc->round;  // rounds run with a non-empty suffix table
+    uint64_t prev_n = n_in;
+    for (int q = r0; q < r_end; ++q) {
+        const RoundRecord &x = rec[q];
+        if (q < EMP_MAX_ROUNDS) {
+            st.sfx_live[q] = x.S;
+            st.pfx_live[q] = x.P;
+            st.edges[q] = x.E;
+            st.ms_update += ms_between(j->upd_ev[2 * q], j->upd_ev[2 * q + 1]);
+            st.update_launches += 1;
+            st.update_bytes += 13 * prev_n + prev_n / 4 + 12 * (x.S + x.P);
+        }
+        if (x.P) emit_record(j, env.L - 1 - q, x.e0, x.e0 + x.E);
+        st.n_edges += x.E;
+        prev_n = x.S + x.P;
+    }
+    st.n_rounds = r_end;
+    return EMP_OK;
 }
 
 emp_status run_job(emp_job *j, cudaStream_t s) {
@@ -316,13 +608,11 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
     EMP_TRY(ensure(j, j->alive, n2));
     EMP_TRY(ensure(j, j->used_s, n2));
     EMP_TRY(ensure(j, j->used_p, n2));
-    EMP_TRY(ensure(j, j->sort_scratch, sort_scratch_bytes(cap)));
+    EMP_TRY(ensure_sort_scratch(j, cap, s));
     EMP_CUDA(cudaMemcpyAsync(j->sk0.p, j->keys0.p, n2 * 8, cudaMemcpyDeviceToDevice, s));
     launch_iota(j->sv0.as<uint32_t>(), n2, s);
-    int res = timed_sort(j, n2, s);
-    const uint64_t *sk = res ? j->sk1.as<uint64_t>() : j->sk0.as<uint64_t>();
-    const uint32_t *sv = res ? j->sv1.as<uint32_t>() : j->sv0.as<uint32_t>();
-    launch_dedup_mark(sk, sv, n2, j->alive.as<uint8_t>(), s);
+    timed_sort(j, n2, s);
+    launch_dedup_mark(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), n2, j->alive.as<uint8_t>(), s);
     EMP_TRY(reset_chain(j, upd_tiles(n2), s));
     launch_init_list(j->keys0.as<uint64_t>(), j->alive.as<uint8_t>(), n, j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(),
                      j->status.as<uint64_t>(), chain_ctr(j), dm + kMiscU, err_word(j), s);
@@ -331,115 +621,29 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
     const uint64_t U = hm[kMiscU];
     st.n_unique = U;
     launch_dup_prefix_half(j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(), U, s);
-    EMP_CUDA(cudaMemsetAsync(j->used_s.p, 0, n2, s));
-    EMP_CUDA(cudaMemsetAsync(j->used_p.p, 0, n2, s));
     cudaEventRecord(ev.e[2], s);
 
     // ---- overlap rounds (overlap.cu:258-290)
-    uint64_t *lk[2] = {j->lk0.as<uint64_t>(), j->lk1.as<uint64_t>()};
-    uint32_t *lv[2] = {j->lv0.as<uint32_t>(), j->lv1.as<uint32_t>()};
-    int cur = 0;
-    uint64_t n_in = 2 * U;
     const int rounds = L - j->p.min_ovlp;
-    for (int r = 0; r < rounds; ++r) {
-        EMP_TRY(reset_chain(j, upd_tiles(n_in), s));
-        EMP_CUDA(cudaMemsetAsync(dm + kMiscNout, 0, 2 * sizeof(uint64_t), s));
-        RoundArgs a{};
-        a.kin = lk[cur];
-        a.vin = lv[cur];
-        a.n_in = n_in;
-        a.kout = lk[cur ^ 1];
-        a.vout = lv[cur ^ 1];
-        a.used_s = j->used_s.as<uint8_t>();
-        a.used_p = j->used_p.as<uint8_t>();
-        a.cols = j->cols.as<uint32_t>();
-        a.wpc = wpc;
-        a.tables = tables;
-        a.L = L;
-        a.round = r;
-        a.status = j->status.as<uint64_t>();
-        a.tile_ctr = chain_ctr(j);
-        a.n_out = dm + kMiscNout;
-        a.s_out = dm + kMiscSout;
-        a.err = err_word(j);
-        launch_update_compact(a, s);
-        EMP_TRY(sync_and_check(j, s));
-        const uint64_t N = hm[kMiscNout], S = hm[kMiscSout], P = N - S;
-        if (S == 0) break;  // loop condition of build_graph (overlap.cu:258)
-        cur ^= 1;
-        n_in = N;
-        if (r < EMP_MAX_ROUNDS) {
-            st.sfx_live[r] = S;
-            st.pfx_live[r] = P;
+    if (rounds > 0) {
+        // the pipeline may need a larger edge buffer: keep the initial list to restart
+        EMP_TRY(ensure(j, j->lk_init, 2 * U * 8 + 8));
+        EMP_TRY(ensure(j, j->lv_init, 2 * U * 4 + 4));
+        EMP_CUDA(cudaMemcpyAsync(j->lk_init.p, j->lk0.p, 2 * U * 8, cudaMemcpyDeviceToDevice, s));
+        EMP_CUDA(cudaMemcpyAsync(j->lv_init.p, j->lv0.p, 2 * U * 4, cudaMemcpyDeviceToDevice, s));
+        uint64_t ecap = j->ecap_hint ? j->ecap_hint : (4 * U > (1u << 20) ? 4 * U : (1u << 20));
+        if (const char *ec = std::getenv("EMP_EDGE_CAP")) ecap = std::strtoull(ec, nullptr, 10) + 1;
+        const RoundEnv env{L, rounds, M, wpc, tables};
+        for (int attempt = 0;; ++attempt) {
+            uint64_t needed = 0;
+            emp_status rc = run_rounds(j, s, env, U, ecap, &needed);
+            if (rc == EMP_OK) break;
+            if (rc != kNeedEdgeRoom || attempt >= 2) return rc == kNeedEdgeRoom ? EMP_E_NOMEM : rc;
+            ecap = needed + needed / 4 + 1024;
+            j->ecap_hint = ecap;
+            EMP_CUDA(cudaMemcpyAsync(j->lk0.p, j->lk_init.p, 2 * U * 8, cudaMemcpyDeviceToDevice, s));
+            EMP_CUDA(cudaMemcpyAsync(j->lv0.p, j->lv_init.p, 2 * U * 4, cudaMemcpyDeviceToDevice, s));
         }
-        st.n_rounds = r + 1;
-        if (P == 0) continue;  // one-sided search partition: no record
-        // both windows below M/2: one search partition, one record (cqutils.cuh:117-121)
-        const bool split = S >= M / 2 || P >= M / 2;
-        // sort a copy of the merged list (the list itself carries over)
-        EMP_CUDA(cudaMemcpyAsync(j->sk0.p, lk[cur], N * 8, cudaMemcpyDeviceToDevice, s));
-        EMP_CUDA(cudaMemcpyAsync(j->sv0.p, lv[cur], N * 4, cudaMemcpyDeviceToDevice, s));
-        res = timed_sort(j, N, s);
-        sk = res ? j->sk1.as<uint64_t>() : j->sk0.as<uint64_t>();
-        sv = res ? j->sv1.as<uint32_t>() : j->sv0.as<uint32_t>();
-        EMP_TRY(ensure(j, j->cnt, N * 4));
-        EMP_TRY(ensure(j, j->offs, N * 8));
-        launch_join_count(sk, sv, N, j->cnt.as<uint32_t>(), s);
-        EMP_TRY(reset_chain(j, scan_tiles(N), s));
-        launch_scan_u32_u64(j->cnt.as<uint32_t>(), j->offs.as<uint64_t>(), N, j->status.as<uint64_t>(), chain_ctr(j),
-                            dm + kMiscE, err_word(j), s);
-        EMP_TRY(sync_and_check(j, s));
-        account_sort(j);
-        const uint64_t E = hm[kMiscE];
-        if (E) {
-            EMP_TRY(ensure(j, j->efrom, E * 4));
-            EMP_TRY(ensure(j, j->eto, E * 4));
-            if (!j->h_from.ensure(E * 4) || !j->h_to.ensure(E * 4)) return EMP_E_NOMEM;
-            launch_join_write(sk, sv, N, j->cnt.as<uint32_t>(), j->offs.as<uint64_t>(), j->efrom.as<uint32_t>(),
-                              j->eto.as<uint32_t>(), j->used_s.as<uint8_t>(), j->used_p.as<uint8_t>(), s);
-            EMP_CUDA(cudaMemcpyAsync(j->h_from.p, j->efrom.p, E * 4, cudaMemcpyDeviceToHost, s));
-            EMP_CUDA(cudaMemcpyAsync(j->h_to.p, j->eto.p, E * 4, cudaMemcpyDeviceToHost, s));
-            EMP_CUDA(cudaStreamSynchronize(s));
-        }
-        const int32_t ovlp = L - 1 - r;
-        auto record = [&](uint64_t e0, uint64_t e1) {
-            const uint64_t ne = e1 - e0;
-            append_bytes(j->out, &ne, 8);
-            append_bytes(j->out, &ovlp, 4);
-            if (ne) {
-                append_bytes(j->out, j->h_from.as<uint32_t>() + e0, ne * 4);
-                append_bytes(j->out, j->h_to.as<uint32_t>() + e0, ne * 4);
-            }
-            st.n_records += 1;
-        };
-        if (!split) {
-            record(0, E);
-        } else {
-            // search partitions of windows M/2; each two-sided one is a record
-            EMP_TRY(ensure(j, j->akeys, S * 8));
-            EMP_TRY(ensure(j, j->apos, S * 4));
-            EMP_TRY(ensure(j, j->bkeys, P * 8));
-            const uint64_t pcap = 4 * (N / (M / 2) + 1) + 1024;
-            EMP_TRY(ensure(j, j->parts, pcap * sizeof(SearchPart)));
-            EMP_TRY(reset_chain(j, upd_tiles(N), s));
-            launch_split_tables(sk, sv, N, j->akeys.as<uint64_t>(), j->apos.as<uint32_t>(), j->bkeys.as<uint64_t>(),
-                                j->status.as<uint64_t>(), chain_ctr(j), err_word(j), s);
-            launch_search_partitions(j->akeys.as<uint64_t>(), S, j->bkeys.as<uint64_t>(), P, M / 2,
-                                     j->apos.as<uint32_t>(), j->offs.as<uint64_t>(), E, j->parts.as<SearchPart>(),
-                                     pcap, dm + kMiscParts, err_word(j), s);
-            EMP_TRY(sync_and_check(j, s));
-            if (hm[kMiscErr] & kErrHang) return EMP_E_HANG;
-            if (hm[kMiscErr] & kErrCapacity) return EMP_E_UNSUPPORTED;
-            const uint64_t np = hm[kMiscParts];
-            if (!j->h_parts.ensure(np * sizeof(SearchPart) + 16)) return EMP_E_NOMEM;
-            EMP_CUDA(cudaMemcpyAsync(j->h_parts.p, j->parts.p, np * sizeof(SearchPart), cudaMemcpyDeviceToHost, s));
-            EMP_CUDA(cudaStreamSynchronize(s));
-            const SearchPart *ps = j->h_parts.as<SearchPart>();
-            for (uint64_t q = 0; q < np; ++q)
-                if (ps[q].pa && ps[q].pb) record(ps[q].e0, ps[q].e1);
-        }
-        st.n_edges += E;
-        if (r < EMP_MAX_ROUNDS) st.edges[r] = E;
     }
     cudaEventRecord(ev.e[3], s);
     cudaEventRecord(ev.e[4], s);
@@ -582,6 +786,12 @@ emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out) {
             return EMP_E_CUDA;
         }
     }
+    for (auto &e : j->upd_ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            emp_job_destroy(j);
+            return EMP_E_CUDA;
+        }
+    }
     *out = j;
     return EMP_OK;
 }
@@ -594,9 +804,13 @@ emp_status emp_job_destroy(emp_job *job) {
                       &job->seq_end, &job->hq, &job->idx, &job->rec_of, &job->keys0, &job->cols, &job->sk0,
                       &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
                       &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
-                      &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts};
+                      &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts, &job->lk_init,
+                      &job->lv_init, &job->bloom_s, &job->bloom_p, &job->ck, &job->cv, &job->ck2, &job->cv2,
+                      &job->records, &job->st_upd, &job->st_cand, &job->st_scan, &job->ctl};
     for (DevBuf *b : bufs) free_buf(job, *b);
     for (auto &e : job->sort_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : job->upd_ev)
         if (e) cudaEventDestroy(e);
     delete job;
     return EMP_OK;
@@ -777,30 +991,37 @@ emp_status emp_sort_pairs(emp_ctx *ctx, uint64_t *d_keys, uint32_t *d_vals, uint
     if (n >= (1ull << 30)) return EMP_E_UNSUPPORTED;
     cudaSetDevice(ctx->device);
     cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
-    void *k1 = nullptr, *v1 = nullptr, *scr = nullptr, *err = nullptr;
-    emp_status st = EMP_OK;
-    if (cudaMalloc(&k1, n * 8) != cudaSuccess || cudaMalloc(&v1, n * 4) != cudaSuccess ||
-        cudaMalloc(&scr, sort_scratch_bytes(n)) != cudaSuccess || cudaMalloc(&err, 8) != cudaSuccess) {
-        cudaGetLastError();
-        st = EMP_E_NOMEM;
-    }
-    if (st == EMP_OK) {
-        cudaMemsetAsync(err, 0, 8, s);
-        int res = sort_pairs(d_keys, d_vals, (uint64_t *)k1, (uint32_t *)v1, n, scr, nullptr, (uint32_t *)err, s);
-        if (res) {
-            cudaMemcpyAsync(d_keys, k1, n * 8, cudaMemcpyDeviceToDevice, s);
-            cudaMemcpyAsync(d_vals, v1, n * 4, cudaMemcpyDeviceToDevice, s);
+    auto grow = [&](DevBuf &b, size_t bytes) -> bool {
+        if (b.bytes >= bytes) return true;
+        b.release();
+        if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            return false;
         }
-        uint32_t herr = 0;
-        cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s);
-        if (cudaStreamSynchronize(s) != cudaSuccess) st = EMP_E_CUDA;
-        else if (herr & kErrSpin) st = EMP_E_TIMEOUT;
+        b.bytes = bytes;
+        return true;
+    };
+    // the working set is kept in the context for the next call
+    if (n > ctx->sort_cap || ctx->sort_calls > 100000) {
+        if (!grow(ctx->sort_k1, n * 8) || !grow(ctx->sort_v1, n * 4) || !grow(ctx->sort_scr, sort_scratch_bytes(n)) ||
+            !grow(ctx->sort_err, 16))
+            return EMP_E_NOMEM;
+        if (cudaMemsetAsync(ctx->sort_scr.p, 0, ctx->sort_scr.bytes, s) != cudaSuccess) return EMP_E_CUDA;
+        ctx->sort_cap = n;
+        ctx->sort_calls = 0;
     }
-    if (k1) cudaFree(k1);
-    if (v1) cudaFree(v1);
-    if (scr) cudaFree(scr);
-    if (err) cudaFree(err);
-    return st;
+    ++ctx->sort_calls;
+    // sort_err: the error word, then (8 bytes in) the device copy of n
+    uint64_t *err = ctx->sort_err.as<uint64_t>();
+    cudaMemsetAsync(err, 0, 8, s);
+    sort_pairs(d_keys, d_vals, ctx->sort_k1.as<uint64_t>(), ctx->sort_v1.as<uint32_t>(), n, ctx->sort_scr.p, err + 1,
+               reinterpret_cast<uint32_t *>(err), s);
+    uint32_t herr = 0;
+    cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return EMP_E_CUDA;
+    if (herr & kErrSpin) return EMP_E_TIMEOUT;
+    return EMP_OK;
 }
 
 }  // extern "C"

@@ -45,18 +45,19 @@ constexpr int kSortRadix = 1 << kSortBits;
 constexpr int kSortPasses = 8;           // 59-bit sort keys
 constexpr uint32_t kSortTile = 4096;
 __host__ __device__ inline uint64_t sort_tiles(uint64_t n) { return (n + kSortTile - 1) / kSortTile; }
-// bytes of zero-initialised scratch a sort of n pairs needs (look-back words,
-// tile counters, histograms)
+// Bytes of scratch a sort of up to n pairs needs (histograms, tile tickets,
+// epoch, look-back words).  Zero it once after allocation; it resets itself
+// between sorts (re-zero after 100000 sorts, before the epoch can wrap).
 size_t sort_scratch_bytes(uint64_t n);
-// Stable sort of (keys, vals) by sort_key(key, val).  Ping-pongs between
-// (k0,v0) and (k1,v1); returns 0 if the result is in (k0,v0), 1 otherwise.
-// hist_host (optional, kSortPasses*kSortRadix u32 pinned) enables skipping
-// passes whose digit is constant (costs one stream synchronisation).
-// pass_events (optional, 2*kSortPasses events): each digit pass is bracketed
-// by events 2p / 2p+1; *passes_run reports which passes ran (bit p).
-int sort_pairs(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, uint64_t n, void *scratch,
-               uint32_t *hist_host, uint32_t *err, cudaStream_t s, cudaEvent_t *pass_events = nullptr,
-               uint32_t *passes_run = nullptr);
+// Stable sort of (keys, vals) by sort_key(key, val), count *n_dev (device)
+// with n_max >= *n_dev sizing the grid.  Ping-pongs between (k0,v0) and
+// (k1,v1); kSortPasses is even, so the result ends in (k0,v0) (returns 0).
+// pass_events (optional, 2*kSortPasses events) bracket each digit pass.
+int sort_pairs_dev(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, const uint64_t *n_dev, uint64_t n_max,
+                   void *scratch, uint32_t *err, cudaStream_t s, cudaEvent_t *pass_events = nullptr);
+// Same with a host count (copied into the device word n_dev first).
+int sort_pairs(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, uint64_t n, void *scratch, uint64_t *n_dev,
+               uint32_t *err, cudaStream_t s, cudaEvent_t *pass_events = nullptr);
 
 // ---- rounds (k_round.cu) --------------------------------------------------
 void launch_dedup_mark(const uint64_t *skeys, const uint32_t *svals, uint64_t n2, uint8_t *alive, cudaStream_t s);
@@ -100,6 +101,53 @@ struct SearchPart {
 void launch_search_partitions(const uint64_t *akeys, uint64_t S, const uint64_t *bkeys, uint64_t P, uint64_t h,
                               const uint32_t *apos, const uint64_t *offs, uint64_t E, SearchPart *parts,
                               uint64_t cap, uint64_t *count, uint32_t *err, cudaStream_t s);
+// ---- device-resident round pipeline (k_pipeline.cu) ----------------------
+struct RoundCtl {
+    uint64_t n;        // entries of the current list (suffixes then prefixes)
+    uint64_t s;        // of which suffixes
+    uint64_t n_next;   // after this round's update
+    uint64_t s_next;
+    uint64_t c;        // candidates of this round
+    uint64_t e_round;  // edges of this round
+    uint64_t e_total;  // edges of all finished pipeline rounds
+    uint32_t round;    // round being run
+    uint32_t done;     // loop finished (suffix table empty or all rounds run)
+    uint32_t cur;      // list buffer holding the current list
+    uint32_t overflow; // the edge buffer was too small
+    uint32_t rounds;   // L - o
+    uint32_t pad0;
+    uint32_t tile_ctr[8];
+};
+struct RoundRecord {
+    uint64_t S, P, E, e0;  // table sizes, edges, first edge of the round
+};
+struct PipeArgs {
+    RoundCtl *ctl;
+    RoundRecord *records;
+    uint64_t *lk0, *lk1;
+    uint32_t *lv0, *lv1;
+    uint8_t *used_s, *used_p;
+    const uint32_t *cols;
+    uint64_t wpc;
+    const HashTables *tables;
+    int L;
+    int bloom_bits;
+    uint32_t *bloom_s, *bloom_p;
+    size_t bloom_bytes;
+    uint64_t *ck, *ck2;
+    uint32_t *cv, *cv2;
+    uint32_t *cnt;
+    uint64_t *offs;
+    uint32_t *efrom, *eto;
+    uint64_t ecap;
+    uint64_t *st_upd, *st_cand, *st_scan;  // epoch-tagged look-back words
+    uint32_t *err;
+};
+// Enqueue one round.  n_max bounds the list size, cand_max the candidates.
+// upd_events (optional, 2 events) bracket the update kernel.
+void launch_pipeline_round(const PipeArgs &a, uint64_t n_max, uint64_t cand_max, void *sort_scratch, cudaStream_t s,
+                           cudaEvent_t *upd_events = nullptr);
+
 void launch_join_count(const uint64_t *skeys, const uint32_t *svals, uint64_t n, uint32_t *cnt, cudaStream_t s);
 void launch_join_write(const uint64_t *skeys, const uint32_t *svals, uint64_t n, const uint32_t *cnt,
                        const uint64_t *offs, uint32_t *from, uint32_t *to, uint8_t *used_s, uint8_t *used_p,

@@ -76,6 +76,9 @@ typedef struct emp_stats {
     double ms_sort_passes; /* device time of all radix-sort digit passes (CUDA events per launch) */
     uint64_t sort_passes;  /* digit-pass launches */
     uint64_t sort_pass_elems; /* sum over those launches of the pairs each one moved */
+    double ms_update;      /* device time of the per-round table update kernel (CUDA events per launch) */
+    uint64_t update_launches; /* its launches that processed entries */
+    uint64_t update_bytes;    /* their algorithmic bytes (13 B read + 1/4 B of bases per entry in, 12 B per entry out) */
     uint64_t sfx_live[EMP_MAX_ROUNDS]; /* suffix-table size in round r */
     uint64_t pfx_live[EMP_MAX_ROUNDS]; /* prefix-table size in round r */
     uint64_t edges[EMP_MAX_ROUNDS];    /* edges written in round r */

@@ -64,6 +64,22 @@ def test_full_size_workload_matches_reference(engine, name):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["tiny", "sub_errors", "dups_palindromes", "split_r128k", "read_len_1"])
+@pytest.mark.parametrize("mode", ["sync_rounds", "edge_restart"])
+def test_round_paths_agree(engine, monkeypatch, name, mode):
+    """The host-synchronised rounds (full sort per round) and the
+    device-resident pipeline restarted after an edge-buffer overflow give the
+    reference's bytes too."""
+    if mode == "sync_rounds":
+        monkeypatch.setenv("EMP_SYNC_ROUNDS", "1")
+    else:
+        monkeypatch.setenv("EMP_EDGE_CAP", "7")
+    case = BY_NAME[name]
+    data, out, st = _run(engine, case)
+    assert hashlib.sha256(out).hexdigest() == GOLDEN[name]["sha256"]
+
+
+@pytest.mark.gpu
 def test_fingerprints_match_oracle(engine):
     for name in ["tiny", "odd_len", "lowercase", "read_len_255", "read_len_1", "dups_palindromes"]:
         data = BY_NAME[name].fastq()
