@@ -191,6 +191,55 @@ EMP_DEV uint64_t lookback_epoch(uint64_t *status, uint32_t tile, uint64_t aggreg
     return excl;
 }
 
+// Warp-parallel lookback_epoch: called by all 32 lanes of ONE warp; each probe
+// reads the 32 nearest unresolved predecessors at once, waits (bounded) until
+// all of them have published, and stops at the nearest inclusive prefix.
+// Returns the exclusive prefix in every lane.
+EMP_DEV uint64_t lookback_epoch_warp(uint64_t *status, uint32_t tile, uint64_t aggregate, uint32_t epoch,
+                                     uint32_t *err) {
+    const int lane = threadIdx.x & 31;
+    epoch &= 0xfffffu;
+    if (tile == 0) {
+        if (lane == 0) st_status(status, ep_word(epoch, kEpInc, aggregate));
+        return 0;
+    }
+    if (lane == 0) st_status(status + tile, ep_word(epoch, kEpAgg, aggregate));
+    uint64_t excl = 0;
+    int64_t t = (int64_t)tile - 1;  // nearest predecessor not yet folded in
+    bool failed = false;
+    while (!failed) {
+        const int64_t idx = t - lane;
+        uint64_t w = 0;
+        uint32_t f = 2;  // before tile 0: an inclusive prefix of 0
+        if (idx >= 0) {
+            uint32_t spins = 0;
+            w = ld_status(status + idx);
+            while ((f = ep_flag(w, epoch)) == 0) {
+                if (++spins > kSpinLimit) {
+                    failed = true;
+                    f = 2;
+                    w = 0;
+                    break;
+                }
+                if (spins > 32) __nanosleep(32);
+                w = ld_status(status + idx);
+            }
+        }
+        failed = __any_sync(0xffffffffu, failed);
+        const uint32_t inc = __ballot_sync(0xffffffffu, f == 2);
+        const int stop = inc ? __ffs(inc) - 1 : 31;  // nearest inclusive prefix in the window
+        uint64_t v = lane <= stop ? (w & kEpVal) : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        if (inc) break;
+        t -= 32;
+    }
+    if (failed && lane == 0) atomicOr(err, kErrSpin);
+    if (lane == 0) st_status(status + tile, ep_word(epoch, kEpInc, excl + aggregate));
+    return excl;
+}
+
 // Block-wide exclusive scan of one value per thread (blockDim.x = NT).
 template <int NT, typename T>
 EMP_DEV T block_exclusive_scan(T v, T *smem_warp /* NT/32 */, T *total) {

@@ -93,6 +93,8 @@ struct emp_job {
     PinnedBuf h_ctl, h_records;
     uint64_t ecap_hint = 0;
     uint64_t sorts_since_clear = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
     cudaEvent_t sort_ev[2 * kSortPasses] = {};
     cudaEvent_t upd_ev[2 * EMP_MAX_ROUNDS] = {};
     uint64_t sort_n = 0;
@@ -360,10 +362,85 @@ emp_status sync_round(emp_job *j, cudaStream_t s, const RoundEnv &env, int r, in
     return EMP_OK;
 }
 
-int bloom_bits_for(uint64_t entries) {
-    uint64_t want = entries * 32;
+// Enqueue pipeline rounds r0 .. rounds-1 after all work already on stream s.
+// One round is captured as a CUDA graph on the context's stream and replayed
+// once per round (every size lives in device memory); the two event nodes
+// around the update kernel are re-pointed to that round's events before each
+// replay.  EMP_NO_GRAPH=1 launches the kernels directly instead.
+void release_graph(emp_job *j) {
+    if (j->graph_exec) cudaGraphExecDestroy(j->graph_exec);
+    if (j->graph) cudaGraphDestroy(j->graph);
+    j->graph_exec = nullptr;
+    j->graph = nullptr;
+}
+
+emp_status launch_rounds_graph(emp_job *j, const PipeArgs &a, uint64_t nmax, int r0, int rounds, cudaStream_t s) {
+    cudaStream_t cs = j->ctx->stream;
+    release_graph(j);
+    if (std::getenv("EMP_NO_GRAPH")) {
+        for (int q = r0; q < rounds; ++q) {
+            launch_pipeline_round(a, nmax, nmax, s, q < EMP_MAX_ROUNDS ? j->upd_ev + 2 * q : nullptr);
+            ++j->sorts_since_clear;
+        }
+        return EMP_OK;
+    }
+    cudaEvent_t join_in = j->sort_ev[0], join_out = j->sort_ev[1];  // free here: the pipeline times no sort pass
+    EMP_CUDA(cudaEventRecord(join_in, s));
+    EMP_CUDA(cudaStreamWaitEvent(cs, join_in, 0));
+    const uint64_t l0 = g_launches.load();
+    cudaGraph_t graph = nullptr;
+    EMP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    launch_pipeline_round(a, nmax, nmax, cs, j->upd_ev);
+    cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+    const uint64_t per_round = g_launches.load() - l0;
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        return EMP_E_CUDA;
+    }
+    cudaGraphExec_t exec = nullptr;
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return EMP_E_CUDA;
+    }
+    // the event-record nodes, in capture order (before / after the update kernel)
+    size_t nn = 0;
+    cudaGraphGetNodes(graph, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    cudaGraphGetNodes(graph, nodes.data(), &nn);
+    cudaGraphNode_t evn[2] = {nullptr, nullptr};
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(nd, &t);
+        if (t != cudaGraphNodeTypeEventRecord) continue;
+        cudaEvent_t e = nullptr;
+        cudaGraphEventRecordNodeGetEvent(nd, &e);
+        if (e == j->upd_ev[0]) evn[0] = nd;
+        if (e == j->upd_ev[1]) evn[1] = nd;
+    }
+    emp_status rc = EMP_OK;
+    for (int q = r0; q < rounds && rc == EMP_OK; ++q) {
+        if (evn[0] && evn[1] && q < EMP_MAX_ROUNDS) {
+            cudaGraphExecEventRecordNodeSetEvent(exec, evn[0], j->upd_ev[2 * q]);
+            cudaGraphExecEventRecordNodeSetEvent(exec, evn[1], j->upd_ev[2 * q + 1]);
+        }
+        if (cudaGraphLaunch(exec, cs) != cudaSuccess) rc = EMP_E_CUDA;
+        ++j->sorts_since_clear;
+    }
+    if (rounds - r0 > 1) count_launch(per_round * (uint64_t)(rounds - r0 - 1));
+    cudaEventRecord(join_out, cs);
+    cudaStreamWaitEvent(s, join_out, 0);
+    j->graph_exec = exec;  // released by release_graph() after the stream synchronises
+    j->graph = graph;
+    return rc;
+}
+
+// log2 of the Bloom filter size for n list entries: 16 bits per entry (at
+// least 32 per entry of the larger table), 2^16 .. 2^30 bits.  The same rule
+// runs on the device (bloom_bits_for_n, k_pipeline.cu) as the lists shrink.
+int bloom_bits_for(uint64_t n) {
     int b = 16;
-    while (b < 30 && (1ull << b) < want) ++b;
+    while (b < 30 && (1ull << b) < 16 * n) ++b;
     return b;
 }
 
@@ -396,7 +473,7 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
 
     // ---- device-resident pipeline for rounds r .. rounds-1
     const uint64_t nmax = n_in;
-    const int bits = bloom_bits_for(S > P ? S : P);
+    const int bits = bloom_bits_for(n_in);
     const size_t bloom_bytes = (size_t)1 << (bits - 3);
     EMP_TRY(ensure(j, j->bloom_s, bloom_bytes));
     EMP_TRY(ensure(j, j->bloom_p, bloom_bytes));
@@ -426,7 +503,11 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
     hc->cur = (uint32_t)cur;
     hc->round = (uint32_t)r;
     hc->rounds = (uint32_t)env.rounds;
+    hc->bloom_bits = (uint32_t)bits;
     EMP_CUDA(cudaMemcpyAsync(j->ctl.p, hc, sizeof(RoundCtl), cudaMemcpyHostToDevice, s));
+    EMP_CUDA(cudaMemsetAsync(j->bloom_s.p, 0, bloom_bytes, s));
+    EMP_CUDA(cudaMemsetAsync(j->bloom_p.p, 0, bloom_bytes, s));
+    launch_sort_prepare(j->sort_scratch.as<SortScratch>(), true, s);
     PipeArgs a{};
     a.ctl = j->ctl.as<RoundCtl>();
     a.records = j->records.as<RoundRecord>();
@@ -440,10 +521,10 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
     a.wpc = env.wpc;
     a.tables = env.tables;
     a.L = env.L;
-    a.bloom_bits = bits;
+    a.bloom_bits_max = bits;
     a.bloom_s = j->bloom_s.as<uint32_t>();
     a.bloom_p = j->bloom_p.as<uint32_t>();
-    a.bloom_bytes = bloom_bytes;
+    a.sort = j->sort_scratch.as<SortScratch>();
     a.ck = j->ck.as<uint64_t>();
     a.ck2 = j->ck2.as<uint64_t>();
     a.cv = j->cv.as<uint32_t>();
@@ -458,15 +539,18 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
     a.st_scan = j->st_scan.as<uint64_t>();
     a.err = err_word(j);
     const int r0 = r;
-    for (int q = r0; q < env.rounds; ++q) {
-        cudaEvent_t *ev = q < EMP_MAX_ROUNDS ? j->upd_ev + 2 * q : nullptr;
-        launch_pipeline_round(a, nmax, nmax, j->sort_scratch.p, s, ev);
-        ++j->sorts_since_clear;
+    emp_status lrc = launch_rounds_graph(j, a, nmax, r0, env.rounds, s);
+    if (lrc != EMP_OK) {
+        cudaStreamSynchronize(j->ctx->stream);
+        release_graph(j);
+        return lrc;
     }
     EMP_CUDA(cudaMemcpyAsync(hc, j->ctl.p, sizeof(RoundCtl), cudaMemcpyDeviceToHost, s));
     EMP_CUDA(cudaMemcpyAsync(j->h_records.p, j->records.p, (size_t)env.rounds * sizeof(RoundRecord),
                              cudaMemcpyDeviceToHost, s));
-    EMP_TRY(sync_and_check(j, s));
+    emp_status src = sync_and_check(j, s);
+    release_graph(j);
+    EMP_TRY(src);
     if (hc->overflow) {
         *needed = hc->e_total;
         return kNeedEdgeRoom;
@@ -812,6 +896,7 @@ emp_status emp_job_destroy(emp_job *job) {
         if (e) cudaEventDestroy(e);
     for (auto &e : job->upd_ev)
         if (e) cudaEventDestroy(e);
+    release_graph(job);
     delete job;
     return EMP_OK;
 }

@@ -56,6 +56,7 @@ __global__ void __launch_bounds__(256) pl_update_filter_kernel(PipeArgs a) {
     const uint64_t n_in = ctl->n;
     const uint32_t cur = ctl->cur;
     const int L = a.L, r = (int)ctl->round;
+    const int bits = (int)ctl->bloom_bits;
     const uint32_t epoch = (uint32_t)(r + 1) * 4u + 0u;
     const uint64_t *kin = cur ? a.lk1 : a.lk0;
     const uint32_t *vin = cur ? a.lv1 : a.lv0;
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(256) pl_update_filter_kernel(PipeArgs a) {
                     keep[c] = true;
                     sfx_kept += t == 0;
                     uint32_t h1, h2;
-                    bloom_bits(k, a.bloom_bits, h1, h2);
+                    bloom_bits(k, bits, h1, h2);
                     uint32_t *bm = t ? a.bloom_p : a.bloom_s;
                     atomicOr(bm + (h1 >> 5), 1u << (h1 & 31));
                     atomicOr(bm + (h2 >> 5), 1u << (h2 & 31));
@@ -109,7 +110,10 @@ __global__ void __launch_bounds__(256) pl_update_filter_kernel(PipeArgs a) {
             running += tot;
         }
         if (sfx_kept) atomicAdd(&s_sfx, sfx_kept);
-        if (threadIdx.x == 0) s_base = lookback_epoch(a.st_upd, tile, running, epoch, a.err);
+        if (threadIdx.x < 32) {
+            const uint64_t b = lookback_epoch_warp(a.st_upd, tile, running, epoch, a.err);
+            if (threadIdx.x == 0) s_base = b;
+        }
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < kChunks; ++c) {
@@ -135,6 +139,7 @@ __global__ void __launch_bounds__(256) pl_candidates_kernel(PipeArgs a) {
     if (*(volatile uint32_t *)&ctl->done) return;
     const uint64_t n = ctl->n_next;
     if (ctl->s_next == 0 || ctl->s_next == n) return;  // one table empty: no edge this round
+    const int bits = (int)ctl->bloom_bits;
     const uint32_t cur = ctl->cur;
     const uint64_t *kin = cur ? a.lk0 : a.lk1;  // the list update_filter just wrote
     const uint32_t *vin = cur ? a.lv0 : a.lv1;
@@ -159,13 +164,16 @@ __global__ void __launch_bounds__(256) pl_candidates_kernel(PipeArgs a) {
             if (e < n) {
                 key[c] = kin[e];
                 val[c] = vin[e];
-                cand[c] = bloom_test((val[c] >> 31) ? a.bloom_s : a.bloom_p, key[c], a.bloom_bits);
+                cand[c] = bloom_test((val[c] >> 31) ? a.bloom_s : a.bloom_p, key[c], bits);
             }
             uint32_t tot;
             ex[c] = running + block_exclusive_scan<256, uint32_t>(cand[c] ? 1u : 0u, s_warp, &tot);
             running += tot;
         }
-        if (threadIdx.x == 0) s_base = lookback_epoch(a.st_cand, tile, running, epoch, a.err);
+        if (threadIdx.x < 32) {
+            const uint64_t b = lookback_epoch_warp(a.st_cand, tile, running, epoch, a.err);
+            if (threadIdx.x == 0) s_base = b;
+        }
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < kChunks; ++c) {
@@ -180,7 +188,17 @@ __global__ void __launch_bounds__(256) pl_candidates_kernel(PipeArgs a) {
     }
 }
 
+// Also clears this round's Bloom filters (the candidates kernel was their last
+// reader) so that the next round starts from empty filters.
 __global__ void pl_join_count_kernel(PipeArgs a) {
+    if (!*(volatile uint32_t *)&a.ctl->done) {
+        const uint64_t words = (1ull << a.ctl->bloom_bits) >> 5;
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words;
+             i += (uint64_t)gridDim.x * blockDim.x) {
+            a.bloom_s[i] = 0;
+            a.bloom_p[i] = 0;
+        }
+    }
     const uint64_t n = a.ctl->c;
     const uint64_t *k = a.ck;
     const uint32_t *v = a.cv;
@@ -228,7 +246,10 @@ __global__ void __launch_bounds__(256) pl_scan_kernel(PipeArgs a) {
             texcl[c] = running + block_exclusive_scan<256, uint64_t>(sum, s_warp, &tot);
             running += tot;
         }
-        if (threadIdx.x == 0) s_base = lookback_epoch(a.st_scan, tile, running, epoch, a.err);
+        if (threadIdx.x < 32) {
+            const uint64_t b = lookback_epoch_warp(a.st_scan, tile, running, epoch, a.err);
+            if (threadIdx.x == 0) s_base = b;
+        }
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -275,7 +296,17 @@ __global__ void pl_join_write_kernel(PipeArgs a) {
     }
 }
 
-__global__ void pl_round_end_kernel(PipeArgs a) {
+// log2 of the Bloom filter size for a round over n entries (32 bits per
+// entry of the larger table, which holds at most n entries), capped.
+EMP_DEV uint32_t bloom_bits_for_n(uint64_t n, int max_bits) {
+    uint32_t b = 16;
+    while ((int)b < max_bits && (1ull << b) < 16 * n) ++b;
+    return b;
+}
+
+// Round bookkeeping, then the next round's preparation: Bloom filter size,
+// candidate-sort scratch (histogram, tickets, look-back epoch).
+__global__ void __launch_bounds__(256) pl_round_end_kernel(PipeArgs a) {
     RoundCtl *ctl = a.ctl;
     if (threadIdx.x == 0 && !ctl->done) {
         const uint64_t S = ctl->s_next, P = ctl->n_next - ctl->s_next;
@@ -294,6 +325,7 @@ __global__ void pl_round_end_kernel(PipeArgs a) {
             ctl->s = S;
             ctl->cur ^= 1u;
             ctl->round = r + 1;
+            ctl->bloom_bits = bloom_bits_for_n(ctl->n_next, a.bloom_bits_max);
             if (r + 1 >= ctl->rounds) ctl->done = 1;
         }
         ctl->n_next = 0;
@@ -301,7 +333,9 @@ __global__ void pl_round_end_kernel(PipeArgs a) {
         ctl->c = 0;
         ctl->e_round = 0;
     }
-    __syncthreads();
+    for (int i = threadIdx.x; i < kSortPasses * kSortRadix; i += blockDim.x) (&a.sort->hist[0][0])[i] = 0;
+    if (threadIdx.x < kSortPasses) a.sort->tile_ctr[threadIdx.x] = 0;
+    if (threadIdx.x == 0) a.sort->epoch = (a.sort->epoch + 1) & 0x1ffffu;
     if (threadIdx.x < 8) ctl->tile_ctr[threadIdx.x] = 0;
 }
 
@@ -309,26 +343,24 @@ static unsigned persistent_grid(uint64_t tiles, unsigned cap) {
     return (unsigned)(tiles < 1 ? 1 : (tiles < cap ? tiles : cap));
 }
 
-void launch_pipeline_round(const PipeArgs &a, uint64_t n_max, uint64_t cand_max, void *sort_scratch, cudaStream_t s,
+void launch_pipeline_round(const PipeArgs &a, uint64_t n_max, uint64_t cand_max, cudaStream_t s,
                            cudaEvent_t *upd_events) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const unsigned gu = persistent_grid(upd_tiles(n_max), (unsigned)sms * 8);
-    count_launch(5);
-    cudaMemsetAsync(a.bloom_s, 0, a.bloom_bytes, s);
-    cudaMemsetAsync(a.bloom_p, 0, a.bloom_bytes, s);
-    if (upd_events) cudaEventRecord(upd_events[0], s);
+    count_launch(6);
+    // External: inside a stream capture these become event-record nodes (timestamps)
+    if (upd_events) cudaEventRecordWithFlags(upd_events[0], s, cudaEventRecordExternal);
     pl_update_filter_kernel<<<gu, 256, 0, s>>>(a);
-    if (upd_events) cudaEventRecord(upd_events[1], s);
+    if (upd_events) cudaEventRecordWithFlags(upd_events[1], s, cudaEventRecordExternal);
     pl_candidates_kernel<<<gu, 256, 0, s>>>(a);
-    sort_pairs_dev(a.ck, a.cv, a.ck2, a.cv2, &a.ctl->c, cand_max, sort_scratch, a.err, s, nullptr);
+    sort_pairs_prepared(a.ck, a.cv, a.ck2, a.cv2, &a.ctl->c, cand_max, a.sort, a.err, s);
     const unsigned gj = (unsigned)sms * 8;
     pl_join_count_kernel<<<gj, 256, 0, s>>>(a);
     pl_scan_kernel<<<persistent_grid(scan_tiles(cand_max), (unsigned)sms * 8), 256, 0, s>>>(a);
     pl_join_write_kernel<<<gj, 256, 0, s>>>(a);
-    pl_round_end_kernel<<<1, 32, 0, s>>>(a);
-    count_launch(1);
+    pl_round_end_kernel<<<1, 256, 0, s>>>(a);
 }
 
 }  // namespace emp

@@ -45,6 +45,17 @@ constexpr int kSortRadix = 1 << kSortBits;
 constexpr int kSortPasses = 8;           // 59-bit sort keys
 constexpr uint32_t kSortTile = 4096;
 __host__ __device__ inline uint64_t sort_tiles(uint64_t n) { return (n + kSortTile - 1) / kSortTile; }
+constexpr uint32_t kSmallSort = 4096;    // up to this many pairs: one CTA sorts in shared memory
+struct SortScratch {
+    uint32_t hist[kSortPasses][kSortRadix];  // digit counts of the pairs being sorted
+    uint32_t tile_ctr[kSortPasses];          // per-pass tile tickets
+    uint32_t epoch;                          // look-back epoch of the current sort
+    uint32_t pad[7];
+    // followed by sort_tiles(n_max) * kSortRadix epoch-tagged look-back words
+};
+// Start a new sort on this scratch: advance the epoch, reset the tickets and
+// (zero_hist) the histogram.  One CTA.
+void launch_sort_prepare(SortScratch *sc, bool zero_hist, cudaStream_t s);
 // Bytes of scratch a sort of up to n pairs needs (histograms, tile tickets,
 // epoch, look-back words).  Zero it once after allocation; it resets itself
 // between sorts (re-zero after 100000 sorts, before the epoch can wrap).
@@ -55,6 +66,10 @@ size_t sort_scratch_bytes(uint64_t n);
 // pass_events (optional, 2*kSortPasses events) bracket each digit pass.
 int sort_pairs_dev(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, const uint64_t *n_dev, uint64_t n_max,
                    void *scratch, uint32_t *err, cudaStream_t s, cudaEvent_t *pass_events = nullptr);
+// The same without the prepare step: the caller has already prepared the
+// scratch (pipeline rounds prepare the next sort in their round_end kernel).
+void sort_pairs_prepared(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, const uint64_t *n_dev,
+                         uint64_t n_max, SortScratch *sc, uint32_t *err, cudaStream_t s);
 // Same with a host count (copied into the device word n_dev first).
 int sort_pairs(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, uint64_t n, void *scratch, uint64_t *n_dev,
                uint32_t *err, cudaStream_t s, cudaEvent_t *pass_events = nullptr);
@@ -115,7 +130,7 @@ struct RoundCtl {
     uint32_t cur;      // list buffer holding the current list
     uint32_t overflow; // the edge buffer was too small
     uint32_t rounds;   // L - o
-    uint32_t pad0;
+    uint32_t bloom_bits;  // log2 of the Bloom filter size in use this round
     uint32_t tile_ctr[8];
 };
 struct RoundRecord {
@@ -131,9 +146,9 @@ struct PipeArgs {
     uint64_t wpc;
     const HashTables *tables;
     int L;
-    int bloom_bits;
+    int bloom_bits_max;  // the filters hold 2^bloom_bits_max bits each
     uint32_t *bloom_s, *bloom_p;
-    size_t bloom_bytes;
+    SortScratch *sort;   // scratch of the candidate sort
     uint64_t *ck, *ck2;
     uint32_t *cv, *cv2;
     uint32_t *cnt;
@@ -145,7 +160,9 @@ struct PipeArgs {
 };
 // Enqueue one round.  n_max bounds the list size, cand_max the candidates.
 // upd_events (optional, 2 events) bracket the update kernel.
-void launch_pipeline_round(const PipeArgs &a, uint64_t n_max, uint64_t cand_max, void *sort_scratch, cudaStream_t s,
+// The Bloom filters must start zeroed and a.sort prepared (launch_sort_prepare)
+// before the first round; every round leaves both ready for the next.
+void launch_pipeline_round(const PipeArgs &a, uint64_t n_max, uint64_t cand_max, cudaStream_t s,
                            cudaEvent_t *upd_events = nullptr);
 
 void launch_join_count(const uint64_t *skeys, const uint32_t *svals, uint64_t n, uint32_t *cnt, cudaStream_t s);
