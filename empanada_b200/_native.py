@@ -60,13 +60,15 @@ class Stats(ctypes.Structure):
         ("ms_update", ctypes.c_double),
         ("update_launches", ctypes.c_uint64),
         ("update_bytes", ctypes.c_uint64),
+        ("ms_round_kernel", ctypes.c_double),
+        ("round_kernel_bytes", ctypes.c_uint64),
         ("sfx_live", ctypes.c_uint64 * MAX_ROUNDS),
         ("pfx_live", ctypes.c_uint64 * MAX_ROUNDS),
         ("edges", ctypes.c_uint64 * MAX_ROUNDS),
     ]
 
     def to_dict(self) -> dict:
-        d = {f: getattr(self, f) for f, _ in self._fields_[:20]}
+        d = {f: getattr(self, f) for f, _ in self._fields_[:22]}
         r = self.n_rounds
         d["sfx_live"] = list(self.sfx_live[:r])
         d["pfx_live"] = list(self.pfx_live[:r])

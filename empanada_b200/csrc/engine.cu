@@ -95,6 +95,8 @@ struct emp_job {
     uint64_t sorts_since_clear = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    DevBuf st_join, st_sort, coop_job, coop_ctl, coop_trace, coop_probe;  // cooperative all-rounds kernel
+    PinnedBuf h_coop;
     cudaEvent_t sort_ev[2 * kSortPasses] = {};
     cudaEvent_t upd_ev[2 * EMP_MAX_ROUNDS] = {};
     uint64_t sort_n = 0;
@@ -444,6 +446,169 @@ int bloom_bits_for(uint64_t n) {
     return b;
 }
 
+// Profiling aid: per-round phase durations (us) of the cooperative kernel.
+void write_coop_trace(emp_job *j, const char *path, int rounds, int r0, const RoundRecord *rec, cudaStream_t s) {
+    std::vector<uint64_t> t((size_t)rounds * kCoopTracePhases);
+    if (cudaMemcpyAsync(t.data(), j->coop_trace.p, t.size() * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return;
+    FILE *f = std::fopen(path, "w");
+    if (!f) return;
+    std::fprintf(f, "round,update_us,candidates_us,sort_a_us,sort_b_us,join_end_us,S,P,C,E\n");
+    for (int i = 0; i + r0 < rounds; ++i) {
+        const uint64_t *p = &t[(size_t)i * kCoopTracePhases];
+        if (!p[4]) break;
+        const uint64_t prev = i ? t[(size_t)(i - 1) * kCoopTracePhases + 4] : p[0];
+        const RoundRecord &x = rec[i + r0];
+        std::fprintf(f, "%d,%.2f,%.2f,%.2f,%.2f,%.2f,%llu,%llu,%llu,%llu\n", i + r0, (p[0] - prev) / 1e3,
+                     (p[1] - p[0]) / 1e3, (p[2] - p[1]) / 1e3, (p[3] - p[2]) / 1e3, (p[4] - p[3]) / 1e3,
+                     (unsigned long long)x.S, (unsigned long long)x.P, (unsigned long long)x.C,
+                     (unsigned long long)x.E);
+    }
+    std::fclose(f);
+}
+
+// Profiling aid: per-CTA stamps (ns after the earliest stamp) of one iteration.
+void write_coop_probe(emp_job *j, const char *path, int grid, cudaStream_t s) {
+    std::vector<uint64_t> t((size_t)grid * kCoopProbePoints);
+    if (cudaMemcpyAsync(t.data(), j->coop_probe.p, t.size() * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return;
+    uint64_t t0 = ~0ull;
+    for (uint64_t x : t)
+        if (x && x < t0) t0 = x;
+    FILE *f = std::fopen(path, "w");
+    if (!f) return;
+    std::fprintf(f, "cta");
+    for (int p = 0; p < kCoopProbePoints; ++p) std::fprintf(f, ",p%d", p);
+    std::fprintf(f, "\n");
+    for (int c = 0; c < grid; ++c) {
+        std::fprintf(f, "%d", c);
+        for (int p = 0; p < kCoopProbePoints; ++p) {
+            const uint64_t x = t[(size_t)c * kCoopProbePoints + p];
+            std::fprintf(f, ",%lld", x ? (long long)(x - t0) : -1ll);
+        }
+        std::fprintf(f, "\n");
+    }
+    std::fclose(f);
+}
+
+// Rounds r0 .. of one job through the cooperative kernel (k_coop.cu): one
+// launch, no host round trip until all rounds are done.  `a` carries the
+// buffers run_rounds allocated for the pipeline.
+emp_status run_rounds_coop(emp_job *j, cudaStream_t s, const RoundEnv &env, const PipeArgs &a, uint64_t nmax,
+                           int bits, int r0, int cur, uint64_t n_in, uint64_t *needed) {
+    emp_stats &st = j->st;
+    EMP_TRY(ensure(j, j->st_join, coop_tiles(nmax) * 8 + 8));
+    EMP_TRY(ensure(j, j->st_sort, sort_tiles(nmax) * kSortRadix * 8 + 8));
+    EMP_TRY(ensure(j, j->coop_job, sizeof(CoopJob)));
+    EMP_TRY(ensure(j, j->coop_ctl, sizeof(CoopCtl)));
+    if (!j->h_coop.ensure(sizeof(CoopJob) + sizeof(CoopCtl))) return EMP_E_NOMEM;
+    EMP_CUDA(cudaMemsetAsync(j->st_upd.p, 0, j->st_upd.bytes, s));
+    EMP_CUDA(cudaMemsetAsync(j->st_cand.p, 0, j->st_cand.bytes, s));
+    EMP_CUDA(cudaMemsetAsync(j->st_join.p, 0, j->st_join.bytes, s));
+    EMP_CUDA(cudaMemsetAsync(j->st_sort.p, 0, j->st_sort.bytes, s));
+    CoopJob *hj = j->h_coop.as<CoopJob>();
+    CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + 1);
+    std::memset(hj, 0, sizeof(CoopJob) + sizeof(CoopCtl));
+    hj->lk[0] = a.lk0;
+    hj->lk[1] = a.lk1;
+    hj->lv[0] = a.lv0;
+    hj->lv[1] = a.lv1;
+    hj->used_s = a.used_s;
+    hj->used_p = a.used_p;
+    hj->cols = a.cols;
+    hj->wpc = a.wpc;
+    hj->tables = a.tables;
+    hj->L = env.L;
+    hj->rounds = env.rounds;
+    hj->bloom_s = a.bloom_s;
+    hj->bloom_p = a.bloom_p;
+    hj->bloom_bits_max = bits;
+    hj->ck = a.ck;
+    hj->ck2 = a.ck2;
+    hj->cv = a.cv;
+    hj->cv2 = a.cv2;
+    hj->efrom = a.efrom;
+    hj->eto = a.eto;
+    hj->ecap = a.ecap;
+    hj->records = a.records;
+    hj->st_upd = a.st_upd;
+    hj->st_cand = a.st_cand;
+    hj->st_join = j->st_join.as<uint64_t>();
+    hj->st_sort = j->st_sort.as<uint64_t>();
+    hj->n = n_in;
+    hj->round = (uint32_t)r0;
+    hj->cur = (uint32_t)cur;
+    hj->bloom_bits[0] = (uint32_t)bits;
+    hc->njobs = 1;
+    hc->active = 1;
+    const char *trace_path = std::getenv("EMP_COOP_TRACE");  // profiling: per-phase timestamps
+    if (trace_path) {
+        EMP_TRY(ensure(j, j->coop_trace, (size_t)env.rounds * kCoopTracePhases * 8));
+        EMP_CUDA(cudaMemsetAsync(j->coop_trace.p, 0, j->coop_trace.bytes, s));
+        hc->trace = j->coop_trace.as<uint64_t>();
+        hc->trace_cap = (uint32_t)env.rounds;
+    }
+    // profiling: per-CTA stamps of one iteration, EMP_COOP_PROBE=<csv path>:<iteration>
+    const char *probe_env = std::getenv("EMP_COOP_PROBE");
+    std::string probe_path;
+    const int grid = coop_grid_size();
+    if (probe_env) {
+        const char *colon = std::strrchr(probe_env, ':');
+        probe_path.assign(probe_env, colon ? (size_t)(colon - probe_env) : std::strlen(probe_env));
+        hc->probe_iter = colon ? (uint32_t)std::atoi(colon + 1) : 0u;
+        EMP_TRY(ensure(j, j->coop_probe, (size_t)grid * kCoopProbePoints * 8));
+        EMP_CUDA(cudaMemsetAsync(j->coop_probe.p, 0, j->coop_probe.bytes, s));
+        hc->probe = j->coop_probe.as<uint64_t>();
+    }
+    EMP_CUDA(cudaMemcpyAsync(j->coop_job.p, hj, sizeof(CoopJob), cudaMemcpyHostToDevice, s));
+    EMP_CUDA(cudaMemcpyAsync(j->coop_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
+    cudaEvent_t e0 = j->upd_ev[0], e1 = j->upd_ev[1];
+    EMP_CUDA(cudaEventRecord(e0, s));
+    EMP_CUDA(launch_coop_rounds(j->coop_job.as<CoopJob>(), j->coop_ctl.as<CoopCtl>(), err_word(j), s));
+    EMP_CUDA(cudaEventRecord(e1, s));
+    EMP_CUDA(cudaMemcpyAsync(hj, j->coop_job.p, sizeof(CoopJob), cudaMemcpyDeviceToHost, s));
+    EMP_CUDA(cudaMemcpyAsync(hc, j->coop_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
+    EMP_CUDA(cudaMemcpyAsync(j->h_records.p, j->records.p, (size_t)env.rounds * sizeof(RoundRecord),
+                             cudaMemcpyDeviceToHost, s));
+    EMP_TRY(sync_and_check(j, s));
+    if (hc->err & kErrSpin) return EMP_E_TIMEOUT;
+    st.ms_round_kernel += ms_between(e0, e1);
+    if (hj->overflow) {
+        *needed = hj->e_total;
+        return kNeedEdgeRoom;
+    }
+    const uint64_t E_all = hj->e_total;
+    if (E_all) {
+        if (!j->h_from.ensure(E_all * 4) || !j->h_to.ensure(E_all * 4)) return EMP_E_NOMEM;
+        EMP_CUDA(cudaMemcpyAsync(j->h_from.p, j->efrom.p, E_all * 4, cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaMemcpyAsync(j->h_to.p, j->eto.p, E_all * 4, cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaStreamSynchronize(s));
+    }
+    const RoundRecord *rec = j->h_records.as<RoundRecord>();
+    const int r_end = (int)hj->round;  // rounds run with a non-empty suffix table
+    if (trace_path) write_coop_trace(j, trace_path, env.rounds, r0, rec, s);
+    if (probe_env) write_coop_probe(j, probe_path.c_str(), grid, s);
+    uint64_t prev_n = n_in;
+    for (int q = r0; q < r_end; ++q) {
+        const RoundRecord &x = rec[q];
+        const uint64_t n_out = x.S + x.P;
+        // update + candidates + candidate sort (about two 24-byte moves per pair) + join
+        st.round_kernel_bytes += 13 * prev_n + prev_n / 4 + 24 * n_out + 72 * x.C + 8 * x.E;
+        if (q < EMP_MAX_ROUNDS) {
+            st.sfx_live[q] = x.S;
+            st.pfx_live[q] = x.P;
+            st.edges[q] = x.E;
+        }
+        if (x.P) emit_record(j, env.L - 1 - q, x.e0, x.e0 + x.E);
+        st.n_edges += x.E;
+        prev_n = n_out;
+    }
+    st.n_rounds = r_end;
+    return EMP_OK;
+}
+
 // All rounds: synchronous ones while a round could split into several search
 // partitions (sizes only shrink), then the device-resident pipeline for the
 // rest with a single synchronisation at the end.  Returns kNeedEdgeRoom with
@@ -539,6 +704,8 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
     a.st_scan = j->st_scan.as<uint64_t>();
     a.err = err_word(j);
     const int r0 = r;
+    if (!std::getenv("EMP_NO_COOP") && coop_grid_size() > 0)
+        return run_rounds_coop(j, s, env, a, nmax, bits, r0, cur, n_in, needed);
     emp_status lrc = launch_rounds_graph(j, a, nmax, r0, env.rounds, s);
     if (lrc != EMP_OK) {
         cudaStreamSynchronize(j->ctx->stream);
@@ -890,7 +1057,9 @@ emp_status emp_job_destroy(emp_job *job) {
                       &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
                       &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts, &job->lk_init,
                       &job->lv_init, &job->bloom_s, &job->bloom_p, &job->ck, &job->cv, &job->ck2, &job->cv2,
-                      &job->records, &job->st_upd, &job->st_cand, &job->st_scan, &job->ctl};
+                      &job->records, &job->st_upd, &job->st_cand, &job->st_scan, &job->ctl, &job->st_join,
+                      &job->st_sort, &job->coop_job, &job->coop_ctl, &job->coop_trace,
+                      &job->coop_probe};
     for (DevBuf *b : bufs) free_buf(job, *b);
     for (auto &e : job->sort_ev)
         if (e) cudaEventDestroy(e);

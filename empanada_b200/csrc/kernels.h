@@ -135,6 +135,7 @@ struct RoundCtl {
 };
 struct RoundRecord {
     uint64_t S, P, E, e0;  // table sizes, edges, first edge of the round
+    uint64_t C;            // candidates sorted (cooperative kernel only)
 };
 struct PipeArgs {
     RoundCtl *ctl;
@@ -164,6 +165,59 @@ struct PipeArgs {
 // before the first round; every round leaves both ready for the next.
 void launch_pipeline_round(const PipeArgs &a, uint64_t n_max, uint64_t cand_max, cudaStream_t s,
                            cudaEvent_t *upd_events = nullptr);
+
+// ---- cooperative multi-job rounds (k_coop.cu) -----------------------------
+constexpr int kCoopMaxJobs = 1024;
+constexpr uint32_t kCoopTile = 4096;  // entries per tile in every phase
+__host__ __device__ inline uint64_t coop_tiles(uint64_t n) { return (n + kCoopTile - 1) / kCoopTile; }
+enum CoopSortMode : uint32_t { kSortNone = 0, kSortSmall = 1, kSortMsd = 2, kSortLsd = 3, kSortRank = 4 };
+struct CoopJob {
+    // fixed for the run (filled by the host)
+    uint64_t *lk[2];
+    uint32_t *lv[2];
+    uint8_t *used_s, *used_p;
+    const uint32_t *cols;
+    uint64_t wpc;
+    const HashTables *tables;
+    int32_t L, rounds;
+    uint32_t *bloom_s, *bloom_p;
+    int32_t bloom_bits_max, pad0;
+    uint64_t *ck, *ck2;  // candidates, n_max capacity
+    uint32_t *cv, *cv2;
+    uint32_t *efrom, *eto;
+    uint64_t ecap;
+    RoundRecord *records;
+    uint64_t *st_upd, *st_cand, *st_join, *st_sort;  // look-back words (zeroed before the launch)
+    // device-updated state (the host sets n, round, cur, bloom_bits[0]; zeroes the rest)
+    uint64_t n, n_next, s_next, c, e_round, e_total;
+    uint32_t round, done, cur, overflow, mode, cand_done, join_done, pad1;
+    uint32_t bloom_bits[2];        // filter size of the kernel's even / odd iterations
+    uint32_t hist[9][kSortRadix];  // candidate sort-key digits 0..7 and the top-8-bit digit
+};
+struct CoopCtl {
+    uint32_t njobs;
+    uint32_t active;    // jobs not finished (the host sets njobs)
+    uint32_t all_done;
+    uint32_t any_lsd;
+    uint32_t bar_count;
+    uint32_t bar_gen;
+    uint32_t err;
+    uint32_t pad;
+    uint32_t ticket[16];
+    uint64_t *trace;  // optional: kCoopTracePhases globaltimer stamps per iteration
+    uint32_t trace_cap;  // iterations the trace holds
+    uint32_t probe_iter;  // iteration whose per-CTA stamps go to `probe`
+    uint64_t *probe;      // optional: kCoopProbePoints stamps per CTA (profiling)
+};
+constexpr int kCoopTracePhases = 8;
+constexpr int kCoopProbePoints = 32;
+constexpr uint32_t kCoopMaxSubs = 4;  // a streaming tile holds up to 4 x 4096 entries (staged in shared memory)
+// Shared memory and grid of the cooperative kernel on the current device
+// (0 when it cannot run cooperatively there).
+size_t coop_smem_bytes();
+int coop_grid_size();
+// Run every remaining round of every job in one cooperative launch.
+cudaError_t launch_coop_rounds(CoopJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
 
 void launch_join_count(const uint64_t *skeys, const uint32_t *svals, uint64_t n, uint32_t *cnt, cudaStream_t s);
 void launch_join_write(const uint64_t *skeys, const uint32_t *svals, uint64_t n, const uint32_t *cnt,

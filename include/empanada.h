@@ -79,6 +79,8 @@ typedef struct emp_stats {
     double ms_update;      /* device time of the per-round table update kernel (CUDA events per launch) */
     uint64_t update_launches; /* its launches that processed entries */
     uint64_t update_bytes;    /* their algorithmic bytes (13 B read + 1/4 B of bases per entry in, 12 B per entry out) */
+    double ms_round_kernel;   /* device time of the cooperative all-rounds kernel (CUDA events), 0 if not used */
+    uint64_t round_kernel_bytes; /* its algorithmic bytes: update + candidates + candidate sort + join, per round */
     uint64_t sfx_live[EMP_MAX_ROUNDS]; /* suffix-table size in round r */
     uint64_t pfx_live[EMP_MAX_ROUNDS]; /* prefix-table size in round r */
     uint64_t edges[EMP_MAX_ROUNDS];    /* edges written in round r */

@@ -65,14 +65,17 @@ def test_full_size_workload_matches_reference(engine, name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["tiny", "sub_errors", "dups_palindromes", "split_r128k", "read_len_1"])
-@pytest.mark.parametrize("mode", ["sync_rounds", "edge_restart"])
+@pytest.mark.parametrize("mode", ["sync_rounds", "graph_rounds", "edge_restart", "graph_edge_restart"])
 def test_round_paths_agree(engine, monkeypatch, name, mode):
-    """The host-synchronised rounds (full sort per round) and the
-    device-resident pipeline restarted after an edge-buffer overflow give the
-    reference's bytes too."""
+    """Every round driver gives the reference's bytes: host-synchronised
+    rounds (full sort per round), the per-round graph pipeline, and either
+    device-resident driver restarted after an edge-buffer overflow (the
+    default driver is the cooperative all-rounds kernel)."""
     if mode == "sync_rounds":
         monkeypatch.setenv("EMP_SYNC_ROUNDS", "1")
-    else:
+    if mode.startswith("graph"):
+        monkeypatch.setenv("EMP_NO_COOP", "1")
+    if mode.endswith("edge_restart"):
         monkeypatch.setenv("EMP_EDGE_CAP", "7")
     case = BY_NAME[name]
     data, out, st = _run(engine, case)
