@@ -226,6 +226,16 @@ class Job:
         return out
 
 
+SORT_STATIC_MAX_PAIRS = _native.SORT_STATIC_MAX_PAIRS
+
+
+def sort_pairs_static(keys_ptr: int, vals_ptr: int, n: int, stream: int = 0) -> None:
+    """Engine.sort_pairs on the current device without any allocation: the
+    working set is the library's static device array, so n is at most
+    SORT_STATIC_MAX_PAIRS, and calls whose GPU work overlaps race on it."""
+    check(_native.lib().emp_sort_pairs_static(keys_ptr, vals_ptr, n, stream or None), "emp_sort_pairs_static")
+
+
 def run_bytes(fastq, device: int = 0, engine: Engine | None = None, **params) -> tuple[bytes, dict]:
     """FASTQ bytes in host memory -> (output.bin bytes, stats)."""
     eng = engine or Engine(device)

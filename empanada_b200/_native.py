@@ -97,7 +97,9 @@ SIGNATURES = {
     "emp_run_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Params), ctypes.c_int,
                                     ctypes.POINTER(Stats)]),
     "emp_sort_pairs": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp]),
+    "emp_sort_pairs_static": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, _vp]),
 }
+SORT_STATIC_MAX_PAIRS = 1 << 20  # EMP_SORT_STATIC_MAX_PAIRS
 
 _lib = None
 

@@ -147,6 +147,17 @@ emp_status emp_run_file(const char *input_path, const char *output_path, const e
  * stream: a cudaStream_t or NULL. */
 emp_status emp_sort_pairs(emp_ctx *ctx, uint64_t *d_keys, uint32_t *d_vals, uint64_t n, void *stream);
 
+/* emp_sort_pairs without any allocation (no counterpart in the reference).
+ * The working set -- alternate key/value buffers, histograms, look-back
+ * words, error word -- lives in one statically sized device array of this
+ * library (about 12.6 MB per device), so n is limited to
+ * EMP_SORT_STATIC_MAX_PAIRS; a larger n returns EMP_E_INVAL.  Runs on the
+ * current device; returns after the sort has finished on `stream`.  All
+ * calls on one device share that array: calls whose GPU work overlaps (other
+ * streams, other host threads) race on it and give wrong results. */
+#define EMP_SORT_STATIC_MAX_PAIRS (1u << 20)
+emp_status emp_sort_pairs_static(uint64_t *d_keys, uint32_t *d_vals, uint64_t n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
