@@ -84,7 +84,7 @@ struct emp_job {
     bool fed_last = false;
     double ms_h2d = 0.0;
     // work buffers
-    DevBuf tile_counts, tile_excl, status, misc, seq_start, seq_end, hq, idx, rec_of, keys0, cols;
+    DevBuf tile_counts, tile_excl, status, misc, seq_start, seq_end, hq, idx, rec_of, keys0, cols, seq2;
     DevBuf sk0, sv0, sk1, sv1, alive, lk0, lv0, lk1, lv1, used_s, used_p, cnt, offs, efrom, eto, sort_scratch;
     DevBuf akeys, apos, bkeys, parts;  // record splitting
     PinnedBuf h_parts;
@@ -96,6 +96,7 @@ struct emp_job {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     DevBuf st_join, st_sort, coop_job, coop_ctl, coop_trace, coop_probe;  // cooperative all-rounds kernel
+    DevBuf bk_lst0, bk_lst1, bk_offs, bk_tile_base, bk_st_a, bk_st_b, bk_scratch, bk_job;  // bucket kernel
     PinnedBuf h_coop;
     cudaEvent_t sort_ev[2 * kSortPasses] = {};
     cudaEvent_t upd_ev[2 * EMP_MAX_ROUNDS] = {};
@@ -256,6 +257,8 @@ struct RoundEnv {
     uint64_t M;
     uint64_t wpc;
     const HashTables *tables;
+    const uint32_t *seq2;  // read-major 2-bit bases, wpr words per read
+    int wpr;
 };
 
 // One round with host synchronisation: used while the tables are large enough
@@ -446,24 +449,29 @@ int bloom_bits_for(uint64_t n) {
     return b;
 }
 
-// Profiling aid: per-round phase durations (us) of the cooperative kernel.
-void write_coop_trace(emp_job *j, const char *path, int rounds, int r0, const RoundRecord *rec, cudaStream_t s) {
+// Profiling aid: per-round phase durations (us) of a cooperative round kernel
+// whose barriers stamp phases 0 .. nph-1 of every iteration.
+void write_coop_trace(emp_job *j, const char *path, int rounds, int r0, const RoundRecord *rec, cudaStream_t s,
+                      int nph, const char *phase_cols) {
     std::vector<uint64_t> t((size_t)rounds * kCoopTracePhases);
     if (cudaMemcpyAsync(t.data(), j->coop_trace.p, t.size() * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return;
     FILE *f = std::fopen(path, "w");
     if (!f) return;
-    std::fprintf(f, "round,update_us,candidates_us,sort_a_us,sort_b_us,join_end_us,S,P,C,E\n");
+    std::fprintf(f, "round,%s,S,P,C,E\n", phase_cols);
     for (int i = 0; i + r0 < rounds; ++i) {
         const uint64_t *p = &t[(size_t)i * kCoopTracePhases];
-        if (!p[4]) break;
-        const uint64_t prev = i ? t[(size_t)(i - 1) * kCoopTracePhases + 4] : p[0];
+        if (!p[nph - 1]) break;
+        uint64_t prev = i ? t[(size_t)(i - 1) * kCoopTracePhases + nph - 1] : p[0];
+        std::fprintf(f, "%d", i + r0);
+        for (int q = 0; q < nph; ++q) {
+            std::fprintf(f, ",%.2f", (p[q] - prev) / 1e3);
+            prev = p[q];
+        }
         const RoundRecord &x = rec[i + r0];
-        std::fprintf(f, "%d,%.2f,%.2f,%.2f,%.2f,%.2f,%llu,%llu,%llu,%llu\n", i + r0, (p[0] - prev) / 1e3,
-                     (p[1] - p[0]) / 1e3, (p[2] - p[1]) / 1e3, (p[3] - p[2]) / 1e3, (p[4] - p[3]) / 1e3,
-                     (unsigned long long)x.S, (unsigned long long)x.P, (unsigned long long)x.C,
-                     (unsigned long long)x.E);
+        std::fprintf(f, ",%llu,%llu,%llu,%llu\n", (unsigned long long)x.S, (unsigned long long)x.P,
+                     (unsigned long long)x.C, (unsigned long long)x.E);
     }
     std::fclose(f);
 }
@@ -588,7 +596,9 @@ emp_status run_rounds_coop(emp_job *j, cudaStream_t s, const RoundEnv &env, cons
     }
     const RoundRecord *rec = j->h_records.as<RoundRecord>();
     const int r_end = (int)hj->round;  // rounds run with a non-empty suffix table
-    if (trace_path) write_coop_trace(j, trace_path, env.rounds, r0, rec, s);
+    if (trace_path)
+        write_coop_trace(j, trace_path, env.rounds, r0, rec, s, 5,
+                         "update_us,candidates_us,sort_a_us,sort_b_us,join_end_us");
     if (probe_env) write_coop_probe(j, probe_path.c_str(), grid, s);
     uint64_t prev_n = n_in;
     for (int q = r0; q < r_end; ++q) {
@@ -596,6 +606,125 @@ emp_status run_rounds_coop(emp_job *j, cudaStream_t s, const RoundEnv &env, cons
         const uint64_t n_out = x.S + x.P;
         // update + candidates + candidate sort (about two 24-byte moves per pair) + join
         st.round_kernel_bytes += 13 * prev_n + prev_n / 4 + 24 * n_out + 72 * x.C + 8 * x.E;
+        if (q < EMP_MAX_ROUNDS) {
+            st.sfx_live[q] = x.S;
+            st.pfx_live[q] = x.P;
+            st.edges[q] = x.E;
+        }
+        if (x.P) emit_record(j, env.L - 1 - q, x.e0, x.e0 + x.E);
+        st.n_edges += x.E;
+        prev_n = n_out;
+    }
+    st.n_rounds = r_end;
+    return EMP_OK;
+}
+
+// Rounds r0 .. of one job through the bucket kernel (k_bucket.cu): one
+// cooperative launch, two grid barriers per round.
+emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, int r0, int cur, uint64_t n_in,
+                             uint64_t ecap, uint64_t *needed) {
+    emp_stats &st = j->st;
+    const uint64_t nmax = n_in;
+    const uint64_t ktiles = bkt_tiles(nmax);
+    EMP_TRY(ensure(j, j->bk_lst0, nmax * sizeof(BktEntry)));
+    EMP_TRY(ensure(j, j->bk_lst1, nmax * sizeof(BktEntry)));
+    EMP_TRY(ensure(j, j->bk_offs, bkt_offs_words(nmax) * 4));
+    EMP_TRY(ensure(j, j->bk_tile_base, ktiles * 8));
+    EMP_TRY(ensure(j, j->bk_st_a, ktiles * 8 + 8));
+    EMP_TRY(ensure(j, j->bk_st_b, ((size_t)1 << bkt_bits(nmax)) * 8 + 8));
+    EMP_TRY(ensure(j, j->bk_scratch, bkt_scratch_bytes(nmax)));
+    EMP_TRY(ensure(j, j->bk_job, sizeof(BktJob)));
+    EMP_TRY(ensure(j, j->coop_ctl, sizeof(CoopCtl)));
+    EMP_TRY(ensure(j, j->efrom, ecap * 4));
+    EMP_TRY(ensure(j, j->eto, ecap * 4));
+    EMP_TRY(ensure(j, j->records, (size_t)env.rounds * sizeof(RoundRecord)));
+    if (!j->h_coop.ensure(sizeof(BktJob) + sizeof(CoopCtl)) ||
+        !j->h_records.ensure((size_t)env.rounds * sizeof(RoundRecord)))
+        return EMP_E_NOMEM;
+    EMP_CUDA(cudaMemsetAsync(j->bk_st_a.p, 0, j->bk_st_a.bytes, s));
+    EMP_CUDA(cudaMemsetAsync(j->bk_st_b.p, 0, j->bk_st_b.bytes, s));
+    BktJob *hj = j->h_coop.as<BktJob>();
+    CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + 1);
+    std::memset(hj, 0, sizeof(BktJob) + sizeof(CoopCtl));
+    hj->lk_in = cur ? j->lk1.as<uint64_t>() : j->lk0.as<uint64_t>();
+    hj->lv_in = cur ? j->lv1.as<uint32_t>() : j->lv0.as<uint32_t>();
+    hj->used_s = j->used_s.as<uint8_t>();
+    hj->used_p = j->used_p.as<uint8_t>();
+    hj->lst[0] = j->bk_lst0.as<BktEntry>();
+    hj->lst[1] = j->bk_lst1.as<BktEntry>();
+    hj->seq2 = env.seq2;
+    hj->wpr = env.wpr;
+    hj->L = env.L;
+    hj->rounds = env.rounds;
+    hj->tables = env.tables;
+    hj->offs = j->bk_offs.as<uint32_t>();
+    hj->tile_base = j->bk_tile_base.as<uint64_t>();
+    hj->st_a = j->bk_st_a.as<uint64_t>();
+    hj->st_b = j->bk_st_b.as<uint64_t>();
+    hj->efrom = j->efrom.as<uint32_t>();
+    hj->eto = j->eto.as<uint32_t>();
+    hj->ecap = ecap;
+    hj->records = j->records.as<RoundRecord>();
+    hj->scratch = j->bk_scratch.as<uint8_t>();
+    hj->n_max = nmax;
+    hj->round = (uint32_t)r0;
+    hj->end_iter = 0xffffffffu;
+    hj->it[0].n_in = n_in;
+    hj->it[0].bb = bkt_bits(n_in);
+    hc->njobs = 1;
+    hc->active = 1;
+    const char *trace_path = std::getenv("EMP_COOP_TRACE");  // profiling: per-phase timestamps
+    if (trace_path) {
+        EMP_TRY(ensure(j, j->coop_trace, (size_t)env.rounds * kCoopTracePhases * 8));
+        EMP_CUDA(cudaMemsetAsync(j->coop_trace.p, 0, j->coop_trace.bytes, s));
+        hc->trace = j->coop_trace.as<uint64_t>();
+        hc->trace_cap = (uint32_t)env.rounds;
+    }
+    const char *probe_env = std::getenv("EMP_COOP_PROBE");  // profiling: per-CTA stamps of one iteration
+    std::string probe_path;
+    const int grid = bucket_grid_size();
+    if (probe_env) {
+        const char *colon = std::strrchr(probe_env, ':');
+        probe_path.assign(probe_env, colon ? (size_t)(colon - probe_env) : std::strlen(probe_env));
+        hc->probe_iter = colon ? (uint32_t)std::atoi(colon + 1) : 0u;
+        EMP_TRY(ensure(j, j->coop_probe, (size_t)grid * kCoopProbePoints * 8));
+        EMP_CUDA(cudaMemsetAsync(j->coop_probe.p, 0, j->coop_probe.bytes, s));
+        hc->probe = j->coop_probe.as<uint64_t>();
+    }
+    EMP_CUDA(cudaMemcpyAsync(j->bk_job.p, hj, sizeof(BktJob), cudaMemcpyHostToDevice, s));
+    EMP_CUDA(cudaMemcpyAsync(j->coop_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
+    cudaEvent_t e0 = j->upd_ev[0], e1 = j->upd_ev[1];
+    EMP_CUDA(cudaEventRecord(e0, s));
+    EMP_CUDA(launch_bucket_rounds(j->bk_job.as<BktJob>(), j->coop_ctl.as<CoopCtl>(), err_word(j), s));
+    EMP_CUDA(cudaEventRecord(e1, s));
+    EMP_CUDA(cudaMemcpyAsync(hj, j->bk_job.p, sizeof(BktJob), cudaMemcpyDeviceToHost, s));
+    EMP_CUDA(cudaMemcpyAsync(hc, j->coop_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
+    EMP_CUDA(cudaMemcpyAsync(j->h_records.p, j->records.p, (size_t)env.rounds * sizeof(RoundRecord),
+                             cudaMemcpyDeviceToHost, s));
+    EMP_TRY(sync_and_check(j, s));
+    if (hc->err & kErrSpin) return EMP_E_TIMEOUT;
+    st.ms_round_kernel += ms_between(e0, e1);
+    if (hj->overflow) {
+        *needed = hj->e_total;
+        return kNeedEdgeRoom;
+    }
+    const uint64_t E_all = hj->e_total;
+    if (E_all) {
+        if (!j->h_from.ensure(E_all * 4) || !j->h_to.ensure(E_all * 4)) return EMP_E_NOMEM;
+        EMP_CUDA(cudaMemcpyAsync(j->h_from.p, j->efrom.p, E_all * 4, cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaMemcpyAsync(j->h_to.p, j->eto.p, E_all * 4, cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaStreamSynchronize(s));
+    }
+    const RoundRecord *rec = j->h_records.as<RoundRecord>();
+    const int r_end = (int)hj->round;  // rounds run with a non-empty suffix table
+    if (trace_path) write_coop_trace(j, trace_path, env.rounds, r0, rec, s, 2, "a_us,b_us");
+    if (probe_env) write_coop_probe(j, probe_path.c_str(), grid, s);
+    uint64_t prev_n = n_in;
+    for (int q = r0; q < r_end; ++q) {
+        const RoundRecord &x = rec[q];
+        const uint64_t n_out = x.S + x.P;
+        // phase A reads each entry and writes the kept ones; phase B gathers them
+        st.round_kernel_bytes += 16 * prev_n + 32 * n_out + 8 * x.E;
         if (q < EMP_MAX_ROUNDS) {
             st.sfx_live[q] = x.S;
             st.pfx_live[q] = x.P;
@@ -635,6 +764,9 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
         ++r;
     }
     if (r >= env.rounds) return EMP_OK;
+    if (!std::getenv("EMP_NO_COOP") && !std::getenv("EMP_NO_BUCKET") && n_in <= kBktMaxEntries &&
+        bucket_grid_size() > 0)
+        return run_rounds_bucket(j, s, env, r, cur, n_in, ecap, needed);
 
     // ---- device-resident pipeline for rounds r .. rounds-1
     const uint64_t nmax = n_in;
@@ -839,10 +971,12 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
     const uint64_t wpc = (n + 15) / 16;
     EMP_TRY(ensure(j, j->rec_of, n * 4));
     EMP_TRY(ensure(j, j->cols, (uint64_t)L * wpc * 4));
+    const int wpr = (L + 15) / 16;
+    EMP_TRY(ensure(j, j->seq2, (uint64_t)n * wpr * 4));
     EMP_TRY(ensure(j, j->keys0, n2 * 8));
     launch_scatter_hq(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), n_rec, j->rec_of.as<uint32_t>(), s);
     launch_fingerprint_pack(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->rec_of.as<uint32_t>(), n, L, tables,
-                            j->keys0.as<uint64_t>(), j->cols.as<uint32_t>(), wpc, s);
+                            j->keys0.as<uint64_t>(), j->cols.as<uint32_t>(), wpc, j->seq2.as<uint32_t>(), wpr, s);
     j->n_ends = n2;
     cudaEventRecord(ev.e[1], s);
 
@@ -884,7 +1018,7 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
         EMP_CUDA(cudaMemcpyAsync(j->lv_init.p, j->lv0.p, 2 * U * 4, cudaMemcpyDeviceToDevice, s));
         uint64_t ecap = j->ecap_hint ? j->ecap_hint : (4 * U > (1u << 20) ? 4 * U : (1u << 20));
         if (const char *ec = std::getenv("EMP_EDGE_CAP")) ecap = std::strtoull(ec, nullptr, 10) + 1;
-        const RoundEnv env{L, rounds, M, wpc, tables};
+        const RoundEnv env{L, rounds, M, wpc, tables, j->seq2.as<uint32_t>(), wpr};
         for (int attempt = 0;; ++attempt) {
             uint64_t needed = 0;
             emp_status rc = run_rounds(j, s, env, U, ecap, &needed);
@@ -1052,14 +1186,15 @@ emp_status emp_job_destroy(emp_job *job) {
     cudaSetDevice(job->ctx->device);
     cudaStreamSynchronize(job->ctx->stream);
     DevBuf *bufs[] = {&job->fq, &job->tile_counts, &job->tile_excl, &job->status, &job->misc, &job->seq_start,
-                      &job->seq_end, &job->hq, &job->idx, &job->rec_of, &job->keys0, &job->cols, &job->sk0,
+                      &job->seq_end, &job->hq, &job->idx, &job->rec_of, &job->keys0, &job->cols, &job->seq2, &job->sk0,
                       &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
                       &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
                       &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts, &job->lk_init,
                       &job->lv_init, &job->bloom_s, &job->bloom_p, &job->ck, &job->cv, &job->ck2, &job->cv2,
                       &job->records, &job->st_upd, &job->st_cand, &job->st_scan, &job->ctl, &job->st_join,
                       &job->st_sort, &job->coop_job, &job->coop_ctl, &job->coop_trace,
-                      &job->coop_probe};
+                      &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_offs, &job->bk_tile_base, &job->bk_st_a,
+                      &job->bk_st_b, &job->bk_scratch, &job->bk_job};
     for (DevBuf *b : bufs) free_buf(job, *b);
     for (auto &e : job->sort_ev)
         if (e) cudaEventDestroy(e);

@@ -31,78 +31,13 @@
 // entries, sized so that one wave of CTAs covers the job when it can.  A tile
 // compacts its survivors into shared memory, resolves its output offset with
 // one look-back and copies them out contiguously.
-#include "sort_block.cuh"
+#include "coop_common.cuh"
 
 namespace emp {
 
-constexpr int kT = kBlkThreads;         // 512
-constexpr int kC = kCoopTile / kT;      // 8 entries per thread per 4096-entry chunk
 constexpr uint32_t kSub = kCoopTile;    // 4096
-constexpr uint64_t kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;
 constexpr size_t kStageBytes = (size_t)kCoopMaxSubs * kSub * (sizeof(uint64_t) + sizeof(uint32_t));
 constexpr size_t kCoopDynSmem = kStageBytes > kBlockSortSmem ? kStageBytes : kBlockSortSmem;
-
-// L1 is not coherent across SMs: everything another CTA of this launch may
-// have written (job state, lists, candidates, used marks) is read around L1,
-// job state through volatile loads and bulk data through ld.global.cg.
-template <class T>
-EMP_DEV T vld(const T &x) {
-    return *(const volatile T *)&x;
-}
-
-EMP_DEV uint64_t globaltimer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Grid barrier (all CTAs co-resident: cooperative launch).  Bounded wait: on
-// timeout the error bit is raised and false returned; the kernel then exits.
-EMP_DEV bool grid_barrier_raw(CoopCtl *ctl, uint32_t *s_flag) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile uint32_t *gen = &ctl->bar_gen;
-        const uint32_t g = *gen;
-        __threadfence();
-        const uint32_t arrived = atomicAdd(&ctl->bar_count, 1u);
-        uint32_t ok = 1;
-        if (arrived == gridDim.x - 1) {
-            ctl->bar_count = 0;
-            __threadfence();
-            atomicAdd(&ctl->bar_gen, 1u);
-        } else {
-            const uint64_t t0 = globaltimer();
-            uint32_t polls = 0;
-            while (*gen == g) {
-                if ((++polls & 255) == 0 && globaltimer() - t0 > kBarrierTimeoutNs) {
-                    atomicOr(&ctl->err, kErrSpin);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(20);
-            }
-        }
-        __threadfence();
-        *s_flag = ok && !(*(volatile uint32_t *)&ctl->err & kErrSpin);
-    }
-    __syncthreads();
-    return *s_flag != 0;
-}
-
-// profiling: stamp point p of this CTA in the probed iteration (a later tile
-// of the same phase overwrites the stamps of an earlier one)
-EMP_DEV void probe(const CoopCtl *ctl, uint32_t iter, int p) {
-    if (threadIdx.x == 0 && ctl->probe && iter == ctl->probe_iter)
-        ctl->probe[(uint64_t)blockIdx.x * kCoopProbePoints + p] = globaltimer();
-}
-
-// barrier + optional phase timestamp (ctl->trace) for profiling
-EMP_DEV bool grid_barrier(CoopCtl *ctl, uint32_t *s_flag, uint32_t iter, int phase) {
-    const bool ok = grid_barrier_raw(ctl, s_flag);
-    if (blockIdx.x == 0 && threadIdx.x == 0 && ctl->trace && iter < ctl->trace_cap)
-        ctl->trace[(uint64_t)iter * kCoopTracePhases + phase] = globaltimer();
-    return ok;
-}
 
 struct CoopShared {
     uint32_t pref[kCoopMaxJobs + 1];  // tile prefix over jobs for the current phase
@@ -116,126 +51,6 @@ struct CoopShared {
     uint32_t tile, flag, sfx, last;
 };
 
-// Tile scans in chunk-major order (element (c, thread) comes before
-// (c, thread+1) and before (c+1, any)) with two __syncthreads per tile:
-// warp ballots / shuffles per chunk, then one warp scans the 8x16 warp counts.
-EMP_DEV uint32_t tile_flag_scan(const bool (&f)[kC], uint32_t (&ex)[kC], uint32_t *s) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t lt = lanemask_lt_u32();
-    uint32_t inw[kC];
-#pragma unroll
-    for (int c = 0; c < kC; ++c) {
-        const uint32_t b = __ballot_sync(0xffffffffu, f[c]);
-        inw[c] = __popc(b & lt);
-        if (lane == 0) s[c * kBlkWarps + warp] = __popc(b);
-    }
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t a[4], sum = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            a[q] = s[lane * 4 + q];
-            sum += a[q];
-        }
-        uint32_t incl = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        uint32_t run = incl - sum;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            s[lane * 4 + q] = run;
-            run += a[q];
-        }
-        if (lane == 31) s[kC * kBlkWarps] = incl;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < kC; ++c) ex[c] = s[c * kBlkWarps + warp] + inw[c];
-    const uint32_t total = s[kC * kBlkWarps];
-    __syncthreads();  // s is reused by the next call
-    return total;
-}
-
-EMP_DEV uint64_t tile_value_scan(const uint32_t (&v)[kC], uint64_t (&ex)[kC], uint64_t *s) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t inw[kC];
-#pragma unroll
-    for (int c = 0; c < kC; ++c) {
-        uint64_t incl = v[c];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        inw[c] = incl - v[c];
-        if (lane == 31) s[c * kBlkWarps + warp] = incl;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        uint64_t a[4], sum = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            a[q] = s[lane * 4 + q];
-            sum += a[q];
-        }
-        uint64_t incl = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        uint64_t run = incl - sum;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            s[lane * 4 + q] = run;
-            run += a[q];
-        }
-        if (lane == 31) s[kC * kBlkWarps] = incl;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < kC; ++c) ex[c] = s[c * kBlkWarps + warp] + inw[c];
-    const uint64_t total = s[kC * kBlkWarps];
-    __syncthreads();
-    return total;
-}
-
-// prefix of per-job tile counts; count(j) evaluated for every job
-template <class F>
-EMP_DEV uint32_t build_prefix(CoopShared &sh, int J, F count) {
-    // each thread takes two consecutive jobs (J <= 1024)
-    const int j0 = 2 * threadIdx.x, j1 = j0 + 1;
-    const uint32_t c0 = j0 < J ? count(j0) : 0u, c1 = j1 < J ? count(j1) : 0u;
-    uint32_t tot;
-    const uint32_t ex = block_exclusive_scan<kT, uint32_t>(c0 + c1, sh.scan32, &tot);
-    if (j0 <= J) sh.pref[j0] = ex;
-    if (j1 <= J) sh.pref[j1] = ex + c0;
-    if (threadIdx.x == 0) sh.pref[J] = tot;
-    __syncthreads();
-    return tot;
-}
-
-// take tiles from the ticket until all `total` are gone; f(job, local tile)
-template <class F>
-EMP_DEV void tile_loop(CoopShared &sh, uint32_t *ticket, int J, uint32_t total, F f) {
-    for (;;) {
-        if (threadIdx.x == 0) sh.tile = atomicAdd(ticket, 1u);
-        __syncthreads();
-        const uint32_t t = sh.tile;
-        __syncthreads();
-        if (t >= total) break;
-        int lo = 0, hi = J;
-        while (hi - lo > 1) {
-            const int m = (lo + hi) >> 1;
-            if (sh.pref[m] <= t) lo = m;
-            else hi = m;
-        }
-        f(lo, t - sh.pref[lo]);
-    }
-}
 
 // 4096-entry chunks per streaming tile: enough that the job's tiles form one
 // wave of CTAs when they can (at most kCoopMaxSubs)

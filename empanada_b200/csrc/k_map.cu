@@ -144,7 +144,8 @@ __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__
                                                                const uint32_t *__restrict__ rec_of, uint64_t n,
                                                                int L, const HashTables *__restrict__ tables,
                                                                uint64_t *__restrict__ keys,
-                                                               uint32_t *__restrict__ cols, uint64_t wpc) {
+                                                               uint32_t *__restrict__ cols, uint64_t wpc,
+                                                               uint32_t *__restrict__ seq2, int wpr) {
     __shared__ uint32_t s_pow1[kMaxReadLen + 1], s_pow2[kMaxReadLen + 1];
     __shared__ uint8_t s_codes[kFpReads * kFpRow];
     for (int i = threadIdx.x; i <= kMaxReadLen; i += blockDim.x) {
@@ -217,6 +218,16 @@ __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__
         }
         cols[(uint64_t)col * wpc + w0 + q] = word;
     }
+    if (!seq2) return;
+    // read-major copy: word w of read i holds positions 16w .. 16w+15
+    for (int p = threadIdx.x; p < kFpReads * wpr; p += blockDim.x) {
+        const int row = p / wpr, w = p - row * wpr;
+        if (i0 + row >= n) break;
+        uint32_t word = 0;
+        for (int m = 0; m < 16 && 16 * w + m < L; ++m)
+            word |= (uint32_t)s_codes[row * kFpRow + 16 * w + m] << (2 * m);
+        seq2[(i0 + row) * wpr + w] = word;
+    }
 }
 
 static unsigned grid_for(uint64_t work, unsigned per_block, unsigned cap) {
@@ -255,11 +266,12 @@ void launch_scatter_hq(const uint32_t *hq, const uint32_t *idx, uint64_t n_rec, 
 
 void launch_fingerprint_pack(const uint8_t *fq, const uint64_t *seq_start, const uint32_t *rec_of, uint64_t n,
                              int L, const HashTables *tables, uint64_t *keys, uint32_t *cols, uint64_t wpc,
-                             cudaStream_t s) {
+                             uint32_t *seq2, int wpr, cudaStream_t s) {
     if (!n) return;
     const uint64_t blocks = (n + kFpReads - 1) / kFpReads;
     count_launch();
-    fingerprint_pack_kernel<<<(unsigned)blocks, 256, 0, s>>>(fq, seq_start, rec_of, n, L, tables, keys, cols, wpc);
+    fingerprint_pack_kernel<<<(unsigned)blocks, 256, 0, s>>>(fq, seq_start, rec_of, n, L, tables, keys, cols, wpc,
+                                                              seq2, wpr);
 }
 
 }  // namespace emp

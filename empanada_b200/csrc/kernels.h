@@ -37,7 +37,7 @@ void launch_scatter_hq(const uint32_t *hq, const uint32_t *idx, uint64_t n_rec, 
 // cols[c * wpc + i/16] holds base c of read i at bits 2*(i%16).
 void launch_fingerprint_pack(const uint8_t *fq, const uint64_t *seq_start, const uint32_t *rec_of, uint64_t n,
                              int L, const HashTables *tables, uint64_t *keys, uint32_t *cols, uint64_t wpc,
-                             cudaStream_t s);
+                             uint32_t *seq2, int wpr, cudaStream_t s);
 
 // ---- radix sort (k_sort.cu) ---------------------------------------------
 constexpr int kSortBits = 8;
@@ -218,6 +218,65 @@ size_t coop_smem_bytes();
 int coop_grid_size();
 // Run every remaining round of every job in one cooperative launch.
 cudaError_t launch_coop_rounds(CoopJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
+
+// ---- bucket rounds (k_bucket.cu) ------------------------------------------
+// Each round of each job: phase A streams the live entries in 4096-entry
+// tiles (drop used ones, hash step, partition the tile by the top bits of the
+// new sort key); phase B gives each key bucket to one CTA, which gathers the
+// bucket's pieces from every tile, finds the keys present in both tables with
+// a hash set, sorts those entries and joins them.
+struct BktEntry {
+    uint64_t key;   // fp1 << 32 | fp2
+    uint32_t val;   // rid | table << 31, or kBktTomb once used
+    uint32_t word;  // cached 16 bases (one seq2 word) of the entry's read
+};
+constexpr uint32_t kBktTomb = 0xffffffffu;
+constexpr uint32_t kBktTile = 4096;                // entries per phase-A tile
+constexpr int kBktMinBits = 8, kBktMaxBits = 12;   // 256 .. 4096 buckets
+constexpr uint64_t kBktTarget = 3072;              // mean entries per bucket aimed at
+constexpr uint64_t kBktMaxEntries = 16ull << 20;   // larger lists use the other drivers
+__host__ __device__ inline uint64_t bkt_tiles(uint64_t n) { return (n + kBktTile - 1) / kBktTile; }
+__host__ __device__ inline uint32_t bkt_bits(uint64_t n) {
+    uint32_t b = kBktMinBits;
+    while (b < (uint32_t)kBktMaxBits && (kBktTarget << b) < n) ++b;
+    return b;
+}
+struct BktIter {         // one per iteration parity
+    uint64_t n_in;       // entries entering phase A
+    uint64_t n_out;      // entries kept by phase A
+    uint64_t s_out;      // of which suffixes
+    uint64_t cands;      // entries found in both tables
+    uint64_t edges;      // edges of the round
+    uint32_t bb;         // bucket bits of the round
+    uint32_t b_done;     // buckets finished
+};
+struct BktJob {
+    const uint64_t *lk_in;   // the list at launch (id order, suffixes then prefixes)
+    const uint32_t *lv_in;
+    const uint8_t *used_s, *used_p;  // marks of rounds run before the launch
+    BktEntry *lst[2];        // lists written by phase A, n_max entries each
+    const uint32_t *seq2;    // read-major 2-bit bases, wpr words per read
+    int32_t wpr, L, rounds, pad0;
+    const HashTables *tables;
+    uint32_t *offs;          // per phase-A tile: 2^bb + 1 bucket starts
+    uint64_t *tile_base;     // per phase-A tile: its first output entry
+    uint64_t *st_a, *st_b;   // look-back words of phase-A tiles and of buckets
+    uint32_t *efrom, *eto;
+    uint64_t ecap;
+    RoundRecord *records;
+    uint8_t *scratch;        // bkt_scratch_bytes(n_max): buckets too big for shared memory
+    uint64_t n_max;
+    uint32_t round;          // next round to run
+    uint32_t end_iter;       // iteration in which the job ended (0xffffffff while running)
+    uint32_t overflow;       // the edge buffer was too small
+    uint32_t pad1;
+    uint64_t e_total;        // edges of the finished rounds of this launch
+    BktIter it[2];
+};
+size_t bkt_scratch_bytes(uint64_t n_max);
+size_t bkt_offs_words(uint64_t n_max);   // u32 words of BktJob::offs
+int bucket_grid_size();                  // 0: no cooperative launch on this device
+cudaError_t launch_bucket_rounds(BktJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
 
 void launch_join_count(const uint64_t *skeys, const uint32_t *svals, uint64_t n, uint32_t *cnt, cudaStream_t s);
 void launch_join_write(const uint64_t *skeys, const uint32_t *svals, uint64_t n, const uint32_t *cnt,

@@ -65,16 +65,19 @@ def test_full_size_workload_matches_reference(engine, name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["tiny", "sub_errors", "dups_palindromes", "split_r128k", "read_len_1"])
-@pytest.mark.parametrize("mode", ["sync_rounds", "graph_rounds", "edge_restart", "graph_edge_restart"])
+@pytest.mark.parametrize("mode", ["sync_rounds", "graph_rounds", "coop_rounds", "edge_restart", "graph_edge_restart",
+                                  "coop_edge_restart"])
 def test_round_paths_agree(engine, monkeypatch, name, mode):
     """Every round driver gives the reference's bytes: host-synchronised
-    rounds (full sort per round), the per-round graph pipeline, and either
-    device-resident driver restarted after an edge-buffer overflow (the
-    default driver is the cooperative all-rounds kernel)."""
+    rounds (full sort per round), the per-round graph pipeline, the Bloom-
+    filter cooperative kernel, and each device-resident driver restarted
+    after an edge-buffer overflow (the default driver is the bucket kernel)."""
     if mode == "sync_rounds":
         monkeypatch.setenv("EMP_SYNC_ROUNDS", "1")
     if mode.startswith("graph"):
         monkeypatch.setenv("EMP_NO_COOP", "1")
+    if mode.startswith("coop"):
+        monkeypatch.setenv("EMP_NO_BUCKET", "1")
     if mode.endswith("edge_restart"):
         monkeypatch.setenv("EMP_EDGE_CAP", "7")
     case = BY_NAME[name]
