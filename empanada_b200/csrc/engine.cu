@@ -96,7 +96,7 @@ struct emp_job {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     DevBuf st_join, st_sort, coop_job, coop_ctl, coop_trace, coop_probe;  // cooperative all-rounds kernel
-    DevBuf bk_lst0, bk_lst1, bk_offs, bk_tile_base, bk_st_a, bk_st_b, bk_scratch, bk_job;  // bucket kernel
+    DevBuf bk_lst0, bk_lst1, bk_offs, bk_tile_base, bk_spans, bk_sfrom, bk_sto, bk_scratch, bk_job;  // bucket kernel
     PinnedBuf h_coop;
     cudaEvent_t sort_ev[2 * kSortPasses] = {};
     cudaEvent_t upd_ev[2 * EMP_MAX_ROUNDS] = {};
@@ -626,12 +626,15 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     emp_stats &st = j->st;
     const uint64_t nmax = n_in;
     const uint64_t ktiles = bkt_tiles(nmax);
+    const int grid = bucket_grid_size();
+    const uint32_t nb_max = bkt_count(nmax, (uint32_t)grid);
     EMP_TRY(ensure(j, j->bk_lst0, nmax * sizeof(BktEntry)));
     EMP_TRY(ensure(j, j->bk_lst1, nmax * sizeof(BktEntry)));
-    EMP_TRY(ensure(j, j->bk_offs, bkt_offs_words(nmax) * 4));
+    EMP_TRY(ensure(j, j->bk_offs, bkt_offs_words(nmax, (uint32_t)grid) * 4));
     EMP_TRY(ensure(j, j->bk_tile_base, ktiles * 8));
-    EMP_TRY(ensure(j, j->bk_st_a, ktiles * 8 + 8));
-    EMP_TRY(ensure(j, j->bk_st_b, ((size_t)1 << bkt_bits(nmax)) * 8 + 8));
+    EMP_TRY(ensure(j, j->bk_spans, (size_t)env.rounds * nb_max * sizeof(BktSpan)));
+    EMP_TRY(ensure(j, j->bk_sfrom, ecap * 4));
+    EMP_TRY(ensure(j, j->bk_sto, ecap * 4));
     EMP_TRY(ensure(j, j->bk_scratch, bkt_scratch_bytes(nmax)));
     EMP_TRY(ensure(j, j->bk_job, sizeof(BktJob)));
     EMP_TRY(ensure(j, j->coop_ctl, sizeof(CoopCtl)));
@@ -641,8 +644,6 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     if (!j->h_coop.ensure(sizeof(BktJob) + sizeof(CoopCtl)) ||
         !j->h_records.ensure((size_t)env.rounds * sizeof(RoundRecord)))
         return EMP_E_NOMEM;
-    EMP_CUDA(cudaMemsetAsync(j->bk_st_a.p, 0, j->bk_st_a.bytes, s));
-    EMP_CUDA(cudaMemsetAsync(j->bk_st_b.p, 0, j->bk_st_b.bytes, s));
     BktJob *hj = j->h_coop.as<BktJob>();
     CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + 1);
     std::memset(hj, 0, sizeof(BktJob) + sizeof(CoopCtl));
@@ -659,18 +660,21 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     hj->tables = env.tables;
     hj->offs = j->bk_offs.as<uint32_t>();
     hj->tile_base = j->bk_tile_base.as<uint64_t>();
-    hj->st_a = j->bk_st_a.as<uint64_t>();
-    hj->st_b = j->bk_st_b.as<uint64_t>();
+    hj->spans = j->bk_spans.as<BktSpan>();
+    hj->sfrom = j->bk_sfrom.as<uint32_t>();
+    hj->sto = j->bk_sto.as<uint32_t>();
     hj->efrom = j->efrom.as<uint32_t>();
     hj->eto = j->eto.as<uint32_t>();
     hj->ecap = ecap;
     hj->records = j->records.as<RoundRecord>();
     hj->scratch = j->bk_scratch.as<uint8_t>();
     hj->n_max = nmax;
+    hj->nb_max = nb_max;
+    hj->r0 = r0;
     hj->round = (uint32_t)r0;
     hj->end_iter = 0xffffffffu;
     hj->it[0].n_in = n_in;
-    hj->it[0].bb = bkt_bits(n_in);
+    hj->it[0].nb = bkt_count(n_in, (uint32_t)grid);
     hc->njobs = 1;
     hc->active = 1;
     const char *trace_path = std::getenv("EMP_COOP_TRACE");  // profiling: per-phase timestamps
@@ -682,7 +686,6 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     }
     const char *probe_env = std::getenv("EMP_COOP_PROBE");  // profiling: per-CTA stamps of one iteration
     std::string probe_path;
-    const int grid = bucket_grid_size();
     if (probe_env) {
         const char *colon = std::strrchr(probe_env, ':');
         probe_path.assign(probe_env, colon ? (size_t)(colon - probe_env) : std::strlen(probe_env));
@@ -1193,8 +1196,8 @@ emp_status emp_job_destroy(emp_job *job) {
                       &job->lv_init, &job->bloom_s, &job->bloom_p, &job->ck, &job->cv, &job->ck2, &job->cv2,
                       &job->records, &job->st_upd, &job->st_cand, &job->st_scan, &job->ctl, &job->st_join,
                       &job->st_sort, &job->coop_job, &job->coop_ctl, &job->coop_trace,
-                      &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_offs, &job->bk_tile_base, &job->bk_st_a,
-                      &job->bk_st_b, &job->bk_scratch, &job->bk_job};
+                      &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_offs, &job->bk_tile_base, &job->bk_spans,
+                      &job->bk_sfrom, &job->bk_sto, &job->bk_scratch, &job->bk_job};
     for (DevBuf *b : bufs) free_buf(job, *b);
     for (auto &e : job->sort_ev)
         if (e) cudaEventDestroy(e);

@@ -1,6 +1,6 @@
 // k_bucket.cu -- every overlap round of one or many read sets in ONE
-// cooperative launch, with two grid barriers per round and no global random
-// access on the streaming side.
+// cooperative launch: two grid barriers per round, no CTA waiting on another
+// inside a phase, no global random access on the streaming side.
 //
 // Round r of a job (overlap.cu:258-290):
 //   A  stream the live entries in 4096-entry tiles: drop entries used in the
@@ -9,23 +9,25 @@
 //      hash step NextSfx / PrevPfx (overlap.cu:57-91) with the base taken from
 //      a 16-base word cached in the entry (one read-major load per 16 rounds:
 //      regenerate_fingerprints + filter_bases, overlap.cu:605-692), and
-//      partition the tile in shared memory by the top bb bits of the entry's
-//      sort key.  The tile's output position comes from a decoupled look-back;
-//      its bucket starts go to offs[tile][0..2^bb].
-//   B  one CTA per bucket (buckets in key order): gather the bucket's piece of
-//      every A tile, insert the suffix keys into a hash set, probe the prefix
-//      keys, keep the entries whose key is in both tables, sort them by the
-//      sort key with the tie order of the reference's stable sort (table,
-//      then rid parity, then read index: the regenerated tables' order), and
-//      join equal-key runs (get_edges, overlap.cu:557-603).  Edge offsets come
-//      from a look-back over the buckets, so the round's edges are in the
-//      reference's order; used entries get a tombstone in the list.  The CTA
+//      partition the tile in shared memory into the round's key buckets.  The
+//      tile's output space comes from one atomic add; its bucket starts go to
+//      offs[tile][0..nb].  List order is irrelevant from here on: B orders
+//      everything it uses by a total order.
+//   B  one CTA per bucket: gather the bucket's piece of every A tile, insert
+//      the suffix keys into a hash set, probe the prefix keys, keep the
+//      entries whose key is in both tables, sort them by the sort key with
+//      the tie order of the reference's stable sort (table, then rid parity,
+//      then read index: the regenerated tables' order), and join equal-key
+//      runs (get_edges, overlap.cu:557-603).  The bucket's edges go to a
+//      staging buffer at an atomically reserved offset, recorded per
+//      (round, bucket); used entries get a tombstone in the list.  The CTA
 //      finishing a job's last bucket records the round and advances the job.
-// Keys equal across tables share a bucket, so every match is found inside one
-// bucket, and bucket order is sort-key order.
+//   end  after the last round, each round's edges are copied from the staging
+//      buffer in bucket order, which is sort-key order: the reference's order.
+// Keys equal across tables share a bucket (the bucket is a function of the
+// key's top bits), so every match is found inside one bucket.
 //
-// Buckets hold 3072 entries on average (2^bb buckets, bb from the list size);
-// one that does not fit shared memory (6144 entries, or 3072 matched
+// A bucket that does not fit shared memory (8192 entries, or 3072 matched
 // entries) uses the job's global scratch region instead, at the bucket's
 // position in the round's bucket order.
 #include "coop_common.cuh"
@@ -34,26 +36,31 @@ namespace emp {
 
 namespace {
 
-constexpr uint32_t kBStage = 6144;  // entries of a bucket staged in shared memory
+constexpr uint32_t kBStage = 8192;  // entries of a bucket staged in shared memory
 constexpr uint32_t kBHash = 8192;   // hash slots in shared memory (power of two)
 constexpr uint32_t kBCand = 3072;   // matched entries sorted in shared memory
 constexpr uint64_t kEmptySlot = ~0ull;  // never a key: fp1, fp2 < 2^29
+constexpr uint32_t kFlag = 0x80000000u; // "matched" mark in a staged entry's position word
 
-// shared-memory layout of phase B (bytes)
+// shared-memory layout of phase B (bytes): the staged bucket (key, val,
+// list position), then a region that holds in turn the gather's owner table
+// (u16 per staged entry), the hash set (u32 slots + the u16 slot of each
+// suffix), and the compacted matched entries; once those are compacted the
+// stage region holds their sort arrays
 constexpr size_t kOffKey = 0;
 constexpr size_t kOffVal = kOffKey + kBStage * 8;
 constexpr size_t kOffPos = kOffVal + kBStage * 4;
-constexpr size_t kOffFlag = kOffPos + kBStage * 4;
-constexpr size_t kOffHash = kOffFlag + kBStage;
-constexpr size_t kOffMatch = kOffHash + kBHash * 8;
-constexpr size_t kBSmem = kOffMatch + kBHash;
-// after the matched entries are compacted, the hash region holds the sort
-// keys, tie keys, chunk order and edge counts of up to kBCand of them
-static_assert(kBCand * (8 + 4 + 4 + 8) <= kBHash * 9, "sort arrays fit the hash region");
+constexpr size_t kOffHash = kOffPos + kBStage * 4;
+constexpr size_t kHashRegion = kBHash * 4 + kBStage * 2;
+constexpr size_t kBSmem = kOffHash + kHashRegion;
+static_assert(kBStage * 2 <= kHashRegion, "owner table fits the hash region");
+static_assert(kBCand * (8 + 4 + 4) <= kHashRegion, "compacted matches fit the hash region");
 static_assert(kOffHash % 16 == 0, "aligned hash region");
-// phase A: 2^kBktMaxBits bucket counters, then the staged tile
-constexpr size_t kASmem = (1u << kBktMaxBits) * 4 + kBktTile * sizeof(BktEntry);
-constexpr size_t kBktSmem = kBSmem > kASmem ? kBSmem : kASmem;
+// phase A: kBktMaxBuckets bucket counters, then the staged tile
+constexpr size_t kASmem = kBktMaxBuckets * 4 + kBktTile * sizeof(BktEntry);
+// end phase: one round's bucket destinations
+constexpr size_t kESmem = (kBktMaxBuckets + 1) * 8;
+constexpr size_t kBktSmem = kBSmem > kASmem ? (kBSmem > kESmem ? kBSmem : kESmem) : kASmem;
 
 struct BShared {
     uint32_t pref[kCoopMaxJobs + 1];
@@ -62,14 +69,13 @@ struct BShared {
     uint64_t seg_start[kT];
     uint32_t seg_pos[kT + 1];
     uint64_t base, tot, gpre;
-    uint32_t tile, flag, sfx, last, c;
+    uint32_t tile, flag, sfx;
 };
 
 // global scratch arrays of a job (n_max entries each, hash arrays 2 n_max)
 struct BScratch {
     uint64_t *key;
     uint32_t *val, *pos;
-    uint8_t *flag;
     uint64_t *hslot;
     uint8_t *hmatch;
     uint64_t *sk;
@@ -92,7 +98,6 @@ __host__ __device__ inline size_t scratch_layout(uint8_t *base, uint64_t N, BScr
     t.key = reinterpret_cast<uint64_t *>(take(N * 8));
     t.val = reinterpret_cast<uint32_t *>(take(N * 4));
     t.pos = reinterpret_cast<uint32_t *>(take(N * 4));
-    t.flag = take(N);
     t.hslot = reinterpret_cast<uint64_t *>(take(2 * N * 8));
     t.hmatch = take(2 * N);
     t.sk = reinterpret_cast<uint64_t *>(take(N * 8));
@@ -116,7 +121,6 @@ EMP_DEV T ldv(const T *p) {
 struct BView {
     uint64_t *key;
     uint32_t *val, *pos;
-    uint8_t *flag;
     uint64_t *hslot;
     uint8_t *hmatch;
     uint32_t hcap;
@@ -145,12 +149,11 @@ EMP_DEV bool before(uint64_t ska, uint32_t tba, uint64_t skb, uint32_t tbb) {
 }
 
 // ---------------------------------------------------------------- phase A
-EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const CoopCtl *ctl, uint32_t *err,
-                    uint8_t *smem) {
+EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const CoopCtl *ctl, uint8_t *smem) {
     probe(ctl, iter, 2);
     const uint32_t p = iter & 1;
     const uint64_t n_in = vld(J.it[p].n_in);
-    const uint32_t bb = vld(J.it[p].bb), NB = 1u << bb, stride = NB + 1;
+    const uint32_t nb = vld(J.it[p].nb), stride = nb + 1;
     const int L = J.L, r = (int)vld(J.round);
     const uint32_t pw1 = J.tables->pow1[L - r - 1], pw2 = J.tables->pow2[L - r - 1];
     const uint32_t inv1 = J.tables->inv1, inv2 = J.tables->inv2;
@@ -158,14 +161,14 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
     const BktEntry *lin = J.lst[p];
     BktEntry *lout = J.lst[p ^ 1];
     uint32_t *hist = reinterpret_cast<uint32_t *>(smem);
-    uint4 *stage = reinterpret_cast<uint4 *>(smem + (1u << kBktMaxBits) * 4);
-    for (uint32_t i = threadIdx.x; i < NB; i += kT) hist[i] = 0;
+    uint4 *stage = reinterpret_cast<uint4 *>(smem + kBktMaxBuckets * 4);
+    for (uint32_t i = threadIdx.x; i < nb; i += kT) hist[i] = 0;
     if (threadIdx.x == 0) sh.sfx = 0;
     __syncthreads();
     const uint64_t base = (uint64_t)k * kBktTile;
     uint64_t key[kC];
     uint32_t val[kC], word[kC], rank[kC], bkt[kC];
-    bool keep[kC], refill[kC];
+    bool keep[kC];
 #pragma unroll
     for (int c = 0; c < kC; ++c) {  // 1: the entries
         const uint64_t e = base + c * kT + threadIdx.x;
@@ -187,7 +190,6 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
     }
 #pragma unroll
     for (int c = 0; c < kC; ++c) {  // 2: used entries; bases not in the cached word
-        refill[c] = false;
         if (!keep[c]) continue;
         const uint32_t v = val[c];
         if (v == kBktTomb) {
@@ -198,8 +200,8 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
         if (first) keep[c] = (t ? J.used_p[rid] : J.used_s[rid]) == 0;
         const bool inc = t == s;  // fwd suffix / RC prefix walk the read forwards
         const int col = inc ? r : L - 1 - r;
-        refill[c] = keep[c] && (first || (col & 15) == (inc ? 0 : 15));
-        if (refill[c]) word[c] = __ldg(J.seq2 + (uint64_t)i * J.wpr + (col >> 4));
+        if (keep[c] && (first || (col & 15) == (inc ? 0 : 15)))
+            word[c] = __ldg(J.seq2 + (uint64_t)i * J.wpr + (col >> 4));
     }
     uint32_t sfx = 0;
 #pragma unroll
@@ -210,17 +212,17 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
         const int col = inc ? r : L - 1 - r;
         const uint32_t b = ((word[c] >> ((col & 15) * 2)) & 3u) ^ (s << 1);
         key[c] = t == 0 ? next_sfx(key[c], b, pw1, pw2) : prev_pfx(key[c], b, inv1, inv2);
-        bkt[c] = (uint32_t)(sort_key(key[c], v) >> (59 - bb));
+        bkt[c] = bkt_of(sort_key(key[c], v), nb);
         rank[c] = atomicAdd(&hist[bkt[c]], 1u);
         sfx += t == 0;
     }
     if (sfx) atomicAdd(&sh.sfx, sfx);
     __syncthreads();
     probe(ctl, iter, 3);
-    // bucket starts: exclusive scan of the NB counters, each thread a run of them
-    const uint32_t per = (NB + kT - 1) / kT;
-    const uint32_t b0 = threadIdx.x * per < NB ? threadIdx.x * per : NB;
-    const uint32_t b1 = b0 + per < NB ? b0 + per : NB;
+    // bucket starts: exclusive scan of the nb counters, each thread a run of them
+    const uint32_t per = (nb + kT - 1) / kT;
+    const uint32_t b0 = threadIdx.x * per < nb ? threadIdx.x * per : nb;
+    const uint32_t b1 = b0 + per < nb ? b0 + per : nb;
     uint32_t run = 0;
     for (uint32_t b = b0; b < b1; ++b) run += hist[b];
     uint32_t kept;
@@ -232,30 +234,24 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
         orow[b] = ex;
         ex += h;
     }
-    if (threadIdx.x == 0) orow[NB] = kept;
-    if (threadIdx.x < 32) {
-        const uint64_t tb = lookback_epoch_warp(J.st_a, k, kept, iter * 2u + 1u, err);
-        if (threadIdx.x == 0) {
-            sh.base = tb;
-            J.tile_base[k] = tb;
-        }
+    if (threadIdx.x == 0) {
+        orow[nb] = kept;
+        const uint64_t ob = atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].n_out),
+                                      (unsigned long long)kept);
+        sh.base = ob;
+        J.tile_base[k] = ob;
+        if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].s_out), (unsigned long long)sh.sfx);
     }
     __syncthreads();
     probe(ctl, iter, 4);
 #pragma unroll
     for (int c = 0; c < kC; ++c) {
         if (!keep[c]) continue;
-        stage[hist[bkt[c]] + rank[c]] =
-            make_uint4((uint32_t)key[c], (uint32_t)(key[c] >> 32), val[c], word[c]);
+        stage[hist[bkt[c]] + rank[c]] = make_uint4((uint32_t)key[c], (uint32_t)(key[c] >> 32), val[c], word[c]);
     }
     __syncthreads();
-    const uint64_t ob = sh.base;
-    uint4 *dst = reinterpret_cast<uint4 *>(lout + ob);
+    uint4 *dst = reinterpret_cast<uint4 *>(lout + sh.base);
     for (uint32_t x = threadIdx.x; x < kept; x += kT) dst[x] = stage[x];
-    if (threadIdx.x == 0) {
-        if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].s_out), (unsigned long long)sh.sfx);
-        if ((uint64_t)k == bkt_tiles(n_in) - 1) J.it[p].n_out = ob + kept;
-    }
     __syncthreads();
     probe(ctl, iter, 5);
 }
@@ -276,59 +272,106 @@ EMP_DEV uint64_t scan_counts(uint64_t *cnt, uint32_t c, BShared &sh) {
     return run;
 }
 
-EMP_DEV void b_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const CoopCtl *ctl, uint32_t *err,
-                    uint8_t *smem) {
-    probe(ctl, iter, 11);
-    const uint32_t p = iter & 1;
-    const uint64_t n_in = vld(J.it[p].n_in);
-    const uint32_t bb = vld(J.it[p].bb), NB = 1u << bb, stride = NB + 1;
-    const uint32_t K = (uint32_t)bkt_tiles(n_in);
-    BktEntry *lst = J.lst[p ^ 1];
+EMP_DEV void set_stage(BView &v, uint8_t *smem) {
+    v.key = reinterpret_cast<uint64_t *>(smem + kOffKey);
+    v.val = reinterpret_cast<uint32_t *>(smem + kOffVal);
+    v.pos = reinterpret_cast<uint32_t *>(smem + kOffPos);
+    v.hslot = nullptr;  // a staged bucket uses match_smem's own hash set
+    v.hmatch = nullptr;
+    v.hcap = 0;
+    v.hpow2 = true;
+}
+EMP_DEV void set_stage(BView &v, const BScratch &gs, uint64_t G, uint32_t total) {
+    v.key = gs.key + G;
+    v.val = gs.val + G;
+    v.pos = gs.pos + G;
+    v.hslot = gs.hslot + 2 * G;
+    v.hmatch = gs.hmatch + 2 * G;
+    v.hcap = 2 * total;
+    v.hpow2 = false;
+}
+
+EMP_DEV void put_entry(const BView &v, uint32_t d, const BktEntry *lst, uint64_t src) {
+    const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(lst + src));
+    v.key[d] = (uint64_t)q.x | ((uint64_t)q.y << 32);
+    v.val[d] = q.z;
+    v.pos[d] = (uint32_t)src;
+}
+
+// Gather bucket b: returns its size and sets up v (shared memory, or the
+// global scratch region at the bucket's place in bucket order).
+EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, const BktEntry *lst, BShared &sh,
+                        uint8_t *smem, BView &v, uint64_t &G) {
     const uint32_t *offs = J.offs;
-    // ---- pass 1: the bucket's size and its position in bucket order
-    {
-        uint64_t tot = 0, gpre = 0;
-        for (uint32_t k = threadIdx.x; k < K; k += kT) {
-            const uint32_t lo = __ldcg(offs + (uint64_t)k * stride + b), hi = __ldcg(offs + (uint64_t)k * stride + b + 1);
-            tot += hi - lo;
-            gpre += lo;
+    const uint32_t stride = nb + 1;
+    if (K <= (uint32_t)kT) {
+        // fast path: one segment per thread; an owner table maps staged
+        // entries to segments
+        const uint32_t k = threadIdx.x;
+        uint32_t lo = 0, cnt = 0;
+        uint64_t start = 0;
+        if (k < K) {
+            lo = __ldcg(offs + (uint64_t)k * stride + b);
+            cnt = __ldcg(offs + (uint64_t)k * stride + b + 1) - lo;
+            start = __ldcg(J.tile_base + k) + lo;
         }
-        uint64_t t1, t2;
-        block_exclusive_scan<kT, uint64_t>(tot, sh.scan64, &t1);
-        block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &t2);
-        if (threadIdx.x == 0) {
-            sh.tot = t1;
-            sh.gpre = t2;
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan<kT, uint32_t>(cnt, sh.scan32, &total);
+        if (total <= kBStage) {
+            G = 0;
+            set_stage(v, smem);
+            uint16_t *owner = reinterpret_cast<uint16_t *>(smem + kOffHash);
+            sh.seg_start[threadIdx.x] = start;
+            sh.seg_pos[threadIdx.x] = ex;
+            for (uint32_t x = ex; x < ex + cnt; ++x) owner[x] = (uint16_t)k;
+            __syncthreads();
+            constexpr int U = 4;
+            for (uint32_t x0 = 0; x0 < total; x0 += U * kT) {
+                uint4 q[U];
+                uint64_t src[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t x = x0 + u * kT + threadIdx.x;
+                    if (x < total) {
+                        const uint32_t o = owner[x];
+                        src[u] = sh.seg_start[o] + (x - sh.seg_pos[o]);
+                        q[u] = __ldcg(reinterpret_cast<const uint4 *>(lst + src[u]));
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t x = x0 + u * kT + threadIdx.x;
+                    if (x < total) {
+                        v.key[x] = (uint64_t)q[u].x | ((uint64_t)q[u].y << 32);
+                        v.val[x] = q[u].z;
+                        v.pos[x] = (uint32_t)src[u];
+                    }
+                }
+            }
+            __syncthreads();
+            return total;
         }
-        __syncthreads();
     }
-    const uint32_t total = (uint32_t)sh.tot;
-    const uint64_t G = sh.gpre;
-    probe(ctl, iter, 12);
-    BScratch gs;
-    scratch_layout(J.scratch, J.n_max, &gs);
-    BView v;
-    const bool in_smem = total <= kBStage;
-    if (in_smem) {
-        v.key = reinterpret_cast<uint64_t *>(smem + kOffKey);
-        v.val = reinterpret_cast<uint32_t *>(smem + kOffVal);
-        v.pos = reinterpret_cast<uint32_t *>(smem + kOffPos);
-        v.flag = smem + kOffFlag;
-        v.hslot = reinterpret_cast<uint64_t *>(smem + kOffHash);
-        v.hmatch = smem + kOffMatch;
-        v.hcap = kBHash;
-        v.hpow2 = true;
+    // general path: many tiles, or a bucket too big for shared memory
+    uint64_t tot = 0, gpre = 0;
+    for (uint32_t k = threadIdx.x; k < K; k += kT) {
+        const uint32_t lo = __ldcg(offs + (uint64_t)k * stride + b), hi = __ldcg(offs + (uint64_t)k * stride + b + 1);
+        tot += hi - lo;
+        gpre += lo;
+    }
+    uint64_t t1, t2;
+    block_exclusive_scan<kT, uint64_t>(tot, sh.scan64, &t1);
+    block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &t2);
+    const uint32_t total = (uint32_t)t1;
+    G = t2;
+    if (total <= kBStage) {
+        G = 0;
+        set_stage(v, smem);
     } else {
-        v.key = gs.key + G;
-        v.val = gs.val + G;
-        v.pos = gs.pos + G;
-        v.flag = gs.flag + G;
-        v.hslot = gs.hslot + 2 * G;
-        v.hmatch = gs.hmatch + 2 * G;
-        v.hcap = 2 * total;
-        v.hpow2 = false;
+        BScratch gs;
+        scratch_layout(J.scratch, J.n_max, &gs);
+        set_stage(v, gs, G, total);
     }
-    // ---- pass 2: gather the bucket's pieces (512 tiles at a time)
     uint32_t gathered = 0;
     for (uint32_t k0 = 0; k0 < K && total; k0 += kT) {
         const uint32_t k = k0 + threadIdx.x;
@@ -343,7 +386,6 @@ EMP_DEV void b_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const Coo
         const uint32_t ex = block_exclusive_scan<kT, uint32_t>(cnt, sh.scan32, &ctot);
         sh.seg_start[threadIdx.x] = start;
         sh.seg_pos[threadIdx.x] = ex;
-        if (threadIdx.x == 0) sh.seg_pos[kT] = ctot;
         __syncthreads();
         for (uint32_t x = threadIdx.x; x < ctot; x += kT) {
             uint32_t lo = 0, hi = kT;  // last segment with seg_pos <= x
@@ -352,211 +394,346 @@ EMP_DEV void b_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const Coo
                 if (sh.seg_pos[m] <= x) lo = m;
                 else hi = m;
             }
-            const uint64_t src = sh.seg_start[lo] + (x - sh.seg_pos[lo]);
-            const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(lst + src));
-            const uint32_t d = gathered + x;
-            v.key[d] = (uint64_t)q.x | ((uint64_t)q.y << 32);
-            v.val[d] = q.z;
-            v.pos[d] = (uint32_t)src;
+            put_entry(v, gathered + x, lst, sh.seg_start[lo] + (x - sh.seg_pos[lo]));
         }
         gathered += ctot;
         __syncthreads();
     }
-    probe(ctl, iter, 13);
-    // ---- matches: suffix keys into the hash set, prefix keys probe it
-    uint32_t c = 0;
-    if (total) {
-        for (uint32_t s = threadIdx.x; s < v.hcap; s += kT) {
-            v.hslot[s] = kEmptySlot;
-            v.hmatch[s] = 0;
+    return total;
+}
+
+// ---- shared-memory fast path of a bucket (the common case)
+// Hash slots are u32: bit 31 matched, bits 13-30 an 18-bit tag of the key,
+// bits 0-12 the staged index of a suffix with that key (keys compared in full
+// through it).  A tag of all ones is never used, so kSlotEmpty is no slot.
+constexpr uint32_t kSlotEmpty = 0xffffffffu;
+constexpr uint32_t kSlotMatched = 0x80000000u;
+static_assert(kBStage <= 8192 && kBHash == 8192, "13-bit staged indices and slot numbers");
+
+EMP_DEV void hash_tag(uint64_t key, uint32_t &slot, uint32_t &tag) {
+    const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 32);
+    slot = h & (kBHash - 1);
+    tag = (h >> 13) & 0x3ffffu;
+    if (tag == 0x3ffffu) tag = 0x3fffeu;
+}
+
+// Mark (kFlag in pos) every staged entry whose key occurs in both tables.
+EMP_DEV void match_smem(uint32_t total, uint8_t *smem) {
+    const uint64_t *key = reinterpret_cast<const uint64_t *>(smem + kOffKey);
+    const uint32_t *val = reinterpret_cast<const uint32_t *>(smem + kOffVal);
+    uint32_t *pos = reinterpret_cast<uint32_t *>(smem + kOffPos);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kOffHash);
+    uint16_t *sslot = reinterpret_cast<uint16_t *>(smem + kOffHash + kBHash * 4);
+    for (uint32_t s = threadIdx.x; s < kBHash; s += kT) slot[s] = kSlotEmpty;
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < total; x += kT) {  // suffixes: insert
+        if (val[x] >> 31) continue;
+        const uint64_t k = key[x];
+        uint32_t s, tag;
+        hash_tag(k, s, tag);
+        const uint32_t mine = (tag << 13) | x;
+        for (uint32_t probes = 0; probes < kBHash; ++probes) {
+            const uint32_t old = atomicCAS(slot + s, kSlotEmpty, mine);
+            if (old == kSlotEmpty || (((old >> 13) & 0x3ffffu) == tag && key[old & 8191u] == k)) break;
+            s = (s + 1) & (kBHash - 1);
         }
-        __syncthreads();
-        for (uint32_t x = threadIdx.x; x < total; x += kT) {
-            if (ldv(v.val + x) >> 31) continue;
-            const uint64_t key = ldv(v.key + x);
-            uint32_t s = slot_of(key, v);
-            for (uint32_t probes = 0; probes < v.hcap; ++probes) {
-                const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long *>(v.hslot + s),
-                                                (unsigned long long)kEmptySlot, (unsigned long long)key);
-                if (prev == kEmptySlot || prev == key) break;
-                s = slot_next(s, v);
+        sslot[x] = (uint16_t)s;
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < total; x += kT) {  // prefixes: probe
+        if (!(val[x] >> 31)) continue;
+        const uint64_t k = key[x];
+        uint32_t s, tag;
+        hash_tag(k, s, tag);
+        for (uint32_t probes = 0; probes < kBHash; ++probes) {
+            const uint32_t w = slot[s];
+            if (w == kSlotEmpty) break;
+            if (((w >> 13) & 0x3ffffu) == tag && key[w & 8191u] == k) {
+                if (!(w & kSlotMatched)) atomicOr(slot + s, kSlotMatched);
+                pos[x] |= kFlag;
+                break;
             }
-        }
-        __syncthreads();
-        for (uint32_t x = threadIdx.x; x < total; x += kT) {  // prefixes
-            if (!(ldv(v.val + x) >> 31)) continue;
-            const uint64_t key = ldv(v.key + x);
-            uint32_t s = slot_of(key, v);
-            uint8_t f = 0;
-            for (uint32_t probes = 0; probes < v.hcap; ++probes) {
-                const uint64_t h = ldv(v.hslot + s);
-                if (h == kEmptySlot) break;
-                if (h == key) {
-                    f = 1;
-                    v.hmatch[s] = 1;
-                    break;
-                }
-                s = slot_next(s, v);
-            }
-            v.flag[x] = f;
-        }
-        __syncthreads();
-        for (uint32_t x = threadIdx.x; x < total; x += kT) {  // suffixes
-            if (ldv(v.val + x) >> 31) continue;
-            const uint64_t key = ldv(v.key + x);
-            uint32_t s = slot_of(key, v);
-            uint8_t f = 0;
-            for (uint32_t probes = 0; probes < v.hcap; ++probes) {
-                const uint64_t h = ldv(v.hslot + s);
-                if (h == key) {
-                    f = ldv(v.hmatch + s);
-                    break;
-                }
-                if (h == kEmptySlot) break;
-                s = slot_next(s, v);
-            }
-            v.flag[x] = f;
-        }
-        __syncthreads();
-        probe(ctl, iter, 14);
-        // compact the matched entries to the front, in place, chunk by chunk
-        for (uint32_t x0 = 0; x0 < total; x0 += kT) {
-            const uint32_t x = x0 + threadIdx.x;
-            const bool f = x < total && ldv(v.flag + x);
-            uint64_t key = 0;
-            uint32_t val = 0, pos = 0;
-            if (f) {
-                key = ldv(v.key + x);
-                val = ldv(v.val + x);
-                pos = ldv(v.pos + x);
-            }
-            uint32_t ctot;
-            const uint32_t ex = block_exclusive_scan<kT, uint32_t>(f ? 1u : 0u, sh.scan32, &ctot);
-            if (f) {
-                v.key[c + ex] = key;
-                v.val[c + ex] = val;
-                v.pos[c + ex] = pos;
-            }
-            c += ctot;
-            __syncthreads();
+            s = (s + 1) & (kBHash - 1);
         }
     }
-    probe(ctl, iter, 15);
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < total; x += kT)  // suffixes: matched?
+        if (!(val[x] >> 31) && (slot[sslot[x]] & kSlotMatched)) pos[x] |= kFlag;
+    __syncthreads();
+}
+
+// The generic matcher (global scratch, or any view): same marks.
+EMP_DEV void match_view(const BView &v, uint32_t total) {
+    for (uint32_t s = threadIdx.x; s < v.hcap; s += kT) {
+        v.hslot[s] = kEmptySlot;
+        v.hmatch[s] = 0;
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < total; x += kT) {
+        if (ldv(v.val + x) >> 31) continue;
+        const uint64_t key = ldv(v.key + x);
+        uint32_t s = slot_of(key, v);
+        for (uint32_t probes = 0; probes < v.hcap; ++probes) {
+            const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long *>(v.hslot + s),
+                                            (unsigned long long)kEmptySlot, (unsigned long long)key);
+            if (prev == kEmptySlot || prev == key) break;
+            s = slot_next(s, v);
+        }
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < total; x += kT) {  // prefixes
+        if (!(ldv(v.val + x) >> 31)) continue;
+        const uint64_t key = ldv(v.key + x);
+        uint32_t s = slot_of(key, v);
+        for (uint32_t probes = 0; probes < v.hcap; ++probes) {
+            const uint64_t h = ldv(v.hslot + s);
+            if (h == kEmptySlot) break;
+            if (h == key) {
+                v.hmatch[s] = 1;
+                v.pos[x] = ldv(v.pos + x) | kFlag;
+                break;
+            }
+            s = slot_next(s, v);
+        }
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < total; x += kT) {  // suffixes
+        if (ldv(v.val + x) >> 31) continue;
+        const uint64_t key = ldv(v.key + x);
+        uint32_t s = slot_of(key, v);
+        for (uint32_t probes = 0; probes < v.hcap; ++probes) {
+            const uint64_t h = ldv(v.hslot + s);
+            if (h == key) {
+                if (ldv(v.hmatch + s)) v.pos[x] = ldv(v.pos + x) | kFlag;
+                break;
+            }
+            if (h == kEmptySlot) break;
+            s = slot_next(s, v);
+        }
+    }
+    __syncthreads();
+}
+
+// Arrays of the matched entries: compacted (key, val, list position), their
+// sort and tie keys, chunk order, edge counts, and the sorted copy.
+struct CandView {
+    uint64_t *ck;
+    uint32_t *cv, *cp;
+    uint64_t *sk;
+    uint32_t *tb, *idx;
+    uint64_t *cnt;
+    uint64_t *skey;
+    uint32_t *sval, *spos;
+};
+
+// Sort the c matched entries by (sort key, tie) and count each suffix's edges;
+// returns the bucket's edge count (cnt then holds exclusive edge offsets).
+EMP_DEV uint64_t sort_and_count(const CandView &w, uint32_t c, BShared &sh) {
+    for (uint32_t x = threadIdx.x; x < c; x += kT) {
+        const uint32_t val = ldv(w.cv + x);
+        w.sk[x] = sort_key(ldv(w.ck + x), val);
+        w.tb[x] = tie_of(val);
+    }
+    __syncthreads();
+    const uint32_t nch = (c + kT - 1) / kT;
+    for (uint32_t q = 0; q < nch; ++q) {  // order within each 512-entry chunk
+        const uint32_t lo = q * kT, m = c - lo < kT ? c - lo : kT;
+        if (threadIdx.x < m) {
+            const uint32_t x = lo + threadIdx.x;
+            const uint64_t skx = ldv(w.sk + x);
+            const uint32_t tbx = ldv(w.tb + x);
+            uint32_t rk = 0;
+            for (uint32_t u = 0; u < m; ++u) rk += before(ldv(w.sk + lo + u), ldv(w.tb + lo + u), skx, tbx);
+            w.idx[lo + rk] = x;
+            w.cnt[x] = rk;
+        }
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < c; x += kT) {  // rank among all chunks
+        const uint64_t skx = ldv(w.sk + x);
+        const uint32_t tbx = ldv(w.tb + x);
+        const uint32_t qx = x / kT;
+        uint32_t rk = (uint32_t)ldv(w.cnt + x);
+        for (uint32_t q = 0; q < nch; ++q) {
+            if (q == qx) continue;
+            const uint32_t lo = q * kT, m = c - lo < kT ? c - lo : kT;
+            uint32_t a = 0, z = m;  // entries of chunk q before x
+            while (a < z) {
+                const uint32_t mid = (a + z) >> 1;
+                const uint32_t y = ldv(w.idx + lo + mid);
+                if (before(ldv(w.sk + y), ldv(w.tb + y), skx, tbx)) a = mid + 1;
+                else z = mid;
+            }
+            rk += a;
+        }
+        w.skey[rk] = ldv(w.ck + x);
+        w.sval[rk] = ldv(w.cv + x);
+        w.spos[rk] = ldv(w.cp + x);
+    }
+    __syncthreads();
+    // join: per suffix, the prefixes of its equal-key run from other reads
+    for (uint32_t i = threadIdx.x; i < c; i += kT) {
+        uint64_t cc = 0;
+        const uint32_t vi = ldv(w.sval + i);
+        if (!(vi >> 31)) {
+            const uint64_t ki = ldv(w.skey + i);
+            const uint32_t ri = (vi & 0x7fffffffu) >> 1;
+            for (uint32_t j = i + 1; j < c && ldv(w.skey + j) == ki; ++j) {
+                const uint32_t vj = ldv(w.sval + j);
+                cc += (vj >> 31) && ((vj & 0x7fffffffu) >> 1) != ri;
+            }
+        }
+        w.cnt[i] = cc;
+    }
+    __syncthreads();
+    return scan_counts(w.cnt, c, sh);
+}
+
+EMP_DEV void b_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const CoopCtl *ctl, uint8_t *smem) {
+    probe(ctl, iter, 11);
+    const uint32_t p = iter & 1;
+    const uint64_t n_in = vld(J.it[p].n_in);
+    const uint32_t nb = vld(J.it[p].nb);
+    const uint32_t K = (uint32_t)bkt_tiles(n_in);
+    BktEntry *lst = J.lst[p ^ 1];
+    BView v;
+    uint64_t G = 0;
+    const uint32_t total = gather(J, b, nb, K, lst, sh, smem, v, G);
+    const bool in_smem = total <= kBStage;
+    probe(ctl, iter, 13);
+    // ---- matches: entries whose key is in both tables get kFlag in pos
+    if (total) {
+        if (in_smem) match_smem(total, smem);
+        else match_view(v, total);
+    }
+    probe(ctl, iter, 14);
+    uint32_t c = 0;
+    for (uint32_t x0 = 0; x0 < total; x0 += kT) {
+        const uint32_t x = x0 + threadIdx.x;
+        c += __syncthreads_count(x < total && (ldv(v.pos + x) & kFlag));
+    }
     if (threadIdx.x == 0 && c) atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].cands), (unsigned long long)c);
     uint64_t E = 0;
+    CandView w;
     if (c) {
-        // ---- sort the matched entries by (sort key, tie)
         if (in_smem && c <= kBCand) {
+            // compact (any order: the sort below fixes it) into the hash
+            // region; the sort arrays then take the stage region
             uint8_t *h = smem + kOffHash;
-            v.sk = reinterpret_cast<uint64_t *>(h);
-            v.tb = reinterpret_cast<uint32_t *>(h + kBCand * 8);
-            v.idx = v.tb + kBCand;
-            v.cnt = reinterpret_cast<uint64_t *>(h + kBCand * 16);
-            v.skey = v.key + kBCand;
-            v.sval = v.val + kBCand;
-            v.spos = v.pos + kBCand;
+            w.ck = reinterpret_cast<uint64_t *>(h);
+            w.cv = reinterpret_cast<uint32_t *>(h + kBCand * 8);
+            w.cp = w.cv + kBCand;
+            if (threadIdx.x == 0) sh.tile = 0;  // compaction counter
+            __syncthreads();
+            const uint32_t lane = threadIdx.x & 31;
+            for (uint32_t x0 = 0; x0 < total; x0 += kT) {
+                const uint32_t x = x0 + threadIdx.x;
+                const uint32_t ps = x < total ? v.pos[x] : 0u;
+                const bool f = (ps & kFlag) != 0;
+                const uint32_t m = __ballot_sync(0xffffffffu, f);
+                if (!m) continue;
+                const uint32_t leader = __ffs(m) - 1;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(&sh.tile, (uint32_t)__popc(m));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (f) {
+                    const uint32_t d = base + __popc(m & lanemask_lt_u32());
+                    w.ck[d] = v.key[x];
+                    w.cv[d] = v.val[x];
+                    w.cp[d] = ps & ~kFlag;
+                }
+            }
+            __syncthreads();
+            uint8_t *s = smem;  // stage region, free now
+            w.sk = reinterpret_cast<uint64_t *>(s);
+            w.tb = reinterpret_cast<uint32_t *>(s + kBCand * 8);
+            w.idx = w.tb + kBCand;
+            w.cnt = reinterpret_cast<uint64_t *>(s + kBCand * 16);
+            w.skey = reinterpret_cast<uint64_t *>(s + kBCand * 24);
+            w.sval = reinterpret_cast<uint32_t *>(s + kBCand * 32);
+            w.spos = w.sval + kBCand;
+            static_assert(kBCand * 40 <= kOffHash, "sort arrays fit the stage region");
         } else {
-            v.sk = gs.sk + G;
-            v.tb = gs.tb + G;
-            v.idx = gs.idx + G;
-            v.cnt = gs.cnt + G;
-            v.skey = gs.skey + G;
-            v.sval = gs.sval + G;
-            v.spos = gs.spos + G;
-        }
-        for (uint32_t x = threadIdx.x; x < c; x += kT) {
-            const uint32_t val = ldv(v.val + x);
-            v.sk[x] = sort_key(ldv(v.key + x), val);
-            v.tb[x] = tie_of(val);
-        }
-        __syncthreads();
-        const uint32_t nch = (c + kT - 1) / kT;
-        for (uint32_t q = 0; q < nch; ++q) {  // order within each 512-entry chunk
-            const uint32_t lo = q * kT, m = c - lo < kT ? c - lo : kT;
-            if (threadIdx.x < m) {
-                const uint32_t x = lo + threadIdx.x;
-                const uint64_t skx = ldv(v.sk + x);
-                const uint32_t tbx = ldv(v.tb + x);
-                uint32_t rk = 0;
-                for (uint32_t u = 0; u < m; ++u) rk += before(ldv(v.sk + lo + u), ldv(v.tb + lo + u), skx, tbx);
-                v.idx[lo + rk] = x;
-                v.cnt[x] = rk;
-            }
-        }
-        __syncthreads();
-        for (uint32_t x = threadIdx.x; x < c; x += kT) {  // rank among all chunks
-            const uint64_t skx = ldv(v.sk + x);
-            const uint32_t tbx = ldv(v.tb + x);
-            const uint32_t qx = x / kT;
-            uint32_t rk = (uint32_t)ldv(v.cnt + x);
-            for (uint32_t q = 0; q < nch; ++q) {
-                if (q == qx) continue;
-                const uint32_t lo = q * kT, m = c - lo < kT ? c - lo : kT;
-                uint32_t a = 0, z = m;  // entries of chunk q before x
-                while (a < z) {
-                    const uint32_t mid = (a + z) >> 1;
-                    const uint32_t y = ldv(v.idx + lo + mid);
-                    if (before(ldv(v.sk + y), ldv(v.tb + y), skx, tbx)) a = mid + 1;
-                    else z = mid;
+            // in place, in order, then the global scratch region of the bucket
+            uint32_t cc = 0;
+            for (uint32_t x0 = 0; x0 < total; x0 += kT) {
+                const uint32_t x = x0 + threadIdx.x;
+                const uint32_t ps = x < total ? ldv(v.pos + x) : 0u;
+                const bool f = (ps & kFlag) != 0;
+                uint64_t key = 0;
+                uint32_t val = 0;
+                if (f) {
+                    key = ldv(v.key + x);
+                    val = ldv(v.val + x);
                 }
-                rk += a;
-            }
-            v.skey[rk] = ldv(v.key + x);
-            v.sval[rk] = ldv(v.val + x);
-            v.spos[rk] = ldv(v.pos + x);
-        }
-        __syncthreads();
-        probe(ctl, iter, 16);
-        // ---- join: per suffix, the prefixes of its equal-key run from other reads
-        for (uint32_t i = threadIdx.x; i < c; i += kT) {
-            uint64_t cc = 0;
-            const uint32_t vi = ldv(v.sval + i);
-            if (!(vi >> 31)) {
-                const uint64_t ki = ldv(v.skey + i);
-                const uint32_t ri = (vi & 0x7fffffffu) >> 1;
-                for (uint32_t j = i + 1; j < c && ldv(v.skey + j) == ki; ++j) {
-                    const uint32_t vj = ldv(v.sval + j);
-                    cc += (vj >> 31) && ((vj & 0x7fffffffu) >> 1) != ri;
+                uint32_t ctot;
+                const uint32_t ex = block_exclusive_scan<kT, uint32_t>(f ? 1u : 0u, sh.scan32, &ctot);
+                if (f) {
+                    v.key[cc + ex] = key;
+                    v.val[cc + ex] = val;
+                    v.pos[cc + ex] = ps & ~kFlag;
                 }
+                cc += ctot;
+                __syncthreads();
             }
-            v.cnt[i] = cc;
+            if (in_smem) {  // the bucket's place in bucket order picks its scratch region
+                uint64_t gpre = 0;
+                const uint32_t stride = nb + 1;
+                for (uint32_t k = threadIdx.x; k < K; k += kT) gpre += __ldcg(J.offs + (uint64_t)k * stride + b);
+                block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &G);
+            }
+            BScratch gs;
+            scratch_layout(J.scratch, J.n_max, &gs);
+            w.ck = v.key;
+            w.cv = v.val;
+            w.cp = v.pos;
+            w.sk = gs.sk + G;
+            w.tb = gs.tb + G;
+            w.idx = gs.idx + G;
+            w.cnt = gs.cnt + G;
+            w.skey = gs.skey + G;
+            w.sval = gs.sval + G;
+            w.spos = gs.spos + G;
         }
-        __syncthreads();
-        E = scan_counts(v.cnt, c, sh);
+        probe(ctl, iter, 15);
+        E = sort_and_count(w, c, sh);
     }
     probe(ctl, iter, 17);
-    if (threadIdx.x < 32) {
-        const uint64_t eb = lookback_epoch_warp(J.st_b, b, E, iter * 2u + 2u, err);
-        if (threadIdx.x == 0) sh.base = eb;
+    if (threadIdx.x == 0) {
+        uint64_t off = 0;
+        if (E) {
+            off = atomicAdd(reinterpret_cast<unsigned long long *>(&J.e_stage), (unsigned long long)E);
+            if (off + E > J.ecap) J.overflow = 1;
+            atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].edges), (unsigned long long)E);
+        }
+        sh.base = off;
+        BktSpan &sp = J.spans[(uint64_t)(vld(J.round) - J.r0) * J.nb_max + b];
+        sp.off = off;
+        sp.cnt = E;
     }
     __syncthreads();
     probe(ctl, iter, 18);
-    if (E) {
-        const uint64_t ebase = vld(J.e_total) + sh.base;
+    if (E && sh.base + E <= J.ecap) {
+        const uint64_t ebase = sh.base;
         for (uint32_t i = threadIdx.x; i < c; i += kT) {
-            const uint32_t vi = ldv(v.sval + i);
+            const uint32_t vi = ldv(w.sval + i);
             if (vi >> 31) continue;
-            const uint64_t ki = ldv(v.skey + i);
+            const uint64_t ki = ldv(w.skey + i);
             const uint32_t si = vi & 0x7fffffffu, ri = si >> 1;
-            const uint64_t o0 = ebase + ldv(v.cnt + i);
+            const uint64_t o0 = ebase + ldv(w.cnt + i);
             uint64_t o = o0;
-            for (uint32_t j = i + 1; j < c && ldv(v.skey + j) == ki; ++j) {
-                const uint32_t vj = ldv(v.sval + j);
+            for (uint32_t j = i + 1; j < c && ldv(w.skey + j) == ki; ++j) {
+                const uint32_t vj = ldv(w.sval + j);
                 const uint32_t pj = vj & 0x7fffffffu;
                 if ((vj >> 31) && (pj >> 1) != ri) {
-                    if (o < J.ecap) {
-                        J.efrom[o] = si;
-                        J.eto[o] = pj;
-                    } else {
-                        J.overflow = 1;
-                    }
-                    lst[ldv(v.spos + j)].val = kBktTomb;
+                    J.sfrom[o] = si;
+                    J.sto[o] = pj;
+                    lst[ldv(w.spos + j)].val = kBktTomb;
                     ++o;
                 }
             }
-            if (o != o0) lst[ldv(v.spos + i)].val = kBktTomb;
+            if (o != o0) lst[ldv(w.spos + i)].val = kBktTomb;
         }
-        if (threadIdx.x == 0) atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].edges), (unsigned long long)E);
     }
     __syncthreads();
     probe(ctl, iter, 19);
@@ -582,6 +759,7 @@ EMP_DEV void round_end(BktJob &x, CoopCtl *ctl, uint32_t iter) {
     rec.E = E;
     rec.e0 = e0;
     rec.C = vld(x.it[p].cands);
+    rec.nb = vld(x.it[p].nb);
     x.e_total = e0 + E;
     x.round = r + 1;
     BktIter &nx = x.it[q];
@@ -590,13 +768,57 @@ EMP_DEV void round_end(BktJob &x, CoopCtl *ctl, uint32_t iter) {
     nx.s_out = 0;
     nx.cands = 0;
     nx.edges = 0;
-    nx.bb = bkt_bits(N);
+    nx.nb = bkt_count(N, gridDim.x);
     nx.b_done = 0;
     if ((int)(r + 1) >= x.rounds) {
         x.end_iter = iter;
         atomicSub(&ctl->active, 1u);
     }
     __threadfence();
+}
+
+// After the last round: each round's edges from the staging buffer to the
+// edge list in bucket order (rounds spread over the CTAs, no grid barrier).
+EMP_DEV void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
+    uint64_t *dest = reinterpret_cast<uint64_t *>(smem);  // nb + 1 bucket starts
+    uint32_t g = 0;
+    for (int j = 0; j < J; ++j) {
+        BktJob &x = jobs[j];
+        if (vld(x.overflow)) continue;
+        const uint32_t r1 = vld(x.round);
+        for (uint32_t r = (uint32_t)x.r0; r < r1; ++r, ++g) {
+            if (g % gridDim.x != blockIdx.x) continue;
+            const RoundRecord &rec = x.records[r];
+            const uint64_t E = __ldcg(&rec.E);
+            if (!E) continue;
+            const uint32_t nb = (uint32_t)__ldcg(&rec.nb);
+            const uint64_t e0 = __ldcg(&rec.e0);
+            const BktSpan *sp = x.spans + (uint64_t)(r - x.r0) * x.nb_max;
+            uint64_t run = 0;
+            for (uint32_t b0 = 0; b0 < nb; b0 += kT) {
+                const uint32_t b = b0 + threadIdx.x;
+                const uint64_t c = b < nb ? __ldcg(&sp[b].cnt) : 0;
+                uint64_t tot;
+                const uint64_t ex = block_exclusive_scan<kT, uint64_t>(c, sh.scan64, &tot);
+                if (b < nb) dest[b] = run + ex;
+                run += tot;
+            }
+            if (threadIdx.x == 0) dest[nb] = run;
+            __syncthreads();
+            for (uint64_t e = threadIdx.x; e < E; e += kT) {
+                uint32_t lo = 0, hi = nb;  // last bucket with dest <= e
+                while (hi - lo > 1) {
+                    const uint32_t m = (lo + hi) >> 1;
+                    if (dest[m] <= e) lo = m;
+                    else hi = m;
+                }
+                const uint64_t src = __ldcg(&sp[lo].off) + (e - dest[lo]);
+                x.efrom[e0 + e] = __ldcg(x.sfrom + src);
+                x.eto[e0 + e] = __ldcg(x.sto + src);
+            }
+            __syncthreads();
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, CoopCtl *ctl, uint32_t *err) {
@@ -614,8 +836,7 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
             return vld(x.end_iter) >= iter ? (uint32_t)bkt_tiles(vld(x.it[p].n_in)) : 0u;
         });
         probe(ctl, iter, 1);
-        tile_loop(sh, &ctl->ticket[0], J, total,
-                  [&](int j, uint32_t k) { a_tile(jobs[j], k, iter, sh, ctl, err, smem); });
+        tile_loop(sh, &ctl->ticket[0], J, total, [&](int j, uint32_t k) { a_tile(jobs[j], k, iter, sh, ctl, smem); });
         probe(ctl, iter, 6);
         if (!grid_barrier(ctl, &sh.flag, iter, 0)) return;
         probe(ctl, iter, 7);
@@ -627,17 +848,17 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
             const BktJob &x = jobs[j];
             if (vld(x.end_iter) < iter) return 0u;
             const uint64_t S = vld(x.it[p].s_out), N = vld(x.it[p].n_out);
-            return (S > 0 && S < N) ? (1u << vld(x.it[p].bb)) : 0u;
+            return (S > 0 && S < N) ? vld(x.it[p].nb) : 0u;
         });
         probe(ctl, iter, 10);
         tile_loop(sh, &ctl->ticket[1], J, total, [&](int j, uint32_t b) {
             BktJob &x = jobs[j];
-            b_tile(x, b, iter, sh, ctl, err, smem);
+            b_tile(x, b, iter, sh, ctl, smem);
             __threadfence();
             __syncthreads();
             if (threadIdx.x == 0) {
-                const uint32_t nb = sh.pref[j + 1] - sh.pref[j];
-                if (atomicAdd(&x.it[p].b_done, 1u) == nb - 1) {
+                const uint32_t nbj = sh.pref[j + 1] - sh.pref[j];
+                if (atomicAdd(&x.it[p].b_done, 1u) == nbj - 1) {
                     __threadfence();
                     round_end(x, ctl, iter);
                 }
@@ -652,14 +873,15 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
         if (!grid_barrier(ctl, &sh.flag, iter, 1)) return;
         probe(ctl, iter, 21);
     }
+    place_edges(jobs, J, sh, smem);
 }
 
 }  // namespace
 
 size_t bkt_scratch_bytes(uint64_t n_max) { return scratch_layout(nullptr, n_max < 1 ? 1 : n_max, nullptr); }
 
-size_t bkt_offs_words(uint64_t n_max) {
-    return (size_t)bkt_tiles(n_max < 1 ? 1 : n_max) * ((1u << bkt_bits(n_max)) + 1);
+size_t bkt_offs_words(uint64_t n_max, uint32_t G) {
+    return (size_t)bkt_tiles(n_max < 1 ? 1 : n_max) * (bkt_count(n_max, G) + 1);
 }
 
 int bucket_grid_size() {

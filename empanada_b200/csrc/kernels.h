@@ -135,7 +135,8 @@ struct RoundCtl {
 };
 struct RoundRecord {
     uint64_t S, P, E, e0;  // table sizes, edges, first edge of the round
-    uint64_t C;            // candidates sorted (cooperative kernel only)
+    uint64_t C;            // candidates sorted (cooperative kernels only)
+    uint64_t nb;           // key buckets of the round (bucket kernel only)
 };
 struct PipeArgs {
     RoundCtl *ctl;
@@ -221,25 +222,34 @@ cudaError_t launch_coop_rounds(CoopJob *jobs, CoopCtl *ctl, uint32_t *err, cudaS
 
 // ---- bucket rounds (k_bucket.cu) ------------------------------------------
 // Each round of each job: phase A streams the live entries in 4096-entry
-// tiles (drop used ones, hash step, partition the tile by the top bits of the
-// new sort key); phase B gives each key bucket to one CTA, which gathers the
+// tiles (drop used ones, hash step, partition the tile into the round's key
+// buckets); phase B gives each key bucket to one CTA, which gathers the
 // bucket's pieces from every tile, finds the keys present in both tables with
-// a hash set, sorts those entries and joins them.
+// a hash set, sorts those entries and joins them.  Neither phase waits on
+// another CTA: output space comes from one atomic per tile or bucket, and the
+// edges are put in bucket order once all rounds are done.
 struct BktEntry {
     uint64_t key;   // fp1 << 32 | fp2
     uint32_t val;   // rid | table << 31, or kBktTomb once used
     uint32_t word;  // cached 16 bases (one seq2 word) of the entry's read
 };
 constexpr uint32_t kBktTomb = 0xffffffffu;
-constexpr uint32_t kBktTile = 4096;                // entries per phase-A tile
-constexpr int kBktMinBits = 8, kBktMaxBits = 12;   // 256 .. 4096 buckets
-constexpr uint64_t kBktTarget = 3072;              // mean entries per bucket aimed at
-constexpr uint64_t kBktMaxEntries = 16ull << 20;   // larger lists use the other drivers
+constexpr uint32_t kBktTile = 4096;               // entries per phase-A tile
+constexpr uint64_t kBktMean = 7168;               // most entries per bucket aimed at (mean)
+constexpr uint32_t kBktMaxBuckets = 4096;
+constexpr uint64_t kBktMaxEntries = 16ull << 20;  // larger lists use the other drivers
 __host__ __device__ inline uint64_t bkt_tiles(uint64_t n) { return (n + kBktTile - 1) / kBktTile; }
-__host__ __device__ inline uint32_t bkt_bits(uint64_t n) {
-    uint32_t b = kBktMinBits;
-    while (b < (uint32_t)kBktMaxBits && (kBktTarget << b) < n) ++b;
-    return b;
+// Buckets of a round with n entries on a grid of G CTAs: whole waves of G,
+// at most kBktMean entries each on average.  Bucket of a sort key sk: its top
+// 24 bits scaled to [0, nb), so bucket order is key order.
+__host__ __device__ inline uint32_t bkt_count(uint64_t n, uint32_t G) {
+    uint64_t waves = (n + (uint64_t)G * kBktMean - 1) / ((uint64_t)G * kBktMean);
+    if (waves < 1) waves = 1;
+    uint64_t nb = waves * G;
+    return (uint32_t)(nb > kBktMaxBuckets ? kBktMaxBuckets : nb);
+}
+__host__ __device__ inline uint32_t bkt_of(uint64_t sk, uint32_t nb) {
+    return (uint32_t)(((sk >> 35) * (uint64_t)nb) >> 24);
 }
 struct BktIter {         // one per iteration parity
     uint64_t n_in;       // entries entering phase A
@@ -247,8 +257,11 @@ struct BktIter {         // one per iteration parity
     uint64_t s_out;      // of which suffixes
     uint64_t cands;      // entries found in both tables
     uint64_t edges;      // edges of the round
-    uint32_t bb;         // bucket bits of the round
+    uint32_t nb;         // buckets of the round
     uint32_t b_done;     // buckets finished
+};
+struct BktSpan {         // one bucket's edges in the staging buffer
+    uint64_t off, cnt;
 };
 struct BktJob {
     const uint64_t *lk_in;   // the list at launch (id order, suffixes then prefixes)
@@ -256,26 +269,28 @@ struct BktJob {
     const uint8_t *used_s, *used_p;  // marks of rounds run before the launch
     BktEntry *lst[2];        // lists written by phase A, n_max entries each
     const uint32_t *seq2;    // read-major 2-bit bases, wpr words per read
-    int32_t wpr, L, rounds, pad0;
+    int32_t wpr, L, rounds, r0;
     const HashTables *tables;
-    uint32_t *offs;          // per phase-A tile: 2^bb + 1 bucket starts
+    uint32_t *offs;          // per phase-A tile: nb + 1 bucket starts
     uint64_t *tile_base;     // per phase-A tile: its first output entry
-    uint64_t *st_a, *st_b;   // look-back words of phase-A tiles and of buckets
-    uint32_t *efrom, *eto;
+    BktSpan *spans;          // [round - r0][bucket]: edges in the staging buffer
+    uint32_t *sfrom, *sto;   // staging buffer (bucket order within a round is restored at the end)
+    uint32_t *efrom, *eto;   // edges of all rounds, in the reference's order
     uint64_t ecap;
     RoundRecord *records;
     uint8_t *scratch;        // bkt_scratch_bytes(n_max): buckets too big for shared memory
     uint64_t n_max;
+    uint32_t nb_max;         // row length of spans
     uint32_t round;          // next round to run
     uint32_t end_iter;       // iteration in which the job ended (0xffffffff while running)
     uint32_t overflow;       // the edge buffer was too small
-    uint32_t pad1;
     uint64_t e_total;        // edges of the finished rounds of this launch
+    uint64_t e_stage;        // staging buffer fill
     BktIter it[2];
 };
 size_t bkt_scratch_bytes(uint64_t n_max);
-size_t bkt_offs_words(uint64_t n_max);   // u32 words of BktJob::offs
-int bucket_grid_size();                  // 0: no cooperative launch on this device
+size_t bkt_offs_words(uint64_t n_max, uint32_t G);  // u32 words of BktJob::offs
+int bucket_grid_size();                             // 0: no cooperative launch on this device
 cudaError_t launch_bucket_rounds(BktJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
 
 void launch_join_count(const uint64_t *skeys, const uint32_t *svals, uint64_t n, uint32_t *cnt, cudaStream_t s);
