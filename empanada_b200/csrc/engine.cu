@@ -96,6 +96,9 @@ struct emp_job {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     DevBuf st_join, st_sort, coop_job, coop_ctl, coop_trace, coop_probe;  // cooperative all-rounds kernel
+    DevBuf dout;                 // output.bin records written on the device (after those in `out`)
+    uint64_t dout_bytes = 0;
+    PinnedBuf h_out;
     DevBuf bk_lst0, bk_lst1, bk_offs, bk_tile_base, bk_spans, bk_sfrom, bk_sto, bk_scratch, bk_job;  // bucket kernel
     PinnedBuf h_coop;
     cudaEvent_t sort_ev[2 * kSortPasses] = {};
@@ -638,8 +641,7 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     EMP_TRY(ensure(j, j->bk_scratch, bkt_scratch_bytes(nmax)));
     EMP_TRY(ensure(j, j->bk_job, sizeof(BktJob)));
     EMP_TRY(ensure(j, j->coop_ctl, sizeof(CoopCtl)));
-    EMP_TRY(ensure(j, j->efrom, ecap * 4));
-    EMP_TRY(ensure(j, j->eto, ecap * 4));
+    EMP_TRY(ensure(j, j->dout, (size_t)env.rounds * 12 + ecap * 8));
     EMP_TRY(ensure(j, j->records, (size_t)env.rounds * sizeof(RoundRecord)));
     if (!j->h_coop.ensure(sizeof(BktJob) + sizeof(CoopCtl)) ||
         !j->h_records.ensure((size_t)env.rounds * sizeof(RoundRecord)))
@@ -663,8 +665,7 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     hj->spans = j->bk_spans.as<BktSpan>();
     hj->sfrom = j->bk_sfrom.as<uint32_t>();
     hj->sto = j->bk_sto.as<uint32_t>();
-    hj->efrom = j->efrom.as<uint32_t>();
-    hj->eto = j->eto.as<uint32_t>();
+    hj->out = j->dout.as<uint8_t>();
     hj->ecap = ecap;
     hj->records = j->records.as<RoundRecord>();
     hj->scratch = j->bk_scratch.as<uint8_t>();
@@ -711,13 +712,6 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
         *needed = hj->e_total;
         return kNeedEdgeRoom;
     }
-    const uint64_t E_all = hj->e_total;
-    if (E_all) {
-        if (!j->h_from.ensure(E_all * 4) || !j->h_to.ensure(E_all * 4)) return EMP_E_NOMEM;
-        EMP_CUDA(cudaMemcpyAsync(j->h_from.p, j->efrom.p, E_all * 4, cudaMemcpyDeviceToHost, s));
-        EMP_CUDA(cudaMemcpyAsync(j->h_to.p, j->eto.p, E_all * 4, cudaMemcpyDeviceToHost, s));
-        EMP_CUDA(cudaStreamSynchronize(s));
-    }
     const RoundRecord *rec = j->h_records.as<RoundRecord>();
     const int r_end = (int)hj->round;  // rounds run with a non-empty suffix table
     if (trace_path) write_coop_trace(j, trace_path, env.rounds, r0, rec, s, 2, "a_us,b_us");
@@ -733,7 +727,10 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
             st.pfx_live[q] = x.P;
             st.edges[q] = x.E;
         }
-        if (x.P) emit_record(j, env.L - 1 - q, x.e0, x.e0 + x.E);
+        if (x.P) {  // the kernel wrote the record into dout
+            j->dout_bytes += 12 + 8 * x.E;
+            st.n_records += 1;
+        }
         st.n_edges += x.E;
         prev_n = n_out;
     }
@@ -754,6 +751,7 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
     std::memset(st.pfx_live, 0, sizeof st.pfx_live);
     std::memset(st.edges, 0, sizeof st.edges);
     j->out.clear();
+    j->dout_bytes = 0;
     EMP_CUDA(cudaMemsetAsync(j->used_s.p, 0, j->used_s.bytes, s));
     EMP_CUDA(cudaMemsetAsync(j->used_p.p, 0, j->used_p.bytes, s));
     int cur = 0, r = 0;
@@ -889,6 +887,7 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
     emp_stats &st = j->st;
     std::memset(&st, 0, sizeof st);
     j->out.clear();
+    j->dout_bytes = 0;
     j->have_result = false;
     j->n_ends = 0;
     st.fastq_bytes = j->F;
@@ -1041,7 +1040,7 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
     st.ms_dedup = ms_between(ev.e[1], ev.e[2]);
     st.ms_rounds = ms_between(ev.e[2], ev.e[3]);
     st.ms_total = ms_between(ev.e[0], ev.e[4]);
-    st.output_bytes = j->out.size();
+    st.output_bytes = j->out.size() + j->dout_bytes;
     st.gpu_launches = g_launches.load() - launches0;
     j->have_result = true;
     return EMP_OK;
@@ -1197,7 +1196,7 @@ emp_status emp_job_destroy(emp_job *job) {
                       &job->records, &job->st_upd, &job->st_cand, &job->st_scan, &job->ctl, &job->st_join,
                       &job->st_sort, &job->coop_job, &job->coop_ctl, &job->coop_trace,
                       &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_offs, &job->bk_tile_base, &job->bk_spans,
-                      &job->bk_sfrom, &job->bk_sto, &job->bk_scratch, &job->bk_job};
+                      &job->bk_sfrom, &job->bk_sto, &job->bk_scratch, &job->bk_job, &job->dout};
     for (DevBuf *b : bufs) free_buf(job, *b);
     for (auto &e : job->sort_ev)
         if (e) cudaEventDestroy(e);
@@ -1242,6 +1241,7 @@ emp_status emp_job_reset(emp_job *job) {
     job->fed_last = false;
     job->ms_h2d = 0.0;
     job->out.clear();
+    job->dout_bytes = 0;
     job->have_result = false;
     job->n_ends = 0;
     return EMP_OK;
@@ -1298,15 +1298,25 @@ emp_status emp_job_run(emp_job *job, void *stream) {
 emp_status emp_job_output_size(emp_job *job, uint64_t *bytes) {
     if (!job || !bytes) return EMP_E_INVAL;
     if (!job->have_result) return EMP_E_STATE;
-    *bytes = job->out.size();
+    *bytes = job->out.size() + job->dout_bytes;
     return EMP_OK;
 }
 
 emp_status emp_job_output_copy(emp_job *job, void *dst, uint64_t cap) {
-    if (!job || (!dst && job->out.size())) return EMP_E_INVAL;
+    if (!job) return EMP_E_INVAL;
+    const uint64_t host = job->out.size(), total = host + job->dout_bytes;
+    if (!dst && total) return EMP_E_INVAL;
     if (!job->have_result) return EMP_E_STATE;
-    if (cap < job->out.size()) return EMP_E_INVAL;
-    if (job->out.size()) std::memcpy(dst, job->out.data(), job->out.size());
+    if (cap < total) return EMP_E_INVAL;
+    if (host) std::memcpy(dst, job->out.data(), host);
+    if (job->dout_bytes) {  // records of the device-resident rounds follow those of the host-driven ones
+        cudaSetDevice(job->ctx->device);
+        if (cudaMemcpy(static_cast<uint8_t *>(dst) + host, job->dout.p, job->dout_bytes, cudaMemcpyDeviceToHost) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return EMP_E_CUDA;
+        }
+    }
     return EMP_OK;
 }
 
@@ -1368,6 +1378,13 @@ emp_status emp_run_file(const char *input_path, const char *output_path, const e
         else {
             if (!job->out.empty() && std::fwrite(job->out.data(), 1, job->out.size(), g) != job->out.size())
                 st = EMP_E_IO;
+            if (st == EMP_OK && job->dout_bytes) {
+                if (!job->h_out.ensure(job->dout_bytes) ||
+                    cudaMemcpy(job->h_out.p, job->dout.p, job->dout_bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+                    st = EMP_E_CUDA;
+                else if (std::fwrite(job->h_out.p, 1, job->dout_bytes, g) != job->dout_bytes)
+                    st = EMP_E_IO;
+            }
             if (std::fclose(g) != 0) st = EMP_E_IO;
         }
         if (stats) *stats = job->st;

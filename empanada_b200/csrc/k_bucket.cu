@@ -22,8 +22,10 @@
 //      staging buffer at an atomically reserved offset, recorded per
 //      (round, bucket); used entries get a tombstone in the list.  The CTA
 //      finishing a job's last bucket records the round and advances the job.
-//   end  after the last round, each round's edges are copied from the staging
-//      buffer in bucket order, which is sort-key order: the reference's order.
+//   end  after the last round, each round's output.bin record is written
+//      (write_edges_binary, overlap.cu:148-161), its edges copied from the
+//      staging buffer in bucket order, which is sort-key order: the
+//      reference's order.
 // Keys equal across tables share a bucket (the bucket is a function of the
 // key's top bits), so every match is found inside one bucket.
 //
@@ -37,7 +39,7 @@ namespace emp {
 namespace {
 
 constexpr uint32_t kBStage = 8192;  // entries of a bucket staged in shared memory
-constexpr uint32_t kBHash = 8192;   // hash slots in shared memory (power of two)
+constexpr uint32_t kBHash = 16384;  // hash slots in shared memory (power of two)
 constexpr uint32_t kBCand = 3072;   // matched entries sorted in shared memory
 constexpr uint64_t kEmptySlot = ~0ull;  // never a key: fp1, fp2 < 2^29
 constexpr uint32_t kFlag = 0x80000000u; // "matched" mark in a staged entry's position word
@@ -56,10 +58,10 @@ constexpr size_t kBSmem = kOffHash + kHashRegion;
 static_assert(kBStage * 2 <= kHashRegion, "owner table fits the hash region");
 static_assert(kBCand * (8 + 4 + 4) <= kHashRegion, "compacted matches fit the hash region");
 static_assert(kOffHash % 16 == 0, "aligned hash region");
-// phase A: kBktMaxBuckets bucket counters, then the staged tile
-constexpr size_t kASmem = kBktMaxBuckets * 4 + kBktTile * sizeof(BktEntry);
-// end phase: one round's bucket destinations
-constexpr size_t kESmem = (kBktMaxBuckets + 1) * 8;
+// phase A: 2 kBktMaxBuckets bin counters, then the staged tile
+constexpr size_t kASmem = kBktMaxBuckets * 8 + kBktTile * sizeof(BktEntry);
+// end phase: one round's bucket destinations, the record offsets of a job
+constexpr size_t kESmem = (kBktMaxBuckets + 1 + kT) * 8;
 constexpr size_t kBktSmem = kBSmem > kASmem ? (kBSmem > kESmem ? kBSmem : kESmem) : kASmem;
 
 struct BShared {
@@ -153,7 +155,9 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
     probe(ctl, iter, 2);
     const uint32_t p = iter & 1;
     const uint64_t n_in = vld(J.it[p].n_in);
-    const uint32_t nb = vld(J.it[p].nb), stride = nb + 1;
+    // bins: (bucket, table), so a tile's piece of a bucket is its suffixes
+    // followed by its prefixes
+    const uint32_t nb = vld(J.it[p].nb), nbin = 2 * nb, stride = nbin + 1;
     const int L = J.L, r = (int)vld(J.round);
     const uint32_t pw1 = J.tables->pow1[L - r - 1], pw2 = J.tables->pow2[L - r - 1];
     const uint32_t inv1 = J.tables->inv1, inv2 = J.tables->inv2;
@@ -161,8 +165,8 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
     const BktEntry *lin = J.lst[p];
     BktEntry *lout = J.lst[p ^ 1];
     uint32_t *hist = reinterpret_cast<uint32_t *>(smem);
-    uint4 *stage = reinterpret_cast<uint4 *>(smem + kBktMaxBuckets * 4);
-    for (uint32_t i = threadIdx.x; i < nb; i += kT) hist[i] = 0;
+    uint4 *stage = reinterpret_cast<uint4 *>(smem + kBktMaxBuckets * 8);
+    for (uint32_t i = threadIdx.x; i < nbin; i += kT) hist[i] = 0;
     if (threadIdx.x == 0) sh.sfx = 0;
     __syncthreads();
     const uint64_t base = (uint64_t)k * kBktTile;
@@ -212,17 +216,17 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
         const int col = inc ? r : L - 1 - r;
         const uint32_t b = ((word[c] >> ((col & 15) * 2)) & 3u) ^ (s << 1);
         key[c] = t == 0 ? next_sfx(key[c], b, pw1, pw2) : prev_pfx(key[c], b, inv1, inv2);
-        bkt[c] = bkt_of(sort_key(key[c], v), nb);
+        bkt[c] = 2 * bkt_of(sort_key(key[c], v), nb) + t;
         rank[c] = atomicAdd(&hist[bkt[c]], 1u);
         sfx += t == 0;
     }
     if (sfx) atomicAdd(&sh.sfx, sfx);
     __syncthreads();
     probe(ctl, iter, 3);
-    // bucket starts: exclusive scan of the nb counters, each thread a run of them
-    const uint32_t per = (nb + kT - 1) / kT;
-    const uint32_t b0 = threadIdx.x * per < nb ? threadIdx.x * per : nb;
-    const uint32_t b1 = b0 + per < nb ? b0 + per : nb;
+    // bin starts: exclusive scan of the nbin counters, each thread a run of them
+    const uint32_t per = (nbin + kT - 1) / kT;
+    const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
+    const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
     uint32_t run = 0;
     for (uint32_t b = b0; b < b1; ++b) run += hist[b];
     uint32_t kept;
@@ -235,7 +239,7 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
         ex += h;
     }
     if (threadIdx.x == 0) {
-        orow[nb] = kept;
+        orow[nbin] = kept;
         const uint64_t ob = atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].n_out),
                                       (unsigned long long)kept);
         sh.base = ob;
@@ -301,33 +305,42 @@ EMP_DEV void put_entry(const BView &v, uint32_t d, const BktEntry *lst, uint64_t
 // Gather bucket b: returns its size and sets up v (shared memory, or the
 // global scratch region at the bucket's place in bucket order).
 EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, const BktEntry *lst, BShared &sh,
-                        uint8_t *smem, BView &v, uint64_t &G) {
+                        uint8_t *smem, BView &v, uint64_t &G, uint32_t &S) {
+    // segments q = 0 .. 2K-1: the suffix piece of tile q, then (q >= K) the
+    // prefix piece of tile q - K, so the bucket is staged suffixes first
     const uint32_t *offs = J.offs;
-    const uint32_t stride = nb + 1;
-    if (K <= (uint32_t)kT) {
+    const uint32_t stride = 2 * nb + 1, Q = 2 * K;
+    auto seg = [&](uint32_t q, uint32_t &lo, uint32_t &cnt) -> uint64_t {  // returns the tile's base
+        const uint32_t k = q < K ? q : q - K, bin = 2 * b + (q < K ? 0u : 1u);
+        lo = __ldcg(offs + (uint64_t)k * stride + bin);
+        cnt = __ldcg(offs + (uint64_t)k * stride + bin + 1) - lo;
+        return k;
+    };
+    if (Q <= (uint32_t)kT) {
         // fast path: one segment per thread; an owner table maps staged
         // entries to segments
-        const uint32_t k = threadIdx.x;
+        const uint32_t q = threadIdx.x;
         uint32_t lo = 0, cnt = 0;
         uint64_t start = 0;
-        if (k < K) {
-            lo = __ldcg(offs + (uint64_t)k * stride + b);
-            cnt = __ldcg(offs + (uint64_t)k * stride + b + 1) - lo;
+        if (q < Q) {
+            const uint64_t k = seg(q, lo, cnt);
             start = __ldcg(J.tile_base + k) + lo;
         }
         uint32_t total;
         const uint32_t ex = block_exclusive_scan<kT, uint32_t>(cnt, sh.scan32, &total);
+        if (q == K) sh.tile = ex;  // suffixes: the segments before the first prefix piece
         if (total <= kBStage) {
             G = 0;
             set_stage(v, smem);
             uint16_t *owner = reinterpret_cast<uint16_t *>(smem + kOffHash);
             sh.seg_start[threadIdx.x] = start;
             sh.seg_pos[threadIdx.x] = ex;
-            for (uint32_t x = ex; x < ex + cnt; ++x) owner[x] = (uint16_t)k;
+            for (uint32_t x = ex; x < ex + cnt; ++x) owner[x] = (uint16_t)q;
             __syncthreads();
+            S = K ? sh.tile : 0u;
             constexpr int U = 4;
             for (uint32_t x0 = 0; x0 < total; x0 += U * kT) {
-                uint4 q[U];
+                uint4 e[U];
                 uint64_t src[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
@@ -335,15 +348,15 @@ EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, co
                     if (x < total) {
                         const uint32_t o = owner[x];
                         src[u] = sh.seg_start[o] + (x - sh.seg_pos[o]);
-                        q[u] = __ldcg(reinterpret_cast<const uint4 *>(lst + src[u]));
+                        e[u] = __ldcg(reinterpret_cast<const uint4 *>(lst + src[u]));
                     }
                 }
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const uint32_t x = x0 + u * kT + threadIdx.x;
                     if (x < total) {
-                        v.key[x] = (uint64_t)q[u].x | ((uint64_t)q[u].y << 32);
-                        v.val[x] = q[u].z;
+                        v.key[x] = (uint64_t)e[u].x | ((uint64_t)e[u].y << 32);
+                        v.val[x] = e[u].z;
                         v.pos[x] = (uint32_t)src[u];
                     }
                 }
@@ -353,17 +366,23 @@ EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, co
         }
     }
     // general path: many tiles, or a bucket too big for shared memory
-    uint64_t tot = 0, gpre = 0;
-    for (uint32_t k = threadIdx.x; k < K; k += kT) {
-        const uint32_t lo = __ldcg(offs + (uint64_t)k * stride + b), hi = __ldcg(offs + (uint64_t)k * stride + b + 1);
-        tot += hi - lo;
-        gpre += lo;
+    uint64_t tot = 0, tsfx = 0, gpre = 0;
+    for (uint32_t q = threadIdx.x; q < Q; q += kT) {
+        uint32_t lo, cnt;
+        seg(q, lo, cnt);
+        tot += cnt;
+        if (q < K) {
+            tsfx += cnt;
+            gpre += lo;  // entries of lower buckets in tile q
+        }
     }
-    uint64_t t1, t2;
+    uint64_t t1, t2, t3;
     block_exclusive_scan<kT, uint64_t>(tot, sh.scan64, &t1);
-    block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &t2);
+    block_exclusive_scan<kT, uint64_t>(tsfx, sh.scan64, &t2);
+    block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &t3);
     const uint32_t total = (uint32_t)t1;
-    G = t2;
+    S = (uint32_t)t2;
+    G = t3;
     if (total <= kBStage) {
         G = 0;
         set_stage(v, smem);
@@ -373,13 +392,12 @@ EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, co
         set_stage(v, gs, G, total);
     }
     uint32_t gathered = 0;
-    for (uint32_t k0 = 0; k0 < K && total; k0 += kT) {
-        const uint32_t k = k0 + threadIdx.x;
-        uint32_t cnt = 0;
+    for (uint32_t q0 = 0; q0 < Q && total; q0 += kT) {
+        const uint32_t q = q0 + threadIdx.x;
+        uint32_t lo = 0, cnt = 0;
         uint64_t start = 0;
-        if (k < K) {
-            const uint32_t lo = __ldcg(offs + (uint64_t)k * stride + b), hi = __ldcg(offs + (uint64_t)k * stride + b + 1);
-            cnt = hi - lo;
+        if (q < Q) {
+            const uint64_t k = seg(q, lo, cnt);
             start = __ldcg(J.tile_base + k) + lo;
         }
         uint32_t ctot;
@@ -388,13 +406,13 @@ EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, co
         sh.seg_pos[threadIdx.x] = ex;
         __syncthreads();
         for (uint32_t x = threadIdx.x; x < ctot; x += kT) {
-            uint32_t lo = 0, hi = kT;  // last segment with seg_pos <= x
-            while (hi - lo > 1) {
-                const uint32_t m = (lo + hi) >> 1;
-                if (sh.seg_pos[m] <= x) lo = m;
+            uint32_t lo2 = 0, hi = kT;  // last segment with seg_pos <= x
+            while (hi - lo2 > 1) {
+                const uint32_t m = (lo2 + hi) >> 1;
+                if (sh.seg_pos[m] <= x) lo2 = m;
                 else hi = m;
             }
-            put_entry(v, gathered + x, lst, sh.seg_start[lo] + (x - sh.seg_pos[lo]));
+            put_entry(v, gathered + x, lst, sh.seg_start[lo2] + (x - sh.seg_pos[lo2]));
         }
         gathered += ctot;
         __syncthreads();
@@ -408,57 +426,87 @@ EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, co
 // through it).  A tag of all ones is never used, so kSlotEmpty is no slot.
 constexpr uint32_t kSlotEmpty = 0xffffffffu;
 constexpr uint32_t kSlotMatched = 0x80000000u;
-static_assert(kBStage <= 8192 && kBHash == 8192, "13-bit staged indices and slot numbers");
+static_assert(kBStage <= 8192 && kBHash == 16384, "13-bit staged indices, 14-bit slot numbers");
 
 EMP_DEV void hash_tag(uint64_t key, uint32_t &slot, uint32_t &tag) {
     const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 32);
     slot = h & (kBHash - 1);
-    tag = (h >> 13) & 0x3ffffu;
+    tag = (h >> 14) & 0x3ffffu;
     if (tag == 0x3ffffu) tag = 0x3fffeu;
+}
+EMP_DEV bool slot_holds(uint32_t w, uint32_t tag, uint64_t k, const uint64_t *key) {
+    return ((w >> 13) & 0x3ffffu) == tag && key[w & 8191u] == k;
 }
 
 // Mark (kFlag in pos) every staged entry whose key occurs in both tables.
-EMP_DEV void match_smem(uint32_t total, uint8_t *smem) {
+// The bucket is staged suffixes first: [0, S) suffixes, [S, total) prefixes.
+// Each thread works on kU entries at once so their shared-memory round trips
+// overlap; a collision falls back to a probe loop.
+EMP_DEV void match_smem(uint32_t total, uint32_t S, uint8_t *smem) {
+    constexpr int kU = 4;
     const uint64_t *key = reinterpret_cast<const uint64_t *>(smem + kOffKey);
-    const uint32_t *val = reinterpret_cast<const uint32_t *>(smem + kOffVal);
     uint32_t *pos = reinterpret_cast<uint32_t *>(smem + kOffPos);
     uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kOffHash);
     uint16_t *sslot = reinterpret_cast<uint16_t *>(smem + kOffHash + kBHash * 4);
     for (uint32_t s = threadIdx.x; s < kBHash; s += kT) slot[s] = kSlotEmpty;
     __syncthreads();
-    for (uint32_t x = threadIdx.x; x < total; x += kT) {  // suffixes: insert
-        if (val[x] >> 31) continue;
-        const uint64_t k = key[x];
-        uint32_t s, tag;
-        hash_tag(k, s, tag);
-        const uint32_t mine = (tag << 13) | x;
-        for (uint32_t probes = 0; probes < kBHash; ++probes) {
-            const uint32_t old = atomicCAS(slot + s, kSlotEmpty, mine);
-            if (old == kSlotEmpty || (((old >> 13) & 0x3ffffu) == tag && key[old & 8191u] == k)) break;
-            s = (s + 1) & (kBHash - 1);
-        }
-        sslot[x] = (uint16_t)s;
-    }
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < total; x += kT) {  // prefixes: probe
-        if (!(val[x] >> 31)) continue;
-        const uint64_t k = key[x];
-        uint32_t s, tag;
-        hash_tag(k, s, tag);
-        for (uint32_t probes = 0; probes < kBHash; ++probes) {
-            const uint32_t w = slot[s];
-            if (w == kSlotEmpty) break;
-            if (((w >> 13) & 0x3ffffu) == tag && key[w & 8191u] == k) {
-                if (!(w & kSlotMatched)) atomicOr(slot + s, kSlotMatched);
-                pos[x] |= kFlag;
-                break;
+    for (uint32_t x0 = 0; x0 < S; x0 += kU * kT) {  // suffixes: insert
+        uint64_t k[kU];
+        uint32_t s[kU], tag[kU], old[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            if (x < S) {
+                k[u] = key[x];
+                hash_tag(k[u], s[u], tag[u]);
+                old[u] = atomicCAS(slot + s[u], kSlotEmpty, (tag[u] << 13) | x);
             }
-            s = (s + 1) & (kBHash - 1);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            if (x >= S) continue;
+            uint32_t sl = s[u], w = old[u];
+            for (uint32_t probes = 1; w != kSlotEmpty && !slot_holds(w, tag[u], k[u], key) && probes < kBHash;
+                 ++probes) {
+                sl = (sl + 1) & (kBHash - 1);
+                w = atomicCAS(slot + sl, kSlotEmpty, (tag[u] << 13) | x);
+            }
+            sslot[x] = (uint16_t)sl;
         }
     }
     __syncthreads();
-    for (uint32_t x = threadIdx.x; x < total; x += kT)  // suffixes: matched?
-        if (!(val[x] >> 31) && (slot[sslot[x]] & kSlotMatched)) pos[x] |= kFlag;
+    for (uint32_t x0 = S; x0 < total; x0 += kU * kT) {  // prefixes: probe
+        uint64_t k[kU];
+        uint32_t s[kU], tag[kU], w[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            if (x < total) {
+                k[u] = key[x];
+                hash_tag(k[u], s[u], tag[u]);
+                w[u] = slot[s[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            if (x >= total) continue;
+            uint32_t sl = s[u], ww = w[u];
+            for (uint32_t probes = 1; ww != kSlotEmpty && probes < kBHash; ++probes) {
+                if (slot_holds(ww, tag[u], k[u], key)) {
+                    if (!(ww & kSlotMatched)) atomicOr(slot + sl, kSlotMatched);
+                    pos[x] |= kFlag;
+                    break;
+                }
+                sl = (sl + 1) & (kBHash - 1);
+                ww = slot[sl];
+            }
+        }
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < S; x += kT)  // suffixes: matched?
+        if (slot[sslot[x]] & kSlotMatched) pos[x] |= kFlag;
     __syncthreads();
 }
 
@@ -598,12 +646,13 @@ EMP_DEV void b_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const Coo
     BktEntry *lst = J.lst[p ^ 1];
     BView v;
     uint64_t G = 0;
-    const uint32_t total = gather(J, b, nb, K, lst, sh, smem, v, G);
+    uint32_t S = 0;
+    const uint32_t total = gather(J, b, nb, K, lst, sh, smem, v, G, S);
     const bool in_smem = total <= kBStage;
     probe(ctl, iter, 13);
     // ---- matches: entries whose key is in both tables get kFlag in pos
     if (total) {
-        if (in_smem) match_smem(total, smem);
+        if (in_smem) match_smem(total, S, smem);
         else match_view(v, total);
     }
     probe(ctl, iter, 14);
@@ -678,8 +727,8 @@ EMP_DEV void b_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const Coo
             }
             if (in_smem) {  // the bucket's place in bucket order picks its scratch region
                 uint64_t gpre = 0;
-                const uint32_t stride = nb + 1;
-                for (uint32_t k = threadIdx.x; k < K; k += kT) gpre += __ldcg(J.offs + (uint64_t)k * stride + b);
+                const uint32_t stride = 2 * nb + 1;
+                for (uint32_t k = threadIdx.x; k < K; k += kT) gpre += __ldcg(J.offs + (uint64_t)k * stride + 2 * b);
                 block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &G);
             }
             BScratch gs;
@@ -781,19 +830,37 @@ EMP_DEV void round_end(BktJob &x, CoopCtl *ctl, uint32_t iter) {
 // edge list in bucket order (rounds spread over the CTAs, no grid barrier).
 EMP_DEV void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
     uint64_t *dest = reinterpret_cast<uint64_t *>(smem);  // nb + 1 bucket starts
+    uint64_t *roff = dest + kBktMaxBuckets + 1;          // byte offset of each round's record
     uint32_t g = 0;
     for (int j = 0; j < J; ++j) {
         BktJob &x = jobs[j];
         if (vld(x.overflow)) continue;
-        const uint32_t r1 = vld(x.round);
-        for (uint32_t r = (uint32_t)x.r0; r < r1; ++r, ++g) {
+        const uint32_t r0 = (uint32_t)x.r0, r1 = vld(x.round);
+        {  // records: one per round with a non-empty prefix table, 12 + 8 E bytes
+            const uint32_t r = r0 + threadIdx.x;
+            uint64_t sz = 0;
+            if (r < r1 && __ldcg(&x.records[r].P)) sz = 12 + 8 * __ldcg(&x.records[r].E);
+            uint64_t tot;
+            const uint64_t ex = block_exclusive_scan<kT, uint64_t>(sz, sh.scan64, &tot);
+            if (r < r1) roff[threadIdx.x] = ex;
+            __syncthreads();
+        }
+        for (uint32_t r = r0; r < r1; ++r, ++g) {
             if (g % gridDim.x != blockIdx.x) continue;
             const RoundRecord &rec = x.records[r];
+            if (!__ldcg(&rec.P)) continue;
             const uint64_t E = __ldcg(&rec.E);
+            uint8_t *o = x.out + roff[r - r0];
+            uint32_t *from = reinterpret_cast<uint32_t *>(o + 12), *to = from + E;
+            if (threadIdx.x == 0) {  // u64 n, i32 ovlp_len (write_edges_binary, overlap.cu:148-161)
+                uint32_t *h = reinterpret_cast<uint32_t *>(o);
+                h[0] = (uint32_t)E;
+                h[1] = (uint32_t)(E >> 32);
+                h[2] = (uint32_t)(x.L - 1 - (int)r);
+            }
             if (!E) continue;
             const uint32_t nb = (uint32_t)__ldcg(&rec.nb);
-            const uint64_t e0 = __ldcg(&rec.e0);
-            const BktSpan *sp = x.spans + (uint64_t)(r - x.r0) * x.nb_max;
+            const BktSpan *sp = x.spans + (uint64_t)(r - r0) * x.nb_max;
             uint64_t run = 0;
             for (uint32_t b0 = 0; b0 < nb; b0 += kT) {
                 const uint32_t b = b0 + threadIdx.x;
@@ -813,8 +880,8 @@ EMP_DEV void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
                     else hi = m;
                 }
                 const uint64_t src = __ldcg(&sp[lo].off) + (e - dest[lo]);
-                x.efrom[e0 + e] = __ldcg(x.sfrom + src);
-                x.eto[e0 + e] = __ldcg(x.sto + src);
+                from[e] = __ldcg(x.sfrom + src);
+                to[e] = __ldcg(x.sto + src);
             }
             __syncthreads();
         }
@@ -881,7 +948,7 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
 size_t bkt_scratch_bytes(uint64_t n_max) { return scratch_layout(nullptr, n_max < 1 ? 1 : n_max, nullptr); }
 
 size_t bkt_offs_words(uint64_t n_max, uint32_t G) {
-    return (size_t)bkt_tiles(n_max < 1 ? 1 : n_max) * (bkt_count(n_max, G) + 1);
+    return (size_t)bkt_tiles(n_max < 1 ? 1 : n_max) * (2 * bkt_count(n_max, G) + 1);
 }
 
 int bucket_grid_size() {

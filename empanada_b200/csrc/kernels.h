@@ -275,7 +275,7 @@ struct BktJob {
     uint64_t *tile_base;     // per phase-A tile: its first output entry
     BktSpan *spans;          // [round - r0][bucket]: edges in the staging buffer
     uint32_t *sfrom, *sto;   // staging buffer (bucket order within a round is restored at the end)
-    uint32_t *efrom, *eto;   // edges of all rounds, in the reference's order
+    uint8_t *out;            // output.bin records of the launch's rounds (12 * rounds + 8 * ecap bytes)
     uint64_t ecap;
     RoundRecord *records;
     uint8_t *scratch;        // bkt_scratch_bytes(n_max): buckets too big for shared memory
