@@ -14,9 +14,11 @@ each rank runs its own job, no data-path collective):
   e2e       reads/s through the C ABI with host buffers: emp_job_reset +
             emp_job_feed_fastq (pinned host -> HBM) + emp_job_run + copy of
             output.bin to host, wall clock per step
-  roofline  the radix-sort digit pass (dominant kernel): algorithmic bytes
-            (24 per pair: 12 read + 12 written) / its event-timed launch time,
-            against the measured HBM copy bandwidth
+  roofline  the dominant kernel (the cooperative kernel that runs every
+            overlap round in one launch): its algorithmic bytes per launch
+            (per round 16 B per entry read, 16 B written and 16 B gathered per
+            kept entry, 8 B per edge) / its event-timed duration, against the
+            measured HBM copy bandwidth
   cpu_baseline  rank 0 at N=1: the reference's own sources built as a CPU
             program (oracle/_ref, Thrust on OpenMP) on a bounded sample
 impl reference: that CPU build alone, timed per step on the bounded sample
@@ -313,6 +315,8 @@ def main():
     upd_ms = 0.0
     upd_bytes = 0
     upd_launches = 0
+    rk_ms = 0.0
+    rk_bytes = 0.0
     with ClockSampler(device) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -331,6 +335,8 @@ def main():
             upd_ms += st["ms_update"]
             upd_bytes += st["update_bytes"]
             upd_launches += st["update_launches"]
+            rk_ms += st["ms_round_kernel"]
+            rk_bytes += st["round_kernel_bytes"]
     barrier()
     clocks = clk.summary()
     total_ms = sum(step_ms)
@@ -366,7 +372,18 @@ def main():
 
     peak, peak_kind = measured_peaks()
     traffic = traffic_summary()
-    if sort_ms >= upd_ms:  # the radix-sort digit pass dominates
+    if rk_ms >= max(sort_ms, upd_ms):  # the all-rounds cooperative kernel dominates
+        per_launch = rk_bytes / args.steps
+        ms, nl = rk_ms, args.steps
+        if os.environ.get("EMP_NO_BUCKET"):
+            kname = "coop_rounds_kernel"
+            what = ("all rounds, Bloom-filter driver: per round 13 B + 1/4 B per entry in, 24 B per kept entry, "
+                    "72 B per candidate, 8 B per edge")
+        else:
+            kname = "bucket_rounds_kernel"
+            what = ("all rounds in one launch: per round 16 B read per entry in, 16 B written + 16 B gathered "
+                    "per kept entry, 8 B per edge")
+    elif sort_ms >= upd_ms:  # the radix-sort digit pass dominates
         per_launch = 24.0 * sort_elems / max(sort_passes, 1)
         ms, nl, kname = sort_ms, sort_passes, "onesweep_kernel"
         what = "radix-sort digit pass: 24 B per pair (12 read, 12 written)"
@@ -380,6 +397,7 @@ def main():
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} (HBM copy, burst)",
                 "traffic": (tb * per_launch) if tb else None, "algorithmic_bytes_per_launch": per_launch,
                 "avg_launch_us": 1000.0 * ms / max(nl, 1), "launches": nl,
+                "round_kernel_ms_per_step": rk_ms / args.steps,
                 "sort_pass_ms_per_step": sort_ms / args.steps, "update_ms_per_step": upd_ms / args.steps}
 
     cpu = None
