@@ -178,6 +178,35 @@ EMP_DEV uint32_t build_prefix(S &sh, int J, F count) {
     return tot;
 }
 
+// tile t of the prefix -> (job, local tile)
+template <class S, class F>
+EMP_DEV void run_tile(S &sh, int J, uint32_t t, F f) {
+    int lo = 0, hi = J;
+    while (hi - lo > 1) {
+        const int m = (lo + hi) >> 1;
+        if (sh.pref[m] <= t) lo = m;
+        else hi = m;
+    }
+    f(lo, t - sh.pref[lo]);
+}
+
+// Tiles without an order between them: CTA i takes tile i first, then the
+// rest from the ticket (offset by the grid); no ticket round trip at all
+// when there are at most as many tiles as CTAs.
+template <class S, class F>
+EMP_DEV void tile_loop_static(S &sh, uint32_t *ticket, int J, uint32_t total, F f) {
+    if (blockIdx.x < total) run_tile(sh, J, blockIdx.x, f);
+    if (total <= gridDim.x) return;
+    for (;;) {
+        if (threadIdx.x == 0) sh.tile = gridDim.x + atomicAdd(ticket, 1u);
+        __syncthreads();
+        const uint32_t t = sh.tile;
+        __syncthreads();
+        if (t >= total) break;
+        run_tile(sh, J, t, f);
+    }
+}
+
 // take tiles from the ticket until all `total` are gone; f(job, local tile)
 template <class S, class F>
 EMP_DEV void tile_loop(S &sh, uint32_t *ticket, int J, uint32_t total, F f) {

@@ -628,13 +628,14 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
                              uint64_t ecap, uint64_t *needed) {
     emp_stats &st = j->st;
     const uint64_t nmax = n_in;
-    const uint64_t ktiles = bkt_tiles(nmax);
     const int grid = bucket_grid_size();
+    const uint64_t ktiles = bkt_max_tiles(nmax, (uint32_t)grid);
     const uint32_t nb_max = bkt_count(nmax, (uint32_t)grid);
+    const size_t offs_words = bkt_offs_words(nmax, (uint32_t)grid);
     EMP_TRY(ensure(j, j->bk_lst0, nmax * sizeof(BktEntry)));
     EMP_TRY(ensure(j, j->bk_lst1, nmax * sizeof(BktEntry)));
-    EMP_TRY(ensure(j, j->bk_offs, bkt_offs_words(nmax, (uint32_t)grid) * 4));
-    EMP_TRY(ensure(j, j->bk_tile_base, ktiles * 8));
+    EMP_TRY(ensure(j, j->bk_offs, 2 * offs_words * 4));
+    EMP_TRY(ensure(j, j->bk_tile_base, 2 * ktiles * 8));
     EMP_TRY(ensure(j, j->bk_spans, (size_t)env.rounds * nb_max * sizeof(BktSpan)));
     EMP_TRY(ensure(j, j->bk_sfrom, ecap * 4));
     EMP_TRY(ensure(j, j->bk_sto, ecap * 4));
@@ -660,8 +661,11 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     hj->L = env.L;
     hj->rounds = env.rounds;
     hj->tables = env.tables;
-    hj->offs = j->bk_offs.as<uint32_t>();
-    hj->tile_base = j->bk_tile_base.as<uint64_t>();
+    hj->n_in = n_in;
+    hj->offs[0] = j->bk_offs.as<uint32_t>();
+    hj->offs[1] = hj->offs[0] + offs_words;
+    hj->tile_base[0] = j->bk_tile_base.as<uint64_t>();
+    hj->tile_base[1] = hj->tile_base[0] + ktiles;
     hj->spans = j->bk_spans.as<BktSpan>();
     hj->sfrom = j->bk_sfrom.as<uint32_t>();
     hj->sto = j->bk_sto.as<uint32_t>();
@@ -674,7 +678,7 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     hj->r0 = r0;
     hj->round = (uint32_t)r0;
     hj->end_iter = 0xffffffffu;
-    hj->it[0].n_in = n_in;
+    hj->it[0].K = (uint32_t)bkt_tiles(n_in);  // the prologue's tiles
     hj->it[0].nb = bkt_count(n_in, (uint32_t)grid);
     hc->njobs = 1;
     hc->active = 1;
@@ -714,14 +718,14 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     }
     const RoundRecord *rec = j->h_records.as<RoundRecord>();
     const int r_end = (int)hj->round;  // rounds run with a non-empty suffix table
-    if (trace_path) write_coop_trace(j, trace_path, env.rounds, r0, rec, s, 2, "a_us,b_us");
+    if (trace_path) write_coop_trace(j, trace_path, env.rounds, r0, rec, s, 1, "round_us");
     if (probe_env) write_coop_probe(j, probe_path.c_str(), grid, s);
     uint64_t prev_n = n_in;
     for (int q = r0; q < r_end; ++q) {
         const RoundRecord &x = rec[q];
         const uint64_t n_out = x.S + x.P;
-        // phase A reads each entry and writes the kept ones; phase B gathers them
-        st.round_kernel_bytes += 16 * prev_n + 32 * n_out + 8 * x.E;
+        // each round gathers its entries and writes the kept ones for the next
+        st.round_kernel_bytes += 16 * prev_n + 16 * n_out + 8 * x.E;
         if (q < EMP_MAX_ROUNDS) {
             st.sfx_live[q] = x.S;
             st.pfx_live[q] = x.P;

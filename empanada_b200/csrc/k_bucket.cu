@@ -1,90 +1,127 @@
 // k_bucket.cu -- every overlap round of one or many read sets in ONE
-// cooperative launch: two grid barriers per round, no CTA waiting on another
-// inside a phase, no global random access on the streaming side.
+// cooperative launch, one grid barrier per round.
 //
-// Round r of a job (overlap.cu:258-290):
-//   A  stream the live entries in 4096-entry tiles: drop entries used in the
-//      previous round (tombstones written by B, or the used marks of rounds
-//      run before the launch: remove_used, overlap.cu:694-710), apply the
-//      hash step NextSfx / PrevPfx (overlap.cu:57-91) with the base taken from
-//      a 16-base word cached in the entry (one read-major load per 16 rounds:
-//      regenerate_fingerprints + filter_bases, overlap.cu:605-692), and
-//      partition the tile in shared memory into the round's key buckets.  The
-//      tile's output space comes from one atomic add; its bucket starts go to
-//      offs[tile][0..nb].  List order is irrelevant from here on: B orders
-//      everything it uses by a total order.
-//   B  one CTA per bucket: gather the bucket's piece of every A tile, insert
-//      the suffix keys into a hash set, probe the prefix keys, keep the
-//      entries whose key is in both tables, sort them by the sort key with
-//      the tie order of the reference's stable sort (table, then rid parity,
-//      then read index: the regenerated tables' order), and join equal-key
-//      runs (get_edges, overlap.cu:557-603).  The bucket's edges go to a
-//      staging buffer at an atomically reserved offset, recorded per
-//      (round, bucket); used entries get a tombstone in the list.  The CTA
-//      finishing a job's last bucket records the round and advances the job.
-//   end  after the last round, each round's output.bin record is written
-//      (write_edges_binary, overlap.cu:148-161), its edges copied from the
-//      staging buffer in bucket order, which is sort-key order: the
-//      reference's order.
-// Keys equal across tables share a bucket (the bucket is a function of the
-// key's top bits), so every match is found inside one bucket.
+// A round's list is a set of tiles of 16-byte entries (key, rid | table, a
+// cached 16-base word of the read); each tile is partitioned into
+// (key bucket, table) bins.  The bucket of an entry is the top 24 bits of its
+// sort key scaled to the round's bucket count, so keys equal across tables
+// share a bucket and bucket order is key order.
 //
-// A bucket that does not fit shared memory (8192 entries, or 3072 matched
-// entries) uses the job's global scratch region instead, at the bucket's
-// position in the round's bucket order.
+//   prologue  the launch's input list (id order; the keys of round r0 - 1)
+//      is streamed in 4096-entry tiles: entries used in the rounds run
+//      before the launch are dropped (remove_used, overlap.cu:694-710), the
+//      hash step NextSfx / PrevPfx (overlap.cu:57-91) gives round r0's keys,
+//      and each tile is partitioned in shared memory.
+//   round r   one CTA per bucket: gather the bucket's piece of every tile
+//      (suffixes first), insert the suffix keys into a hash set, probe the
+//      prefix keys, rank the entries present in both tables by (sort key,
+//      rid parity, read index) -- the order of the reference's stable sort
+//      over its regenerated tables (regenerate_fingerprints,
+//      overlap.cu:605-692) -- and join equal-key runs (get_edges,
+//      overlap.cu:557-603).  The bucket's edges go to a staging buffer at an
+//      atomically reserved offset.  Then the same CTA drops the bucket's used
+//      entries, applies round r+1's hash step to the rest (the base from the
+//      cached word; one read-major load per 16 rounds) and writes them as one
+//      partitioned tile of round r+1's list.  The CTA finishing a job's last
+//      bucket records the round and prepares the job's next one.
+//   end  every round's output.bin record (write_edges_binary,
+//      overlap.cu:148-161) is written with its edges in bucket order, which
+//      is sort-key order: the reference's order.
+//
+// A bucket that does not fit shared memory (7168 entries, or 1024 matched
+// entries) uses the job's global scratch region at the bucket's position in
+// bucket order instead.
 #include "coop_common.cuh"
+
+// Steps that run once per launch or only for oversized buckets are kept out
+// of line, so their registers do not weigh on the per-bucket path.
+#define EMP_COLD __device__ __noinline__
 
 namespace emp {
 
 namespace {
 
-constexpr uint32_t kBStage = 8192;  // entries of a bucket staged in shared memory
+constexpr uint32_t kBStage = 7168;  // entries of a bucket staged in shared memory
 constexpr uint32_t kBHash = 16384;  // hash slots in shared memory (power of two)
-constexpr uint32_t kBCand = 3072;   // matched entries sorted in shared memory
+constexpr uint32_t kBCand = 1024;   // matched entries sorted in shared memory
+constexpr uint32_t kSegMax = 4096;  // tile pieces gathered through the owner table
 constexpr uint64_t kEmptySlot = ~0ull;  // never a key: fp1, fp2 < 2^29
-constexpr uint32_t kFlag = 0x80000000u; // "matched" mark in a staged entry's position word
+constexpr uint8_t kMatched = 1, kUsed = 2;
 
-// shared-memory layout of phase B (bytes): the staged bucket (key, val,
-// list position), then a region that holds in turn the gather's owner table
-// (u16 per staged entry), the hash set (u32 slots + the u16 slot of each
-// suffix), and the compacted matched entries; once those are compacted the
-// stage region holds their sort arrays
+// Shared memory of a round tile: the staged bucket, then a region used in
+// turn by the gather (piece table + owner of each staged entry), the hash set
+// (u32 slots + the slot of each suffix), the matched entries and their sort
+// arrays, and the next round's partition (bin counters + permutation).
 constexpr size_t kOffKey = 0;
 constexpr size_t kOffVal = kOffKey + kBStage * 8;
-constexpr size_t kOffPos = kOffVal + kBStage * 4;
-constexpr size_t kOffHash = kOffPos + kBStage * 4;
-constexpr size_t kHashRegion = kBHash * 4 + kBStage * 2;
-constexpr size_t kBSmem = kOffHash + kHashRegion;
-static_assert(kBStage * 2 <= kHashRegion, "owner table fits the hash region");
-static_assert(kBCand * (8 + 4 + 4) <= kHashRegion, "compacted matches fit the hash region");
-static_assert(kOffHash % 16 == 0, "aligned hash region");
-// phase A: 2 kBktMaxBuckets bin counters, then the staged tile
-constexpr size_t kASmem = kBktMaxBuckets * 8 + kBktTile * sizeof(BktEntry);
+constexpr size_t kOffWord = kOffVal + kBStage * 4;
+constexpr size_t kOffFlag = kOffWord + kBStage * 4;
+constexpr size_t kOffReg = kOffFlag + kBStage;
+constexpr size_t kRegion = kBHash * 4 + kBStage * 2;
+constexpr size_t kRSmem = kOffReg + kRegion;
+static_assert(kOffReg % 16 == 0, "aligned region");
+// gather
+constexpr size_t kGSegStart = 0;                          // u64 [kSegMax]
+constexpr size_t kGSegPos = kGSegStart + kSegMax * 8;     // u32 [kSegMax + 1]
+constexpr size_t kGOwner = kGSegPos + (kSegMax + 4) * 4;  // u16 [kBStage]
+static_assert(kGOwner + kBStage * 2 <= kRegion, "gather tables fit the region");
+// hash set
+constexpr size_t kHSlot = 0;                 // u32 [kBHash]
+constexpr size_t kHSuffixSlot = kBHash * 4;  // u16 [kBStage]
+// matched entries
+constexpr size_t kCKey = 0;                       // u64 [kBCand]
+constexpr size_t kCVal = kCKey + kBCand * 8;      // u32
+constexpr size_t kCIdx = kCVal + kBCand * 4;      // u32 (staged index)
+constexpr size_t kCSk = kCIdx + kBCand * 4;       // u64 sort keys
+constexpr size_t kCTb = kCSk + kBCand * 8;        // u32 tie keys
+constexpr size_t kCOrd = kCTb + kBCand * 4;       // u32 chunk order
+constexpr size_t kCCnt = kCOrd + kBCand * 4;      // u64 edge counts / offsets
+constexpr size_t kCSKey = kCCnt + kBCand * 8;     // u64 sorted keys
+constexpr size_t kCSVal = kCSKey + kBCand * 8;    // u32
+constexpr size_t kCSIdx = kCSVal + kBCand * 4;    // u32
+static_assert(kCSIdx + kBCand * 4 <= kRegion, "matched entries fit the region");
+// next round's partition
+constexpr size_t kPHist = 0;                                // u32 [2 kBktMaxBuckets]
+constexpr size_t kPInv = kPHist + 2 * kBktMaxBuckets * 4;   // u16 [kBStage]
+constexpr size_t kPRank = kPInv + kBStage * 2;              // u16 [kBStage]
+constexpr size_t kPBin = kPRank + kBStage * 2;              // u16 [kBStage]
+static_assert(kPBin + kBStage * 2 <= kRegion, "partition tables fit the region");
+static_assert(2 * kBktMaxBuckets <= 65536, "bins fit u16");
+// prologue tile: bin counters, then the staged tile
+constexpr size_t kASmem = 2 * kBktMaxBuckets * 4 + kBktTile * sizeof(BktEntry);
 // end phase: one round's bucket destinations, the record offsets of a job
 constexpr size_t kESmem = (kBktMaxBuckets + 1 + kT) * 8;
-constexpr size_t kBktSmem = kBSmem > kASmem ? (kBSmem > kESmem ? kBSmem : kESmem) : kASmem;
+constexpr size_t kBktSmem = kRSmem > kASmem ? (kRSmem > kESmem ? kRSmem : kESmem) : kASmem;
 
 struct BShared {
     uint32_t pref[kCoopMaxJobs + 1];
     uint32_t scan32[32];
     uint64_t scan64[32];
-    uint64_t seg_start[kT];
-    uint32_t seg_pos[kT + 1];
-    uint64_t base, tot, gpre;
-    uint32_t tile, flag, sfx;
+    uint64_t base;
+    uint32_t tile, flag, sfx, cnt;
+    const CoopCtl *pctl;  // profiling stamps from inside the steps of a tile
+    uint32_t piter;
 };
+EMP_DEV void sprobe(const BShared &sh, int p) { probe(sh.pctl, sh.piter, p); }
 
-// global scratch arrays of a job (n_max entries each, hash arrays 2 n_max)
+// A job's global scratch (N = n_max entries per array, 2N hash slots): a
+// bucket that does not fit shared memory uses the region of its position in
+// bucket order.
 struct BScratch {
     uint64_t *key;
-    uint32_t *val, *pos;
+    uint32_t *val, *word;
+    uint8_t *flag;
     uint64_t *hslot;
     uint8_t *hmatch;
+    uint32_t *sslot;
+    uint64_t *ck;
+    uint32_t *cv, *cx;
     uint64_t *sk;
-    uint32_t *tb, *idx;
+    uint32_t *tb, *ord;
     uint64_t *cnt;
     uint64_t *skey;
-    uint32_t *sval, *spos;
+    uint32_t *sval, *sidx;
+    uint32_t *rank;
 };
 
 __host__ __device__ inline size_t al256(size_t x) { return (x + 255) / 256 * 256; }
@@ -99,16 +136,22 @@ __host__ __device__ inline size_t scratch_layout(uint8_t *base, uint64_t N, BScr
     BScratch t;
     t.key = reinterpret_cast<uint64_t *>(take(N * 8));
     t.val = reinterpret_cast<uint32_t *>(take(N * 4));
-    t.pos = reinterpret_cast<uint32_t *>(take(N * 4));
+    t.word = reinterpret_cast<uint32_t *>(take(N * 4));
+    t.flag = take(N);
     t.hslot = reinterpret_cast<uint64_t *>(take(2 * N * 8));
     t.hmatch = take(2 * N);
+    t.sslot = reinterpret_cast<uint32_t *>(take(N * 4));
+    t.ck = reinterpret_cast<uint64_t *>(take(N * 8));
+    t.cv = reinterpret_cast<uint32_t *>(take(N * 4));
+    t.cx = reinterpret_cast<uint32_t *>(take(N * 4));
     t.sk = reinterpret_cast<uint64_t *>(take(N * 8));
     t.tb = reinterpret_cast<uint32_t *>(take(N * 4));
-    t.idx = reinterpret_cast<uint32_t *>(take(N * 4));
+    t.ord = reinterpret_cast<uint32_t *>(take(N * 4));
     t.cnt = reinterpret_cast<uint64_t *>(take(N * 8));
     t.skey = reinterpret_cast<uint64_t *>(take(N * 8));
     t.sval = reinterpret_cast<uint32_t *>(take(N * 4));
-    t.spos = reinterpret_cast<uint32_t *>(take(N * 4));
+    t.sidx = reinterpret_cast<uint32_t *>(take(N * 4));
+    t.rank = reinterpret_cast<uint32_t *>(take(N * 4));
     if (s) *s = t;
     return o;
 }
@@ -120,25 +163,20 @@ EMP_DEV T ldv(const T *p) {
     return __isShared(p) ? *p : __ldcg(p);
 }
 
-struct BView {
+struct Stage {  // the staged bucket
     uint64_t *key;
-    uint32_t *val, *pos;
-    uint64_t *hslot;
-    uint8_t *hmatch;
-    uint32_t hcap;
-    bool hpow2;
+    uint32_t *val, *word;
+    uint8_t *flag;
+};
+struct Cands {  // the matched entries
+    uint64_t *ck;
+    uint32_t *cv, *cx;
     uint64_t *sk;
-    uint32_t *tb, *idx;
+    uint32_t *tb, *ord;
     uint64_t *cnt;
     uint64_t *skey;
-    uint32_t *sval, *spos;
+    uint32_t *sval, *sidx;
 };
-
-EMP_DEV uint32_t slot_of(uint64_t key, const BView &v) {
-    const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 32);
-    return v.hpow2 ? (h & (v.hcap - 1)) : (h % v.hcap);
-}
-EMP_DEV uint32_t slot_next(uint32_t s, const BView &v) { return s + 1 == v.hcap ? 0 : s + 1; }
 
 // tie order of equal sort keys in the reference's stable sort: rid parity,
 // then read index (the regenerated tables list even rids, then odd rids)
@@ -150,80 +188,95 @@ EMP_DEV bool before(uint64_t ska, uint32_t tba, uint64_t skb, uint32_t tbb) {
     return ska < skb || (ska == skb && tba < tbb);
 }
 
-// ---------------------------------------------------------------- phase A
-EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const CoopCtl *ctl, uint8_t *smem) {
-    probe(ctl, iter, 2);
-    const uint32_t p = iter & 1;
-    const uint64_t n_in = vld(J.it[p].n_in);
-    // bins: (bucket, table), so a tile's piece of a bucket is its suffixes
-    // followed by its prefixes
-    const uint32_t nb = vld(J.it[p].nb), nbin = 2 * nb, stride = nbin + 1;
-    const int L = J.L, r = (int)vld(J.round);
-    const uint32_t pw1 = J.tables->pow1[L - r - 1], pw2 = J.tables->pow2[L - r - 1];
-    const uint32_t inv1 = J.tables->inv1, inv2 = J.tables->inv2;
-    const bool first = iter == 0;
-    const BktEntry *lin = J.lst[p];
-    BktEntry *lout = J.lst[p ^ 1];
+// Hash step of round r for one entry: key and cached word updated in place.
+struct StepArgs {
+    int L, r;
+    uint32_t pw1, pw2, inv1, inv2;
+    bool refill_all;  // the cached words are not valid (the launch's input list)
+    const uint32_t *seq2;
+    int wpr;
+};
+EMP_DEV StepArgs step_args(const BktJob &J, int r, bool refill_all) {
+    StepArgs a;
+    a.L = J.L;
+    a.r = r;
+    a.pw1 = J.tables->pow1[J.L - r - 1];
+    a.pw2 = J.tables->pow2[J.L - r - 1];
+    a.inv1 = J.tables->inv1;
+    a.inv2 = J.tables->inv2;
+    a.refill_all = refill_all;
+    a.seq2 = J.seq2;
+    a.wpr = J.wpr;
+    return a;
+}
+// column of the read's base that round r removes from the entry's key: a
+// forward suffix or an RC prefix walks the read forwards (column r), the
+// others backwards (column L-1-r)
+EMP_DEV int step_col(const StepArgs &a, uint32_t val, bool &inc) {
+    const uint32_t t = val >> 31, s = val & 1u;
+    inc = t == s;
+    return inc ? a.r : a.L - 1 - a.r;
+}
+EMP_DEV bool needs_refill(const StepArgs &a, uint32_t val) {
+    bool inc;
+    const int col = step_col(a, val, inc);
+    return a.refill_all || (col & 15) == (inc ? 0 : 15);
+}
+EMP_DEV uint32_t refill_word(const StepArgs &a, uint32_t val) {
+    bool inc;
+    const int col = step_col(a, val, inc);
+    return __ldg(a.seq2 + (uint64_t)((val & 0x7fffffffu) >> 1) * a.wpr + (col >> 4));
+}
+EMP_DEV uint64_t step_key(const StepArgs &a, uint64_t key, uint32_t val, uint32_t word) {
+    bool inc;
+    const int col = step_col(a, val, inc);
+    const uint32_t t = val >> 31, s = val & 1u;
+    const uint32_t b = ((word >> ((col & 15) * 2)) & 3u) ^ (s << 1);
+    return t == 0 ? next_sfx(key, b, a.pw1, a.pw2) : prev_pfx(key, b, a.inv1, a.inv2);
+}
+
+// ---------------------------------------------------------------- prologue
+// Tile k of the launch's input list -> round r0's list (tile k).
+EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
+    BktIter &I = J.it[0];
+    const uint64_t n_in = J.n_in;
+    const uint32_t nb = I.nb, nbin = 2 * nb, stride = nbin + 1;
+    const StepArgs a = step_args(J, J.r0, true);
     uint32_t *hist = reinterpret_cast<uint32_t *>(smem);
-    uint4 *stage = reinterpret_cast<uint4 *>(smem + kBktMaxBuckets * 8);
+    uint4 *stage = reinterpret_cast<uint4 *>(smem + 2 * kBktMaxBuckets * 4);
     for (uint32_t i = threadIdx.x; i < nbin; i += kT) hist[i] = 0;
     if (threadIdx.x == 0) sh.sfx = 0;
     __syncthreads();
     const uint64_t base = (uint64_t)k * kBktTile;
     uint64_t key[kC];
-    uint32_t val[kC], word[kC], rank[kC], bkt[kC];
+    uint32_t val[kC], word[kC], rank[kC], bin[kC];
     bool keep[kC];
 #pragma unroll
-    for (int c = 0; c < kC; ++c) {  // 1: the entries
+    for (int c = 0; c < kC; ++c) {  // the entries
         const uint64_t e = base + c * kT + threadIdx.x;
         keep[c] = e < n_in;
-        key[c] = 0;
-        val[c] = 0;
-        word[c] = 0;
-        if (keep[c]) {
-            if (first) {
-                key[c] = __ldcg(J.lk_in + e);
-                val[c] = __ldcg(J.lv_in + e);
-            } else {
-                const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(lin + e));
-                key[c] = (uint64_t)q.x | ((uint64_t)q.y << 32);
-                val[c] = q.z;
-                word[c] = q.w;
-            }
-        }
+        key[c] = keep[c] ? __ldcg(J.lk_in + e) : 0;
+        val[c] = keep[c] ? __ldcg(J.lv_in + e) : 0;
     }
 #pragma unroll
-    for (int c = 0; c < kC; ++c) {  // 2: used entries; bases not in the cached word
+    for (int c = 0; c < kC; ++c) {  // used before the launch; the base words
+        word[c] = 0;
         if (!keep[c]) continue;
-        const uint32_t v = val[c];
-        if (v == kBktTomb) {
-            keep[c] = false;
-            continue;
-        }
-        const uint32_t rid = v & 0x7fffffffu, t = v >> 31, s = rid & 1u, i = rid >> 1;
-        if (first) keep[c] = (t ? J.used_p[rid] : J.used_s[rid]) == 0;
-        const bool inc = t == s;  // fwd suffix / RC prefix walk the read forwards
-        const int col = inc ? r : L - 1 - r;
-        if (keep[c] && (first || (col & 15) == (inc ? 0 : 15)))
-            word[c] = __ldg(J.seq2 + (uint64_t)i * J.wpr + (col >> 4));
+        const uint32_t rid = val[c] & 0x7fffffffu;
+        keep[c] = ((val[c] >> 31) ? J.used_p[rid] : J.used_s[rid]) == 0;
+        if (keep[c]) word[c] = refill_word(a, val[c]);
     }
     uint32_t sfx = 0;
 #pragma unroll
-    for (int c = 0; c < kC; ++c) {  // 3: hash step, bucket, rank within the tile's bucket
+    for (int c = 0; c < kC; ++c) {  // hash step, bin, rank within the tile's bin
         if (!keep[c]) continue;
-        const uint32_t v = val[c], rid = v & 0x7fffffffu, t = v >> 31, s = rid & 1u;
-        const bool inc = t == s;
-        const int col = inc ? r : L - 1 - r;
-        const uint32_t b = ((word[c] >> ((col & 15) * 2)) & 3u) ^ (s << 1);
-        key[c] = t == 0 ? next_sfx(key[c], b, pw1, pw2) : prev_pfx(key[c], b, inv1, inv2);
-        bkt[c] = 2 * bkt_of(sort_key(key[c], v), nb) + t;
-        rank[c] = atomicAdd(&hist[bkt[c]], 1u);
-        sfx += t == 0;
+        key[c] = step_key(a, key[c], val[c], word[c]);
+        bin[c] = 2 * bkt_of(sort_key(key[c], val[c]), nb) + (val[c] >> 31);
+        rank[c] = atomicAdd(&hist[bin[c]], 1u);
+        sfx += (val[c] >> 31) == 0;
     }
     if (sfx) atomicAdd(&sh.sfx, sfx);
     __syncthreads();
-    probe(ctl, iter, 3);
-    // bin starts: exclusive scan of the nbin counters, each thread a run of them
     const uint32_t per = (nbin + kT - 1) / kT;
     const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
     const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
@@ -231,7 +284,7 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
     for (uint32_t b = b0; b < b1; ++b) run += hist[b];
     uint32_t kept;
     uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &kept);
-    uint32_t *orow = J.offs + (uint64_t)k * stride;
+    uint32_t *orow = J.offs[0] + (uint64_t)k * stride;
     for (uint32_t b = b0; b < b1; ++b) {
         const uint32_t h = hist[b];
         hist[b] = ex;
@@ -240,136 +293,54 @@ EMP_DEV void a_tile(BktJob &J, uint32_t k, uint32_t iter, BShared &sh, const Coo
     }
     if (threadIdx.x == 0) {
         orow[nbin] = kept;
-        const uint64_t ob = atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].n_out),
-                                      (unsigned long long)kept);
+        const uint64_t ob = atomicAdd(reinterpret_cast<unsigned long long *>(&I.n), (unsigned long long)kept);
         sh.base = ob;
-        J.tile_base[k] = ob;
-        if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].s_out), (unsigned long long)sh.sfx);
+        J.tile_base[0][k] = ob;
+        if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&I.s), (unsigned long long)sh.sfx);
     }
     __syncthreads();
-    probe(ctl, iter, 4);
 #pragma unroll
     for (int c = 0; c < kC; ++c) {
         if (!keep[c]) continue;
-        stage[hist[bkt[c]] + rank[c]] = make_uint4((uint32_t)key[c], (uint32_t)(key[c] >> 32), val[c], word[c]);
+        stage[hist[bin[c]] + rank[c]] = make_uint4((uint32_t)key[c], (uint32_t)(key[c] >> 32), val[c], word[c]);
     }
     __syncthreads();
-    uint4 *dst = reinterpret_cast<uint4 *>(lout + sh.base);
+    uint4 *dst = reinterpret_cast<uint4 *>(J.lst[0] + sh.base);
     for (uint32_t x = threadIdx.x; x < kept; x += kT) dst[x] = stage[x];
     __syncthreads();
-    probe(ctl, iter, 5);
 }
 
-// ---------------------------------------------------------------- phase B
-// exclusive scan of cnt[0..c) in place (u64), returns the total
-EMP_DEV uint64_t scan_counts(uint64_t *cnt, uint32_t c, BShared &sh) {
-    uint64_t run = 0;
-    for (uint32_t x0 = 0; x0 < c; x0 += kT) {
-        const uint32_t x = x0 + threadIdx.x;
-        const uint64_t v = x < c ? ldv(cnt + x) : 0;
-        uint64_t tot;
-        const uint64_t ex = block_exclusive_scan<kT, uint64_t>(v, sh.scan64, &tot);
-        if (x < c) cnt[x] = run + ex;
-        run += tot;
-        __syncthreads();
-    }
-    return run;
-}
-
-EMP_DEV void set_stage(BView &v, uint8_t *smem) {
-    v.key = reinterpret_cast<uint64_t *>(smem + kOffKey);
-    v.val = reinterpret_cast<uint32_t *>(smem + kOffVal);
-    v.pos = reinterpret_cast<uint32_t *>(smem + kOffPos);
-    v.hslot = nullptr;  // a staged bucket uses match_smem's own hash set
-    v.hmatch = nullptr;
-    v.hcap = 0;
-    v.hpow2 = true;
-}
-EMP_DEV void set_stage(BView &v, const BScratch &gs, uint64_t G, uint32_t total) {
-    v.key = gs.key + G;
-    v.val = gs.val + G;
-    v.pos = gs.pos + G;
-    v.hslot = gs.hslot + 2 * G;
-    v.hmatch = gs.hmatch + 2 * G;
-    v.hcap = 2 * total;
-    v.hpow2 = false;
-}
-
-EMP_DEV void put_entry(const BView &v, uint32_t d, const BktEntry *lst, uint64_t src) {
+// ---------------------------------------------------------------- gather
+EMP_DEV void put_entry(const Stage &v, uint32_t d, const BktEntry *lst, uint64_t src) {
     const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(lst + src));
     v.key[d] = (uint64_t)q.x | ((uint64_t)q.y << 32);
     v.val[d] = q.z;
-    v.pos[d] = (uint32_t)src;
+    v.word[d] = q.w;
+    v.flag[d] = 0;
 }
 
-// Gather bucket b: returns its size and sets up v (shared memory, or the
-// global scratch region at the bucket's place in bucket order).
-EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, const BktEntry *lst, BShared &sh,
-                        uint8_t *smem, BView &v, uint64_t &G, uint32_t &S) {
-    // segments q = 0 .. 2K-1: the suffix piece of tile q, then (q >= K) the
-    // prefix piece of tile q - K, so the bucket is staged suffixes first
-    const uint32_t *offs = J.offs;
+// Gather bucket b of a round whose list has K tiles partitioned into nb
+// buckets.  Pieces q = 0 .. 2K-1: the suffix piece of tile q, then (q >= K)
+// the prefix piece of tile q - K, so the bucket is staged suffixes first.
+// Returns the bucket's size; S = its suffixes, G = its position in bucket
+// order (entries of lower buckets), v = shared memory or the scratch region.
+// The gather for many pieces (more than kSegMax) or a bucket too big for
+// shared memory: 512 pieces at a time, a binary search per staged entry.
+EMP_COLD uint32_t gather_general(const BktJob &J, const BktEntry *lst, const uint32_t *offs, const uint64_t *tbase,
+                                 uint32_t K, uint32_t nb, uint32_t b, BShared &sh, uint8_t *smem, Stage &v,
+                                 uint32_t &S, uint64_t &G) {
     const uint32_t stride = 2 * nb + 1, Q = 2 * K;
-    auto seg = [&](uint32_t q, uint32_t &lo, uint32_t &cnt) -> uint64_t {  // returns the tile's base
+    uint8_t *reg = smem + kOffReg;
+    auto piece = [&](uint32_t q, uint32_t &lo, uint32_t &cnt) -> uint32_t {  // returns the tile
         const uint32_t k = q < K ? q : q - K, bin = 2 * b + (q < K ? 0u : 1u);
         lo = __ldcg(offs + (uint64_t)k * stride + bin);
         cnt = __ldcg(offs + (uint64_t)k * stride + bin + 1) - lo;
         return k;
     };
-    if (Q <= (uint32_t)kT) {
-        // fast path: one segment per thread; an owner table maps staged
-        // entries to segments
-        const uint32_t q = threadIdx.x;
-        uint32_t lo = 0, cnt = 0;
-        uint64_t start = 0;
-        if (q < Q) {
-            const uint64_t k = seg(q, lo, cnt);
-            start = __ldcg(J.tile_base + k) + lo;
-        }
-        uint32_t total;
-        const uint32_t ex = block_exclusive_scan<kT, uint32_t>(cnt, sh.scan32, &total);
-        if (q == K) sh.tile = ex;  // suffixes: the segments before the first prefix piece
-        if (total <= kBStage) {
-            G = 0;
-            set_stage(v, smem);
-            uint16_t *owner = reinterpret_cast<uint16_t *>(smem + kOffHash);
-            sh.seg_start[threadIdx.x] = start;
-            sh.seg_pos[threadIdx.x] = ex;
-            for (uint32_t x = ex; x < ex + cnt; ++x) owner[x] = (uint16_t)q;
-            __syncthreads();
-            S = K ? sh.tile : 0u;
-            constexpr int U = 4;
-            for (uint32_t x0 = 0; x0 < total; x0 += U * kT) {
-                uint4 e[U];
-                uint64_t src[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const uint32_t x = x0 + u * kT + threadIdx.x;
-                    if (x < total) {
-                        const uint32_t o = owner[x];
-                        src[u] = sh.seg_start[o] + (x - sh.seg_pos[o]);
-                        e[u] = __ldcg(reinterpret_cast<const uint4 *>(lst + src[u]));
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const uint32_t x = x0 + u * kT + threadIdx.x;
-                    if (x < total) {
-                        v.key[x] = (uint64_t)e[u].x | ((uint64_t)e[u].y << 32);
-                        v.val[x] = e[u].z;
-                        v.pos[x] = (uint32_t)src[u];
-                    }
-                }
-            }
-            __syncthreads();
-            return total;
-        }
-    }
-    // general path: many tiles, or a bucket too big for shared memory
     uint64_t tot = 0, tsfx = 0, gpre = 0;
     for (uint32_t q = threadIdx.x; q < Q; q += kT) {
         uint32_t lo, cnt;
-        seg(q, lo, cnt);
+        piece(q, lo, cnt);
         tot += cnt;
         if (q < K) {
             tsfx += cnt;
@@ -384,35 +355,42 @@ EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, co
     S = (uint32_t)t2;
     G = t3;
     if (total <= kBStage) {
-        G = 0;
-        set_stage(v, smem);
+        v.key = reinterpret_cast<uint64_t *>(smem + kOffKey);
+        v.val = reinterpret_cast<uint32_t *>(smem + kOffVal);
+        v.word = reinterpret_cast<uint32_t *>(smem + kOffWord);
+        v.flag = smem + kOffFlag;
     } else {
         BScratch gs;
         scratch_layout(J.scratch, J.n_max, &gs);
-        set_stage(v, gs, G, total);
+        v.key = gs.key + G;
+        v.val = gs.val + G;
+        v.word = gs.word + G;
+        v.flag = gs.flag + G;
     }
+    uint64_t *seg_start = reinterpret_cast<uint64_t *>(reg + kGSegStart);
+    uint32_t *seg_pos = reinterpret_cast<uint32_t *>(reg + kGSegPos);
     uint32_t gathered = 0;
     for (uint32_t q0 = 0; q0 < Q && total; q0 += kT) {
         const uint32_t q = q0 + threadIdx.x;
         uint32_t lo = 0, cnt = 0;
         uint64_t start = 0;
         if (q < Q) {
-            const uint64_t k = seg(q, lo, cnt);
-            start = __ldcg(J.tile_base + k) + lo;
+            const uint32_t k = piece(q, lo, cnt);
+            start = __ldcg(tbase + k) + lo;
         }
         uint32_t ctot;
         const uint32_t ex = block_exclusive_scan<kT, uint32_t>(cnt, sh.scan32, &ctot);
-        sh.seg_start[threadIdx.x] = start;
-        sh.seg_pos[threadIdx.x] = ex;
+        seg_start[threadIdx.x] = start;
+        seg_pos[threadIdx.x] = ex;
         __syncthreads();
         for (uint32_t x = threadIdx.x; x < ctot; x += kT) {
-            uint32_t lo2 = 0, hi = kT;  // last segment with seg_pos <= x
+            uint32_t lo2 = 0, hi = kT;  // last piece with seg_pos <= x
             while (hi - lo2 > 1) {
                 const uint32_t m = (lo2 + hi) >> 1;
-                if (sh.seg_pos[m] <= x) lo2 = m;
+                if (seg_pos[m] <= x) lo2 = m;
                 else hi = m;
             }
-            put_entry(v, gathered + x, lst, sh.seg_start[lo2] + (x - sh.seg_pos[lo2]));
+            put_entry(v, gathered + x, lst, seg_start[lo2] + (x - seg_pos[lo2]));
         }
         gathered += ctot;
         __syncthreads();
@@ -420,7 +398,99 @@ EMP_DEV uint32_t gather(const BktJob &J, uint32_t b, uint32_t nb, uint32_t K, co
     return total;
 }
 
-// ---- shared-memory fast path of a bucket (the common case)
+EMP_DEV uint32_t gather(const BktJob &J, const BktEntry *lst, const uint32_t *offs, const uint64_t *tbase,
+                        uint32_t K, uint32_t nb, uint32_t b, BShared &sh, uint8_t *smem, Stage &v, uint32_t &S,
+                        uint64_t &G) {
+    const uint32_t stride = 2 * nb + 1, Q = 2 * K;
+    uint8_t *reg = smem + kOffReg;
+    auto piece = [&](uint32_t q, uint32_t &lo, uint32_t &cnt) -> uint32_t {  // returns the tile
+        const uint32_t k = q < K ? q : q - K, bin = 2 * b + (q < K ? 0u : 1u);
+        lo = __ldcg(offs + (uint64_t)k * stride + bin);
+        cnt = __ldcg(offs + (uint64_t)k * stride + bin + 1) - lo;
+        return k;
+    };
+    if (Q <= kSegMax) {
+        // each thread takes up to 8 consecutive pieces; an owner table maps
+        // staged entries to pieces
+        uint64_t *seg_start = reinterpret_cast<uint64_t *>(reg + kGSegStart);
+        uint32_t *seg_pos = reinterpret_cast<uint32_t *>(reg + kGSegPos);
+        uint16_t *owner = reinterpret_cast<uint16_t *>(reg + kGOwner);
+        constexpr int kPer = kSegMax / kT;
+        const uint32_t per = (Q + kT - 1) / kT;  // pieces of each thread, 1..kPer
+        const uint32_t q0 = threadIdx.x * per;
+        uint32_t cnt[kPer];
+        uint32_t run = 0;
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            const uint32_t q = q0 + i;
+            cnt[i] = 0;
+            if (i < (int)per && q < Q) {
+                uint32_t lo;
+                const uint32_t k = piece(q, lo, cnt[i]);
+                seg_start[q] = __ldcg(tbase + k) + lo;
+            }
+            run += cnt[i];
+        }
+        uint32_t total;
+        uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &total);
+        sprobe(sh, 11);
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            const uint32_t q = q0 + i;
+            if (i < (int)per && q < Q) {
+                seg_pos[q] = ex;
+                if (q == K) sh.cnt = ex;  // suffixes: the pieces before the first prefix piece
+            }
+            ex += cnt[i];
+        }
+        if (threadIdx.x == 0) seg_pos[Q] = total;
+        if (total <= kBStage) {
+            G = 0;
+            v.key = reinterpret_cast<uint64_t *>(smem + kOffKey);
+            v.val = reinterpret_cast<uint32_t *>(smem + kOffVal);
+            v.word = reinterpret_cast<uint32_t *>(smem + kOffWord);
+            v.flag = smem + kOffFlag;
+            __syncthreads();
+            // owner table: one warp per piece
+            const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            for (uint32_t q = warp; q < Q; q += kT / 32) {
+                const uint32_t lo = seg_pos[q], hi = seg_pos[q + 1];
+                for (uint32_t x = lo + lane; x < hi; x += 32) owner[x] = (uint16_t)q;
+            }
+            __syncthreads();
+            S = sh.cnt;
+            sprobe(sh, 12);
+            constexpr int U = 4;
+            for (uint32_t x0 = 0; x0 < total; x0 += U * kT) {
+                uint4 e[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t x = x0 + u * kT + threadIdx.x;
+                    if (x < total) {
+                        const uint32_t o = owner[x];
+                        e[u] = __ldcg(reinterpret_cast<const uint4 *>(lst + seg_start[o] + (x - seg_pos[o])));
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t x = x0 + u * kT + threadIdx.x;
+                    if (x < total) {
+                        v.key[x] = (uint64_t)e[u].x | ((uint64_t)e[u].y << 32);
+                        v.val[x] = e[u].z;
+                        v.word[x] = e[u].w;
+                        v.flag[x] = 0;
+                    }
+                }
+            }
+            __syncthreads();
+            return total;
+        }
+        __syncthreads();
+    }
+    return gather_general(J, lst, offs, tbase, K, nb, b, sh, smem, v, S, G);
+}
+
+// ---------------------------------------------------------------- matching
 // Hash slots are u32: bit 31 matched, bits 13-30 an 18-bit tag of the key,
 // bits 0-12 the staged index of a suffix with that key (keys compared in full
 // through it).  A tag of all ones is never used, so kSlotEmpty is no slot.
@@ -438,17 +508,18 @@ EMP_DEV bool slot_holds(uint32_t w, uint32_t tag, uint64_t k, const uint64_t *ke
     return ((w >> 13) & 0x3ffffu) == tag && key[w & 8191u] == k;
 }
 
-// Mark (kFlag in pos) every staged entry whose key occurs in both tables.
-// The bucket is staged suffixes first: [0, S) suffixes, [S, total) prefixes.
-// Each thread works on kU entries at once so their shared-memory round trips
-// overlap; a collision falls back to a probe loop.
-EMP_DEV void match_smem(uint32_t total, uint32_t S, uint8_t *smem) {
+// Flag kMatched on every staged entry whose key occurs in both tables; the
+// bucket is staged in shared memory, suffixes [0, S), prefixes [S, total).
+// Each thread works on kU entries at once so that their shared-memory round
+// trips overlap; a collision falls back to a probe loop.
+EMP_COLD void match_smem(uint32_t total, uint32_t S, uint8_t *smem) {
     constexpr int kU = 4;
     const uint64_t *key = reinterpret_cast<const uint64_t *>(smem + kOffKey);
-    uint32_t *pos = reinterpret_cast<uint32_t *>(smem + kOffPos);
-    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kOffHash);
-    uint16_t *sslot = reinterpret_cast<uint16_t *>(smem + kOffHash + kBHash * 4);
-    for (uint32_t s = threadIdx.x; s < kBHash; s += kT) slot[s] = kSlotEmpty;
+    uint8_t *flag = smem + kOffFlag;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kOffReg + kHSlot);
+    uint16_t *sslot = reinterpret_cast<uint16_t *>(smem + kOffReg + kHSuffixSlot);
+    for (uint32_t s = threadIdx.x; s < kBHash / 4; s += kT)
+        reinterpret_cast<uint4 *>(slot)[s] = make_uint4(kSlotEmpty, kSlotEmpty, kSlotEmpty, kSlotEmpty);
     __syncthreads();
     for (uint32_t x0 = 0; x0 < S; x0 += kU * kT) {  // suffixes: insert
         uint64_t k[kU];
@@ -496,7 +567,7 @@ EMP_DEV void match_smem(uint32_t total, uint32_t S, uint8_t *smem) {
             for (uint32_t probes = 1; ww != kSlotEmpty && probes < kBHash; ++probes) {
                 if (slot_holds(ww, tag[u], k[u], key)) {
                     if (!(ww & kSlotMatched)) atomicOr(slot + sl, kSlotMatched);
-                    pos[x] |= kFlag;
+                    flag[x] = kMatched;
                     break;
                 }
                 sl = (sl + 1) & (kBHash - 1);
@@ -506,77 +577,234 @@ EMP_DEV void match_smem(uint32_t total, uint32_t S, uint8_t *smem) {
     }
     __syncthreads();
     for (uint32_t x = threadIdx.x; x < S; x += kT)  // suffixes: matched?
-        if (slot[sslot[x]] & kSlotMatched) pos[x] |= kFlag;
+        if (slot[sslot[x]] & kSlotMatched) flag[x] = kMatched;
     __syncthreads();
 }
 
-// The generic matcher (global scratch, or any view): same marks.
-EMP_DEV void match_view(const BView &v, uint32_t total) {
-    for (uint32_t s = threadIdx.x; s < v.hcap; s += kT) {
-        v.hslot[s] = kEmptySlot;
-        v.hmatch[s] = 0;
+// Cheaper matcher for the usual bucket, where few entries match: a 2-bit
+// Bloom filter of the suffix keys (128K bits) passes a few prefixes; a second
+// filter of those prefixes' keys passes a few suffixes; the two short lists
+// are compared in full.  No entry that matches is filtered out, so the flags
+// equal match_smem's.  Returns false (flags untouched) when the lists would
+// be long; the caller then uses match_smem.
+constexpr uint32_t kFilterWords = 4096;  // 128K bits per filter
+constexpr uint32_t kListMax = 1024;
+constexpr size_t kFBm1 = 0, kFBm2 = kFilterWords * 4, kFPl = 2 * kFilterWords * 4, kFSl = kFPl + kListMax * 2;
+static_assert(kFSl + kListMax * 2 <= kRegion, "filters and lists fit the region");
+
+EMP_DEV void filter_bits(uint64_t key, uint32_t &b1, uint32_t &b2) {
+    const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 32);
+    b1 = h & (kFilterWords * 32 - 1);
+    b2 = (h >> 15) & (kFilterWords * 32 - 1);
+}
+EMP_DEV bool filter_has(const uint32_t *bm, uint32_t b1, uint32_t b2) {
+    return ((bm[b1 >> 5] >> (b1 & 31)) & (bm[b2 >> 5] >> (b2 & 31)) & 1u) != 0;
+}
+// warp-aggregated append of x to list (count in *n); false once it is full
+EMP_DEV void list_push(bool f, uint32_t x, uint16_t *list, uint32_t *n) {
+    const uint32_t m = __ballot_sync(0xffffffffu, f);
+    if (!m) return;
+    const uint32_t lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(n, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const uint32_t d = base + __popc(m & lanemask_lt_u32());
+    if (f && d < kListMax) list[d] = (uint16_t)x;
+}
+
+EMP_DEV bool match_filter(uint32_t total, uint32_t S, uint8_t *smem, BShared &sh) {
+    const uint64_t *key = reinterpret_cast<const uint64_t *>(smem + kOffKey);
+    uint8_t *flag = smem + kOffFlag;
+    uint8_t *reg = smem + kOffReg;
+    uint32_t *bm1 = reinterpret_cast<uint32_t *>(reg + kFBm1);
+    uint32_t *bm2 = reinterpret_cast<uint32_t *>(reg + kFBm2);
+    uint16_t *pl = reinterpret_cast<uint16_t *>(reg + kFPl);
+    uint16_t *sl = reinterpret_cast<uint16_t *>(reg + kFSl);
+    for (uint32_t i = threadIdx.x; i < 2 * kFilterWords / 4; i += kT)
+        reinterpret_cast<uint4 *>(bm1)[i] = make_uint4(0, 0, 0, 0);  // bm1 and bm2
+    if (threadIdx.x == 0) {
+        sh.cnt = 0;
+        sh.tile = 0;
     }
     __syncthreads();
-    for (uint32_t x = threadIdx.x; x < total; x += kT) {
-        if (ldv(v.val + x) >> 31) continue;
+    for (uint32_t x = threadIdx.x; x < S; x += kT) {  // suffix keys into filter 1
+        uint32_t b1, b2;
+        filter_bits(key[x], b1, b2);
+        atomicOr(bm1 + (b1 >> 5), 1u << (b1 & 31));
+        atomicOr(bm1 + (b2 >> 5), 1u << (b2 & 31));
+    }
+    __syncthreads();
+    for (uint32_t x0 = S; x0 < total; x0 += kT) {  // prefixes through filter 1, their keys into filter 2
+        const uint32_t x = x0 + threadIdx.x;
+        bool f = false;
+        if (x < total) {
+            uint32_t b1, b2;
+            filter_bits(key[x], b1, b2);
+            f = filter_has(bm1, b1, b2);
+            if (f) {
+                atomicOr(bm2 + (b1 >> 5), 1u << (b1 & 31));
+                atomicOr(bm2 + (b2 >> 5), 1u << (b2 & 31));
+            }
+        }
+        list_push(f, x, pl, &sh.cnt);
+    }
+    __syncthreads();
+    const uint32_t np = sh.cnt;
+    if (np > kListMax) return false;
+    for (uint32_t x0 = 0; x0 < S; x0 += kT) {  // suffixes through filter 2
+        const uint32_t x = x0 + threadIdx.x;
+        bool f = false;
+        if (x < S) {
+            uint32_t b1, b2;
+            filter_bits(key[x], b1, b2);
+            f = filter_has(bm2, b1, b2);
+        }
+        list_push(f, x, sl, &sh.tile);
+    }
+    __syncthreads();
+    const uint32_t ns = sh.tile;
+    if (ns > kListMax) return false;
+    for (uint32_t i = threadIdx.x; i < np; i += kT) {  // the two lists in full
+        const uint32_t xp = pl[i];
+        const uint64_t kp = key[xp];
+        bool hit = false;
+        for (uint32_t j = 0; j < ns; ++j) {
+            const uint32_t xs = sl[j];
+            if (key[xs] == kp) {
+                flag[xs] = kMatched;
+                hit = true;
+            }
+        }
+        if (hit) flag[xp] = kMatched;
+    }
+    __syncthreads();
+    return true;
+}
+
+// The same for a bucket staged in global scratch: open addressing on the full
+// keys, 2 x total slots, in the bucket's scratch region.
+EMP_COLD void match_global(const Stage &v, uint32_t total, uint32_t S, const BScratch &gs, uint64_t G) {
+    uint64_t *hslot = gs.hslot + 2 * G;
+    uint8_t *hmatch = gs.hmatch + 2 * G;
+    uint32_t *sslot = gs.sslot + G;
+    const uint32_t hcap = 2 * total;
+    auto slot_of = [&](uint64_t key) -> uint32_t {
+        return (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 32) % hcap;
+    };
+    for (uint32_t s = threadIdx.x; s < hcap; s += kT) {
+        hslot[s] = kEmptySlot;
+        hmatch[s] = 0;
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < S; x += kT) {
         const uint64_t key = ldv(v.key + x);
-        uint32_t s = slot_of(key, v);
-        for (uint32_t probes = 0; probes < v.hcap; ++probes) {
-            const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long *>(v.hslot + s),
+        uint32_t s = slot_of(key);
+        for (uint32_t probes = 0; probes < hcap; ++probes) {
+            const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long *>(hslot + s),
                                             (unsigned long long)kEmptySlot, (unsigned long long)key);
             if (prev == kEmptySlot || prev == key) break;
-            s = slot_next(s, v);
+            s = s + 1 == hcap ? 0 : s + 1;
+        }
+        sslot[x] = s;
+    }
+    __syncthreads();
+    for (uint32_t x = S + threadIdx.x; x < total; x += kT) {
+        const uint64_t key = ldv(v.key + x);
+        uint32_t s = slot_of(key);
+        for (uint32_t probes = 0; probes < hcap; ++probes) {
+            const uint64_t h = ldv(hslot + s);
+            if (h == kEmptySlot) break;
+            if (h == key) {
+                hmatch[s] = 1;
+                v.flag[x] = kMatched;
+                break;
+            }
+            s = s + 1 == hcap ? 0 : s + 1;
         }
     }
     __syncthreads();
-    for (uint32_t x = threadIdx.x; x < total; x += kT) {  // prefixes
-        if (!(ldv(v.val + x) >> 31)) continue;
-        const uint64_t key = ldv(v.key + x);
-        uint32_t s = slot_of(key, v);
-        for (uint32_t probes = 0; probes < v.hcap; ++probes) {
-            const uint64_t h = ldv(v.hslot + s);
-            if (h == kEmptySlot) break;
-            if (h == key) {
-                v.hmatch[s] = 1;
-                v.pos[x] = ldv(v.pos + x) | kFlag;
-                break;
-            }
-            s = slot_next(s, v);
-        }
-    }
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < total; x += kT) {  // suffixes
-        if (ldv(v.val + x) >> 31) continue;
-        const uint64_t key = ldv(v.key + x);
-        uint32_t s = slot_of(key, v);
-        for (uint32_t probes = 0; probes < v.hcap; ++probes) {
-            const uint64_t h = ldv(v.hslot + s);
-            if (h == key) {
-                if (ldv(v.hmatch + s)) v.pos[x] = ldv(v.pos + x) | kFlag;
-                break;
-            }
-            if (h == kEmptySlot) break;
-            s = slot_next(s, v);
-        }
-    }
+    for (uint32_t x = threadIdx.x; x < S; x += kT)
+        if (ldv(hmatch + ldv(sslot + x))) v.flag[x] = kMatched;
     __syncthreads();
 }
 
-// Arrays of the matched entries: compacted (key, val, list position), their
-// sort and tie keys, chunk order, edge counts, and the sorted copy.
-struct CandView {
-    uint64_t *ck;
-    uint32_t *cv, *cp;
-    uint64_t *sk;
-    uint32_t *tb, *idx;
-    uint64_t *cnt;
-    uint64_t *skey;
-    uint32_t *sval, *spos;
-};
+// ---------------------------------------------------------------- sort + join
+// exclusive scan of cnt[0..c) in place (u64), returns the total
+EMP_DEV uint64_t scan_counts(uint64_t *cnt, uint32_t c, BShared &sh) {
+    uint64_t run = 0;
+    for (uint32_t x0 = 0; x0 < c; x0 += kT) {
+        const uint32_t x = x0 + threadIdx.x;
+        const uint64_t v = x < c ? ldv(cnt + x) : 0;
+        uint64_t tot;
+        const uint64_t ex = block_exclusive_scan<kT, uint64_t>(v, sh.scan64, &tot);
+        if (x < c) cnt[x] = run + ex;
+        run += tot;
+        __syncthreads();
+    }
+    return run;
+}
 
-// Sort the c matched entries by (sort key, tie) and count each suffix's edges;
-// returns the bucket's edge count (cnt then holds exclusive edge offsets).
-EMP_DEV uint64_t sort_and_count(const CandView &w, uint32_t c, BShared &sh) {
+// Rank the c matched entries by (sort key, tie) into skey/sval/sidx and count
+// each suffix's edges; returns the bucket's edge count (cnt then holds
+// exclusive edge offsets).  Chunks of 512 are ranked by comparing all pairs,
+// then each entry adds, per other chunk, the entries before it (binary
+// search), so any c works.
+EMP_DEV uint64_t join_count(const Cands &w, uint32_t c, BShared &sh);
+
+// Sort of up to kBCand matched entries of bucket b in shared memory: a
+// counting pass into 1024 finer bins (the same top-24-bit field of the sort
+// key, scaled to nb * 1024 bins, so bin order is key order), then each entry
+// ranked among the members of its bin.  Returns the bucket's edge count.
+constexpr uint32_t kFine = 1024;
+constexpr size_t kCFine = kCSIdx + kBCand * 4;  // u32 [kFine + 1] bin starts
+static_assert(kCFine + (kFine + 4) * 4 <= kRegion, "fine bins fit the region");
+
+EMP_DEV uint64_t sort_fine(const Cands &w, uint32_t c, uint32_t b, uint32_t nb, uint8_t *smem, BShared &sh) {
+    uint32_t *hist = reinterpret_cast<uint32_t *>(smem + kOffReg + kCFine);
+    uint32_t *tmp = reinterpret_cast<uint32_t *>(w.cnt);  // staged order, before the edge counts
+    const uint64_t scale = (uint64_t)nb * kFine, lo_bin = (uint64_t)b * kFine;
+    for (uint32_t i = threadIdx.x; i <= kFine; i += kT) hist[i] = 0;
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < c; x += kT) {
+        const uint32_t val = w.cv[x];
+        const uint64_t sk = sort_key(w.ck[x], val);
+        w.sk[x] = sk;
+        w.tb[x] = tie_of(val);
+        const uint32_t f = (uint32_t)((((sk >> 35) * scale) >> 24) - lo_bin);
+        w.ord[x] = (f << 16) | atomicAdd(&hist[f], 1u);
+    }
+    __syncthreads();
+    {  // bin starts: two bins per thread
+        const uint32_t f0 = 2 * threadIdx.x;
+        const uint32_t a0 = hist[f0], a1 = hist[f0 + 1];
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan<kT, uint32_t>(a0 + a1, sh.scan32, &tot);
+        hist[f0] = ex;
+        hist[f0 + 1] = ex + a0;
+        if (threadIdx.x == 0) hist[kFine] = tot;
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < c; x += kT) tmp[hist[w.ord[x] >> 16] + (w.ord[x] & 0xffffu)] = x;
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < c; q += kT) {
+        const uint32_t x = tmp[q], f = w.ord[x] >> 16;
+        const uint32_t lo = hist[f], hi = hist[f + 1];
+        const uint64_t skx = w.sk[x];
+        const uint32_t tbx = w.tb[x];
+        uint32_t r = lo;
+        for (uint32_t y = lo; y < hi; ++y) {
+            const uint32_t z = tmp[y];
+            r += before(w.sk[z], w.tb[z], skx, tbx);
+        }
+        w.skey[r] = w.ck[x];
+        w.sval[r] = w.cv[x];
+        w.sidx[r] = w.cx[x];
+    }
+    __syncthreads();
+    return join_count(w, c, sh);
+}
+
+EMP_COLD uint64_t sort_and_count(const Cands &w, uint32_t c, BShared &sh) {
     for (uint32_t x = threadIdx.x; x < c; x += kT) {
         const uint32_t val = ldv(w.cv + x);
         w.sk[x] = sort_key(ldv(w.ck + x), val);
@@ -584,7 +812,7 @@ EMP_DEV uint64_t sort_and_count(const CandView &w, uint32_t c, BShared &sh) {
     }
     __syncthreads();
     const uint32_t nch = (c + kT - 1) / kT;
-    for (uint32_t q = 0; q < nch; ++q) {  // order within each 512-entry chunk
+    for (uint32_t q = 0; q < nch; ++q) {
         const uint32_t lo = q * kT, m = c - lo < kT ? c - lo : kT;
         if (threadIdx.x < m) {
             const uint32_t x = lo + threadIdx.x;
@@ -592,12 +820,12 @@ EMP_DEV uint64_t sort_and_count(const CandView &w, uint32_t c, BShared &sh) {
             const uint32_t tbx = ldv(w.tb + x);
             uint32_t rk = 0;
             for (uint32_t u = 0; u < m; ++u) rk += before(ldv(w.sk + lo + u), ldv(w.tb + lo + u), skx, tbx);
-            w.idx[lo + rk] = x;
+            w.ord[lo + rk] = x;
             w.cnt[x] = rk;
         }
     }
     __syncthreads();
-    for (uint32_t x = threadIdx.x; x < c; x += kT) {  // rank among all chunks
+    for (uint32_t x = threadIdx.x; x < c; x += kT) {
         const uint64_t skx = ldv(w.sk + x);
         const uint32_t tbx = ldv(w.tb + x);
         const uint32_t qx = x / kT;
@@ -605,10 +833,10 @@ EMP_DEV uint64_t sort_and_count(const CandView &w, uint32_t c, BShared &sh) {
         for (uint32_t q = 0; q < nch; ++q) {
             if (q == qx) continue;
             const uint32_t lo = q * kT, m = c - lo < kT ? c - lo : kT;
-            uint32_t a = 0, z = m;  // entries of chunk q before x
+            uint32_t a = 0, z = m;
             while (a < z) {
                 const uint32_t mid = (a + z) >> 1;
-                const uint32_t y = ldv(w.idx + lo + mid);
+                const uint32_t y = ldv(w.ord + lo + mid);
                 if (before(ldv(w.sk + y), ldv(w.tb + y), skx, tbx)) a = mid + 1;
                 else z = mid;
             }
@@ -616,10 +844,16 @@ EMP_DEV uint64_t sort_and_count(const CandView &w, uint32_t c, BShared &sh) {
         }
         w.skey[rk] = ldv(w.ck + x);
         w.sval[rk] = ldv(w.cv + x);
-        w.spos[rk] = ldv(w.cp + x);
+        w.sidx[rk] = ldv(w.cx + x);
     }
     __syncthreads();
-    // join: per suffix, the prefixes of its equal-key run from other reads
+    return join_count(w, c, sh);
+}
+
+// Per suffix of the sorted matched entries: the prefixes of its equal-key run
+// from other reads.  Returns the bucket's edge count; cnt then holds each
+// suffix's exclusive edge offset.
+EMP_DEV uint64_t join_count(const Cands &w, uint32_t c, BShared &sh) {
     for (uint32_t i = threadIdx.x; i < c; i += kT) {
         uint64_t cc = 0;
         const uint32_t vi = ldv(w.sval + i);
@@ -637,123 +871,358 @@ EMP_DEV uint64_t sort_and_count(const CandView &w, uint32_t c, BShared &sh) {
     return scan_counts(w.cnt, c, sh);
 }
 
-EMP_DEV void b_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const CoopCtl *ctl, uint8_t *smem) {
-    probe(ctl, iter, 11);
-    const uint32_t p = iter & 1;
-    const uint64_t n_in = vld(J.it[p].n_in);
-    const uint32_t nb = vld(J.it[p].nb);
-    const uint32_t K = (uint32_t)bkt_tiles(n_in);
-    BktEntry *lst = J.lst[p ^ 1];
-    BView v;
-    uint64_t G = 0;
-    uint32_t S = 0;
-    const uint32_t total = gather(J, b, nb, K, lst, sh, smem, v, G, S);
-    const bool in_smem = total <= kBStage;
-    probe(ctl, iter, 13);
-    // ---- matches: entries whose key is in both tables get kFlag in pos
-    if (total) {
-        if (in_smem) match_smem(total, S, smem);
-        else match_view(v, total);
+// ---------------------------------------------------------------- next round
+// Drop the used entries of the staged bucket, apply round a.r's hash step to
+// the rest and write them as tile `tile` of the next list, partitioned into
+// nb buckets.  Returns nothing; counts go to the next list's BktIter.
+// Bin starts of the next tile (in place in hist), its offs row, its place in
+// the next list; returns the kept count.
+EMP_DEV uint32_t close_tile(uint32_t *hist, uint32_t nbin, uint32_t tile, uint32_t *offs, uint64_t *tbase,
+                            BktIter &nx, BShared &sh) {
+    const uint32_t per = (nbin + kT - 1) / kT;
+    const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
+    const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
+    uint32_t run = 0;
+    for (uint32_t b = b0; b < b1; ++b) run += hist[b];
+    uint32_t kept;
+    uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &kept);
+    uint32_t *orow = offs + (uint64_t)tile * (nbin + 1);
+    for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t h = hist[b];
+        hist[b] = ex;
+        orow[b] = ex;
+        ex += h;
     }
-    probe(ctl, iter, 14);
-    uint32_t c = 0;
+    if (threadIdx.x == 0) {
+        orow[nbin] = kept;
+        const uint64_t ob = kept ? atomicAdd(reinterpret_cast<unsigned long long *>(&nx.n), (unsigned long long)kept)
+                                 : 0ull;
+        sh.base = ob;
+        tbase[tile] = ob;
+        if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.s), (unsigned long long)sh.sfx);
+    }
+    __syncthreads();
+    return kept;
+}
+
+// write_next for a bucket staged in shared memory: the same steps on the
+// shared arrays, the tile permuted in shared memory and written in order.
+EMP_DEV void write_next_smem(uint32_t total, const StepArgs &a, uint32_t nb, uint32_t tile, BktEntry *lout,
+                             uint32_t *offs, uint64_t *tbase, BktIter &nx, BShared &sh, uint8_t *smem) {
+    uint64_t *key = reinterpret_cast<uint64_t *>(smem + kOffKey);
+    uint32_t *val = reinterpret_cast<uint32_t *>(smem + kOffVal);
+    uint32_t *word = reinterpret_cast<uint32_t *>(smem + kOffWord);
+    const uint8_t *flag = smem + kOffFlag;
+    uint8_t *reg = smem + kOffReg;
+    uint32_t *hist = reinterpret_cast<uint32_t *>(reg + kPHist);
+    uint16_t *inv = reinterpret_cast<uint16_t *>(reg + kPInv);
+    uint16_t *rank16 = reinterpret_cast<uint16_t *>(reg + kPRank);
+    uint16_t *bin16 = reinterpret_cast<uint16_t *>(reg + kPBin);
+    const uint32_t nbin = 2 * nb;
+    for (uint32_t i = threadIdx.x; i < nbin; i += kT) hist[i] = 0;
+    if (threadIdx.x == 0) sh.sfx = 0;
+    __syncthreads();
+    uint32_t sfx = 0;
+    constexpr int kU = 4;  // entries per thread in flight
+    for (uint32_t x0 = 0; x0 < total; x0 += kU * kT) {
+        bool act[kU];
+        uint32_t vl[kU], wd[kU];
+        uint64_t ky[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            act[u] = x < total && !(flag[x] & kUsed);
+            if (act[u]) {
+                vl[u] = val[x];
+                wd[u] = word[x];
+                ky[u] = key[x];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            if (act[u] && needs_refill(a, vl[u])) wd[u] = refill_word(a, vl[u]);
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if (!act[u]) continue;
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            ky[u] = step_key(a, ky[u], vl[u], wd[u]);
+            key[x] = ky[u];
+            word[x] = wd[u];
+            const uint32_t bn = 2 * bkt_of(sort_key(ky[u], vl[u]), nb) + (vl[u] >> 31);
+            rank16[x] = (uint16_t)atomicAdd(&hist[bn], 1u);
+            bin16[x] = (uint16_t)bn;
+            sfx += (vl[u] >> 31) == 0;
+        }
+    }
+    if (sfx) atomicAdd(&sh.sfx, sfx);
+    __syncthreads();
+    sprobe(sh, 13);
+    const uint32_t kept = close_tile(hist, nbin, tile, offs, tbase, nx, sh);
+    sprobe(sh, 14);
+    for (uint32_t x = threadIdx.x; x < total; x += kT)
+        if (!(flag[x] & kUsed)) inv[hist[bin16[x]] + rank16[x]] = (uint16_t)x;
+    __syncthreads();
+    sprobe(sh, 15);
+    uint4 *dst = reinterpret_cast<uint4 *>(lout + sh.base);
+    for (uint32_t d = threadIdx.x; d < kept; d += kT) {
+        const uint32_t x = inv[d];
+        const uint64_t k = key[x];
+        dst[d] = make_uint4((uint32_t)k, (uint32_t)(k >> 32), val[x], word[x]);
+    }
+    __syncthreads();
+}
+
+EMP_COLD void write_next(BktJob &J, const Stage &v, uint32_t total, bool in_smem, const StepArgs &a, uint32_t nb,
+                         uint32_t tile, BktEntry *lout, uint32_t *offs, uint64_t *tbase, BktIter &nx, BShared &sh,
+                         uint8_t *smem, const BScratch &gs, uint64_t G) {
+    uint8_t *reg = smem + kOffReg;
+    uint32_t *hist = reinterpret_cast<uint32_t *>(reg + kPHist);
+    uint16_t *inv = reinterpret_cast<uint16_t *>(reg + kPInv);
+    uint16_t *rank16 = reinterpret_cast<uint16_t *>(reg + kPRank);
+    uint16_t *bin16 = reinterpret_cast<uint16_t *>(reg + kPBin);
+    uint32_t *rank32 = gs.rank + G;
+    const uint32_t nbin = 2 * nb, stride = nbin + 1;
+    for (uint32_t i = threadIdx.x; i < nbin; i += kT) hist[i] = 0;
+    if (threadIdx.x == 0) sh.sfx = 0;
+    __syncthreads();
+    uint32_t sfx = 0;
+    constexpr int kU = 4;  // entries per thread in flight
+    for (uint32_t x0 = 0; x0 < total; x0 += kU * kT) {
+        bool act[kU];
+        uint32_t val[kU], word[kU];
+        uint64_t key[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            act[u] = x < total && !(ldv(v.flag + x) & kUsed);
+            if (act[u]) {
+                val[u] = ldv(v.val + x);
+                word[u] = ldv(v.word + x);
+                key[u] = ldv(v.key + x);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            if (act[u] && needs_refill(a, val[u])) word[u] = refill_word(a, val[u]);
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if (!act[u]) continue;
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            key[u] = step_key(a, key[u], val[u], word[u]);
+            v.key[x] = key[u];
+            v.word[x] = word[u];
+            const uint32_t bn = 2 * bkt_of(sort_key(key[u], val[u]), nb) + (val[u] >> 31);
+            const uint32_t rk = atomicAdd(&hist[bn], 1u);
+            if (in_smem) {
+                rank16[x] = (uint16_t)rk;
+                bin16[x] = (uint16_t)bn;
+            } else {
+                rank32[x] = rk;
+            }
+            sfx += (val[u] >> 31) == 0;
+        }
+    }
+    if (sfx) atomicAdd(&sh.sfx, sfx);
+    __syncthreads();
+    sprobe(sh, 13);
+    const uint32_t per = (nbin + kT - 1) / kT;
+    const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
+    const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
+    uint32_t run = 0;
+    for (uint32_t b = b0; b < b1; ++b) run += hist[b];
+    uint32_t kept;
+    uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &kept);
+    uint32_t *orow = offs + (uint64_t)tile * stride;
+    for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t h = hist[b];
+        hist[b] = ex;
+        orow[b] = ex;
+        ex += h;
+    }
+    if (threadIdx.x == 0) {
+        orow[nbin] = kept;
+        const uint64_t ob = kept ? atomicAdd(reinterpret_cast<unsigned long long *>(&nx.n), (unsigned long long)kept)
+                                 : 0ull;
+        sh.base = ob;
+        tbase[tile] = ob;
+        if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.s), (unsigned long long)sh.sfx);
+    }
+    __syncthreads();
+    sprobe(sh, 14);
+    BktEntry *dst = lout + sh.base;
+    if (in_smem) {  // permute in shared memory, then write the tile in order
+        for (uint32_t x = threadIdx.x; x < total; x += kT)
+            if (!(v.flag[x] & kUsed)) inv[hist[bin16[x]] + rank16[x]] = (uint16_t)x;
+        __syncthreads();
+        sprobe(sh, 15);
+        for (uint32_t d = threadIdx.x; d < kept; d += kT) {
+            const uint32_t x = inv[d];
+            const uint64_t key = v.key[x];
+            reinterpret_cast<uint4 *>(dst)[d] = make_uint4((uint32_t)key, (uint32_t)(key >> 32), v.val[x], v.word[x]);
+        }
+    } else {
+        for (uint32_t x = threadIdx.x; x < total; x += kT) {
+            if (ldv(v.flag + x) & kUsed) continue;
+            const uint64_t key = ldv(v.key + x);
+            const uint32_t val = ldv(v.val + x);
+            const uint32_t bn = 2 * bkt_of(sort_key(key, val), nb) + (val >> 31);
+            reinterpret_cast<uint4 *>(dst)[hist[bn] + ldv(rank32 + x)] =
+                make_uint4((uint32_t)key, (uint32_t)(key >> 32), val, ldv(v.word + x));
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------- a round tile
+EMP_DEV Cands cands_smem(uint8_t *smem) {
+    uint8_t *reg = smem + kOffReg;
+    Cands w;
+    w.ck = reinterpret_cast<uint64_t *>(reg + kCKey);
+    w.cv = reinterpret_cast<uint32_t *>(reg + kCVal);
+    w.cx = reinterpret_cast<uint32_t *>(reg + kCIdx);
+    w.sk = reinterpret_cast<uint64_t *>(reg + kCSk);
+    w.tb = reinterpret_cast<uint32_t *>(reg + kCTb);
+    w.ord = reinterpret_cast<uint32_t *>(reg + kCOrd);
+    w.cnt = reinterpret_cast<uint64_t *>(reg + kCCnt);
+    w.skey = reinterpret_cast<uint64_t *>(reg + kCSKey);
+    w.sval = reinterpret_cast<uint32_t *>(reg + kCSVal);
+    w.sidx = reinterpret_cast<uint32_t *>(reg + kCSIdx);
+    return w;
+}
+EMP_DEV Cands cands_global(const BktJob &J, uint64_t G) {
+    BScratch gs;
+    scratch_layout(J.scratch, J.n_max, &gs);
+    Cands w;
+    w.ck = gs.ck + G;
+    w.cv = gs.cv + G;
+    w.cx = gs.cx + G;
+    w.sk = gs.sk + G;
+    w.tb = gs.tb + G;
+    w.ord = gs.ord + G;
+    w.cnt = gs.cnt + G;
+    w.skey = gs.skey + G;
+    w.sval = gs.sval + G;
+    w.sidx = gs.sidx + G;
+    return w;
+}
+
+// Compact the matched staged entries into w (any order: the ranking fixes
+// it), writing at most cap of them; returns how many there are.
+EMP_DEV uint32_t compact(const Stage &v, uint32_t total, const Cands &w, uint32_t cap, BShared &sh) {
+    if (threadIdx.x == 0) sh.tile = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
     for (uint32_t x0 = 0; x0 < total; x0 += kT) {
         const uint32_t x = x0 + threadIdx.x;
-        c += __syncthreads_count(x < total && (ldv(v.pos + x) & kFlag));
+        const bool f = x < total && (ldv(v.flag + x) & kMatched);
+        const uint32_t m = __ballot_sync(0xffffffffu, f);
+        if (!m) continue;
+        const uint32_t leader = __ffs(m) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(&sh.tile, (uint32_t)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        const uint32_t d = base + __popc(m & lanemask_lt_u32());
+        if (f && d < cap) {
+            w.ck[d] = ldv(v.key + x);
+            w.cv[d] = ldv(v.val + x);
+            w.cx[d] = x;
+        }
     }
-    if (threadIdx.x == 0 && c) atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].cands), (unsigned long long)c);
+    __syncthreads();
+    return sh.tile;
+}
+
+// More than kBCand matched entries, or a bucket staged in scratch: the
+// matched entries go to the bucket's scratch region and are ranked there.
+EMP_COLD uint64_t big_count(const BktJob &J, const Stage &v, uint32_t total, bool in_smem, uint64_t &G, uint32_t K,
+                            uint32_t nb, uint32_t b, const uint32_t *offs, BShared &sh, uint32_t &c) {
+    if (in_smem) {  // the bucket's position in bucket order picks its scratch region
+        uint64_t gpre = 0;
+        const uint32_t stride = 2 * nb + 1;
+        for (uint32_t k = threadIdx.x; k < K; k += kT) gpre += __ldcg(offs + (uint64_t)k * stride + 2 * b);
+        block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &G);
+    }
+    const Cands w = cands_global(J, G);
+    c = compact(v, total, w, total, sh);
+    return c ? sort_and_count(w, c, sh) : 0;
+}
+
+// Edges of the ranked matched entries at ebase (only when they fit), and
+// the used marks: a suffix with an edge, a prefix that got one.
+EMP_DEV void write_edges(BktJob &J, const Cands &w, uint32_t c, uint64_t ebase, bool room, const Stage &v) {
+    for (uint32_t i = threadIdx.x; i < c; i += kT) {
+        const uint32_t vi = ldv(w.sval + i);
+        if (vi >> 31) continue;
+        const uint64_t ki = ldv(w.skey + i);
+        const uint32_t si = vi & 0x7fffffffu, ri = si >> 1;
+        const uint64_t o0 = ebase + ldv(w.cnt + i);
+        uint64_t o = o0;
+        for (uint32_t j = i + 1; j < c && ldv(w.skey + j) == ki; ++j) {
+            const uint32_t vj = ldv(w.sval + j);
+            const uint32_t pj = vj & 0x7fffffffu;
+            if ((vj >> 31) && (pj >> 1) != ri) {
+                if (room) {
+                    J.sfrom[o] = si;
+                    J.sto[o] = pj;
+                }
+                v.flag[ldv(w.sidx + j)] = kMatched | kUsed;
+                ++o;
+            }
+        }
+        if (o != o0) v.flag[ldv(w.sidx + i)] = kMatched | kUsed;
+    }
+    __syncthreads();
+}
+
+EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const CoopCtl *ctl, uint8_t *smem) {
+    probe(ctl, iter, 2);
+    if (threadIdx.x == 0) {
+        sh.pctl = ctl;
+        sh.piter = iter;
+    }
+    __syncthreads();
+    const uint32_t cur = iter % 3, nxt = (iter + 1) % 3;
+    BktIter &I = J.it[cur];
+    // slots are rewritten every third iteration by other CTAs: read around L1
+    const uint32_t K = vld(I.K), nb = vld(I.nb);
+    const uint32_t *offs = J.offs[iter & 1];
+    Stage v;
+    uint32_t S = 0;
+    uint64_t G = 0;
+    const uint32_t total = gather(J, J.lst[iter & 1], offs, J.tile_base[iter & 1], K, nb, b, sh, smem, v, S, G);
+    const bool in_smem = total <= kBStage;
+    probe(ctl, iter, 3);
+    // ---- entries whose key is in both tables: flagged, compacted, ranked, joined
+    uint32_t c = 0;
     uint64_t E = 0;
-    CandView w;
-    if (c) {
-        if (in_smem && c <= kBCand) {
-            // compact (any order: the sort below fixes it) into the hash
-            // region; the sort arrays then take the stage region
-            uint8_t *h = smem + kOffHash;
-            w.ck = reinterpret_cast<uint64_t *>(h);
-            w.cv = reinterpret_cast<uint32_t *>(h + kBCand * 8);
-            w.cp = w.cv + kBCand;
-            if (threadIdx.x == 0) sh.tile = 0;  // compaction counter
-            __syncthreads();
-            const uint32_t lane = threadIdx.x & 31;
-            for (uint32_t x0 = 0; x0 < total; x0 += kT) {
-                const uint32_t x = x0 + threadIdx.x;
-                const uint32_t ps = x < total ? v.pos[x] : 0u;
-                const bool f = (ps & kFlag) != 0;
-                const uint32_t m = __ballot_sync(0xffffffffu, f);
-                if (!m) continue;
-                const uint32_t leader = __ffs(m) - 1;
-                uint32_t base = 0;
-                if (lane == leader) base = atomicAdd(&sh.tile, (uint32_t)__popc(m));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (f) {
-                    const uint32_t d = base + __popc(m & lanemask_lt_u32());
-                    w.ck[d] = v.key[x];
-                    w.cv[d] = v.val[x];
-                    w.cp[d] = ps & ~kFlag;
-                }
-            }
-            __syncthreads();
-            uint8_t *s = smem;  // stage region, free now
-            w.sk = reinterpret_cast<uint64_t *>(s);
-            w.tb = reinterpret_cast<uint32_t *>(s + kBCand * 8);
-            w.idx = w.tb + kBCand;
-            w.cnt = reinterpret_cast<uint64_t *>(s + kBCand * 16);
-            w.skey = reinterpret_cast<uint64_t *>(s + kBCand * 24);
-            w.sval = reinterpret_cast<uint32_t *>(s + kBCand * 32);
-            w.spos = w.sval + kBCand;
-            static_assert(kBCand * 40 <= kOffHash, "sort arrays fit the stage region");
+    bool small = false;
+    if (S && S < total) {
+        if (in_smem) {
+            if (!match_filter(total, S, smem, sh)) match_smem(total, S, smem);
+            probe(ctl, iter, 4);
+            c = compact(v, total, cands_smem(smem), kBCand, sh);
+            small = c <= kBCand;
         } else {
-            // in place, in order, then the global scratch region of the bucket
-            uint32_t cc = 0;
-            for (uint32_t x0 = 0; x0 < total; x0 += kT) {
-                const uint32_t x = x0 + threadIdx.x;
-                const uint32_t ps = x < total ? ldv(v.pos + x) : 0u;
-                const bool f = (ps & kFlag) != 0;
-                uint64_t key = 0;
-                uint32_t val = 0;
-                if (f) {
-                    key = ldv(v.key + x);
-                    val = ldv(v.val + x);
-                }
-                uint32_t ctot;
-                const uint32_t ex = block_exclusive_scan<kT, uint32_t>(f ? 1u : 0u, sh.scan32, &ctot);
-                if (f) {
-                    v.key[cc + ex] = key;
-                    v.val[cc + ex] = val;
-                    v.pos[cc + ex] = ps & ~kFlag;
-                }
-                cc += ctot;
-                __syncthreads();
-            }
-            if (in_smem) {  // the bucket's place in bucket order picks its scratch region
-                uint64_t gpre = 0;
-                const uint32_t stride = 2 * nb + 1;
-                for (uint32_t k = threadIdx.x; k < K; k += kT) gpre += __ldcg(J.offs + (uint64_t)k * stride + 2 * b);
-                block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &G);
-            }
             BScratch gs;
             scratch_layout(J.scratch, J.n_max, &gs);
-            w.ck = v.key;
-            w.cv = v.val;
-            w.cp = v.pos;
-            w.sk = gs.sk + G;
-            w.tb = gs.tb + G;
-            w.idx = gs.idx + G;
-            w.cnt = gs.cnt + G;
-            w.skey = gs.skey + G;
-            w.sval = gs.sval + G;
-            w.spos = gs.spos + G;
+            match_global(v, total, S, gs, G);
         }
-        probe(ctl, iter, 15);
-        E = sort_and_count(w, c, sh);
+        probe(ctl, iter, 5);
+        if (small) {
+            if (c) E = sort_fine(cands_smem(smem), c, b, nb, smem, sh);
+        } else {
+            E = big_count(J, v, total, in_smem, G, K, nb, b, offs, sh, c);
+        }
+        if (threadIdx.x == 0 && c)
+            atomicAdd(reinterpret_cast<unsigned long long *>(&I.cands), (unsigned long long)c);
     }
-    probe(ctl, iter, 17);
+    probe(ctl, iter, 6);
     if (threadIdx.x == 0) {
         uint64_t off = 0;
         if (E) {
             off = atomicAdd(reinterpret_cast<unsigned long long *>(&J.e_stage), (unsigned long long)E);
             if (off + E > J.ecap) J.overflow = 1;
-            atomicAdd(reinterpret_cast<unsigned long long *>(&J.it[p].edges), (unsigned long long)E);
+            atomicAdd(reinterpret_cast<unsigned long long *>(&I.edges), (unsigned long long)E);
         }
         sh.base = off;
         BktSpan &sp = J.spans[(uint64_t)(vld(J.round) - J.r0) * J.nb_max + b];
@@ -761,74 +1230,68 @@ EMP_DEV void b_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const Coo
         sp.cnt = E;
     }
     __syncthreads();
-    probe(ctl, iter, 18);
-    if (E && sh.base + E <= J.ecap) {
-        const uint64_t ebase = sh.base;
-        for (uint32_t i = threadIdx.x; i < c; i += kT) {
-            const uint32_t vi = ldv(w.sval + i);
-            if (vi >> 31) continue;
-            const uint64_t ki = ldv(w.skey + i);
-            const uint32_t si = vi & 0x7fffffffu, ri = si >> 1;
-            const uint64_t o0 = ebase + ldv(w.cnt + i);
-            uint64_t o = o0;
-            for (uint32_t j = i + 1; j < c && ldv(w.skey + j) == ki; ++j) {
-                const uint32_t vj = ldv(w.sval + j);
-                const uint32_t pj = vj & 0x7fffffffu;
-                if ((vj >> 31) && (pj >> 1) != ri) {
-                    J.sfrom[o] = si;
-                    J.sto[o] = pj;
-                    lst[ldv(w.spos + j)].val = kBktTomb;
-                    ++o;
-                }
-            }
-            if (o != o0) lst[ldv(w.spos + i)].val = kBktTomb;
+    if (E) write_edges(J, small ? cands_smem(smem) : cands_global(J, G), c, sh.base, sh.base + E <= J.ecap, v);
+    probe(ctl, iter, 7);
+    // ---- round r+1's tile b
+    const int r = (int)vld(J.round);
+    if (r + 1 < J.rounds) {
+        BktIter &N = J.it[nxt];
+        const uint32_t nb_next = vld(N.nb);
+        const StepArgs a = step_args(J, r + 1, false);
+        if (in_smem) {
+            write_next_smem(total, a, nb_next, b, J.lst[(iter + 1) & 1], J.offs[(iter + 1) & 1],
+                            J.tile_base[(iter + 1) & 1], N, sh, smem);
+        } else {
+            BScratch gs;
+            scratch_layout(J.scratch, J.n_max, &gs);
+            write_next(J, v, total, false, a, nb_next, b, J.lst[(iter + 1) & 1], J.offs[(iter + 1) & 1],
+                       J.tile_base[(iter + 1) & 1], N, sh, smem, gs, G);
         }
     }
-    __syncthreads();
-    probe(ctl, iter, 19);
+    probe(ctl, iter, 8);
 }
 
-// Record the round and advance the job (one thread, once every bucket of the
-// round is done).  Writes only the other parity's iteration state.
-EMP_DEV void round_end(BktJob &x, CoopCtl *ctl, uint32_t iter) {
-    const uint32_t p = iter & 1, q = p ^ 1;
-    const uint64_t N = vld(x.it[p].n_out), S = vld(x.it[p].s_out), P = N - S;
+// Record round r (slot cur) and prepare round r+2's slot; ends the job when
+// round r+1 would have no suffix or would be past the last round.  One
+// thread, once every bucket of the round is done.  It writes only slot nn,
+// which no CTA reads in this iteration.
+EMP_COLD void round_end(BktJob &x, CoopCtl *ctl, uint32_t iter) {
+    const uint32_t cur = iter % 3, nxt = (iter + 1) % 3, nn = (iter + 2) % 3;
+    const BktIter &I = x.it[cur];
+    const BktIter &N = x.it[nxt];
+    const uint64_t n = vld(I.n), S = vld(I.s), P = n - S;
     const uint32_t r = vld(x.round);
-    if (S == 0) {  // build_graph's loop condition: no suffix left
-        x.end_iter = iter;
-        atomicSub(&ctl->active, 1u);
-        __threadfence();
-        return;
-    }
-    const uint64_t E = P ? vld(x.it[p].edges) : 0;
+    const uint64_t E = P ? vld(I.edges) : 0;
     const uint64_t e0 = vld(x.e_total);
     RoundRecord &rec = x.records[r];
     rec.S = S;
     rec.P = P;
     rec.E = E;
     rec.e0 = e0;
-    rec.C = vld(x.it[p].cands);
-    rec.nb = vld(x.it[p].nb);
+    rec.C = vld(I.cands);
+    rec.nb = vld(I.nb);
     x.e_total = e0 + E;
     x.round = r + 1;
-    BktIter &nx = x.it[q];
-    nx.n_in = N;
-    nx.n_out = 0;
-    nx.s_out = 0;
-    nx.cands = 0;
-    nx.edges = 0;
-    nx.nb = bkt_count(N, gridDim.x);
-    nx.b_done = 0;
-    if ((int)(r + 1) >= x.rounds) {
-        x.end_iter = iter;
+    if ((int)(r + 1) >= x.rounds || vld(N.s) == 0) {  // build_graph's loop condition (overlap.cu:258)
+        x.end_iter = iter + 1;
         atomicSub(&ctl->active, 1u);
+        __threadfence();
+        return;
     }
+    BktIter &M = x.it[nn];
+    M.n = 0;
+    M.s = 0;
+    M.cands = 0;
+    M.edges = 0;
+    M.b_done = 0;
+    M.K = vld(N.nb);                         // round r+1 writes one tile per bucket
+    M.nb = bkt_count(vld(N.n), gridDim.x);   // and partitions it by round r+1's size
     __threadfence();
 }
 
-// After the last round: each round's edges from the staging buffer to the
-// edge list in bucket order (rounds spread over the CTAs, no grid barrier).
-EMP_DEV void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
+// After the last round: each round's record, edges from the staging buffer in
+// bucket order (rounds spread over the CTAs, no grid barrier).
+EMP_COLD void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
     uint64_t *dest = reinterpret_cast<uint64_t *>(smem);  // nb + 1 bucket starts
     uint64_t *roff = dest + kBktMaxBuckets + 1;          // byte offset of each round's record
     uint32_t g = 0;
@@ -888,57 +1351,57 @@ EMP_DEV void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
     }
 }
 
-__global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, CoopCtl *ctl, uint32_t *err) {
+__global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, CoopCtl *ctl, uint32_t *) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ BShared sh;
     const int J = (int)ctl->njobs;
+    // ---- prologue: the launch's input lists -> round r0's lists
+    uint32_t total = build_prefix(sh, J, [&](int j) -> uint32_t { return (uint32_t)bkt_tiles(jobs[j].n_in); });
+    tile_loop(sh, &ctl->ticket[0], J, total, [&](int j, uint32_t k) { prologue_tile(jobs[j], k, sh, smem); });
+    if (!grid_barrier(ctl, &sh.flag, 0, 7)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int j = 0; j < J; ++j) {  // round r0 runs only with a suffix left
+            BktJob &x = jobs[j];
+            BktIter &N = x.it[1];
+            N.K = vld(x.it[0].nb);
+            N.nb = bkt_count(vld(x.it[0].n), gridDim.x);
+            if (vld(x.it[0].s) == 0 || x.r0 >= x.rounds) {
+                x.end_iter = 0;
+                atomicSub(&ctl->active, 1u);
+            }
+        }
+        __threadfence();
+    }
+    if (!grid_barrier(ctl, &sh.flag, 0, 6)) return;
+    // ---- rounds
     for (uint32_t iter = 0;; ++iter) {
         if (vld(ctl->active) == 0) break;
-        const uint32_t p = iter & 1;
-        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ticket[1] = 0;  // bucket ticket of the last iteration
+        const uint32_t cur = iter % 3;
+        uint32_t *ticket = &ctl->ticket[1 + (iter & 1)];
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ticket[1 + ((iter + 1) & 1)] = 0;  // last iteration's
         probe(ctl, iter, 0);
-        // ---- A: stream, hash step, partition
-        uint32_t total = build_prefix(sh, J, [&](int j) -> uint32_t {
-            const BktJob &x = jobs[j];
-            return vld(x.end_iter) >= iter ? (uint32_t)bkt_tiles(vld(x.it[p].n_in)) : 0u;
-        });
-        probe(ctl, iter, 1);
-        tile_loop(sh, &ctl->ticket[0], J, total, [&](int j, uint32_t k) { a_tile(jobs[j], k, iter, sh, ctl, smem); });
-        probe(ctl, iter, 6);
-        if (!grid_barrier(ctl, &sh.flag, iter, 0)) return;
-        probe(ctl, iter, 7);
-        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ticket[0] = 0;
-        // ---- B: buckets; the last bucket of a job ends its round.  The
-        // prefix reads only state round_end leaves alone (it writes the other
-        // parity and end_iter, which stays >= iter for this iteration).
         total = build_prefix(sh, J, [&](int j) -> uint32_t {
             const BktJob &x = jobs[j];
-            if (vld(x.end_iter) < iter) return 0u;
-            const uint64_t S = vld(x.it[p].s_out), N = vld(x.it[p].n_out);
-            return (S > 0 && S < N) ? vld(x.it[p].nb) : 0u;
+            return iter < vld(x.end_iter) ? vld(x.it[cur].nb) : 0u;
         });
-        probe(ctl, iter, 10);
-        tile_loop(sh, &ctl->ticket[1], J, total, [&](int j, uint32_t b) {
+        probe(ctl, iter, 1);
+        tile_loop_static(sh, ticket, J, total, [&](int j, uint32_t b) {
             BktJob &x = jobs[j];
-            b_tile(x, b, iter, sh, ctl, smem);
+            round_tile(x, b, iter, sh, ctl, smem);
             __threadfence();
             __syncthreads();
             if (threadIdx.x == 0) {
                 const uint32_t nbj = sh.pref[j + 1] - sh.pref[j];
-                if (atomicAdd(&x.it[p].b_done, 1u) == nbj - 1) {
+                if (atomicAdd(&x.it[cur].b_done, 1u) == nbj - 1) {
                     __threadfence();
                     round_end(x, ctl, iter);
                 }
             }
             __syncthreads();
         });
-        // running jobs without buckets this round: round end by CTA (j mod grid)
-        for (int j = blockIdx.x; j < J; j += gridDim.x)
-            if (threadIdx.x == 0 && sh.pref[j + 1] == sh.pref[j] && vld(jobs[j].end_iter) >= iter)
-                round_end(jobs[j], ctl, iter);
-        probe(ctl, iter, 20);
-        if (!grid_barrier(ctl, &sh.flag, iter, 1)) return;
-        probe(ctl, iter, 21);
+        probe(ctl, iter, 9);
+        if (!grid_barrier(ctl, &sh.flag, iter, 0)) return;
+        probe(ctl, iter, 10);
     }
     place_edges(jobs, J, sh, smem);
 }
@@ -947,8 +1410,13 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
 
 size_t bkt_scratch_bytes(uint64_t n_max) { return scratch_layout(nullptr, n_max < 1 ? 1 : n_max, nullptr); }
 
+uint64_t bkt_max_tiles(uint64_t n_max, uint32_t G) {
+    const uint64_t a = bkt_tiles(n_max < 1 ? 1 : n_max), b = bkt_count(n_max, G);
+    return a > b ? a : b;
+}
+
 size_t bkt_offs_words(uint64_t n_max, uint32_t G) {
-    return (size_t)bkt_tiles(n_max < 1 ? 1 : n_max) * (2 * bkt_count(n_max, G) + 1);
+    return (size_t)bkt_max_tiles(n_max, G) * (2 * bkt_count(n_max, G) + 1);
 }
 
 int bucket_grid_size() {

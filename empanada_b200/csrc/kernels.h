@@ -221,21 +221,22 @@ int coop_grid_size();
 cudaError_t launch_coop_rounds(CoopJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
 
 // ---- bucket rounds (k_bucket.cu) ------------------------------------------
-// Each round of each job: phase A streams the live entries in 4096-entry
-// tiles (drop used ones, hash step, partition the tile into the round's key
-// buckets); phase B gives each key bucket to one CTA, which gathers the
-// bucket's pieces from every tile, finds the keys present in both tables with
-// a hash set, sorts those entries and joins them.  Neither phase waits on
-// another CTA: output space comes from one atomic per tile or bucket, and the
-// edges are put in bucket order once all rounds are done.
+// A list of 16-byte entries lives as tiles, each tile partitioned into
+// (key bucket, table) bins.  A prologue partitions the launch's input list;
+// then each round gives each key bucket to one CTA, which gathers the
+// bucket's piece of every tile, finds the keys present in both tables with a
+// hash set, sorts and joins those entries, drops the used ones, applies the
+// next round's hash step to the rest and writes them as one tile of the next
+// round's list.  One grid barrier per round; output space comes from one
+// atomic per tile, and the edges are put in bucket order once all rounds are
+// done.
 struct BktEntry {
     uint64_t key;   // fp1 << 32 | fp2
-    uint32_t val;   // rid | table << 31, or kBktTomb once used
+    uint32_t val;   // rid | table << 31
     uint32_t word;  // cached 16 bases (one seq2 word) of the entry's read
 };
-constexpr uint32_t kBktTomb = 0xffffffffu;
-constexpr uint32_t kBktTile = 4096;               // entries per phase-A tile
-constexpr uint64_t kBktMean = 7168;               // most entries per bucket aimed at (mean)
+constexpr uint32_t kBktTile = 4096;               // entries per prologue tile
+constexpr uint64_t kBktMean = 6300;               // entries per bucket aimed at (mean)
 constexpr uint32_t kBktMaxBuckets = 4096;
 constexpr uint64_t kBktMaxEntries = 16ull << 20;  // larger lists use the other drivers
 __host__ __device__ inline uint64_t bkt_tiles(uint64_t n) { return (n + kBktTile - 1) / kBktTile; }
@@ -251,14 +252,15 @@ __host__ __device__ inline uint32_t bkt_count(uint64_t n, uint32_t G) {
 __host__ __device__ inline uint32_t bkt_of(uint64_t sk, uint32_t nb) {
     return (uint32_t)(((sk >> 35) * (uint64_t)nb) >> 24);
 }
-struct BktIter {         // one per iteration parity
-    uint64_t n_in;       // entries entering phase A
-    uint64_t n_out;      // entries kept by phase A
-    uint64_t s_out;      // of which suffixes
-    uint64_t cands;      // entries found in both tables
-    uint64_t edges;      // edges of the round
-    uint32_t nb;         // buckets of the round
-    uint32_t b_done;     // buckets finished
+struct BktIter {         // one round's list (three slots, by iteration mod 3)
+    uint64_t n;          // entries (an atomic count while the list is written)
+    uint64_t s;          // of which suffixes
+    uint64_t cands;      // entries found in both tables in this round
+    uint64_t edges;      // edges of this round
+    uint32_t K;          // tiles holding the list
+    uint32_t nb;         // key buckets the tiles are partitioned into
+    uint32_t b_done;     // buckets of this round finished
+    uint32_t pad;
 };
 struct BktSpan {         // one bucket's edges in the staging buffer
     uint64_t off, cnt;
@@ -267,12 +269,13 @@ struct BktJob {
     const uint64_t *lk_in;   // the list at launch (id order, suffixes then prefixes)
     const uint32_t *lv_in;
     const uint8_t *used_s, *used_p;  // marks of rounds run before the launch
-    BktEntry *lst[2];        // lists written by phase A, n_max entries each
+    uint64_t n_in;           // entries of that list
+    BktEntry *lst[2];        // the current and the next round's list, n_max entries each
+    uint32_t *offs[2];       // per tile: 2 nb + 1 bin starts
+    uint64_t *tile_base[2];  // per tile: its first entry in lst
     const uint32_t *seq2;    // read-major 2-bit bases, wpr words per read
     int32_t wpr, L, rounds, r0;
     const HashTables *tables;
-    uint32_t *offs;          // per phase-A tile: nb + 1 bucket starts
-    uint64_t *tile_base;     // per phase-A tile: its first output entry
     BktSpan *spans;          // [round - r0][bucket]: edges in the staging buffer
     uint32_t *sfrom, *sto;   // staging buffer (bucket order within a round is restored at the end)
     uint8_t *out;            // output.bin records of the launch's rounds (12 * rounds + 8 * ecap bytes)
@@ -282,14 +285,15 @@ struct BktJob {
     uint64_t n_max;
     uint32_t nb_max;         // row length of spans
     uint32_t round;          // next round to run
-    uint32_t end_iter;       // iteration in which the job ended (0xffffffff while running)
+    uint32_t end_iter;       // first iteration the job does not run (0xffffffff while running)
     uint32_t overflow;       // the edge buffer was too small
     uint64_t e_total;        // edges of the finished rounds of this launch
     uint64_t e_stage;        // staging buffer fill
-    BktIter it[2];
+    BktIter it[3];
 };
 size_t bkt_scratch_bytes(uint64_t n_max);
-size_t bkt_offs_words(uint64_t n_max, uint32_t G);  // u32 words of BktJob::offs
+size_t bkt_offs_words(uint64_t n_max, uint32_t G);  // u32 words of one BktJob::offs buffer
+uint64_t bkt_max_tiles(uint64_t n_max, uint32_t G); // entries of one BktJob::tile_base buffer
 int bucket_grid_size();                             // 0: no cooperative launch on this device
 cudaError_t launch_bucket_rounds(BktJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
 
