@@ -381,8 +381,8 @@ def main():
                     "72 B per candidate, 8 B per edge")
         else:
             kname = "bucket_rounds_kernel"
-            what = ("all rounds in one launch: per round 16 B read per entry in, 16 B written + 16 B gathered "
-                    "per kept entry, 8 B per edge")
+            what = ("all rounds in one launch: per round 16 B gathered per entry, 16 B written per entry kept "
+                    "for the next round, 8 B per edge")
     elif sort_ms >= upd_ms:  # the radix-sort digit pass dominates
         per_launch = 24.0 * sort_elems / max(sort_passes, 1)
         ms, nl, kname = sort_ms, sort_passes, "onesweep_kernel"

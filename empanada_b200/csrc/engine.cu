@@ -99,7 +99,7 @@ struct emp_job {
     DevBuf dout;                 // output.bin records written on the device (after those in `out`)
     uint64_t dout_bytes = 0;
     PinnedBuf h_out;
-    DevBuf bk_lst0, bk_lst1, bk_offs, bk_tile_base, bk_spans, bk_sfrom, bk_sto, bk_scratch, bk_job;  // bucket kernel
+    DevBuf bk_lst0, bk_lst1, bk_offs, bk_tile_base, bk_spans, bk_sfrom, bk_sto, bk_scratch, bk_job, bk_meta;  // bucket kernel
     PinnedBuf h_coop;
     cudaEvent_t sort_ev[2 * kSortPasses] = {};
     cudaEvent_t upd_ev[2 * EMP_MAX_ROUNDS] = {};
@@ -641,6 +641,8 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     EMP_TRY(ensure(j, j->bk_sto, ecap * 4));
     EMP_TRY(ensure(j, j->bk_scratch, bkt_scratch_bytes(nmax)));
     EMP_TRY(ensure(j, j->bk_job, sizeof(BktJob)));
+    EMP_TRY(ensure(j, j->bk_meta, ((size_t)env.rounds + 1) * sizeof(BktRound)));
+    EMP_CUDA(cudaMemsetAsync(j->bk_meta.p, 0, ((size_t)env.rounds + 1) * sizeof(BktRound), s));
     EMP_TRY(ensure(j, j->coop_ctl, sizeof(CoopCtl)));
     EMP_TRY(ensure(j, j->dout, (size_t)env.rounds * 12 + ecap * 8));
     EMP_TRY(ensure(j, j->records, (size_t)env.rounds * sizeof(RoundRecord)));
@@ -676,10 +678,7 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     hj->n_max = nmax;
     hj->nb_max = nb_max;
     hj->r0 = r0;
-    hj->round = (uint32_t)r0;
-    hj->end_iter = 0xffffffffu;
-    hj->it[0].K = (uint32_t)bkt_tiles(n_in);  // the prologue's tiles
-    hj->it[0].nb = bkt_count(n_in, (uint32_t)grid);
+    hj->meta = j->bk_meta.as<BktRound>();
     hc->njobs = 1;
     hc->active = 1;
     const char *trace_path = std::getenv("EMP_COOP_TRACE");  // profiling: per-phase timestamps
@@ -1200,7 +1199,8 @@ emp_status emp_job_destroy(emp_job *job) {
                       &job->records, &job->st_upd, &job->st_cand, &job->st_scan, &job->ctl, &job->st_join,
                       &job->st_sort, &job->coop_job, &job->coop_ctl, &job->coop_trace,
                       &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_offs, &job->bk_tile_base, &job->bk_spans,
-                      &job->bk_sfrom, &job->bk_sto, &job->bk_scratch, &job->bk_job, &job->dout};
+                      &job->bk_sfrom, &job->bk_sto, &job->bk_scratch, &job->bk_job, &job->dout,
+                      &job->bk_meta};
     for (DevBuf *b : bufs) free_buf(job, *b);
     for (auto &e : job->sort_ev)
         if (e) cudaEventDestroy(e);

@@ -90,7 +90,7 @@ static_assert(2 * kBktMaxBuckets <= 65536, "bins fit u16");
 // prologue tile: bin counters, then the staged tile
 constexpr size_t kASmem = 2 * kBktMaxBuckets * 4 + kBktTile * sizeof(BktEntry);
 // end phase: one round's bucket destinations, the record offsets of a job
-constexpr size_t kESmem = (kBktMaxBuckets + 1 + kT) * 8;
+constexpr size_t kESmem = (kBktMaxBuckets + 1 + 3 * kT) * 8;
 constexpr size_t kBktSmem = kRSmem > kASmem ? (kRSmem > kESmem ? kRSmem : kESmem) : kASmem;
 
 struct BShared {
@@ -101,6 +101,8 @@ struct BShared {
     uint32_t tile, flag, sfx, cnt;
     const CoopCtl *pctl;  // profiling stamps from inside the steps of a tile
     uint32_t piter;
+    HashTables tab;       // powers and inverses (every job of a launch shares them)
+    uint32_t shp_K[kCoopMaxJobs], shp_nb[kCoopMaxJobs], shp_nbn[kCoopMaxJobs];  // this iteration's shapes
 };
 EMP_DEV void sprobe(const BShared &sh, int p) { probe(sh.pctl, sh.piter, p); }
 
@@ -196,14 +198,14 @@ struct StepArgs {
     const uint32_t *seq2;
     int wpr;
 };
-EMP_DEV StepArgs step_args(const BktJob &J, int r, bool refill_all) {
+EMP_DEV StepArgs step_args(const BktJob &J, const HashTables &tab, int r, bool refill_all) {
     StepArgs a;
     a.L = J.L;
     a.r = r;
-    a.pw1 = J.tables->pow1[J.L - r - 1];
-    a.pw2 = J.tables->pow2[J.L - r - 1];
-    a.inv1 = J.tables->inv1;
-    a.inv2 = J.tables->inv2;
+    a.pw1 = tab.pow1[J.L - r - 1];
+    a.pw2 = tab.pow2[J.L - r - 1];
+    a.inv1 = tab.inv1;
+    a.inv2 = tab.inv2;
     a.refill_all = refill_all;
     a.seq2 = J.seq2;
     a.wpr = J.wpr;
@@ -238,10 +240,10 @@ EMP_DEV uint64_t step_key(const StepArgs &a, uint64_t key, uint32_t val, uint32_
 // ---------------------------------------------------------------- prologue
 // Tile k of the launch's input list -> round r0's list (tile k).
 EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
-    BktIter &I = J.it[0];
+    BktRound &I = J.meta[J.r0];
     const uint64_t n_in = J.n_in;
-    const uint32_t nb = I.nb, nbin = 2 * nb, stride = nbin + 1;
-    const StepArgs a = step_args(J, J.r0, true);
+    const uint32_t nb = bkt_count(n_in, gridDim.x), nbin = 2 * nb, stride = nbin + 1;
+    const StepArgs a = step_args(J, sh.tab, J.r0, true);
     uint32_t *hist = reinterpret_cast<uint32_t *>(smem);
     uint4 *stage = reinterpret_cast<uint4 *>(smem + 2 * kBktMaxBuckets * 4);
     for (uint32_t i = threadIdx.x; i < nbin; i += kT) hist[i] = 0;
@@ -460,7 +462,7 @@ EMP_DEV uint32_t gather(const BktJob &J, const BktEntry *lst, const uint32_t *of
             __syncthreads();
             S = sh.cnt;
             sprobe(sh, 12);
-            constexpr int U = 4;
+            constexpr int U = 8;
             for (uint32_t x0 = 0; x0 < total; x0 += U * kT) {
                 uint4 e[U];
 #pragma unroll
@@ -874,11 +876,11 @@ EMP_DEV uint64_t join_count(const Cands &w, uint32_t c, BShared &sh) {
 // ---------------------------------------------------------------- next round
 // Drop the used entries of the staged bucket, apply round a.r's hash step to
 // the rest and write them as tile `tile` of the next list, partitioned into
-// nb buckets.  Returns nothing; counts go to the next list's BktIter.
+// nb buckets.  Returns nothing; counts go to the next round's BktRound.
 // Bin starts of the next tile (in place in hist), its offs row, its place in
 // the next list; returns the kept count.
 EMP_DEV uint32_t close_tile(uint32_t *hist, uint32_t nbin, uint32_t tile, uint32_t *offs, uint64_t *tbase,
-                            BktIter &nx, BShared &sh) {
+                            BktRound &nx, BShared &sh) {
     const uint32_t per = (nbin + kT - 1) / kT;
     const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
     const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
@@ -908,7 +910,7 @@ EMP_DEV uint32_t close_tile(uint32_t *hist, uint32_t nbin, uint32_t tile, uint32
 // write_next for a bucket staged in shared memory: the same steps on the
 // shared arrays, the tile permuted in shared memory and written in order.
 EMP_DEV void write_next_smem(uint32_t total, const StepArgs &a, uint32_t nb, uint32_t tile, BktEntry *lout,
-                             uint32_t *offs, uint64_t *tbase, BktIter &nx, BShared &sh, uint8_t *smem) {
+                             uint32_t *offs, uint64_t *tbase, BktRound &nx, BShared &sh, uint8_t *smem) {
     uint64_t *key = reinterpret_cast<uint64_t *>(smem + kOffKey);
     uint32_t *val = reinterpret_cast<uint32_t *>(smem + kOffVal);
     uint32_t *word = reinterpret_cast<uint32_t *>(smem + kOffWord);
@@ -973,7 +975,7 @@ EMP_DEV void write_next_smem(uint32_t total, const StepArgs &a, uint32_t nb, uin
 }
 
 EMP_COLD void write_next(BktJob &J, const Stage &v, uint32_t total, bool in_smem, const StepArgs &a, uint32_t nb,
-                         uint32_t tile, BktEntry *lout, uint32_t *offs, uint64_t *tbase, BktIter &nx, BShared &sh,
+                         uint32_t tile, BktEntry *lout, uint32_t *offs, uint64_t *tbase, BktRound &nx, BShared &sh,
                          uint8_t *smem, const BScratch &gs, uint64_t G) {
     uint8_t *reg = smem + kOffReg;
     uint32_t *hist = reinterpret_cast<uint32_t *>(reg + kPHist);
@@ -1174,17 +1176,38 @@ EMP_DEV void write_edges(BktJob &J, const Cands &w, uint32_t c, uint64_t ebase, 
     __syncthreads();
 }
 
-EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const CoopCtl *ctl, uint8_t *smem) {
+// Shape of round r0 + iter of a job, the same in every CTA: counts of earlier
+// rounds are final once the grid barrier before the iteration has passed.
+struct RoundShape {
+    bool active;       // the round runs: r < rounds and a suffix left (overlap.cu:258)
+    int r;
+    uint32_t K;        // tiles of the round's list
+    uint32_t nb;       // its key buckets
+    uint32_t nb_next;  // key buckets of the next round's list
+};
+EMP_DEV RoundShape round_shape(const BktJob &J, uint32_t iter) {
+    RoundShape z;
+    z.r = J.r0 + (int)iter;
+    z.active = z.r < J.rounds && __ldcg(&J.meta[z.r].s) > 0;
+    z.K = z.nb = z.nb_next = 0;
+    if (!z.active) return z;
+    z.nb = iter ? bkt_count(__ldcg(&J.meta[z.r - 1].n), gridDim.x) : bkt_count(J.n_in, gridDim.x);
+    z.K = iter == 0 ? (uint32_t)bkt_tiles(J.n_in)
+                    : (iter == 1 ? bkt_count(J.n_in, gridDim.x) : bkt_count(__ldcg(&J.meta[z.r - 2].n), gridDim.x));
+    z.nb_next = bkt_count(__ldcg(&J.meta[z.r].n), gridDim.x);
+    return z;
+}
+
+EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &z, BShared &sh, const CoopCtl *ctl,
+                        uint8_t *smem) {
     probe(ctl, iter, 2);
     if (threadIdx.x == 0) {
         sh.pctl = ctl;
         sh.piter = iter;
     }
     __syncthreads();
-    const uint32_t cur = iter % 3, nxt = (iter + 1) % 3;
-    BktIter &I = J.it[cur];
-    // slots are rewritten every third iteration by other CTAs: read around L1
-    const uint32_t K = vld(I.K), nb = vld(I.nb);
+    BktRound &I = J.meta[z.r];
+    const uint32_t K = z.K, nb = z.nb;
     const uint32_t *offs = J.offs[iter & 1];
     Stage v;
     uint32_t S = 0;
@@ -1225,7 +1248,7 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const
             atomicAdd(reinterpret_cast<unsigned long long *>(&I.edges), (unsigned long long)E);
         }
         sh.base = off;
-        BktSpan &sp = J.spans[(uint64_t)(vld(J.round) - J.r0) * J.nb_max + b];
+        BktSpan &sp = J.spans[(uint64_t)(z.r - J.r0) * J.nb_max + b];
         sp.off = off;
         sp.cnt = E;
     }
@@ -1233,11 +1256,10 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const
     if (E) write_edges(J, small ? cands_smem(smem) : cands_global(J, G), c, sh.base, sh.base + E <= J.ecap, v);
     probe(ctl, iter, 7);
     // ---- round r+1's tile b
-    const int r = (int)vld(J.round);
-    if (r + 1 < J.rounds) {
-        BktIter &N = J.it[nxt];
-        const uint32_t nb_next = vld(N.nb);
-        const StepArgs a = step_args(J, r + 1, false);
+    if (z.r + 1 < J.rounds) {
+        BktRound &N = J.meta[z.r + 1];
+        const uint32_t nb_next = z.nb_next;
+        const StepArgs a = step_args(J, sh.tab, z.r + 1, false);
         if (in_smem) {
             write_next_smem(total, a, nb_next, b, J.lst[(iter + 1) & 1], J.offs[(iter + 1) & 1],
                             J.tile_base[(iter + 1) & 1], N, sh, smem);
@@ -1251,92 +1273,82 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, BShared &sh, const
     probe(ctl, iter, 8);
 }
 
-// Record round r (slot cur) and prepare round r+2's slot; ends the job when
-// round r+1 would have no suffix or would be past the last round.  One
-// thread, once every bucket of the round is done.  It writes only slot nn,
-// which no CTA reads in this iteration.
-EMP_COLD void round_end(BktJob &x, CoopCtl *ctl, uint32_t iter) {
-    const uint32_t cur = iter % 3, nxt = (iter + 1) % 3, nn = (iter + 2) % 3;
-    const BktIter &I = x.it[cur];
-    const BktIter &N = x.it[nxt];
-    const uint64_t n = vld(I.n), S = vld(I.s), P = n - S;
-    const uint32_t r = vld(x.round);
-    const uint64_t E = P ? vld(I.edges) : 0;
-    const uint64_t e0 = vld(x.e_total);
-    RoundRecord &rec = x.records[r];
-    rec.S = S;
-    rec.P = P;
-    rec.E = E;
-    rec.e0 = e0;
-    rec.C = vld(I.cands);
-    rec.nb = vld(I.nb);
-    x.e_total = e0 + E;
-    x.round = r + 1;
-    if ((int)(r + 1) >= x.rounds || vld(N.s) == 0) {  // build_graph's loop condition (overlap.cu:258)
-        x.end_iter = iter + 1;
-        atomicSub(&ctl->active, 1u);
-        __threadfence();
-        return;
-    }
-    BktIter &M = x.it[nn];
-    M.n = 0;
-    M.s = 0;
-    M.cands = 0;
-    M.edges = 0;
-    M.b_done = 0;
-    M.K = vld(N.nb);                         // round r+1 writes one tile per bucket
-    M.nb = bkt_count(vld(N.n), gridDim.x);   // and partitions it by round r+1's size
-    __threadfence();
-}
-
 // After the last round: each round's record, edges from the staging buffer in
 // bucket order (rounds spread over the CTAs, no grid barrier).
 EMP_COLD void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
     uint64_t *dest = reinterpret_cast<uint64_t *>(smem);  // nb + 1 bucket starts
-    uint64_t *roff = dest + kBktMaxBuckets + 1;          // byte offset of each round's record
+    uint64_t *roff = dest + kBktMaxBuckets + 1;          // per round of the job: record offset,
+    uint64_t *rE = roff + kT;                            // edge count,
+    uint64_t *rnb = rE + kT;                             // bucket count
     uint32_t g = 0;
     for (int j = 0; j < J; ++j) {
         BktJob &x = jobs[j];
-        if (vld(x.overflow)) continue;
-        const uint32_t r0 = (uint32_t)x.r0, r1 = vld(x.round);
-        {  // records: one per round with a non-empty prefix table, 12 + 8 E bytes
-            const uint32_t r = r0 + threadIdx.x;
-            uint64_t sz = 0;
-            if (r < r1 && __ldcg(&x.records[r].P)) sz = 12 + 8 * __ldcg(&x.records[r].E);
-            uint64_t tot;
-            const uint64_t ex = block_exclusive_scan<kT, uint64_t>(sz, sh.scan64, &tot);
-            if (r < r1) roff[threadIdx.x] = ex;
-            __syncthreads();
+        const uint32_t r0 = (uint32_t)x.r0;
+        // the rounds that ran: round r ran iff r < rounds and it had a suffix
+        // (build_graph's loop condition, overlap.cu:258)
+        const uint32_t r = r0 + threadIdx.x;
+        const bool ran = (int)r < x.rounds && __ldcg(&x.meta[r].s) > 0;
+        const uint32_t r1 = r0 + (uint32_t)__syncthreads_count(ran);  // rounds run form a prefix
+        uint64_t S = 0, P = 0, E = 0, C = 0, nb = 0;
+        if (r < r1) {
+            const BktRound &m = x.meta[r];
+            S = __ldcg(&m.s);
+            P = __ldcg(&m.n) - S;
+            E = P ? __ldcg(&m.edges) : 0;
+            C = __ldcg(&m.cands);
+            nb = r == r0 ? bkt_count(x.n_in, gridDim.x) : bkt_count(__ldcg(&x.meta[r - 1].n), gridDim.x);
         }
-        for (uint32_t r = r0; r < r1; ++r, ++g) {
+        uint64_t e_all, bytes;
+        const uint64_t e0 = block_exclusive_scan<kT, uint64_t>(E, sh.scan64, &e_all);
+        const uint64_t off = block_exclusive_scan<kT, uint64_t>(P ? 12 + 8 * E : 0, sh.scan64, &bytes);
+        if (r < r1) {
+            roff[threadIdx.x] = off;
+            rE[threadIdx.x] = E;
+            rnb[threadIdx.x] = nb;
+            if (blockIdx.x == 0) {
+                RoundRecord &rec = x.records[r];
+                rec.S = S;
+                rec.P = P;
+                rec.E = E;
+                rec.e0 = e0;
+                rec.C = C;
+                rec.nb = nb;
+            }
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            x.round = r1;
+            x.e_total = e_all;
+        }
+        __syncthreads();
+        if (vld(x.overflow)) continue;
+        for (uint32_t q = r0; q < r1; ++q, ++g) {
             if (g % gridDim.x != blockIdx.x) continue;
-            const RoundRecord &rec = x.records[r];
-            if (!__ldcg(&rec.P)) continue;
-            const uint64_t E = __ldcg(&rec.E);
-            uint8_t *o = x.out + roff[r - r0];
-            uint32_t *from = reinterpret_cast<uint32_t *>(o + 12), *to = from + E;
+            if (__ldcg(&x.meta[q].n) == __ldcg(&x.meta[q].s)) continue;  // no prefix: no record
+            const uint64_t Eq = rE[q - r0];
+            uint8_t *o = x.out + roff[q - r0];
+            uint32_t *from = reinterpret_cast<uint32_t *>(o + 12), *to = from + Eq;
             if (threadIdx.x == 0) {  // u64 n, i32 ovlp_len (write_edges_binary, overlap.cu:148-161)
                 uint32_t *h = reinterpret_cast<uint32_t *>(o);
-                h[0] = (uint32_t)E;
-                h[1] = (uint32_t)(E >> 32);
-                h[2] = (uint32_t)(x.L - 1 - (int)r);
+                h[0] = (uint32_t)Eq;
+                h[1] = (uint32_t)(Eq >> 32);
+                h[2] = (uint32_t)(x.L - 1 - (int)q);
             }
-            if (!E) continue;
-            const uint32_t nb = (uint32_t)__ldcg(&rec.nb);
-            const BktSpan *sp = x.spans + (uint64_t)(r - r0) * x.nb_max;
+            if (!Eq) continue;
+            const uint32_t nbq = (uint32_t)rnb[q - r0];
+            const BktSpan *sp = x.spans + (uint64_t)(q - r0) * x.nb_max;
             uint64_t run = 0;
-            for (uint32_t b0 = 0; b0 < nb; b0 += kT) {
+            for (uint32_t b0 = 0; b0 < nbq; b0 += kT) {
                 const uint32_t b = b0 + threadIdx.x;
-                const uint64_t c = b < nb ? __ldcg(&sp[b].cnt) : 0;
+                const uint64_t c = b < nbq ? __ldcg(&sp[b].cnt) : 0;
                 uint64_t tot;
                 const uint64_t ex = block_exclusive_scan<kT, uint64_t>(c, sh.scan64, &tot);
-                if (b < nb) dest[b] = run + ex;
+                if (b < nbq) dest[b] = run + ex;
                 run += tot;
             }
-            if (threadIdx.x == 0) dest[nb] = run;
+            if (threadIdx.x == 0) dest[nbq] = run;
             __syncthreads();
-            for (uint64_t e = threadIdx.x; e < E; e += kT) {
-                uint32_t lo = 0, hi = nb;  // last bucket with dest <= e
+            for (uint64_t e = threadIdx.x; e < Eq; e += kT) {
+                uint32_t lo = 0, hi = nbq;  // last bucket with dest <= e
                 while (hi - lo > 1) {
                     const uint32_t m = (lo + hi) >> 1;
                     if (dest[m] <= e) lo = m;
@@ -1348,6 +1360,7 @@ EMP_COLD void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
             }
             __syncthreads();
         }
+        __syncthreads();
     }
 }
 
@@ -1355,49 +1368,35 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ BShared sh;
     const int J = (int)ctl->njobs;
+    for (uint32_t i = threadIdx.x; i < sizeof(HashTables) / 4; i += kT)
+        reinterpret_cast<uint32_t *>(&sh.tab)[i] = reinterpret_cast<const uint32_t *>(jobs[0].tables)[i];
+    __syncthreads();
     // ---- prologue: the launch's input lists -> round r0's lists
     uint32_t total = build_prefix(sh, J, [&](int j) -> uint32_t { return (uint32_t)bkt_tiles(jobs[j].n_in); });
     tile_loop(sh, &ctl->ticket[0], J, total, [&](int j, uint32_t k) { prologue_tile(jobs[j], k, sh, smem); });
     if (!grid_barrier(ctl, &sh.flag, 0, 7)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        for (int j = 0; j < J; ++j) {  // round r0 runs only with a suffix left
-            BktJob &x = jobs[j];
-            BktIter &N = x.it[1];
-            N.K = vld(x.it[0].nb);
-            N.nb = bkt_count(vld(x.it[0].n), gridDim.x);
-            if (vld(x.it[0].s) == 0 || x.r0 >= x.rounds) {
-                x.end_iter = 0;
-                atomicSub(&ctl->active, 1u);
-            }
-        }
-        __threadfence();
-    }
-    if (!grid_barrier(ctl, &sh.flag, 0, 6)) return;
-    // ---- rounds
+    // ---- rounds: round r0 + iter of every job that still runs
     for (uint32_t iter = 0;; ++iter) {
-        if (vld(ctl->active) == 0) break;
-        const uint32_t cur = iter % 3;
         uint32_t *ticket = &ctl->ticket[1 + (iter & 1)];
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ticket[1 + ((iter + 1) & 1)] = 0;  // last iteration's
         probe(ctl, iter, 0);
         total = build_prefix(sh, J, [&](int j) -> uint32_t {
-            const BktJob &x = jobs[j];
-            return iter < vld(x.end_iter) ? vld(x.it[cur].nb) : 0u;
+            const RoundShape z = round_shape(jobs[j], iter);
+            sh.shp_K[j] = z.K;
+            sh.shp_nb[j] = z.nb;
+            sh.shp_nbn[j] = z.nb_next;
+            return z.active ? z.nb : 0u;
         });
+        if (total == 0) break;  // no job has a round left
         probe(ctl, iter, 1);
         tile_loop_static(sh, ticket, J, total, [&](int j, uint32_t b) {
-            BktJob &x = jobs[j];
-            round_tile(x, b, iter, sh, ctl, smem);
-            __threadfence();
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                const uint32_t nbj = sh.pref[j + 1] - sh.pref[j];
-                if (atomicAdd(&x.it[cur].b_done, 1u) == nbj - 1) {
-                    __threadfence();
-                    round_end(x, ctl, iter);
-                }
-            }
-            __syncthreads();
+            RoundShape z;
+            z.active = true;
+            z.r = jobs[j].r0 + (int)iter;
+            z.K = sh.shp_K[j];
+            z.nb = sh.shp_nb[j];
+            z.nb_next = sh.shp_nbn[j];
+            round_tile(jobs[j], b, iter, z, sh, ctl, smem);
         });
         probe(ctl, iter, 9);
         if (!grid_barrier(ctl, &sh.flag, iter, 0)) return;

@@ -252,15 +252,11 @@ __host__ __device__ inline uint32_t bkt_count(uint64_t n, uint32_t G) {
 __host__ __device__ inline uint32_t bkt_of(uint64_t sk, uint32_t nb) {
     return (uint32_t)(((sk >> 35) * (uint64_t)nb) >> 24);
 }
-struct BktIter {         // one round's list (three slots, by iteration mod 3)
-    uint64_t n;          // entries (an atomic count while the list is written)
+struct BktRound {        // counts of one round (atomic while the round, or its list, is written)
+    uint64_t n;          // entries of the round's list
     uint64_t s;          // of which suffixes
-    uint64_t cands;      // entries found in both tables in this round
-    uint64_t edges;      // edges of this round
-    uint32_t K;          // tiles holding the list
-    uint32_t nb;         // key buckets the tiles are partitioned into
-    uint32_t b_done;     // buckets of this round finished
-    uint32_t pad;
+    uint64_t cands;      // entries found in both tables
+    uint64_t edges;      // edges of the round
 };
 struct BktSpan {         // one bucket's edges in the staging buffer
     uint64_t off, cnt;
@@ -284,12 +280,12 @@ struct BktJob {
     uint8_t *scratch;        // bkt_scratch_bytes(n_max): buckets too big for shared memory
     uint64_t n_max;
     uint32_t nb_max;         // row length of spans
-    uint32_t round;          // next round to run
-    uint32_t end_iter;       // first iteration the job does not run (0xffffffff while running)
+    uint32_t round;          // rounds run (set at the end of the launch)
+    uint32_t pad1;
     uint32_t overflow;       // the edge buffer was too small
     uint64_t e_total;        // edges of the finished rounds of this launch
     uint64_t e_stage;        // staging buffer fill
-    BktIter it[3];
+    BktRound *meta;          // [rounds + 1], zeroed; round r at meta[r]
 };
 size_t bkt_scratch_bytes(uint64_t n_max);
 size_t bkt_offs_words(uint64_t n_max, uint32_t G);  // u32 words of one BktJob::offs buffer
