@@ -16,9 +16,9 @@ each rank runs its own job, no data-path collective):
             output.bin to host, wall clock per step
   roofline  the dominant kernel (the cooperative kernel that runs every
             overlap round in one launch): its algorithmic bytes per launch
-            (per round 16 B per entry read, 16 B written and 16 B gathered per
-            kept entry, 8 B per edge) / its event-timed duration, against the
-            measured HBM copy bandwidth
+            (per round 16 B gathered per entry, 16 B written per entry kept
+            for the next round, 8 B per edge) / its event-timed duration,
+            against the measured HBM copy bandwidth
   cpu_baseline  rank 0 at N=1: the reference's own sources built as a CPU
             program (oracle/_ref, Thrust on OpenMP) on a bounded sample
 impl reference: that CPU build alone, timed per step on the bounded sample
@@ -45,6 +45,25 @@ CPU_SAMPLE_READS = 200_000
 def env_rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(
         os.environ.get("WORLD_SIZE", "1"))
+
+
+def reduce_max_over_ranks(x: float, dist, device) -> float:
+    """The largest x over all ranks (every rank gets it); x itself without a
+    process group.  Timings of replicas are combined this way: the job is as
+    slow as its slowest rank."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, reads_per_rank: int, steps: int, seconds: float) -> float:
+    """Whole-job reads/s of `world` replicas, each running `steps` jobs of
+    `reads_per_rank` reads in `seconds` (the slowest rank's time)."""
+    return world * reads_per_rank * steps / seconds
 
 
 def measured_peaks():
@@ -341,11 +360,8 @@ def main():
     clocks = clk.summary()
     total_ms = sum(step_ms)
     out_bytes = st["output_bytes"]
-    if dist is not None:
-        t = torch.tensor([total_ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * workload.n_reads * args.steps / (total_ms / 1000.0)
+    total_ms = reduce_max_over_ranks(total_ms, dist, f"cuda:{device}")
+    value = replica_throughput(world, workload.n_reads, args.steps, total_ms / 1000.0)
     job.close()
 
     # ---- e2e: host FASTQ in, output.bin out, through the C ABI
@@ -364,11 +380,8 @@ def main():
             e2e_s.append(dt)
     job.close()
     e2e_total = sum(e2e_s)
-    if dist is not None:
-        t = torch.tensor([e2e_total], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * workload.n_reads * len(e2e_s) / e2e_total
+    e2e_total = reduce_max_over_ranks(e2e_total, dist, f"cuda:{device}")
+    e2e_value = replica_throughput(world, workload.n_reads, len(e2e_s), e2e_total)
 
     peak, peak_kind = measured_peaks()
     traffic = traffic_summary()
