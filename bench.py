@@ -259,6 +259,106 @@ def sort_microbench(args):
     eng.close()
 
 
+def batched_bench(args):
+    """Config 4: independent read sets as one batch (emp_batch_run) per step,
+    against the same sets run job by job (emp_job_run each)."""
+    import numpy as np
+    import torch
+
+    import empanada_b200
+    from empanada_b200 import synth
+
+    sets = synth.batched_sets(n_sets=args.batch_sets, genome_max=args.batch_genome_max)
+    sizes = [synth.fastq_size(w) for w in sets]
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    t0 = time.perf_counter()
+    host = torch.empty(int(offs[-1]), dtype=torch.uint8, pin_memory=True)
+    host_np = host.numpy()
+    for w, a, b in zip(sets, offs[:-1], offs[1:]):
+        synth.fastq_into(w, host_np[a:b])
+    gen_s = time.perf_counter() - t0
+    reads = sum(w.n_reads for w in sets)
+    device = 0
+    torch.cuda.set_device(device)
+    stream = torch.cuda.current_stream(device)
+    sptr = stream.cuda_stream
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    eng = empanada_b200.Engine(device)
+    jobs = [eng.job(min_ovlp=w.min_ovlp) for w in sets]
+    for j, a, b in zip(jobs, offs[:-1], offs[1:]):
+        j.reserve(int(b - a))
+        j.feed(host_np[a:b], last=True)
+
+    def timed(fn, steps, warmup):
+        ms = []
+        for i in range(warmup + steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            if i >= warmup:
+                ms.append(e0.elapsed_time(e1))
+        return ms
+
+    with ClockSampler(device) as clk:
+        batch_ms = timed(lambda: eng.run_batch(jobs, sptr), args.steps, args.warmup)
+    clocks = clk.summary()
+    outs = [j.output() for j in jobs]
+    launches = jobs[0].stats()["gpu_launches"]  # the first job's counter spans the whole batch
+    plain_steps = max(1, min(args.steps, 3))
+
+    def plain():
+        for j in jobs:
+            j.run(sptr)
+
+    plain_ms = timed(plain, plain_steps, 1)
+    same = all(j.output() == o for j, o in zip(jobs, outs))
+    for j in jobs:
+        j.close()
+    # e2e: every set's FASTQ from pinned host memory, the batch, every output.bin back
+    out_cap = max(len(o) for o in outs) + 16
+    out_host = torch.empty(out_cap, dtype=torch.uint8, pin_memory=True).numpy()
+    jobs = [eng.job(min_ovlp=w.min_ovlp) for w in sets]
+    for j, a, b in zip(jobs, offs[:-1], offs[1:]):
+        j.reserve(int(b - a))
+    e2e_s = []
+    d2h = 0
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for j, a, b in zip(jobs, offs[:-1], offs[1:]):
+            j.reset()
+            j.feed(host_np[a:b], last=True)
+        eng.run_batch(jobs)
+        d2h = sum(j.output_into(out_host) for j in jobs)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_s.append(dt)
+    for j in jobs:
+        j.close()
+    eng.close()
+    tb = sum(batch_ms) / len(batch_ms)
+    tp = sum(plain_ms) / len(plain_ms)
+    line = {"metric": "reads/s, batched read sets (fingerprint+sort+overlap)", "value": reads / (tb / 1e3),
+            "unit": "reads/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tb,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded generator empanada_b200/csrc/synth_reads.c)",
+            "config": {"workload": f"batched: {len(sets)} read sets, genome log-uniform 50 kbp-"
+                                   f"{args.batch_genome_max // 1000} kbp, read length 100-255, coverage 10-80x, "
+                                   "0.1% substitutions, -o 31",
+                       "reads": reads, "fastq_bytes": int(offs[-1]),
+                       "l2": "inputs larger than L2; 256 MB L2 flush before every timed step"},
+            "plain": {"value": reads / (tp / 1e3), "ms_per_step": tp, "steps": plain_steps,
+                      "what": "the same sets job by job (emp_job_run each), device time"},
+            "batched_over_plain": tp / tb, "outputs_identical": same, "gpu_launches": launches,
+            "e2e": {"value": reads * len(e2e_s) / sum(e2e_s), "unit": "reads/s",
+                    "h2d_bytes_per_step": int(offs[-1]), "d2h_bytes_per_step": int(d2h)},
+            "clocks": clocks, "host_generate_s": gen_s}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -270,8 +370,14 @@ def main():
     ap.add_argument("--kernel", default=None, choices=[None, "sort"],
                     help="microbenchmark one kernel instead of the whole path")
     ap.add_argument("--pairs", type=int, default=1 << 24)
+    ap.add_argument("--batch-sets", type=int, default=256, help="read sets of --workload batched")
+    ap.add_argument("--batch-genome-max", type=int, default=5_000_000,
+                    help="largest genome of --workload batched (log-uniform from 50 kbp)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload == "batched":
+        batched_bench(args)
+        return
 
     from empanada_b200 import synth
 

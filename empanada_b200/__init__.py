@@ -150,6 +150,14 @@ class Engine:
     def job(self, **params) -> "Job":
         return Job(self, _params(**params))
 
+    def run_batch(self, jobs: "list[Job]", stream: int = 0) -> None:
+        """Run independent jobs of this engine as one batch (emp_batch_run):
+        each job's output equals what Job.run gives it alone."""
+        if not jobs:
+            return
+        arr = (ctypes.c_void_p * len(jobs))(*[j.handle for j in jobs])
+        check(self._lib.emp_batch_run(self.handle, arr, len(jobs), stream or None), "emp_batch_run")
+
     def sort_pairs(self, keys_ptr: int, vals_ptr: int, n: int, stream: int = 0) -> None:
         """Stable device sort of (u64 fingerprint, u32 value) pairs in place."""
         check(self._lib.emp_sort_pairs(self.handle, keys_ptr, vals_ptr, n, stream or None), "emp_sort_pairs")

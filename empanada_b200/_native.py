@@ -90,6 +90,7 @@ SIGNATURES = {
     "emp_job_reserve": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "emp_job_reset": (ctypes.c_int, [_vp]),
     "emp_job_run": (ctypes.c_int, [_vp, _vp]),
+    "emp_batch_run": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.c_int, _vp]),
     "emp_job_output_size": (ctypes.c_int, [_vp, _u64p]),
     "emp_job_output_copy": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64]),
     "emp_job_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats)]),

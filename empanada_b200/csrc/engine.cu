@@ -73,6 +73,17 @@ struct emp_ctx {
     DevBuf sort_k1, sort_v1, sort_scr, sort_err;
     uint64_t sort_cap = 0;
     uint64_t sort_calls = 0;
+    // emp_batch_run: the BktJob array and control block of one launch, their
+    // host copies, and the launch's events
+    DevBuf batch_jobs, batch_ctl;
+    PinnedBuf h_batch;
+    cudaEvent_t batch_ev[2] = {};
+};
+
+struct JobPrep {
+    uint64_t n = 0, n_rec = 0, U = 0, M = 0, wpc = 0, ecap = 0, launches0 = 0;
+    int L = 0, wpr = 0, rounds = 0;
+    bool done = false;  // nothing more to run (empty input, no reads)
 };
 
 struct emp_job {
@@ -107,6 +118,9 @@ struct emp_job {
     bool sort_timed = false;
     PinnedBuf h_misc, h_hist, h_from, h_to;
     uint64_t n_ends = 0;
+    // map-phase state (map_begin .. map_list) and its events
+    JobPrep prep;
+    cudaEvent_t map_ev[5] = {};
     // results
     std::vector<uint8_t> out;
     emp_stats st{};
@@ -124,9 +138,8 @@ constexpr emp_status kNeedEdgeRoom = -1000;
 
 emp_status cuda_status(cudaError_t e) { return e == cudaSuccess ? EMP_OK : (e == cudaErrorMemoryAllocation ? EMP_E_NOMEM : EMP_E_CUDA); }
 
-emp_status ensure(emp_job *j, DevBuf &b, size_t bytes) {
+emp_status ctx_ensure(emp_ctx *c, DevBuf &b, size_t bytes) {
     if (bytes <= b.bytes) return EMP_OK;
-    emp_ctx *c = j->ctx;
     const size_t old = b.bytes;
     if (c->budget && c->in_use - old + bytes > c->budget) return EMP_E_NOMEM;
     b.release();
@@ -142,6 +155,8 @@ emp_status ensure(emp_job *j, DevBuf &b, size_t bytes) {
     c->in_use += bytes;
     return EMP_OK;
 }
+
+emp_status ensure(emp_job *j, DevBuf &b, size_t bytes) { return ctx_ensure(j->ctx, b, bytes); }
 
 void free_buf(emp_job *j, DevBuf &b) {
     j->ctx->in_use -= b.bytes;
@@ -622,16 +637,15 @@ emp_status run_rounds_coop(emp_job *j, cudaStream_t s, const RoundEnv &env, cons
     return EMP_OK;
 }
 
-// Rounds r0 .. of one job through the bucket kernel (k_bucket.cu): one
-// cooperative launch, two grid barriers per round.
-emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, int r0, int cur, uint64_t n_in,
-                             uint64_t ecap, uint64_t *needed) {
-    emp_stats &st = j->st;
+// Buffers and launch description (host copy *hj) of rounds r0 .. of one job
+// in the bucket kernel (k_bucket.cu).  `wave`: bucket counts are multiples
+// of it (the grid when the job has the GPU alone, 1 in a batch).
+emp_status bucket_prepare(emp_job *j, cudaStream_t s, const RoundEnv &env, int r0, int cur, uint64_t n_in,
+                          uint64_t ecap, uint32_t wave, BktJob *hj) {
     const uint64_t nmax = n_in;
-    const int grid = bucket_grid_size();
-    const uint64_t ktiles = bkt_max_tiles(nmax, (uint32_t)grid);
-    const uint32_t nb_max = bkt_count(nmax, (uint32_t)grid);
-    const size_t offs_words = bkt_offs_words(nmax, (uint32_t)grid);
+    const uint64_t ktiles = bkt_max_tiles(nmax, wave);
+    const uint32_t nb_max = bkt_count(nmax, wave);
+    const size_t offs_words = bkt_offs_words(nmax, wave);
     EMP_TRY(ensure(j, j->bk_lst0, nmax * sizeof(BktEntry)));
     EMP_TRY(ensure(j, j->bk_lst1, nmax * sizeof(BktEntry)));
     EMP_TRY(ensure(j, j->bk_offs, 2 * offs_words * 4));
@@ -640,18 +654,12 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     EMP_TRY(ensure(j, j->bk_sfrom, ecap * 4));
     EMP_TRY(ensure(j, j->bk_sto, ecap * 4));
     EMP_TRY(ensure(j, j->bk_scratch, bkt_scratch_bytes(nmax)));
-    EMP_TRY(ensure(j, j->bk_job, sizeof(BktJob)));
     EMP_TRY(ensure(j, j->bk_meta, ((size_t)env.rounds + 1) * sizeof(BktRound)));
     EMP_CUDA(cudaMemsetAsync(j->bk_meta.p, 0, ((size_t)env.rounds + 1) * sizeof(BktRound), s));
-    EMP_TRY(ensure(j, j->coop_ctl, sizeof(CoopCtl)));
     EMP_TRY(ensure(j, j->dout, (size_t)env.rounds * 12 + ecap * 8));
     EMP_TRY(ensure(j, j->records, (size_t)env.rounds * sizeof(RoundRecord)));
-    if (!j->h_coop.ensure(sizeof(BktJob) + sizeof(CoopCtl)) ||
-        !j->h_records.ensure((size_t)env.rounds * sizeof(RoundRecord)))
-        return EMP_E_NOMEM;
-    BktJob *hj = j->h_coop.as<BktJob>();
-    CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + 1);
-    std::memset(hj, 0, sizeof(BktJob) + sizeof(CoopCtl));
+    if (!j->h_records.ensure((size_t)env.rounds * sizeof(RoundRecord))) return EMP_E_NOMEM;
+    std::memset(hj, 0, sizeof(BktJob));
     hj->lk_in = cur ? j->lk1.as<uint64_t>() : j->lk0.as<uint64_t>();
     hj->lv_in = cur ? j->lv1.as<uint32_t>() : j->lv0.as<uint32_t>();
     hj->used_s = j->used_s.as<uint8_t>();
@@ -677,8 +685,65 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     hj->scratch = j->bk_scratch.as<uint8_t>();
     hj->n_max = nmax;
     hj->nb_max = nb_max;
+    hj->wave = wave;
     hj->r0 = r0;
     hj->meta = j->bk_meta.as<BktRound>();
+    return EMP_OK;
+}
+
+// Queue the copy of the job's round records to the host.
+emp_status bucket_fetch(emp_job *j, const RoundEnv &env, cudaStream_t s) {
+    EMP_CUDA(cudaMemcpyAsync(j->h_records.p, j->records.p, (size_t)env.rounds * sizeof(RoundRecord),
+                             cudaMemcpyDeviceToHost, s));
+    return EMP_OK;
+}
+
+// After the launch and a synchronisation: the job's counts and output size
+// from its launch description (copied back) and records.  kNeedEdgeRoom with
+// *needed set when its edge buffer was too small.
+emp_status bucket_collect(emp_job *j, int r0, uint64_t n_in, const BktJob &hj, uint64_t *needed) {
+    emp_stats &st = j->st;
+    if (hj.overflow) {
+        *needed = hj.e_total;
+        return kNeedEdgeRoom;
+    }
+    const RoundRecord *rec = j->h_records.as<RoundRecord>();
+    const int r_end = (int)hj.round;  // rounds run with a non-empty suffix table
+    uint64_t prev_n = n_in;
+    for (int q = r0; q < r_end; ++q) {
+        const RoundRecord &x = rec[q];
+        const uint64_t n_out = x.S + x.P;
+        // each round gathers its entries and writes the kept ones for the next
+        st.round_kernel_bytes += 16 * prev_n + 16 * n_out + 8 * x.E;
+        if (q < EMP_MAX_ROUNDS) {
+            st.sfx_live[q] = x.S;
+            st.pfx_live[q] = x.P;
+            st.edges[q] = x.E;
+        }
+        if (x.P) {  // the kernel wrote the record into dout
+            j->dout_bytes += 12 + 8 * x.E;
+            st.n_records += 1;
+        }
+        st.n_edges += x.E;
+        prev_n = n_out;
+    }
+    st.n_rounds = r_end;
+    return EMP_OK;
+}
+
+// Rounds r0 .. of one job alone in the bucket kernel: one cooperative launch,
+// one grid barrier per round.
+emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, int r0, int cur, uint64_t n_in,
+                             uint64_t ecap, uint64_t *needed) {
+    emp_stats &st = j->st;
+    const int grid = bucket_grid_size();
+    EMP_TRY(ensure(j, j->bk_job, sizeof(BktJob)));
+    EMP_TRY(ensure(j, j->coop_ctl, sizeof(CoopCtl)));
+    if (!j->h_coop.ensure(sizeof(BktJob) + sizeof(CoopCtl))) return EMP_E_NOMEM;
+    BktJob *hj = j->h_coop.as<BktJob>();
+    CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + 1);
+    EMP_TRY(bucket_prepare(j, s, env, r0, cur, n_in, ecap, (uint32_t)grid, hj));
+    std::memset(hc, 0, sizeof(CoopCtl));
     hc->njobs = 1;
     hc->active = 1;
     const char *trace_path = std::getenv("EMP_COOP_TRACE");  // profiling: per-phase timestamps
@@ -706,46 +771,17 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     EMP_CUDA(cudaEventRecord(e1, s));
     EMP_CUDA(cudaMemcpyAsync(hj, j->bk_job.p, sizeof(BktJob), cudaMemcpyDeviceToHost, s));
     EMP_CUDA(cudaMemcpyAsync(hc, j->coop_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
-    EMP_CUDA(cudaMemcpyAsync(j->h_records.p, j->records.p, (size_t)env.rounds * sizeof(RoundRecord),
-                             cudaMemcpyDeviceToHost, s));
+    EMP_TRY(bucket_fetch(j, env, s));
     EMP_TRY(sync_and_check(j, s));
     if (hc->err & kErrSpin) return EMP_E_TIMEOUT;
     st.ms_round_kernel += ms_between(e0, e1);
-    if (hj->overflow) {
-        *needed = hj->e_total;
-        return kNeedEdgeRoom;
-    }
-    const RoundRecord *rec = j->h_records.as<RoundRecord>();
-    const int r_end = (int)hj->round;  // rounds run with a non-empty suffix table
-    if (trace_path) write_coop_trace(j, trace_path, env.rounds, r0, rec, s, 1, "round_us");
+    if (trace_path) write_coop_trace(j, trace_path, env.rounds, r0, j->h_records.as<RoundRecord>(), s, 1, "round_us");
     if (probe_env) write_coop_probe(j, probe_path.c_str(), grid, s);
-    uint64_t prev_n = n_in;
-    for (int q = r0; q < r_end; ++q) {
-        const RoundRecord &x = rec[q];
-        const uint64_t n_out = x.S + x.P;
-        // each round gathers its entries and writes the kept ones for the next
-        st.round_kernel_bytes += 16 * prev_n + 16 * n_out + 8 * x.E;
-        if (q < EMP_MAX_ROUNDS) {
-            st.sfx_live[q] = x.S;
-            st.pfx_live[q] = x.P;
-            st.edges[q] = x.E;
-        }
-        if (x.P) {  // the kernel wrote the record into dout
-            j->dout_bytes += 12 + 8 * x.E;
-            st.n_records += 1;
-        }
-        st.n_edges += x.E;
-        prev_n = n_out;
-    }
-    st.n_rounds = r_end;
-    return EMP_OK;
+    return bucket_collect(j, r0, n_in, *hj, needed);
 }
 
-// All rounds: synchronous ones while a round could split into several search
-// partitions (sizes only shrink), then the device-resident pipeline for the
-// rest with a single synchronisation at the end.  Returns kNeedEdgeRoom with
-// *needed set when the pipeline's edge buffer (ecap edges) was too small.
-emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t U, uint64_t ecap, uint64_t *needed) {
+// Round counters, output and used marks of a job, before its rounds.
+emp_status rounds_prelude(emp_job *j, cudaStream_t s) {
     emp_stats &st = j->st;
     st.n_rounds = 0;
     st.n_edges = 0;
@@ -757,6 +793,16 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
     j->dout_bytes = 0;
     EMP_CUDA(cudaMemsetAsync(j->used_s.p, 0, j->used_s.bytes, s));
     EMP_CUDA(cudaMemsetAsync(j->used_p.p, 0, j->used_p.bytes, s));
+    return EMP_OK;
+}
+
+// All rounds: synchronous ones while a round could split into several search
+// partitions (sizes only shrink), then the device-resident pipeline for the
+// rest with a single synchronisation at the end.  Returns kNeedEdgeRoom with
+// *needed set when the pipeline's edge buffer (ecap edges) was too small.
+emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t U, uint64_t ecap, uint64_t *needed) {
+    emp_stats &st = j->st;
+    EMP_TRY(rounds_prelude(j, s));
     int cur = 0, r = 0;
     uint64_t n_in = 2 * U, S = U, P = U;
     const uint64_t M = env.M;
@@ -886,105 +932,132 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
     return EMP_OK;
 }
 
-emp_status run_job(emp_job *j, cudaStream_t s) {
+// The map phase of a job, in stages that each end where the host must read
+// a count before sizing the next step (one stream synchronisation between
+// stages; a batch of jobs shares it).  A stage returns EMP_OK with j->prep.done
+// set once the job has nothing more to run.
+emp_status map_begin(emp_job *j, cudaStream_t s) {
     emp_stats &st = j->st;
     std::memset(&st, 0, sizeof st);
     j->out.clear();
     j->dout_bytes = 0;
     j->have_result = false;
     j->n_ends = 0;
+    j->prep = JobPrep{};
     st.fastq_bytes = j->F;
     st.ms_h2d = j->ms_h2d;
-    const uint64_t launches0 = g_launches.load();
-    const uint64_t M = j->p.reduce_mem / 16;
-    if (M < 2) return EMP_E_INVAL;
-    const uint64_t F = j->F;
-    const HashTables *tables = j->ctx->tables.as<HashTables>();
-    Events ev;
-    cudaEventRecord(ev.e[0], s);
-
+    j->prep.launches0 = g_launches.load();
+    j->prep.M = j->p.reduce_mem / 16;
+    if (j->prep.M < 2) return EMP_E_INVAL;
+    cudaEventRecord(j->map_ev[0], s);
     EMP_TRY(ensure(j, j->misc, kMiscSlots * sizeof(uint64_t)));
     if (!j->h_misc.ensure(kMiscSlots * sizeof(uint64_t)) || !j->h_hist.ensure(kSortPasses * kSortRadix * 4))
         return EMP_E_NOMEM;
+    EMP_CUDA(cudaMemsetAsync(j->misc.p, 0, kMiscSlots * sizeof(uint64_t), s));
+    const uint64_t F = j->F;
+    if (!F) return EMP_OK;
+    // ---- K1: newline index
+    const uint64_t T = parse_tiles(F);
+    EMP_TRY(ensure(j, j->tile_counts, T * 4));
+    EMP_TRY(ensure(j, j->tile_excl, T * 8));
+    launch_nl_count(j->fq.as<uint8_t>(), F, j->tile_counts.as<uint32_t>(), s);
+    EMP_TRY(reset_chain(j, scan_tiles(T), s));
+    launch_scan_u32_u64(j->tile_counts.as<uint32_t>(), j->tile_excl.as<uint64_t>(), T, j->status.as<uint64_t>(),
+                        chain_ctr(j), j->misc.as<uint64_t>() + kMiscTotal, err_word(j), s);
+    return EMP_OK;
+}
+
+// queue the copy of the job's device words that the next stage reads
+emp_status map_fetch(emp_job *j, cudaStream_t s) {
+    EMP_CUDA(cudaMemcpyAsync(j->h_misc.p, j->misc.p, kMiscSlots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    return EMP_OK;
+}
+emp_status map_check(emp_job *j) {
+    return (j->h_misc.as<uint64_t>()[kMiscErr] & kErrSpin) ? EMP_E_TIMEOUT : EMP_OK;
+}
+
+// nothing (more) to run: close the job's timings
+void map_finish_empty(emp_job *j, cudaStream_t s) {
+    cudaEventRecord(j->map_ev[4], s);
+    j->prep.done = true;
+}
+
+emp_status map_records(emp_job *j, cudaStream_t s) {
+    EMP_TRY(map_check(j));
     uint64_t *hm = j->h_misc.as<uint64_t>();
     uint64_t *dm = j->misc.as<uint64_t>();
-    EMP_CUDA(cudaMemsetAsync(j->misc.p, 0, kMiscSlots * sizeof(uint64_t), s));
-
-    uint64_t n = 0, n_rec = 0;
-    int L = 0;
-    if (F) {
-        // ---- K1: newline index
-        const uint64_t T = parse_tiles(F);
-        EMP_TRY(ensure(j, j->tile_counts, T * 4));
-        EMP_TRY(ensure(j, j->tile_excl, T * 8));
-        launch_nl_count(j->fq.as<uint8_t>(), F, j->tile_counts.as<uint32_t>(), s);
-        EMP_TRY(reset_chain(j, scan_tiles(T), s));
-        launch_scan_u32_u64(j->tile_counts.as<uint32_t>(), j->tile_excl.as<uint64_t>(), T, j->status.as<uint64_t>(),
-                            chain_ctr(j), dm + kMiscTotal, err_word(j), s);
-        EMP_TRY(sync_and_check(j, s));
-        const uint64_t total_nl = hm[kMiscTotal];
-        n_rec = total_nl ? (total_nl + 3) / 4 : 0;
-        if (n_rec) {
-            EMP_TRY(ensure(j, j->seq_start, n_rec * 8));
-            EMP_TRY(ensure(j, j->seq_end, n_rec * 8));
-            launch_nl_locate(j->fq.as<uint8_t>(), F, j->tile_excl.as<uint64_t>(), j->seq_start.as<uint64_t>(),
-                             j->seq_end.as<uint64_t>(), s);
-            if ((total_nl - 1) % 4 == 0) {  // last sequence line ends at end of input
-                hm[kMiscSlots - 1] = F;
-                EMP_CUDA(cudaMemcpyAsync(j->seq_end.as<uint64_t>() + n_rec - 1, hm + kMiscSlots - 1, 8,
-                                         cudaMemcpyHostToDevice, s));
-            }
-            // ---- K2a: classify records
-            EMP_TRY(ensure(j, j->hq, n_rec * 4));
-            EMP_TRY(ensure(j, j->idx, n_rec * 4));
-            const uint32_t mm[2] = {0xffffffffu, 0u};
-            std::memcpy(hm + kMiscLen, mm, 8);
-            EMP_CUDA(cudaMemcpyAsync(dm + kMiscLen, hm + kMiscLen, 8, cudaMemcpyHostToDevice, s));
-            launch_classify(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->seq_end.as<uint64_t>(), n_rec,
-                            j->hq.as<uint32_t>(), reinterpret_cast<uint32_t *>(dm + kMiscLen), err_word(j), s);
-            EMP_TRY(reset_chain(j, scan_tiles(n_rec), s));
-            launch_scan_u32_u32(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), n_rec, j->status.as<uint64_t>(),
-                                chain_ctr(j), dm + kMiscN, err_word(j), s);
-            EMP_TRY(sync_and_check(j, s));
-            if (hm[kMiscErr] & kErrBadBase) return EMP_E_FORMAT;
-            n = hm[kMiscN];
-            uint32_t mm2[2];
-            std::memcpy(mm2, hm + kMiscLen, 8);
-            if (n) {
-                if (mm2[0] != mm2[1]) return EMP_E_FORMAT;
-                L = (int)mm2[0];
-                if (mm2[0] > (uint32_t)kMaxReadLen) return EMP_E_UNSUPPORTED;
-            }
-        }
+    const uint64_t F = j->F;
+    const uint64_t total_nl = F ? hm[kMiscTotal] : 0;
+    const uint64_t n_rec = total_nl ? (total_nl + 3) / 4 : 0;
+    j->prep.n_rec = n_rec;
+    if (!n_rec) {
+        map_finish_empty(j, s);
+        return EMP_OK;
     }
+    EMP_TRY(ensure(j, j->seq_start, n_rec * 8));
+    EMP_TRY(ensure(j, j->seq_end, n_rec * 8));
+    launch_nl_locate(j->fq.as<uint8_t>(), F, j->tile_excl.as<uint64_t>(), j->seq_start.as<uint64_t>(),
+                     j->seq_end.as<uint64_t>(), s);
+    if ((total_nl - 1) % 4 == 0) {  // last sequence line ends at end of input
+        hm[kMiscSlots - 1] = F;
+        EMP_CUDA(cudaMemcpyAsync(j->seq_end.as<uint64_t>() + n_rec - 1, hm + kMiscSlots - 1, 8,
+                                 cudaMemcpyHostToDevice, s));
+    }
+    // ---- K2a: classify records
+    EMP_TRY(ensure(j, j->hq, n_rec * 4));
+    EMP_TRY(ensure(j, j->idx, n_rec * 4));
+    const uint32_t mm[2] = {0xffffffffu, 0u};
+    std::memcpy(hm + kMiscLen, mm, 8);
+    EMP_CUDA(cudaMemcpyAsync(dm + kMiscLen, hm + kMiscLen, 8, cudaMemcpyHostToDevice, s));
+    launch_classify(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->seq_end.as<uint64_t>(), n_rec,
+                    j->hq.as<uint32_t>(), reinterpret_cast<uint32_t *>(dm + kMiscLen), err_word(j), s);
+    EMP_TRY(reset_chain(j, scan_tiles(n_rec), s));
+    launch_scan_u32_u32(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), n_rec, j->status.as<uint64_t>(), chain_ctr(j),
+                        dm + kMiscN, err_word(j), s);
+    return EMP_OK;
+}
+
+emp_status map_keys(emp_job *j, cudaStream_t s) {
+    EMP_TRY(map_check(j));
+    JobPrep &q = j->prep;
+    uint64_t *hm = j->h_misc.as<uint64_t>();
+    uint64_t *dm = j->misc.as<uint64_t>();
+    emp_stats &st = j->st;
+    if (hm[kMiscErr] & kErrBadBase) return EMP_E_FORMAT;
+    const uint64_t n = hm[kMiscN];
+    uint32_t mm2[2];
+    std::memcpy(mm2, hm + kMiscLen, 8);
+    int L = 0;
+    if (n) {
+        if (mm2[0] != mm2[1]) return EMP_E_FORMAT;
+        L = (int)mm2[0];
+        if (mm2[0] > (uint32_t)kMaxReadLen) return EMP_E_UNSUPPORTED;
+    }
+    q.n = n;
+    q.L = L;
     st.n_reads = n;
     st.read_len = L;
     if (n == 0) {
-        cudaEventRecord(ev.e[4], s);
-        EMP_CUDA(cudaStreamSynchronize(s));
-        st.ms_total = ms_between(ev.e[0], ev.e[4]);
-        st.gpu_launches = g_launches.load() - launches0;
-        j->have_result = true;
+        map_finish_empty(j, s);
         return EMP_OK;
     }
     if (j->p.min_ovlp < 0) return EMP_E_INVAL;
     const uint64_t n2 = 2 * n;
     if (n2 >= (1ull << 31)) return EMP_E_UNSUPPORTED;
-    if (n2 > M) return EMP_E_UNSUPPORTED;  // out-of-core merge-tree order not emulated yet
-
+    if (n2 > q.M) return EMP_E_UNSUPPORTED;  // out-of-core merge-tree order not emulated yet
+    const HashTables *tables = j->ctx->tables.as<HashTables>();
     // ---- K2b: fingerprints + 2-bit column store
-    const uint64_t wpc = (n + 15) / 16;
+    q.wpc = (n + 15) / 16;
+    q.wpr = (L + 15) / 16;
     EMP_TRY(ensure(j, j->rec_of, n * 4));
-    EMP_TRY(ensure(j, j->cols, (uint64_t)L * wpc * 4));
-    const int wpr = (L + 15) / 16;
-    EMP_TRY(ensure(j, j->seq2, (uint64_t)n * wpr * 4));
+    EMP_TRY(ensure(j, j->cols, (uint64_t)L * q.wpc * 4));
+    EMP_TRY(ensure(j, j->seq2, (uint64_t)n * q.wpr * 4));
     EMP_TRY(ensure(j, j->keys0, n2 * 8));
-    launch_scatter_hq(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), n_rec, j->rec_of.as<uint32_t>(), s);
+    launch_scatter_hq(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), q.n_rec, j->rec_of.as<uint32_t>(), s);
     launch_fingerprint_pack(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->rec_of.as<uint32_t>(), n, L, tables,
-                            j->keys0.as<uint64_t>(), j->cols.as<uint32_t>(), wpc, j->seq2.as<uint32_t>(), wpr, s);
+                            j->keys0.as<uint64_t>(), j->cols.as<uint32_t>(), q.wpc, j->seq2.as<uint32_t>(), q.wpr, s);
     j->n_ends = n2;
-    cudaEventRecord(ev.e[1], s);
-
+    cudaEventRecord(j->map_ev[1], s);
     // ---- fingerprint sort + duplicate removal (overlap.cu:212-225)
     const uint64_t cap = 2 * n2;  // both tables, each at most n2 entries
     EMP_TRY(ensure(j, j->sk0, cap * 8));
@@ -1006,47 +1079,210 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
     EMP_TRY(reset_chain(j, upd_tiles(n2), s));
     launch_init_list(j->keys0.as<uint64_t>(), j->alive.as<uint8_t>(), n, j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(),
                      j->status.as<uint64_t>(), chain_ctr(j), dm + kMiscU, err_word(j), s);
-    EMP_TRY(sync_and_check(j, s));
-    account_sort(j);
-    const uint64_t U = hm[kMiscU];
-    st.n_unique = U;
-    launch_dup_prefix_half(j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(), U, s);
-    cudaEventRecord(ev.e[2], s);
+    return EMP_OK;
+}
 
-    // ---- overlap rounds (overlap.cu:258-290)
-    const int rounds = L - j->p.min_ovlp;
-    if (rounds > 0) {
-        // the pipeline may need a larger edge buffer: keep the initial list to restart
-        EMP_TRY(ensure(j, j->lk_init, 2 * U * 8 + 8));
-        EMP_TRY(ensure(j, j->lv_init, 2 * U * 4 + 4));
-        EMP_CUDA(cudaMemcpyAsync(j->lk_init.p, j->lk0.p, 2 * U * 8, cudaMemcpyDeviceToDevice, s));
-        EMP_CUDA(cudaMemcpyAsync(j->lv_init.p, j->lv0.p, 2 * U * 4, cudaMemcpyDeviceToDevice, s));
-        uint64_t ecap = j->ecap_hint ? j->ecap_hint : (4 * U > (1u << 20) ? 4 * U : (1u << 20));
-        if (const char *ec = std::getenv("EMP_EDGE_CAP")) ecap = std::strtoull(ec, nullptr, 10) + 1;
-        const RoundEnv env{L, rounds, M, wpc, tables, j->seq2.as<uint32_t>(), wpr};
-        for (int attempt = 0;; ++attempt) {
-            uint64_t needed = 0;
-            emp_status rc = run_rounds(j, s, env, U, ecap, &needed);
-            if (rc == EMP_OK) break;
-            if (rc != kNeedEdgeRoom || attempt >= 2) return rc == kNeedEdgeRoom ? EMP_E_NOMEM : rc;
-            ecap = needed + needed / 4 + 1024;
-            j->ecap_hint = ecap;
-            EMP_CUDA(cudaMemcpyAsync(j->lk0.p, j->lk_init.p, 2 * U * 8, cudaMemcpyDeviceToDevice, s));
-            EMP_CUDA(cudaMemcpyAsync(j->lv0.p, j->lv_init.p, 2 * U * 4, cudaMemcpyDeviceToDevice, s));
-        }
+// The initial list (suffixes then prefixes) is ready; the rounds environment
+// follows.  Also keeps the list for a restart with a larger edge buffer.
+emp_status map_list(emp_job *j, cudaStream_t s) {
+    EMP_TRY(map_check(j));
+    JobPrep &q = j->prep;
+    account_sort(j);
+    const uint64_t U = j->h_misc.as<uint64_t>()[kMiscU];
+    q.U = U;
+    j->st.n_unique = U;
+    launch_dup_prefix_half(j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(), U, s);
+    cudaEventRecord(j->map_ev[2], s);
+    q.rounds = q.L - j->p.min_ovlp;
+    if (q.rounds <= 0) return EMP_OK;
+    EMP_TRY(ensure(j, j->lk_init, 2 * U * 8 + 8));
+    EMP_TRY(ensure(j, j->lv_init, 2 * U * 4 + 4));
+    EMP_CUDA(cudaMemcpyAsync(j->lk_init.p, j->lk0.p, 2 * U * 8, cudaMemcpyDeviceToDevice, s));
+    EMP_CUDA(cudaMemcpyAsync(j->lv_init.p, j->lv0.p, 2 * U * 4, cudaMemcpyDeviceToDevice, s));
+    q.ecap = j->ecap_hint ? j->ecap_hint : (4 * U > (1u << 20) ? 4 * U : (1u << 20));
+    if (const char *ec = std::getenv("EMP_EDGE_CAP")) q.ecap = std::strtoull(ec, nullptr, 10) + 1;
+    return EMP_OK;
+}
+
+RoundEnv job_env(emp_job *j) {
+    const JobPrep &q = j->prep;
+    return RoundEnv{q.L, q.rounds, q.M, q.wpc, j->ctx->tables.as<HashTables>(), j->seq2.as<uint32_t>(), q.wpr};
+}
+
+// All rounds of one job, restarting with a larger edge buffer when needed.
+emp_status job_rounds(emp_job *j, cudaStream_t s) {
+    JobPrep &q = j->prep;
+    if (q.rounds <= 0) return EMP_OK;
+    const RoundEnv env = job_env(j);
+    for (int attempt = 0;; ++attempt) {
+        uint64_t needed = 0;
+        emp_status rc = run_rounds(j, s, env, q.U, q.ecap, &needed);
+        if (rc == EMP_OK) return EMP_OK;
+        if (rc != kNeedEdgeRoom || attempt >= 2) return rc == kNeedEdgeRoom ? EMP_E_NOMEM : rc;
+        q.ecap = needed + needed / 4 + 1024;
+        j->ecap_hint = q.ecap;
+        EMP_CUDA(cudaMemcpyAsync(j->lk0.p, j->lk_init.p, 2 * q.U * 8, cudaMemcpyDeviceToDevice, s));
+        EMP_CUDA(cudaMemcpyAsync(j->lv0.p, j->lv_init.p, 2 * q.U * 4, cudaMemcpyDeviceToDevice, s));
     }
-    cudaEventRecord(ev.e[3], s);
-    cudaEventRecord(ev.e[4], s);
+}
+
+// Timings and counts of a finished job (after its stream is synchronised).
+void job_finish(emp_job *j) {
+    emp_stats &st = j->st;
+    if (!j->prep.done) {
+        st.ms_map = ms_between(j->map_ev[0], j->map_ev[1]);
+        st.ms_dedup = ms_between(j->map_ev[1], j->map_ev[2]);
+        st.ms_rounds = ms_between(j->map_ev[2], j->map_ev[3]);
+    }
+    st.ms_total = ms_between(j->map_ev[0], j->map_ev[4]);
+    st.output_bytes = j->out.size() + j->dout_bytes;
+    st.gpu_launches = g_launches.load() - j->prep.launches0;
+    j->have_result = true;
+}
+
+emp_status run_job(emp_job *j, cudaStream_t s) {
+    EMP_TRY(map_begin(j, s));
+    EMP_TRY(map_fetch(j, s));
+    EMP_CUDA(cudaStreamSynchronize(s));
+    EMP_TRY(map_records(j, s));
+    if (!j->prep.done) {
+        EMP_TRY(sync_and_check(j, s));
+        EMP_TRY(map_keys(j, s));
+    }
+    if (!j->prep.done) {
+        EMP_TRY(sync_and_check(j, s));
+        EMP_TRY(map_list(j, s));
+        EMP_TRY(job_rounds(j, s));
+        cudaEventRecord(j->map_ev[3], s);
+        cudaEventRecord(j->map_ev[4], s);
+    }
     EMP_TRY(sync_and_check(j, s));
     EMP_CUDA(cudaGetLastError());
-    st.ms_map = ms_between(ev.e[0], ev.e[1]);
-    st.ms_dedup = ms_between(ev.e[1], ev.e[2]);
-    st.ms_rounds = ms_between(ev.e[2], ev.e[3]);
-    st.ms_total = ms_between(ev.e[0], ev.e[4]);
-    st.output_bytes = j->out.size() + j->dout_bytes;
-    st.gpu_launches = g_launches.load() - launches0;
-    j->have_result = true;
+    job_finish(j);
     return EMP_OK;
+}
+
+// ---- batches -------------------------------------------------------------
+
+// A job's rounds can join a batched bucket launch when all of them fit the
+// bucket kernel from round 0: no round could split into several search
+// partitions (S, P < M/2) and the list fits the kernel.
+bool batch_eligible(const emp_job *j) {
+    const JobPrep &q = j->prep;
+    return q.rounds > 0 && q.U < q.M / 2 && 2 * q.U <= kBktMaxEntries && !std::getenv("EMP_SYNC_ROUNDS") &&
+           !std::getenv("EMP_NO_COOP") && !std::getenv("EMP_NO_BUCKET");
+}
+
+// The rounds of jobs[idx[..]] (all eligible, lists ready) in one launch of
+// the bucket kernel; per-job status in rc.  A job whose edge buffer was too
+// small runs its rounds again alone with a larger one.
+emp_status batch_rounds(emp_ctx *ctx, emp_job **jobs, const std::vector<int> &idx, std::vector<emp_status> &rc,
+                        cudaStream_t s) {
+    const size_t nb = idx.size();
+    EMP_TRY(ctx_ensure(ctx, ctx->batch_jobs, nb * sizeof(BktJob)));
+    EMP_TRY(ctx_ensure(ctx, ctx->batch_ctl, sizeof(CoopCtl)));
+    if (!ctx->h_batch.ensure(nb * sizeof(BktJob) + sizeof(CoopCtl))) return EMP_E_NOMEM;
+    if (!ctx->batch_ev[0]) {
+        for (auto &e : ctx->batch_ev) EMP_CUDA(cudaEventCreate(&e));
+    }
+    BktJob *hj = ctx->h_batch.as<BktJob>();
+    CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + nb);
+    for (size_t k = 0; k < nb; ++k) {
+        emp_job *j = jobs[idx[k]];
+        const JobPrep &q = j->prep;
+        EMP_TRY(rounds_prelude(j, s));
+        EMP_TRY(bucket_prepare(j, s, job_env(j), 0, 0, 2 * q.U, q.ecap, 1u, &hj[k]));
+    }
+    std::memset(hc, 0, sizeof(CoopCtl));
+    hc->njobs = (uint32_t)nb;
+    hc->active = (uint32_t)nb;
+    EMP_CUDA(cudaMemcpyAsync(ctx->batch_jobs.p, hj, nb * sizeof(BktJob), cudaMemcpyHostToDevice, s));
+    EMP_CUDA(cudaMemcpyAsync(ctx->batch_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
+    EMP_CUDA(cudaEventRecord(ctx->batch_ev[0], s));
+    EMP_CUDA(launch_bucket_rounds(ctx->batch_jobs.as<BktJob>(), ctx->batch_ctl.as<CoopCtl>(),
+                                  err_word(jobs[idx[0]]), s));
+    EMP_CUDA(cudaEventRecord(ctx->batch_ev[1], s));
+    EMP_CUDA(cudaMemcpyAsync(hj, ctx->batch_jobs.p, nb * sizeof(BktJob), cudaMemcpyDeviceToHost, s));
+    EMP_CUDA(cudaMemcpyAsync(hc, ctx->batch_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
+    for (size_t k = 0; k < nb; ++k) EMP_TRY(bucket_fetch(jobs[idx[k]], job_env(jobs[idx[k]]), s));
+    EMP_CUDA(cudaStreamSynchronize(s));
+    if (hc->err & kErrSpin) return EMP_E_TIMEOUT;
+    const float ms = ms_between(ctx->batch_ev[0], ctx->batch_ev[1]);
+    for (size_t k = 0; k < nb; ++k) {
+        emp_job *j = jobs[idx[k]];
+        JobPrep &q = j->prep;
+        j->st.ms_round_kernel += ms;  // the whole batch's launch
+        uint64_t needed = 0;
+        emp_status r = bucket_collect(j, 0, 2 * q.U, hj[k], &needed);
+        if (r == kNeedEdgeRoom) {  // alone again, with room for every edge
+            q.ecap = needed + needed / 4 + 1024;
+            j->ecap_hint = q.ecap;
+            r = job_rounds(j, s);
+        }
+        rc[idx[k]] = r;
+    }
+    return EMP_OK;
+}
+
+// Every job of a batch through the map phase (one synchronisation per stage
+// for the whole batch), the rounds of the eligible ones in one bucket-kernel
+// launch, the others' rounds one job after another.
+emp_status run_batch(emp_ctx *ctx, emp_job **jobs, int n, cudaStream_t s) {
+    std::vector<emp_status> rc((size_t)n, EMP_OK);
+    auto live = [&](int i) { return rc[i] == EMP_OK && !jobs[i]->prep.done; };
+    auto fail = [&](int i, emp_status e) {
+        if (rc[i] == EMP_OK) rc[i] = e;
+    };
+    for (int i = 0; i < n; ++i) {
+        fail(i, map_begin(jobs[i], s));
+        if (rc[i] == EMP_OK) fail(i, map_fetch(jobs[i], s));
+    }
+    EMP_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < n; ++i) {
+        if (!live(i)) continue;
+        fail(i, map_records(jobs[i], s));
+        if (live(i)) fail(i, map_fetch(jobs[i], s));
+    }
+    EMP_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < n; ++i) {
+        if (!live(i)) continue;
+        fail(i, map_keys(jobs[i], s));
+        if (live(i)) fail(i, map_fetch(jobs[i], s));
+    }
+    EMP_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> batch, alone;
+    for (int i = 0; i < n; ++i) {
+        if (!live(i)) continue;
+        fail(i, map_list(jobs[i], s));
+        if (!live(i)) continue;
+        if (batch_eligible(jobs[i])) batch.push_back(i);
+        else alone.push_back(i);
+    }
+    if (!batch.empty()) {
+        const emp_status e = batch_rounds(ctx, jobs, batch, rc, s);
+        if (e != EMP_OK)
+            for (int i : batch) fail(i, e);
+    }
+    for (int i : alone) fail(i, job_rounds(jobs[i], s));
+    for (int i = 0; i < n; ++i) {
+        if (!live(i)) continue;
+        cudaEventRecord(jobs[i]->map_ev[3], s);
+        cudaEventRecord(jobs[i]->map_ev[4], s);
+    }
+    for (int i = 0; i < n; ++i)
+        if (rc[i] == EMP_OK) fail(i, map_fetch(jobs[i], s));
+    EMP_CUDA(cudaStreamSynchronize(s));
+    EMP_CUDA(cudaGetLastError());
+    emp_status first = EMP_OK;
+    for (int i = 0; i < n; ++i) {
+        if (rc[i] == EMP_OK) fail(i, map_check(jobs[i]));
+        if (rc[i] == EMP_OK) job_finish(jobs[i]);
+        else {
+            jobs[i]->have_result = false;
+            if (first == EMP_OK) first = rc[i];
+        }
+    }
+    return first;
 }
 
 }  // namespace
@@ -1158,6 +1394,9 @@ emp_status emp_ctx_destroy(emp_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
+    for (auto &e : ctx->batch_ev)
+        if (e) cudaEventDestroy(e);
+    ctx->in_use -= ctx->batch_jobs.bytes + ctx->batch_ctl.bytes;
     delete ctx;
     return EMP_OK;
 }
@@ -1177,6 +1416,12 @@ emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out) {
         }
     }
     for (auto &e : j->upd_ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            emp_job_destroy(j);
+            return EMP_E_CUDA;
+        }
+    }
+    for (auto &e : j->map_ev) {
         if (cudaEventCreate(&e) != cudaSuccess) {
             emp_job_destroy(j);
             return EMP_E_CUDA;
@@ -1205,6 +1450,8 @@ emp_status emp_job_destroy(emp_job *job) {
     for (auto &e : job->sort_ev)
         if (e) cudaEventDestroy(e);
     for (auto &e : job->upd_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : job->map_ev)
         if (e) cudaEventDestroy(e);
     release_graph(job);
     delete job;
@@ -1295,6 +1542,24 @@ emp_status emp_job_run(emp_job *job, void *stream) {
         cudaStreamSynchronize(s);
         cudaGetLastError();
         job->have_result = false;
+    }
+    return st;
+}
+
+emp_status emp_batch_run(emp_ctx *ctx, emp_job **jobs, int njobs, void *stream) {
+    if (!ctx || njobs < 0 || (njobs && !jobs) || njobs > kCoopMaxJobs) return EMP_E_INVAL;
+    for (int i = 0; i < njobs; ++i) {
+        if (!jobs[i] || jobs[i]->ctx != ctx) return EMP_E_INVAL;
+        for (int k = 0; k < i; ++k)
+            if (jobs[k] == jobs[i]) return EMP_E_INVAL;
+    }
+    if (!njobs) return EMP_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return EMP_E_CUDA;
+    cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
+    emp_status st = run_batch(ctx, jobs, njobs, s);
+    if (st != EMP_OK) {
+        cudaStreamSynchronize(s);
+        cudaGetLastError();
     }
     return st;
 }

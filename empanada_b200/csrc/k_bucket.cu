@@ -242,7 +242,7 @@ EMP_DEV uint64_t step_key(const StepArgs &a, uint64_t key, uint32_t val, uint32_
 EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
     BktRound &I = J.meta[J.r0];
     const uint64_t n_in = J.n_in;
-    const uint32_t nb = bkt_count(n_in, gridDim.x), nbin = 2 * nb, stride = nbin + 1;
+    const uint32_t nb = bkt_count(n_in, J.wave), nbin = 2 * nb, stride = nbin + 1;
     const StepArgs a = step_args(J, sh.tab, J.r0, true);
     uint32_t *hist = reinterpret_cast<uint32_t *>(smem);
     uint4 *stage = reinterpret_cast<uint4 *>(smem + 2 * kBktMaxBuckets * 4);
@@ -1191,10 +1191,10 @@ EMP_DEV RoundShape round_shape(const BktJob &J, uint32_t iter) {
     z.active = z.r < J.rounds && __ldcg(&J.meta[z.r].s) > 0;
     z.K = z.nb = z.nb_next = 0;
     if (!z.active) return z;
-    z.nb = iter ? bkt_count(__ldcg(&J.meta[z.r - 1].n), gridDim.x) : bkt_count(J.n_in, gridDim.x);
+    z.nb = iter ? bkt_count(__ldcg(&J.meta[z.r - 1].n), J.wave) : bkt_count(J.n_in, J.wave);
     z.K = iter == 0 ? (uint32_t)bkt_tiles(J.n_in)
-                    : (iter == 1 ? bkt_count(J.n_in, gridDim.x) : bkt_count(__ldcg(&J.meta[z.r - 2].n), gridDim.x));
-    z.nb_next = bkt_count(__ldcg(&J.meta[z.r].n), gridDim.x);
+                    : (iter == 1 ? bkt_count(J.n_in, J.wave) : bkt_count(__ldcg(&J.meta[z.r - 2].n), J.wave));
+    z.nb_next = bkt_count(__ldcg(&J.meta[z.r].n), J.wave);
     return z;
 }
 
@@ -1296,7 +1296,7 @@ EMP_COLD void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
             P = __ldcg(&m.n) - S;
             E = P ? __ldcg(&m.edges) : 0;
             C = __ldcg(&m.cands);
-            nb = r == r0 ? bkt_count(x.n_in, gridDim.x) : bkt_count(__ldcg(&x.meta[r - 1].n), gridDim.x);
+            nb = r == r0 ? bkt_count(x.n_in, x.wave) : bkt_count(__ldcg(&x.meta[r - 1].n), x.wave);
         }
         uint64_t e_all, bytes;
         const uint64_t e0 = block_exclusive_scan<kT, uint64_t>(E, sh.scan64, &e_all);

@@ -281,7 +281,7 @@ struct BktJob {
     uint64_t n_max;
     uint32_t nb_max;         // row length of spans
     uint32_t round;          // rounds run (set at the end of the launch)
-    uint32_t pad1;
+    uint32_t wave;           // bucket counts are multiples of this (the grid for a job alone)
     uint32_t overflow;       // the edge buffer was too small
     uint64_t e_total;        // edges of the finished rounds of this launch
     uint64_t e_stage;        // staging buffer fill

@@ -86,6 +86,25 @@ OUT_OF_CORE = Workload("out_of_core: 100 Mbp genome (5% repeat families), 150 bp
                        repeat_frac=0.05, min_ovlp=31, map_mem="1g", reduce_mem="1g")
 WORKLOADS = {"small": SMALL, "larger": LARGER, "out_of_core": OUT_OF_CORE}
 
+
+def batched_sets(n_sets: int = 256, seed: int = 4, genome_min: int = 50_000, genome_max: int = 5_000_000,
+                 len_min: int = 100, len_max: int = 255, cov_min: float = 10.0, cov_max: float = 80.0,
+                 sub_rate: float = 0.001, min_ovlp: int = 31) -> list[Workload]:
+    """Independent read sets of a batch: genome size log-uniform in
+    [genome_min, genome_max], read length uniform in [len_min, len_max]
+    (fixed within a set), coverage uniform in [cov_min, cov_max], uniform
+    substitutions at sub_rate, each set with its own seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_sets):
+        g = int(round(np.exp(rng.uniform(np.log(genome_min), np.log(genome_max)))))
+        L = int(rng.integers(len_min, len_max + 1))
+        cov = float(rng.uniform(cov_min, cov_max))
+        n = max(1, int(g * cov / L))
+        out.append(Workload(f"set{k}: {g} bp genome, {n} x {L} bp", seed=seed * 1_000_003 + k, genome_len=g,
+                            n_reads=n, read_len=L, sub_rate=sub_rate, min_ovlp=min_ovlp))
+    return out
+
 _lib = None
 
 

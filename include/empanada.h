@@ -125,6 +125,16 @@ emp_status emp_job_reset(emp_job *job);
  * (overlap.cu:206-293).  stream: a cudaStream_t, or NULL for the context's. */
 emp_status emp_job_run(emp_job *job, void *stream);
 
+/* emp_job_run of njobs independent jobs of one context (at most 1024, each
+ * once) as one batch: the map phase of every job with one stream
+ * synchronisation per stage for the whole batch, and the rounds of all jobs
+ * whose lists fit the bucket kernel in a single launch of it.  Replaces one
+ * run of the reference's whole program (main.cu:42-71, then build_graph,
+ * overlap.cu:206-293) per read set; each job's output is byte-identical to
+ * emp_job_run's.  Returns the first failing job's status (jobs that failed
+ * have no result; the others do), EMP_OK when all succeeded. */
+emp_status emp_batch_run(emp_ctx *ctx, emp_job **jobs, int njobs, void *stream);
+
 /* output.bin bytes of the last run (write_edges_binary, overlap.cu:148-161). */
 emp_status emp_job_output_size(emp_job *job, uint64_t *bytes);
 emp_status emp_job_output_copy(emp_job *job, void *dst, uint64_t cap);
