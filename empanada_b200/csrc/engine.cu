@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <string>
 #include <vector>
 
@@ -98,6 +99,7 @@ struct emp_job {
     DevBuf tile_counts, tile_excl, status, misc, seq_start, seq_end, hq, idx, rec_of, keys0, cols, seq2;
     DevBuf sk0, sv0, sk1, sv1, alive, lk0, lv0, lk1, lv1, used_s, used_p, cnt, offs, efrom, eto, sort_scratch;
     DevBuf akeys, apos, bkeys, parts;  // record splitting
+    DevBuf xk0, xv0, xk1, xv1, ring_k, ring_v, cparts;  // sort of a table larger than M
     PinnedBuf h_parts;
     // device-resident round pipeline
     DevBuf lk_init, lv_init, bloom_s, bloom_p, ck, cv, ck2, cv2, records, st_upd, st_cand, st_scan, ctl;
@@ -257,6 +259,55 @@ void timed_sort(emp_job *j, uint64_t n, cudaStream_t s) {
                j->sort_scratch.p, j->misc.as<uint64_t>() + kMiscSortN, err_word(j), s, j->sort_ev);
 }
 
+// stable sort of (k, v)[0..n) in place through (k1, v1), on the job's sort scratch
+void seg_sort(emp_job *j, uint64_t *k, uint32_t *v, uint64_t *k1, uint32_t *v1, uint64_t n, cudaStream_t s) {
+    ++j->sorts_since_clear;
+    sort_pairs(k, v, k1, v1, n, j->sort_scratch.p, j->misc.as<uint64_t>() + kMiscSortN, err_word(j), s);
+}
+
+// The reference's fingerprint sort of a table of n > M entries
+// (cq_sort_by_key, cqutils.cuh:180-247; kernels in k_chunked.cu), in place
+// on (k, v)[0..n), which hold the table in list order; (k1, v1): n entries
+// of scratch.  lst: the table's list values for the read-end ranks that cut
+// the chunks, null for the initial table (ids 0..n-1 in order).
+emp_status chunked_sort(emp_job *j, uint64_t *k, uint32_t *v, uint64_t *k1, uint32_t *v1, uint64_t n, uint64_t M,
+                        const uint32_t *lst, cudaStream_t s) {
+    const uint64_t C = 2 * n, h = M / 2;
+    EMP_TRY(ensure(j, j->xk0, n * 8));
+    EMP_TRY(ensure(j, j->xv0, n * 4));
+    EMP_TRY(ensure(j, j->xk1, n * 8));
+    EMP_TRY(ensure(j, j->xv1, n * 4));
+    EMP_TRY(ensure(j, j->ring_k, C * 8));
+    EMP_TRY(ensure(j, j->ring_v, C * 4));
+    const uint64_t pcap = n / (h ? h : 1) + 8;  // partitions of one merge of at most n entries
+    EMP_TRY(ensure(j, j->cparts, pcap * sizeof(ChunkPart)));
+    // sorted by key, then (stably) by chunk: each chunk sorted on its own
+    seg_sort(j, k, v, k1, v1, n, s);
+    launch_chunk_keys(v, n, lst, M, j->xk0.as<uint64_t>(), j->xv0.as<uint32_t>(), s);
+    seg_sort(j, j->xk0.as<uint64_t>(), j->xv0.as<uint32_t>(), j->xk1.as<uint64_t>(), j->xv1.as<uint32_t>(), n, s);
+    uint64_t *rk = j->ring_k.as<uint64_t>();
+    uint32_t *rv = j->ring_v.as<uint32_t>();
+    launch_ring_gather(k, v, j->xv0.as<uint32_t>(), n, rk, rv, s);
+    // the FIFO of sorted tables (ring start, entries), oldest first
+    std::deque<std::pair<uint64_t, uint64_t>> q;
+    for (uint64_t off = 0; off < n; off += M) q.emplace_back(off, n - off < M ? n - off : M);
+    uint64_t tail = n;  // ring position after the newest table
+    uint64_t *count = j->misc.as<uint64_t>() + kMiscParts;
+    while (q.size() > 1) {
+        const auto a = q.front();
+        q.pop_front();
+        const auto b = q.front();
+        q.pop_front();
+        const uint64_t no = a.second + b.second;
+        launch_merge(rk, rv, C, a.first, a.second, b.first, b.second, tail, h, j->cparts.as<ChunkPart>(), pcap,
+                     count, err_word(j), s);
+        q.emplace_back(tail, no);
+        tail = (tail + no) % C;
+    }
+    launch_ring_copy(rk, rv, C, q.front().first, n, k, v, s);
+    return EMP_OK;
+}
+
 // Record `ne` edges from the host edge arrays into output.bin (overlap.cu:148-161).
 void emit_record(emp_job *j, int32_t ovlp, uint64_t e0, uint64_t e1) {
     const uint64_t ne = e1 - e0;
@@ -328,9 +379,17 @@ emp_status sync_round(emp_job *j, cudaStream_t s, const RoundEnv &env, int r, in
     st.n_rounds = r + 1;
     if (P == 0) return EMP_OK;  // one-sided search partition: no record
     const bool split = S >= M / 2 || P >= M / 2;
-    // sort a copy of the merged list (the list itself carries over)
+    // sort a copy of the merged list (the list itself carries over); a table
+    // larger than M first takes the order of the reference's chunked sort,
+    // which the stable sort of both tables then keeps among equal keys
     EMP_CUDA(cudaMemcpyAsync(j->sk0.p, lk[cur], N * 8, cudaMemcpyDeviceToDevice, s));
     EMP_CUDA(cudaMemcpyAsync(j->sv0.p, lv[cur], N * 4, cudaMemcpyDeviceToDevice, s));
+    if (S > M)
+        EMP_TRY(chunked_sort(j, j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), j->sk1.as<uint64_t>(),
+                             j->sv1.as<uint32_t>(), S, M, lv[cur], s));
+    if (P > M)
+        EMP_TRY(chunked_sort(j, j->sk0.as<uint64_t>() + S, j->sv0.as<uint32_t>() + S, j->sk1.as<uint64_t>() + S,
+                             j->sv1.as<uint32_t>() + S, P, M, lv[cur] + S, s));
     timed_sort(j, N, s);
     const uint64_t *sk = j->sk0.as<uint64_t>();
     const uint32_t *sv = j->sv0.as<uint32_t>();
@@ -1044,7 +1103,6 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
     if (j->p.min_ovlp < 0) return EMP_E_INVAL;
     const uint64_t n2 = 2 * n;
     if (n2 >= (1ull << 31)) return EMP_E_UNSUPPORTED;
-    if (n2 > q.M) return EMP_E_UNSUPPORTED;  // out-of-core merge-tree order not emulated yet
     const HashTables *tables = j->ctx->tables.as<HashTables>();
     // ---- K2b: fingerprints + 2-bit column store
     q.wpc = (n + 15) / 16;
@@ -1074,7 +1132,13 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
     EMP_TRY(ensure_sort_scratch(j, cap, s));
     EMP_CUDA(cudaMemcpyAsync(j->sk0.p, j->keys0.p, n2 * 8, cudaMemcpyDeviceToDevice, s));
     launch_iota(j->sv0.as<uint32_t>(), n2, s);
-    timed_sort(j, n2, s);
+    if (n2 > q.M) {  // chunked sort and its duplicate-removal walk (2n > M)
+        EMP_TRY(chunked_sort(j, j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), j->sk1.as<uint64_t>(),
+                             j->sv1.as<uint32_t>(), n2, q.M, nullptr, s));
+        launch_unique_walk(j->sk0.as<uint64_t>(), n2, q.M, err_word(j), s);
+    } else {
+        timed_sort(j, n2, s);
+    }
     launch_dedup_mark(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), n2, j->alive.as<uint8_t>(), s);
     EMP_TRY(reset_chain(j, upd_tiles(n2), s));
     launch_init_list(j->keys0.as<uint64_t>(), j->alive.as<uint8_t>(), n, j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(),
@@ -1087,6 +1151,8 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
 emp_status map_list(emp_job *j, cudaStream_t s) {
     EMP_TRY(map_check(j));
     JobPrep &q = j->prep;
+    if (j->h_misc.as<uint64_t>()[kMiscErr] & kErrHang) return EMP_E_HANG;
+    if (j->h_misc.as<uint64_t>()[kMiscErr] & kErrCapacity) return EMP_E_UNSUPPORTED;
     account_sort(j);
     const uint64_t U = j->h_misc.as<uint64_t>()[kMiscU];
     q.U = U;
@@ -1445,7 +1511,8 @@ emp_status emp_job_destroy(emp_job *job) {
                       &job->st_sort, &job->coop_job, &job->coop_ctl, &job->coop_trace,
                       &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_offs, &job->bk_tile_base, &job->bk_spans,
                       &job->bk_sfrom, &job->bk_sto, &job->bk_scratch, &job->bk_job, &job->dout,
-                      &job->bk_meta};
+                      &job->bk_meta, &job->xk0, &job->xv0, &job->xk1, &job->xv1, &job->ring_k, &job->ring_v,
+                      &job->cparts};
     for (DevBuf *b : bufs) free_buf(job, *b);
     for (auto &e : job->sort_ev)
         if (e) cudaEventDestroy(e);

@@ -74,6 +74,31 @@ void sort_pairs_prepared(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1,
 int sort_pairs(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, uint64_t n, void *scratch, uint64_t *n_dev,
                uint32_t *err, cudaStream_t s, cudaEvent_t *pass_events = nullptr);
 
+// ---- sort of a table larger than M (k_chunked.cu) --------------------------
+struct ChunkPart {  // one merge partition: A entries [a0, a0+pa), B entries [b0, b0+pb)
+    uint64_t a0, pa, b0, pb;
+};
+// Chunk of each entry of (v)[0..n) as a sort key ((rank / M) << 32) with its
+// index: rank = read-end id when lst is null (the table holds ids 0..n-1 in
+// order), else the entry's rank among the ids of lst (the table in list
+// order: even ids ascending, then odd ids ascending).
+void launch_chunk_keys(const uint32_t *v, uint64_t n, const uint32_t *lst, uint64_t M, uint64_t *ck, uint32_t *ci,
+                       cudaStream_t s);
+// (rk, rv)[i] = (k, v)[idx[i]], i < n
+void launch_ring_gather(const uint64_t *k, const uint32_t *v, const uint32_t *idx, uint64_t n, uint64_t *rk,
+                        uint32_t *rv, cudaStream_t s);
+// (k, v)[i] = ring entry start + i (ring of C entries), i < n
+void launch_ring_copy(const uint64_t *rk, const uint32_t *rv, uint64_t C, uint64_t start, uint64_t n, uint64_t *k,
+                      uint32_t *v, cudaStream_t s);
+// Merge ring tables A (start sa, nA entries) and B into the one at so, along
+// the reference's merge partitions of windows h; parts: room for cap.
+void launch_merge(uint64_t *rk, uint32_t *rv, uint64_t C, uint64_t sa, uint64_t nA, uint64_t sb, uint64_t nB,
+                  uint64_t so, uint64_t h, ChunkPart *parts, uint64_t cap, uint64_t *count, uint32_t *err,
+                  cudaStream_t s);
+// kErrHang when the reference's duplicate-removal partition walk over the
+// sorted keys k[0..n) stops advancing.
+void launch_unique_walk(const uint64_t *k, uint64_t n, uint64_t M, uint32_t *err, cudaStream_t s);
+
 // ---- rounds (k_round.cu) --------------------------------------------------
 void launch_dedup_mark(const uint64_t *skeys, const uint32_t *svals, uint64_t n2, uint8_t *alive, cudaStream_t s);
 // rid order (evens ascending, then odds ascending) of the alive read-ends

@@ -127,6 +127,31 @@ def edge_sub_errors() -> bytes:
     return fastq(_reads(rng, _genome(rng, 15000), 2000, 120, sub=0.01))
 
 
+def edge_ooc_dups() -> bytes:
+    """Duplicated and reverse-complemented reads spread over the file, so equal
+    fingerprints fall into different M-chunks of the reference's sort."""
+    rng = random.Random(21)
+    g = _genome(rng, 6000)
+    reads = _reads(rng, g, 1500, 64, sub=0.002)
+    out = reads[:]
+    for k in range(400):
+        d = reads[rng.randrange(len(reads))]
+        out.insert(rng.randrange(len(out) + 1), revcomp(d) if k % 3 == 0 else d)
+    return fastq(out)
+
+
+def edge_ooc_hang() -> bytes:
+    """1100 copies of one read among others: with -r 16k (M = 1024) the
+    reference's duplicate-removal partition walk meets a run of 1100 equal
+    keys that fills its window and stops advancing."""
+    rng = random.Random(22)
+    g = _genome(rng, 4000)
+    reads = _reads(rng, g, 300, 50)
+    out = reads + [reads[7]] * 1100
+    rng.shuffle(out)
+    return fastq(out)
+
+
 @dataclasses.dataclass(frozen=True)
 class Case:
     name: str
@@ -175,6 +200,15 @@ CASES = [
     Case("o_ge_L", ("-o", "100"), edge="lowercase"),
     Case("split_r128k", ("-o", "31", "-r", "128k"), synth=TINY),
     Case("out_of_core_r16k", ("-o", "31", "-r", "16k"), synth=TINY),
+    Case("out_of_core_r4k", ("-o", "31", "-r", "4k"), synth=TINY),
+    Case("out_of_core_r1k_odd", ("-o", "27", "-r", "1040"), synth={"seed": 103, "genome_len": 8_000,
+                                                                    "n_reads": 700, "read_len": 60,
+                                                                    "sub_rate": 0.002}),
+    Case("out_of_core_dups_r16k", ("-o", "20", "-r", "16k"), edge="ooc_dups"),
+    Case("out_of_core_repeats_r32k", ("-o", "25", "-r", "32k"),
+         synth={"seed": 104, "genome_len": 60_000, "n_reads": 5000, "read_len": 90, "sub_rate": 0.001,
+                "repeat_frac": 0.2, "rep_min_len": 300, "rep_max_len": 900, "rep_min_copies": 2,
+                "rep_max_copies": 12, "rep_divergence": 0.002}),
     Case("small", ("-o", "31"), synth={}, big=True),
     Case("larger", ("-o", "75", "-m", "8g", "-r", "12g", "-b", "16m", "-c", "64m"),
          synth={"seed": 2, "genome_len": 5_000_000, "n_reads": 1_200_000, "read_len": 250, "sub_rate": 0.001},

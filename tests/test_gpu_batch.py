@@ -1,7 +1,8 @@
 """emp_batch_run: every job of a batch gives the bytes it gives alone.
 
-The golden cases (reference digests) run as one batch, including a job the
-engine rejects (2n > M) and jobs with no reads or no rounds; synthetic read
+The golden cases (reference digests) run as one batch, including jobs with
+no reads or no rounds and out-of-core ones (2n > M); a failing job leaves
+the others their results; synthetic read
 sets of the batched workload's kind (mixed genome sizes, read lengths and
 coverages) are compared with their own emp_job_run outputs.
 """
@@ -18,7 +19,7 @@ from empanada_b200 import _native, synth
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 GOLDEN = json.load(open(os.path.join(HERE, "golden.json")))
 
-BATCH_CASES = [c.name for c in CASES if not c.big and c.name != "out_of_core_r16k"] + ["small"]
+BATCH_CASES = [c.name for c in CASES if not c.big] + ["small"]
 
 
 def _job(engine, case):
@@ -52,14 +53,18 @@ def test_batch_of_golden_cases_matches_reference(engine):
 
 @pytest.mark.gpu
 def test_batch_failure_leaves_other_jobs(engine):
-    """A job the engine rejects fails alone: the batch returns its status and
-    the other jobs have their results."""
-    names = ["tiny", "out_of_core_r16k", "sub_errors"]
-    jobs = [_job(engine, BY_NAME[n]) for n in names]
+    """A job that fails (here: input on which the reference never
+    terminates) fails alone: the batch returns its status and the other jobs
+    have their results."""
+    import cases
+
+    jobs = [_job(engine, BY_NAME["tiny"]), engine.job(min_ovlp=20, reduce_mem="16k"),
+            _job(engine, BY_NAME["sub_errors"])]
+    jobs[1].feed(cases.edge_ooc_hang())
     try:
         with pytest.raises(_native.EmpError) as ei:
             engine.run_batch(jobs)
-        assert ei.value.code == _native.EMP_E_UNSUPPORTED
+        assert ei.value.code == _native.EMP_E_HANG
         assert _digest(jobs[0]) == GOLDEN["tiny"]["sha256"]
         assert _digest(jobs[2]) == GOLDEN["sub_errors"]["sha256"]
         with pytest.raises(_native.EmpError):

@@ -98,6 +98,18 @@ def test_oracle_errors():
     assert e.value.code == bind.E_INVAL
 
 
+def test_oracle_duplicate_walk_hang():
+    """A run of equal keys that fills the reference's duplicate-removal window
+    (cq_get_partitions never advances): the oracle reports the hang."""
+    import cases
+
+    with pytest.raises(bind.OracleError) as e:
+        bind.run(cases.edge_ooc_hang(), 20, 16 << 10)
+    assert e.value.code == bind.E_HANG
+    out, _ = bind.run(cases.edge_ooc_hang(), 20, 1 << 30)  # in core: no walk
+    assert len(out) > 0
+
+
 @pytest.mark.skipif(not os.path.exists(bind.REF_CPU), reason="reference not built here (needs its sources)")
 @pytest.mark.parametrize("seed", range(6))
 def test_oracle_matches_reference_random(seed):
