@@ -346,7 +346,7 @@ def batched_bench(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (seeded generator empanada_b200/csrc/synth_reads.c)",
             "config": {"workload": f"batched: {len(sets)} read sets, genome log-uniform 50 kbp-"
-                                   f"{args.batch_genome_max // 1000} kbp, read length 100-255, coverage 10-80x, "
+                                   f"{args.batch_genome_max // 1000} kbp, read length 100-300, coverage 10-80x, "
                                    "0.1% substitutions, -o 31",
                        "reads": reads, "fastq_bytes": int(offs[-1]),
                        "l2": "inputs larger than L2; 256 MB L2 flush before every timed step"},

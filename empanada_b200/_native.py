@@ -21,7 +21,7 @@ EMP_E_STATE = -6
 EMP_E_IO = -7
 EMP_E_UNSUPPORTED = -8
 EMP_E_HANG = -9
-MAX_ROUNDS = 256
+MAX_ROUNDS = 512
 
 # every function include/empanada.h declares, with its ctypes signature
 _u64p = ctypes.POINTER(ctypes.c_uint64)

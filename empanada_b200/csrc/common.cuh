@@ -22,7 +22,12 @@ constexpr uint32_t kP2 = 536870879u;  // 2^29 - 33
 constexpr uint32_t kR1 = 5u;
 constexpr uint32_t kR2 = 7u;
 constexpr uint32_t kMask29 = (1u << 29) - 1u;
-constexpr int kMaxReadLen = 255;      // MAX_RD_LEN, assembly.cuh:17
+// Longest read.  The reference's MAX_RD_LEN (assembly.cuh:17) is 255: its u8
+// lengths and 256-entry power tables overflow beyond it, so its results are
+// undefined there.  Here the same exact hash runs on to 512 bases, with the
+// power tables extended to match.
+constexpr int kMaxReadLen = 512;
+constexpr int kRefMaxReadLen = 255;
 
 // Error bits raised by kernels into the job's device error word.
 enum ErrBits : uint32_t {
@@ -32,7 +37,7 @@ enum ErrBits : uint32_t {
     kErrHang = 8u,      // the reference would loop forever on this input
 };
 
-// Powers R^i mod P for i <= 255 and the radix inverses (fingerprint.cu:26-34,
+// Powers R^i mod P for i <= kMaxReadLen and the radix inverses (fingerprint.cu:26-34,
 // overlap.cu:121-122).  Lives in device memory; staged into shared memory by
 // the kernels that need it.
 struct HashTables {

@@ -861,6 +861,9 @@ emp_status rounds_prelude(emp_job *j, cudaStream_t s) {
 // *needed set when the pipeline's edge buffer (ecap edges) was too small.
 emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t U, uint64_t ecap, uint64_t *needed) {
     emp_stats &st = j->st;
+    if (!j->upd_ev[0]) {  // per-round events, made when a job first runs rounds on its own
+        for (auto &e : j->upd_ev) EMP_CUDA(cudaEventCreate(&e));
+    }
     EMP_TRY(rounds_prelude(j, s));
     int cur = 0, r = 0;
     uint64_t n_in = 2 * U, S = U, P = U;
@@ -1476,12 +1479,6 @@ emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out) {
     else emp_params_default(&j->p);
     cudaSetDevice(ctx->device);
     for (auto &e : j->sort_ev) {
-        if (cudaEventCreate(&e) != cudaSuccess) {
-            emp_job_destroy(j);
-            return EMP_E_CUDA;
-        }
-    }
-    for (auto &e : j->upd_ev) {
         if (cudaEventCreate(&e) != cudaSuccess) {
             emp_job_destroy(j);
             return EMP_E_CUDA;

@@ -136,9 +136,9 @@ __global__ void scatter_hq_kernel(const uint32_t *__restrict__ hq, const uint32_
         if (hq[k]) rec_of[idx[k]] = (uint32_t)k;
 }
 
-constexpr int kFpReads = 128;  // reads per CTA (8 warps x 16)
-constexpr int kFpRow = 256;    // shared-memory row stride of the code tile
-
+// PER: bases per lane at most (L <= 32 PER); READS reads per CTA (8 warps,
+// READS / 8 reads each), their 2-bit codes staged in a READS x 32 PER tile.
+template <int PER, int READS>
 __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__restrict__ fq,
                                                                const uint64_t *__restrict__ seq_start,
                                                                const uint32_t *__restrict__ rec_of, uint64_t n,
@@ -147,25 +147,26 @@ __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__
                                                                uint32_t *__restrict__ cols, uint64_t wpc,
                                                                uint32_t *__restrict__ seq2, int wpr) {
     __shared__ uint32_t s_pow1[kMaxReadLen + 1], s_pow2[kMaxReadLen + 1];
-    __shared__ uint8_t s_codes[kFpReads * kFpRow];
+    constexpr int kFpRow = 32 * PER, kRowsPerWarp = READS / 8, kGroups = READS / 16;
+    __shared__ uint8_t s_codes[READS * kFpRow];
     for (int i = threadIdx.x; i <= kMaxReadLen; i += blockDim.x) {
         s_pow1[i] = tables->pow1[i];
         s_pow2[i] = tables->pow2[i];
     }
     __syncthreads();
-    const uint64_t i0 = (uint64_t)blockIdx.x * kFpReads;
+    const uint64_t i0 = (uint64_t)blockIdx.x * READS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = (L + 31) >> 5;  // bases per lane, <= 8
+    const int per = (L + 31) >> 5;  // bases per lane, <= PER
     const int a = min(lane * per, L), b = min(a + per, L);
-    for (int m = 0; m < 16; ++m) {
-        const int row = warp * 16 + m;
+    for (int m = 0; m < kRowsPerWarp; ++m) {
+        const int row = warp * kRowsPerWarp + m;
         const uint64_t i = i0 + row;
         if (i >= n) break;
         const uint8_t *s = fq + seq_start[rec_of[i]];
-        uint32_t cod[8];
+        uint32_t cod[PER];
         uint32_t hf1 = 0, hf2 = 0, hr1 = 0, hr2 = 0;
 #pragma unroll
-        for (int jj = 0; jj < 8; ++jj) {
+        for (int jj = 0; jj < PER; ++jj) {
             const int j = a + jj;
             cod[jj] = 0;
             if (j < b) {
@@ -177,7 +178,7 @@ __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__
             }
         }
 #pragma unroll
-        for (int jj = 7; jj >= 0; --jj) {
+        for (int jj = PER - 1; jj >= 0; --jj) {
             if (a + jj < b) {
                 const uint32_t e = (cod[jj] ^ 2u) + 1u;  // complement
                 hr1 = horner1(hr1, e);
@@ -207,8 +208,8 @@ __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__
     }
     __syncthreads();
     const uint64_t w0 = i0 >> 4;
-    for (int p = threadIdx.x; p < L * 8; p += blockDim.x) {
-        const int col = p >> 3, q = p & 7;
+    for (int p = threadIdx.x; p < L * kGroups; p += blockDim.x) {
+        const int col = p / kGroups, q = p % kGroups;
         if (w0 + q >= wpc) continue;
         uint32_t word = 0;
 #pragma unroll
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__
     }
     if (!seq2) return;
     // read-major copy: word w of read i holds positions 16w .. 16w+15
-    for (int p = threadIdx.x; p < kFpReads * wpr; p += blockDim.x) {
+    for (int p = threadIdx.x; p < READS * wpr; p += blockDim.x) {
         const int row = p / wpr, w = p - row * wpr;
         if (i0 + row >= n) break;
         uint32_t word = 0;
@@ -268,10 +269,15 @@ void launch_fingerprint_pack(const uint8_t *fq, const uint64_t *seq_start, const
                              int L, const HashTables *tables, uint64_t *keys, uint32_t *cols, uint64_t wpc,
                              uint32_t *seq2, int wpr, cudaStream_t s) {
     if (!n) return;
-    const uint64_t blocks = (n + kFpReads - 1) / kFpReads;
     count_launch();
-    fingerprint_pack_kernel<<<(unsigned)blocks, 256, 0, s>>>(fq, seq_start, rec_of, n, L, tables, keys, cols, wpc,
-                                                              seq2, wpr);
+    if (L <= 256) {
+        fingerprint_pack_kernel<8, 128><<<(unsigned)((n + 127) / 128), 256, 0, s>>>(fq, seq_start, rec_of, n, L, tables,
+                                                                                 keys, cols, wpc, seq2, wpr);
+    } else {
+        static_assert(kMaxReadLen <= 512, "16 bases per lane");
+        fingerprint_pack_kernel<16, 64><<<(unsigned)((n + 63) / 64), 256, 0, s>>>(fq, seq_start, rec_of, n, L, tables,
+                                                                               keys, cols, wpc, seq2, wpr);
+    }
 }
 
 }  // namespace emp

@@ -88,7 +88,7 @@ WORKLOADS = {"small": SMALL, "larger": LARGER, "out_of_core": OUT_OF_CORE}
 
 
 def batched_sets(n_sets: int = 256, seed: int = 4, genome_min: int = 50_000, genome_max: int = 5_000_000,
-                 len_min: int = 100, len_max: int = 255, cov_min: float = 10.0, cov_max: float = 80.0,
+                 len_min: int = 100, len_max: int = 300, cov_min: float = 10.0, cov_max: float = 80.0,
                  sub_rate: float = 0.001, min_ovlp: int = 31) -> list[Workload]:
     """Independent read sets of a batch: genome size log-uniform in
     [genome_min, genome_max], read length uniform in [len_min, len_max]

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define EMP_ABI_VERSION 1
+#define EMP_ABI_VERSION 2
 
 typedef int emp_status;
 #define EMP_OK 0
@@ -41,7 +41,7 @@ typedef int emp_status;
 #define EMP_E_FORMAT (-5)      /* kept reads of unequal length, or a base outside ACGTacgt */
 #define EMP_E_STATE (-6)       /* call out of order (e.g. feed after run) */
 #define EMP_E_IO (-7)          /* file could not be read or written */
-#define EMP_E_UNSUPPORTED (-8) /* read length above 255 (reference: undefined) */
+#define EMP_E_UNSUPPORTED (-8) /* read length above 512 (the reference stops at 255; above it its result is undefined) */
 #define EMP_E_HANG (-9)        /* input on which the reference never terminates */
 
 typedef struct emp_ctx emp_ctx;
@@ -56,7 +56,7 @@ typedef struct emp_params {
     uint64_t kv_chunksz;   /* -c, count (default 64m) */
 } emp_params;
 
-#define EMP_MAX_ROUNDS 256
+#define EMP_MAX_ROUNDS 512
 
 typedef struct emp_stats {
     uint64_t n_reads;      /* reads kept after the N filter */

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libempanada_oracle.so")
 REF_CPU = os.path.join(HERE, "_ref", "empanada_ref_cpu")
 REF_GPU = os.path.join(HERE, "_ref", "empanada_ref_gpu")
-MAX_ROUNDS = 256
+MAX_ROUNDS = 512
 
 OK, E_INVAL, E_NOMEM, E_FORMAT, E_UNSUPPORTED, E_HANG = 0, -1, -2, -5, -8, -9
 

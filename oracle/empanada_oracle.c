@@ -29,8 +29,9 @@
  * Inputs on which the reference loops forever (a run of >= M equal keys in
  * cq_get_partitions, or a (0,0) search partition) return EMP_ORACLE_E_HANG.
  * Inputs on which the reference's result is undefined (unequal read lengths,
- * bases outside ACGTacgt that survive the N filter, reads longer than 255)
- * return EMP_ORACLE_E_FORMAT / EMP_ORACLE_E_UNSUPPORTED.
+ * bases outside ACGTacgt that survive the N filter) return EMP_ORACLE_E_FORMAT;
+ * reads longer than 512 return EMP_ORACLE_E_UNSUPPORTED (lengths 256-512 are
+ * the reference's undefined range, extended with the same exact hash).
  */
 #include "empanada_oracle.h"
 
@@ -42,7 +43,11 @@
 #define PRIME2 536870879u
 #define RADIX1 5u
 #define RADIX2 7u
-#define MAX_RD_LEN 255
+/* The reference's MAX_RD_LEN (assembly.cuh:17) is 255; beyond it its u8
+ * lengths and 256-entry power tables overflow and its result is undefined.
+ * This restatement carries the same exact hash on to 512 bases (the CUDA
+ * path's limit), so reads of 256-512 bases are checked against it alone. */
+#define MAX_RD_LEN 512
 
 static uint32_t MOD1[MAX_RD_LEN + 1], MOD2[MAX_RD_LEN + 1];
 static uint32_t INV1, INV2;

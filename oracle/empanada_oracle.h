@@ -25,10 +25,10 @@ extern "C" {
 #define EMP_ORACLE_E_INVAL (-1)
 #define EMP_ORACLE_E_NOMEM (-2)
 #define EMP_ORACLE_E_FORMAT (-5)      /* unequal read lengths / unsupported base */
-#define EMP_ORACLE_E_UNSUPPORTED (-8) /* read length above 255 */
+#define EMP_ORACLE_E_UNSUPPORTED (-8) /* read length above 512 */
 #define EMP_ORACLE_E_HANG (-9)        /* input on which the reference never terminates */
 
-#define EMP_ORACLE_MAX_ROUNDS 256
+#define EMP_ORACLE_MAX_ROUNDS 512
 
 typedef struct emp_oracle_stats {
     uint64_t n_reads;        /* reads kept after the N filter */

@@ -109,9 +109,10 @@ def test_batch_reuse_and_repeat(engine):
 
 @pytest.mark.gpu
 def test_batch_of_synthetic_sets_matches_single_runs(engine):
-    """64 read sets of mixed genome size (20-300 kbp), read length (100-255)
-    and coverage (10-80x) with 0.1 % substitutions, as one batch and one by one."""
-    sets = synth.batched_sets(n_sets=64, seed=11, genome_min=20_000, genome_max=300_000)
+    """64 read sets of mixed genome size (20-300 kbp), read length (100-300)
+    and coverage (10-80x) with 0.1 % substitutions, as one batch and one by
+    one; two of them also against the oracle."""
+    sets = synth.batched_sets(n_sets=64, seed=11, genome_min=20_000, genome_max=300_000, len_max=300)
     jobs = []
     try:
         for w in sets:
@@ -123,6 +124,12 @@ def test_batch_of_synthetic_sets_matches_single_runs(engine):
         for w, j, g in zip(sets, jobs, got):
             j.run()
             assert j.output() == g, w.name
+        from oracle import bind
+
+        small = sorted(range(len(sets)), key=lambda k: sets[k].n_reads)[:2]
+        for k in small:
+            ref, _ = bind.run(synth.fastq_bytes(sets[k]), sets[k].min_ovlp)
+            assert got[k] == ref, sets[k].name
     finally:
         for j in jobs:
             j.close()

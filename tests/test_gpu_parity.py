@@ -120,11 +120,56 @@ def test_duplicate_walk_hang_is_reported(engine):
     assert out == ref
 
 
+def _long_reads(L, n, seed, sub=0.002):
+    """Reads beyond the reference's MAX_RD_LEN (its result is undefined
+    there): checked against the oracle's extension of the same hash."""
+    from empanada_b200 import synth
+
+    w = synth.Workload(f"L{L}", seed=seed, genome_len=max(4 * L, n * L // 12), n_reads=n, read_len=L, sub_rate=sub)
+    return synth.fastq_bytes(w)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,o", [(256, 31), (300, 31), (384, 200), (512, 31), (512, 500)])
+def test_long_reads_match_oracle(engine, L, o):
+    data = _long_reads(L, 3000, seed=L + o)
+    out, st = empanada_b200.run_bytes(data, engine=engine, min_ovlp=o)
+    ref, rst = bind.run(data, o)
+    assert st["read_len"] == L
+    assert out == ref
+    assert st["n_edges"] == rst["n_edges"] and st["n_rounds"] == rst["n_rounds"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["sync_rounds", "graph_rounds", "coop_rounds", "split_r64k"])
+def test_long_reads_round_paths(engine, monkeypatch, mode):
+    if mode == "sync_rounds":
+        monkeypatch.setenv("EMP_SYNC_ROUNDS", "1")
+    if mode == "graph_rounds":
+        monkeypatch.setenv("EMP_NO_COOP", "1")
+    if mode == "coop_rounds":
+        monkeypatch.setenv("EMP_NO_BUCKET", "1")
+    r = 64 << 10 if mode == "split_r64k" else 1 << 30
+    data = _long_reads(300, 2500, seed=7)
+    out, _ = empanada_b200.run_bytes(data, engine=engine, min_ovlp=40, reduce_mem=r)
+    ref, _ = bind.run(data, 40, r)
+    assert out == ref
+
+
+@pytest.mark.gpu
+def test_read_longer_than_512_is_unsupported(engine):
+    with engine.job() as job:
+        job.feed(_long_reads(513, 50, seed=3))
+        with pytest.raises(empanada_b200._native.EmpError) as e:
+            job.run()
+        assert e.value.code == empanada_b200._native.EMP_E_UNSUPPORTED
+
+
 @pytest.mark.gpu
 def test_fingerprints_match_oracle(engine):
-    for name in ["tiny", "odd_len", "lowercase", "read_len_255", "read_len_1", "dups_palindromes"]:
-        data = BY_NAME[name].fastq()
-        with engine.job(min_ovlp=BY_NAME[name].min_ovlp()) as job:
+    for name in ["tiny", "odd_len", "lowercase", "read_len_255", "read_len_1", "dups_palindromes", 257, 300, 512]:
+        data = _long_reads(name, 700, seed=name) if isinstance(name, int) else BY_NAME[name].fastq()
+        with engine.job(min_ovlp=31 if isinstance(name, int) else BY_NAME[name].min_ovlp()) as job:
             job.feed(data)
             job.run()
             got = job.fingerprints()

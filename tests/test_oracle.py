@@ -46,7 +46,7 @@ def test_known_answers():
 def test_rolling_steps_match_direct_hashes():
     rng = random.Random(5)
     for _ in range(200):
-        s = "".join(rng.choice("ACGT") for _ in range(rng.randint(2, 255)))
+        s = "".join(rng.choice("ACGT") for _ in range(rng.randint(2, 512)))  # 256-512: extended range
         assert bind.hash_of(s) == H(s)
         assert bind.next_sfx(H(s), s[0], len(s)) == H(s[1:])
         k = H(s)
@@ -91,11 +91,54 @@ def test_oracle_errors():
         bind.run(fastq(["ACGR", "ACGT"]), 1)
     assert e.value.code == bind.E_FORMAT
     with pytest.raises(bind.OracleError) as e:
-        bind.run(fastq(["A" * 256, "C" * 256]), 31)
+        bind.run(fastq(["A" * 513, "C" * 513]), 31)
     assert e.value.code == bind.E_UNSUPPORTED
     with pytest.raises(bind.OracleError) as e:
         bind.run(fastq(["ACGT"]), 1, reduce_mem=16)
     assert e.value.code == bind.E_INVAL
+
+
+def test_oracle_long_reads_follow_the_hash_definition():
+    """Reads of 256-512 bases (beyond the reference's MAX_RD_LEN, where its
+    result is undefined): the oracle's fingerprints are the exact hash of
+    each read-end and its edges join exactly the overlapping read-ends."""
+    rng = random.Random(23)
+    for L in (256, 300, 512):
+        g = "".join(rng.choice("ACGT") for _ in range(3 * L))
+        reads = []
+        for _ in range(12):
+            p = rng.randrange(0, len(g) - L + 1)
+            s = g[p:p + L]
+            reads.append(revcomp(s) if rng.random() < 0.5 else s)
+        data = fastq(reads)
+        keys, n, LL = bind.fingerprints(data)
+        assert (n, LL) == (len(reads), L)
+        for i, s in enumerate(reads):
+            assert int(keys[2 * i]) == H(s) and int(keys[2 * i + 1]) == H(revcomp(s))
+        o = L // 2
+        out, st = bind.run(data, o)
+        ends = [x for s in reads for x in (s, revcomp(s))]
+        got = set()
+        for ov, frm, to in _records(out):
+            for a, b in zip(frm, to):
+                assert ends[a][L - ov:] == ends[b][:ov]  # suffix of a equals prefix of b
+                got.add((int(a), int(b)))
+        assert st["n_edges"] == len(got) > 0
+
+
+def _records(data: bytes):
+    import struct
+
+    out, p = [], 0
+    while p < len(data):
+        n, ov = struct.unpack_from("<Qi", data, p)
+        p += 12
+        frm = struct.unpack_from(f"<{n}I", data, p)
+        p += 4 * n
+        to = struct.unpack_from(f"<{n}I", data, p)
+        p += 4 * n
+        out.append((ov, frm, to))
+    return out
 
 
 def test_oracle_duplicate_walk_hang():
