@@ -410,7 +410,6 @@ def main():
     host = torch.empty(F, dtype=torch.uint8, pin_memory=True)
     host_np = host.numpy()
     synth.fastq_into(workload, host_np)
-    out_host = torch.empty(64 << 20, dtype=torch.uint8, pin_memory=True).numpy()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")  # > 126 MB L2
 
     eng = empanada_b200.Engine(device)
@@ -471,6 +470,7 @@ def main():
     job.close()
 
     # ---- e2e: host FASTQ in, output.bin out, through the C ABI
+    out_host = torch.empty(out_bytes + 4096, dtype=torch.uint8, pin_memory=True).numpy()
     job = eng.job(**params)
     job.reserve(F)
     e2e_s = []

@@ -84,7 +84,9 @@ LARGER = Workload("larger: 5 Mbp genome, 1.2M x 250 bp reads, 0.1% subs, -o 75 -
 OUT_OF_CORE = Workload("out_of_core: 100 Mbp genome (5% repeat families), 150 bp reads at 50x, -m 1g -r 1g",
                        seed=3, genome_len=100_000_000, n_reads=33_333_333, read_len=150,
                        repeat_frac=0.05, min_ovlp=31, map_mem="1g", reduce_mem="1g")
-WORKLOADS = {"small": SMALL, "larger": LARGER, "out_of_core": OUT_OF_CORE}
+OUT_OF_CORE_HBM = dataclasses.replace(OUT_OF_CORE, name="out_of_core, HBM-sized blocks: as out_of_core with "
+                                      "-m 160g -r 160g", map_mem="160g", reduce_mem="160g")
+WORKLOADS = {"small": SMALL, "larger": LARGER, "out_of_core": OUT_OF_CORE, "out_of_core_hbm": OUT_OF_CORE_HBM}
 
 
 def batched_sets(n_sets: int = 256, seed: int = 4, genome_min: int = 50_000, genome_max: int = 5_000_000,

@@ -181,6 +181,9 @@ class Case:
 
 
 TINY = {"seed": 101, "genome_len": 50_000, "n_reads": 3000, "read_len": 100}
+CONFIG3_TENTH = {"seed": 3, "genome_len": 10_000_000, "n_reads": 3_333_333, "read_len": 150, "repeat_frac": 0.05,
+                 "rep_min_len": 1000, "rep_max_len": 5000, "rep_min_copies": 2, "rep_max_copies": 50,
+                 "rep_divergence": 0.01}
 CASES = [
     Case("tiny", ("-o", "31"), synth=TINY),
     Case("tiny_m16k_b1k", ("-o", "31", "-m", "16k", "-b", "1k", "-c", "1k"), synth=TINY),
@@ -209,6 +212,11 @@ CASES = [
          synth={"seed": 104, "genome_len": 60_000, "n_reads": 5000, "read_len": 90, "sub_rate": 0.001,
                 "repeat_frac": 0.2, "rep_min_len": 300, "rep_max_len": 900, "rep_min_copies": 2,
                 "rep_max_copies": 12, "rep_divergence": 0.002}),
+    # config 3 at a tenth of its size: 10 Mbp genome, 5 % repeat families
+    # (1-5 kbp copies, 2-50 each, 1 % divergence), 150 bp reads at 50x;
+    # at -r 100m (M = 6.55M < 2n) the fingerprint sort goes out of core
+    Case("repeats_10m_r100m", ("-o", "31", "-r", "100m"), synth=CONFIG3_TENTH, big=True),
+    Case("repeats_10m", ("-o", "31"), synth=CONFIG3_TENTH, big=True),
     Case("small", ("-o", "31"), synth={}, big=True),
     Case("larger", ("-o", "75", "-m", "8g", "-r", "12g", "-b", "16m", "-c", "64m"),
          synth={"seed": 2, "genome_len": 5_000_000, "n_reads": 1_200_000, "read_len": 250, "sub_rate": 0.001},

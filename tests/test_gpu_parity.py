@@ -51,9 +51,10 @@ def test_case_matches_reference(engine, name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["small", "larger"])
+@pytest.mark.parametrize("name", ["small", "larger", "repeats_10m", "repeats_10m_r100m"])
 def test_full_size_workload_matches_reference(engine, name):
-    """Configs 1 and 2 at full size: byte-identical to the reference's output.bin."""
+    """Configs 1 and 2 at full size, config 3 at a tenth (in core, and out of
+    core at -r 100m): byte-identical to the reference's output.bin."""
     case = BY_NAME[name]
     g = GOLDEN[name]
     data, out, st = _run(engine, case)
