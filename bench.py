@@ -27,6 +27,7 @@ impl reference: that CPU build alone, timed per step on the bounded sample
 from __future__ import annotations
 
 import argparse
+import collections
 import json
 import os
 import statistics
@@ -359,6 +360,138 @@ def batched_bench(args):
     print(json.dumps(line), flush=True)
 
 
+def served_bench(args):
+    """Config 5: Poisson arrivals of read-set jobs (sizes as the batched sets,
+    2 % heavy jobs of a 50 Mbp genome at 30x) into an emp_server, per
+    arrival rate; the same arrival stream run job by job (emp_job_run in
+    arrival order) for comparison.  Latency: scheduled arrival -> output.bin
+    on the host (the request's FASTQ is copied in at arrival)."""
+    import numpy as np
+    import torch
+
+    import empanada_b200
+    from empanada_b200 import synth
+
+    rng = np.random.default_rng(5)
+    pool = synth.batched_sets(n_sets=args.serve_pool, seed=6, genome_max=args.batch_genome_max)
+    heavy = [synth.Workload(f"heavy{k}: 50 Mbp genome at 30x, {L} bp", seed=7_000 + k, genome_len=50_000_000,
+                            n_reads=50_000_000 * 30 // L, read_len=L, sub_rate=0.001, min_ovlp=31)
+             for k, L in enumerate((150, 250))]
+    sets = pool + heavy
+    sizes = [synth.fastq_size(w) for w in sets]
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    t0 = time.perf_counter()
+    host = torch.empty(int(offs[-1]), dtype=torch.uint8, pin_memory=True)
+    host_np = host.numpy()
+    for w, a, b in zip(sets, offs[:-1], offs[1:]):
+        synth.fastq_into(w, host_np[a:b])
+    gen_s = time.perf_counter() - t0
+    device = 0
+    torch.cuda.set_device(device)
+    eng = empanada_b200.Engine(device)
+    # each set alone: the outputs every served job must reproduce
+    digests = []
+    with eng.job() as j:
+        for w, a, b in zip(sets, offs[:-1], offs[1:]):
+            j.reset()
+            j.feed(host_np[a:b], last=True)
+            j.run()
+            digests.append(hash(j.output()))
+    out_host = torch.empty(1 << 30, dtype=torch.uint8, pin_memory=True).numpy()
+    # idle jobs kept per read set, so that a job's device buffers (which only
+    # grow) stay the size of the requests it serves
+    free_jobs = {}
+
+    def get_job(k):
+        lst = free_jobs.setdefault(k, [])
+        return lst.pop() if lst else eng.job(min_ovlp=31)
+
+    def stream(lam, n):
+        t = np.cumsum(rng.exponential(1.0 / lam, size=n))
+        kinds = np.where(rng.random(n) < 0.02, len(pool) + rng.integers(0, len(heavy), n),
+                         rng.integers(0, len(pool), n))
+        return t, kinds
+
+    def run(lam, served):
+        """Requests wait on the host until they are taken: one at a time for
+        the job-by-job arm, up to 64 per step for the server while its own
+        queue is empty (it admitted everything submitted so far)."""
+        t_arr, kinds = stream(lam, int(min(max(args.serve_min_jobs, lam * args.serve_seconds), args.serve_max_jobs)))
+        n = len(t_arr)
+        lat = np.zeros(n)
+        ok = True
+        reads = 0
+        srv = (empanada_b200.Server(eng, rounds_per_launch=args.serve_rounds, hbm_budget_bytes=args.serve_budget << 30)
+               if served else None)
+        pending = collections.deque()
+        held = {}
+        nxt = done = 0
+        start = time.perf_counter()
+        while done < n:
+            now = time.perf_counter() - start
+            while nxt < n and t_arr[nxt] <= now:
+                pending.append((nxt, int(kinds[nxt])))
+                nxt += 1
+            fin = []
+            if served:
+                if pending and srv.counts()[0] == 0:
+                    for _ in range(min(64, len(pending))):
+                        i, k = pending.popleft()
+                        j = get_job(k)
+                        j.reset()
+                        j.feed(host_np[offs[k]:offs[k + 1]], last=True)
+                        srv.submit(j)
+                        held[j.handle.value] = (i, k)
+                if held:
+                    fin = [(j,) + held.pop(j.handle.value) for j in srv.step()]
+            elif pending:
+                i, k = pending.popleft()
+                j = get_job(k)
+                j.reset()
+                j.feed(host_np[offs[k]:offs[k + 1]], last=True)
+                j.run()
+                fin = [(j, i, k)]
+            if not fin and not held and not pending and nxt < n:
+                time.sleep(max(0.0, min(t_arr[nxt] - (time.perf_counter() - start), 0.002)))
+            for j, i, k in fin:
+                nbytes = j.output_into(out_host) if j.status() == 0 else -1
+                lat[i] = time.perf_counter() - start - t_arr[i]
+                ok = ok and nbytes >= 0 and hash(out_host[:nbytes].tobytes()) == digests[k]
+                reads += sets[k].n_reads
+                free_jobs[k].append(j)
+                done += 1
+        span = time.perf_counter() - start
+        if srv:
+            srv.close()
+        return {"jobs": n, "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "reads_per_s": reads / span, "seconds": span, "outputs_identical": bool(ok)}
+
+    rates = [float(x) for x in args.serve_rates.split(",")]
+    with ClockSampler(device) as clk:
+        served = {str(l): run(l, True) for l in rates}
+        plain = {str(l): run(l, False) for l in rates}
+    clocks = clk.summary()
+    for lst in free_jobs.values():
+        for j in lst:
+            j.close()
+    eng.close()
+    line = {"metric": "served: p50/p99 latency (arrival -> output.bin on host) and reads/s per arrival rate",
+            "value": served[str(rates[-1])]["reads_per_s"], "unit": "reads/s", "n_gpus": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded generator empanada_b200/csrc/synth_reads.c)",
+            "config": {"workload": f"served: Poisson arrivals; a pool of {len(pool)} read sets drawn as the batched "
+                                   f"sets (genome 50 kbp-{args.batch_genome_max // 1000} kbp log-uniform, 100-300 bp, "
+                                   "10-80x, 0.1% substitutions) plus 2% heavy jobs (50 Mbp genome at 30x, 150 or "
+                                   "250 bp), -o 31; jobs per rate: rate x "
+                                   f"{args.serve_seconds} s within [{args.serve_min_jobs}, {args.serve_max_jobs}]",
+                       "rounds_per_launch": args.serve_rounds, "admission_budget_gib": args.serve_budget,
+                       "rates_per_s": rates},
+            "served": served, "plain": plain, "clocks": clocks, "host_generate_s": gen_s,
+            "e2e": {"value": served[str(rates[-1])]["reads_per_s"], "unit": "reads/s",
+                    "what": "every request's FASTQ copied in at arrival and its output.bin copied out"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -373,8 +506,18 @@ def main():
     ap.add_argument("--batch-sets", type=int, default=256, help="read sets of --workload batched")
     ap.add_argument("--batch-genome-max", type=int, default=5_000_000,
                     help="largest genome of --workload batched (log-uniform from 50 kbp)")
+    ap.add_argument("--serve-rates", default="1,2,5,10,20,50,100,200", help="arrival rates (jobs/s) of --workload served")
+    ap.add_argument("--serve-seconds", type=float, default=4.0)
+    ap.add_argument("--serve-min-jobs", type=int, default=20)
+    ap.add_argument("--serve-max-jobs", type=int, default=400)
+    ap.add_argument("--serve-pool", type=int, default=48)
+    ap.add_argument("--serve-rounds", type=int, default=16, help="bucket-kernel rounds per launch")
+    ap.add_argument("--serve-budget", type=int, default=100, help="admission budget of the server, GiB")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload == "served":
+        served_bench(args)
+        return
     if args.workload == "batched":
         batched_bench(args)
         return

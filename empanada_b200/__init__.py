@@ -204,6 +204,10 @@ class Job:
     def run(self, stream: int = 0) -> None:
         check(self._lib.emp_job_run(self.handle, stream or None), "emp_job_run")
 
+    def status(self) -> int:
+        """Status of the last run (EMP_E_STATE while there is none)."""
+        return int(self._lib.emp_job_status(self.handle))
+
     def output(self) -> bytes:
         n = ctypes.c_uint64()
         check(self._lib.emp_job_output_size(self.handle, ctypes.byref(n)), "output_size")
@@ -232,6 +236,54 @@ class Job:
             check(self._lib.emp_job_fingerprints(self.handle, out.ctypes.data, out.size, ctypes.byref(n)),
                   "fingerprints")
         return out
+
+
+class Server:
+    """An emp_server: continuous batching of submitted jobs on one Engine.
+
+    submit() takes a fed Job; step() runs one scheduling step and returns the
+    jobs that finished (each with status() set).  A job belongs to the server
+    from submit() until a step returns it."""
+
+    def __init__(self, engine: Engine, rounds_per_launch: int = 16, max_jobs: int = 256,
+                 hbm_budget_bytes: int = 0):
+        self.engine = engine
+        self._lib = engine._lib
+        p = _native.ServerParams(int(rounds_per_launch), int(max_jobs), int(hbm_budget_bytes))
+        h = ctypes.c_void_p()
+        check(self._lib.emp_server_create(engine.handle, ctypes.byref(p), ctypes.byref(h)), "emp_server_create")
+        self.handle = h
+        self._held: dict[int, "Job"] = {}
+        self._out = (ctypes.c_void_p * 1024)()
+
+    def submit(self, job: "Job") -> None:
+        check(self._lib.emp_server_submit(self.handle, job.handle), "emp_server_submit")
+        self._held[job.handle.value] = job
+
+    def step(self) -> list["Job"]:
+        n = ctypes.c_int()
+        rc = self._lib.emp_server_step(self.handle, self._out, len(self._out), ctypes.byref(n))
+        done = [self._held.pop(self._out[i]) for i in range(n.value)]
+        check(rc, "emp_server_step")
+        return done
+
+    def counts(self) -> tuple[int, int, int]:
+        q, f, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._lib.emp_server_counts(self.handle, ctypes.byref(q), ctypes.byref(f), ctypes.byref(d)),
+              "emp_server_counts")
+        return q.value, f.value, d.value
+
+    def close(self):
+        if self.handle:
+            self._lib.emp_server_destroy(self.handle)
+            self.handle = None
+            self._held.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 SORT_STATIC_MAX_PAIRS = _native.SORT_STATIC_MAX_PAIRS

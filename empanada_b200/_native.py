@@ -38,6 +38,14 @@ class Params(ctypes.Structure):
     ]
 
 
+class ServerParams(ctypes.Structure):
+    _fields_ = [
+        ("rounds_per_launch", ctypes.c_int32),
+        ("max_jobs", ctypes.c_int32),
+        ("hbm_budget_bytes", ctypes.c_uint64),
+    ]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("n_reads", ctypes.c_uint64),
@@ -91,6 +99,14 @@ SIGNATURES = {
     "emp_job_reset": (ctypes.c_int, [_vp]),
     "emp_job_run": (ctypes.c_int, [_vp, _vp]),
     "emp_batch_run": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.c_int, _vp]),
+    "emp_job_status": (ctypes.c_int, [_vp]),
+    "emp_server_params_default": (ctypes.c_int, [ctypes.POINTER(ServerParams)]),
+    "emp_server_create": (ctypes.c_int, [_vp, ctypes.POINTER(ServerParams), ctypes.POINTER(_vp)]),
+    "emp_server_destroy": (ctypes.c_int, [_vp]),
+    "emp_server_submit": (ctypes.c_int, [_vp, _vp]),
+    "emp_server_step": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "emp_server_counts": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int)]),
     "emp_job_output_size": (ctypes.c_int, [_vp, _u64p]),
     "emp_job_output_copy": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64]),
     "emp_job_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats)]),

@@ -9,6 +9,7 @@
 // All tables stay in HBM; the only host traffic is the FASTQ in and the
 // edge list out.  output.bin records are assembled on the host exactly as
 // write_edges_binary (overlap.cu:148-161) writes them.
+#include <algorithm>
 #include <cerrno>
 #include <chrono>
 #include <cstdio>
@@ -123,6 +124,12 @@ struct emp_job {
     // map-phase state (map_begin .. map_list) and its events
     JobPrep prep;
     cudaEvent_t map_ev[5] = {};
+    // served: the job's bucket-kernel descriptor between launches, its
+    // admission estimate, and whether a server holds it
+    BktJob bk{};
+    uint64_t admit_est = 0;
+    emp_server *server = nullptr;
+    emp_status last_rc = EMP_E_STATE;  // status of the last run (EMP_E_STATE: none yet)
     // results
     std::vector<uint8_t> out;
     emp_stats st{};
@@ -869,16 +876,17 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
     uint64_t n_in = 2 * U, S = U, P = U;
     const uint64_t M = env.M;
     const bool force_sync = std::getenv("EMP_SYNC_ROUNDS") != nullptr;
-    while (r < env.rounds && (force_sync || S >= M / 2 || P >= M / 2)) {
+    const bool bucket = !std::getenv("EMP_NO_COOP") && !std::getenv("EMP_NO_BUCKET") && bucket_grid_size() > 0;
+    // host-synchronised rounds (one full sort each) also carry a list too
+    // large for the bucket kernel until it fits
+    while (r < env.rounds && (force_sync || S >= M / 2 || P >= M / 2 || (bucket && n_in > kBktMaxEntries))) {
         bool stop = false;
         EMP_TRY(sync_round(j, s, env, r, cur, n_in, S, P, stop));
         if (stop) return EMP_OK;
         ++r;
     }
     if (r >= env.rounds) return EMP_OK;
-    if (!std::getenv("EMP_NO_COOP") && !std::getenv("EMP_NO_BUCKET") && n_in <= kBktMaxEntries &&
-        bucket_grid_size() > 0)
-        return run_rounds_bucket(j, s, env, r, cur, n_in, ecap, needed);
+    if (bucket) return run_rounds_bucket(j, s, env, r, cur, n_in, ecap, needed);
 
     // ---- device-resident pipeline for rounds r .. rounds-1
     const uint64_t nmax = n_in;
@@ -1293,11 +1301,10 @@ emp_status batch_rounds(emp_ctx *ctx, emp_job **jobs, const std::vector<int> &id
     return EMP_OK;
 }
 
-// Every job of a batch through the map phase (one synchronisation per stage
-// for the whole batch), the rounds of the eligible ones in one bucket-kernel
-// launch, the others' rounds one job after another.
-emp_status run_batch(emp_ctx *ctx, emp_job **jobs, int n, cudaStream_t s) {
-    std::vector<emp_status> rc((size_t)n, EMP_OK);
+// The map phase of jobs[0..n) with one stream synchronisation per stage for
+// all of them; a job that fails gets its status in rc.  Jobs left with rc
+// EMP_OK and prep.done unset have their lists ready for the rounds.
+emp_status map_batch(emp_job **jobs, int n, std::vector<emp_status> &rc, cudaStream_t s) {
     auto live = [&](int i) { return rc[i] == EMP_OK && !jobs[i]->prep.done; };
     auto fail = [&](int i, emp_status e) {
         if (rc[i] == EMP_OK) rc[i] = e;
@@ -1319,39 +1326,193 @@ emp_status run_batch(emp_ctx *ctx, emp_job **jobs, int n, cudaStream_t s) {
         if (live(i)) fail(i, map_fetch(jobs[i], s));
     }
     EMP_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < n; ++i)
+        if (live(i)) fail(i, map_list(jobs[i], s));
+    return EMP_OK;
+}
+
+// Close jobs[0..n) whose work is all queued: their last events, one
+// synchronisation, then results (rc[i] == EMP_OK) or none.  Sets each job's
+// last_rc; returns the first failure.
+emp_status close_jobs(emp_job **jobs, int n, std::vector<emp_status> &rc, cudaStream_t s) {
+    for (int i = 0; i < n; ++i) {
+        if (rc[i] != EMP_OK) continue;
+        if (!jobs[i]->prep.done) {
+            cudaEventRecord(jobs[i]->map_ev[3], s);
+            cudaEventRecord(jobs[i]->map_ev[4], s);
+        }
+        rc[i] = map_fetch(jobs[i], s);
+    }
+    EMP_CUDA(cudaStreamSynchronize(s));
+    EMP_CUDA(cudaGetLastError());
+    emp_status first = EMP_OK;
+    for (int i = 0; i < n; ++i) {
+        if (rc[i] == EMP_OK) rc[i] = map_check(jobs[i]);
+        if (rc[i] == EMP_OK) {
+            job_finish(jobs[i]);
+        } else {
+            jobs[i]->have_result = false;
+            if (first == EMP_OK) first = rc[i];
+        }
+        jobs[i]->last_rc = rc[i];
+    }
+    return first;
+}
+
+// Every job of a batch through the map phase, the rounds of the eligible
+// ones in one bucket-kernel launch, the others' rounds one job after another.
+emp_status run_batch(emp_ctx *ctx, emp_job **jobs, int n, cudaStream_t s) {
+    std::vector<emp_status> rc((size_t)n, EMP_OK);
+    EMP_TRY(map_batch(jobs, n, rc, s));
     std::vector<int> batch, alone;
     for (int i = 0; i < n; ++i) {
-        if (!live(i)) continue;
-        fail(i, map_list(jobs[i], s));
-        if (!live(i)) continue;
+        if (rc[i] != EMP_OK || jobs[i]->prep.done) continue;
         if (batch_eligible(jobs[i])) batch.push_back(i);
         else alone.push_back(i);
     }
     if (!batch.empty()) {
         const emp_status e = batch_rounds(ctx, jobs, batch, rc, s);
         if (e != EMP_OK)
-            for (int i : batch) fail(i, e);
+            for (int i : batch)
+                if (rc[i] == EMP_OK) rc[i] = e;
     }
-    for (int i : alone) fail(i, job_rounds(jobs[i], s));
-    for (int i = 0; i < n; ++i) {
-        if (!live(i)) continue;
-        cudaEventRecord(jobs[i]->map_ev[3], s);
-        cudaEventRecord(jobs[i]->map_ev[4], s);
+    for (int i : alone) rc[i] = job_rounds(jobs[i], s);
+    return close_jobs(jobs, n, rc, s);
+}
+
+// ---- served jobs -----------------------------------------------------------
+
+// Device footprint assumed for a queued job before its reads are known
+// (admission): the FASTQ, about 400 B of tables and lists per read at
+// 100+ bases per read (so 3 B per FASTQ byte), and the fixed minimum of the
+// edge and output buffers.
+uint64_t served_footprint(uint64_t F) { return 4 * F + (64ull << 20); }
+
+}  // namespace
+
+struct emp_server {
+    emp_ctx *ctx = nullptr;
+    emp_server_params p{};
+    std::deque<emp_job *> queue;     // submitted, not yet admitted
+    std::vector<emp_job *> live;     // in the bucket-kernel batch
+    std::vector<emp_job *> finished; // completed, not yet handed out
+    uint64_t admitted = 0;           // footprint estimates of the admitted jobs
+    DevBuf d_jobs, d_ctl;
+    PinnedBuf h_jobs;
+    cudaEvent_t ev[2] = {};
+    uint64_t launches = 0;
+};
+
+namespace {
+
+// a finished job waits in `finished` (still held by the server) until a step hands it out
+void server_complete(emp_server *srv, emp_job *j) {
+    srv->admitted -= j->admit_est;
+    j->admit_est = 0;
+    srv->finished.push_back(j);
+}
+
+// Admit queued jobs and run their map phase; start the eligible ones in the
+// batch, run the others alone; then one bucket-kernel launch of at most
+// rounds_per_launch iterations over every job in the batch, after which the
+// jobs with no round left complete.
+emp_status server_step(emp_server *srv, cudaStream_t s) {
+    emp_ctx *ctx = srv->ctx;
+    const uint64_t budget = srv->p.hbm_budget_bytes ? srv->p.hbm_budget_bytes : ctx->budget;
+    std::vector<emp_job *> adm;
+    while (!srv->queue.empty() && (int)(srv->live.size() + adm.size()) < srv->p.max_jobs) {
+        emp_job *j = srv->queue.front();
+        const uint64_t est = served_footprint(j->F);
+        if (budget && srv->admitted + est > budget && !(srv->live.empty() && adm.empty())) break;
+        srv->queue.pop_front();
+        srv->admitted += est;
+        j->admit_est = est;
+        adm.push_back(j);
     }
-    for (int i = 0; i < n; ++i)
-        if (rc[i] == EMP_OK) fail(i, map_fetch(jobs[i], s));
-    EMP_CUDA(cudaStreamSynchronize(s));
-    EMP_CUDA(cudaGetLastError());
-    emp_status first = EMP_OK;
-    for (int i = 0; i < n; ++i) {
-        if (rc[i] == EMP_OK) fail(i, map_check(jobs[i]));
-        if (rc[i] == EMP_OK) job_finish(jobs[i]);
-        else {
-            jobs[i]->have_result = false;
-            if (first == EMP_OK) first = rc[i];
+    if (!adm.empty()) {
+        const int n = (int)adm.size();
+        std::vector<emp_status> rc((size_t)n, EMP_OK);
+        EMP_TRY(map_batch(adm.data(), n, rc, s));
+        std::vector<emp_job *> close;
+        std::vector<emp_status> crc;
+        for (int i = 0; i < n; ++i) {
+            emp_job *j = adm[i];
+            JobPrep &q = j->prep;
+            if (rc[i] == EMP_OK && !q.done && batch_eligible(j)) {
+                rc[i] = rounds_prelude(j, s);
+                if (rc[i] == EMP_OK) rc[i] = bucket_prepare(j, s, job_env(j), 0, 0, 2 * q.U, q.ecap, 1u, &j->bk);
+                if (rc[i] == EMP_OK) {
+                    srv->live.push_back(j);
+                    continue;
+                }
+            } else if (rc[i] == EMP_OK && !q.done) {
+                rc[i] = job_rounds(j, s);  // too large for the batch, or rounds that split: alone
+            }
+            close.push_back(j);
+            crc.push_back(rc[i]);
+        }
+        if (!close.empty()) {
+            close_jobs(close.data(), (int)close.size(), crc, s);
+            for (emp_job *j : close) server_complete(srv, j);
         }
     }
-    return first;
+    if (srv->live.empty()) return EMP_OK;
+    const size_t nb = srv->live.size();
+    EMP_TRY(ctx_ensure(ctx, srv->d_jobs, nb * sizeof(BktJob)));
+    EMP_TRY(ctx_ensure(ctx, srv->d_ctl, sizeof(CoopCtl)));
+    if (!srv->h_jobs.ensure(nb * sizeof(BktJob) + sizeof(CoopCtl))) return EMP_E_NOMEM;
+    if (!srv->ev[0]) {
+        for (auto &e : srv->ev) EMP_CUDA(cudaEventCreate(&e));
+    }
+    BktJob *hj = srv->h_jobs.as<BktJob>();
+    CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + nb);
+    for (size_t k = 0; k < nb; ++k) hj[k] = srv->live[k]->bk;
+    std::memset(hc, 0, sizeof(CoopCtl));
+    hc->njobs = (uint32_t)nb;
+    hc->active = (uint32_t)nb;
+    hc->iter_cap = (uint32_t)srv->p.rounds_per_launch;
+    EMP_CUDA(cudaMemcpyAsync(srv->d_jobs.p, hj, nb * sizeof(BktJob), cudaMemcpyHostToDevice, s));
+    EMP_CUDA(cudaMemcpyAsync(srv->d_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
+    EMP_CUDA(cudaEventRecord(srv->ev[0], s));
+    EMP_CUDA(launch_bucket_rounds(srv->d_jobs.as<BktJob>(), srv->d_ctl.as<CoopCtl>(), err_word(srv->live[0]), s));
+    EMP_CUDA(cudaEventRecord(srv->ev[1], s));
+    EMP_CUDA(cudaMemcpyAsync(hj, srv->d_jobs.p, nb * sizeof(BktJob), cudaMemcpyDeviceToHost, s));
+    EMP_CUDA(cudaMemcpyAsync(hc, srv->d_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
+    EMP_CUDA(cudaStreamSynchronize(s));
+    ++srv->launches;
+    const bool timed_out = (hc->err & kErrSpin) != 0;
+    const float ms = ms_between(srv->ev[0], srv->ev[1]);
+    std::vector<emp_job *> still, done;
+    for (size_t k = 0; k < nb; ++k) {
+        emp_job *j = srv->live[k];
+        j->bk = hj[k];
+        j->st.ms_round_kernel += ms;  // every launch the job took part in
+        if (timed_out || j->bk.done) {
+            done.push_back(j);
+            if (!timed_out) EMP_TRY(bucket_fetch(j, job_env(j), s));
+        } else {
+            j->bk.iter0 += hc->iters;
+            still.push_back(j);
+        }
+    }
+    srv->live.swap(still);
+    if (done.empty()) return EMP_OK;
+    EMP_CUDA(cudaStreamSynchronize(s));
+    std::vector<emp_status> rc(done.size(), timed_out ? EMP_E_TIMEOUT : EMP_OK);
+    for (size_t k = 0; k < done.size() && !timed_out; ++k) {
+        emp_job *j = done[k];
+        JobPrep &q = j->prep;
+        uint64_t needed = 0;
+        rc[k] = bucket_collect(j, 0, 2 * q.U, j->bk, &needed);
+        if (rc[k] == kNeedEdgeRoom) {  // alone again, with room for every edge
+            q.ecap = needed + needed / 4 + 1024;
+            j->ecap_hint = q.ecap;
+            rc[k] = job_rounds(j, s);
+        }
+    }
+    close_jobs(done.data(), (int)done.size(), rc, s);
+    for (emp_job *j : done) server_complete(srv, j);
+    return timed_out ? EMP_E_TIMEOUT : EMP_OK;
 }
 
 }  // namespace
@@ -1496,6 +1657,7 @@ emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out) {
 
 emp_status emp_job_destroy(emp_job *job) {
     if (!job) return EMP_E_INVAL;
+    if (job->server) return EMP_E_STATE;
     cudaSetDevice(job->ctx->device);
     cudaStreamSynchronize(job->ctx->stream);
     DevBuf *bufs[] = {&job->fq, &job->tile_counts, &job->tile_excl, &job->status, &job->misc, &job->seq_start,
@@ -1524,6 +1686,7 @@ emp_status emp_job_destroy(emp_job *job) {
 
 emp_status emp_job_reserve(emp_job *job, uint64_t bytes) {
     if (!job) return EMP_E_INVAL;
+    if (job->server) return EMP_E_STATE;
     if (bytes <= job->fq.bytes) return EMP_OK;
     cudaSetDevice(job->ctx->device);
     DevBuf nb;
@@ -1550,6 +1713,7 @@ emp_status emp_job_reserve(emp_job *job, uint64_t bytes) {
 
 emp_status emp_job_reset(emp_job *job) {
     if (!job) return EMP_E_INVAL;
+    if (job->server) return EMP_E_STATE;
     cudaSetDevice(job->ctx->device);
     cudaStreamSynchronize(job->ctx->stream);
     job->F = 0;
@@ -1564,6 +1728,7 @@ emp_status emp_job_reset(emp_job *job) {
 
 static emp_status feed(emp_job *job, const void *src, uint64_t n, int last, cudaMemcpyKind kind) {
     if (!job || (n && !src)) return EMP_E_INVAL;
+    if (job->server) return EMP_E_STATE;
     if (job->fed_last) return EMP_E_STATE;
     cudaSetDevice(job->ctx->device);
     if (job->F + n > job->fq.bytes) {
@@ -1600,6 +1765,7 @@ emp_status emp_job_feed_fastq_device(emp_job *job, const void *dev_bytes, uint64
 emp_status emp_job_run(emp_job *job, void *stream) {
     if (!job) return EMP_E_INVAL;
     if (cudaSetDevice(job->ctx->device) != cudaSuccess) return EMP_E_CUDA;
+    if (job->server) return EMP_E_STATE;
     cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : job->ctx->stream;
     emp_status st = run_job(job, s);
     if (st != EMP_OK) {
@@ -1607,13 +1773,14 @@ emp_status emp_job_run(emp_job *job, void *stream) {
         cudaGetLastError();
         job->have_result = false;
     }
+    job->last_rc = st;
     return st;
 }
 
 emp_status emp_batch_run(emp_ctx *ctx, emp_job **jobs, int njobs, void *stream) {
     if (!ctx || njobs < 0 || (njobs && !jobs) || njobs > kCoopMaxJobs) return EMP_E_INVAL;
     for (int i = 0; i < njobs; ++i) {
-        if (!jobs[i] || jobs[i]->ctx != ctx) return EMP_E_INVAL;
+        if (!jobs[i] || jobs[i]->ctx != ctx || jobs[i]->server) return EMP_E_INVAL;
         for (int k = 0; k < i; ++k)
             if (jobs[k] == jobs[i]) return EMP_E_INVAL;
     }
@@ -1626,6 +1793,90 @@ emp_status emp_batch_run(emp_ctx *ctx, emp_job **jobs, int njobs, void *stream) 
         cudaGetLastError();
     }
     return st;
+}
+
+emp_status emp_job_status(emp_job *job) { return job ? job->last_rc : EMP_E_INVAL; }
+
+emp_status emp_server_params_default(emp_server_params *p) {
+    if (!p) return EMP_E_INVAL;
+    p->rounds_per_launch = 16;
+    p->max_jobs = 256;
+    p->hbm_budget_bytes = 0;
+    return EMP_OK;
+}
+
+emp_status emp_server_create(emp_ctx *ctx, const emp_server_params *p, emp_server **out) {
+    if (!ctx || !out) return EMP_E_INVAL;
+    *out = nullptr;
+    emp_server_params q;
+    if (p) q = *p;
+    else emp_server_params_default(&q);
+    if (q.rounds_per_launch < 1 || q.max_jobs < 1 || q.max_jobs > kCoopMaxJobs) return EMP_E_INVAL;
+    emp_server *srv = new (std::nothrow) emp_server();
+    if (!srv) return EMP_E_NOMEM;
+    srv->ctx = ctx;
+    srv->p = q;
+    *out = srv;
+    return EMP_OK;
+}
+
+emp_status emp_server_destroy(emp_server *srv) {
+    if (!srv) return EMP_E_INVAL;
+    cudaSetDevice(srv->ctx->device);
+    cudaStreamSynchronize(srv->ctx->stream);
+    auto drop = [](emp_job *j) {
+        j->server = nullptr;
+        j->admit_est = 0;
+        j->have_result = false;
+        j->last_rc = EMP_E_STATE;
+    };
+    for (emp_job *j : srv->queue) drop(j);
+    for (emp_job *j : srv->live) drop(j);
+    for (emp_job *j : srv->finished) j->server = nullptr;
+    for (auto &e : srv->ev)
+        if (e) cudaEventDestroy(e);
+    srv->ctx->in_use -= srv->d_jobs.bytes + srv->d_ctl.bytes;
+    delete srv;
+    return EMP_OK;
+}
+
+emp_status emp_server_submit(emp_server *srv, emp_job *job) {
+    if (!srv || !job || job->ctx != srv->ctx) return EMP_E_INVAL;
+    if (job->server) return EMP_E_STATE;
+    if ((int)(srv->queue.size() + srv->live.size() + srv->finished.size()) >= (1 << 20)) return EMP_E_NOMEM;
+    job->server = srv;
+    job->have_result = false;
+    job->last_rc = EMP_E_STATE;
+    srv->queue.push_back(job);
+    return EMP_OK;
+}
+
+emp_status emp_server_step(emp_server *srv, emp_job **done, int cap, int *n_done) {
+    if (!srv || cap < 0 || (cap && !done)) return EMP_E_INVAL;
+    if (n_done) *n_done = 0;
+    if (cudaSetDevice(srv->ctx->device) != cudaSuccess) return EMP_E_CUDA;
+    cudaStream_t s = srv->ctx->stream;
+    emp_status st = server_step(srv, s);
+    if (st != EMP_OK) {
+        cudaStreamSynchronize(s);
+        cudaGetLastError();
+    }
+    const int k = (int)std::min<size_t>((size_t)cap, srv->finished.size());
+    for (int i = 0; i < k; ++i) {
+        done[i] = srv->finished[i];
+        done[i]->server = nullptr;
+    }
+    srv->finished.erase(srv->finished.begin(), srv->finished.begin() + k);
+    if (n_done) *n_done = k;
+    return st;
+}
+
+emp_status emp_server_counts(emp_server *srv, int *queued, int *in_flight, int *finished) {
+    if (!srv) return EMP_E_INVAL;
+    if (queued) *queued = (int)srv->queue.size();
+    if (in_flight) *in_flight = (int)srv->live.size();
+    if (finished) *finished = (int)srv->finished.size();
+    return EMP_OK;
 }
 
 emp_status emp_job_output_size(emp_job *job, uint64_t *bytes) {

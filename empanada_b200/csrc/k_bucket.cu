@@ -1273,9 +1273,11 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
     probe(ctl, iter, 8);
 }
 
-// After the last round: each round's record, edges from the staging buffer in
-// bucket order (rounds spread over the CTAs, no grid barrier).
-EMP_COLD void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
+// After the launch's last iteration (its run), for every job with no round left:
+// each round's record, edges from the staging buffer in bucket order (rounds
+// spread over the CTAs, no grid barrier).  Jobs that still have rounds are
+// left as they are for the next launch.
+EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_t *smem) {
     uint64_t *dest = reinterpret_cast<uint64_t *>(smem);  // nb + 1 bucket starts
     uint64_t *roff = dest + kBktMaxBuckets + 1;          // per round of the job: record offset,
     uint64_t *rE = roff + kT;                            // edge count,
@@ -1283,6 +1285,8 @@ EMP_COLD void place_edges(BktJob *jobs, int J, BShared &sh, uint8_t *smem) {
     uint32_t g = 0;
     for (int j = 0; j < J; ++j) {
         BktJob &x = jobs[j];
+        if (round_shape(x, x.iter0 + its).active) continue;  // resumes in the next launch
+        if (blockIdx.x == 0 && threadIdx.x == 0) x.done = 1;
         const uint32_t r0 = (uint32_t)x.r0;
         // the rounds that ran: round r ran iff r < rounds and it had a suffix
         // (build_graph's loop condition, overlap.cu:258)
@@ -1371,38 +1375,46 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
     for (uint32_t i = threadIdx.x; i < sizeof(HashTables) / 4; i += kT)
         reinterpret_cast<uint32_t *>(&sh.tab)[i] = reinterpret_cast<const uint32_t *>(jobs[0].tables)[i];
     __syncthreads();
-    // ---- prologue: the launch's input lists -> round r0's lists
-    uint32_t total = build_prefix(sh, J, [&](int j) -> uint32_t { return (uint32_t)bkt_tiles(jobs[j].n_in); });
+    // ---- prologue: the input lists of the jobs this launch starts -> their round r0 lists
+    uint32_t total = build_prefix(sh, J, [&](int j) -> uint32_t {
+        return jobs[j].iter0 == 0 ? (uint32_t)bkt_tiles(jobs[j].n_in) : 0u;
+    });
     tile_loop(sh, &ctl->ticket[0], J, total, [&](int j, uint32_t k) { prologue_tile(jobs[j], k, sh, smem); });
     if (!grid_barrier(ctl, &sh.flag, 0, 7)) return;
-    // ---- rounds: round r0 + iter of every job that still runs
-    for (uint32_t iter = 0;; ++iter) {
-        uint32_t *ticket = &ctl->ticket[1 + (iter & 1)];
-        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ticket[1 + ((iter + 1) & 1)] = 0;  // last iteration's
-        probe(ctl, iter, 0);
+    // ---- rounds: iteration iter0 + it of every job (round r0 + iter0 + it)
+    // that still runs, for at most iter_cap iterations; a job resumes in a
+    // later launch from the lists and counts the last iteration left behind
+    const uint32_t cap = ctl->iter_cap ? ctl->iter_cap : 0xffffffffu;
+    uint32_t it = 0;
+    for (; it < cap; ++it) {
+        uint32_t *ticket = &ctl->ticket[1 + (it & 1)];
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ticket[1 + ((it + 1) & 1)] = 0;  // last iteration's
+        probe(ctl, it, 0);
         total = build_prefix(sh, J, [&](int j) -> uint32_t {
-            const RoundShape z = round_shape(jobs[j], iter);
+            const RoundShape z = round_shape(jobs[j], jobs[j].iter0 + it);
             sh.shp_K[j] = z.K;
             sh.shp_nb[j] = z.nb;
             sh.shp_nbn[j] = z.nb_next;
             return z.active ? z.nb : 0u;
         });
         if (total == 0) break;  // no job has a round left
-        probe(ctl, iter, 1);
+        probe(ctl, it, 1);
         tile_loop_static(sh, ticket, J, total, [&](int j, uint32_t b) {
+            const uint32_t g = jobs[j].iter0 + it;
             RoundShape z;
             z.active = true;
-            z.r = jobs[j].r0 + (int)iter;
+            z.r = jobs[j].r0 + (int)g;
             z.K = sh.shp_K[j];
             z.nb = sh.shp_nb[j];
             z.nb_next = sh.shp_nbn[j];
-            round_tile(jobs[j], b, iter, z, sh, ctl, smem);
+            round_tile(jobs[j], b, g, z, sh, ctl, smem);
         });
-        probe(ctl, iter, 9);
-        if (!grid_barrier(ctl, &sh.flag, iter, 0)) return;
-        probe(ctl, iter, 10);
+        probe(ctl, it, 9);
+        if (!grid_barrier(ctl, &sh.flag, it, 0)) return;
+        probe(ctl, it, 10);
     }
-    place_edges(jobs, J, sh, smem);
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = it;
+    place_edges(jobs, J, it, sh, smem);
 }
 
 }  // namespace

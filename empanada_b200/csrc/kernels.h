@@ -234,6 +234,8 @@ struct CoopCtl {
     uint32_t trace_cap;  // iterations the trace holds
     uint32_t probe_iter;  // iteration whose per-CTA stamps go to `probe`
     uint64_t *probe;      // optional: kCoopProbePoints stamps per CTA (profiling)
+    uint32_t iter_cap;    // bucket kernel: iterations this launch runs at most (0: until every job is done)
+    uint32_t iters;       // bucket kernel: iterations it ran
 };
 constexpr int kCoopTracePhases = 8;
 constexpr int kCoopProbePoints = 32;
@@ -308,6 +310,8 @@ struct BktJob {
     uint32_t round;          // rounds run (set at the end of the launch)
     uint32_t wave;           // bucket counts are multiples of this (the grid for a job alone)
     uint32_t overflow;       // the edge buffer was too small
+    uint32_t iter0;          // iterations run by earlier launches (0: the launch starts the job)
+    uint32_t done;           // set at the end of a launch after which the job has no round left
     uint64_t e_total;        // edges of the finished rounds of this launch
     uint64_t e_stage;        // staging buffer fill
     BktRound *meta;          // [rounds + 1], zeroed; round r at meta[r]

@@ -46,6 +46,7 @@ typedef int emp_status;
 
 typedef struct emp_ctx emp_ctx;
 typedef struct emp_job emp_job;
+typedef struct emp_server emp_server;
 
 /* The reference's command-line options (config.h:282-290). */
 typedef struct emp_params {
@@ -134,6 +135,36 @@ emp_status emp_job_run(emp_job *job, void *stream);
  * emp_job_run's.  Returns the first failing job's status (jobs that failed
  * have no result; the others do), EMP_OK when all succeeded. */
 emp_status emp_batch_run(emp_ctx *ctx, emp_job **jobs, int njobs, void *stream);
+
+/* Status of the job's last run (emp_job_run, a batch or a server):
+ * EMP_E_STATE while it has none. */
+emp_status emp_job_status(emp_job *job);
+
+/* Served jobs (no counterpart in the reference, which is one process per
+ * read set): a request loop with continuous batching.  Fed jobs are
+ * submitted; each step admits queued jobs (first come, first served, while
+ * the footprint estimates of the jobs in flight stay within the budget: 4 B
+ * per FASTQ byte + 64 MiB per job), runs their map phase, adds them to the
+ * batch, and runs one bucket-kernel launch of at most rounds_per_launch
+ * rounds of every job in the batch; jobs join and leave the batch between
+ * launches.  A job too large for the batch, or whose rounds split into
+ * several search partitions, runs alone within the step.  Every job's output
+ * equals its emp_job_run output.  A job held by a server (submitted, not yet
+ * handed out by a step) accepts no other call. */
+typedef struct emp_server_params {
+    int32_t rounds_per_launch; /* bucket-kernel rounds per launch (default 16) */
+    int32_t max_jobs;          /* jobs in the batch at most, <= 1024 (default 256) */
+    uint64_t hbm_budget_bytes; /* admission budget (0: the context's, or none) */
+} emp_server_params;
+emp_status emp_server_params_default(emp_server_params *p);
+emp_status emp_server_create(emp_ctx *ctx, const emp_server_params *p, emp_server **out);
+/* Jobs still queued or in the batch are released without a result. */
+emp_status emp_server_destroy(emp_server *srv);
+emp_status emp_server_submit(emp_server *srv, emp_job *job);
+/* One step; up to cap finished jobs are handed out in done[0..*n_done)
+ * (each with emp_job_status set), the rest wait for the next step. */
+emp_status emp_server_step(emp_server *srv, emp_job **done, int cap, int *n_done);
+emp_status emp_server_counts(emp_server *srv, int *queued, int *in_flight, int *finished);
 
 /* output.bin bytes of the last run (write_edges_binary, overlap.cu:148-161). */
 emp_status emp_job_output_size(emp_job *job, uint64_t *bytes);

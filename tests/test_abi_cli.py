@@ -110,3 +110,23 @@ def test_engine_without_gpu_raises():
         pytest.skip("GPU present")
     with pytest.raises(empanada_b200.EmpError):
         empanada_b200.Engine(0)
+
+
+def test_server_and_batch_arguments_without_a_gpu():
+    """The serving and batch entry points validate their arguments before
+    touching a device."""
+    import ctypes
+
+    from empanada_b200 import _native
+
+    lib = _native.lib()
+    p = _native.ServerParams()
+    assert lib.emp_server_params_default(ctypes.byref(p)) == 0
+    assert (p.rounds_per_launch, p.max_jobs, p.hbm_budget_bytes) == (16, 256, 0)
+    out = ctypes.c_void_p()
+    assert lib.emp_server_create(None, ctypes.byref(p), ctypes.byref(out)) == _native.EMP_E_INVAL
+    assert lib.emp_server_submit(None, None) == _native.EMP_E_INVAL
+    assert lib.emp_server_step(None, None, 0, None) == _native.EMP_E_INVAL
+    assert lib.emp_server_destroy(None) == _native.EMP_E_INVAL
+    assert lib.emp_batch_run(None, None, 0, None) == _native.EMP_E_INVAL
+    assert lib.emp_job_status(None) == _native.EMP_E_INVAL
