@@ -189,6 +189,10 @@ class Job:
         """Drop the fed input and last result; keep the device buffers."""
         check(self._lib.emp_job_reset(self.handle), "emp_job_reset")
 
+    def trim(self) -> None:
+        """Drop the fed input and last result; give the device buffers back to the engine's pool."""
+        check(self._lib.emp_job_trim(self.handle), "emp_job_trim")
+
     def feed(self, data, last: bool = True) -> None:
         """Append host FASTQ bytes (bytes, bytearray or a uint8 numpy array)."""
         if isinstance(data, np.ndarray):
@@ -266,6 +270,11 @@ class Server:
         done = [self._held.pop(self._out[i]) for i in range(n.value)]
         check(rc, "emp_server_step")
         return done
+
+    def stats(self) -> dict:
+        st = _native.ServerStats()
+        check(self._lib.emp_server_get_stats(self.handle, ctypes.byref(st)), "emp_server_get_stats")
+        return {f: getattr(st, f) for f, _ in st._fields_}
 
     def counts(self) -> tuple[int, int, int]:
         q, f, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -46,6 +46,21 @@ class ServerParams(ctypes.Structure):
     ]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_uint64),
+        ("admitted", ctypes.c_uint64),
+        ("launches", ctypes.c_uint64),
+        ("rounds", ctypes.c_uint64),
+        ("batch_jobs", ctypes.c_uint64),
+        ("ms_kernel", ctypes.c_double),
+        ("ms_admit", ctypes.c_double),
+        ("ms_map", ctypes.c_double),
+        ("ms_alone", ctypes.c_double),
+        ("alone", ctypes.c_uint64),
+    ]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("n_reads", ctypes.c_uint64),
@@ -97,6 +112,7 @@ SIGNATURES = {
     "emp_job_feed_fastq_device": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int]),
     "emp_job_reserve": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "emp_job_reset": (ctypes.c_int, [_vp]),
+    "emp_job_trim": (ctypes.c_int, [_vp]),
     "emp_job_run": (ctypes.c_int, [_vp, _vp]),
     "emp_batch_run": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.c_int, _vp]),
     "emp_job_status": (ctypes.c_int, [_vp]),
@@ -105,6 +121,7 @@ SIGNATURES = {
     "emp_server_destroy": (ctypes.c_int, [_vp]),
     "emp_server_submit": (ctypes.c_int, [_vp, _vp]),
     "emp_server_step": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "emp_server_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStats)]),
     "emp_server_counts": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                          ctypes.POINTER(ctypes.c_int)]),
     "emp_job_output_size": (ctypes.c_int, [_vp, _u64p]),

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -32,14 +33,20 @@ namespace {
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    cudaStream_t pool_stream = nullptr;  // set: from the context's pool, freed in this stream's order
+    bool pooled = false;
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pooled) cudaFreeAsync(p, pool_stream);
+            else cudaFree(p);
+        }
         p = nullptr;
         bytes = 0;
+        pooled = false;
     }
     template <class T>
     T *as() const { return reinterpret_cast<T *>(p); }
@@ -48,12 +55,26 @@ struct DevBuf {
 struct PinnedBuf {
     void *p = nullptr;
     size_t bytes = 0;
-    ~PinnedBuf() { if (p) cudaFreeHost(p); }
-    bool ensure(size_t b) {
-        if (b <= bytes) return true;
-        if (p) cudaFreeHost(p);
+    bool owned = true;  // false: a piece of the context's host slab
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf &) = delete;
+    PinnedBuf &operator=(const PinnedBuf &) = delete;
+    ~PinnedBuf() { drop(); }
+    void drop() {
+        if (p && owned) cudaFreeHost(p);
         p = nullptr;
         bytes = 0;
+        owned = true;
+    }
+    void bind(void *q, size_t b) {
+        drop();
+        p = q;
+        bytes = b;
+        owned = false;
+    }
+    bool ensure(size_t b) {
+        if (b <= bytes) return true;
+        drop();
         size_t nb = b < 4096 ? 4096 : b + b / 2;
         if (cudaHostAlloc(&p, nb, cudaHostAllocDefault) != cudaSuccess) { p = nullptr; return false; }
         bytes = nb;
@@ -63,6 +84,38 @@ struct PinnedBuf {
     T *as() const { return reinterpret_cast<T *>(p); }
 };
 
+// Pinned host slots for the small per-job host words (counts, histograms,
+// launch descriptors, round records), carved from 4 MiB chunks: page-locking
+// a small buffer costs about a millisecond, so a job takes a slot instead.
+constexpr size_t kSlotBytes = 64 << 10;
+constexpr size_t kSlotChunk = 4 << 20;
+constexpr size_t kSlotMisc = 0, kSlotHist = 4 << 10, kSlotCoop = 12 << 10, kSlotCtl = 24 << 10,
+                 kSlotRecords = 28 << 10;
+struct HostSlab {
+    std::mutex mu;
+    std::vector<void *> chunks, free_slots;
+    ~HostSlab() {
+        for (void *c : chunks) cudaFreeHost(c);
+    }
+    void *take() {
+        std::lock_guard<std::mutex> g(mu);
+        if (free_slots.empty()) {
+            void *c = nullptr;
+            if (cudaHostAlloc(&c, kSlotChunk, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+            chunks.push_back(c);
+            for (size_t o = 0; o + kSlotBytes <= kSlotChunk; o += kSlotBytes)
+                free_slots.push_back(static_cast<uint8_t *>(c) + o);
+        }
+        void *q = free_slots.back();
+        free_slots.pop_back();
+        return q;
+    }
+    void give(void *q) {
+        std::lock_guard<std::mutex> g(mu);
+        free_slots.push_back(q);
+    }
+};
+
 }  // namespace
 
 struct emp_ctx {
@@ -70,11 +123,15 @@ struct emp_ctx {
     uint64_t budget = 0;
     uint64_t in_use = 0;
     cudaStream_t stream = nullptr;
+    // device memory of the jobs' work buffers: a stream-ordered pool that keeps
+    // what is freed, so that a job's buffers come and go without cudaMalloc
+    cudaMemPool_t pool = nullptr;
     DevBuf tables;  // HashTables
     // emp_sort_pairs working set, kept for the next call
     DevBuf sort_k1, sort_v1, sort_scr, sort_err;
     uint64_t sort_cap = 0;
     uint64_t sort_calls = 0;
+    HostSlab slab;
     // emp_batch_run: the BktJob array and control block of one launch, their
     // host copies, and the launch's events
     DevBuf batch_jobs, batch_ctl;
@@ -130,6 +187,8 @@ struct emp_job {
     uint64_t admit_est = 0;
     emp_server *server = nullptr;
     emp_status last_rc = EMP_E_STATE;  // status of the last run (EMP_E_STATE: none yet)
+    void *slot = nullptr;              // the job's slot of the context's host slab
+    cudaStream_t stream = nullptr;     // stream of the current run
     // results
     std::vector<uint8_t> out;
     emp_stats st{};
@@ -147,25 +206,38 @@ constexpr emp_status kNeedEdgeRoom = -1000;
 
 emp_status cuda_status(cudaError_t e) { return e == cudaSuccess ? EMP_OK : (e == cudaErrorMemoryAllocation ? EMP_E_NOMEM : EMP_E_CUDA); }
 
-emp_status ctx_ensure(emp_ctx *c, DevBuf &b, size_t bytes) {
+// Grow b to at least `bytes` from the context's pool, in the order of stream
+// s (the old contents are not kept).
+emp_status ctx_ensure(emp_ctx *c, DevBuf &b, size_t bytes, cudaStream_t s) {
     if (bytes <= b.bytes) return EMP_OK;
     const size_t old = b.bytes;
     if (c->budget && c->in_use - old + bytes > c->budget) return EMP_E_NOMEM;
+    if (b.p && b.pooled) {
+        cudaFreeAsync(b.p, s);
+        b.p = nullptr;
+        b.bytes = 0;
+        b.pooled = false;
+    }
     b.release();
     c->in_use -= old;
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, c->pool, s);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return EMP_E_NOMEM;
     }
     b.p = p;
     b.bytes = bytes;
+    b.pooled = true;
+    b.pool_stream = c->stream;
     c->in_use += bytes;
     return EMP_OK;
 }
 
-emp_status ensure(emp_job *j, DevBuf &b, size_t bytes) { return ctx_ensure(j->ctx, b, bytes); }
+// a job's buffers grow in the order of the stream its current run uses
+emp_status ensure(emp_job *j, DevBuf &b, size_t bytes) {
+    return ctx_ensure(j->ctx, b, bytes, j->stream ? j->stream : j->ctx->stream);
+}
 
 void free_buf(emp_job *j, DevBuf &b) {
     j->ctx->in_use -= b.bytes;
@@ -1008,6 +1080,7 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
 // set once the job has nothing more to run.
 emp_status map_begin(emp_job *j, cudaStream_t s) {
     emp_stats &st = j->st;
+    j->stream = s;
     std::memset(&st, 0, sizeof st);
     j->out.clear();
     j->dout_bytes = 0;
@@ -1256,8 +1329,8 @@ bool batch_eligible(const emp_job *j) {
 emp_status batch_rounds(emp_ctx *ctx, emp_job **jobs, const std::vector<int> &idx, std::vector<emp_status> &rc,
                         cudaStream_t s) {
     const size_t nb = idx.size();
-    EMP_TRY(ctx_ensure(ctx, ctx->batch_jobs, nb * sizeof(BktJob)));
-    EMP_TRY(ctx_ensure(ctx, ctx->batch_ctl, sizeof(CoopCtl)));
+    EMP_TRY(ctx_ensure(ctx, ctx->batch_jobs, nb * sizeof(BktJob), s));
+    EMP_TRY(ctx_ensure(ctx, ctx->batch_ctl, sizeof(CoopCtl), s));
     if (!ctx->h_batch.ensure(nb * sizeof(BktJob) + sizeof(CoopCtl))) return EMP_E_NOMEM;
     if (!ctx->batch_ev[0]) {
         for (auto &e : ctx->batch_ev) EMP_CUDA(cudaEventCreate(&e));
@@ -1400,7 +1473,7 @@ struct emp_server {
     DevBuf d_jobs, d_ctl;
     PinnedBuf h_jobs;
     cudaEvent_t ev[2] = {};
-    uint64_t launches = 0;
+    emp_server_stats st{};
 };
 
 namespace {
@@ -1418,6 +1491,9 @@ void server_complete(emp_server *srv, emp_job *j) {
 // jobs with no round left complete.
 emp_status server_step(emp_server *srv, cudaStream_t s) {
     emp_ctx *ctx = srv->ctx;
+    emp_server_stats &ss = srv->st;
+    ss.steps += 1;
+    const auto t0 = std::chrono::steady_clock::now();
     const uint64_t budget = srv->p.hbm_budget_bytes ? srv->p.hbm_budget_bytes : ctx->budget;
     std::vector<emp_job *> adm;
     while (!srv->queue.empty() && (int)(srv->live.size() + adm.size()) < srv->p.max_jobs) {
@@ -1433,6 +1509,8 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         const int n = (int)adm.size();
         std::vector<emp_status> rc((size_t)n, EMP_OK);
         EMP_TRY(map_batch(adm.data(), n, rc, s));
+        const auto t1 = std::chrono::steady_clock::now();
+        ss.ms_map += std::chrono::duration<double, std::milli>(t1 - t0).count();
         std::vector<emp_job *> close;
         std::vector<emp_status> crc;
         for (int i = 0; i < n; ++i) {
@@ -1446,7 +1524,10 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
                     continue;
                 }
             } else if (rc[i] == EMP_OK && !q.done) {
+                const auto ta = std::chrono::steady_clock::now();
                 rc[i] = job_rounds(j, s);  // too large for the batch, or rounds that split: alone
+                ss.alone += 1;
+                ss.ms_alone += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
             }
             close.push_back(j);
             crc.push_back(rc[i]);
@@ -1455,11 +1536,13 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
             close_jobs(close.data(), (int)close.size(), crc, s);
             for (emp_job *j : close) server_complete(srv, j);
         }
+        ss.admitted += (uint64_t)n;
+        ss.ms_admit += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     if (srv->live.empty()) return EMP_OK;
     const size_t nb = srv->live.size();
-    EMP_TRY(ctx_ensure(ctx, srv->d_jobs, nb * sizeof(BktJob)));
-    EMP_TRY(ctx_ensure(ctx, srv->d_ctl, sizeof(CoopCtl)));
+    EMP_TRY(ctx_ensure(ctx, srv->d_jobs, nb * sizeof(BktJob), s));
+    EMP_TRY(ctx_ensure(ctx, srv->d_ctl, sizeof(CoopCtl), s));
     if (!srv->h_jobs.ensure(nb * sizeof(BktJob) + sizeof(CoopCtl))) return EMP_E_NOMEM;
     if (!srv->ev[0]) {
         for (auto &e : srv->ev) EMP_CUDA(cudaEventCreate(&e));
@@ -1479,9 +1562,12 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
     EMP_CUDA(cudaMemcpyAsync(hj, srv->d_jobs.p, nb * sizeof(BktJob), cudaMemcpyDeviceToHost, s));
     EMP_CUDA(cudaMemcpyAsync(hc, srv->d_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
     EMP_CUDA(cudaStreamSynchronize(s));
-    ++srv->launches;
     const bool timed_out = (hc->err & kErrSpin) != 0;
     const float ms = ms_between(srv->ev[0], srv->ev[1]);
+    ss.launches += 1;
+    ss.rounds += hc->iters;
+    ss.batch_jobs += nb;
+    ss.ms_kernel += ms;
     std::vector<emp_job *> still, done;
     for (size_t k = 0; k < nb; ++k) {
         emp_job *j = srv->live[k];
@@ -1600,9 +1686,22 @@ emp_status emp_ctx_create(int device, uint64_t hbm_budget_bytes, emp_ctx **out) 
         delete c;
         return EMP_E_CUDA;
     }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&c->pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return EMP_E_CUDA;
+    }
+    uint64_t keep = ~0ull;  // keep freed memory in the pool
+    cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     void *p = nullptr;
     if (cudaMalloc(&p, sizeof(HashTables)) != cudaSuccess) {
         cudaStreamDestroy(c->stream);
+        cudaMemPoolDestroy(c->pool);
         delete c;
         return EMP_E_NOMEM;
     }
@@ -1612,6 +1711,7 @@ emp_status emp_ctx_create(int device, uint64_t hbm_budget_bytes, emp_ctx **out) 
     host_tables(h);
     if (cudaMemcpy(p, &h, sizeof h, cudaMemcpyHostToDevice) != cudaSuccess) {
         cudaStreamDestroy(c->stream);
+        cudaMemPoolDestroy(c->pool);
         delete c;
         return EMP_E_CUDA;
     }
@@ -1623,10 +1723,14 @@ emp_status emp_ctx_destroy(emp_ctx *ctx) {
     if (!ctx) return EMP_E_INVAL;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    cudaStreamDestroy(ctx->stream);
     for (auto &e : ctx->batch_ev)
         if (e) cudaEventDestroy(e);
     ctx->in_use -= ctx->batch_jobs.bytes + ctx->batch_ctl.bytes;
+    ctx->batch_jobs.release();
+    ctx->batch_ctl.release();
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return EMP_OK;
 }
@@ -1651,7 +1755,46 @@ emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out) {
             return EMP_E_CUDA;
         }
     }
+    static_assert(kSlotHist >= kMiscSlots * sizeof(uint64_t) && kSlotCoop - kSlotHist >= kSortPasses * kSortRadix * 4,
+                  "slab layout");
+    static_assert(kSlotCtl - kSlotCoop >= sizeof(CoopJob) + sizeof(CoopCtl) &&
+                      kSlotCtl - kSlotCoop >= sizeof(BktJob) + sizeof(CoopCtl),
+                  "slab layout");
+    static_assert(kSlotRecords - kSlotCtl >= sizeof(RoundCtl) &&
+                      kSlotBytes - kSlotRecords >= EMP_MAX_ROUNDS * sizeof(RoundRecord),
+                  "slab layout");
+    j->slot = ctx->slab.take();
+    if (!j->slot) {
+        emp_job_destroy(j);
+        return EMP_E_NOMEM;
+    }
+    uint8_t *sl = static_cast<uint8_t *>(j->slot);
+    j->h_misc.bind(sl + kSlotMisc, kSlotHist - kSlotMisc);
+    j->h_hist.bind(sl + kSlotHist, kSlotCoop - kSlotHist);
+    j->h_coop.bind(sl + kSlotCoop, kSlotCtl - kSlotCoop);
+    j->h_ctl.bind(sl + kSlotCtl, kSlotRecords - kSlotCtl);
+    j->h_records.bind(sl + kSlotRecords, kSlotBytes - kSlotRecords);
     *out = j;
+    return EMP_OK;
+}
+
+static void release_buffers(emp_job *job);
+
+emp_status emp_job_trim(emp_job *job) {
+    if (!job) return EMP_E_INVAL;
+    if (job->server) return EMP_E_STATE;
+    cudaSetDevice(job->ctx->device);
+    cudaStreamSynchronize(job->ctx->stream);
+    release_graph(job);
+    release_buffers(job);
+    job->F = 0;
+    job->fed_last = false;
+    job->ms_h2d = 0.0;
+    job->have_result = false;
+    job->out.clear();
+    job->dout_bytes = 0;
+    job->n_ends = 0;
+    job->last_rc = EMP_E_STATE;
     return EMP_OK;
 }
 
@@ -1660,6 +1803,28 @@ emp_status emp_job_destroy(emp_job *job) {
     if (job->server) return EMP_E_STATE;
     cudaSetDevice(job->ctx->device);
     cudaStreamSynchronize(job->ctx->stream);
+    release_buffers(job);
+    for (auto &e : job->sort_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : job->upd_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : job->map_ev)
+        if (e) cudaEventDestroy(e);
+    release_graph(job);
+    if (job->slot) {
+        job->h_misc.drop();
+        job->h_hist.drop();
+        job->h_coop.drop();
+        job->h_ctl.drop();
+        job->h_records.drop();
+        job->ctx->slab.give(job->slot);
+    }
+    delete job;
+    return EMP_OK;
+}
+
+// every device buffer of the job back to the context (its pool)
+static void release_buffers(emp_job *job) {
     DevBuf *bufs[] = {&job->fq, &job->tile_counts, &job->tile_excl, &job->status, &job->misc, &job->seq_start,
                       &job->seq_end, &job->hq, &job->idx, &job->rec_of, &job->keys0, &job->cols, &job->seq2, &job->sk0,
                       &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
@@ -1673,15 +1838,7 @@ emp_status emp_job_destroy(emp_job *job) {
                       &job->bk_meta, &job->xk0, &job->xv0, &job->xk1, &job->xv1, &job->ring_k, &job->ring_v,
                       &job->cparts};
     for (DevBuf *b : bufs) free_buf(job, *b);
-    for (auto &e : job->sort_ev)
-        if (e) cudaEventDestroy(e);
-    for (auto &e : job->upd_ev)
-        if (e) cudaEventDestroy(e);
-    for (auto &e : job->map_ev)
-        if (e) cudaEventDestroy(e);
-    release_graph(job);
-    delete job;
-    return EMP_OK;
+    job->sorts_since_clear = 0;
 }
 
 emp_status emp_job_reserve(emp_job *job, uint64_t bytes) {
@@ -1692,22 +1849,25 @@ emp_status emp_job_reserve(emp_job *job, uint64_t bytes) {
     DevBuf nb;
     emp_ctx *c = job->ctx;
     if (c->budget && c->in_use + bytes > c->budget) return EMP_E_NOMEM;
-    if (cudaMalloc(&nb.p, bytes + 16) != cudaSuccess) {
+    if (cudaMallocFromPoolAsync(&nb.p, bytes + 16, c->pool, c->stream) != cudaSuccess) {
         cudaGetLastError();
         return EMP_E_NOMEM;
     }
     nb.bytes = bytes + 16;
+    nb.pooled = true;
+    nb.pool_stream = c->stream;
     c->in_use += nb.bytes;
-    if (job->F) {
-        if (cudaMemcpyAsync(nb.p, job->fq.p, job->F, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess ||
-            cudaStreamSynchronize(c->stream) != cudaSuccess)
-            return EMP_E_CUDA;
-    }
+    if (job->F && cudaMemcpyAsync(nb.p, job->fq.p, job->F, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+        return EMP_E_CUDA;
     free_buf(job, job->fq);
     job->fq.p = nb.p;
     job->fq.bytes = nb.bytes;
+    job->fq.pooled = true;
+    job->fq.pool_stream = c->stream;
     nb.p = nullptr;
     nb.bytes = 0;
+    nb.pooled = false;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return EMP_E_CUDA;
     return EMP_OK;
 }
 
@@ -1869,6 +2029,12 @@ emp_status emp_server_step(emp_server *srv, emp_job **done, int cap, int *n_done
     srv->finished.erase(srv->finished.begin(), srv->finished.begin() + k);
     if (n_done) *n_done = k;
     return st;
+}
+
+emp_status emp_server_get_stats(emp_server *srv, emp_server_stats *st) {
+    if (!srv || !st) return EMP_E_INVAL;
+    *st = srv->st;
+    return EMP_OK;
 }
 
 emp_status emp_server_counts(emp_server *srv, int *queued, int *in_flight, int *finished) {

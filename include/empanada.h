@@ -120,6 +120,11 @@ emp_status emp_job_reserve(emp_job *job, uint64_t bytes);
 /* Forget the fed input and the last result but keep every device buffer, so
  * the job can take the next read set without new allocations. */
 emp_status emp_job_reset(emp_job *job);
+/* Forget the fed input and the last result and give every device buffer
+ * back to the context's memory pool (stream-ordered, no device-wide
+ * synchronisation), so that idle jobs hold no device memory; the next run
+ * takes its buffers from the pool again. */
+emp_status emp_job_trim(emp_job *job);
 
 /* Map + reduce phases: main.cu:42-71 (read_block, transpose_reads,
  * get_reverse_complements, generate_fingerprint_read_pairs) and build_graph
@@ -165,6 +170,19 @@ emp_status emp_server_submit(emp_server *srv, emp_job *job);
  * (each with emp_job_status set), the rest wait for the next step. */
 emp_status emp_server_step(emp_server *srv, emp_job **done, int cap, int *n_done);
 emp_status emp_server_counts(emp_server *srv, int *queued, int *in_flight, int *finished);
+typedef struct emp_server_stats {
+    uint64_t steps;      /* emp_server_step calls */
+    uint64_t admitted;   /* jobs admitted */
+    uint64_t launches;   /* bucket-kernel launches */
+    uint64_t rounds;     /* launch iterations (each runs one round of every job in the batch) */
+    uint64_t batch_jobs; /* sum over launches of the jobs in the batch */
+    double ms_kernel;    /* device time of those launches */
+    double ms_admit;     /* host wall time of admission + map phase + jobs run alone */
+    double ms_map;       /* of which the map phase */
+    double ms_alone;     /* of which jobs run alone */
+    uint64_t alone;      /* jobs run alone */
+} emp_server_stats;
+emp_status emp_server_get_stats(emp_server *srv, emp_server_stats *st);
 
 /* output.bin bytes of the last run (write_edges_binary, overlap.cu:148-161). */
 emp_status emp_job_output_size(emp_job *job, uint64_t *bytes);

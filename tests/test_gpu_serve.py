@@ -144,3 +144,27 @@ def test_served_job_is_held(engine):
     j.run()
     assert hashlib.sha256(j.output()).hexdigest() == GOLDEN["tiny"]["sha256"]
     j.close()
+
+
+@pytest.mark.gpu
+def test_trim_returns_buffers_and_job_runs_again(engine):
+    """emp_job_trim drops the result and the device buffers; the job then
+    takes another read set (a larger one) and gives the same bytes as a
+    fresh job."""
+    j = _job(engine, "tiny")
+    j.run()
+    first = j.output()
+    j.trim()
+    with pytest.raises(_native.EmpError) as e:
+        j.output()
+    assert e.value.code == _native.EMP_E_STATE
+    other = synth.fastq_bytes(synth.batched_sets(n_sets=1, seed=13, genome_max=200_000)[0])
+    j.feed(other)
+    j.run()
+    fresh, _ = empanada_b200.run_bytes(other, engine=engine, min_ovlp=31)
+    assert j.output() == fresh
+    j.trim()
+    j.feed(BY_NAME["tiny"].fastq())
+    j.run()
+    assert j.output() == first
+    j.close()
