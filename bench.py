@@ -442,7 +442,7 @@ def served_bench(args):
                         i, k = pending.popleft()
                         j = get_job(k)
                         j.reset()
-                        j.feed(host_np[offs[k]:offs[k + 1]], last=True)
+                        j.feed_async(host_np[offs[k]:offs[k + 1]], last=True)
                         srv.submit(j)
                         held[j.handle.value] = (i, k)
                 t2 = time.perf_counter()

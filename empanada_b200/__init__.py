@@ -202,6 +202,14 @@ class Job:
             buf = bytes(data)
             check(self._lib.emp_job_feed_fastq(self.handle, ctypes.c_char_p(buf), len(buf), int(last)), "feed")
 
+    def feed_async(self, arr: np.ndarray, last: bool = True) -> None:
+        """feed() without waiting for the copy; arr (uint8, contiguous, ideally
+        page-locked) must stay unchanged until the job's next run starts."""
+        if arr.dtype != np.uint8 or not arr.flags.c_contiguous:
+            raise ValueError("feed_async takes a contiguous uint8 array")
+        self._async_keep = arr
+        check(self._lib.emp_job_feed_fastq_async(self.handle, arr.ctypes.data, arr.size, int(last)), "feed_async")
+
     def feed_device(self, ptr: int, nbytes: int, last: bool = True) -> None:
         check(self._lib.emp_job_feed_fastq_device(self.handle, ptr, nbytes, int(last)), "feed_device")
 

@@ -110,6 +110,7 @@ SIGNATURES = {
     "emp_job_destroy": (ctypes.c_int, [_vp]),
     "emp_job_feed_fastq": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int]),
     "emp_job_feed_fastq_device": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int]),
+    "emp_job_feed_fastq_async": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int]),
     "emp_job_reserve": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "emp_job_reset": (ctypes.c_int, [_vp]),
     "emp_job_trim": (ctypes.c_int, [_vp]),

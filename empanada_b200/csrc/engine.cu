@@ -123,6 +123,7 @@ struct emp_ctx {
     uint64_t budget = 0;
     uint64_t in_use = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // asynchronous FASTQ feeds
     // device memory of the jobs' work buffers: a stream-ordered pool that keeps
     // what is freed, so that a job's buffers come and go without cudaMalloc
     cudaMemPool_t pool = nullptr;
@@ -181,6 +182,10 @@ struct emp_job {
     // map-phase state (map_begin .. map_list) and its events
     JobPrep prep;
     cudaEvent_t map_ev[5] = {};
+    // asynchronous feeds: copies on the context's copy stream, bracketed by
+    // these events; the next run waits for feed_ev[1]
+    cudaEvent_t feed_ev[2] = {};
+    bool feed_pending = false;
     // served: the job's bucket-kernel descriptor between launches, its
     // admission estimate, and whether a server holds it
     BktJob bk{};
@@ -276,6 +281,16 @@ struct Events {
     Events() { for (auto &x : e) cudaEventCreate(&x); }
     ~Events() { for (auto &x : e) cudaEventDestroy(x); }
 };
+
+float ms_between(cudaEvent_t a, cudaEvent_t b);
+// time between two events that may not have completed yet: 0 until they have
+float ms_between_later(cudaEvent_t a, cudaEvent_t b) {
+    if (cudaEventQuery(b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0.f;
+    }
+    return ms_between(a, b);
+}
 
 float ms_between(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0.f;
@@ -1081,6 +1096,11 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
 emp_status map_begin(emp_job *j, cudaStream_t s) {
     emp_stats &st = j->st;
     j->stream = s;
+    if (j->feed_pending) {  // the FASTQ is still being copied in
+        EMP_CUDA(cudaStreamWaitEvent(s, j->feed_ev[1], 0));
+        j->feed_pending = false;
+        j->ms_h2d += ms_between_later(j->feed_ev[0], j->feed_ev[1]);
+    }
     std::memset(&st, 0, sizeof st);
     j->out.clear();
     j->dout_bytes = 0;
@@ -1698,6 +1718,12 @@ emp_status emp_ctx_create(int device, uint64_t hbm_budget_bytes, emp_ctx **out) 
     }
     uint64_t keep = ~0ull;  // keep freed memory in the pool
     cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        cudaMemPoolDestroy(c->pool);
+        delete c;
+        return EMP_E_CUDA;
+    }
     void *p = nullptr;
     if (cudaMalloc(&p, sizeof(HashTables)) != cudaSuccess) {
         cudaStreamDestroy(c->stream);
@@ -1730,6 +1756,8 @@ emp_status emp_ctx_destroy(emp_ctx *ctx) {
     ctx->batch_ctl.release();
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return EMP_OK;
@@ -1785,6 +1813,8 @@ emp_status emp_job_trim(emp_job *job) {
     if (job->server) return EMP_E_STATE;
     cudaSetDevice(job->ctx->device);
     cudaStreamSynchronize(job->ctx->stream);
+    if (job->feed_pending) cudaEventSynchronize(job->feed_ev[1]);
+    job->feed_pending = false;
     release_graph(job);
     release_buffers(job);
     job->F = 0;
@@ -1803,6 +1833,9 @@ emp_status emp_job_destroy(emp_job *job) {
     if (job->server) return EMP_E_STATE;
     cudaSetDevice(job->ctx->device);
     cudaStreamSynchronize(job->ctx->stream);
+    if (job->feed_pending) cudaEventSynchronize(job->feed_ev[1]);
+    for (auto &e : job->feed_ev)
+        if (e) cudaEventDestroy(e);
     release_buffers(job);
     for (auto &e : job->sort_ev)
         if (e) cudaEventDestroy(e);
@@ -1846,6 +1879,7 @@ emp_status emp_job_reserve(emp_job *job, uint64_t bytes) {
     if (job->server) return EMP_E_STATE;
     if (bytes <= job->fq.bytes) return EMP_OK;
     cudaSetDevice(job->ctx->device);
+    if (job->feed_pending && cudaEventSynchronize(job->feed_ev[1]) != cudaSuccess) return EMP_E_CUDA;
     DevBuf nb;
     emp_ctx *c = job->ctx;
     if (c->budget && c->in_use + bytes > c->budget) return EMP_E_NOMEM;
@@ -1876,6 +1910,8 @@ emp_status emp_job_reset(emp_job *job) {
     if (job->server) return EMP_E_STATE;
     cudaSetDevice(job->ctx->device);
     cudaStreamSynchronize(job->ctx->stream);
+    if (job->feed_pending) cudaEventSynchronize(job->feed_ev[1]);
+    job->feed_pending = false;
     job->F = 0;
     job->fed_last = false;
     job->ms_h2d = 0.0;
@@ -1891,6 +1927,11 @@ static emp_status feed(emp_job *job, const void *src, uint64_t n, int last, cuda
     if (job->server) return EMP_E_STATE;
     if (job->fed_last) return EMP_E_STATE;
     cudaSetDevice(job->ctx->device);
+    if (job->feed_pending) {
+        if (cudaEventSynchronize(job->feed_ev[1]) != cudaSuccess) return EMP_E_CUDA;
+        job->ms_h2d += ms_between(job->feed_ev[0], job->feed_ev[1]);
+        job->feed_pending = false;
+    }
     if (job->F + n > job->fq.bytes) {
         uint64_t want = job->F + n;
         if (!last) want += want / 2;
@@ -1916,6 +1957,48 @@ static emp_status feed(emp_job *job, const void *src, uint64_t n, int last, cuda
 
 emp_status emp_job_feed_fastq(emp_job *job, const char *bytes, uint64_t n, int last) {
     return feed(job, bytes, n, last, cudaMemcpyHostToDevice);
+}
+
+emp_status emp_job_feed_fastq_async(emp_job *job, const char *bytes, uint64_t n, int last) {
+    if (!job || (n && !bytes)) return EMP_E_INVAL;
+    if (job->server) return EMP_E_STATE;
+    if (job->fed_last) return EMP_E_STATE;
+    cudaSetDevice(job->ctx->device);
+    emp_ctx *c = job->ctx;
+    cudaStream_t cs = c->copy_stream;
+    if (!job->feed_ev[0]) {
+        for (auto &e : job->feed_ev) EMP_CUDA(cudaEventCreate(&e));
+    }
+    if (!job->feed_pending) EMP_CUDA(cudaEventRecord(job->feed_ev[0], cs));
+    if (job->F + n > job->fq.bytes) {  // grow in the copy stream's order
+        uint64_t want = job->F + n;
+        if (!last) want += want / 2;
+        if (c->budget && c->in_use - job->fq.bytes + want + 16 > c->budget) return EMP_E_NOMEM;
+        void *p = nullptr;
+        if (cudaMallocFromPoolAsync(&p, want + 16, c->pool, cs) != cudaSuccess) {
+            cudaGetLastError();
+            return EMP_E_NOMEM;
+        }
+        if (job->F) EMP_CUDA(cudaMemcpyAsync(p, job->fq.p, job->F, cudaMemcpyDeviceToDevice, cs));
+        if (job->fq.p) {
+            if (job->fq.pooled) cudaFreeAsync(job->fq.p, cs);
+            else {
+                cudaStreamSynchronize(cs);
+                cudaFree(job->fq.p);
+            }
+        }
+        c->in_use += want + 16 - job->fq.bytes;
+        job->fq.p = p;
+        job->fq.bytes = want + 16;
+        job->fq.pooled = true;
+        job->fq.pool_stream = c->stream;
+    }
+    if (n) EMP_CUDA(cudaMemcpyAsync(job->fq.as<uint8_t>() + job->F, bytes, n, cudaMemcpyHostToDevice, cs));
+    EMP_CUDA(cudaEventRecord(job->feed_ev[1], cs));
+    job->feed_pending = true;
+    job->F += n;
+    if (last) job->fed_last = true;
+    return EMP_OK;
 }
 
 emp_status emp_job_feed_fastq_device(emp_job *job, const void *dev_bytes, uint64_t n, int last) {

@@ -113,6 +113,11 @@ emp_status emp_job_destroy(emp_job *job);
  * replaces read_block's file reads (preprocess.cu:195-237).  `last` marks
  * the final piece. */
 emp_status emp_job_feed_fastq(emp_job *job, const char *bytes, uint64_t n, int last);
+/* emp_job_feed_fastq without waiting for the copy: it runs on the
+ * context's copy stream (concurrently with other jobs' kernels) and the
+ * job's next run waits for it.  `bytes` must stay valid and unchanged until
+ * then; page-locked memory makes the copy truly asynchronous. */
+emp_status emp_job_feed_fastq_async(emp_job *job, const char *bytes, uint64_t n, int last);
 /* Same for bytes already in device memory on the context's device. */
 emp_status emp_job_feed_fastq_device(emp_job *job, const void *dev_bytes, uint64_t n, int last);
 /* Reserve device room for `bytes` of FASTQ (optional; avoids regrowth). */

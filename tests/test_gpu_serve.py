@@ -168,3 +168,28 @@ def test_trim_returns_buffers_and_job_runs_again(engine):
     j.run()
     assert j.output() == first
     j.close()
+
+
+@pytest.mark.gpu
+def test_feed_async_pieces(engine):
+    """Asynchronous feeds (page-locked pieces, split at arbitrary bytes, mixed
+    with a synchronous one) give the reference's bytes."""
+    import numpy as np
+    import torch
+
+    data = BY_NAME["sub_errors"].fastq()
+    host = torch.empty(len(data), dtype=torch.uint8, pin_memory=True).numpy()
+    host[:] = np.frombuffer(data, dtype=np.uint8)
+    a, b = len(data) // 3, 2 * len(data) // 3
+    with engine.job(min_ovlp=40) as j:
+        j.feed_async(host[:a], last=False)
+        j.feed_async(host[a:b], last=False)
+        j.feed(host[b:], last=True)
+        j.run()
+        assert hashlib.sha256(j.output()).hexdigest() == GOLDEN["sub_errors"]["sha256"]
+        j.reset()
+        j.feed_async(host[:b], last=False)
+        j.feed_async(host[b:], last=True)
+        j.run()
+        assert hashlib.sha256(j.output()).hexdigest() == GOLDEN["sub_errors"]["sha256"]
+        assert j.stats()["ms_h2d"] >= 0.0
