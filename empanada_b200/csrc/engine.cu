@@ -1505,15 +1505,15 @@ void server_complete(emp_server *srv, emp_job *j) {
     srv->finished.push_back(j);
 }
 
-// Admit queued jobs and run their map phase; start the eligible ones in the
-// batch, run the others alone; then one bucket-kernel launch of at most
-// rounds_per_launch iterations over every job in the batch, after which the
-// jobs with no round left complete.
+// One step: the launch of at most rounds_per_launch rounds of every job in
+// the batch goes first, so that the FASTQ copies of newly admitted jobs run
+// beside it; then the admitted jobs' map phase (queued behind the launch),
+// the eligible ones joining the batch for the next step and the others run
+// alone; then the launch's results: jobs with no round left complete.
 emp_status server_step(emp_server *srv, cudaStream_t s) {
     emp_ctx *ctx = srv->ctx;
     emp_server_stats &ss = srv->st;
     ss.steps += 1;
-    const auto t0 = std::chrono::steady_clock::now();
     const uint64_t budget = srv->p.hbm_budget_bytes ? srv->p.hbm_budget_bytes : ctx->budget;
     std::vector<emp_job *> adm;
     while (!srv->queue.empty() && (int)(srv->live.size() + adm.size()) < srv->p.max_jobs) {
@@ -1525,7 +1525,36 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         j->admit_est = est;
         adm.push_back(j);
     }
+    // ---- the launch (not waited for yet)
+    const size_t nb = srv->live.size();
+    BktJob *hj = nullptr;
+    CoopCtl *hc = nullptr;
+    if (nb) {
+        EMP_TRY(ctx_ensure(ctx, srv->d_jobs, nb * sizeof(BktJob), s));
+        EMP_TRY(ctx_ensure(ctx, srv->d_ctl, sizeof(CoopCtl), s));
+        if (!srv->h_jobs.ensure(nb * sizeof(BktJob) + sizeof(CoopCtl))) return EMP_E_NOMEM;
+        if (!srv->ev[0]) {
+            for (auto &e : srv->ev) EMP_CUDA(cudaEventCreate(&e));
+        }
+        hj = srv->h_jobs.as<BktJob>();
+        hc = reinterpret_cast<CoopCtl *>(hj + nb);
+        for (size_t k = 0; k < nb; ++k) hj[k] = srv->live[k]->bk;
+        std::memset(hc, 0, sizeof(CoopCtl));
+        hc->njobs = (uint32_t)nb;
+        hc->active = (uint32_t)nb;
+        hc->iter_cap = (uint32_t)srv->p.rounds_per_launch;
+        EMP_CUDA(cudaMemcpyAsync(srv->d_jobs.p, hj, nb * sizeof(BktJob), cudaMemcpyHostToDevice, s));
+        EMP_CUDA(cudaMemcpyAsync(srv->d_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
+        EMP_CUDA(cudaEventRecord(srv->ev[0], s));
+        EMP_CUDA(launch_bucket_rounds(srv->d_jobs.as<BktJob>(), srv->d_ctl.as<CoopCtl>(), err_word(srv->live[0]), s));
+        EMP_CUDA(cudaEventRecord(srv->ev[1], s));
+        EMP_CUDA(cudaMemcpyAsync(hj, srv->d_jobs.p, nb * sizeof(BktJob), cudaMemcpyDeviceToHost, s));
+        EMP_CUDA(cudaMemcpyAsync(hc, srv->d_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
+    }
+    // ---- the admitted jobs' map phase
+    std::vector<emp_job *> joining;
     if (!adm.empty()) {
+        const auto t0 = std::chrono::steady_clock::now();
         const int n = (int)adm.size();
         std::vector<emp_status> rc((size_t)n, EMP_OK);
         EMP_TRY(map_batch(adm.data(), n, rc, s));
@@ -1540,7 +1569,7 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
                 rc[i] = rounds_prelude(j, s);
                 if (rc[i] == EMP_OK) rc[i] = bucket_prepare(j, s, job_env(j), 0, 0, 2 * q.U, q.ecap, 1u, &j->bk);
                 if (rc[i] == EMP_OK) {
-                    srv->live.push_back(j);
+                    joining.push_back(j);
                     continue;
                 }
             } else if (rc[i] == EMP_OK && !q.done) {
@@ -1559,28 +1588,11 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         ss.admitted += (uint64_t)n;
         ss.ms_admit += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
-    if (srv->live.empty()) return EMP_OK;
-    const size_t nb = srv->live.size();
-    EMP_TRY(ctx_ensure(ctx, srv->d_jobs, nb * sizeof(BktJob), s));
-    EMP_TRY(ctx_ensure(ctx, srv->d_ctl, sizeof(CoopCtl), s));
-    if (!srv->h_jobs.ensure(nb * sizeof(BktJob) + sizeof(CoopCtl))) return EMP_E_NOMEM;
-    if (!srv->ev[0]) {
-        for (auto &e : srv->ev) EMP_CUDA(cudaEventCreate(&e));
+    if (!nb) {
+        srv->live.swap(joining);
+        return EMP_OK;
     }
-    BktJob *hj = srv->h_jobs.as<BktJob>();
-    CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + nb);
-    for (size_t k = 0; k < nb; ++k) hj[k] = srv->live[k]->bk;
-    std::memset(hc, 0, sizeof(CoopCtl));
-    hc->njobs = (uint32_t)nb;
-    hc->active = (uint32_t)nb;
-    hc->iter_cap = (uint32_t)srv->p.rounds_per_launch;
-    EMP_CUDA(cudaMemcpyAsync(srv->d_jobs.p, hj, nb * sizeof(BktJob), cudaMemcpyHostToDevice, s));
-    EMP_CUDA(cudaMemcpyAsync(srv->d_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
-    EMP_CUDA(cudaEventRecord(srv->ev[0], s));
-    EMP_CUDA(launch_bucket_rounds(srv->d_jobs.as<BktJob>(), srv->d_ctl.as<CoopCtl>(), err_word(srv->live[0]), s));
-    EMP_CUDA(cudaEventRecord(srv->ev[1], s));
-    EMP_CUDA(cudaMemcpyAsync(hj, srv->d_jobs.p, nb * sizeof(BktJob), cudaMemcpyDeviceToHost, s));
-    EMP_CUDA(cudaMemcpyAsync(hc, srv->d_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
+    // ---- the launch's results
     EMP_CUDA(cudaStreamSynchronize(s));
     const bool timed_out = (hc->err & kErrSpin) != 0;
     const float ms = ms_between(srv->ev[0], srv->ev[1]);
@@ -1601,6 +1613,7 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
             still.push_back(j);
         }
     }
+    still.insert(still.end(), joining.begin(), joining.end());
     srv->live.swap(still);
     if (done.empty()) return EMP_OK;
     EMP_CUDA(cudaStreamSynchronize(s));
