@@ -1157,6 +1157,8 @@ emp_status map_records(emp_job *j, cudaStream_t s) {
         map_finish_empty(j, s);
         return EMP_OK;
     }
+    // the map kernels load the FASTQ as aligned 16-byte blocks
+    if (reinterpret_cast<uintptr_t>(j->fq.p) & 15u) return EMP_E_CUDA;
     EMP_TRY(ensure(j, j->seq_start, n_rec * 8));
     EMP_TRY(ensure(j, j->seq_end, n_rec * 8));
     launch_nl_locate(j->fq.as<uint8_t>(), F, j->tile_excl.as<uint64_t>(), j->seq_start.as<uint64_t>(),

@@ -13,13 +13,18 @@
 //   nl_count      newline count of each 16 KB tile (16-byte vector loads)
 //   nl_locate     global line id of every newline -> start/end of each
 //                 record's sequence line
-//   classify      one warp per record: N filter, ACGT check, length
+//   classify      one warp per record, lane j taking bytes 16j..16j+15 of the
+//                 sequence line (aligned 16-byte loads, neighbours shared by
+//                 shuffle): N filter, ACGT check, length
 //   scatter_hq    kept read i -> record index
 //   fingerprint_pack
-//                 one warp per read: lane-chunk Horner hashes of the read and
-//                 of its reverse complement, combined with R^k from shared
-//                 memory; the CTA then writes 128 reads x L columns of 2-bit
-//                 codes as whole 32-byte column segments.
+//                 one warp per read (two per warp-iteration when L <= 256),
+//                 lane j taking bases 16j..16j+15: Horner hashes of its chunk
+//                 for the read and its reverse complement, combined with R^k
+//                 from shared memory; the chunk is also the read-major 2-bit
+//                 word j, and each lane gathers its 16 column words of the
+//                 warp's 16 reads in registers; the CTA writes 128 reads x L
+//                 columns as whole 32-byte column segments.
 #include "kernels.h"
 
 namespace emp {
@@ -92,6 +97,63 @@ __global__ void __launch_bounds__(256) nl_locate_kernel(const uint8_t *__restric
     }
 }
 
+// Bytes [s, s + 16) of the FASTQ (only those below `end` are meaningful),
+// for a group of consecutive lanes whose starts s differ by 16 from lane to
+// lane (lane j: s = a + 16 j): each lane loads the aligned 16 bytes at or
+// before s, takes the following aligned 16 from the next lane (the group's
+// last lane, `last`, loads them), and funnels.  Every lane of the warp must
+// call it.  Loads touch only 16-byte blocks that hold a byte below `end` (the
+// buffer starts 16-byte aligned and holds 16 bytes of slack past the data).
+EMP_DEV void load16(const uint8_t *__restrict__ fq, uint64_t s, uint64_t end, bool last, uint32_t w[4]) {
+    const uint64_t A = s & ~15ull;
+    const uint32_t o = (uint32_t)(s & 15ull);  // the same in every lane
+    uint4 c0 = make_uint4(0, 0, 0, 0), c1;
+    if (A < end) c0 = *reinterpret_cast<const uint4 *>(fq + A);
+    c1.x = __shfl_down_sync(0xffffffffu, c0.x, 1);
+    c1.y = __shfl_down_sync(0xffffffffu, c0.y, 1);
+    c1.z = __shfl_down_sync(0xffffffffu, c0.z, 1);
+    c1.w = __shfl_down_sync(0xffffffffu, c0.w, 1);
+    if (last) {  // the block after the group's last lane's
+        c1 = make_uint4(0, 0, 0, 0);
+        if (o && A + 16 < end) c1 = *reinterpret_cast<const uint4 *>(fq + A + 16);
+    }
+    const uint32_t v[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    const uint32_t q = o >> 2, sh = (o & 3u) * 8u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {  // word q + k of the pair, shifted by sh bits
+        uint32_t lo = v[k], hi = v[k + 1];
+        if (q == 1) { lo = v[k + 1]; hi = v[k + 2]; }
+        if (q == 2) { lo = v[k + 2]; hi = v[k + 3]; }
+        if (q == 3) { lo = v[k + 3]; hi = v[k + 4]; }
+        w[k] = __funnelshift_r(lo, hi, sh);
+    }
+}
+EMP_DEV uint32_t byte_of(const uint32_t w[4], int t) { return (w[t >> 2] >> (8 * (t & 3))) & 0xffu; }
+
+// 0x80 in every byte of t that is zero, 0 elsewhere (no carries between bytes)
+EMP_DEV uint32_t zero_bytes(uint32_t t) { return ~(((t & 0x7f7f7f7fu) + 0x7f7f7f7fu) | t | 0x7f7f7f7fu); }
+
+// N-class and non-ACGT bytes among the first `valid` of w (any of each)
+EMP_DEV void check16(const uint32_t w[4], int valid, bool &has_n, bool &bad) {
+    uint32_t nm = 0, bm = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int vb = valid - 4 * k;
+        const uint32_t m = vb >= 4 ? 0x80808080u : (vb <= 0 ? 0u : ((1u << (8 * vb)) - 1u) & 0x80808080u);
+        const uint32_t x = w[k], f = x | 0x20202020u;  // case folded
+        // markNs == 9 (is_n_class): bits 7-6 = 01 and bit 3 set
+        nm |= zero_bytes((x & 0xc8c8c8c8u) ^ 0x48484848u) & m;
+        const uint32_t ok = zero_bytes(f ^ 0x61616161u) | zero_bytes(f ^ 0x63636363u) |
+                            zero_bytes(f ^ 0x67676767u) | zero_bytes(f ^ 0x74747474u);  // a c g t
+        bm |= ~ok & m;
+    }
+    has_n |= nm != 0;
+    bad |= bm != 0;
+}
+
+// One warp per 32 consecutive records: their sequence-line bounds in one
+// load, then record by record (the next record's first 512 bytes loaded
+// while the current one is checked); hq written for the 32 at once.
 __global__ void __launch_bounds__(256) classify_kernel(const uint8_t *__restrict__ fq,
                                                        const uint64_t *__restrict__ seq_start,
                                                        const uint64_t *__restrict__ seq_end, uint64_t n_rec,
@@ -99,26 +161,50 @@ __global__ void __launch_bounds__(256) classify_kernel(const uint8_t *__restrict
                                                        uint32_t *err) {
     const int lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t groups = (n_rec + 31) / 32;
     uint32_t lmin = 0xffffffffu, lmax = 0, bad_any = 0;
-    for (uint64_t k = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); k < n_rec; k += warps) {
-        const uint64_t a = seq_start[k], b = seq_end[k];
-        const uint64_t len = b > a ? b - a : 0;
-        bool has_n = false, bad = false;
-        for (uint64_t o = a + lane; o < b; o += 32) {
-            const uint8_t c = fq[o];
-            has_n |= is_n_class(c);
-            bad |= !is_acgt(c);
+    for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < groups; g += warps) {
+        const uint64_t k0 = g * 32, kl = k0 + lane;
+        uint64_t ma = 0, mb = 0;
+        if (kl < n_rec) {
+            ma = seq_start[kl];
+            mb = seq_end[kl];
         }
-        has_n = __any_sync(0xffffffffu, has_n);
-        bad = __any_sync(0xffffffffu, bad);
-        const bool keep = !has_n && len > 0;
-        if (lane == 0) hq[k] = keep ? 1u : 0u;
-        if (keep) {
-            const uint32_t l32 = len > 0xffffffffull ? 0xffffffffu : (uint32_t)len;
-            lmin = min(lmin, l32);
-            lmax = max(lmax, l32);
-            bad_any |= bad ? 1u : 0u;
+        const int cnt = (int)(n_rec - k0 < 32 ? n_rec - k0 : 32);
+        uint32_t w[4];
+        {
+            const uint64_t a = __shfl_sync(0xffffffffu, ma, 0), b = __shfl_sync(0xffffffffu, mb, 0);
+            load16(fq, a + 16 * (uint64_t)lane, b, lane == 31, w);
         }
+        bool my_keep = false;
+        for (int r = 0; r < cnt; ++r) {
+            const uint64_t a = __shfl_sync(0xffffffffu, ma, r), b = __shfl_sync(0xffffffffu, mb, r);
+            uint32_t wn[4] = {0, 0, 0, 0};
+            if (r + 1 < cnt) {
+                const uint64_t an = __shfl_sync(0xffffffffu, ma, r + 1), bn = __shfl_sync(0xffffffffu, mb, r + 1);
+                load16(fq, an + 16 * (uint64_t)lane, bn, lane == 31, wn);
+            }
+            const uint64_t len = b > a ? b - a : 0;
+            bool has_n = false, bad = false;
+            for (uint64_t c0 = 0; 16 * c0 < len; c0 += 32) {  // 32 chunks of 16 bytes per pass
+                const uint64_t s = a + 16 * (c0 + lane);
+                if (c0) load16(fq, s, b, lane == 31, w);
+                check16(w, s < b ? (int)(b - s < 16 ? b - s : 16) : 0, has_n, bad);
+            }
+            has_n = __any_sync(0xffffffffu, has_n);
+            bad = __any_sync(0xffffffffu, bad);
+            const bool keep = !has_n && len > 0;
+            if (lane == r) my_keep = keep;
+            if (keep) {
+                const uint32_t l32 = len > 0xffffffffull ? 0xffffffffu : (uint32_t)len;
+                lmin = min(lmin, l32);
+                lmax = max(lmax, l32);
+                bad_any |= bad ? 1u : 0u;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) w[k] = wn[k];
+        }
+        if (kl < n_rec) hq[kl] = my_keep ? 1u : 0u;
     }
     if (lane == 0) {
         if (lmax) {
@@ -136,9 +222,10 @@ __global__ void scatter_hq_kernel(const uint32_t *__restrict__ hq, const uint32_
         if (hq[k]) rec_of[idx[k]] = (uint32_t)k;
 }
 
-// PER: bases per lane at most (L <= 32 PER); READS reads per CTA (8 warps,
-// READS / 8 reads each), their 2-bit codes staged in a READS x 32 PER tile.
-template <int PER, int READS>
+// One warp, 16 reads of the CTA's 128 (rows warp*16 .. warp*16+15).  TWO:
+// L <= 256, so the two half-warps take two reads at once (lanes 16h + j take
+// chunk j of read m + h).  Lane chunk j holds bases 16j .. 16j+15.
+template <bool TWO>
 __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__restrict__ fq,
                                                                const uint64_t *__restrict__ seq_start,
                                                                const uint32_t *__restrict__ rec_of, uint64_t n,
@@ -146,88 +233,107 @@ __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__
                                                                uint64_t *__restrict__ keys,
                                                                uint32_t *__restrict__ cols, uint64_t wpc,
                                                                uint32_t *__restrict__ seq2, int wpr) {
+    constexpr int kReads = 128;
     __shared__ uint32_t s_pow1[kMaxReadLen + 1], s_pow2[kMaxReadLen + 1];
-    constexpr int kFpRow = 32 * PER, kRowsPerWarp = READS / 8, kGroups = READS / 16;
-    __shared__ uint8_t s_codes[READS * kFpRow];
+    __shared__ uint32_t s_colw[8][kMaxReadLen];  // [warp][column]: the warp's 16-read column words
     for (int i = threadIdx.x; i <= kMaxReadLen; i += blockDim.x) {
         s_pow1[i] = tables->pow1[i];
         s_pow2[i] = tables->pow2[i];
     }
     __syncthreads();
-    const uint64_t i0 = (uint64_t)blockIdx.x * READS;
+    const uint64_t i0 = (uint64_t)blockIdx.x * kReads;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = (L + 31) >> 5;  // bases per lane, <= PER
-    const int a = min(lane * per, L), b = min(a + per, L);
-    for (int m = 0; m < kRowsPerWarp; ++m) {
-        const int row = warp * kRowsPerWarp + m;
-        const uint64_t i = i0 + row;
-        if (i >= n) break;
-        const uint8_t *s = fq + seq_start[rec_of[i]];
-        uint32_t cod[PER];
-        uint32_t hf1 = 0, hf2 = 0, hr1 = 0, hr2 = 0;
+    const int half = TWO ? lane >> 4 : 0;
+    const int j = TWO ? lane & 15 : lane;  // the lane's chunk
+    const int nch = (L + 15) >> 4;
+    const bool act = j < nch;
+    const int vb = act ? min(16, L - 16 * j) : 0;  // bases of the chunk
+    const int q = min(16 * (j + 1), L);
+    const uint32_t pf1 = s_pow1[act ? L - q : 0], pf2 = s_pow2[act ? L - q : 0];
+    const uint32_t pr1 = s_pow1[act ? 16 * j : 0], pr2 = s_pow2[act ? 16 * j : 0];
+    // sequence starts of the warp's 16 reads (lane m holds read m's)
+    const uint64_t r0 = i0 + (uint64_t)warp * 16;
+    uint64_t my_start = 0;
+    if (lane < 16 && r0 + lane < n) my_start = seq_start[rec_of[r0 + lane]];
+    uint32_t colw[16];
 #pragma unroll
-        for (int jj = 0; jj < PER; ++jj) {
-            const int j = a + jj;
-            cod[jj] = 0;
-            if (j < b) {
-                const uint32_t v = base_code(s[j]);
-                cod[jj] = v;
-                s_codes[row * kFpRow + j] = (uint8_t)v;
+    for (int t = 0; t < 16; ++t) colw[t] = 0;
+    constexpr int kStep = TWO ? 2 : 1;
+    const bool last = TWO ? j == 15 : lane == 31;
+    uint32_t w[4];  // the chunk of read m; the next read's is loaded while m is hashed
+    {
+        const uint64_t a = __shfl_sync(0xffffffffu, my_start, half);
+        load16(fq, a + 16 * (uint64_t)j, r0 + half < n ? a + (uint64_t)L : 0, last, w);
+    }
+    for (int m0 = 0; m0 < 16; m0 += kStep) {
+        const int m = m0 + half;
+        const uint64_t i = r0 + m;
+        const bool live = i < n;
+        if (!__any_sync(0xffffffffu, live)) break;
+        uint32_t wn[4] = {0, 0, 0, 0};
+        if (m0 + kStep < 16) {
+            const int mn = m + kStep;
+            const uint64_t an = __shfl_sync(0xffffffffu, my_start, mn);
+            load16(fq, an + 16 * (uint64_t)j, r0 + mn < n ? an + (uint64_t)L : 0, last, wn);
+        }
+        uint32_t hf1 = 0, hf2 = 0, hr1 = 0, hr2 = 0, word = 0;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            if (live && t < vb) {
+                const uint32_t v = base_code((uint8_t)byte_of(w, t));
+                word |= v << (2 * t);
                 hf1 = horner1(hf1, v + 1);
                 hf2 = horner2(hf2, v + 1);
             }
         }
 #pragma unroll
-        for (int jj = PER - 1; jj >= 0; --jj) {
-            if (a + jj < b) {
-                const uint32_t e = (cod[jj] ^ 2u) + 1u;  // complement
+        for (int t = 15; t >= 0; --t) {
+            if (live && t < vb) {
+                const uint32_t e = (((word >> (2 * t)) & 3u) ^ 2u) + 1u;  // complement
                 hr1 = horner1(hr1, e);
                 hr2 = horner2(hr2, e);
             }
         }
-        uint64_t f1 = 0, f2 = 0, r1 = 0, r2 = 0;
-        if (a < b) {
-            f1 = mod1((uint64_t)hf1 * s_pow1[L - b]);
-            f2 = mod2((uint64_t)hf2 * s_pow2[L - b]);
-            r1 = mod1((uint64_t)hr1 * s_pow1[a]);
-            r2 = mod2((uint64_t)hr2 * s_pow2[a]);
+        uint64_t f1 = 0, f2 = 0, g1 = 0, g2 = 0;
+        if (live && act) {
+            f1 = mod1((uint64_t)hf1 * pf1);
+            f2 = mod2((uint64_t)hf2 * pf2);
+            g1 = mod1((uint64_t)hr1 * pr1);
+            g2 = mod2((uint64_t)hr2 * pr2);
         }
 #pragma unroll
-        for (int o = 16; o; o >>= 1) {
+        for (int o = TWO ? 8 : 16; o; o >>= 1) {
             f1 += __shfl_xor_sync(0xffffffffu, f1, o);
             f2 += __shfl_xor_sync(0xffffffffu, f2, o);
-            r1 += __shfl_xor_sync(0xffffffffu, r1, o);
-            r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+            g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+            g2 += __shfl_xor_sync(0xffffffffu, g2, o);
         }
-        if (lane == 0) {
+        if (live && j == 0) {
             ulonglong2 kv;
             kv.x = ((uint64_t)mod1(f1) << 32) | mod2(f2);
-            kv.y = ((uint64_t)mod1(r1) << 32) | mod2(r2);
+            kv.y = ((uint64_t)mod1(g1) << 32) | mod2(g2);
             *reinterpret_cast<ulonglong2 *>(keys + 2 * i) = kv;
         }
+        if (live && act && seq2) seq2[i * wpr + j] = word;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) colw[t] |= ((word >> (2 * t)) & 3u) << (2 * m);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) w[k] = wn[k];
+    }
+    if (TWO) {  // the half-warps hold the even and odd reads' bits
+#pragma unroll
+        for (int t = 0; t < 16; ++t) colw[t] |= __shfl_xor_sync(0xffffffffu, colw[t], 16);
+    }
+    if (act && half == 0) {
+#pragma unroll
+        for (int t = 0; t < 16; ++t)
+            if (16 * j + t < L) s_colw[warp][16 * j + t] = colw[t];
     }
     __syncthreads();
     const uint64_t w0 = i0 >> 4;
-    for (int p = threadIdx.x; p < L * kGroups; p += blockDim.x) {
-        const int col = p / kGroups, q = p % kGroups;
-        if (w0 + q >= wpc) continue;
-        uint32_t word = 0;
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const int row = q * 16 + m;
-            if (i0 + row < n) word |= (uint32_t)s_codes[row * kFpRow + col] << (2 * m);
-        }
-        cols[(uint64_t)col * wpc + w0 + q] = word;
-    }
-    if (!seq2) return;
-    // read-major copy: word w of read i holds positions 16w .. 16w+15
-    for (int p = threadIdx.x; p < READS * wpr; p += blockDim.x) {
-        const int row = p / wpr, w = p - row * wpr;
-        if (i0 + row >= n) break;
-        uint32_t word = 0;
-        for (int m = 0; m < 16 && 16 * w + m < L; ++m)
-            word |= (uint32_t)s_codes[row * kFpRow + 16 * w + m] << (2 * m);
-        seq2[(i0 + row) * wpr + w] = word;
+    for (int p = threadIdx.x; p < L * 8; p += blockDim.x) {
+        const int col = p >> 3, qq = p & 7;
+        if (w0 + qq < wpc) cols[(uint64_t)col * wpc + w0 + qq] = s_colw[qq][col];
     }
 }
 
@@ -255,8 +361,8 @@ void launch_classify(const uint8_t *fq, const uint64_t *seq_start, const uint64_
                      uint32_t *hq, uint32_t *len_minmax, uint32_t *err, cudaStream_t s) {
     if (!n_rec) return;
     count_launch();
-    classify_kernel<<<grid_for(n_rec, 8, 148 * 16), 256, 0, s>>>(fq, seq_start, seq_end, n_rec, hq, len_minmax,
-                                                                   err);
+    classify_kernel<<<grid_for((n_rec + 31) / 32, 8, 148 * 16), 256, 0, s>>>(fq, seq_start, seq_end, n_rec, hq,
+                                                                               len_minmax, err);
 }
 
 void launch_scatter_hq(const uint32_t *hq, const uint32_t *idx, uint64_t n_rec, uint32_t *rec_of, cudaStream_t s) {
@@ -270,14 +376,14 @@ void launch_fingerprint_pack(const uint8_t *fq, const uint64_t *seq_start, const
                              uint32_t *seq2, int wpr, cudaStream_t s) {
     if (!n) return;
     count_launch();
-    if (L <= 256) {
-        fingerprint_pack_kernel<8, 128><<<(unsigned)((n + 127) / 128), 256, 0, s>>>(fq, seq_start, rec_of, n, L, tables,
-                                                                                 keys, cols, wpc, seq2, wpr);
-    } else {
-        static_assert(kMaxReadLen <= 512, "16 bases per lane");
-        fingerprint_pack_kernel<16, 64><<<(unsigned)((n + 63) / 64), 256, 0, s>>>(fq, seq_start, rec_of, n, L, tables,
-                                                                               keys, cols, wpc, seq2, wpr);
-    }
+    static_assert(kMaxReadLen <= 512, "32 lanes x 16 bases");
+    const unsigned blocks = (unsigned)((n + 127) / 128);
+    if (L <= 256)
+        fingerprint_pack_kernel<true><<<blocks, 256, 0, s>>>(fq, seq_start, rec_of, n, L, tables, keys, cols, wpc, seq2,
+                                                              wpr);
+    else
+        fingerprint_pack_kernel<false><<<blocks, 256, 0, s>>>(fq, seq_start, rec_of, n, L, tables, keys, cols, wpc,
+                                                               seq2, wpr);
 }
 
 }  // namespace emp
