@@ -400,7 +400,7 @@ EMP_COLD uint32_t gather_general(const BktJob &J, const BktEntry *lst, const uin
     return total;
 }
 
-EMP_DEV uint32_t gather(const BktJob &J, const BktEntry *lst, const uint32_t *offs, const uint64_t *tbase,
+EMP_COLD uint32_t gather(const BktJob &J, const BktEntry *lst, const uint32_t *offs, const uint64_t *tbase,
                         uint32_t K, uint32_t nb, uint32_t b, BShared &sh, uint8_t *smem, Stage &v, uint32_t &S,
                         uint64_t &G) {
     const uint32_t stride = 2 * nb + 1, Q = 2 * K;
@@ -909,7 +909,7 @@ EMP_DEV uint32_t close_tile(uint32_t *hist, uint32_t nbin, uint32_t tile, uint32
 
 // write_next for a bucket staged in shared memory: the same steps on the
 // shared arrays, the tile permuted in shared memory and written in order.
-EMP_DEV void write_next_smem(uint32_t total, const StepArgs &a, uint32_t nb, uint32_t tile, BktEntry *lout,
+EMP_COLD void write_next_smem(uint32_t total, const StepArgs a, uint32_t nb, uint32_t tile, BktEntry *lout,
                              uint32_t *offs, uint64_t *tbase, BktRound &nx, BShared &sh, uint8_t *smem) {
     uint64_t *key = reinterpret_cast<uint64_t *>(smem + kOffKey);
     uint32_t *val = reinterpret_cast<uint32_t *>(smem + kOffVal);
