@@ -263,7 +263,7 @@ struct BktEntry {
     uint32_t word;  // cached 16 bases (one seq2 word) of the entry's read
 };
 constexpr uint32_t kBktTile = 4096;               // entries per prologue tile
-constexpr uint64_t kBktMean = 6300;               // entries per bucket aimed at (mean)
+constexpr uint64_t kBktMean = 6700;               // entries per bucket aimed at (mean; 5.7 sigma below the staging limit)
 constexpr uint32_t kBktMaxBuckets = 4096;
 constexpr uint64_t kBktMaxEntries = 16ull << 20;  // larger lists use the other drivers
 __host__ __device__ inline uint64_t bkt_tiles(uint64_t n) { return (n + kBktTile - 1) / kBktTile; }
