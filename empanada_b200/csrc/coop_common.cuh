@@ -28,11 +28,14 @@ EMP_DEV uint64_t globaltimer() {
 
 // Grid barrier (all CTAs co-resident: cooperative launch).  Bounded wait: on
 // timeout the error bit is raised and false returned; the kernel then exits.
-EMP_DEV bool grid_barrier_raw(CoopCtl *ctl, uint32_t *s_flag) {
+// *s_gen (shared, zero at kernel start, like the control block's counters)
+// holds the barriers this CTA has passed, so arriving costs one atomic and
+// waiting one poll loop; another CTA's timeout is seen while polling.
+EMP_DEV bool grid_barrier_raw(CoopCtl *ctl, uint32_t *s_flag, uint32_t *s_gen) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile uint32_t *gen = &ctl->bar_gen;
-        const uint32_t g = *gen;
+        const uint32_t g = *s_gen;
         __threadfence();
         const uint32_t arrived = atomicAdd(&ctl->bar_count, 1u);
         uint32_t ok = 1;
@@ -44,7 +47,8 @@ EMP_DEV bool grid_barrier_raw(CoopCtl *ctl, uint32_t *s_flag) {
             const uint64_t t0 = globaltimer();
             uint32_t polls = 0;
             while (*gen == g) {
-                if ((++polls & 255) == 0 && globaltimer() - t0 > kBarrierTimeoutNs) {
+                if ((++polls & 255) == 0 &&
+                    (globaltimer() - t0 > kBarrierTimeoutNs || (*(volatile uint32_t *)&ctl->err & kErrSpin))) {
                     atomicOr(&ctl->err, kErrSpin);
                     ok = 0;
                     break;
@@ -53,7 +57,8 @@ EMP_DEV bool grid_barrier_raw(CoopCtl *ctl, uint32_t *s_flag) {
             }
         }
         __threadfence();
-        *s_flag = ok && !(*(volatile uint32_t *)&ctl->err & kErrSpin);
+        *s_gen = g + 1;
+        *s_flag = ok;
     }
     __syncthreads();
     return *s_flag != 0;
@@ -67,8 +72,8 @@ EMP_DEV void probe(const CoopCtl *ctl, uint32_t iter, int p) {
 }
 
 // barrier + optional phase timestamp (ctl->trace) for profiling
-EMP_DEV bool grid_barrier(CoopCtl *ctl, uint32_t *s_flag, uint32_t iter, int phase) {
-    const bool ok = grid_barrier_raw(ctl, s_flag);
+EMP_DEV bool grid_barrier(CoopCtl *ctl, uint32_t *s_flag, uint32_t *s_gen, uint32_t iter, int phase) {
+    const bool ok = grid_barrier_raw(ctl, s_flag, s_gen);
     if (blockIdx.x == 0 && threadIdx.x == 0 && ctl->trace && iter < ctl->trace_cap)
         ctl->trace[(uint64_t)iter * kCoopTracePhases + phase] = globaltimer();
     return ok;

@@ -99,6 +99,7 @@ struct BShared {
     uint64_t scan64[32];
     uint64_t base;
     uint32_t tile, flag, sfx, cnt;
+    uint32_t gen;  // grid barriers passed
     const CoopCtl *pctl;  // profiling stamps from inside the steps of a tile
     uint32_t piter;
     HashTables tab;       // powers and inverses (every job of a launch shares them)
@@ -1188,13 +1189,18 @@ struct RoundShape {
 EMP_DEV RoundShape round_shape(const BktJob &J, uint32_t iter) {
     RoundShape z;
     z.r = J.r0 + (int)iter;
-    z.active = z.r < J.rounds && __ldcg(&J.meta[z.r].s) > 0;
     z.K = z.nb = z.nb_next = 0;
+    z.active = false;
+    if (z.r >= J.rounds) return z;
+    // the four counts in one round trip (meta has rounds + 1 entries)
+    const uint64_t s = __ldcg(&J.meta[z.r].s), n = __ldcg(&J.meta[z.r].n);
+    const uint64_t n1 = iter >= 1 ? __ldcg(&J.meta[z.r - 1].n) : J.n_in;
+    const uint64_t n2 = iter >= 2 ? __ldcg(&J.meta[z.r - 2].n) : J.n_in;
+    z.active = s > 0;
     if (!z.active) return z;
-    z.nb = iter ? bkt_count(__ldcg(&J.meta[z.r - 1].n), J.wave) : bkt_count(J.n_in, J.wave);
-    z.K = iter == 0 ? (uint32_t)bkt_tiles(J.n_in)
-                    : (iter == 1 ? bkt_count(J.n_in, J.wave) : bkt_count(__ldcg(&J.meta[z.r - 2].n), J.wave));
-    z.nb_next = bkt_count(__ldcg(&J.meta[z.r].n), J.wave);
+    z.nb = bkt_count(n1, J.wave);
+    z.K = iter == 0 ? (uint32_t)bkt_tiles(J.n_in) : bkt_count(n2, J.wave);
+    z.nb_next = bkt_count(n, J.wave);
     return z;
 }
 
@@ -1374,13 +1380,14 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
     const int J = (int)ctl->njobs;
     for (uint32_t i = threadIdx.x; i < sizeof(HashTables) / 4; i += kT)
         reinterpret_cast<uint32_t *>(&sh.tab)[i] = reinterpret_cast<const uint32_t *>(jobs[0].tables)[i];
+    if (threadIdx.x == 0) sh.gen = 0;
     __syncthreads();
     // ---- prologue: the input lists of the jobs this launch starts -> their round r0 lists
     uint32_t total = build_prefix(sh, J, [&](int j) -> uint32_t {
         return jobs[j].iter0 == 0 ? (uint32_t)bkt_tiles(jobs[j].n_in) : 0u;
     });
     tile_loop(sh, &ctl->ticket[0], J, total, [&](int j, uint32_t k) { prologue_tile(jobs[j], k, sh, smem); });
-    if (!grid_barrier(ctl, &sh.flag, 0, 7)) return;
+    if (!grid_barrier(ctl, &sh.flag, &sh.gen, 0, 7)) return;
     // ---- rounds: iteration iter0 + it of every job (round r0 + iter0 + it)
     // that still runs, for at most iter_cap iterations; a job resumes in a
     // later launch from the lists and counts the last iteration left behind
@@ -1410,7 +1417,7 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
             round_tile(jobs[j], b, g, z, sh, ctl, smem);
         });
         probe(ctl, it, 9);
-        if (!grid_barrier(ctl, &sh.flag, it, 0)) return;
+        if (!grid_barrier(ctl, &sh.flag, &sh.gen, it, 0)) return;
         probe(ctl, it, 10);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = it;

@@ -49,6 +49,7 @@ struct CoopShared {
     uint64_t cnt64[kC * kBlkWarps + 1];
     uint64_t base;
     uint32_t tile, flag, sfx, last;
+    uint32_t gen;  // grid barriers passed
 };
 
 
@@ -395,6 +396,8 @@ __global__ void __launch_bounds__(kT, 1) coop_rounds_kernel(CoopJob *jobs, CoopC
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ CoopShared sh;
     const int J = (int)ctl->njobs;
+    if (threadIdx.x == 0) sh.gen = 0;
+    __syncthreads();
     for (uint32_t iter = 0;; ++iter) {
         if (vld(ctl->active) == 0) break;
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ticket[13] = 0;  // join ticket of the last iteration
@@ -410,7 +413,7 @@ __global__ void __launch_bounds__(kT, 1) coop_rounds_kernel(CoopJob *jobs, CoopC
         tile_loop(sh, &ctl->ticket[0], J, total,
                   [&](int j, uint32_t lt) { update_tile(jobs[j], lt, iter, sh, ctl, err, smem); });
         probe(ctl, iter, 6);
-        if (!grid_barrier(ctl, &sh.flag, iter, 0)) return;
+        if (!grid_barrier(ctl, &sh.flag, &sh.gen, iter, 0)) return;
         probe(ctl, iter, 7);
         // ---- 2: candidates
         total = build_prefix(sh, J, [&](int j) -> uint32_t {
@@ -422,7 +425,7 @@ __global__ void __launch_bounds__(kT, 1) coop_rounds_kernel(CoopJob *jobs, CoopC
         tile_loop(sh, &ctl->ticket[1], J, total,
                   [&](int j, uint32_t lt) { cand_tile(jobs[j], lt, iter, sh, ctl, err, smem); });
         probe(ctl, iter, 9);
-        if (!grid_barrier(ctl, &sh.flag, iter, 1)) return;
+        if (!grid_barrier(ctl, &sh.flag, &sh.gen, iter, 1)) return;
         probe(ctl, iter, 14);
         // ---- 3a: single-CTA sorts and the MSD scatter pass
         total = build_prefix(sh, J, [&](int j) -> uint32_t {
@@ -445,7 +448,7 @@ __global__ void __launch_bounds__(kT, 1) coop_rounds_kernel(CoopJob *jobs, CoopC
                           (iter * 9u + 8u) & 0xfffffu, err, smem);
         });
         probe(ctl, iter, 15);
-        if (!grid_barrier(ctl, &sh.flag, iter, 2)) return;
+        if (!grid_barrier(ctl, &sh.flag, &sh.gen, iter, 2)) return;
         probe(ctl, iter, 16);
         // ---- 3b: per-bucket sorts of the MSD jobs, first LSD pass
         total = build_prefix(sh, J, [&](int j) -> uint32_t {
@@ -480,10 +483,10 @@ __global__ void __launch_bounds__(kT, 1) coop_rounds_kernel(CoopJob *jobs, CoopC
                               vld(x.c), lt, 8 * p, sh.bucket, x.st_sort, (iter * 9u + (uint32_t)p) & 0xfffffu, err,
                               smem);
             });
-            if (p < kSortPasses - 1 && !grid_barrier(ctl, &sh.flag, iter, 6)) return;
+            if (p < kSortPasses - 1 && !grid_barrier(ctl, &sh.flag, &sh.gen, iter, 6)) return;
         }
         probe(ctl, iter, 17);
-        if (!grid_barrier(ctl, &sh.flag, iter, 3)) return;
+        if (!grid_barrier(ctl, &sh.flag, &sh.gen, iter, 3)) return;
         probe(ctl, iter, 18);
         // ---- 4: join, clears, round end
         if (blockIdx.x == 0 && threadIdx.x < 13) ctl->ticket[threadIdx.x] = 0;  // phases 1-3 are over
@@ -526,7 +529,7 @@ __global__ void __launch_bounds__(kT, 1) coop_rounds_kernel(CoopJob *jobs, CoopC
             if (threadIdx.x == 0 && sh.pref[j + 1] == sh.pref[j] && !vld(jobs[j].done)) round_end(jobs[j], ctl, iter);
         }
         probe(ctl, iter, 24);
-        if (!grid_barrier(ctl, &sh.flag, iter, 4)) return;
+        if (!grid_barrier(ctl, &sh.flag, &sh.gen, iter, 4)) return;
         probe(ctl, iter, 25);
     }
 }
