@@ -235,6 +235,19 @@ class Job:
         check(self._lib.emp_job_output_copy(self.handle, arr.ctypes.data, arr.nbytes), "output_copy")
         return int(n.value)
 
+    def edges(self) -> list[tuple[int, np.ndarray, np.ndarray]]:
+        """The last run's records through emp_job_edges: (ovlp_len, from, to) each."""
+        out = []
+
+        def sink(_user, ovlp, n, frm, to):
+            out.append((int(ovlp), np.ctypeslib.as_array(frm, (n,)).copy() if n else np.zeros(0, np.uint32),
+                        np.ctypeslib.as_array(to, (n,)).copy() if n else np.zeros(0, np.uint32)))
+            return 0
+
+        cb = _native.EDGE_SINK(sink)
+        check(self._lib.emp_job_edges(self.handle, cb, None), "emp_job_edges")
+        return out
+
     def stats(self) -> dict:
         st = _native.Stats()
         check(self._lib.emp_job_stats(self.handle, ctypes.byref(st)), "stats")

@@ -38,6 +38,11 @@ class Params(ctypes.Structure):
     ]
 
 
+# int (*emp_edge_sink)(void *user, int32_t ovlp_len, uint64_t n, const uint32_t *from, const uint32_t *to)
+EDGE_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint64,
+                             ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32))
+
+
 class ServerParams(ctypes.Structure):
     _fields_ = [
         ("rounds_per_launch", ctypes.c_int32),
@@ -128,6 +133,7 @@ SIGNATURES = {
     "emp_job_output_size": (ctypes.c_int, [_vp, _u64p]),
     "emp_job_output_copy": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64]),
     "emp_job_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats)]),
+    "emp_job_edges": (ctypes.c_int, [_vp, EDGE_SINK, _vp]),
     "emp_job_fingerprints": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, _u64p]),
     "emp_run_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Params), ctypes.c_int,
                                     ctypes.POINTER(Stats)]),

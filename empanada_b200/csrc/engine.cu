@@ -2168,6 +2168,45 @@ emp_status emp_job_output_copy(emp_job *job, void *dst, uint64_t cap) {
     return EMP_OK;
 }
 
+emp_status emp_job_edges(emp_job *job, emp_edge_sink cb, void *user) {
+    if (!job || !cb) return EMP_E_INVAL;
+    if (!job->have_result) return EMP_E_STATE;
+    const uint64_t total = job->out.size() + job->dout_bytes;
+    std::vector<uint8_t> buf;
+    const uint8_t *p = job->out.data();
+    if (job->dout_bytes) {  // one host copy of the whole output
+        try {
+            buf.resize(total);
+        } catch (...) {
+            return EMP_E_NOMEM;
+        }
+        EMP_TRY(emp_job_output_copy(job, buf.data(), total));
+        p = buf.data();
+    }
+    std::vector<uint32_t> from, to;  // aligned copies of one record's arrays
+    for (uint64_t o = 0; o + 12 <= total;) {
+        uint64_t n;
+        int32_t ovlp;
+        std::memcpy(&n, p + o, 8);
+        std::memcpy(&ovlp, p + o + 8, 4);
+        o += 12;
+        if (n > (total - o) / 8) return EMP_E_STATE;  // a malformed record cannot come from a run
+        try {
+            from.resize(n);
+            to.resize(n);
+        } catch (...) {
+            return EMP_E_NOMEM;
+        }
+        if (n) {
+            std::memcpy(from.data(), p + o, 4 * n);
+            std::memcpy(to.data(), p + o + 4 * n, 4 * n);
+        }
+        o += 8 * n;
+        if (cb(user, ovlp, n, from.data(), to.data())) break;
+    }
+    return EMP_OK;
+}
+
 emp_status emp_job_stats(emp_job *job, emp_stats *st) {
     if (!job || !st) return EMP_E_INVAL;
     if (!job->have_result) return EMP_E_STATE;

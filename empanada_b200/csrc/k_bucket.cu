@@ -807,6 +807,30 @@ EMP_DEV uint64_t sort_fine(const Cands &w, uint32_t c, uint32_t b, uint32_t nb, 
     return join_count(w, c, sh);
 }
 
+// The same for a few matched entries (c <= kSmallRank): each one's rank is
+// the number of entries before it, all pairs compared in shared memory.
+constexpr uint32_t kSmallRank = 96;
+EMP_DEV uint64_t rank_small(const Cands &w, uint32_t c, BShared &sh) {
+    if (threadIdx.x < c) {
+        const uint32_t val = w.cv[threadIdx.x];
+        w.sk[threadIdx.x] = sort_key(w.ck[threadIdx.x], val);
+        w.tb[threadIdx.x] = tie_of(val);
+    }
+    __syncthreads();
+    if (threadIdx.x < c) {
+        const uint32_t x = threadIdx.x;
+        const uint64_t skx = w.sk[x];
+        const uint32_t tbx = w.tb[x];
+        uint32_t r = 0;
+        for (uint32_t y = 0; y < c; ++y) r += before(w.sk[y], w.tb[y], skx, tbx);
+        w.skey[r] = w.ck[x];
+        w.sval[r] = w.cv[x];
+        w.sidx[r] = w.cx[x];
+    }
+    __syncthreads();
+    return join_count(w, c, sh);
+}
+
 EMP_COLD uint64_t sort_and_count(const Cands &w, uint32_t c, BShared &sh) {
     for (uint32_t x = threadIdx.x; x < c; x += kT) {
         const uint32_t val = ldv(w.cv + x);
@@ -1238,7 +1262,7 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
         }
         probe(ctl, iter, 5);
         if (small) {
-            if (c) E = sort_fine(cands_smem(smem), c, b, nb, smem, sh);
+            if (c) E = c <= kSmallRank ? rank_small(cands_smem(smem), c, sh) : sort_fine(cands_smem(smem), c, b, nb, smem, sh);
         } else {
             E = big_count(J, v, total, in_smem, G, K, nb, b, offs, sh, c);
         }

@@ -193,6 +193,12 @@ emp_status emp_server_get_stats(emp_server *srv, emp_server_stats *st);
 emp_status emp_job_output_size(emp_job *job, uint64_t *bytes);
 emp_status emp_job_output_copy(emp_job *job, void *dst, uint64_t cap);
 emp_status emp_job_stats(emp_job *job, emp_stats *st);
+/* The last run's records in output.bin order, one call per record:
+ * overlap length, edge count n, and the n (from, to) read-end ids (arrays
+ * valid during the call).  A nonzero return stops the walk.  The records
+ * write_edges_binary would write (overlap.cu:148-161), without the file. */
+typedef int (*emp_edge_sink)(void *user, int32_t ovlp_len, uint64_t n, const uint32_t *from, const uint32_t *to);
+emp_status emp_job_edges(emp_job *job, emp_edge_sink cb, void *user);
 
 /* Full-length fingerprints of every read-end of the last run, indexed by
  * read-end id (generate_fingerprint_read_pairs, fingerprint.cu:75-115).

@@ -177,3 +177,20 @@ def test_fingerprints_match_oracle(engine):
         want, n, L = bind.fingerprints(data)
         assert got.size == 2 * n
         assert (got == want).all(), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["tiny", "split_r128k", "out_of_core_r4k", "empty_input", "o_ge_L"])
+def test_edge_sink_walks_output_records(engine, name):
+    """emp_job_edges hands out exactly the records of output.bin, in order."""
+    case = BY_NAME[name]
+    a = list(case.args)
+    o = dict(zip(a[::2], a[1::2]))
+    with engine.job(min_ovlp=int(o.get("-o", 31)), reduce_mem=o.get("-r", "1g")) as job:
+        job.feed(case.fastq())
+        job.run()
+        recs = job.edges()
+        want = empanada_b200.decode_output(job.output())
+    assert len(recs) == len(want)
+    for (ov, f, t), (ov2, f2, t2) in zip(recs, want):
+        assert ov == ov2 and (f == f2).all() and (t == t2).all()
