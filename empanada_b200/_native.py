@@ -48,6 +48,7 @@ class ServerParams(ctypes.Structure):
         ("rounds_per_launch", ctypes.c_int32),
         ("max_jobs", ctypes.c_int32),
         ("hbm_budget_bytes", ctypes.c_uint64),
+        ("rounds_per_launch_idle", ctypes.c_int32),
     ]
 
 

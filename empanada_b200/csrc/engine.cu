@@ -1544,7 +1544,9 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         std::memset(hc, 0, sizeof(CoopCtl));
         hc->njobs = (uint32_t)nb;
         hc->active = (uint32_t)nb;
-        hc->iter_cap = (uint32_t)srv->p.rounds_per_launch;
+        // short launches while jobs wait to join, long ones when none does
+        hc->iter_cap = (uint32_t)(srv->queue.empty() && adm.empty() ? srv->p.rounds_per_launch_idle
+                                                                     : srv->p.rounds_per_launch);
         EMP_CUDA(cudaMemcpyAsync(srv->d_jobs.p, hj, nb * sizeof(BktJob), cudaMemcpyHostToDevice, s));
         EMP_CUDA(cudaMemcpyAsync(srv->d_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
         EMP_CUDA(cudaEventRecord(srv->ev[0], s));
@@ -2060,6 +2062,7 @@ emp_status emp_server_params_default(emp_server_params *p) {
     p->rounds_per_launch = 16;
     p->max_jobs = 256;
     p->hbm_budget_bytes = 0;
+    p->rounds_per_launch_idle = 256;
     return EMP_OK;
 }
 
@@ -2069,7 +2072,8 @@ emp_status emp_server_create(emp_ctx *ctx, const emp_server_params *p, emp_serve
     emp_server_params q;
     if (p) q = *p;
     else emp_server_params_default(&q);
-    if (q.rounds_per_launch < 1 || q.max_jobs < 1 || q.max_jobs > kCoopMaxJobs) return EMP_E_INVAL;
+    if (q.rounds_per_launch < 1 || q.rounds_per_launch_idle < 1 || q.max_jobs < 1 || q.max_jobs > kCoopMaxJobs)
+        return EMP_E_INVAL;
     emp_server *srv = new (std::nothrow) emp_server();
     if (!srv) return EMP_E_NOMEM;
     srv->ctx = ctx;

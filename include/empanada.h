@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define EMP_ABI_VERSION 2
+#define EMP_ABI_VERSION 3
 
 typedef int emp_status;
 #define EMP_OK 0
@@ -165,6 +165,7 @@ typedef struct emp_server_params {
     int32_t rounds_per_launch; /* bucket-kernel rounds per launch (default 16) */
     int32_t max_jobs;          /* jobs in the batch at most, <= 1024 (default 256) */
     uint64_t hbm_budget_bytes; /* admission budget (0: the context's, or none) */
+    int32_t rounds_per_launch_idle; /* the same while no job waits to join (default 256) */
 } emp_server_params;
 emp_status emp_server_params_default(emp_server_params *p);
 emp_status emp_server_create(emp_ctx *ctx, const emp_server_params *p, emp_server **out);

@@ -40,7 +40,8 @@ def test_served_golden_cases_staggered(engine, rounds_per_launch):
     every output is the reference's."""
     jobs = {n: _job(engine, n) for n in NAMES}
     order = NAMES[::2] + NAMES[1::2]
-    with empanada_b200.Server(engine, rounds_per_launch=rounds_per_launch, max_jobs=8) as srv:
+    with empanada_b200.Server(engine, rounds_per_launch=rounds_per_launch, rounds_per_launch_idle=rounds_per_launch,
+                              max_jobs=8) as srv:
         done = []
         for k in range(0, len(order), 3):
             for n in order[k:k + 3]:
@@ -52,6 +53,20 @@ def test_served_golden_cases_staggered(engine, rounds_per_launch):
         assert j.status() == 0, n
         assert hashlib.sha256(j.output()).hexdigest() == GOLDEN[n]["sha256"], n
         j.close()
+
+
+@pytest.mark.gpu
+def test_served_idle_launches_run_longer(engine):
+    """With no job waiting, a launch runs up to rounds_per_launch_idle rounds:
+    a lone job needs fewer launches, and its bytes do not change."""
+    j = _job(engine, "sub_errors")
+    with empanada_b200.Server(engine, rounds_per_launch=2, rounds_per_launch_idle=1000) as srv:
+        srv.submit(j)
+        _drain(srv)
+        st = srv.stats()
+    assert st["launches"] <= 2
+    assert hashlib.sha256(j.output()).hexdigest() == GOLDEN["sub_errors"]["sha256"]
+    j.close()
 
 
 @pytest.mark.gpu
