@@ -152,14 +152,17 @@ EMP_DEV void check16(const uint32_t w[4], int valid, bool &has_n, bool &bad) {
 }
 
 // One warp per 32 consecutive records: their sequence-line bounds in one
-// load, then record by record (the next record's first 512 bytes loaded
-// while the current one is checked); hq written for the 32 at once.
+// load, then two records at a time, one per half-warp (lanes 16h + j take
+// bytes 16j .. 16j+15 of record 2p + h, 256 bytes per pass), the next pair's
+// first pass loaded while the current pair is checked; hq written for the 32
+// at once.
 __global__ void __launch_bounds__(256) classify_kernel(const uint8_t *__restrict__ fq,
                                                        const uint64_t *__restrict__ seq_start,
                                                        const uint64_t *__restrict__ seq_end, uint64_t n_rec,
                                                        uint32_t *__restrict__ hq, uint32_t *len_minmax,
                                                        uint32_t *err) {
-    const int lane = threadIdx.x & 31;
+    const uint32_t full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, h = lane >> 4, j = lane & 15;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     const uint64_t groups = (n_rec + 31) / 32;
     uint32_t lmin = 0xffffffffu, lmax = 0, bad_any = 0;
@@ -173,39 +176,51 @@ __global__ void __launch_bounds__(256) classify_kernel(const uint8_t *__restrict
         const int cnt = (int)(n_rec - k0 < 32 ? n_rec - k0 : 32);
         uint32_t w[4];
         {
-            const uint64_t a = __shfl_sync(0xffffffffu, ma, 0), b = __shfl_sync(0xffffffffu, mb, 0);
-            load16(fq, a + 16 * (uint64_t)lane, b, lane == 31, w);
+            const uint64_t a = __shfl_sync(full, ma, h), b = __shfl_sync(full, mb, h);
+            load16(fq, a + 16 * (uint64_t)j, h < cnt ? b : 0, j == 15, w);
         }
         bool my_keep = false;
-        for (int r = 0; r < cnt; ++r) {
-            const uint64_t a = __shfl_sync(0xffffffffu, ma, r), b = __shfl_sync(0xffffffffu, mb, r);
+        for (int p = 0; 2 * p < cnt; ++p) {
+            const int r = 2 * p + h;  // this half's record
+            const bool live = r < cnt;
+            const uint64_t a = __shfl_sync(full, ma, r), br = __shfl_sync(full, mb, r);  // every lane shuffles
+            const uint64_t b = live ? br : 0;
             uint32_t wn[4] = {0, 0, 0, 0};
-            if (r + 1 < cnt) {
-                const uint64_t an = __shfl_sync(0xffffffffu, ma, r + 1), bn = __shfl_sync(0xffffffffu, mb, r + 1);
-                load16(fq, an + 16 * (uint64_t)lane, bn, lane == 31, wn);
+            if (2 * p + 2 < cnt) {
+                const int rn = r + 2;
+                const uint64_t an = __shfl_sync(full, ma, rn & 31), bn = __shfl_sync(full, mb, rn & 31);
+                load16(fq, an + 16 * (uint64_t)j, rn < cnt ? bn : 0, j == 15, wn);
             }
             const uint64_t len = b > a ? b - a : 0;
+            const uint32_t np = (uint32_t)((len + 255) / 256);
+            const uint32_t passes = max(np, __shfl_xor_sync(full, np, 16));
             bool has_n = false, bad = false;
-            for (uint64_t c0 = 0; 16 * c0 < len; c0 += 32) {  // 32 chunks of 16 bytes per pass
-                const uint64_t s = a + 16 * (c0 + lane);
-                if (c0) load16(fq, s, b, lane == 31, w);
+            for (uint32_t c0 = 0; c0 < passes; ++c0) {  // 16 chunks of 16 bytes per pass and half
+                const uint64_t s = a + 256 * (uint64_t)c0 + 16 * (uint64_t)j;
+                if (c0) load16(fq, s, b, j == 15, w);
                 check16(w, s < b ? (int)(b - s < 16 ? b - s : 16) : 0, has_n, bad);
             }
-            has_n = __any_sync(0xffffffffu, has_n);
-            bad = __any_sync(0xffffffffu, bad);
-            const bool keep = !has_n && len > 0;
-            if (lane == r) my_keep = keep;
+            const uint32_t mn = __ballot_sync(full, has_n), mbad = __ballot_sync(full, bad);
+            const bool hn = ((mn >> (16 * h)) & 0xffffu) != 0, hb = ((mbad >> (16 * h)) & 0xffffu) != 0;
+            const bool keep = live && !hn && len > 0;
+            const uint32_t kb = __ballot_sync(full, keep);
+            if (lane == 2 * p) my_keep = kb & 1u;
+            if (lane == 2 * p + 1) my_keep = (kb >> 16) & 1u;
             if (keep) {
                 const uint32_t l32 = len > 0xffffffffull ? 0xffffffffu : (uint32_t)len;
                 lmin = min(lmin, l32);
                 lmax = max(lmax, l32);
-                bad_any |= bad ? 1u : 0u;
+                bad_any |= hb ? 1u : 0u;
             }
 #pragma unroll
             for (int k = 0; k < 4; ++k) w[k] = wn[k];
         }
         if (kl < n_rec) hq[kl] = my_keep ? 1u : 0u;
     }
+    // both halves' extremes
+    lmin = min(lmin, __shfl_xor_sync(full, lmin, 16));
+    lmax = max(lmax, __shfl_xor_sync(full, lmax, 16));
+    bad_any |= __shfl_xor_sync(full, bad_any, 16);
     if (lane == 0) {
         if (lmax) {
             atomicMin(len_minmax, lmin);
