@@ -59,41 +59,50 @@ __global__ void __launch_bounds__(256) nl_count_kernel(const uint8_t *__restrict
 }
 
 // Newline g ends line g.  Line 4k+1 is record k's sequence: it starts after
-// newline 4k and ends at newline 4k+1.
+// newline 4k and ends at newline 4k+1.  Thread t of a tile takes its 64
+// consecutive bytes (4 x 16-byte loads): one CTA scan of the per-thread
+// newline counts gives each thread the line id of its first newline.
 __global__ void __launch_bounds__(256) nl_locate_kernel(const uint8_t *__restrict__ fq, uint64_t F,
                                                         const uint64_t *__restrict__ tile_excl,
                                                         uint64_t *__restrict__ seq_start,
                                                         uint64_t *__restrict__ seq_end) {
     __shared__ uint32_t s_warp[8];
-    const uint64_t base = (uint64_t)blockIdx.x * kParseTile;
-    uint64_t g = tile_excl[blockIdx.x];
-#pragma unroll 1
-    for (int k = 0; k < 4; ++k) {
-        const uint64_t off = base + ((uint64_t)k * 256 + threadIdx.x) * 16;
-        uint32_t w[4] = {0, 0, 0, 0};
-        if (off + 16 <= F) {
-            uint4 v = *reinterpret_cast<const uint4 *>(fq + off);
-            w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
-        } else {
-            for (int b = 0; b < 16; ++b)
-                if (off + b < F) w[b >> 2] |= (uint32_t)fq[off + b] << (8 * (b & 3));
-        }
-        uint32_t cnt = nl_in_word(w[0]) + nl_in_word(w[1]) + nl_in_word(w[2]) + nl_in_word(w[3]);
-        uint32_t tot;
-        uint64_t my = g + block_exclusive_scan<256, uint32_t>(cnt, s_warp, &tot);
-        if (cnt) {
+    const uint64_t base = (uint64_t)blockIdx.x * kParseTile + (uint64_t)threadIdx.x * 64;
+    uint32_t w[16];
 #pragma unroll
-            for (int b = 0; b < 16; ++b) {
-                if (((w[b >> 2] >> (8 * (b & 3))) & 0xffu) == '\n') {
-                    const uint64_t pos = off + b;
-                    const uint32_t r = (uint32_t)(my & 3u);
-                    if (r == 0) seq_start[my >> 2] = pos + 1;
-                    else if (r == 1) seq_end[my >> 2] = pos;
-                    ++my;
-                }
-            }
+    for (int k = 0; k < 4; ++k) {
+        const uint64_t off = base + 16 * k;
+        if (off + 16 <= F) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4 *>(fq + off));
+            w[4 * k] = v.x;
+            w[4 * k + 1] = v.y;
+            w[4 * k + 2] = v.z;
+            w[4 * k + 3] = v.w;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) w[4 * k + q] = 0;
+            for (int bb = 0; bb < 16; ++bb)
+                if (off + bb < F) w[4 * k + (bb >> 2)] |= (uint32_t)fq[off + bb] << (8 * (bb & 3));
         }
-        g += tot;
+    }
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) cnt += nl_in_word(w[q]);
+    uint32_t tot;
+    uint64_t my = tile_excl[blockIdx.x] + block_exclusive_scan<256, uint32_t>(cnt, s_warp, &tot);
+    if (!cnt) return;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        uint32_t m = __vcmpeq4(w[q], 0x0a0a0a0au);  // 0xff in each newline byte
+        while (m) {
+            const int bb = (__ffs(m) - 1) >> 3;
+            m &= ~(0xffu << (8 * bb));
+            const uint64_t pos = base + 4 * q + bb;
+            const uint32_t r = (uint32_t)(my & 3u);
+            if (r == 0) seq_start[my >> 2] = pos + 1;
+            else if (r == 1) seq_end[my >> 2] = pos;
+            ++my;
+        }
     }
 }
 
@@ -291,24 +300,47 @@ __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__
             const uint64_t an = __shfl_sync(0xffffffffu, my_start, mn);
             load16(fq, an + 16 * (uint64_t)j, r0 + mn < n ? an + (uint64_t)L : 0, last, wn);
         }
+        static_assert(kR1 == 5u && kR2 == 7u, "powers of the radices below");
+        // four bases per step: the 4-base Horner value needs no reduction
+        // (at most 4 (R^3 + R^2 + R + 1) = 1600), one fold per step
         uint32_t hf1 = 0, hf2 = 0, hr1 = 0, hr2 = 0, word = 0;
+        const int vbl = live ? vb : 0;
+        uint32_t cw[4];
 #pragma unroll
-        for (int t = 0; t < 16; ++t) {
-            if (live && t < vb) {
-                const uint32_t v = base_code((uint8_t)byte_of(w, t));
-                word |= v << (2 * t);
-                hf1 = horner1(hf1, v + 1);
-                hf2 = horner2(hf2, v + 1);
+        for (int k = 0; k < 4; ++k) cw[k] = (w[k] >> 1) & 0x03030303u;  // base codes, one per byte
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {  // forward, first base most significant
+            const int nk = min(max(vbl - 4 * k, 0), 4);
+            const uint32_t e = cw[k] + 0x01010101u;
+            const uint32_t e0 = e & 0xffu, e1 = (e >> 8) & 0xffu, e2 = (e >> 16) & 0xffu, e3 = e >> 24;
+            if (nk == 4) {
+                hf1 = mod1((uint64_t)hf1 * 625u + (e0 * 125u + e1 * 25u + e2 * 5u + e3));
+                hf2 = mod2((uint64_t)hf2 * 2401u + (e0 * 343u + e1 * 49u + e2 * 7u + e3));
+            } else if (nk > 0) {  // the read's last bases
+                uint32_t a1 = e0, a2 = e0, p1 = 5u, p2 = 7u;
+                if (nk > 1) a1 = a1 * 5u + e1, a2 = a2 * 7u + e1, p1 = 25u, p2 = 49u;
+                if (nk > 2) a1 = a1 * 5u + e2, a2 = a2 * 7u + e2, p1 = 125u, p2 = 343u;
+                hf1 = mod1((uint64_t)hf1 * p1 + a1);
+                hf2 = mod2((uint64_t)hf2 * p2 + a2);
             }
+            uint32_t y = (cw[k] | (cw[k] >> 6)) & 0x000f000fu;  // four 2-bit codes -> 8 bits
+            word |= ((y & 0xfu) | ((y >> 12) & 0xf0u)) << (8 * k);
         }
 #pragma unroll
-        for (int t = 15; t >= 0; --t) {
-            if (live && t < vb) {
-                const uint32_t e = (((word >> (2 * t)) & 3u) ^ 2u) + 1u;  // complement
-                hr1 = horner1(hr1, e);
-                hr2 = horner2(hr2, e);
+        for (int k = 3; k >= 0; --k) {  // reverse complement: sum of e'_t R^t, highest t first
+            const int nk = min(max(vbl - 4 * k, 0), 4);
+            const uint32_t e = (cw[k] ^ 0x02020202u) + 0x01010101u;  // complement
+            const uint32_t e0 = e & 0xffu, e1 = (e >> 8) & 0xffu, e2 = (e >> 16) & 0xffu, e3 = e >> 24;
+            if (nk > 0) {
+                uint32_t g1 = e0, g2 = e0;
+                if (nk > 1) g1 += e1 * 5u, g2 += e1 * 7u;
+                if (nk > 2) g1 += e2 * 25u, g2 += e2 * 49u;
+                if (nk > 3) g1 += e3 * 125u, g2 += e3 * 343u;
+                hr1 = mod1((uint64_t)hr1 * 625u + g1);  // words below the top one are full
+                hr2 = mod2((uint64_t)hr2 * 2401u + g2);
             }
         }
+        word &= vbl >= 16 ? 0xffffffffu : (1u << (2 * vbl)) - 1u;
         uint64_t f1 = 0, f2 = 0, g1 = 0, g2 = 0;
         if (live && act) {
             f1 = mod1((uint64_t)hf1 * pf1);
