@@ -171,7 +171,7 @@ struct emp_job {
     DevBuf dout;                 // output.bin records written on the device (after those in `out`)
     uint64_t dout_bytes = 0;
     PinnedBuf h_out;
-    DevBuf bk_lst0, bk_lst1, bk_offs, bk_tile_base, bk_spans, bk_sfrom, bk_sto, bk_scratch, bk_job, bk_meta;  // bucket kernel
+    DevBuf bk_lst0, bk_lst1, bk_cnt, bk_spill, bk_spans, bk_sfrom, bk_sto, bk_scratch, bk_job, bk_meta;  // bucket kernel
     PinnedBuf h_coop;
     cudaEvent_t sort_ev[2 * kSortPasses] = {};
     cudaEvent_t upd_ev[2 * EMP_MAX_ROUNDS] = {};
@@ -796,13 +796,20 @@ emp_status run_rounds_coop(emp_job *j, cudaStream_t s, const RoundEnv &env, cons
 emp_status bucket_prepare(emp_job *j, cudaStream_t s, const RoundEnv &env, int r0, int cur, uint64_t n_in,
                           uint64_t ecap, uint32_t wave, BktJob *hj) {
     const uint64_t nmax = n_in;
-    const uint64_t ktiles = bkt_max_tiles(nmax, wave);
     const uint32_t nb_max = bkt_count(nmax, wave);
-    const size_t offs_words = bkt_offs_words(nmax, wave);
-    EMP_TRY(ensure(j, j->bk_lst0, nmax * sizeof(BktEntry)));
-    EMP_TRY(ensure(j, j->bk_lst1, nmax * sizeof(BktEntry)));
-    EMP_TRY(ensure(j, j->bk_offs, 2 * offs_words * 4));
-    EMP_TRY(ensure(j, j->bk_tile_base, 2 * ktiles * 8));
+    uint32_t cap = kBktRegionCap;
+    if (const char *c = std::getenv("EMP_BKT_REGION_CAP")) {  // testing: small regions force the spill path
+        const long v = std::strtol(c, nullptr, 10);
+        if (v >= 1 && v <= (long)kBktRegionCap) cap = (uint32_t)v;
+    }
+    const uint64_t list_entries = (uint64_t)nb_max * 2 * cap;
+    const uint64_t iters = (uint64_t)(env.rounds - r0) + 1;  // lists of iterations 0 .. rounds - r0
+    const size_t cnt_bytes = iters * 2 * nb_max * 4;
+    EMP_TRY(ensure(j, j->bk_lst0, list_entries * sizeof(BktEntry)));
+    EMP_TRY(ensure(j, j->bk_lst1, list_entries * sizeof(BktEntry)));
+    EMP_TRY(ensure(j, j->bk_cnt, cnt_bytes + iters * 4));
+    EMP_TRY(ensure(j, j->bk_spill, 2 * nmax * (sizeof(BktEntry) + 4)));
+    EMP_CUDA(cudaMemsetAsync(j->bk_cnt.p, 0, cnt_bytes + iters * 4, s));
     EMP_TRY(ensure(j, j->bk_spans, (size_t)env.rounds * nb_max * sizeof(BktSpan)));
     EMP_TRY(ensure(j, j->bk_sfrom, ecap * 4));
     EMP_TRY(ensure(j, j->bk_sto, ecap * 4));
@@ -825,10 +832,13 @@ emp_status bucket_prepare(emp_job *j, cudaStream_t s, const RoundEnv &env, int r
     hj->rounds = env.rounds;
     hj->tables = env.tables;
     hj->n_in = n_in;
-    hj->offs[0] = j->bk_offs.as<uint32_t>();
-    hj->offs[1] = hj->offs[0] + offs_words;
-    hj->tile_base[0] = j->bk_tile_base.as<uint64_t>();
-    hj->tile_base[1] = hj->tile_base[0] + ktiles;
+    hj->cnt = j->bk_cnt.as<uint32_t>();
+    hj->spill_n = hj->cnt + iters * 2 * nb_max;
+    hj->spill[0] = j->bk_spill.as<BktEntry>();
+    hj->spill[1] = hj->spill[0] + nmax;
+    hj->spill_tag[0] = reinterpret_cast<uint32_t *>(hj->spill[1] + nmax);
+    hj->spill_tag[1] = hj->spill_tag[0] + nmax;
+    hj->cap = cap;
     hj->spans = j->bk_spans.as<BktSpan>();
     hj->sfrom = j->bk_sfrom.as<uint32_t>();
     hj->sto = j->bk_sto.as<uint32_t>();
@@ -1883,7 +1893,7 @@ static void release_buffers(emp_job *job) {
                       &job->lv_init, &job->bloom_s, &job->bloom_p, &job->ck, &job->cv, &job->ck2, &job->cv2,
                       &job->records, &job->st_upd, &job->st_cand, &job->st_scan, &job->ctl, &job->st_join,
                       &job->st_sort, &job->coop_job, &job->coop_ctl, &job->coop_trace,
-                      &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_offs, &job->bk_tile_base, &job->bk_spans,
+                      &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_cnt, &job->bk_spill, &job->bk_spans,
                       &job->bk_sfrom, &job->bk_sto, &job->bk_scratch, &job->bk_job, &job->dout,
                       &job->bk_meta, &job->xk0, &job->xv0, &job->xk1, &job->xv1, &job->ring_k, &job->ring_v,
                       &job->cparts};

@@ -44,7 +44,6 @@ namespace {
 constexpr uint32_t kBStage = 7168;  // entries of a bucket staged in shared memory
 constexpr uint32_t kBHash = 16384;  // hash slots in shared memory (power of two)
 constexpr uint32_t kBCand = 1024;   // matched entries sorted in shared memory
-constexpr uint32_t kSegMax = 4096;  // tile pieces gathered through the owner table
 constexpr uint64_t kEmptySlot = ~0ull;  // never a key: fp1, fp2 < 2^29
 constexpr uint8_t kMatched = 1, kUsed = 2;
 
@@ -60,11 +59,6 @@ constexpr size_t kOffReg = kOffFlag + kBStage;
 constexpr size_t kRegion = kBHash * 4 + kBStage * 2;
 constexpr size_t kRSmem = kOffReg + kRegion;
 static_assert(kOffReg % 16 == 0, "aligned region");
-// gather
-constexpr size_t kGSegStart = 0;                          // u64 [kSegMax]
-constexpr size_t kGSegPos = kGSegStart + kSegMax * 8;     // u32 [kSegMax + 1]
-constexpr size_t kGOwner = kGSegPos + (kSegMax + 4) * 4;  // u16 [kBStage]
-static_assert(kGOwner + kBStage * 2 <= kRegion, "gather tables fit the region");
 // hash set
 constexpr size_t kHSlot = 0;                 // u32 [kBHash]
 constexpr size_t kHSuffixSlot = kBHash * 4;  // u16 [kBStage]
@@ -88,7 +82,7 @@ constexpr size_t kPBin = kPRank + kBStage * 2;              // u16 [kBStage]
 static_assert(kPBin + kBStage * 2 <= kRegion, "partition tables fit the region");
 static_assert(2 * kBktMaxBuckets <= 65536, "bins fit u16");
 // prologue tile: bin counters, then the staged tile
-constexpr size_t kASmem = 2 * kBktMaxBuckets * 4 + kBktTile * sizeof(BktEntry);
+constexpr size_t kASmem = 2 * kBktMaxBuckets * 4 + kBktTile * sizeof(BktEntry) + kBktTile * 2;
 // end phase: one round's bucket destinations, the record offsets of a job
 constexpr size_t kESmem = (kBktMaxBuckets + 1 + 3 * kT) * 8;
 constexpr size_t kBktSmem = kRSmem > kASmem ? (kRSmem > kESmem ? kRSmem : kESmem) : kASmem;
@@ -238,15 +232,112 @@ EMP_DEV uint64_t step_key(const StepArgs &a, uint64_t key, uint32_t val, uint32_
     return t == 0 ? next_sfx(key, b, a.pw1, a.pw2) : prev_pfx(key, b, a.inv1, a.inv2);
 }
 
+// ---------------------------------------------------------------- lists
+// The list of iteration g as read (round r0 + g) and as written.
+struct ListIn {
+    const uint4 *lst;      // regions, bin-major
+    uint32_t cap;          // entries per region
+    const uint4 *spill;    // entries past a region's capacity ...
+    const uint32_t *stag;  // ... and their bins
+    const uint32_t *spill_n;
+    const uint32_t *cnt;   // entries of each bin
+};
+struct ListOut {
+    uint4 *lst;
+    uint32_t cap;
+    uint4 *spill;
+    uint32_t *stag;
+    uint32_t *spill_n;
+    uint32_t *cnt;
+};
+EMP_DEV ListIn list_in(const BktJob &J, uint32_t g) {
+    ListIn l;
+    l.lst = reinterpret_cast<const uint4 *>(J.lst[g & 1]);
+    l.cap = J.cap;
+    l.spill = reinterpret_cast<const uint4 *>(J.spill[g & 1]);
+    l.stag = J.spill_tag[g & 1];
+    l.spill_n = J.spill_n + g;
+    l.cnt = J.cnt + (uint64_t)g * 2 * J.nb_max;
+    return l;
+}
+EMP_DEV ListOut list_out(const BktJob &J, uint32_t g) {
+    ListOut l;
+    l.lst = reinterpret_cast<uint4 *>(J.lst[g & 1]);
+    l.cap = J.cap;
+    l.spill = reinterpret_cast<uint4 *>(J.spill[g & 1]);
+    l.stag = J.spill_tag[g & 1];
+    l.spill_n = J.spill_n + g;
+    l.cnt = J.cnt + (uint64_t)g * 2 * J.nb_max;
+    return l;
+}
+// entry e at position pos of bin `bin`: in the bin's region, or spilled
+EMP_DEV void put_list(const ListOut &o, uint32_t bin, uint32_t pos, const uint4 &e) {
+    if (pos < o.cap) {
+        o.lst[(uint64_t)bin * o.cap + pos] = e;
+    } else {
+        const uint32_t q = atomicAdd(o.spill_n, 1u);
+        o.spill[q] = e;
+        o.stag[q] = bin;
+    }
+}
+
+// hist[b] (this tile's count of bin b) -> its local start; returns the
+// tile's entry count.
+EMP_DEV uint32_t bin_starts(uint32_t *hist, uint32_t nbin, BShared &sh) {
+    const uint32_t per = (nbin + kT - 1) / kT;
+    const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
+    const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
+    uint32_t run = 0;
+    for (uint32_t b = b0; b < b1; ++b) run += hist[b];
+    uint32_t kept;
+    uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &kept);
+    for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t h = hist[b];
+        hist[b] = ex;
+        ex += h;
+    }
+    __syncthreads();
+    return kept;
+}
+
+// Reserve this tile's entries of every bin in the list's bin counters
+// (hist[b] = the bin's local start on entry).  Afterwards hist[b] = the
+// bin's global position minus its local start (mod 2^32), or the global
+// position itself when `base` is set.
+EMP_DEV void reserve_bins(uint32_t *hist, uint32_t nbin, uint32_t kept, uint32_t *cnt, bool base) {
+    constexpr int kMaxPer = 2 * kBktMaxBuckets / kT;
+    const uint32_t per = (nbin + kT - 1) / kT;
+    const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
+    const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
+    uint32_t v[kMaxPer];
+#pragma unroll
+    for (int i = 0; i < kMaxPer; ++i) {
+        const uint32_t b = b0 + i;
+        v[i] = 0;
+        if (b < b1) {
+            const uint32_t lo = hist[b], hi = b + 1 < nbin ? hist[b + 1] : kept;
+            const uint32_t g = hi > lo ? atomicAdd(cnt + b, hi - lo) : 0u;
+            v[i] = base ? g : g - lo;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kMaxPer; ++i)
+        if (b0 + i < b1) hist[b0 + i] = v[i];
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------- prologue
-// Tile k of the launch's input list -> round r0's list (tile k).
+// Tile k of the launch's input list -> round r0's list (iteration 0's bins).
 EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
     BktRound &I = J.meta[J.r0];
     const uint64_t n_in = J.n_in;
-    const uint32_t nb = bkt_count(n_in, J.wave), nbin = 2 * nb, stride = nbin + 1;
+    const uint32_t nb = bkt_count(n_in, J.wave), nbin = 2 * nb;
     const StepArgs a = step_args(J, sh.tab, J.r0, true);
+    const ListOut lo = list_out(J, 0);
     uint32_t *hist = reinterpret_cast<uint32_t *>(smem);
     uint4 *stage = reinterpret_cast<uint4 *>(smem + 2 * kBktMaxBuckets * 4);
+    uint16_t *sbin = reinterpret_cast<uint16_t *>(stage + kBktTile);
     for (uint32_t i = threadIdx.x; i < nbin; i += kT) hist[i] = 0;
     if (threadIdx.x == 0) sh.sfx = 0;
     __syncthreads();
@@ -280,83 +371,50 @@ EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
     }
     if (sfx) atomicAdd(&sh.sfx, sfx);
     __syncthreads();
-    const uint32_t per = (nbin + kT - 1) / kT;
-    const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
-    const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
-    uint32_t run = 0;
-    for (uint32_t b = b0; b < b1; ++b) run += hist[b];
-    uint32_t kept;
-    uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &kept);
-    uint32_t *orow = J.offs[0] + (uint64_t)k * stride;
-    for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t h = hist[b];
-        hist[b] = ex;
-        orow[b] = ex;
-        ex += h;
-    }
+    const uint32_t kept = bin_starts(hist, nbin, sh);
     if (threadIdx.x == 0) {
-        orow[nbin] = kept;
-        const uint64_t ob = atomicAdd(reinterpret_cast<unsigned long long *>(&I.n), (unsigned long long)kept);
-        sh.base = ob;
-        J.tile_base[0][k] = ob;
+        if (kept) atomicAdd(reinterpret_cast<unsigned long long *>(&I.n), (unsigned long long)kept);
         if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&I.s), (unsigned long long)sh.sfx);
     }
-    __syncthreads();
 #pragma unroll
-    for (int c = 0; c < kC; ++c) {
+    for (int c = 0; c < kC; ++c) {  // the tile in bin order
         if (!keep[c]) continue;
-        stage[hist[bin[c]] + rank[c]] = make_uint4((uint32_t)key[c], (uint32_t)(key[c] >> 32), val[c], word[c]);
+        const uint32_t d = hist[bin[c]] + rank[c];
+        stage[d] = make_uint4((uint32_t)key[c], (uint32_t)(key[c] >> 32), val[c], word[c]);
+        sbin[d] = (uint16_t)bin[c];
     }
     __syncthreads();
-    uint4 *dst = reinterpret_cast<uint4 *>(J.lst[0] + sh.base);
-    for (uint32_t x = threadIdx.x; x < kept; x += kT) dst[x] = stage[x];
+    reserve_bins(hist, nbin, kept, lo.cnt, false);
+    for (uint32_t x = threadIdx.x; x < kept; x += kT) put_list(lo, sbin[x], x + hist[sbin[x]], stage[x]);
     __syncthreads();
 }
 
 // ---------------------------------------------------------------- gather
-EMP_DEV void put_entry(const Stage &v, uint32_t d, const BktEntry *lst, uint64_t src) {
-    const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(lst + src));
+EMP_DEV void put_entry(const Stage &v, uint32_t d, const uint4 *src) {
+    const uint4 q = __ldcg(src);
     v.key[d] = (uint64_t)q.x | ((uint64_t)q.y << 32);
     v.val[d] = q.z;
     v.word[d] = q.w;
     v.flag[d] = 0;
 }
 
-// Gather bucket b of a round whose list has K tiles partitioned into nb
-// buckets.  Pieces q = 0 .. 2K-1: the suffix piece of tile q, then (q >= K)
-// the prefix piece of tile q - K, so the bucket is staged suffixes first.
-// Returns the bucket's size; S = its suffixes, G = its position in bucket
-// order (entries of lower buckets), v = shared memory or the scratch region.
-// The gather for many pieces (more than kSegMax) or a bucket too big for
-// shared memory: 512 pieces at a time, a binary search per staged entry.
-EMP_COLD uint32_t gather_general(const BktJob &J, const BktEntry *lst, const uint32_t *offs, const uint64_t *tbase,
-                                 uint32_t K, uint32_t nb, uint32_t b, BShared &sh, uint8_t *smem, Stage &v,
-                                 uint32_t &S, uint64_t &G) {
-    const uint32_t stride = 2 * nb + 1, Q = 2 * K;
-    uint8_t *reg = smem + kOffReg;
-    auto piece = [&](uint32_t q, uint32_t &lo, uint32_t &cnt) -> uint32_t {  // returns the tile
-        const uint32_t k = q < K ? q : q - K, bin = 2 * b + (q < K ? 0u : 1u);
-        lo = __ldcg(offs + (uint64_t)k * stride + bin);
-        cnt = __ldcg(offs + (uint64_t)k * stride + bin + 1) - lo;
-        return k;
-    };
-    uint64_t tot = 0, tsfx = 0, gpre = 0;
-    for (uint32_t q = threadIdx.x; q < Q; q += kT) {
-        uint32_t lo, cnt;
-        piece(q, lo, cnt);
-        tot += cnt;
-        if (q < K) {
-            tsfx += cnt;
-            gpre += lo;  // entries of lower buckets in tile q
-        }
-    }
-    uint64_t t1, t2, t3;
-    block_exclusive_scan<kT, uint64_t>(tot, sh.scan64, &t1);
-    block_exclusive_scan<kT, uint64_t>(tsfx, sh.scan64, &t2);
-    block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &t3);
-    const uint32_t total = (uint32_t)t1;
-    S = (uint32_t)t2;
-    G = t3;
+// Entries of the list's bins below bin `bin` (the bucket's position in
+// bucket order: its region of the global scratch).
+EMP_DEV uint64_t bins_below(const uint32_t *cnt, uint32_t bin, BShared &sh) {
+    uint64_t pre = 0;
+    for (uint32_t q = threadIdx.x; q < bin; q += kT) pre += __ldcg(cnt + q);
+    uint64_t tot;
+    block_exclusive_scan<kT, uint64_t>(pre, sh.scan64, &tot);
+    return tot;
+}
+
+// Bucket b with spilled entries or too big for shared memory: the region
+// parts, then the bins' spilled entries found in the list's spill area;
+// staged in shared memory when it fits, else in the scratch region G.
+EMP_COLD uint32_t gather_general(const BktJob &J, const ListIn li, uint32_t b, uint32_t cS, uint32_t cP, BShared &sh,
+                                 uint8_t *smem, Stage &v, uint64_t &G) {
+    const uint32_t total = cS + cP;
+    G = bins_below(li.cnt, 2 * b, sh);
     if (total <= kBStage) {
         v.key = reinterpret_cast<uint64_t *>(smem + kOffKey);
         v.val = reinterpret_cast<uint32_t *>(smem + kOffVal);
@@ -370,127 +428,72 @@ EMP_COLD uint32_t gather_general(const BktJob &J, const BktEntry *lst, const uin
         v.word = gs.word + G;
         v.flag = gs.flag + G;
     }
-    uint64_t *seg_start = reinterpret_cast<uint64_t *>(reg + kGSegStart);
-    uint32_t *seg_pos = reinterpret_cast<uint32_t *>(reg + kGSegPos);
-    uint32_t gathered = 0;
-    for (uint32_t q0 = 0; q0 < Q && total; q0 += kT) {
-        const uint32_t q = q0 + threadIdx.x;
-        uint32_t lo = 0, cnt = 0;
-        uint64_t start = 0;
-        if (q < Q) {
-            const uint32_t k = piece(q, lo, cnt);
-            start = __ldcg(tbase + k) + lo;
+    const uint32_t rS = cS < li.cap ? cS : li.cap, rP = cP < li.cap ? cP : li.cap;
+    const uint4 *rs = li.lst + (uint64_t)(2 * b) * li.cap, *rp = li.lst + (uint64_t)(2 * b + 1) * li.cap;
+    for (uint32_t x = threadIdx.x; x < rS; x += kT) put_entry(v, x, rs + x);
+    for (uint32_t x = threadIdx.x; x < rP; x += kT) put_entry(v, cS + x, rp + x);
+    if (cS > li.cap || cP > li.cap) {
+        if (threadIdx.x == 0) {
+            sh.cnt = 0;
+            sh.tile = 0;
         }
-        uint32_t ctot;
-        const uint32_t ex = block_exclusive_scan<kT, uint32_t>(cnt, sh.scan32, &ctot);
-        seg_start[threadIdx.x] = start;
-        seg_pos[threadIdx.x] = ex;
         __syncthreads();
-        for (uint32_t x = threadIdx.x; x < ctot; x += kT) {
-            uint32_t lo2 = 0, hi = kT;  // last piece with seg_pos <= x
-            while (hi - lo2 > 1) {
-                const uint32_t m = (lo2 + hi) >> 1;
-                if (seg_pos[m] <= x) lo2 = m;
-                else hi = m;
-            }
-            put_entry(v, gathered + x, lst, seg_start[lo2] + (x - seg_pos[lo2]));
+        const uint32_t ns = __ldcg(li.spill_n);
+        for (uint32_t q = threadIdx.x; q < ns; q += kT) {
+            const uint32_t t = __ldcg(li.stag + q);
+            if (t == 2 * b) put_entry(v, rS + atomicAdd(&sh.cnt, 1u), li.spill + q);
+            else if (t == 2 * b + 1) put_entry(v, cS + rP + atomicAdd(&sh.tile, 1u), li.spill + q);
         }
-        gathered += ctot;
-        __syncthreads();
     }
+    __syncthreads();
     return total;
 }
 
-EMP_COLD uint32_t gather(const BktJob &J, const BktEntry *lst, const uint32_t *offs, const uint64_t *tbase,
-                        uint32_t K, uint32_t nb, uint32_t b, BShared &sh, uint8_t *smem, Stage &v, uint32_t &S,
-                        uint64_t &G) {
-    const uint32_t stride = 2 * nb + 1, Q = 2 * K;
-    uint8_t *reg = smem + kOffReg;
-    auto piece = [&](uint32_t q, uint32_t &lo, uint32_t &cnt) -> uint32_t {  // returns the tile
-        const uint32_t k = q < K ? q : q - K, bin = 2 * b + (q < K ? 0u : 1u);
-        lo = __ldcg(offs + (uint64_t)k * stride + bin);
-        cnt = __ldcg(offs + (uint64_t)k * stride + bin + 1) - lo;
-        return k;
-    };
-    if (Q <= kSegMax) {
-        // each thread takes up to 8 consecutive pieces; an owner table maps
-        // staged entries to pieces
-        uint64_t *seg_start = reinterpret_cast<uint64_t *>(reg + kGSegStart);
-        uint32_t *seg_pos = reinterpret_cast<uint32_t *>(reg + kGSegPos);
-        uint16_t *owner = reinterpret_cast<uint16_t *>(reg + kGOwner);
-        constexpr int kPer = kSegMax / kT;
-        const uint32_t per = (Q + kT - 1) / kT;  // pieces of each thread, 1..kPer
-        const uint32_t q0 = threadIdx.x * per;
-        uint32_t cnt[kPer];
-        uint32_t run = 0;
+// Gather bucket b of the list: its suffix region, then its prefix region
+// (two contiguous runs), so the bucket is staged suffixes first.  Returns the
+// bucket's size; S = its suffixes, G = its position in bucket order (for the
+// global scratch), v = shared memory or the scratch region.
+EMP_COLD uint32_t gather(const BktJob &J, const ListIn li, uint32_t b, BShared &sh, uint8_t *smem, Stage &v,
+                         uint32_t &S, uint64_t &G) {
+    if (threadIdx.x == 0) {
+        sh.cnt = __ldcg(li.cnt + 2 * b);
+        sh.tile = __ldcg(li.cnt + 2 * b + 1);
+    }
+    __syncthreads();
+    const uint32_t cS = sh.cnt, cP = sh.tile, total = cS + cP;
+    S = cS;
+    sprobe(sh, 11);
+    if (total <= kBStage && cS <= li.cap && cP <= li.cap) {
+        G = 0;
+        v.key = reinterpret_cast<uint64_t *>(smem + kOffKey);
+        v.val = reinterpret_cast<uint32_t *>(smem + kOffVal);
+        v.word = reinterpret_cast<uint32_t *>(smem + kOffWord);
+        v.flag = smem + kOffFlag;
+        const uint64_t rs = (uint64_t)(2 * b) * li.cap, rp = (uint64_t)(2 * b + 1) * li.cap;
+        sprobe(sh, 12);
+        constexpr int U = 8;
+        for (uint32_t x0 = 0; x0 < total; x0 += U * kT) {
+            uint4 e[U];
 #pragma unroll
-        for (int i = 0; i < kPer; ++i) {
-            const uint32_t q = q0 + i;
-            cnt[i] = 0;
-            if (i < (int)per && q < Q) {
-                uint32_t lo;
-                const uint32_t k = piece(q, lo, cnt[i]);
-                seg_start[q] = __ldcg(tbase + k) + lo;
+            for (int u = 0; u < U; ++u) {
+                const uint32_t x = x0 + u * kT + threadIdx.x;
+                if (x < total) e[u] = __ldcg(li.lst + (x < cS ? rs + x : rp + (x - cS)));
             }
-            run += cnt[i];
-        }
-        uint32_t total;
-        uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &total);
-        sprobe(sh, 11);
 #pragma unroll
-        for (int i = 0; i < kPer; ++i) {
-            const uint32_t q = q0 + i;
-            if (i < (int)per && q < Q) {
-                seg_pos[q] = ex;
-                if (q == K) sh.cnt = ex;  // suffixes: the pieces before the first prefix piece
-            }
-            ex += cnt[i];
-        }
-        if (threadIdx.x == 0) seg_pos[Q] = total;
-        if (total <= kBStage) {
-            G = 0;
-            v.key = reinterpret_cast<uint64_t *>(smem + kOffKey);
-            v.val = reinterpret_cast<uint32_t *>(smem + kOffVal);
-            v.word = reinterpret_cast<uint32_t *>(smem + kOffWord);
-            v.flag = smem + kOffFlag;
-            __syncthreads();
-            // owner table: one warp per piece
-            const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-            for (uint32_t q = warp; q < Q; q += kT / 32) {
-                const uint32_t lo = seg_pos[q], hi = seg_pos[q + 1];
-                for (uint32_t x = lo + lane; x < hi; x += 32) owner[x] = (uint16_t)q;
-            }
-            __syncthreads();
-            S = sh.cnt;
-            sprobe(sh, 12);
-            constexpr int U = 8;
-            for (uint32_t x0 = 0; x0 < total; x0 += U * kT) {
-                uint4 e[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const uint32_t x = x0 + u * kT + threadIdx.x;
-                    if (x < total) {
-                        const uint32_t o = owner[x];
-                        e[u] = __ldcg(reinterpret_cast<const uint4 *>(lst + seg_start[o] + (x - seg_pos[o])));
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const uint32_t x = x0 + u * kT + threadIdx.x;
-                    if (x < total) {
-                        v.key[x] = (uint64_t)e[u].x | ((uint64_t)e[u].y << 32);
-                        v.val[x] = e[u].z;
-                        v.word[x] = e[u].w;
-                        v.flag[x] = 0;
-                    }
+            for (int u = 0; u < U; ++u) {
+                const uint32_t x = x0 + u * kT + threadIdx.x;
+                if (x < total) {
+                    v.key[x] = (uint64_t)e[u].x | ((uint64_t)e[u].y << 32);
+                    v.val[x] = e[u].z;
+                    v.word[x] = e[u].w;
+                    v.flag[x] = 0;
                 }
             }
-            __syncthreads();
-            return total;
         }
         __syncthreads();
+        return total;
     }
-    return gather_general(J, lst, offs, tbase, K, nb, b, sh, smem, v, S, G);
+    return gather_general(J, li, b, cS, cP, sh, smem, v, G);
 }
 
 // ---------------------------------------------------------------- matching
@@ -900,42 +903,10 @@ EMP_DEV uint64_t join_count(const Cands &w, uint32_t c, BShared &sh) {
 
 // ---------------------------------------------------------------- next round
 // Drop the used entries of the staged bucket, apply round a.r's hash step to
-// the rest and write them as tile `tile` of the next list, partitioned into
-// nb buckets.  Returns nothing; counts go to the next round's BktRound.
-// Bin starts of the next tile (in place in hist), its offs row, its place in
-// the next list; returns the kept count.
-EMP_DEV uint32_t close_tile(uint32_t *hist, uint32_t nbin, uint32_t tile, uint32_t *offs, uint64_t *tbase,
-                            BktRound &nx, BShared &sh) {
-    const uint32_t per = (nbin + kT - 1) / kT;
-    const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
-    const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
-    uint32_t run = 0;
-    for (uint32_t b = b0; b < b1; ++b) run += hist[b];
-    uint32_t kept;
-    uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &kept);
-    uint32_t *orow = offs + (uint64_t)tile * (nbin + 1);
-    for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t h = hist[b];
-        hist[b] = ex;
-        orow[b] = ex;
-        ex += h;
-    }
-    if (threadIdx.x == 0) {
-        orow[nbin] = kept;
-        const uint64_t ob = kept ? atomicAdd(reinterpret_cast<unsigned long long *>(&nx.n), (unsigned long long)kept)
-                                 : 0ull;
-        sh.base = ob;
-        tbase[tile] = ob;
-        if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.s), (unsigned long long)sh.sfx);
-    }
-    __syncthreads();
-    return kept;
-}
-
-// write_next for a bucket staged in shared memory: the same steps on the
-// shared arrays, the tile permuted in shared memory and written in order.
-EMP_COLD void write_next_smem(uint32_t total, const StepArgs a, uint32_t nb, uint32_t tile, BktEntry *lout,
-                             uint32_t *offs, uint64_t *tbase, BktRound &nx, BShared &sh, uint8_t *smem) {
+// the rest and write them into the next list's bins (nb buckets).  Counts go
+// to the next round's BktRound.
+EMP_COLD void write_next_smem(uint32_t total, const StepArgs a, uint32_t nb, const ListOut lo, BktRound &nx,
+                              BShared &sh, uint8_t *smem) {
     uint64_t *key = reinterpret_cast<uint64_t *>(smem + kOffKey);
     uint32_t *val = reinterpret_cast<uint32_t *>(smem + kOffVal);
     uint32_t *word = reinterpret_cast<uint32_t *>(smem + kOffWord);
@@ -984,31 +955,34 @@ EMP_COLD void write_next_smem(uint32_t total, const StepArgs a, uint32_t nb, uin
     if (sfx) atomicAdd(&sh.sfx, sfx);
     __syncthreads();
     sprobe(sh, 13);
-    const uint32_t kept = close_tile(hist, nbin, tile, offs, tbase, nx, sh);
-    sprobe(sh, 14);
-    for (uint32_t x = threadIdx.x; x < total; x += kT)
+    const uint32_t kept = bin_starts(hist, nbin, sh);
+    if (threadIdx.x == 0) {
+        if (kept) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.n), (unsigned long long)kept);
+        if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.s), (unsigned long long)sh.sfx);
+    }
+    for (uint32_t x = threadIdx.x; x < total; x += kT)  // the kept entries in bin order
         if (!(flag[x] & kUsed)) inv[hist[bin16[x]] + rank16[x]] = (uint16_t)x;
     __syncthreads();
+    sprobe(sh, 14);
+    reserve_bins(hist, nbin, kept, lo.cnt, false);
     sprobe(sh, 15);
-    uint4 *dst = reinterpret_cast<uint4 *>(lout + sh.base);
-    for (uint32_t d = threadIdx.x; d < kept; d += kT) {
-        const uint32_t x = inv[d];
+    for (uint32_t d = threadIdx.x; d < kept; d += kT) {  // each bin a contiguous run of its region
+        const uint32_t x = inv[d], bin = bin16[x];
         const uint64_t k = key[x];
-        dst[d] = make_uint4((uint32_t)k, (uint32_t)(k >> 32), val[x], word[x]);
+        put_list(lo, bin, d + hist[bin], make_uint4((uint32_t)k, (uint32_t)(k >> 32), val[x], word[x]));
     }
     __syncthreads();
 }
 
 EMP_COLD void write_next(BktJob &J, const Stage &v, uint32_t total, bool in_smem, const StepArgs &a, uint32_t nb,
-                         uint32_t tile, BktEntry *lout, uint32_t *offs, uint64_t *tbase, BktRound &nx, BShared &sh,
-                         uint8_t *smem, const BScratch &gs, uint64_t G) {
+                         const ListOut lo, BktRound &nx, BShared &sh, uint8_t *smem, const BScratch &gs, uint64_t G) {
     uint8_t *reg = smem + kOffReg;
     uint32_t *hist = reinterpret_cast<uint32_t *>(reg + kPHist);
     uint16_t *inv = reinterpret_cast<uint16_t *>(reg + kPInv);
     uint16_t *rank16 = reinterpret_cast<uint16_t *>(reg + kPRank);
     uint16_t *bin16 = reinterpret_cast<uint16_t *>(reg + kPBin);
     uint32_t *rank32 = gs.rank + G;
-    const uint32_t nbin = 2 * nb, stride = nbin + 1;
+    const uint32_t nbin = 2 * nb;
     for (uint32_t i = threadIdx.x; i < nbin; i += kT) hist[i] = 0;
     if (threadIdx.x == 0) sh.sfx = 0;
     __syncthreads();
@@ -1052,49 +1026,31 @@ EMP_COLD void write_next(BktJob &J, const Stage &v, uint32_t total, bool in_smem
     if (sfx) atomicAdd(&sh.sfx, sfx);
     __syncthreads();
     sprobe(sh, 13);
-    const uint32_t per = (nbin + kT - 1) / kT;
-    const uint32_t b0 = threadIdx.x * per < nbin ? threadIdx.x * per : nbin;
-    const uint32_t b1 = b0 + per < nbin ? b0 + per : nbin;
-    uint32_t run = 0;
-    for (uint32_t b = b0; b < b1; ++b) run += hist[b];
-    uint32_t kept;
-    uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &kept);
-    uint32_t *orow = offs + (uint64_t)tile * stride;
-    for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t h = hist[b];
-        hist[b] = ex;
-        orow[b] = ex;
-        ex += h;
-    }
+    const uint32_t kept = bin_starts(hist, nbin, sh);
     if (threadIdx.x == 0) {
-        orow[nbin] = kept;
-        const uint64_t ob = kept ? atomicAdd(reinterpret_cast<unsigned long long *>(&nx.n), (unsigned long long)kept)
-                                 : 0ull;
-        sh.base = ob;
-        tbase[tile] = ob;
+        if (kept) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.n), (unsigned long long)kept);
         if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.s), (unsigned long long)sh.sfx);
     }
-    __syncthreads();
     sprobe(sh, 14);
-    BktEntry *dst = lout + sh.base;
-    if (in_smem) {  // permute in shared memory, then write the tile in order
+    if (in_smem) {  // permute in shared memory, then write each bin as a run
         for (uint32_t x = threadIdx.x; x < total; x += kT)
             if (!(v.flag[x] & kUsed)) inv[hist[bin16[x]] + rank16[x]] = (uint16_t)x;
         __syncthreads();
+        reserve_bins(hist, nbin, kept, lo.cnt, false);
         sprobe(sh, 15);
         for (uint32_t d = threadIdx.x; d < kept; d += kT) {
-            const uint32_t x = inv[d];
+            const uint32_t x = inv[d], bin = bin16[x];
             const uint64_t key = v.key[x];
-            reinterpret_cast<uint4 *>(dst)[d] = make_uint4((uint32_t)key, (uint32_t)(key >> 32), v.val[x], v.word[x]);
+            put_list(lo, bin, d + hist[bin], make_uint4((uint32_t)key, (uint32_t)(key >> 32), v.val[x], v.word[x]));
         }
     } else {
+        reserve_bins(hist, nbin, kept, lo.cnt, true);  // hist[bin] = the bin's global position
         for (uint32_t x = threadIdx.x; x < total; x += kT) {
             if (ldv(v.flag + x) & kUsed) continue;
             const uint64_t key = ldv(v.key + x);
             const uint32_t val = ldv(v.val + x);
             const uint32_t bn = 2 * bkt_of(sort_key(key, val), nb) + (val >> 31);
-            reinterpret_cast<uint4 *>(dst)[hist[bn] + ldv(rank32 + x)] =
-                make_uint4((uint32_t)key, (uint32_t)(key >> 32), val, ldv(v.word + x));
+            put_list(lo, bn, hist[bn] + ldv(rank32 + x), make_uint4((uint32_t)key, (uint32_t)(key >> 32), val, ldv(v.word + x)));
         }
     }
     __syncthreads();
@@ -1161,14 +1117,9 @@ EMP_DEV uint32_t compact(const Stage &v, uint32_t total, const Cands &w, uint32_
 
 // More than kBCand matched entries, or a bucket staged in scratch: the
 // matched entries go to the bucket's scratch region and are ranked there.
-EMP_COLD uint64_t big_count(const BktJob &J, const Stage &v, uint32_t total, bool in_smem, uint64_t &G, uint32_t K,
-                            uint32_t nb, uint32_t b, const uint32_t *offs, BShared &sh, uint32_t &c) {
-    if (in_smem) {  // the bucket's position in bucket order picks its scratch region
-        uint64_t gpre = 0;
-        const uint32_t stride = 2 * nb + 1;
-        for (uint32_t k = threadIdx.x; k < K; k += kT) gpre += __ldcg(offs + (uint64_t)k * stride + 2 * b);
-        block_exclusive_scan<kT, uint64_t>(gpre, sh.scan64, &G);
-    }
+EMP_COLD uint64_t big_count(const BktJob &J, const Stage &v, uint32_t total, bool in_smem, uint64_t &G, uint32_t b,
+                            const uint32_t *cnt, BShared &sh, uint32_t &c) {
+    if (in_smem) G = bins_below(cnt, 2 * b, sh);  // the bucket's position in bucket order picks its scratch region
     const Cands w = cands_global(J, G);
     c = compact(v, total, w, total, sh);
     return c ? sort_and_count(w, c, sh) : 0;
@@ -1237,12 +1188,12 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
     }
     __syncthreads();
     BktRound &I = J.meta[z.r];
-    const uint32_t K = z.K, nb = z.nb;
-    const uint32_t *offs = J.offs[iter & 1];
+    const uint32_t nb = z.nb;
+    const ListIn li = list_in(J, iter);
     Stage v;
     uint32_t S = 0;
     uint64_t G = 0;
-    const uint32_t total = gather(J, J.lst[iter & 1], offs, J.tile_base[iter & 1], K, nb, b, sh, smem, v, S, G);
+    const uint32_t total = gather(J, li, b, sh, smem, v, S, G);
     const bool in_smem = total <= kBStage;
     probe(ctl, iter, 3);
     // ---- entries whose key is in both tables: flagged, compacted, ranked, joined
@@ -1264,7 +1215,7 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
         if (small) {
             if (c) E = c <= kSmallRank ? rank_small(cands_smem(smem), c, sh) : sort_fine(cands_smem(smem), c, b, nb, smem, sh);
         } else {
-            E = big_count(J, v, total, in_smem, G, K, nb, b, offs, sh, c);
+            E = big_count(J, v, total, in_smem, G, b, li.cnt, sh, c);
         }
         if (threadIdx.x == 0 && c)
             atomicAdd(reinterpret_cast<unsigned long long *>(&I.cands), (unsigned long long)c);
@@ -1290,14 +1241,13 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
         BktRound &N = J.meta[z.r + 1];
         const uint32_t nb_next = z.nb_next;
         const StepArgs a = step_args(J, sh.tab, z.r + 1, false);
+        const ListOut lo = list_out(J, iter + 1);
         if (in_smem) {
-            write_next_smem(total, a, nb_next, b, J.lst[(iter + 1) & 1], J.offs[(iter + 1) & 1],
-                            J.tile_base[(iter + 1) & 1], N, sh, smem);
+            write_next_smem(total, a, nb_next, lo, N, sh, smem);
         } else {
             BScratch gs;
             scratch_layout(J.scratch, J.n_max, &gs);
-            write_next(J, v, total, false, a, nb_next, b, J.lst[(iter + 1) & 1], J.offs[(iter + 1) & 1],
-                       J.tile_base[(iter + 1) & 1], N, sh, smem, gs, G);
+            write_next(J, v, total, false, a, nb_next, lo, N, sh, smem, gs, G);
         }
     }
     probe(ctl, iter, 8);
@@ -1452,14 +1402,7 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
 
 size_t bkt_scratch_bytes(uint64_t n_max) { return scratch_layout(nullptr, n_max < 1 ? 1 : n_max, nullptr); }
 
-uint64_t bkt_max_tiles(uint64_t n_max, uint32_t G) {
-    const uint64_t a = bkt_tiles(n_max < 1 ? 1 : n_max), b = bkt_count(n_max, G);
-    return a > b ? a : b;
-}
 
-size_t bkt_offs_words(uint64_t n_max, uint32_t G) {
-    return (size_t)bkt_max_tiles(n_max, G) * (2 * bkt_count(n_max, G) + 1);
-}
 
 int bucket_grid_size() {
     int dev = 0, sms = 0, coop = 0, occ = 0;

@@ -293,9 +293,16 @@ struct BktJob {
     const uint32_t *lv_in;
     const uint8_t *used_s, *used_p;  // marks of rounds run before the launch
     uint64_t n_in;           // entries of that list
-    BktEntry *lst[2];        // the current and the next round's list, n_max entries each
-    uint32_t *offs[2];       // per tile: 2 nb + 1 bin starts
-    uint64_t *tile_base[2];  // per tile: its first entry in lst
+    // The current and the next round's list: one region of `cap` entries per
+    // (bucket, table) bin, bin = 2 bucket + table, filled through the round's
+    // bin counters; entries past a region's capacity go to the list's spill
+    // area with their bin as tag.
+    BktEntry *lst[2];        // nb_max * 2 * cap entries each
+    uint32_t *cnt;           // [iteration][2 nb_max]: entries reserved in each bin (zeroed at the start)
+    BktEntry *spill[2];      // n_max entries each
+    uint32_t *spill_tag[2];  // their bins
+    uint32_t *spill_n;       // [iteration]: spilled entries (zeroed at the start)
+    uint32_t cap;            // region capacity (entries)
     const uint32_t *seq2;    // read-major 2-bit bases, wpr words per read
     int32_t wpr, L, rounds, r0;
     const HashTables *tables;
@@ -317,8 +324,7 @@ struct BktJob {
     BktRound *meta;          // [rounds + 1], zeroed; round r at meta[r]
 };
 size_t bkt_scratch_bytes(uint64_t n_max);
-size_t bkt_offs_words(uint64_t n_max, uint32_t G);  // u32 words of one BktJob::offs buffer
-uint64_t bkt_max_tiles(uint64_t n_max, uint32_t G); // entries of one BktJob::tile_base buffer
+constexpr uint32_t kBktRegionCap = 4096;  // entries per (bucket, table) region: 12 sigma above the mean of 3350
 int bucket_grid_size();                             // 0: no cooperative launch on this device
 cudaError_t launch_bucket_rounds(BktJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
 

@@ -68,12 +68,18 @@ def test_full_size_workload_matches_reference(engine, name):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["tiny", "sub_errors", "dups_palindromes", "split_r128k", "read_len_1"])
 @pytest.mark.parametrize("mode", ["sync_rounds", "graph_rounds", "coop_rounds", "edge_restart", "graph_edge_restart",
-                                  "coop_edge_restart"])
+                                  "coop_edge_restart", "region_spill", "region_spill_some"])
 def test_round_paths_agree(engine, monkeypatch, name, mode):
     """Every round driver gives the reference's bytes: host-synchronised
     rounds (full sort per round), the per-round graph pipeline, the Bloom-
     filter cooperative kernel, and each device-resident driver restarted
-    after an edge-buffer overflow (the default driver is the bucket kernel)."""
+    after an edge-buffer overflow (the default driver is the bucket kernel);
+    and the bucket kernel with list regions so small that most (or some)
+    entries go to the spill area."""
+    if mode == "region_spill":
+        monkeypatch.setenv("EMP_BKT_REGION_CAP", "7")
+    if mode == "region_spill_some":
+        monkeypatch.setenv("EMP_BKT_REGION_CAP", "40")
     if mode == "sync_rounds":
         monkeypatch.setenv("EMP_SYNC_ROUNDS", "1")
     if mode.startswith("graph"):
