@@ -913,7 +913,6 @@ EMP_COLD void write_next_smem(uint32_t total, const StepArgs a, uint32_t nb, con
     const uint8_t *flag = smem + kOffFlag;
     uint8_t *reg = smem + kOffReg;
     uint32_t *hist = reinterpret_cast<uint32_t *>(reg + kPHist);
-    uint16_t *inv = reinterpret_cast<uint16_t *>(reg + kPInv);
     uint16_t *rank16 = reinterpret_cast<uint16_t *>(reg + kPRank);
     uint16_t *bin16 = reinterpret_cast<uint16_t *>(reg + kPBin);
     const uint32_t nbin = 2 * nb;
@@ -960,16 +959,14 @@ EMP_COLD void write_next_smem(uint32_t total, const StepArgs a, uint32_t nb, con
         if (kept) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.n), (unsigned long long)kept);
         if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.s), (unsigned long long)sh.sfx);
     }
-    for (uint32_t x = threadIdx.x; x < total; x += kT)  // the kept entries in bin order
-        if (!(flag[x] & kUsed)) inv[hist[bin16[x]] + rank16[x]] = (uint16_t)x;
-    __syncthreads();
     sprobe(sh, 14);
-    reserve_bins(hist, nbin, kept, lo.cnt, false);
+    reserve_bins(hist, nbin, kept, lo.cnt, true);  // hist[bin] = the bin's global position
     sprobe(sh, 15);
-    for (uint32_t d = threadIdx.x; d < kept; d += kT) {  // each bin a contiguous run of its region
-        const uint32_t x = inv[d], bin = bin16[x];
+    for (uint32_t x = threadIdx.x; x < total; x += kT) {  // each entry at its bin's position + its rank
+        if (flag[x] & kUsed) continue;
+        const uint32_t bin = bin16[x];
         const uint64_t k = key[x];
-        put_list(lo, bin, d + hist[bin], make_uint4((uint32_t)k, (uint32_t)(k >> 32), val[x], word[x]));
+        put_list(lo, bin, hist[bin] + rank16[x], make_uint4((uint32_t)k, (uint32_t)(k >> 32), val[x], word[x]));
     }
     __syncthreads();
 }
