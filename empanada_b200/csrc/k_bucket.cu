@@ -390,6 +390,14 @@ EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
 }
 
 // ---------------------------------------------------------------- gather
+// global -> shared copy of 4 or 8 bytes that completes asynchronously
+// (cp.async; cp.async.wait_all waits for this thread's copies)
+EMP_DEV void cp_async(void *dst_smem, const void *src, int bytes) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_smem);
+    if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
 EMP_DEV void put_entry(const Stage &v, uint32_t d, const uint4 *src) {
     const uint4 q = __ldcg(src);
     v.key[d] = (uint64_t)q.x | ((uint64_t)q.y << 32);
@@ -471,25 +479,16 @@ EMP_COLD uint32_t gather(const BktJob &J, const ListIn li, uint32_t b, BShared &
         v.flag = smem + kOffFlag;
         const uint64_t rs = (uint64_t)(2 * b) * li.cap, rp = (uint64_t)(2 * b + 1) * li.cap;
         sprobe(sh, 12);
-        constexpr int U = 8;
-        for (uint32_t x0 = 0; x0 < total; x0 += U * kT) {
-            uint4 e[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t x = x0 + u * kT + threadIdx.x;
-                if (x < total) e[u] = __ldcg(li.lst + (x < cS ? rs + x : rp + (x - cS)));
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t x = x0 + u * kT + threadIdx.x;
-                if (x < total) {
-                    v.key[x] = (uint64_t)e[u].x | ((uint64_t)e[u].y << 32);
-                    v.val[x] = e[u].z;
-                    v.word[x] = e[u].w;
-                    v.flag[x] = 0;
-                }
-            }
+        // asynchronous copies straight into the staged arrays (every entry's
+        // copies in flight at once, no registers): key 8 bytes, value 4, word 4
+        for (uint32_t x = threadIdx.x; x < total; x += kT) {
+            const uint4 *e = li.lst + (x < cS ? rs + x : rp + (x - cS));
+            cp_async(v.key + x, e, 8);
+            cp_async(v.val + x, reinterpret_cast<const uint8_t *>(e) + 8, 4);
+            cp_async(v.word + x, reinterpret_cast<const uint8_t *>(e) + 12, 4);
+            v.flag[x] = 0;
         }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
         __syncthreads();
         return total;
     }
