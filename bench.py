@@ -376,7 +376,6 @@ def served_bench(args):
     import empanada_b200
     from empanada_b200 import synth
 
-    rng = np.random.default_rng(5)
     pool = synth.batched_sets(n_sets=args.serve_pool, seed=6, genome_max=args.batch_genome_max)
     heavy = [synth.Workload(f"heavy{k}: 50 Mbp genome at 30x, {L} bp", seed=7_000 + k, genome_len=50_000_000,
                             n_reads=50_000_000 * 30 // L, read_len=L, sub_rate=0.001, min_ovlp=31)
@@ -410,6 +409,8 @@ def served_bench(args):
         return free_jobs.pop() if free_jobs else eng.job(min_ovlp=31)
 
     def stream(lam, n):
+        # seeded by the rate alone: both arms (and a re-run) see the same arrivals
+        rng = np.random.default_rng([5, int(round(lam * 1000))])
         t = np.cumsum(rng.exponential(1.0 / lam, size=n))
         kinds = np.where(rng.random(n) < 0.02, len(pool) + rng.integers(0, len(heavy), n),
                          rng.integers(0, len(pool), n))
@@ -431,6 +432,7 @@ def served_bench(args):
         nxt = done = 0
         t_feed = t_step = t_out = 0.0
         steps = 0
+        dev_ms = dict.fromkeys(("ms_map", "ms_dedup", "ms_rounds", "ms_round_kernel", "ms_total"), 0.0)
         start = time.perf_counter()
         while done < n:
             now = time.perf_counter() - start
@@ -472,6 +474,9 @@ def served_bench(args):
             for j, i, k in fin:
                 nbytes = j.output_into(out_host) if j.status() == 0 else -1
                 lat[i] = time.perf_counter() - start - t_arr[i]
+                js = j.stats()
+                for f in dev_ms:
+                    dev_ms[f] += js[f]
                 ok = ok and nbytes >= 0 and zlib.crc32(out_host[:nbytes]) == digests[k]
                 reads += sets[k].n_reads
                 j.trim()
@@ -483,9 +488,10 @@ def served_bench(args):
         if srv:
             sst = srv.stats()
             srv.close()
-        return {"jobs": n, "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+        return {"jobs": n, "heavy_jobs": int((kinds >= len(pool)).sum()), "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "reads_per_s": reads / span, "seconds": span, "outputs_identical": bool(ok),
                 "host_s": {"feed": t_feed, "run_or_step": t_step, "output": t_out, "steps": steps},
+                "job_device_ms": dev_ms,
                 "server": sst}
 
     rates = [float(x) for x in args.serve_rates.split(",")]

@@ -271,7 +271,7 @@ class Server:
     from submit() until a step returns it."""
 
     def __init__(self, engine: Engine, rounds_per_launch: int = 16, max_jobs: int = 256,
-                 hbm_budget_bytes: int = 0, rounds_per_launch_idle: int = 256):
+                 hbm_budget_bytes: int = 0, rounds_per_launch_idle: int = 64):
         self.engine = engine
         self._lib = engine._lib
         p = _native.ServerParams(int(rounds_per_launch), int(max_jobs), int(hbm_budget_bytes),

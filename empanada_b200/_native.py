@@ -64,6 +64,9 @@ class ServerStats(ctypes.Structure):
         ("ms_map", ctypes.c_double),
         ("ms_alone", ctypes.c_double),
         ("alone", ctypes.c_uint64),
+        ("ms_wait", ctypes.c_double),
+        ("ms_results", ctypes.c_double),
+        ("ms_launch", ctypes.c_double),
     ]
 
 

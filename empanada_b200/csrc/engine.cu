@@ -1526,6 +1526,7 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
     emp_ctx *ctx = srv->ctx;
     emp_server_stats &ss = srv->st;
     ss.steps += 1;
+    const auto ts = std::chrono::steady_clock::now();
     const uint64_t budget = srv->p.hbm_budget_bytes ? srv->p.hbm_budget_bytes : ctx->budget;
     std::vector<emp_job *> adm;
     while (!srv->queue.empty() && (int)(srv->live.size() + adm.size()) < srv->p.max_jobs) {
@@ -1565,6 +1566,7 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         EMP_CUDA(cudaMemcpyAsync(hj, srv->d_jobs.p, nb * sizeof(BktJob), cudaMemcpyDeviceToHost, s));
         EMP_CUDA(cudaMemcpyAsync(hc, srv->d_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
     }
+    ss.ms_launch += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ts).count();
     // ---- the admitted jobs' map phase
     std::vector<emp_job *> joining;
     if (!adm.empty()) {
@@ -1576,10 +1578,13 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         ss.ms_map += std::chrono::duration<double, std::milli>(t1 - t0).count();
         std::vector<emp_job *> close;
         std::vector<emp_status> crc;
+        // a lone job in an idle server (nothing in flight, nothing queued)
+        // runs alone, as emp_job_run runs it: one launch for all its rounds
+        const bool solo = nb == 0 && n == 1 && srv->queue.empty();
         for (int i = 0; i < n; ++i) {
             emp_job *j = adm[i];
             JobPrep &q = j->prep;
-            if (rc[i] == EMP_OK && !q.done && batch_eligible(j)) {
+            if (rc[i] == EMP_OK && !q.done && batch_eligible(j) && !solo) {
                 rc[i] = rounds_prelude(j, s);
                 if (rc[i] == EMP_OK) rc[i] = bucket_prepare(j, s, job_env(j), 0, 0, 2 * q.U, q.ecap, 1u, &j->bk);
                 if (rc[i] == EMP_OK) {
@@ -1588,7 +1593,7 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
                 }
             } else if (rc[i] == EMP_OK && !q.done) {
                 const auto ta = std::chrono::steady_clock::now();
-                rc[i] = job_rounds(j, s);  // too large for the batch, or rounds that split: alone
+                rc[i] = job_rounds(j, s);  // too large for the batch, rounds that split, or solo: alone
                 ss.alone += 1;
                 ss.ms_alone += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
             }
@@ -1607,7 +1612,15 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         return EMP_OK;
     }
     // ---- the launch's results
+    const auto tw = std::chrono::steady_clock::now();
     EMP_CUDA(cudaStreamSynchronize(s));
+    const auto tr = std::chrono::steady_clock::now();
+    ss.ms_wait += std::chrono::duration<double, std::milli>(tr - tw).count();
+    struct ResultClock {
+        double &acc;
+        std::chrono::steady_clock::time_point t;
+        ~ResultClock() { acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count(); }
+    } result_clock{ss.ms_results, tr};
     const bool timed_out = (hc->err & kErrSpin) != 0;
     const float ms = ms_between(srv->ev[0], srv->ev[1]);
     ss.launches += 1;
@@ -2072,7 +2085,7 @@ emp_status emp_server_params_default(emp_server_params *p) {
     p->rounds_per_launch = 16;
     p->max_jobs = 256;
     p->hbm_budget_bytes = 0;
-    p->rounds_per_launch_idle = 256;
+    p->rounds_per_launch_idle = 64;
     return EMP_OK;
 }
 
@@ -2088,6 +2101,18 @@ emp_status emp_server_create(emp_ctx *ctx, const emp_server_params *p, emp_serve
     if (!srv) return EMP_E_NOMEM;
     srv->ctx = ctx;
     srv->p = q;
+    // launch descriptors for max_jobs up front: growing them later would free
+    // pinned memory, which waits for the device, in the middle of a step
+    cudaSetDevice(ctx->device);
+    const size_t desc = (size_t)q.max_jobs * sizeof(BktJob);
+    emp_status st = srv->h_jobs.ensure(desc + sizeof(CoopCtl)) ? EMP_OK : EMP_E_NOMEM;
+    if (st == EMP_OK) st = ctx_ensure(ctx, srv->d_jobs, desc, ctx->stream);
+    if (st == EMP_OK) st = ctx_ensure(ctx, srv->d_ctl, sizeof(CoopCtl), ctx->stream);
+    if (st != EMP_OK) {
+        ctx->in_use -= srv->d_jobs.bytes + srv->d_ctl.bytes;
+        delete srv;
+        return st;
+    }
     *out = srv;
     return EMP_OK;
 }

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define EMP_ABI_VERSION 3
+#define EMP_ABI_VERSION 4
 
 typedef int emp_status;
 #define EMP_OK 0
@@ -158,14 +158,16 @@ emp_status emp_job_status(emp_job *job);
  * batch, and runs one bucket-kernel launch of at most rounds_per_launch
  * rounds of every job in the batch; jobs join and leave the batch between
  * launches.  A job too large for the batch, or whose rounds split into
- * several search partitions, runs alone within the step.  Every job's output
+ * several search partitions, runs alone within the step, and so does a job
+ * admitted alone into an idle server (no job in flight or queued), as
+ * emp_job_run runs it.  Every job's output
  * equals its emp_job_run output.  A job held by a server (submitted, not yet
  * handed out by a step) accepts no other call. */
 typedef struct emp_server_params {
     int32_t rounds_per_launch; /* bucket-kernel rounds per launch (default 16) */
     int32_t max_jobs;          /* jobs in the batch at most, <= 1024 (default 256) */
     uint64_t hbm_budget_bytes; /* admission budget (0: the context's, or none) */
-    int32_t rounds_per_launch_idle; /* the same while no job waits to join (default 256) */
+    int32_t rounds_per_launch_idle; /* the same while no job waits to join (default 64) */
 } emp_server_params;
 emp_status emp_server_params_default(emp_server_params *p);
 emp_status emp_server_create(emp_ctx *ctx, const emp_server_params *p, emp_server **out);
@@ -187,6 +189,9 @@ typedef struct emp_server_stats {
     double ms_map;       /* of which the map phase */
     double ms_alone;     /* of which jobs run alone */
     uint64_t alone;      /* jobs run alone */
+    double ms_wait;      /* host wall time waiting for the launch once admission is done */
+    double ms_results;   /* host wall time of launch results: copies back, completed jobs closed */
+    double ms_launch;    /* host wall time from the step's start to the launch queued */
 } emp_server_stats;
 emp_status emp_server_get_stats(emp_server *srv, emp_server_stats *st);
 

@@ -33,7 +33,7 @@ def test_header_declarations_are_exported():
 
 def test_abi_version_and_status_strings():
     lib = _native.lib()
-    assert lib.emp_abi_version() == 3
+    assert lib.emp_abi_version() == 4
     for code in range(0, -10, -1):
         assert lib.emp_status_string(code)
     assert _native.status_string(_native.EMP_E_FORMAT).startswith("reads of unequal length")
@@ -122,7 +122,7 @@ def test_server_and_batch_arguments_without_a_gpu():
     lib = _native.lib()
     p = _native.ServerParams()
     assert lib.emp_server_params_default(ctypes.byref(p)) == 0
-    assert (p.rounds_per_launch, p.max_jobs, p.hbm_budget_bytes, p.rounds_per_launch_idle) == (16, 256, 0, 256)
+    assert (p.rounds_per_launch, p.max_jobs, p.hbm_budget_bytes, p.rounds_per_launch_idle) == (16, 256, 0, 64)
     out = ctypes.c_void_p()
     assert lib.emp_server_create(None, ctypes.byref(p), ctypes.byref(out)) == _native.EMP_E_INVAL
     assert lib.emp_server_submit(None, None) == _native.EMP_E_INVAL

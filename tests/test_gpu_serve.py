@@ -58,15 +58,43 @@ def test_served_golden_cases_staggered(engine, rounds_per_launch):
 @pytest.mark.gpu
 def test_served_idle_launches_run_longer(engine):
     """With no job waiting, a launch runs up to rounds_per_launch_idle rounds:
-    a lone job needs fewer launches, and its bytes do not change."""
-    j = _job(engine, "sub_errors")
+    two jobs admitted together need one launch, and their bytes do not change."""
+    names = ("sub_errors", "odd_len")
+    jobs = [_job(engine, n) for n in names]
     with empanada_b200.Server(engine, rounds_per_launch=2, rounds_per_launch_idle=1000) as srv:
-        srv.submit(j)
+        for j in jobs:
+            srv.submit(j)
         _drain(srv)
         st = srv.stats()
-    assert st["launches"] <= 2
-    assert hashlib.sha256(j.output()).hexdigest() == GOLDEN["sub_errors"]["sha256"]
-    j.close()
+    assert st["launches"] == 1 and st["batch_jobs"] == 2 and st["alone"] == 0
+    for n, j in zip(names, jobs):
+        assert hashlib.sha256(j.output()).hexdigest() == GOLDEN[n]["sha256"], n
+        j.close()
+
+
+@pytest.mark.gpu
+def test_served_lone_job_in_idle_server_runs_alone(engine):
+    """A job admitted alone into an idle server runs as emp_job_run runs it
+    (no batched launch); a job admitted while another is in flight joins the
+    batch."""
+    a, b = _job(engine, "sub_errors"), _job(engine, "odd_len")
+    with empanada_b200.Server(engine, rounds_per_launch=1, rounds_per_launch_idle=1) as srv:
+        srv.submit(a)
+        done = srv.step()
+        st = srv.stats()
+        assert done == [a] and st["alone"] == 1 and st["launches"] == 0
+        a2 = _job(engine, "sub_errors")
+        srv.submit(a2)
+        srv.submit(b)
+        srv.step()  # both admitted together: they join the batch
+        done = _drain(srv)
+        st = srv.stats()
+    assert sorted(j.handle.value for j in done) == sorted((a2.handle.value, b.handle.value))
+    assert st["alone"] == 1 and st["launches"] >= 1
+    for n, j in (("sub_errors", a), ("sub_errors", a2), ("odd_len", b)):
+        assert j.status() == 0
+        assert hashlib.sha256(j.output()).hexdigest() == GOLDEN[n]["sha256"], n
+        j.close()
 
 
 @pytest.mark.gpu
