@@ -1192,6 +1192,17 @@ emp_status map_records(emp_job *j, cudaStream_t s) {
     return EMP_OK;
 }
 
+// Whether a round of a job of n reads may run outside the bucket kernel (the
+// host-synchronised rounds, the pipeline and the per-round cooperative
+// kernel read bases from the column store; the bucket kernel from seq2).
+// Each table holds at most 2n entries and the list at most 4n, so with
+// 2n < M/2 and 4n within the bucket kernel's list limit every round runs
+// there.
+bool columns_needed(uint64_t n, uint64_t M) {
+    const bool bucket = !std::getenv("EMP_NO_COOP") && !std::getenv("EMP_NO_BUCKET") && bucket_grid_size() > 0;
+    return std::getenv("EMP_SYNC_ROUNDS") || !bucket || 2 * n >= M / 2 || 4 * n > kBktMaxEntries;
+}
+
 emp_status map_keys(emp_job *j, cudaStream_t s) {
     EMP_TRY(map_check(j));
     JobPrep &q = j->prep;
@@ -1224,12 +1235,14 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
     q.wpc = (n + 15) / 16;
     q.wpr = (L + 15) / 16;
     EMP_TRY(ensure(j, j->rec_of, n * 4));
-    EMP_TRY(ensure(j, j->cols, (uint64_t)L * q.wpc * 4));
+    const bool want_cols = columns_needed(n, q.M);
+    if (want_cols) EMP_TRY(ensure(j, j->cols, (uint64_t)L * q.wpc * 4));
     EMP_TRY(ensure(j, j->seq2, (uint64_t)n * q.wpr * 4));
     EMP_TRY(ensure(j, j->keys0, n2 * 8));
     launch_scatter_hq(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), q.n_rec, j->rec_of.as<uint32_t>(), s);
     launch_fingerprint_pack(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->rec_of.as<uint32_t>(), n, L, tables,
-                            j->keys0.as<uint64_t>(), j->cols.as<uint32_t>(), q.wpc, j->seq2.as<uint32_t>(), q.wpr, s);
+                            j->keys0.as<uint64_t>(), want_cols ? j->cols.as<uint32_t>() : nullptr, q.wpc,
+                            j->seq2.as<uint32_t>(), q.wpr, s);
     j->n_ends = n2;
     cudaEventRecord(j->map_ev[1], s);
     // ---- fingerprint sort + duplicate removal (overlap.cu:212-225)

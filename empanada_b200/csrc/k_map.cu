@@ -362,11 +362,14 @@ __global__ void __launch_bounds__(256) fingerprint_pack_kernel(const uint8_t *__
             *reinterpret_cast<ulonglong2 *>(keys + 2 * i) = kv;
         }
         if (live && act && seq2) seq2[i * wpr + j] = word;
+        if (cols) {
 #pragma unroll
-        for (int t = 0; t < 16; ++t) colw[t] |= ((word >> (2 * t)) & 3u) << (2 * m);
+            for (int t = 0; t < 16; ++t) colw[t] |= ((word >> (2 * t)) & 3u) << (2 * m);
+        }
 #pragma unroll
         for (int k = 0; k < 4; ++k) w[k] = wn[k];
     }
+    if (!cols) return;  // no column store wanted (every round runs in the bucket kernel)
     if (TWO) {  // the half-warps hold the even and odd reads' bits
 #pragma unroll
         for (int t = 0; t < 16; ++t) colw[t] |= __shfl_xor_sync(0xffffffffu, colw[t], 16);
