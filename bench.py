@@ -45,6 +45,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "reads/s (fingerprint+sort+overlap) on 1 B200; served-mix p50/p99 latency vs plain"
 CPU_SAMPLE_READS = 200_000
+CPU_SAMPLE_READS_1T = 50_000  # the one-thread run of the reference CPU build
 
 
 def env_rank():
@@ -171,9 +172,17 @@ def cpu_baseline_block(workload, steps: int = 1):
     with tempfile.TemporaryDirectory() as td:
         fq = os.path.join(td, "sample.fq")
         synth.write_fastq(sample, fq)
+        single = None
         if os.path.exists(bind.REF_CPU):
             times = [cpu_reference_run(fq, workload.cli_args(), threads, td)[0] for _ in range(steps)]
             kind, cores = "reference", threads
+            # the same build on one host thread (OMP_NUM_THREADS=1), a smaller sample
+            one = workload.scaled(min(CPU_SAMPLE_READS_1T, workload.n_reads))
+            fq1 = os.path.join(td, "sample1.fq")
+            synth.write_fastq(one, fq1)
+            t1 = cpu_reference_run(fq1, workload.cli_args(), 1, td)[0]
+            single = {"value": one.n_reads / t1, "unit": "reads/s", "cores": 1,
+                      "sample": f"first {one.n_reads} reads of the workload"}
         else:
             data = open(fq, "rb").read()
             times = []
@@ -186,7 +195,8 @@ def cpu_baseline_block(workload, steps: int = 1):
     return {"value": v, "unit": "reads/s", "cores": cores, "kind": kind,
             "sample": f"first {sample.n_reads} reads of the workload (same genome and error model), "
                       f"{'reference sources built with Thrust on OpenMP' if kind == 'reference' else 'oracle C port'}; "
-                      f"compute time = wall minus the reference's read_input; median of {len(times)}"}, times
+                      f"compute time = wall minus the reference's read_input; median of {len(times)}",
+            "single_thread": single}, times
 
 
 def run_reference_arm(args, workload):
