@@ -321,7 +321,10 @@ def batched_bench(args):
         batch_ms = timed(lambda: eng.run_batch(jobs, sptr), args.steps, args.warmup)
     clocks = clk.summary()
     outs = [j.output() for j in jobs]
-    launches = jobs[0].stats()["gpu_launches"]  # the first job's counter spans the whole batch
+    jst = [j.stats() for j in jobs]
+    launches = jst[0]["gpu_launches"]  # the first job's counter spans the whole batch
+    # the batched bucket-kernel launch of the last step (every job in the batch carries its time)
+    batch_kernel_ms = float(np.median([x["ms_round_kernel"] for x in jst]))
     plain_steps = max(1, min(args.steps, 3))
 
     def plain():
@@ -367,7 +370,7 @@ def batched_bench(args):
                        "l2": "inputs larger than L2; 256 MB L2 flush before every timed step"},
             "plain": {"value": reads / (tp / 1e3), "ms_per_step": tp, "steps": plain_steps,
                       "what": "the same sets job by job (emp_job_run each), device time"},
-            "batched_over_plain": tp / tb, "outputs_identical": same, "gpu_launches": launches,
+            "batched_over_plain": tp / tb, "batch_kernel_ms": batch_kernel_ms, "outputs_identical": same, "gpu_launches": launches,
             "e2e": {"value": reads * len(e2e_s) / sum(e2e_s), "unit": "reads/s",
                     "h2d_bytes_per_step": int(offs[-1]), "d2h_bytes_per_step": int(d2h)},
             "clocks": clocks, "host_generate_s": gen_s}
@@ -435,7 +438,8 @@ def served_bench(args):
         lat = np.zeros(n)
         ok = True
         reads = 0
-        srv = (empanada_b200.Server(eng, rounds_per_launch=args.serve_rounds, hbm_budget_bytes=args.serve_budget << 30)
+        srv = (empanada_b200.Server(eng, rounds_per_launch=args.serve_rounds, hbm_budget_bytes=args.serve_budget << 30,
+                                    batch_max_entries=args.serve_batch_max)
                if served else None)
         pending = collections.deque()
         held = {}
@@ -525,6 +529,7 @@ def served_bench(args):
                                    "250 bp), -o 31; jobs per rate: rate x "
                                    f"{args.serve_seconds} s within [{args.serve_min_jobs}, {args.serve_max_jobs}]",
                        "rounds_per_launch": args.serve_rounds, "admission_budget_gib": args.serve_budget,
+                       "batch_max_entries": args.serve_batch_max,
                        "rates_per_s": rates},
             "served": served, "plain": plain, "clocks": clocks, "host_generate_s": gen_s,
             "e2e": {"value": served[str(rates[-1])]["reads_per_s"], "unit": "reads/s",
@@ -552,6 +557,8 @@ def main():
     ap.add_argument("--serve-max-jobs", type=int, default=400)
     ap.add_argument("--serve-pool", type=int, default=48)
     ap.add_argument("--serve-rounds", type=int, default=16, help="bucket-kernel rounds per launch")
+    ap.add_argument("--serve-batch-max", type=int, default=0,
+                    help="served jobs with a longer first round list run alone (0: the bucket kernel's limit)")
     ap.add_argument("--serve-budget", type=int, default=100, help="admission budget of the server, GiB")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

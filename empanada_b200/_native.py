@@ -49,6 +49,7 @@ class ServerParams(ctypes.Structure):
         ("max_jobs", ctypes.c_int32),
         ("hbm_budget_bytes", ctypes.c_uint64),
         ("rounds_per_launch_idle", ctypes.c_int32),
+        ("batch_max_entries", ctypes.c_uint64),
     ]
 
 

@@ -1597,7 +1597,8 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         for (int i = 0; i < n; ++i) {
             emp_job *j = adm[i];
             JobPrep &q = j->prep;
-            if (rc[i] == EMP_OK && !q.done && batch_eligible(j) && !solo) {
+            const bool fits = !srv->p.batch_max_entries || 2 * q.U <= srv->p.batch_max_entries;
+            if (rc[i] == EMP_OK && !q.done && batch_eligible(j) && fits && !solo) {
                 rc[i] = rounds_prelude(j, s);
                 if (rc[i] == EMP_OK) rc[i] = bucket_prepare(j, s, job_env(j), 0, 0, 2 * q.U, q.ecap, 1u, &j->bk);
                 if (rc[i] == EMP_OK) {
@@ -2099,6 +2100,7 @@ emp_status emp_server_params_default(emp_server_params *p) {
     p->max_jobs = 256;
     p->hbm_budget_bytes = 0;
     p->rounds_per_launch_idle = 64;
+    p->batch_max_entries = 0;
     return EMP_OK;
 }
 

@@ -168,6 +168,7 @@ typedef struct emp_server_params {
     int32_t max_jobs;          /* jobs in the batch at most, <= 1024 (default 256) */
     uint64_t hbm_budget_bytes; /* admission budget (0: the context's, or none) */
     int32_t rounds_per_launch_idle; /* the same while no job waits to join (default 64) */
+    uint64_t batch_max_entries; /* a job whose first round list is longer runs alone (0: the bucket kernel's 16M) */
 } emp_server_params;
 emp_status emp_server_params_default(emp_server_params *p);
 emp_status emp_server_create(emp_ctx *ctx, const emp_server_params *p, emp_server **out);

@@ -122,7 +122,8 @@ def test_server_and_batch_arguments_without_a_gpu():
     lib = _native.lib()
     p = _native.ServerParams()
     assert lib.emp_server_params_default(ctypes.byref(p)) == 0
-    assert (p.rounds_per_launch, p.max_jobs, p.hbm_budget_bytes, p.rounds_per_launch_idle) == (16, 256, 0, 64)
+    assert (p.rounds_per_launch, p.max_jobs, p.hbm_budget_bytes, p.rounds_per_launch_idle,
+            p.batch_max_entries) == (16, 256, 0, 64, 0)
     out = ctypes.c_void_p()
     assert lib.emp_server_create(None, ctypes.byref(p), ctypes.byref(out)) == _native.EMP_E_INVAL
     assert lib.emp_server_submit(None, None) == _native.EMP_E_INVAL
