@@ -98,6 +98,24 @@ def test_served_lone_job_in_idle_server_runs_alone(engine):
 
 
 @pytest.mark.gpu
+def test_served_batch_max_entries_sends_jobs_alone(engine):
+    """With batch_max_entries below every job's list, jobs admitted together
+    all run alone (no batched launch) and give the reference's bytes."""
+    names = ("sub_errors", "odd_len", "tiny")
+    jobs = [_job(engine, n) for n in names]
+    with empanada_b200.Server(engine, batch_max_entries=1) as srv:
+        for j in jobs:
+            srv.submit(j)
+        _drain(srv)
+        st = srv.stats()
+    assert st["alone"] == len(names) and st["launches"] == 0
+    for n, j in zip(names, jobs):
+        assert j.status() == 0
+        assert hashlib.sha256(j.output()).hexdigest() == GOLDEN[n]["sha256"], n
+        j.close()
+
+
+@pytest.mark.gpu
 def test_served_mix_equals_alone(engine):
     """Mixed read sets (20-300 kbp genomes, 100-300 bp reads) submitted in
     waves: each output equals the job run alone."""
