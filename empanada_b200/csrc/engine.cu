@@ -118,6 +118,8 @@ struct HostSlab {
 
 }  // namespace
 
+constexpr int kMapStreams = 8;
+
 struct emp_ctx {
     int device = 0;
     uint64_t budget = 0;
@@ -138,6 +140,10 @@ struct emp_ctx {
     DevBuf batch_jobs, batch_ctl;
     PinnedBuf h_batch;
     cudaEvent_t batch_ev[2] = {};
+    // the map phase of a batch of jobs: jobs on kMapStreams streams, so that
+    // the small kernels of small read sets run side by side
+    cudaStream_t map_streams[kMapStreams] = {};
+    cudaEvent_t map_ev[kMapStreams + 1] = {};
 };
 
 struct JobPrep {
@@ -1427,26 +1433,55 @@ emp_status map_batch(emp_job **jobs, int n, std::vector<emp_status> &rc, cudaStr
     auto fail = [&](int i, emp_status e) {
         if (rc[i] == EMP_OK) rc[i] = e;
     };
-    for (int i = 0; i < n; ++i) {
-        fail(i, map_begin(jobs[i], s));
-        if (rc[i] == EMP_OK) fail(i, map_fetch(jobs[i], s));
+    // job i on stream i mod K (K = 1: s itself), every stream after s's work so far
+    emp_ctx *ctx = n ? jobs[0]->ctx : nullptr;
+    const int K = n > 1 ? std::min(n, kMapStreams) : 1;
+    std::vector<cudaStream_t> st((size_t)K, s);
+    if (K > 1) {
+        for (int k = 0; k <= kMapStreams; ++k)
+            if (!ctx->map_ev[k]) EMP_CUDA(cudaEventCreateWithFlags(&ctx->map_ev[k], cudaEventDisableTiming));
+        EMP_CUDA(cudaEventRecord(ctx->map_ev[kMapStreams], s));
+        for (int k = 0; k < K; ++k) {
+            if (!ctx->map_streams[k]) EMP_CUDA(cudaStreamCreateWithFlags(&ctx->map_streams[k], cudaStreamNonBlocking));
+            st[k] = ctx->map_streams[k];
+            EMP_CUDA(cudaStreamWaitEvent(st[k], ctx->map_ev[kMapStreams], 0));
+        }
     }
-    EMP_CUDA(cudaStreamSynchronize(s));
-    for (int i = 0; i < n; ++i) {
-        if (!live(i)) continue;
-        fail(i, map_records(jobs[i], s));
-        if (live(i)) fail(i, map_fetch(jobs[i], s));
+    auto sync_all = [&]() -> emp_status {
+        for (cudaStream_t q : st) EMP_CUDA(cudaStreamSynchronize(q));
+        return EMP_OK;
+    };
+    auto stages = [&]() -> emp_status {
+        for (int i = 0; i < n; ++i) {
+            fail(i, map_begin(jobs[i], st[i % K]));
+            if (rc[i] == EMP_OK) fail(i, map_fetch(jobs[i], st[i % K]));
+        }
+        EMP_TRY(sync_all());
+        for (int i = 0; i < n; ++i) {
+            if (!live(i)) continue;
+            fail(i, map_records(jobs[i], st[i % K]));
+            if (live(i)) fail(i, map_fetch(jobs[i], st[i % K]));
+        }
+        EMP_TRY(sync_all());
+        for (int i = 0; i < n; ++i) {
+            if (!live(i)) continue;
+            fail(i, map_keys(jobs[i], st[i % K]));
+            if (live(i)) fail(i, map_fetch(jobs[i], st[i % K]));
+        }
+        EMP_TRY(sync_all());
+        for (int i = 0; i < n; ++i)
+            if (live(i)) fail(i, map_list(jobs[i], st[i % K]));
+        return EMP_OK;
+    };
+    const emp_status e = stages();
+    if (K > 1) {  // the rest of the jobs' work (and any error path) is on s, after all of this
+        for (int k = 0; k < K; ++k) {
+            cudaEventRecord(ctx->map_ev[k], st[k]);
+            cudaStreamWaitEvent(s, ctx->map_ev[k], 0);
+        }
+        for (int i = 0; i < n; ++i) jobs[i]->stream = s;
     }
-    EMP_CUDA(cudaStreamSynchronize(s));
-    for (int i = 0; i < n; ++i) {
-        if (!live(i)) continue;
-        fail(i, map_keys(jobs[i], s));
-        if (live(i)) fail(i, map_fetch(jobs[i], s));
-    }
-    EMP_CUDA(cudaStreamSynchronize(s));
-    for (int i = 0; i < n; ++i)
-        if (live(i)) fail(i, map_list(jobs[i], s));
-    return EMP_OK;
+    return e;
 }
 
 // Close jobs[0..n) whose work is all queued: their last events, one
@@ -1808,6 +1843,14 @@ emp_status emp_ctx_destroy(emp_ctx *ctx) {
     ctx->in_use -= ctx->batch_jobs.bytes + ctx->batch_ctl.bytes;
     ctx->batch_jobs.release();
     ctx->batch_ctl.release();
+    for (int k = 0; k < kMapStreams; ++k) {
+        if (ctx->map_streams[k]) {
+            cudaStreamSynchronize(ctx->map_streams[k]);
+            cudaStreamDestroy(ctx->map_streams[k]);
+        }
+    }
+    for (auto &e : ctx->map_ev)
+        if (e) cudaEventDestroy(e);
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
     cudaStreamSynchronize(ctx->copy_stream);
