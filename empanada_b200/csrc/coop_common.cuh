@@ -28,25 +28,25 @@ EMP_DEV uint64_t globaltimer() {
 
 // Grid barrier (all CTAs co-resident: cooperative launch).  Bounded wait: on
 // timeout the error bit is raised and false returned; the kernel then exits.
-// *s_gen (shared, zero at kernel start, like the control block's counters)
-// holds the barriers this CTA has passed, so arriving costs one atomic and
-// waiting one poll loop; another CTA's timeout is seen while polling.
+// The arrival counter only grows (zero at launch, like the rest of the
+// control block): *s_gen (shared, zero at kernel start) holds the barriers
+// this CTA has passed, so barrier g is passed once the counter reaches
+// (g + 1) x grid.  Arriving costs one atomic and waiting one poll loop, with
+// no reset on the last arrival's path; another CTA's timeout is seen while
+// polling.
 EMP_DEV bool grid_barrier_raw(CoopCtl *ctl, uint32_t *s_flag, uint32_t *s_gen) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile uint32_t *gen = &ctl->bar_gen;
+        volatile uint32_t *count = &ctl->bar_count;
         const uint32_t g = *s_gen;
+        const uint32_t target = (g + 1) * gridDim.x;
         __threadfence();
-        const uint32_t arrived = atomicAdd(&ctl->bar_count, 1u);
+        const uint32_t arrived = atomicAdd(&ctl->bar_count, 1u) + 1;
         uint32_t ok = 1;
-        if (arrived == gridDim.x - 1) {
-            ctl->bar_count = 0;
-            __threadfence();
-            atomicAdd(&ctl->bar_gen, 1u);
-        } else {
+        if (arrived < target) {
             const uint64_t t0 = globaltimer();
             uint32_t polls = 0;
-            while (*gen == g) {
+            while (*count < target) {
                 if ((++polls & 255) == 0 &&
                     (globaltimer() - t0 > kBarrierTimeoutNs || (*(volatile uint32_t *)&ctl->err & kErrSpin))) {
                     atomicOr(&ctl->err, kErrSpin);

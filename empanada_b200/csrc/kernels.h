@@ -225,8 +225,8 @@ struct CoopCtl {
     uint32_t active;    // jobs not finished (the host sets njobs)
     uint32_t all_done;
     uint32_t any_lsd;
-    uint32_t bar_count;
-    uint32_t bar_gen;
+    uint32_t bar_count;  // grid-barrier arrivals since the launch
+    uint32_t bar_gen;    // unused
     uint32_t err;
     uint32_t pad;
     uint32_t ticket[16];
