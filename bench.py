@@ -565,6 +565,12 @@ def main():
     ap.add_argument("--serve-budget", type=int, default=100, help="admission budget of the server, GiB")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.impl == "reference" and args.workload in ("served", "batched"):
+        if env_rank()[0] == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference runs one read set per process and "
+                              "has no batched or served mode; bench.py --impl reference times its CPU build on "
+                              "the single-set workloads"}), flush=True)
+        return
     if args.workload == "served":
         served_bench(args)
         return
