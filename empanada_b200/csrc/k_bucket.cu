@@ -1400,9 +1400,10 @@ size_t bkt_scratch_bytes(uint64_t n_max) { return scratch_layout(nullptr, n_max 
 
 
 
-int bucket_grid_size() {
-    int dev = 0, sms = 0, coop = 0, occ = 0;
-    cudaGetDevice(&dev);
+// Found once per device (the first call on it sets the kernel's shared
+// memory attribute) and kept: the engine asks for every job.
+static int bucket_grid_size_find(int dev) {
+    int sms = 0, coop = 0, occ = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
     if (!coop) return 0;
@@ -1416,6 +1417,22 @@ int bucket_grid_size() {
         return 0;
     }
     return occ >= 1 ? sms : 0;  // one CTA per SM
+}
+
+int bucket_grid_size() {
+    constexpr int kDevs = 64;
+    static std::atomic<int> grid[kDevs] = {};  // grid + 1; 0: not found yet
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) {
+        cudaGetLastError();
+        return bucket_grid_size_find(dev);
+    }
+    int g = grid[dev].load(std::memory_order_relaxed);
+    if (g == 0) {
+        g = bucket_grid_size_find(dev) + 1;
+        grid[dev].store(g, std::memory_order_relaxed);
+    }
+    return g - 1;
 }
 
 cudaError_t launch_bucket_rounds(BktJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s) {

@@ -536,9 +536,10 @@ __global__ void __launch_bounds__(kT, 1) coop_rounds_kernel(CoopJob *jobs, CoopC
 
 size_t coop_smem_bytes() { return kCoopDynSmem; }
 
-int coop_grid_size() {
-    int dev = 0, sms = 0, coop = 0, occ = 0;
-    cudaGetDevice(&dev);
+// Found once per device (the first call on it sets the kernel's shared
+// memory attribute) and kept: the engine asks for every job.
+static int coop_grid_size_find(int dev) {
+    int sms = 0, coop = 0, occ = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
     if (!coop) return 0;
@@ -552,6 +553,22 @@ int coop_grid_size() {
         return 0;
     }
     return occ >= 1 ? sms : 0;  // one CTA per SM
+}
+
+int coop_grid_size() {
+    constexpr int kDevs = 64;
+    static std::atomic<int> grid[kDevs] = {};  // grid + 1; 0: not found yet
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) {
+        cudaGetLastError();
+        return coop_grid_size_find(dev);
+    }
+    int g = grid[dev].load(std::memory_order_relaxed);
+    if (g == 0) {
+        g = coop_grid_size_find(dev) + 1;
+        grid[dev].store(g, std::memory_order_relaxed);
+    }
+    return g - 1;
 }
 
 cudaError_t launch_coop_rounds(CoopJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s) {
