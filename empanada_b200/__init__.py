@@ -17,6 +17,7 @@ Every entry point calls the CUDA path; there is no CPU fallback.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import dataclasses
 import struct
@@ -31,7 +32,7 @@ __all__ = ["Config", "parse_args", "parse_size", "Engine", "Job", "run_bytes", "
            "EmpError", "UsageExit"]
 
 DEFAULTS = {"o": "31", "m": "1g", "r": "1g", "b": "32m", "c": "64m"}
-_OPTIONS = [  # (shortname, longname, description, default) as in config.h:282-290
+_OPTIONS = [  # (shortname, longname, description, default) as in config.h:120-140
     ("o", "min-overlap", "minimum overlap length", "31"),
     ("m", "map-mem", "device memory during the fingerprint generation phase", "1g"),
     ("r", "reduce-mem", "device memory during the overlap-detection phase", "1g"),
@@ -161,6 +162,33 @@ class Engine:
     def sort_pairs(self, keys_ptr: int, vals_ptr: int, n: int, stream: int = 0) -> None:
         """Stable device sort of (u64 fingerprint, u32 value) pairs in place."""
         check(self._lib.emp_sort_pairs(self.handle, keys_ptr, vals_ptr, n, stream or None), "emp_sort_pairs")
+
+    def tuning(self) -> dict:
+        """The context's engine choices (emp_ctx_get_tuning), defaults filled in."""
+        t = _native.Tuning()
+        check(self._lib.emp_ctx_get_tuning(self.handle, ctypes.byref(t)), "emp_ctx_get_tuning")
+        return t.to_dict()
+
+    def set_tuning(self, **choices) -> None:
+        """Change some engine choices (emp_ctx_set_tuning); the others keep
+        their current values.  Every choice gives the same output.bin."""
+        t = _native.Tuning()
+        check(self._lib.emp_ctx_get_tuning(self.handle, ctypes.byref(t)), "emp_ctx_get_tuning")
+        for k, v in choices.items():
+            if k not in t.to_dict():
+                raise KeyError(f"unknown tuning field {k!r}")
+            setattr(t, k, int(v))
+        check(self._lib.emp_ctx_set_tuning(self.handle, ctypes.byref(t)), "emp_ctx_set_tuning")
+
+    @contextlib.contextmanager
+    def tuned(self, **choices):
+        """set_tuning for the duration of a with-block, then the previous choices."""
+        before = self.tuning()
+        self.set_tuning(**choices)
+        try:
+            yield self
+        finally:
+            self.set_tuning(**before)
 
 
 class Job:

@@ -38,6 +38,22 @@ class Params(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("round_driver", ctypes.c_int32),
+        ("bucket_mean", ctypes.c_uint32),
+        ("region_cap", ctypes.c_uint32),
+        ("reserved0", ctypes.c_uint32),
+        ("edge_cap", ctypes.c_uint64),
+        ("wait_limit_ns", ctypes.c_uint64),
+        ("block_next_wait", ctypes.c_int32),
+        ("reserved1", ctypes.c_int32),
+    ]
+
+    def to_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("reserved")}
+
+
 # int (*emp_edge_sink)(void *user, int32_t ovlp_len, uint64_t n, const uint32_t *from, const uint32_t *to)
 EDGE_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint64,
                              ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32))
@@ -116,6 +132,9 @@ SIGNATURES = {
     "emp_parse_size": (ctypes.c_int, [ctypes.c_char_p, _u64p]),
     "emp_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(_vp)]),
     "emp_ctx_destroy": (ctypes.c_int, [_vp]),
+    "emp_tuning_default": (ctypes.c_int, [ctypes.POINTER(Tuning)]),
+    "emp_ctx_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
+    "emp_ctx_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
     "emp_job_create": (ctypes.c_int, [_vp, ctypes.POINTER(Params), ctypes.POINTER(_vp)]),
     "emp_job_destroy": (ctypes.c_int, [_vp]),
     "emp_job_feed_fastq": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int]),

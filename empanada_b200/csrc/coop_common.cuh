@@ -1,5 +1,5 @@
 // coop_common.cuh -- pieces shared by the cooperative persistent round
-// kernels (k_coop.cu, k_bucket.cu): 512-thread CTAs, one per SM, all
+// kernel (k_bucket.cu): 512-thread CTAs, one per SM, all
 // co-resident (cooperative launch), bounded grid barriers, tile tickets over
 // the tiles of many jobs, chunk-major tile scans.
 #pragma once
@@ -10,7 +10,6 @@ namespace emp {
 
 constexpr int kT = kBlkThreads;         // 512
 constexpr int kC = kCoopTile / kT;      // 8 entries per thread per 4096-entry chunk
-constexpr uint64_t kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;
 
 // L1 is not coherent across SMs: everything another CTA of this launch may
 // have written (job state, lists, candidates, used marks) is read around L1,
@@ -39,7 +38,8 @@ EMP_DEV bool grid_barrier_raw(CoopCtl *ctl, uint32_t *s_flag, uint32_t *s_gen) {
     if (threadIdx.x == 0) {
         volatile uint32_t *count = &ctl->bar_count;
         const uint32_t g = *s_gen;
-        const uint32_t target = (g + 1) * gridDim.x;
+        const uint32_t target = (g + 1) * gridDim.x + ctl->bar_extra;
+        const uint64_t limit = ctl->wait_ns ? ctl->wait_ns : kBarrierTimeoutNs;
         __threadfence();
         const uint32_t arrived = atomicAdd(&ctl->bar_count, 1u) + 1;
         uint32_t ok = 1;
@@ -48,7 +48,7 @@ EMP_DEV bool grid_barrier_raw(CoopCtl *ctl, uint32_t *s_flag, uint32_t *s_gen) {
             uint32_t polls = 0;
             while (*count < target) {
                 if ((++polls & 255) == 0 &&
-                    (globaltimer() - t0 > kBarrierTimeoutNs || (*(volatile uint32_t *)&ctl->err & kErrSpin))) {
+                    (globaltimer() - t0 > limit || (*(volatile uint32_t *)&ctl->err & kErrSpin))) {
                     atomicOr(&ctl->err, kErrSpin);
                     ok = 0;
                     break;

@@ -13,11 +13,14 @@
 #include <cerrno>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <mutex>
 #include <string>
 #include <vector>
+
+#include <sys/stat.h>
 
 #include "../../include/empanada.h"
 #include "kernels.h"
@@ -144,6 +147,11 @@ struct emp_ctx {
     // the small kernels of small read sets run side by side
     cudaStream_t map_streams[kMapStreams] = {};
     cudaEvent_t map_ev[kMapStreams + 1] = {};
+    emp_tuning tune{};  // engine choices (zero fields: defaults)
+    // profiling aids, read from the environment when the context is made:
+    // EMP_COOP_TRACE=<file> (per-round durations of the bucket kernel),
+    // EMP_COOP_PROBE=<file>[:iteration] (per-CTA stamps of one iteration)
+    std::string trace_path, probe_spec;
 };
 
 struct JobPrep {
@@ -166,14 +174,12 @@ struct emp_job {
     DevBuf akeys, apos, bkeys, parts;  // record splitting
     DevBuf xk0, xv0, xk1, xv1, ring_k, ring_v, cparts;  // sort of a table larger than M
     PinnedBuf h_parts;
-    // device-resident round pipeline
-    DevBuf lk_init, lv_init, bloom_s, bloom_p, ck, cv, ck2, cv2, records, st_upd, st_cand, st_scan, ctl;
-    PinnedBuf h_ctl, h_records;
+    // the initial list (kept for a rerun with a larger edge buffer), round records
+    DevBuf lk_init, lv_init, records;
+    PinnedBuf h_records;
     uint64_t ecap_hint = 0;
     uint64_t sorts_since_clear = 0;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-    DevBuf st_join, st_sort, coop_job, coop_ctl, coop_trace, coop_probe;  // cooperative all-rounds kernel
+    DevBuf coop_ctl, coop_trace, coop_probe;  // bucket kernel: control block, profiling stamps
     DevBuf dout;                 // output.bin records written on the device (after those in `out`)
     uint64_t dout_bytes = 0;
     PinnedBuf h_out;
@@ -544,88 +550,6 @@ emp_status sync_round(emp_job *j, cudaStream_t s, const RoundEnv &env, int r, in
     return EMP_OK;
 }
 
-// Enqueue pipeline rounds r0 .. rounds-1 after all work already on stream s.
-// One round is captured as a CUDA graph on the context's stream and replayed
-// once per round (every size lives in device memory); the two event nodes
-// around the update kernel are re-pointed to that round's events before each
-// replay.  EMP_NO_GRAPH=1 launches the kernels directly instead.
-void release_graph(emp_job *j) {
-    if (j->graph_exec) cudaGraphExecDestroy(j->graph_exec);
-    if (j->graph) cudaGraphDestroy(j->graph);
-    j->graph_exec = nullptr;
-    j->graph = nullptr;
-}
-
-emp_status launch_rounds_graph(emp_job *j, const PipeArgs &a, uint64_t nmax, int r0, int rounds, cudaStream_t s) {
-    cudaStream_t cs = j->ctx->stream;
-    release_graph(j);
-    if (std::getenv("EMP_NO_GRAPH")) {
-        for (int q = r0; q < rounds; ++q) {
-            launch_pipeline_round(a, nmax, nmax, s, q < EMP_MAX_ROUNDS ? j->upd_ev + 2 * q : nullptr);
-            ++j->sorts_since_clear;
-        }
-        return EMP_OK;
-    }
-    cudaEvent_t join_in = j->sort_ev[0], join_out = j->sort_ev[1];  // free here: the pipeline times no sort pass
-    EMP_CUDA(cudaEventRecord(join_in, s));
-    EMP_CUDA(cudaStreamWaitEvent(cs, join_in, 0));
-    const uint64_t l0 = g_launches.load();
-    cudaGraph_t graph = nullptr;
-    EMP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    launch_pipeline_round(a, nmax, nmax, cs, j->upd_ev);
-    cudaError_t ce = cudaStreamEndCapture(cs, &graph);
-    const uint64_t per_round = g_launches.load() - l0;
-    if (ce != cudaSuccess) {
-        cudaGetLastError();
-        return EMP_E_CUDA;
-    }
-    cudaGraphExec_t exec = nullptr;
-    ce = cudaGraphInstantiate(&exec, graph, 0);
-    if (ce != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        return EMP_E_CUDA;
-    }
-    // the event-record nodes, in capture order (before / after the update kernel)
-    size_t nn = 0;
-    cudaGraphGetNodes(graph, nullptr, &nn);
-    std::vector<cudaGraphNode_t> nodes(nn);
-    cudaGraphGetNodes(graph, nodes.data(), &nn);
-    cudaGraphNode_t evn[2] = {nullptr, nullptr};
-    for (cudaGraphNode_t nd : nodes) {
-        cudaGraphNodeType t;
-        cudaGraphNodeGetType(nd, &t);
-        if (t != cudaGraphNodeTypeEventRecord) continue;
-        cudaEvent_t e = nullptr;
-        cudaGraphEventRecordNodeGetEvent(nd, &e);
-        if (e == j->upd_ev[0]) evn[0] = nd;
-        if (e == j->upd_ev[1]) evn[1] = nd;
-    }
-    emp_status rc = EMP_OK;
-    for (int q = r0; q < rounds && rc == EMP_OK; ++q) {
-        if (evn[0] && evn[1] && q < EMP_MAX_ROUNDS) {
-            cudaGraphExecEventRecordNodeSetEvent(exec, evn[0], j->upd_ev[2 * q]);
-            cudaGraphExecEventRecordNodeSetEvent(exec, evn[1], j->upd_ev[2 * q + 1]);
-        }
-        if (cudaGraphLaunch(exec, cs) != cudaSuccess) rc = EMP_E_CUDA;
-        ++j->sorts_since_clear;
-    }
-    if (rounds - r0 > 1) count_launch(per_round * (uint64_t)(rounds - r0 - 1));
-    cudaEventRecord(join_out, cs);
-    cudaStreamWaitEvent(s, join_out, 0);
-    j->graph_exec = exec;  // released by release_graph() after the stream synchronises
-    j->graph = graph;
-    return rc;
-}
-
-// log2 of the Bloom filter size for n list entries: 16 bits per entry (at
-// least 32 per entry of the larger table), 2^16 .. 2^30 bits.  The same rule
-// runs on the device (bloom_bits_for_n, k_pipeline.cu) as the lists shrink.
-int bloom_bits_for(uint64_t n) {
-    int b = 16;
-    while (b < 30 && (1ull << b) < 16 * n) ++b;
-    return b;
-}
-
 // Profiling aid: per-round phase durations (us) of a cooperative round kernel
 // whose barriers stamp phases 0 .. nph-1 of every iteration.
 void write_coop_trace(emp_job *j, const char *path, int rounds, int r0, const RoundRecord *rec, cudaStream_t s,
@@ -678,122 +602,21 @@ void write_coop_probe(emp_job *j, const char *path, int grid, cudaStream_t s) {
     std::fclose(f);
 }
 
-// Rounds r0 .. of one job through the cooperative kernel (k_coop.cu): one
-// launch, no host round trip until all rounds are done.  `a` carries the
-// buffers run_rounds allocated for the pipeline.
-emp_status run_rounds_coop(emp_job *j, cudaStream_t s, const RoundEnv &env, const PipeArgs &a, uint64_t nmax,
-                           int bits, int r0, int cur, uint64_t n_in, uint64_t *needed) {
-    emp_stats &st = j->st;
-    EMP_TRY(ensure(j, j->st_join, coop_tiles(nmax) * 8 + 8));
-    EMP_TRY(ensure(j, j->st_sort, sort_tiles(nmax) * kSortRadix * 8 + 8));
-    EMP_TRY(ensure(j, j->coop_job, sizeof(CoopJob)));
-    EMP_TRY(ensure(j, j->coop_ctl, sizeof(CoopCtl)));
-    if (!j->h_coop.ensure(sizeof(CoopJob) + sizeof(CoopCtl))) return EMP_E_NOMEM;
-    EMP_CUDA(cudaMemsetAsync(j->st_upd.p, 0, j->st_upd.bytes, s));
-    EMP_CUDA(cudaMemsetAsync(j->st_cand.p, 0, j->st_cand.bytes, s));
-    EMP_CUDA(cudaMemsetAsync(j->st_join.p, 0, j->st_join.bytes, s));
-    EMP_CUDA(cudaMemsetAsync(j->st_sort.p, 0, j->st_sort.bytes, s));
-    CoopJob *hj = j->h_coop.as<CoopJob>();
-    CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + 1);
-    std::memset(hj, 0, sizeof(CoopJob) + sizeof(CoopCtl));
-    hj->lk[0] = a.lk0;
-    hj->lk[1] = a.lk1;
-    hj->lv[0] = a.lv0;
-    hj->lv[1] = a.lv1;
-    hj->used_s = a.used_s;
-    hj->used_p = a.used_p;
-    hj->cols = a.cols;
-    hj->wpc = a.wpc;
-    hj->tables = a.tables;
-    hj->L = env.L;
-    hj->rounds = env.rounds;
-    hj->bloom_s = a.bloom_s;
-    hj->bloom_p = a.bloom_p;
-    hj->bloom_bits_max = bits;
-    hj->ck = a.ck;
-    hj->ck2 = a.ck2;
-    hj->cv = a.cv;
-    hj->cv2 = a.cv2;
-    hj->efrom = a.efrom;
-    hj->eto = a.eto;
-    hj->ecap = a.ecap;
-    hj->records = a.records;
-    hj->st_upd = a.st_upd;
-    hj->st_cand = a.st_cand;
-    hj->st_join = j->st_join.as<uint64_t>();
-    hj->st_sort = j->st_sort.as<uint64_t>();
-    hj->n = n_in;
-    hj->round = (uint32_t)r0;
-    hj->cur = (uint32_t)cur;
-    hj->bloom_bits[0] = (uint32_t)bits;
-    hc->njobs = 1;
-    hc->active = 1;
-    const char *trace_path = std::getenv("EMP_COOP_TRACE");  // profiling: per-phase timestamps
-    if (trace_path) {
-        EMP_TRY(ensure(j, j->coop_trace, (size_t)env.rounds * kCoopTracePhases * 8));
-        EMP_CUDA(cudaMemsetAsync(j->coop_trace.p, 0, j->coop_trace.bytes, s));
-        hc->trace = j->coop_trace.as<uint64_t>();
-        hc->trace_cap = (uint32_t)env.rounds;
+// Whether rounds may run in the bucket kernel on this context (cooperative
+// launch available, not turned off by the tuning).
+bool bucket_rounds_usable(const emp_ctx *c) { return c->tune.round_driver == 0 && bucket_grid_size() > 0; }
+
+// The control block of a bucket-kernel launch: the context's grid-barrier
+// limit, and the testing barrier that no arrival completes (used once).
+void coop_ctl_init(emp_ctx *c, CoopCtl *hc, uint32_t njobs) {
+    std::memset(hc, 0, sizeof(CoopCtl));
+    hc->njobs = njobs;
+    hc->active = njobs;
+    hc->wait_ns = c->tune.wait_limit_ns;
+    if (c->tune.block_next_wait) {
+        hc->bar_extra = 1;
+        c->tune.block_next_wait = 0;
     }
-    // profiling: per-CTA stamps of one iteration, EMP_COOP_PROBE=<csv path>:<iteration>
-    const char *probe_env = std::getenv("EMP_COOP_PROBE");
-    std::string probe_path;
-    const int grid = coop_grid_size();
-    if (probe_env) {
-        const char *colon = std::strrchr(probe_env, ':');
-        probe_path.assign(probe_env, colon ? (size_t)(colon - probe_env) : std::strlen(probe_env));
-        hc->probe_iter = colon ? (uint32_t)std::atoi(colon + 1) : 0u;
-        EMP_TRY(ensure(j, j->coop_probe, (size_t)grid * kCoopProbePoints * 8));
-        EMP_CUDA(cudaMemsetAsync(j->coop_probe.p, 0, j->coop_probe.bytes, s));
-        hc->probe = j->coop_probe.as<uint64_t>();
-    }
-    EMP_CUDA(cudaMemcpyAsync(j->coop_job.p, hj, sizeof(CoopJob), cudaMemcpyHostToDevice, s));
-    EMP_CUDA(cudaMemcpyAsync(j->coop_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
-    cudaEvent_t e0 = j->upd_ev[0], e1 = j->upd_ev[1];
-    EMP_CUDA(cudaEventRecord(e0, s));
-    EMP_CUDA(launch_coop_rounds(j->coop_job.as<CoopJob>(), j->coop_ctl.as<CoopCtl>(), err_word(j), s));
-    EMP_CUDA(cudaEventRecord(e1, s));
-    EMP_CUDA(cudaMemcpyAsync(hj, j->coop_job.p, sizeof(CoopJob), cudaMemcpyDeviceToHost, s));
-    EMP_CUDA(cudaMemcpyAsync(hc, j->coop_ctl.p, sizeof(CoopCtl), cudaMemcpyDeviceToHost, s));
-    EMP_CUDA(cudaMemcpyAsync(j->h_records.p, j->records.p, (size_t)env.rounds * sizeof(RoundRecord),
-                             cudaMemcpyDeviceToHost, s));
-    EMP_TRY(sync_and_check(j, s));
-    if (hc->err & kErrSpin) return EMP_E_TIMEOUT;
-    st.ms_round_kernel += ms_between(e0, e1);
-    if (hj->overflow) {
-        *needed = hj->e_total;
-        return kNeedEdgeRoom;
-    }
-    const uint64_t E_all = hj->e_total;
-    if (E_all) {
-        if (!j->h_from.ensure(E_all * 4) || !j->h_to.ensure(E_all * 4)) return EMP_E_NOMEM;
-        EMP_CUDA(cudaMemcpyAsync(j->h_from.p, j->efrom.p, E_all * 4, cudaMemcpyDeviceToHost, s));
-        EMP_CUDA(cudaMemcpyAsync(j->h_to.p, j->eto.p, E_all * 4, cudaMemcpyDeviceToHost, s));
-        EMP_CUDA(cudaStreamSynchronize(s));
-    }
-    const RoundRecord *rec = j->h_records.as<RoundRecord>();
-    const int r_end = (int)hj->round;  // rounds run with a non-empty suffix table
-    if (trace_path)
-        write_coop_trace(j, trace_path, env.rounds, r0, rec, s, 5,
-                         "update_us,candidates_us,sort_a_us,sort_b_us,join_end_us");
-    if (probe_env) write_coop_probe(j, probe_path.c_str(), grid, s);
-    uint64_t prev_n = n_in;
-    for (int q = r0; q < r_end; ++q) {
-        const RoundRecord &x = rec[q];
-        const uint64_t n_out = x.S + x.P;
-        // update + candidates + candidate sort (about two 24-byte moves per pair) + join
-        st.round_kernel_bytes += 13 * prev_n + prev_n / 4 + 24 * n_out + 72 * x.C + 8 * x.E;
-        if (q < EMP_MAX_ROUNDS) {
-            st.sfx_live[q] = x.S;
-            st.pfx_live[q] = x.P;
-            st.edges[q] = x.E;
-        }
-        if (x.P) emit_record(j, env.L - 1 - q, x.e0, x.e0 + x.E);
-        st.n_edges += x.E;
-        prev_n = n_out;
-    }
-    st.n_rounds = r_end;
-    return EMP_OK;
 }
 
 // Buffers and launch description (host copy *hj) of rounds r0 .. of one job
@@ -802,12 +625,10 @@ emp_status run_rounds_coop(emp_job *j, cudaStream_t s, const RoundEnv &env, cons
 emp_status bucket_prepare(emp_job *j, cudaStream_t s, const RoundEnv &env, int r0, int cur, uint64_t n_in,
                           uint64_t ecap, uint32_t wave, BktJob *hj) {
     const uint64_t nmax = n_in;
-    const uint32_t nb_max = bkt_count(nmax, wave);
-    uint32_t cap = kBktRegionCap;
-    if (const char *c = std::getenv("EMP_BKT_REGION_CAP")) {  // testing: small regions force the spill path
-        const long v = std::strtol(c, nullptr, 10);
-        if (v >= 1 && v <= (long)kBktRegionCap) cap = (uint32_t)v;
-    }
+    const emp_tuning &tu = j->ctx->tune;
+    const uint32_t mean = tu.bucket_mean ? tu.bucket_mean : kBktMean;
+    const uint32_t nb_max = bkt_count(nmax, wave, mean);
+    const uint32_t cap = tu.region_cap ? tu.region_cap : kBktRegionCap;
     const uint64_t list_entries = (uint64_t)nb_max * 2 * cap;
     const uint64_t iters = (uint64_t)(env.rounds - r0) + 1;  // lists of iterations 0 .. rounds - r0
     const size_t cnt_bytes = iters * 2 * nb_max * 4;
@@ -855,6 +676,7 @@ emp_status bucket_prepare(emp_job *j, cudaStream_t s, const RoundEnv &env, int r
     hj->n_max = nmax;
     hj->nb_max = nb_max;
     hj->wave = wave;
+    hj->mean = mean;
     hj->r0 = r0;
     hj->meta = j->bk_meta.as<BktRound>();
     return EMP_OK;
@@ -912,17 +734,15 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
     BktJob *hj = j->h_coop.as<BktJob>();
     CoopCtl *hc = reinterpret_cast<CoopCtl *>(hj + 1);
     EMP_TRY(bucket_prepare(j, s, env, r0, cur, n_in, ecap, (uint32_t)grid, hj));
-    std::memset(hc, 0, sizeof(CoopCtl));
-    hc->njobs = 1;
-    hc->active = 1;
-    const char *trace_path = std::getenv("EMP_COOP_TRACE");  // profiling: per-phase timestamps
+    coop_ctl_init(j->ctx, hc, 1);
+    const char *trace_path = j->ctx->trace_path.empty() ? nullptr : j->ctx->trace_path.c_str();
     if (trace_path) {
         EMP_TRY(ensure(j, j->coop_trace, (size_t)env.rounds * kCoopTracePhases * 8));
         EMP_CUDA(cudaMemsetAsync(j->coop_trace.p, 0, j->coop_trace.bytes, s));
         hc->trace = j->coop_trace.as<uint64_t>();
         hc->trace_cap = (uint32_t)env.rounds;
     }
-    const char *probe_env = std::getenv("EMP_COOP_PROBE");  // profiling: per-CTA stamps of one iteration
+    const char *probe_env = j->ctx->probe_spec.empty() ? nullptr : j->ctx->probe_spec.c_str();
     std::string probe_path;
     if (probe_env) {
         const char *colon = std::strrchr(probe_env, ':');
@@ -970,7 +790,6 @@ emp_status rounds_prelude(emp_job *j, cudaStream_t s) {
 // rest with a single synchronisation at the end.  Returns kNeedEdgeRoom with
 // *needed set when the pipeline's edge buffer (ecap edges) was too small.
 emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t U, uint64_t ecap, uint64_t *needed) {
-    emp_stats &st = j->st;
     if (!j->upd_ev[0]) {  // per-round events, made when a job first runs rounds on its own
         for (auto &e : j->upd_ev) EMP_CUDA(cudaEventCreate(&e));
     }
@@ -978,131 +797,18 @@ emp_status run_rounds(emp_job *j, cudaStream_t s, const RoundEnv &env, uint64_t 
     int cur = 0, r = 0;
     uint64_t n_in = 2 * U, S = U, P = U;
     const uint64_t M = env.M;
-    const bool force_sync = std::getenv("EMP_SYNC_ROUNDS") != nullptr;
-    const bool bucket = !std::getenv("EMP_NO_COOP") && !std::getenv("EMP_NO_BUCKET") && bucket_grid_size() > 0;
-    // host-synchronised rounds (one full sort each) also carry a list too
-    // large for the bucket kernel until it fits
-    while (r < env.rounds && (force_sync || S >= M / 2 || P >= M / 2 || (bucket && n_in > kBktMaxEntries))) {
+    const bool bucket = bucket_rounds_usable(j->ctx);
+    // host-synchronised rounds (one full sort each) while a round may split
+    // into several search partitions, and while the list is too large for the
+    // bucket kernel
+    while (r < env.rounds && (!bucket || S >= M / 2 || P >= M / 2 || n_in > kBktMaxEntries)) {
         bool stop = false;
         EMP_TRY(sync_round(j, s, env, r, cur, n_in, S, P, stop));
         if (stop) return EMP_OK;
         ++r;
     }
     if (r >= env.rounds) return EMP_OK;
-    if (bucket) return run_rounds_bucket(j, s, env, r, cur, n_in, ecap, needed);
-
-    // ---- device-resident pipeline for rounds r .. rounds-1
-    const uint64_t nmax = n_in;
-    const int bits = bloom_bits_for(n_in);
-    const size_t bloom_bytes = (size_t)1 << (bits - 3);
-    EMP_TRY(ensure(j, j->bloom_s, bloom_bytes));
-    EMP_TRY(ensure(j, j->bloom_p, bloom_bytes));
-    EMP_TRY(ensure(j, j->ck, nmax * 8 + 8));
-    EMP_TRY(ensure(j, j->ck2, nmax * 8 + 8));
-    EMP_TRY(ensure(j, j->cv, nmax * 4 + 4));
-    EMP_TRY(ensure(j, j->cv2, nmax * 4 + 4));
-    EMP_TRY(ensure(j, j->cnt, nmax * 4 + 4));
-    EMP_TRY(ensure(j, j->offs, nmax * 8 + 8));
-    EMP_TRY(ensure(j, j->efrom, ecap * 4));
-    EMP_TRY(ensure(j, j->eto, ecap * 4));
-    EMP_TRY(ensure(j, j->records, (size_t)env.rounds * sizeof(RoundRecord)));
-    EMP_TRY(ensure(j, j->st_upd, upd_tiles(nmax) * 8 + 8));
-    EMP_TRY(ensure(j, j->st_cand, upd_tiles(nmax) * 8 + 8));
-    EMP_TRY(ensure(j, j->st_scan, scan_tiles(nmax) * 8 + 8));
-    EMP_TRY(ensure(j, j->ctl, sizeof(RoundCtl)));
-    EMP_TRY(ensure_sort_scratch(j, nmax, s));
-    if (!j->h_ctl.ensure(sizeof(RoundCtl)) || !j->h_records.ensure((size_t)env.rounds * sizeof(RoundRecord)))
-        return EMP_E_NOMEM;
-    EMP_CUDA(cudaMemsetAsync(j->st_upd.p, 0, j->st_upd.bytes, s));
-    EMP_CUDA(cudaMemsetAsync(j->st_cand.p, 0, j->st_cand.bytes, s));
-    EMP_CUDA(cudaMemsetAsync(j->st_scan.p, 0, j->st_scan.bytes, s));
-    RoundCtl *hc = j->h_ctl.as<RoundCtl>();
-    std::memset(hc, 0, sizeof(RoundCtl));
-    hc->n = n_in;
-    hc->s = S;
-    hc->cur = (uint32_t)cur;
-    hc->round = (uint32_t)r;
-    hc->rounds = (uint32_t)env.rounds;
-    hc->bloom_bits = (uint32_t)bits;
-    EMP_CUDA(cudaMemcpyAsync(j->ctl.p, hc, sizeof(RoundCtl), cudaMemcpyHostToDevice, s));
-    EMP_CUDA(cudaMemsetAsync(j->bloom_s.p, 0, bloom_bytes, s));
-    EMP_CUDA(cudaMemsetAsync(j->bloom_p.p, 0, bloom_bytes, s));
-    launch_sort_prepare(j->sort_scratch.as<SortScratch>(), true, s);
-    PipeArgs a{};
-    a.ctl = j->ctl.as<RoundCtl>();
-    a.records = j->records.as<RoundRecord>();
-    a.lk0 = j->lk0.as<uint64_t>();
-    a.lk1 = j->lk1.as<uint64_t>();
-    a.lv0 = j->lv0.as<uint32_t>();
-    a.lv1 = j->lv1.as<uint32_t>();
-    a.used_s = j->used_s.as<uint8_t>();
-    a.used_p = j->used_p.as<uint8_t>();
-    a.cols = j->cols.as<uint32_t>();
-    a.wpc = env.wpc;
-    a.tables = env.tables;
-    a.L = env.L;
-    a.bloom_bits_max = bits;
-    a.bloom_s = j->bloom_s.as<uint32_t>();
-    a.bloom_p = j->bloom_p.as<uint32_t>();
-    a.sort = j->sort_scratch.as<SortScratch>();
-    a.ck = j->ck.as<uint64_t>();
-    a.ck2 = j->ck2.as<uint64_t>();
-    a.cv = j->cv.as<uint32_t>();
-    a.cv2 = j->cv2.as<uint32_t>();
-    a.cnt = j->cnt.as<uint32_t>();
-    a.offs = j->offs.as<uint64_t>();
-    a.efrom = j->efrom.as<uint32_t>();
-    a.eto = j->eto.as<uint32_t>();
-    a.ecap = ecap;
-    a.st_upd = j->st_upd.as<uint64_t>();
-    a.st_cand = j->st_cand.as<uint64_t>();
-    a.st_scan = j->st_scan.as<uint64_t>();
-    a.err = err_word(j);
-    const int r0 = r;
-    if (!std::getenv("EMP_NO_COOP") && coop_grid_size() > 0)
-        return run_rounds_coop(j, s, env, a, nmax, bits, r0, cur, n_in, needed);
-    emp_status lrc = launch_rounds_graph(j, a, nmax, r0, env.rounds, s);
-    if (lrc != EMP_OK) {
-        cudaStreamSynchronize(j->ctx->stream);
-        release_graph(j);
-        return lrc;
-    }
-    EMP_CUDA(cudaMemcpyAsync(hc, j->ctl.p, sizeof(RoundCtl), cudaMemcpyDeviceToHost, s));
-    EMP_CUDA(cudaMemcpyAsync(j->h_records.p, j->records.p, (size_t)env.rounds * sizeof(RoundRecord),
-                             cudaMemcpyDeviceToHost, s));
-    emp_status src = sync_and_check(j, s);
-    release_graph(j);
-    EMP_TRY(src);
-    if (hc->overflow) {
-        *needed = hc->e_total;
-        return kNeedEdgeRoom;
-    }
-    const uint64_t E_all = hc->e_total;
-    if (E_all) {
-        if (!j->h_from.ensure(E_all * 4) || !j->h_to.ensure(E_all * 4)) return EMP_E_NOMEM;
-        EMP_CUDA(cudaMemcpyAsync(j->h_from.p, j->efrom.p, E_all * 4, cudaMemcpyDeviceToHost, s));
-        EMP_CUDA(cudaMemcpyAsync(j->h_to.p, j->eto.p, E_all * 4, cudaMemcpyDeviceToHost, s));
-        EMP_CUDA(cudaStreamSynchronize(s));
-    }
-    const RoundRecord *rec = j->h_records.as<RoundRecord>();
-    const int r_end = (int)hc->round;  // rounds run with a non-empty suffix table
-    uint64_t prev_n = n_in;
-    for (int q = r0; q < r_end; ++q) {
-        const RoundRecord &x = rec[q];
-        if (q < EMP_MAX_ROUNDS) {
-            st.sfx_live[q] = x.S;
-            st.pfx_live[q] = x.P;
-            st.edges[q] = x.E;
-            st.ms_update += ms_between(j->upd_ev[2 * q], j->upd_ev[2 * q + 1]);
-            st.update_launches += 1;
-            st.update_bytes += 13 * prev_n + prev_n / 4 + 12 * (x.S + x.P);
-        }
-        if (x.P) emit_record(j, env.L - 1 - q, x.e0, x.e0 + x.E);
-        st.n_edges += x.E;
-        prev_n = x.S + x.P;
-    }
-    st.n_rounds = r_end;
-    return EMP_OK;
+    return run_rounds_bucket(j, s, env, r, cur, n_in, ecap, needed);
 }
 
 // The map phase of a job, in stages that each end where the host must read
@@ -1204,9 +910,8 @@ emp_status map_records(emp_job *j, cudaStream_t s) {
 // Each table holds at most 2n entries and the list at most 4n, so with
 // 2n < M/2 and 4n within the bucket kernel's list limit every round runs
 // there.
-bool columns_needed(uint64_t n, uint64_t M) {
-    const bool bucket = !std::getenv("EMP_NO_COOP") && !std::getenv("EMP_NO_BUCKET") && bucket_grid_size() > 0;
-    return std::getenv("EMP_SYNC_ROUNDS") || !bucket || 2 * n >= M / 2 || 4 * n > kBktMaxEntries;
+bool columns_needed(const emp_ctx *c, uint64_t n, uint64_t M) {
+    return !bucket_rounds_usable(c) || 2 * n >= M / 2 || 4 * n > kBktMaxEntries;
 }
 
 emp_status map_keys(emp_job *j, cudaStream_t s) {
@@ -1241,7 +946,7 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
     q.wpc = (n + 15) / 16;
     q.wpr = (L + 15) / 16;
     EMP_TRY(ensure(j, j->rec_of, n * 4));
-    const bool want_cols = columns_needed(n, q.M);
+    const bool want_cols = columns_needed(j->ctx, n, q.M);
     if (want_cols) EMP_TRY(ensure(j, j->cols, (uint64_t)L * q.wpc * 4));
     EMP_TRY(ensure(j, j->seq2, (uint64_t)n * q.wpr * 4));
     EMP_TRY(ensure(j, j->keys0, n2 * 8));
@@ -1300,8 +1005,8 @@ emp_status map_list(emp_job *j, cudaStream_t s) {
     EMP_TRY(ensure(j, j->lv_init, 2 * U * 4 + 4));
     EMP_CUDA(cudaMemcpyAsync(j->lk_init.p, j->lk0.p, 2 * U * 8, cudaMemcpyDeviceToDevice, s));
     EMP_CUDA(cudaMemcpyAsync(j->lv_init.p, j->lv0.p, 2 * U * 4, cudaMemcpyDeviceToDevice, s));
-    q.ecap = j->ecap_hint ? j->ecap_hint : (4 * U > (1u << 20) ? 4 * U : (1u << 20));
-    if (const char *ec = std::getenv("EMP_EDGE_CAP")) q.ecap = std::strtoull(ec, nullptr, 10) + 1;
+    const uint64_t ecap0 = j->ctx->tune.edge_cap ? j->ctx->tune.edge_cap : (4 * U > (1u << 20) ? 4 * U : (1u << 20));
+    q.ecap = j->ecap_hint ? j->ecap_hint : ecap0;
     return EMP_OK;
 }
 
@@ -1370,8 +1075,7 @@ emp_status run_job(emp_job *j, cudaStream_t s) {
 // partitions (S, P < M/2) and the list fits the kernel.
 bool batch_eligible(const emp_job *j) {
     const JobPrep &q = j->prep;
-    return q.rounds > 0 && q.U < q.M / 2 && 2 * q.U <= kBktMaxEntries && !std::getenv("EMP_SYNC_ROUNDS") &&
-           !std::getenv("EMP_NO_COOP") && !std::getenv("EMP_NO_BUCKET");
+    return q.rounds > 0 && q.U < q.M / 2 && 2 * q.U <= kBktMaxEntries && bucket_rounds_usable(j->ctx);
 }
 
 // The rounds of jobs[idx[..]] (all eligible, lists ready) in one launch of
@@ -1394,9 +1098,7 @@ emp_status batch_rounds(emp_ctx *ctx, emp_job **jobs, const std::vector<int> &id
         EMP_TRY(rounds_prelude(j, s));
         EMP_TRY(bucket_prepare(j, s, job_env(j), 0, 0, 2 * q.U, q.ecap, 1u, &hj[k]));
     }
-    std::memset(hc, 0, sizeof(CoopCtl));
-    hc->njobs = (uint32_t)nb;
-    hc->active = (uint32_t)nb;
+    coop_ctl_init(ctx, hc, (uint32_t)nb);
     EMP_CUDA(cudaMemcpyAsync(ctx->batch_jobs.p, hj, nb * sizeof(BktJob), cudaMemcpyHostToDevice, s));
     EMP_CUDA(cudaMemcpyAsync(ctx->batch_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
     EMP_CUDA(cudaEventRecord(ctx->batch_ev[0], s));
@@ -1600,9 +1302,7 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         hj = srv->h_jobs.as<BktJob>();
         hc = reinterpret_cast<CoopCtl *>(hj + nb);
         for (size_t k = 0; k < nb; ++k) hj[k] = srv->live[k]->bk;
-        std::memset(hc, 0, sizeof(CoopCtl));
-        hc->njobs = (uint32_t)nb;
-        hc->active = (uint32_t)nb;
+        coop_ctl_init(ctx, hc, (uint32_t)nb);
         // short launches while jobs wait to join, long ones when none does
         hc->iter_cap = (uint32_t)(srv->queue.empty() && adm.empty() ? srv->p.rounds_per_launch_idle
                                                                      : srv->p.rounds_per_launch);
@@ -1774,6 +1474,37 @@ emp_status emp_parse_size(const char *s, uint64_t *bytes) {
     return st;
 }
 
+emp_status emp_tuning_default(emp_tuning *t) {
+    if (!t) return EMP_E_INVAL;
+    std::memset(t, 0, sizeof *t);
+    t->bucket_mean = kBktMean;
+    t->region_cap = kBktRegionCap;
+    t->wait_limit_ns = kBarrierTimeoutNs;
+    return EMP_OK;
+}
+
+emp_status emp_ctx_set_tuning(emp_ctx *ctx, const emp_tuning *t) {
+    if (!ctx || !t) return EMP_E_INVAL;
+    if (t->round_driver < 0 || t->round_driver > 1) return EMP_E_INVAL;
+    if (t->bucket_mean && (t->bucket_mean < kBktMeanMin || t->bucket_mean > 7000)) return EMP_E_INVAL;
+    if (t->region_cap > kBktRegionCap) return EMP_E_INVAL;
+    ctx->tune = *t;
+    return EMP_OK;
+}
+
+emp_status emp_ctx_get_tuning(emp_ctx *ctx, emp_tuning *t) {
+    if (!ctx || !t) return EMP_E_INVAL;
+    emp_tuning_default(t);
+    const emp_tuning &c = ctx->tune;
+    t->round_driver = c.round_driver;
+    if (c.bucket_mean) t->bucket_mean = c.bucket_mean;
+    if (c.region_cap) t->region_cap = c.region_cap;
+    t->edge_cap = c.edge_cap;
+    if (c.wait_limit_ns) t->wait_limit_ns = c.wait_limit_ns;
+    t->block_next_wait = c.block_next_wait;
+    return EMP_OK;
+}
+
 emp_status emp_ctx_create(int device, uint64_t hbm_budget_bytes, emp_ctx **out) {
     if (!out) return EMP_E_INVAL;
     *out = nullptr;
@@ -1791,6 +1522,8 @@ emp_status emp_ctx_create(int device, uint64_t hbm_budget_bytes, emp_ctx **out) 
     if (!c) return EMP_E_NOMEM;
     c->device = device;
     c->budget = hbm_budget_bytes;
+    if (const char *t = std::getenv("EMP_COOP_TRACE")) c->trace_path = t;
+    if (const char *t = std::getenv("EMP_COOP_PROBE")) c->probe_spec = t;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return EMP_E_CUDA;
@@ -1882,11 +1615,9 @@ emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out) {
     }
     static_assert(kSlotHist >= kMiscSlots * sizeof(uint64_t) && kSlotCoop - kSlotHist >= kSortPasses * kSortRadix * 4,
                   "slab layout");
-    static_assert(kSlotCtl - kSlotCoop >= sizeof(CoopJob) + sizeof(CoopCtl) &&
-                      kSlotCtl - kSlotCoop >= sizeof(BktJob) + sizeof(CoopCtl),
+    static_assert(kSlotCtl - kSlotCoop >= sizeof(BktJob) + sizeof(CoopCtl),
                   "slab layout");
-    static_assert(kSlotRecords - kSlotCtl >= sizeof(RoundCtl) &&
-                      kSlotBytes - kSlotRecords >= EMP_MAX_ROUNDS * sizeof(RoundRecord),
+    static_assert(kSlotBytes - kSlotRecords >= EMP_MAX_ROUNDS * sizeof(RoundRecord),
                   "slab layout");
     j->slot = ctx->slab.take();
     if (!j->slot) {
@@ -1897,7 +1628,6 @@ emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out) {
     j->h_misc.bind(sl + kSlotMisc, kSlotHist - kSlotMisc);
     j->h_hist.bind(sl + kSlotHist, kSlotCoop - kSlotHist);
     j->h_coop.bind(sl + kSlotCoop, kSlotCtl - kSlotCoop);
-    j->h_ctl.bind(sl + kSlotCtl, kSlotRecords - kSlotCtl);
     j->h_records.bind(sl + kSlotRecords, kSlotBytes - kSlotRecords);
     *out = j;
     return EMP_OK;
@@ -1912,7 +1642,6 @@ emp_status emp_job_trim(emp_job *job) {
     cudaStreamSynchronize(job->ctx->stream);
     if (job->feed_pending) cudaEventSynchronize(job->feed_ev[1]);
     job->feed_pending = false;
-    release_graph(job);
     release_buffers(job);
     job->F = 0;
     job->fed_last = false;
@@ -1940,12 +1669,10 @@ emp_status emp_job_destroy(emp_job *job) {
         if (e) cudaEventDestroy(e);
     for (auto &e : job->map_ev)
         if (e) cudaEventDestroy(e);
-    release_graph(job);
     if (job->slot) {
         job->h_misc.drop();
         job->h_hist.drop();
         job->h_coop.drop();
-        job->h_ctl.drop();
         job->h_records.drop();
         job->ctx->slab.give(job->slot);
     }
@@ -1960,9 +1687,7 @@ static void release_buffers(emp_job *job) {
                       &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
                       &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
                       &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts, &job->lk_init,
-                      &job->lv_init, &job->bloom_s, &job->bloom_p, &job->ck, &job->cv, &job->ck2, &job->cv2,
-                      &job->records, &job->st_upd, &job->st_cand, &job->st_scan, &job->ctl, &job->st_join,
-                      &job->st_sort, &job->coop_job, &job->coop_ctl, &job->coop_trace,
+                      &job->lv_init, &job->records, &job->coop_ctl, &job->coop_trace,
                       &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_cnt, &job->bk_spill, &job->bk_spans,
                       &job->bk_sfrom, &job->bk_sto, &job->bk_scratch, &job->bk_job, &job->dout,
                       &job->bk_meta, &job->xk0, &job->xv0, &job->xk1, &job->xv1, &job->ring_k, &job->ring_v,
@@ -2333,29 +2058,61 @@ emp_status emp_run_file(const char *input_path, const char *output_path, const e
         emp_ctx_destroy(ctx);
         return st;
     }
-    // read the input (a missing file reads as empty, like the reference's ifstream)
-    FILE *f = std::fopen(input_path, "rb");
-    if (f) {
-        std::fseek(f, 0, SEEK_END);
-        long sz = std::ftell(f);
-        std::fseek(f, 0, SEEK_SET);
-        if (sz > 0) {
-            PinnedBuf hb;
-            const size_t chunk = 256ull << 20;
-            if (!hb.ensure(chunk)) st = EMP_E_NOMEM;
-            if (st == EMP_OK) st = emp_job_reserve(job, (uint64_t)sz);
-            uint64_t left = (uint64_t)sz;
-            while (st == EMP_OK && left) {
-                size_t want = left < chunk ? (size_t)left : chunk;
-                size_t got = std::fread(hb.p, 1, want, f);
-                if (got != want) { st = EMP_E_IO; break; }
-                left -= got;
-                st = emp_job_feed_fastq(job, hb.as<char>(), got, left == 0);
+    bool ran = false;
+    // Read the input.  A missing file reads as empty, like the reference's
+    // ifstream; a path that exists but is not a readable regular file is an
+    // EMP_E_IO error.  Two pinned buffers alternate: chunk k+1 is read from
+    // the file while chunk k copies to the device on the copy stream.
+    struct stat sb;
+    if (::stat(input_path, &sb) != 0) {
+        if (errno != ENOENT) st = EMP_E_IO;
+    } else if (!S_ISREG(sb.st_mode)) {
+        st = EMP_E_IO;
+    } else if (sb.st_size > 0 && st == EMP_OK) {
+        FILE *f = std::fopen(input_path, "rb");
+        if (!f) st = EMP_E_IO;
+        const uint64_t size = (uint64_t)sb.st_size;
+        const size_t chunk = 128ull << 20;
+        PinnedBuf hb[2];
+        cudaEvent_t copied[2] = {nullptr, nullptr};
+        if (st == EMP_OK && (cudaEventCreateWithFlags(&copied[0], cudaEventDisableTiming) != cudaSuccess ||
+                             cudaEventCreateWithFlags(&copied[1], cudaEventDisableTiming) != cudaSuccess))
+            st = EMP_E_CUDA;
+        if (st == EMP_OK) st = emp_job_reserve(job, size);
+        uint64_t left = size;
+        for (int k = 0; st == EMP_OK && left; ++k) {
+            const int b = k & 1;
+            if (k >= 2 && cudaEventSynchronize(copied[b]) != cudaSuccess) {  // the copy that used this buffer
+                st = EMP_E_CUDA;
+                break;
             }
+            const size_t want = left < chunk ? (size_t)left : chunk;
+            if (!hb[b].ensure(want)) {
+                st = EMP_E_NOMEM;
+                break;
+            }
+            const size_t got = std::fread(hb[b].p, 1, want, f);
+            if (got != want) {
+                st = EMP_E_IO;
+                break;
+            }
+            left -= got;
+            st = emp_job_feed_fastq_async(job, hb[b].as<char>(), got, left == 0);
+            if (st == EMP_OK && cudaEventRecord(copied[b], ctx->copy_stream) != cudaSuccess) st = EMP_E_CUDA;
         }
-        std::fclose(f);
+        if (f) std::fclose(f);
+        if (st == EMP_OK) st = emp_job_run(job, nullptr);  // waits for the last copy
+        cudaStreamSynchronize(ctx->copy_stream);  // the pinned buffers are released below
+        for (cudaEvent_t e : copied)
+            if (e) cudaEventDestroy(e);
+        if (st != EMP_OK) {
+            emp_job_destroy(job);
+            emp_ctx_destroy(ctx);
+            return st;
+        }
+        ran = true;
     }
-    if (st == EMP_OK) st = emp_job_run(job, nullptr);
+    if (st == EMP_OK && !ran) st = emp_job_run(job, nullptr);
     if (st == EMP_OK) {
         FILE *g = std::fopen(output_path, "wb");
         if (!g) st = EMP_E_IO;

@@ -1,34 +1,36 @@
 // k_bucket.cu -- every overlap round of one or many read sets in ONE
 // cooperative launch, one grid barrier per round.
 //
-// A round's list is a set of tiles of 16-byte entries (key, rid | table, a
-// cached 16-base word of the read); each tile is partitioned into
-// (key bucket, table) bins.  The bucket of an entry is the top 24 bits of its
-// sort key scaled to the round's bucket count, so keys equal across tables
-// share a bucket and bucket order is key order.
+// A round's list holds 16-byte entries (key, rid | table, a cached 16-base
+// word of the read), kept as one region of `cap` entries per (key bucket,
+// table) bin; entries past a region's capacity go to a spill area tagged
+// with their bin.  The bucket of an entry is the top 24 bits of its sort key
+// scaled to the round's bucket count, so keys equal across tables share a
+// bucket and bucket order is key order.
 //
 //   prologue  the launch's input list (id order; the keys of round r0 - 1)
 //      is streamed in 4096-entry tiles: entries used in the rounds run
 //      before the launch are dropped (remove_used, overlap.cu:694-710), the
 //      hash step NextSfx / PrevPfx (overlap.cu:57-91) gives round r0's keys,
-//      and each tile is partitioned in shared memory.
-//   round r   one CTA per bucket: gather the bucket's piece of every tile
-//      (suffixes first), insert the suffix keys into a hash set, probe the
-//      prefix keys, rank the entries present in both tables by (sort key,
-//      rid parity, read index) -- the order of the reference's stable sort
-//      over its regenerated tables (regenerate_fingerprints,
-//      overlap.cu:605-692) -- and join equal-key runs (get_edges,
-//      overlap.cu:557-603).  The bucket's edges go to a staging buffer at an
-//      atomically reserved offset.  Then the same CTA drops the bucket's used
-//      entries, applies round r+1's hash step to the rest (the base from the
-//      cached word; one read-major load per 16 rounds) and writes them as one
-//      partitioned tile of round r+1's list.  The CTA finishing a job's last
-//      bucket records the round and prepares the job's next one.
+//      and each entry goes into its bin of round r0's list.
+//   round r   one CTA per bucket: stage the bucket's suffix region, then its
+//      prefix region (two contiguous runs, cp.async), flag the keys present
+//      in both tables (a two-level filter, a tagged hash set as fallback),
+//      rank the flagged entries by (sort key, rid parity, read index) -- the
+//      order of the reference's stable sort over its regenerated tables
+//      (regenerate_fingerprints, overlap.cu:605-692) -- and join equal-key
+//      runs (get_edges, overlap.cu:557-603).  The bucket's edges go to a
+//      staging buffer at an atomically reserved offset.  Then the same CTA
+//      drops the bucket's used entries, applies round r+1's hash step to the
+//      rest (the base from the cached word; one read-major load per 16
+//      rounds) and writes them into round r+1's bins: positions reserved per
+//      bin from a shared-memory histogram (up to kBktMaxBuckets buckets), or
+//      one atomic per run of equal bins in a warp (more buckets).
 //   end  every round's output.bin record (write_edges_binary,
 //      overlap.cu:148-161) is written with its edges in bucket order, which
 //      is sort-key order: the reference's order.
 //
-// A bucket that does not fit shared memory (7168 entries, or 1024 matched
+// A bucket that does not fit shared memory (7168 entries, or 2816 matched
 // entries) uses the job's global scratch region at the bucket's position in
 // bucket order instead.
 #include "coop_common.cuh"
@@ -43,7 +45,6 @@ namespace {
 
 constexpr uint32_t kBStage = 7168;  // entries of a bucket staged in shared memory
 constexpr uint32_t kBHash = 16384;  // hash slots in shared memory (power of two)
-constexpr uint32_t kBCand = 1024;   // matched entries sorted in shared memory
 constexpr uint64_t kEmptySlot = ~0ull;  // never a key: fp1, fp2 < 2^29
 constexpr uint8_t kMatched = 1, kUsed = 2;
 
@@ -62,18 +63,6 @@ static_assert(kOffReg % 16 == 0, "aligned region");
 // hash set
 constexpr size_t kHSlot = 0;                 // u32 [kBHash]
 constexpr size_t kHSuffixSlot = kBHash * 4;  // u16 [kBStage]
-// matched entries
-constexpr size_t kCKey = 0;                       // u64 [kBCand]
-constexpr size_t kCVal = kCKey + kBCand * 8;      // u32
-constexpr size_t kCIdx = kCVal + kBCand * 4;      // u32 (staged index)
-constexpr size_t kCSk = kCIdx + kBCand * 4;       // u64 sort keys
-constexpr size_t kCTb = kCSk + kBCand * 8;        // u32 tie keys
-constexpr size_t kCOrd = kCTb + kBCand * 4;       // u32 chunk order
-constexpr size_t kCCnt = kCOrd + kBCand * 4;      // u64 edge counts / offsets
-constexpr size_t kCSKey = kCCnt + kBCand * 8;     // u64 sorted keys
-constexpr size_t kCSVal = kCSKey + kBCand * 8;    // u32
-constexpr size_t kCSIdx = kCSVal + kBCand * 4;    // u32
-static_assert(kCSIdx + kBCand * 4 <= kRegion, "matched entries fit the region");
 // next round's partition
 constexpr size_t kPHist = 0;                                // u32 [2 kBktMaxBuckets]
 constexpr size_t kPInv = kPHist + 2 * kBktMaxBuckets * 4;   // u16 [kBStage]
@@ -92,7 +81,7 @@ struct BShared {
     uint32_t scan32[32];
     uint64_t scan64[32];
     uint64_t base;
-    uint32_t tile, flag, sfx, cnt;
+    uint32_t tile, flag, sfx, cnt, kept;
     uint32_t gen;  // grid barriers passed
     const CoopCtl *pctl;  // profiling stamps from inside the steps of a tile
     uint32_t piter;
@@ -281,6 +270,34 @@ EMP_DEV void put_list(const ListOut &o, uint32_t bin, uint32_t pos, const uint4 
     }
 }
 
+// Lists of more than kBktMaxBuckets buckets, whose bins do not fit a
+// shared-memory histogram: an entry takes its position from the bin counter
+// directly, one atomic per run of equal bins within the warp.  Every lane of
+// the warp calls it; lanes with act = false only vote.
+EMP_DEV void put_direct(const ListOut &o, bool act, uint32_t bin, const uint4 &e) {
+    const uint32_t m = __ballot_sync(0xffffffffu, act);
+    if (!act) return;
+    const uint32_t peers = __match_any_sync(m, bin);
+    const uint32_t lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    uint32_t pos = 0;
+    if (lane == leader) pos = atomicAdd(o.cnt + bin, (uint32_t)__popc(peers));
+    pos = __shfl_sync(peers, pos, leader);
+    put_list(o, bin, pos + __popc(peers & lanemask_lt_u32()), e);
+}
+
+// Add this CTA's kept entries and suffixes to a round's counts (sh.kept and
+// sh.sfx zeroed, then a __syncthreads, before the per-thread counts came in).
+EMP_DEV void add_counts(BktRound &nx, uint32_t kept, uint32_t sfx, BShared &sh) {
+    if (kept) atomicAdd(&sh.kept, kept);
+    if (sfx) atomicAdd(&sh.sfx, sfx);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (sh.kept) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.n), (unsigned long long)sh.kept);
+        if (sh.sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&nx.s), (unsigned long long)sh.sfx);
+    }
+    __syncthreads();
+}
+
 // hist[b] (this tile's count of bin b) -> its local start; returns the
 // tile's entry count.
 EMP_DEV uint32_t bin_starts(uint32_t *hist, uint32_t nbin, BShared &sh) {
@@ -332,14 +349,19 @@ EMP_DEV void reserve_bins(uint32_t *hist, uint32_t nbin, uint32_t kept, uint32_t
 EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
     BktRound &I = J.meta[J.r0];
     const uint64_t n_in = J.n_in;
-    const uint32_t nb = bkt_count(n_in, J.wave), nbin = 2 * nb;
+    const uint32_t nb = bkt_count(n_in, J.wave, J.mean), nbin = 2 * nb;
     const StepArgs a = step_args(J, sh.tab, J.r0, true);
     const ListOut lo = list_out(J, 0);
     uint32_t *hist = reinterpret_cast<uint32_t *>(smem);
     uint4 *stage = reinterpret_cast<uint4 *>(smem + 2 * kBktMaxBuckets * 4);
     uint16_t *sbin = reinterpret_cast<uint16_t *>(stage + kBktTile);
-    for (uint32_t i = threadIdx.x; i < nbin; i += kT) hist[i] = 0;
-    if (threadIdx.x == 0) sh.sfx = 0;
+    const bool direct = nb > kBktMaxBuckets;
+    if (!direct)
+        for (uint32_t i = threadIdx.x; i < nbin; i += kT) hist[i] = 0;
+    if (threadIdx.x == 0) {
+        sh.sfx = 0;
+        sh.kept = 0;
+    }
     __syncthreads();
     const uint64_t base = (uint64_t)k * kBktTile;
     uint64_t key[kC];
@@ -359,6 +381,22 @@ EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
         const uint32_t rid = val[c] & 0x7fffffffu;
         keep[c] = ((val[c] >> 31) ? J.used_p[rid] : J.used_s[rid]) == 0;
         if (keep[c]) word[c] = refill_word(a, val[c]);
+    }
+    if (direct) {  // hash step, bin, position straight from the bin counter
+        uint32_t kept = 0, sfx = 0;
+#pragma unroll
+        for (int c = 0; c < kC; ++c) {
+            uint32_t bn = 0;
+            if (keep[c]) {
+                key[c] = step_key(a, key[c], val[c], word[c]);
+                bn = 2 * bkt_of(sort_key(key[c], val[c]), nb) + (val[c] >> 31);
+                ++kept;
+                sfx += (val[c] >> 31) == 0;
+            }
+            put_direct(lo, keep[c], bn, make_uint4((uint32_t)key[c], (uint32_t)(key[c] >> 32), val[c], word[c]));
+        }
+        add_counts(I, kept, sfx, sh);
+        return;
     }
     uint32_t sfx = 0;
 #pragma unroll
@@ -756,83 +794,6 @@ EMP_DEV uint64_t scan_counts(uint64_t *cnt, uint32_t c, BShared &sh) {
 // search), so any c works.
 EMP_DEV uint64_t join_count(const Cands &w, uint32_t c, BShared &sh);
 
-// Sort of up to kBCand matched entries of bucket b in shared memory: a
-// counting pass into 1024 finer bins (the same top-24-bit field of the sort
-// key, scaled to nb * 1024 bins, so bin order is key order), then each entry
-// ranked among the members of its bin.  Returns the bucket's edge count.
-constexpr uint32_t kFine = 1024;
-constexpr size_t kCFine = kCSIdx + kBCand * 4;  // u32 [kFine + 1] bin starts
-static_assert(kCFine + (kFine + 4) * 4 <= kRegion, "fine bins fit the region");
-
-EMP_DEV uint64_t sort_fine(const Cands &w, uint32_t c, uint32_t b, uint32_t nb, uint8_t *smem, BShared &sh) {
-    uint32_t *hist = reinterpret_cast<uint32_t *>(smem + kOffReg + kCFine);
-    uint32_t *tmp = reinterpret_cast<uint32_t *>(w.cnt);  // staged order, before the edge counts
-    const uint64_t scale = (uint64_t)nb * kFine, lo_bin = (uint64_t)b * kFine;
-    for (uint32_t i = threadIdx.x; i <= kFine; i += kT) hist[i] = 0;
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < c; x += kT) {
-        const uint32_t val = w.cv[x];
-        const uint64_t sk = sort_key(w.ck[x], val);
-        w.sk[x] = sk;
-        w.tb[x] = tie_of(val);
-        const uint32_t f = (uint32_t)((((sk >> 35) * scale) >> 24) - lo_bin);
-        w.ord[x] = (f << 16) | atomicAdd(&hist[f], 1u);
-    }
-    __syncthreads();
-    {  // bin starts: two bins per thread
-        const uint32_t f0 = 2 * threadIdx.x;
-        const uint32_t a0 = hist[f0], a1 = hist[f0 + 1];
-        uint32_t tot;
-        const uint32_t ex = block_exclusive_scan<kT, uint32_t>(a0 + a1, sh.scan32, &tot);
-        hist[f0] = ex;
-        hist[f0 + 1] = ex + a0;
-        if (threadIdx.x == 0) hist[kFine] = tot;
-    }
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < c; x += kT) tmp[hist[w.ord[x] >> 16] + (w.ord[x] & 0xffffu)] = x;
-    __syncthreads();
-    for (uint32_t q = threadIdx.x; q < c; q += kT) {
-        const uint32_t x = tmp[q], f = w.ord[x] >> 16;
-        const uint32_t lo = hist[f], hi = hist[f + 1];
-        const uint64_t skx = w.sk[x];
-        const uint32_t tbx = w.tb[x];
-        uint32_t r = lo;
-        for (uint32_t y = lo; y < hi; ++y) {
-            const uint32_t z = tmp[y];
-            r += before(w.sk[z], w.tb[z], skx, tbx);
-        }
-        w.skey[r] = w.ck[x];
-        w.sval[r] = w.cv[x];
-        w.sidx[r] = w.cx[x];
-    }
-    __syncthreads();
-    return join_count(w, c, sh);
-}
-
-// The same for a few matched entries (c <= kSmallRank): each one's rank is
-// the number of entries before it, all pairs compared in shared memory.
-constexpr uint32_t kSmallRank = 96;
-EMP_DEV uint64_t rank_small(const Cands &w, uint32_t c, BShared &sh) {
-    if (threadIdx.x < c) {
-        const uint32_t val = w.cv[threadIdx.x];
-        w.sk[threadIdx.x] = sort_key(w.ck[threadIdx.x], val);
-        w.tb[threadIdx.x] = tie_of(val);
-    }
-    __syncthreads();
-    if (threadIdx.x < c) {
-        const uint32_t x = threadIdx.x;
-        const uint64_t skx = w.sk[x];
-        const uint32_t tbx = w.tb[x];
-        uint32_t r = 0;
-        for (uint32_t y = 0; y < c; ++y) r += before(w.sk[y], w.tb[y], skx, tbx);
-        w.skey[r] = w.ck[x];
-        w.sval[r] = w.cv[x];
-        w.sidx[r] = w.cx[x];
-    }
-    __syncthreads();
-    return join_count(w, c, sh);
-}
-
 EMP_COLD uint64_t sort_and_count(const Cands &w, uint32_t c, BShared &sh) {
     for (uint32_t x = threadIdx.x; x < c; x += kT) {
         const uint32_t val = ldv(w.cv + x);
@@ -900,7 +861,236 @@ EMP_DEV uint64_t join_count(const Cands &w, uint32_t c, BShared &sh) {
     return scan_counts(w.cnt, c, sh);
 }
 
+// ---------------------------------------------------------------- matched entries in shared memory
+// Up to kBCand matched entries of a bucket staged in shared memory are ranked
+// there, 26 bytes each in the region; their keys and values are read from the
+// stage through their staged index.
+constexpr uint32_t kBCand = 2816;
+constexpr uint32_t kFine = 1024;    // fine bins of the ranking
+constexpr uint32_t kSmallRank = 96; // up to this many: all pairs compared
+constexpr size_t kSCx = 0;                                  // u16 staged index, compaction order
+constexpr size_t kSSk = (kSCx + kBCand * 2 + 7) / 8 * 8;    // u64 sort key
+constexpr size_t kSTb = kSSk + kBCand * 8;                  // u32 tie key
+constexpr size_t kSOrd = kSTb + kBCand * 4;                 // u32 fine bin << 16 | rank within the bin
+constexpr size_t kSTmp = kSOrd + kBCand * 4;                // u16 compaction index, grouped by fine bin
+constexpr size_t kSIdx = kSTmp + kBCand * 2;                // u16 staged index in (sort key, tie) order
+constexpr size_t kSCnt = (kSIdx + kBCand * 2 + 3) / 4 * 4;  // u32 edges of each suffix, then their offsets
+constexpr size_t kSHist = kSCnt + kBCand * 4;               // u32 [kFine + 1] fine-bin starts
+static_assert(kSHist + (kFine + 1) * 4 <= kRegion, "matched entries fit the region");
+static_assert(kBStage <= 65535 && kFine == 2 * kT, "u16 staged indices; two fine bins per thread");
+
+struct CandS {
+    uint16_t *cx, *tmp, *sidx;
+    uint64_t *sk;
+    uint32_t *tb, *ord, *cnt, *hist;
+};
+EMP_DEV CandS cand_s(uint8_t *smem) {
+    uint8_t *reg = smem + kOffReg;
+    CandS w;
+    w.cx = reinterpret_cast<uint16_t *>(reg + kSCx);
+    w.sk = reinterpret_cast<uint64_t *>(reg + kSSk);
+    w.tb = reinterpret_cast<uint32_t *>(reg + kSTb);
+    w.ord = reinterpret_cast<uint32_t *>(reg + kSOrd);
+    w.tmp = reinterpret_cast<uint16_t *>(reg + kSTmp);
+    w.sidx = reinterpret_cast<uint16_t *>(reg + kSIdx);
+    w.cnt = reinterpret_cast<uint32_t *>(reg + kSCnt);
+    w.hist = reinterpret_cast<uint32_t *>(reg + kSHist);
+    return w;
+}
+
+// The staged indices of the matched entries into w.cx (any order: the
+// ranking fixes it), at most kBCand of them; returns how many there are.
+EMP_DEV uint32_t compact_s(const uint8_t *flag, uint32_t total, const CandS &w, BShared &sh) {
+    if (threadIdx.x == 0) sh.tile = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t x0 = 0; x0 < total; x0 += kT) {
+        const uint32_t x = x0 + threadIdx.x;
+        const bool f = x < total && (flag[x] & kMatched);
+        const uint32_t m = __ballot_sync(0xffffffffu, f);
+        if (!m) continue;
+        const uint32_t leader = __ffs(m) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(&sh.tile, (uint32_t)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        const uint32_t d = base + __popc(m & lanemask_lt_u32());
+        if (f && d < kBCand) w.cx[d] = (uint16_t)x;
+    }
+    __syncthreads();
+    return sh.tile;
+}
+
+// Rank the c <= kBCand matched entries of bucket b (nb buckets) by (sort key,
+// tie): w.sidx[rank] = staged index.  Up to kSmallRank entries compare all
+// pairs; more are counted into kFine finer bins (the same top-24-bit field of
+// the sort key scaled to nb * kFine bins, so bin order is key order) and
+// ranked among the members of their bin.
+EMP_DEV void rank_s(const CandS &w, uint32_t c, uint32_t b, uint32_t nb, const uint64_t *key, const uint32_t *val,
+                    BShared &sh) {
+    for (uint32_t x = threadIdx.x; x < c; x += kT) {
+        const uint32_t sx = w.cx[x], v = val[sx];
+        w.sk[x] = sort_key(key[sx], v);
+        w.tb[x] = tie_of(v);
+    }
+    __syncthreads();
+    if (c <= kSmallRank) {
+        if (threadIdx.x < c) {
+            const uint32_t x = threadIdx.x;
+            const uint64_t skx = w.sk[x];
+            const uint32_t tbx = w.tb[x];
+            uint32_t r = 0;
+            for (uint32_t y = 0; y < c; ++y) r += before(w.sk[y], w.tb[y], skx, tbx);
+            w.sidx[r] = w.cx[x];
+        }
+        __syncthreads();
+        return;
+    }
+    uint32_t *hist = w.hist;
+    const uint64_t scale = (uint64_t)nb * kFine, lo_bin = (uint64_t)b * kFine;
+    for (uint32_t i = threadIdx.x; i <= kFine; i += kT) hist[i] = 0;
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < c; x += kT) {
+        const uint32_t f = (uint32_t)((((w.sk[x] >> 35) * scale) >> 24) - lo_bin);
+        w.ord[x] = (f << 16) | atomicAdd(&hist[f], 1u);
+    }
+    __syncthreads();
+    {  // bin starts: two bins per thread
+        const uint32_t f0 = 2 * threadIdx.x;
+        const uint32_t a0 = hist[f0], a1 = hist[f0 + 1];
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan<kT, uint32_t>(a0 + a1, sh.scan32, &tot);
+        hist[f0] = ex;
+        hist[f0 + 1] = ex + a0;
+        if (threadIdx.x == 0) hist[kFine] = tot;
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < c; x += kT) w.tmp[hist[w.ord[x] >> 16] + (w.ord[x] & 0xffffu)] = (uint16_t)x;
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < c; q += kT) {
+        const uint32_t x = w.tmp[q], f = w.ord[x] >> 16;
+        const uint32_t lo = hist[f], hi = hist[f + 1];
+        const uint64_t skx = w.sk[x];
+        const uint32_t tbx = w.tb[x];
+        uint32_t r = lo;
+        for (uint32_t y = lo; y < hi; ++y) {
+            const uint32_t z = w.tmp[y];
+            r += before(w.sk[z], w.tb[z], skx, tbx);
+        }
+        w.sidx[r] = w.cx[x];
+    }
+    __syncthreads();
+}
+
+// Per suffix of the ranked entries: the prefixes of its equal-key run from
+// other reads (get_edges, overlap.cu:557-603).  w.cnt then holds each one's
+// exclusive edge offset; returns the bucket's edge count.
+EMP_DEV uint64_t join_count_s(const CandS &w, uint32_t c, const uint64_t *key, const uint32_t *val, BShared &sh) {
+    for (uint32_t i = threadIdx.x; i < c; i += kT) {
+        uint32_t cc = 0;
+        const uint32_t si = w.sidx[i], vi = val[si];
+        if (!(vi >> 31)) {
+            const uint64_t ki = key[si];
+            const uint32_t ri = (vi & 0x7fffffffu) >> 1;
+            for (uint32_t j = i + 1; j < c; ++j) {
+                const uint32_t sj = w.sidx[j];
+                if (key[sj] != ki) break;
+                const uint32_t vj = val[sj];
+                cc += (vj >> 31) && ((vj & 0x7fffffffu) >> 1) != ri;
+            }
+        }
+        w.cnt[i] = cc;
+    }
+    __syncthreads();
+    uint32_t run = 0;
+    for (uint32_t x0 = 0; x0 < c; x0 += kT) {
+        const uint32_t x = x0 + threadIdx.x;
+        const uint32_t v = x < c ? w.cnt[x] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan<kT, uint32_t>(v, sh.scan32, &tot);
+        if (x < c) w.cnt[x] = run + ex;
+        run += tot;
+        __syncthreads();
+    }
+    return run;
+}
+
+// The bucket's edges at ebase (only when they fit) and the used marks: a
+// suffix with an edge, a prefix that got one.
+EMP_DEV void write_edges_s(BktJob &J, const CandS &w, uint32_t c, uint64_t ebase, bool room, const uint64_t *key,
+                           const uint32_t *val, uint8_t *flag) {
+    for (uint32_t i = threadIdx.x; i < c; i += kT) {
+        const uint32_t si = w.sidx[i], vi = val[si];
+        if (vi >> 31) continue;
+        const uint64_t ki = key[si];
+        const uint32_t rs = vi & 0x7fffffffu, ri = rs >> 1;
+        const uint64_t o0 = ebase + w.cnt[i];
+        uint64_t o = o0;
+        for (uint32_t j = i + 1; j < c; ++j) {
+            const uint32_t sj = w.sidx[j];
+            if (key[sj] != ki) break;
+            const uint32_t vj = val[sj], pj = vj & 0x7fffffffu;
+            if ((vj >> 31) && (pj >> 1) != ri) {
+                if (room) {
+                    J.sfrom[o] = rs;
+                    J.sto[o] = pj;
+                }
+                flag[sj] = kMatched | kUsed;
+                ++o;
+            }
+        }
+        if (o != o0) flag[si] = kMatched | kUsed;
+    }
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------- next round
+// The next list has more than kBktMaxBuckets buckets: drop the used entries,
+// apply round a.r's hash step to the rest and put each one straight at a
+// position taken from its bin's counter (the stage may be shared memory or
+// global scratch).
+EMP_COLD void write_next_direct(const Stage &v, uint32_t total, const StepArgs a, uint32_t nb, const ListOut lo,
+                                BktRound &nx, BShared &sh) {
+    if (threadIdx.x == 0) {
+        sh.sfx = 0;
+        sh.kept = 0;
+    }
+    __syncthreads();
+    uint32_t kept = 0, sfx = 0;
+    constexpr int kU = 4;  // entries per thread in flight
+    for (uint32_t x0 = 0; x0 < total; x0 += kU * kT) {
+        bool act[kU];
+        uint32_t vl[kU], wd[kU];
+        uint64_t ky[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            act[u] = x < total && !(ldv(v.flag + x) & kUsed);
+            vl[u] = wd[u] = 0;
+            ky[u] = 0;
+            if (act[u]) {
+                vl[u] = ldv(v.val + x);
+                wd[u] = ldv(v.word + x);
+                ky[u] = ldv(v.key + x);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            if (act[u] && needs_refill(a, vl[u])) wd[u] = refill_word(a, vl[u]);
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            uint32_t bn = 0;
+            if (act[u]) {
+                ky[u] = step_key(a, ky[u], vl[u], wd[u]);
+                bn = 2 * bkt_of(sort_key(ky[u], vl[u]), nb) + (vl[u] >> 31);
+                ++kept;
+                sfx += (vl[u] >> 31) == 0;
+            }
+            put_direct(lo, act[u], bn, make_uint4((uint32_t)ky[u], (uint32_t)(ky[u] >> 32), vl[u], wd[u]));
+        }
+    }
+    add_counts(nx, kept, sfx, sh);
+}
+
 // Drop the used entries of the staged bucket, apply round a.r's hash step to
 // the rest and write them into the next list's bins (nb buckets).  Counts go
 // to the next round's BktRound.
@@ -1053,21 +1243,6 @@ EMP_COLD void write_next(BktJob &J, const Stage &v, uint32_t total, bool in_smem
 }
 
 // ---------------------------------------------------------------- a round tile
-EMP_DEV Cands cands_smem(uint8_t *smem) {
-    uint8_t *reg = smem + kOffReg;
-    Cands w;
-    w.ck = reinterpret_cast<uint64_t *>(reg + kCKey);
-    w.cv = reinterpret_cast<uint32_t *>(reg + kCVal);
-    w.cx = reinterpret_cast<uint32_t *>(reg + kCIdx);
-    w.sk = reinterpret_cast<uint64_t *>(reg + kCSk);
-    w.tb = reinterpret_cast<uint32_t *>(reg + kCTb);
-    w.ord = reinterpret_cast<uint32_t *>(reg + kCOrd);
-    w.cnt = reinterpret_cast<uint64_t *>(reg + kCCnt);
-    w.skey = reinterpret_cast<uint64_t *>(reg + kCSKey);
-    w.sval = reinterpret_cast<uint32_t *>(reg + kCSVal);
-    w.sidx = reinterpret_cast<uint32_t *>(reg + kCSIdx);
-    return w;
-}
 EMP_DEV Cands cands_global(const BktJob &J, uint64_t G) {
     BScratch gs;
     scratch_layout(J.scratch, J.n_max, &gs);
@@ -1169,9 +1344,9 @@ EMP_DEV RoundShape round_shape(const BktJob &J, uint32_t iter) {
     const uint64_t n2 = iter >= 2 ? __ldcg(&J.meta[z.r - 2].n) : J.n_in;
     z.active = s > 0;
     if (!z.active) return z;
-    z.nb = bkt_count(n1, J.wave);
-    z.K = iter == 0 ? (uint32_t)bkt_tiles(J.n_in) : bkt_count(n2, J.wave);
-    z.nb_next = bkt_count(n, J.wave);
+    z.nb = bkt_count(n1, J.wave, J.mean);
+    z.K = iter == 0 ? (uint32_t)bkt_tiles(J.n_in) : bkt_count(n2, J.wave, J.mean);
+    z.nb_next = bkt_count(n, J.wave, J.mean);
     return z;
 }
 
@@ -1200,7 +1375,7 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
         if (in_smem) {
             if (!match_filter(total, S, smem, sh)) match_smem(total, S, smem);
             probe(ctl, iter, 4);
-            c = compact(v, total, cands_smem(smem), kBCand, sh);
+            c = compact_s(smem + kOffFlag, total, cand_s(smem), sh);
             small = c <= kBCand;
         } else {
             BScratch gs;
@@ -1209,7 +1384,12 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
         }
         probe(ctl, iter, 5);
         if (small) {
-            if (c) E = c <= kSmallRank ? rank_small(cands_smem(smem), c, sh) : sort_fine(cands_smem(smem), c, b, nb, smem, sh);
+            if (c) {
+                const uint64_t *skey = reinterpret_cast<const uint64_t *>(smem + kOffKey);
+                const uint32_t *sval = reinterpret_cast<const uint32_t *>(smem + kOffVal);
+                rank_s(cand_s(smem), c, b, nb, skey, sval, sh);
+                E = join_count_s(cand_s(smem), c, skey, sval, sh);
+            }
         } else {
             E = big_count(J, v, total, in_smem, G, b, li.cnt, sh, c);
         }
@@ -1230,7 +1410,14 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
         sp.cnt = E;
     }
     __syncthreads();
-    if (E) write_edges(J, small ? cands_smem(smem) : cands_global(J, G), c, sh.base, sh.base + E <= J.ecap, v);
+    if (E) {
+        const bool room = sh.base + E <= J.ecap;
+        if (small)
+            write_edges_s(J, cand_s(smem), c, sh.base, room, reinterpret_cast<const uint64_t *>(smem + kOffKey),
+                          reinterpret_cast<const uint32_t *>(smem + kOffVal), smem + kOffFlag);
+        else
+            write_edges(J, cands_global(J, G), c, sh.base, room, v);
+    }
     probe(ctl, iter, 7);
     // ---- round r+1's tile b
     if (z.r + 1 < J.rounds) {
@@ -1238,7 +1425,9 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
         const uint32_t nb_next = z.nb_next;
         const StepArgs a = step_args(J, sh.tab, z.r + 1, false);
         const ListOut lo = list_out(J, iter + 1);
-        if (in_smem) {
+        if (nb_next > kBktMaxBuckets) {
+            write_next_direct(v, total, a, nb_next, lo, N, sh);
+        } else if (in_smem) {
             write_next_smem(total, a, nb_next, lo, N, sh, smem);
         } else {
             BScratch gs;
@@ -1276,7 +1465,7 @@ EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_
             P = __ldcg(&m.n) - S;
             E = P ? __ldcg(&m.edges) : 0;
             C = __ldcg(&m.cands);
-            nb = r == r0 ? bkt_count(x.n_in, x.wave) : bkt_count(__ldcg(&x.meta[r - 1].n), x.wave);
+            nb = r == r0 ? bkt_count(x.n_in, x.wave, x.mean) : bkt_count(__ldcg(&x.meta[r - 1].n), x.wave, x.mean);
         }
         uint64_t e_all, bytes;
         const uint64_t e0 = block_exclusive_scan<kT, uint64_t>(E, sh.scan64, &e_all);
@@ -1316,29 +1505,34 @@ EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_
             if (!Eq) continue;
             const uint32_t nbq = (uint32_t)rnb[q - r0];
             const BktSpan *sp = x.spans + (uint64_t)(q - r0) * x.nb_max;
-            uint64_t run = 0;
-            for (uint32_t b0 = 0; b0 < nbq; b0 += kT) {
-                const uint32_t b = b0 + threadIdx.x;
-                const uint64_t c = b < nbq ? __ldcg(&sp[b].cnt) : 0;
-                uint64_t tot;
-                const uint64_t ex = block_exclusive_scan<kT, uint64_t>(c, sh.scan64, &tot);
-                if (b < nbq) dest[b] = run + ex;
-                run += tot;
-            }
-            if (threadIdx.x == 0) dest[nbq] = run;
-            __syncthreads();
-            for (uint64_t e = threadIdx.x; e < Eq; e += kT) {
-                uint32_t lo = 0, hi = nbq;  // last bucket with dest <= e
-                while (hi - lo > 1) {
-                    const uint32_t m = (lo + hi) >> 1;
-                    if (dest[m] <= e) lo = m;
-                    else hi = m;
+            uint64_t run = 0;  // edges of the buckets before the chunk
+            for (uint32_t c0 = 0; c0 < nbq; c0 += kBktMaxBuckets) {  // chunks of buckets: dest fits shared memory
+                const uint32_t cn = nbq - c0 < kBktMaxBuckets ? nbq - c0 : kBktMaxBuckets;
+                uint64_t crun = run;
+                for (uint32_t b0 = 0; b0 < cn; b0 += kT) {
+                    const uint32_t b = b0 + threadIdx.x;
+                    const uint64_t c = b < cn ? __ldcg(&sp[c0 + b].cnt) : 0;
+                    uint64_t tot;
+                    const uint64_t ex = block_exclusive_scan<kT, uint64_t>(c, sh.scan64, &tot);
+                    if (b < cn) dest[b] = crun + ex;
+                    crun += tot;
                 }
-                const uint64_t src = __ldcg(&sp[lo].off) + (e - dest[lo]);
-                from[e] = __ldcg(x.sfrom + src);
-                to[e] = __ldcg(x.sto + src);
+                if (threadIdx.x == 0) dest[cn] = crun;
+                __syncthreads();
+                for (uint64_t e = run + threadIdx.x; e < crun; e += kT) {
+                    uint32_t lo = 0, hi = cn;  // last bucket of the chunk with dest <= e
+                    while (hi - lo > 1) {
+                        const uint32_t m = (lo + hi) >> 1;
+                        if (dest[m] <= e) lo = m;
+                        else hi = m;
+                    }
+                    const uint64_t src = __ldcg(&sp[c0 + lo].off) + (e - dest[lo]);
+                    from[e] = __ldcg(x.sfrom + src);
+                    to[e] = __ldcg(x.sto + src);
+                }
+                __syncthreads();
+                run = crun;
             }
-            __syncthreads();
         }
         __syncthreads();
     }

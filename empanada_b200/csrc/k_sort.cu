@@ -18,6 +18,8 @@
 //            memory, one contiguous run per digit.
 // The element count is read from device memory and no step needs the host,
 // so a sort is a fixed sequence of launches (it can be captured in a graph).
+#include <atomic>
+
 #include "sort_block.cuh"
 
 namespace emp {
@@ -95,23 +97,36 @@ __global__ void __launch_bounds__(kBlkThreads, 2) onesweep_kernel(
     }
 }
 
-static int g_setup_device = -1;
-static int g_sm_count = 148;
-static int onesweep_ctas_per_sm = 2;
-
-static void sort_setup() {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev == g_setup_device) return;
+// Persistent onesweep grid of a device: SMs x resident CTAs per SM.  Found
+// once per device (the first call sets the kernels' shared-memory
+// attributes) and kept in a per-device atomic, so host threads driving
+// different devices neither race nor see each other's grid.
+static unsigned sort_grid_find(int dev) {
     cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOnesweepSmem);
     cudaFuncSetAttribute(small_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlockSortSmem);
-    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
-    int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, onesweep_kernel, kBlkThreads, kOnesweepSmem) ==
-            cudaSuccess && occ > 0)
-        onesweep_ctas_per_sm = occ;
+    int sms = 148, occ = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, onesweep_kernel, kBlkThreads, kOnesweepSmem) !=
+            cudaSuccess || occ < 1)
+        occ = 1;
     cudaGetLastError();
-    g_setup_device = dev;
+    return (unsigned)(sms > 0 ? sms : 148) * (unsigned)occ;
+}
+
+static unsigned sort_setup() {
+    constexpr int kDevs = 64;
+    static std::atomic<unsigned> grid[kDevs] = {};  // 0: not found yet
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) {
+        cudaGetLastError();
+        return sort_grid_find(dev < 0 ? 0 : dev);
+    }
+    unsigned g = grid[dev].load(std::memory_order_acquire);
+    if (g == 0) {
+        g = sort_grid_find(dev);
+        grid[dev].store(g, std::memory_order_release);
+    }
+    return g;
 }
 
 void launch_sort_prepare(SortScratch *sc, bool zero_hist, cudaStream_t s) {
@@ -121,11 +136,10 @@ void launch_sort_prepare(SortScratch *sc, bool zero_hist, cudaStream_t s) {
 
 static void launch_sort_body(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, const uint64_t *n_dev,
                              uint64_t n_max, SortScratch *sc, uint32_t *err, cudaStream_t s, cudaEvent_t *ev) {
-    sort_setup();
+    const uint64_t cap = sort_setup();
     const uint64_t tiles = sort_tiles(n_max < 1 ? 1 : n_max);
     const uint64_t hb = (n_max + 255) / 256;
     const unsigned hblocks = (unsigned)(hb < 1 ? 1 : (hb < 148 * 4 ? hb : 148 * 4));
-    const uint64_t cap = (uint64_t)g_sm_count * onesweep_ctas_per_sm;
     const unsigned grid = (unsigned)(tiles < cap ? tiles : cap);
     count_launch(2 + kSortPasses);
     sort_hist_kernel<<<hblocks, 256, 0, s>>>(k0, v0, n_dev, sc);

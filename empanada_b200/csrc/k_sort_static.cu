@@ -62,8 +62,8 @@ emp_status static_scratch(uint8_t **out) {
 extern "C" emp_status emp_sort_pairs_static(uint64_t *d_keys, uint32_t *d_vals, uint64_t n, void *stream) {
     using namespace emp;
     if (n > kStaticMaxPairs) return EMP_E_INVAL;
+    if (n && (!d_keys || !d_vals)) return EMP_E_INVAL;  // the argument check of emp_sort_pairs
     if (n < 2) return EMP_OK;
-    if (!d_keys || !d_vals) return EMP_E_INVAL;
     uint8_t *base = nullptr;
     const emp_status rc = static_scratch(&base);
     if (rc != EMP_OK) return rc;

@@ -141,85 +141,17 @@ struct SearchPart {
 void launch_search_partitions(const uint64_t *akeys, uint64_t S, const uint64_t *bkeys, uint64_t P, uint64_t h,
                               const uint32_t *apos, const uint64_t *offs, uint64_t E, SearchPart *parts,
                               uint64_t cap, uint64_t *count, uint32_t *err, cudaStream_t s);
-// ---- device-resident round pipeline (k_pipeline.cu) ----------------------
-struct RoundCtl {
-    uint64_t n;        // entries of the current list (suffixes then prefixes)
-    uint64_t s;        // of which suffixes
-    uint64_t n_next;   // after this round's update
-    uint64_t s_next;
-    uint64_t c;        // candidates of this round
-    uint64_t e_round;  // edges of this round
-    uint64_t e_total;  // edges of all finished pipeline rounds
-    uint32_t round;    // round being run
-    uint32_t done;     // loop finished (suffix table empty or all rounds run)
-    uint32_t cur;      // list buffer holding the current list
-    uint32_t overflow; // the edge buffer was too small
-    uint32_t rounds;   // L - o
-    uint32_t bloom_bits;  // log2 of the Bloom filter size in use this round
-    uint32_t tile_ctr[8];
-};
+// ---- per-round counts of the all-rounds kernel --------------------------
 struct RoundRecord {
     uint64_t S, P, E, e0;  // table sizes, edges, first edge of the round
-    uint64_t C;            // candidates sorted (cooperative kernels only)
+    uint64_t C;            // entries found in both tables (ranked and joined)
     uint64_t nb;           // key buckets of the round (bucket kernel only)
 };
-struct PipeArgs {
-    RoundCtl *ctl;
-    RoundRecord *records;
-    uint64_t *lk0, *lk1;
-    uint32_t *lv0, *lv1;
-    uint8_t *used_s, *used_p;
-    const uint32_t *cols;
-    uint64_t wpc;
-    const HashTables *tables;
-    int L;
-    int bloom_bits_max;  // the filters hold 2^bloom_bits_max bits each
-    uint32_t *bloom_s, *bloom_p;
-    SortScratch *sort;   // scratch of the candidate sort
-    uint64_t *ck, *ck2;
-    uint32_t *cv, *cv2;
-    uint32_t *cnt;
-    uint64_t *offs;
-    uint32_t *efrom, *eto;
-    uint64_t ecap;
-    uint64_t *st_upd, *st_cand, *st_scan;  // epoch-tagged look-back words
-    uint32_t *err;
-};
-// Enqueue one round.  n_max bounds the list size, cand_max the candidates.
-// upd_events (optional, 2 events) bracket the update kernel.
-// The Bloom filters must start zeroed and a.sort prepared (launch_sort_prepare)
-// before the first round; every round leaves both ready for the next.
-void launch_pipeline_round(const PipeArgs &a, uint64_t n_max, uint64_t cand_max, cudaStream_t s,
-                           cudaEvent_t *upd_events = nullptr);
-
-// ---- cooperative multi-job rounds (k_coop.cu) -----------------------------
+// ---- cooperative multi-job launches (k_bucket.cu) --------------------------
 constexpr int kCoopMaxJobs = 1024;
 constexpr uint32_t kCoopTile = 4096;  // entries per tile in every phase
 __host__ __device__ inline uint64_t coop_tiles(uint64_t n) { return (n + kCoopTile - 1) / kCoopTile; }
-enum CoopSortMode : uint32_t { kSortNone = 0, kSortSmall = 1, kSortMsd = 2, kSortLsd = 3, kSortRank = 4 };
-struct CoopJob {
-    // fixed for the run (filled by the host)
-    uint64_t *lk[2];
-    uint32_t *lv[2];
-    uint8_t *used_s, *used_p;
-    const uint32_t *cols;
-    uint64_t wpc;
-    const HashTables *tables;
-    int32_t L, rounds;
-    uint32_t *bloom_s, *bloom_p;
-    int32_t bloom_bits_max, pad0;
-    uint64_t *ck, *ck2;  // candidates, n_max capacity
-    uint32_t *cv, *cv2;
-    uint32_t *efrom, *eto;
-    uint64_t ecap;
-    RoundRecord *records;
-    uint64_t *st_upd, *st_cand, *st_join, *st_sort;  // look-back words (zeroed before the launch)
-    // device-updated state (the host sets n, round, cur, bloom_bits[0]; zeroes the rest)
-    uint64_t n, n_next, s_next, c, e_round, e_total;
-    uint32_t round, done, cur, overflow, mode, cand_done, join_done, pad1;
-    uint32_t bloom_bits[2];        // filter size of the kernel's even / odd iterations
-    uint32_t hist[9][kSortRadix];  // candidate sort-key digits 0..7 and the top-8-bit digit
-};
+constexpr uint64_t kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;  // default limit of a grid-barrier wait
 struct CoopCtl {
     uint32_t njobs;
     uint32_t active;    // jobs not finished (the host sets njobs)
@@ -236,45 +168,41 @@ struct CoopCtl {
     uint64_t *probe;      // optional: kCoopProbePoints stamps per CTA (profiling)
     uint32_t iter_cap;    // bucket kernel: iterations this launch runs at most (0: until every job is done)
     uint32_t iters;       // bucket kernel: iterations it ran
+    uint64_t wait_ns;     // limit of each grid-barrier wait (0: kBarrierTimeoutNs)
+    uint32_t bar_extra;   // testing: added to every barrier's target, so that no arrival completes one
+    uint32_t pad2;
 };
 constexpr int kCoopTracePhases = 8;
 constexpr int kCoopProbePoints = 32;
-constexpr uint32_t kCoopMaxSubs = 4;  // a streaming tile holds up to 4 x 4096 entries (staged in shared memory)
-// Shared memory and grid of the cooperative kernel on the current device
-// (0 when it cannot run cooperatively there).
-size_t coop_smem_bytes();
-int coop_grid_size();
-// Run every remaining round of every job in one cooperative launch.
-cudaError_t launch_coop_rounds(CoopJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
-
 // ---- bucket rounds (k_bucket.cu) ------------------------------------------
-// A list of 16-byte entries lives as tiles, each tile partitioned into
-// (key bucket, table) bins.  A prologue partitions the launch's input list;
-// then each round gives each key bucket to one CTA, which gathers the
-// bucket's piece of every tile, finds the keys present in both tables with a
-// hash set, sorts and joins those entries, drops the used ones, applies the
-// next round's hash step to the rest and writes them as one tile of the next
-// round's list.  One grid barrier per round; output space comes from one
-// atomic per tile, and the edges are put in bucket order once all rounds are
-// done.
+// A round's list of 16-byte entries is kept as one region per (key bucket,
+// table) bin.  A prologue bins the launch's input list; then each round gives
+// each key bucket to one CTA, which stages the bucket's two regions, finds
+// the keys present in both tables, ranks and joins those entries, drops the
+// used ones, applies the next round's hash step to the rest and writes them
+// into the next round's bins (positions reserved from per-bin counters).  One
+// grid barrier per round; the edges are put in bucket order once all rounds
+// are done.
 struct BktEntry {
     uint64_t key;   // fp1 << 32 | fp2
     uint32_t val;   // rid | table << 31
     uint32_t word;  // cached 16 bases (one seq2 word) of the entry's read
 };
 constexpr uint32_t kBktTile = 4096;               // entries per prologue tile
-constexpr uint64_t kBktMean = 6700;               // entries per bucket aimed at (mean; 5.7 sigma below the staging limit)
-constexpr uint32_t kBktMaxBuckets = 4096;
-constexpr uint64_t kBktMaxEntries = 16ull << 20;  // larger lists use the other drivers
+constexpr uint32_t kBktMean = 6700;               // entries per bucket aimed at (mean; 5.7 sigma below the staging limit)
+constexpr uint32_t kBktMeanMin = 1024;            // tuning range of the mean
+constexpr uint32_t kBktMaxBuckets = 4096;         // up to this many buckets a CTA bins its entries in shared memory
+constexpr uint32_t kBktHugeBuckets = 1u << 20;    // above kBktMaxBuckets: one global atomic per run of equal bins
+constexpr uint64_t kBktMaxEntries = 320ull << 20; // larger lists run host-synchronised rounds until they fit
 __host__ __device__ inline uint64_t bkt_tiles(uint64_t n) { return (n + kBktTile - 1) / kBktTile; }
 // Buckets of a round with n entries on a grid of G CTAs: whole waves of G,
-// at most kBktMean entries each on average.  Bucket of a sort key sk: its top
+// at most `mean` entries each on average.  Bucket of a sort key sk: its top
 // 24 bits scaled to [0, nb), so bucket order is key order.
-__host__ __device__ inline uint32_t bkt_count(uint64_t n, uint32_t G) {
-    uint64_t waves = (n + (uint64_t)G * kBktMean - 1) / ((uint64_t)G * kBktMean);
+__host__ __device__ inline uint32_t bkt_count(uint64_t n, uint32_t G, uint32_t mean) {
+    uint64_t waves = (n + (uint64_t)G * mean - 1) / ((uint64_t)G * mean);
     if (waves < 1) waves = 1;
     uint64_t nb = waves * G;
-    return (uint32_t)(nb > kBktMaxBuckets ? kBktMaxBuckets : nb);
+    return (uint32_t)(nb > kBktHugeBuckets ? kBktHugeBuckets : nb);
 }
 __host__ __device__ inline uint32_t bkt_of(uint64_t sk, uint32_t nb) {
     return (uint32_t)(((sk >> 35) * (uint64_t)nb) >> 24);
@@ -316,6 +244,7 @@ struct BktJob {
     uint32_t nb_max;         // row length of spans
     uint32_t round;          // rounds run (set at the end of the launch)
     uint32_t wave;           // bucket counts are multiples of this (the grid for a job alone)
+    uint32_t mean;           // entries per bucket aimed at (bkt_count)
     uint32_t overflow;       // the edge buffer was too small
     uint32_t iter0;          // iterations run by earlier launches (0: the launch starts the job)
     uint32_t done;           // set at the end of a launch after which the job has no round left

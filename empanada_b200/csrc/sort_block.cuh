@@ -1,6 +1,6 @@
-// sort_block.cuh -- block-level pieces of the stable LSD radix sort, shared by
-// the standalone sort kernels (k_sort.cu) and the cooperative round kernel
-// (k_coop.cu).  512 threads per CTA, 8 pairs per thread, 4096-pair tiles.
+// sort_block.cuh -- block-level pieces of the stable LSD radix sort (k_sort.cu)
+// and the shared helpers of the cooperative round kernel (k_bucket.cu).
+// 512 threads per CTA, 8 pairs per thread, 4096-pair tiles.
 #pragma once
 
 #include "kernels.h"

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define EMP_ABI_VERSION 4
+#define EMP_ABI_VERSION 5
 
 typedef int emp_status;
 #define EMP_OK 0
@@ -48,7 +48,7 @@ typedef struct emp_ctx emp_ctx;
 typedef struct emp_job emp_job;
 typedef struct emp_server emp_server;
 
-/* The reference's command-line options (config.h:282-290). */
+/* The reference's command-line options (config.h:120-140). */
 typedef struct emp_params {
     int32_t min_ovlp;      /* -o, minimum overlap length (default 31) */
     uint64_t map_mem;      /* -m, bytes (default 1g); FASTQ block = map_mem/16 (main.cu:16) */
@@ -91,7 +91,7 @@ typedef struct emp_stats {
 const char *emp_status_string(emp_status st);
 int emp_abi_version(void);
 
-/* Defaults of config.h:285-289 (o=31, m=1g, r=1g, b=32m, c=64m). */
+/* Defaults of config.h:124-128 (o=31, m=1g, r=1g, b=32m, c=64m). */
 emp_status emp_params_default(emp_params *p);
 
 /* hmsize2bytes (config.h:75-100): digits with an optional k/K/m/M/g/G
@@ -104,6 +104,30 @@ emp_status emp_parse_size(const char *s, uint64_t *bytes);
  * precomputeModulos/init_match (fingerprint.cu:26-34, overlap.cu:117-127). */
 emp_status emp_ctx_create(int device, uint64_t hbm_budget_bytes, emp_ctx **out);
 emp_status emp_ctx_destroy(emp_ctx *ctx);
+
+/* Engine choices of a context; they have no counterpart in the reference.
+ * Every choice gives the same output.bin: they trade speed and memory (the
+ * autotuner, empanada_b200.tune, picks them by timing) or serve tests.  A
+ * zero field means its default.  Set them while no job of the context runs. */
+typedef struct emp_tuning {
+    int32_t round_driver;     /* 0: the bucket kernel for every round that cannot split into
+                                 several search partitions; 1: host-synchronised rounds only */
+    uint32_t bucket_mean;     /* bucket kernel: entries per key bucket aimed at, 1024..7000 (default 6700) */
+    uint32_t region_cap;      /* bucket kernel: entries per (bucket, table) region, 1..4096 (default 4096);
+                                 a region's overflow goes to a spill area */
+    uint32_t reserved0;
+    uint64_t edge_cap;        /* first edge-buffer size in edges (default: 4 per read-end, at least 2^20);
+                                 a run that needs more reruns its rounds with a larger one */
+    uint64_t wait_limit_ns;   /* time limit of every grid-barrier wait of the bucket kernel (default 20 s) */
+    int32_t block_next_wait;  /* testing: the context's next bucket-kernel launch meets a grid barrier
+                                 that no arrival completes, so its waits run out after wait_limit_ns and
+                                 the run returns EMP_E_TIMEOUT; that launch clears the flag */
+    int32_t reserved1;
+} emp_tuning;
+emp_status emp_tuning_default(emp_tuning *t);
+/* EMP_E_INVAL for a value outside its range (the context keeps its choices). */
+emp_status emp_ctx_set_tuning(emp_ctx *ctx, const emp_tuning *t);
+emp_status emp_ctx_get_tuning(emp_ctx *ctx, emp_tuning *t);
 
 /* One job = one read set with the reference's options. */
 emp_status emp_job_create(emp_ctx *ctx, const emp_params *p, emp_job **out);
@@ -224,14 +248,21 @@ emp_status emp_run_file(const char *input_path, const char *output_path, const e
  * stream: a cudaStream_t or NULL. */
 emp_status emp_sort_pairs(emp_ctx *ctx, uint64_t *d_keys, uint32_t *d_vals, uint64_t n, void *stream);
 
-/* emp_sort_pairs without any allocation (no counterpart in the reference).
- * The working set -- alternate key/value buffers, histograms, look-back
- * words, error word -- lives in one statically sized device array of this
- * library (about 12.6 MB per device), so n is limited to
- * EMP_SORT_STATIC_MAX_PAIRS; a larger n returns EMP_E_INVAL.  Runs on the
- * current device; returns after the sort has finished on `stream`.  All
- * calls on one device share that array: calls whose GPU work overlaps (other
- * streams, other host threads) race on it and give wrong results. */
+/* emp_sort_pairs without any allocation; it has no counterpart in the
+ * reference.  For callers that must not allocate device memory: a host
+ * program that owns the whole device through an arena or allocator of its
+ * own (an extra cudaMalloc would bypass its accounting, or fail once the
+ * arena holds the memory), and latency-bound loops in which cudaMalloc or
+ * cudaFree would synchronise the device.  The working set -- alternate
+ * key/value buffers, histograms, look-back words, error word -- lives in one
+ * statically sized device array of this library (about 12.6 MB, held on
+ * every device that loads the library until the process exits), so n is
+ * limited to EMP_SORT_STATIC_MAX_PAIRS; a larger n returns EMP_E_INVAL.
+ * Runs on the current device; the first call on a device looks up the
+ * array's device address (make that first call before any stream capture).
+ * Returns after the sort has finished on `stream`.  All calls on one device
+ * share the array: calls whose GPU work overlaps (other streams, other host
+ * threads) race on it and give wrong results. */
 #define EMP_SORT_STATIC_MAX_PAIRS (1u << 20)
 emp_status emp_sort_pairs_static(uint64_t *d_keys, uint32_t *d_vals, uint64_t n, void *stream);
 

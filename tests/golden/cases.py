@@ -159,6 +159,9 @@ class Case:
     edge: str | None = None     # name of an edge_* builder
     synth: dict | None = None   # empanada_b200.synth.Workload fields
     big: bool = False           # digest only (output too large to commit)
+    # options the reference itself is run with when they must differ from
+    # `args` (same output by construction; the reason is given at the case)
+    ref_args: tuple | None = None
 
     def min_ovlp(self) -> int:
         a = list(self.args)
@@ -184,6 +187,9 @@ TINY = {"seed": 101, "genome_len": 50_000, "n_reads": 3000, "read_len": 100}
 CONFIG3_TENTH = {"seed": 3, "genome_len": 10_000_000, "n_reads": 3_333_333, "read_len": 150, "repeat_frac": 0.05,
                  "rep_min_len": 1000, "rep_max_len": 5000, "rep_min_copies": 2, "rep_max_copies": 50,
                  "rep_divergence": 0.01}
+CONFIG3 = {"seed": 3, "genome_len": 100_000_000, "n_reads": 33_333_333, "read_len": 150, "repeat_frac": 0.05,
+           "rep_min_len": 1000, "rep_max_len": 5000, "rep_min_copies": 2, "rep_max_copies": 50,
+           "rep_divergence": 0.01}
 CASES = [
     Case("tiny", ("-o", "31"), synth=TINY),
     Case("tiny_m16k_b1k", ("-o", "31", "-m", "16k", "-b", "1k", "-c", "1k"), synth=TINY),
@@ -217,6 +223,19 @@ CASES = [
     # at -r 100m (M = 6.55M < 2n) the fingerprint sort goes out of core
     Case("repeats_10m_r100m", ("-o", "31", "-r", "100m"), synth=CONFIG3_TENTH, big=True),
     Case("repeats_10m", ("-o", "31"), synth=CONFIG3_TENTH, big=True),
+    # config 3 at full size: 100 Mbp genome with 5 % repeat families, 33.3M
+    # x 150 bp reads (10.5 GB FASTQ).  At -m 1g -r 1g the reference streams
+    # 64 MiB blocks and M = 64Mi pairs < 2n, so its fingerprint sort is
+    # chunked and the first rounds split into records of M/2 windows.
+    Case("config3_r1g", ("-o", "31", "-m", "1g", "-r", "1g"), synth=CONFIG3, big=True),
+    # HBM-sized: every table fits one chunk (2n <= M) and every round table
+    # fits one search window (|table| <= M/2), so the output is the same for
+    # every -r of at least 4g and any -m.  The reference's host build is run
+    # at -m 1g -r 4g: at -r 160g its match buffer (13 B x M = 130 GB,
+    # overlap.cu:120) exceeds host memory, and at -m 160g one 10 GB block
+    # overflows its int offsets (preprocess.cu:98-182).
+    Case("config3_hbm", ("-o", "31", "-m", "160g", "-r", "160g"), synth=CONFIG3, big=True,
+         ref_args=("-o", "31", "-m", "1g", "-r", "4g")),
     Case("small", ("-o", "31"), synth={}, big=True),
     Case("larger", ("-o", "75", "-m", "8g", "-r", "12g", "-b", "16m", "-c", "64m"),
          synth={"seed": 2, "genome_len": 5_000_000, "n_reads": 1_200_000, "read_len": 250, "sub_rate": 0.001},

@@ -44,10 +44,13 @@ def main(names: list[str]) -> int:
             with open(inp, "wb") as f:
                 f.write(data)
             t0 = time.time()
-            p = bind.run_reference_cpu(inp, out, list(case.args), cwd=td)
+            ref_args = list(case.ref_args or case.args)
+            p = bind.run_reference_cpu(inp, out, ref_args, cwd=td)
             dt = time.time() - t0
             rec = {"args": list(case.args), "fastq_sha256": hashlib.sha256(data).hexdigest(),
                    "fastq_size": len(data), "reference_exit": p.returncode, "reference_seconds": round(dt, 2)}
+            if case.ref_args:
+                rec["reference_args"] = ref_args
             if p.returncode == 0 and os.path.exists(out):
                 ref = open(out, "rb").read()
                 rec["sha256"] = hashlib.sha256(ref).hexdigest()

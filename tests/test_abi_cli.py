@@ -33,7 +33,7 @@ def test_header_declarations_are_exported():
 
 def test_abi_version_and_status_strings():
     lib = _native.lib()
-    assert lib.emp_abi_version() == 4
+    assert lib.emp_abi_version() == 5
     for code in range(0, -10, -1):
         assert lib.emp_status_string(code)
     assert _native.status_string(_native.EMP_E_FORMAT).startswith("reads of unequal length")
@@ -44,6 +44,19 @@ def test_params_default_matches_config_h():
     assert _native.lib().emp_params_default(ctypes.byref(p)) == 0
     assert (p.min_ovlp, p.map_mem, p.reduce_mem, p.base_blocksz, p.kv_chunksz) == (31, 1 << 30, 1 << 30, 32 << 20,
                                                                                    64 << 20)
+
+
+def test_tuning_defaults_and_validation_without_a_gpu():
+    """emp_tuning_default fills every choice; the context setters reject a
+    missing context before touching a device."""
+    t = _native.Tuning()
+    lib = _native.lib()
+    assert lib.emp_tuning_default(ctypes.byref(t)) == 0
+    assert t.to_dict() == {"round_driver": 0, "bucket_mean": 6700, "region_cap": 4096, "edge_cap": 0,
+                           "wait_limit_ns": 20_000_000_000, "block_next_wait": 0}
+    assert lib.emp_tuning_default(None) == _native.EMP_E_INVAL
+    assert lib.emp_ctx_set_tuning(None, ctypes.byref(t)) == _native.EMP_E_INVAL
+    assert lib.emp_ctx_get_tuning(None, ctypes.byref(t)) == _native.EMP_E_INVAL
 
 
 @pytest.mark.parametrize("s,v", [("31", 31), ("0", 0), ("1k", 1024), ("1K", 1024), ("16m", 16 << 20),

@@ -75,13 +75,13 @@ def test_batch_failure_leaves_other_jobs(engine):
 
 
 @pytest.mark.gpu
-def test_batch_edge_restart(engine, monkeypatch):
+def test_batch_edge_restart(engine):
     """Edge buffers too small for every job: each runs again alone."""
-    monkeypatch.setenv("EMP_EDGE_CAP", "7")
     names = ["tiny", "sub_errors", "dups_palindromes", "read_len_255"]
     jobs = [_job(engine, BY_NAME[n]) for n in names]
     try:
-        engine.run_batch(jobs)
+        with engine.tuned(edge_cap=8):
+            engine.run_batch(jobs)
         for name, job in zip(names, jobs):
             assert _digest(job) == GOLDEN[name]["sha256"], name
     finally:

@@ -4,6 +4,7 @@ Every case of tests/golden/cases.py runs through the C ABI (emp_job_*); the
 output.bin bytes must equal the reference's (sha256 from golden.json, and the
 verbatim fixture where committed) and the oracle's.
 """
+import dataclasses
 import hashlib
 import json
 import os
@@ -66,45 +67,106 @@ def test_full_size_workload_matches_reference(engine, name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["tiny", "sub_errors", "dups_palindromes", "split_r128k", "read_len_1"])
-@pytest.mark.parametrize("mode", ["sync_rounds", "graph_rounds", "coop_rounds", "edge_restart", "graph_edge_restart",
-                                  "coop_edge_restart", "region_spill", "region_spill_some"])
-def test_round_paths_agree(engine, monkeypatch, name, mode):
-    """Every round driver gives the reference's bytes: host-synchronised
-    rounds (full sort per round), the per-round graph pipeline, the Bloom-
-    filter cooperative kernel, and each device-resident driver restarted
-    after an edge-buffer overflow (the default driver is the bucket kernel);
-    and the bucket kernel with list regions so small that most (or some)
-    entries go to the spill area."""
-    if mode == "region_spill":
-        monkeypatch.setenv("EMP_BKT_REGION_CAP", "7")
-    if mode == "region_spill_some":
-        monkeypatch.setenv("EMP_BKT_REGION_CAP", "40")
-    if mode == "sync_rounds":
-        monkeypatch.setenv("EMP_SYNC_ROUNDS", "1")
-    if mode.startswith("graph"):
-        monkeypatch.setenv("EMP_NO_COOP", "1")
-    if mode.startswith("coop"):
-        monkeypatch.setenv("EMP_NO_BUCKET", "1")
-    if mode.endswith("edge_restart"):
-        monkeypatch.setenv("EMP_EDGE_CAP", "7")
+@pytest.mark.parametrize("name", ["config3_hbm", "config3_r1g"])
+def test_config3_full_size_matches_reference(engine, name):
+    """Config 3 at full size (100 Mbp genome with 5 % repeat families, 33.3M
+    x 150 bp reads, 10.5 GB of FASTQ): HBM-sized (-m 160g -r 160g, every
+    table in one chunk and one search window) and -m 1g -r 1g (the
+    fingerprint sort chunked, the first rounds split into records of M/2
+    windows).  output.bin must equal the reference's byte for byte."""
+    import numpy as np
+
+    from empanada_b200 import synth
+
     case = BY_NAME[name]
-    data, out, st = _run(engine, case)
+    g = GOLDEN.get(name)
+    if not g or "sha256" not in g:
+        pytest.fail(f"no golden digest for {name}: run tests/golden/make_golden.py {name}")
+    w = dataclasses.replace(synth.SMALL, **case.synth)
+    buf = np.empty(synth.fastq_size(w), dtype=np.uint8)
+    synth.fastq_into(w, buf)
+    assert buf.size == g["fastq_size"]
+    a = list(case.args)
+    opts = dict(zip(a[::2], a[1::2]))
+    with engine.job(min_ovlp=int(opts["-o"]), map_mem=opts["-m"], reduce_mem=opts["-r"]) as job:
+        job.feed(buf)
+        del buf
+        job.run()
+        st = job.stats()
+        out = job.output()
+    assert st["n_edges"] == g["edges"]
+    assert st["n_records"] == g["records"]
+    assert len(out) == g["size"]
+    assert hashlib.sha256(out).hexdigest() == g["sha256"]
+
+
+ROUND_MODES = {
+    "default": {},
+    "sync_rounds": {"round_driver": 1},
+    "edge_restart": {"edge_cap": 8},
+    "sync_edge_restart": {"round_driver": 1, "edge_cap": 8},
+    "region_spill": {"region_cap": 7},
+    "region_spill_some": {"region_cap": 40},
+    "small_buckets": {"bucket_mean": 1024},
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["tiny", "sub_errors", "dups_palindromes", "split_r128k", "read_len_1"])
+@pytest.mark.parametrize("mode", sorted(ROUND_MODES))
+def test_round_paths_agree(engine, name, mode):
+    """Every round driver and engine choice gives the reference's bytes:
+    host-synchronised rounds (full sort per round), the bucket kernel (the
+    default), each restarted after an edge-buffer overflow, the bucket kernel
+    with list regions so small that most (or some) entries go to the spill
+    area, and with smaller buckets."""
+    case = BY_NAME[name]
+    with engine.tuned(**ROUND_MODES[mode]):
+        data, out, st = _run(engine, case)
     assert hashlib.sha256(out).hexdigest() == GOLDEN[name]["sha256"]
+
+
+@pytest.mark.gpu
+def test_many_buckets_direct_binning(engine):
+    """More than 4096 key buckets in a round (the 1.2M x 250 bp workload at
+    1024 entries per bucket): entries take their list positions straight from
+    the bin counters instead of a shared-memory histogram."""
+    case = BY_NAME["larger"]
+    with engine.tuned(bucket_mean=1024):
+        data, out, st = _run(engine, case)
+    assert hashlib.sha256(out).hexdigest() == GOLDEN["larger"]["sha256"]
+
+
+@pytest.mark.gpu
+def test_grid_barrier_timeout_is_reported(engine):
+    """A grid-barrier wait that runs out (a barrier no arrival completes,
+    with a 2 ms limit) ends the launch with EMP_E_TIMEOUT on the host; the
+    engine then runs the same job, and another, correctly."""
+    case = BY_NAME["tiny"]
+    with engine.tuned(wait_limit_ns=2_000_000, block_next_wait=1):
+        with engine.job(min_ovlp=case.min_ovlp()) as job:
+            job.feed(case.fastq())
+            with pytest.raises(empanada_b200._native.EmpError) as e:
+                job.run()
+            assert e.value.code == empanada_b200._native.EMP_E_TIMEOUT
+            assert engine.tuning()["block_next_wait"] == 0  # used up by that launch
+            job.reset()
+            job.feed(case.fastq())
+            job.run()
+            assert hashlib.sha256(job.output()).hexdigest() == GOLDEN["tiny"]["sha256"]
+    data, out, st = _run(engine, BY_NAME["sub_errors"])
+    assert hashlib.sha256(out).hexdigest() == GOLDEN["sub_errors"]["sha256"]
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", OUT_OF_CORE)
 @pytest.mark.parametrize("mode", ["default", "sync_rounds", "edge_restart"])
-def test_out_of_core_order(engine, monkeypatch, name, mode):
+def test_out_of_core_order(engine, name, mode):
     """2n > M: the reference's chunked sort (M-entry chunks merged through a
     FIFO) decides the duplicate survivors and the tie order of the large
     rounds; every round driver gives the reference's bytes."""
-    if mode == "sync_rounds":
-        monkeypatch.setenv("EMP_SYNC_ROUNDS", "1")
-    if mode == "edge_restart":
-        monkeypatch.setenv("EMP_EDGE_CAP", "7")
-    data, out, st = _run(engine, BY_NAME[name])
+    with engine.tuned(**ROUND_MODES[mode]):
+        data, out, st = _run(engine, BY_NAME[name])
     g = GOLDEN[name]
     assert hashlib.sha256(out).hexdigest() == g["sha256"]
     assert st["n_unique"] == g["unique"]
@@ -148,17 +210,12 @@ def test_long_reads_match_oracle(engine, L, o):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["sync_rounds", "graph_rounds", "coop_rounds", "split_r64k"])
-def test_long_reads_round_paths(engine, monkeypatch, mode):
-    if mode == "sync_rounds":
-        monkeypatch.setenv("EMP_SYNC_ROUNDS", "1")
-    if mode == "graph_rounds":
-        monkeypatch.setenv("EMP_NO_COOP", "1")
-    if mode == "coop_rounds":
-        monkeypatch.setenv("EMP_NO_BUCKET", "1")
+@pytest.mark.parametrize("mode", ["sync_rounds", "small_buckets", "split_r64k"])
+def test_long_reads_round_paths(engine, mode):
     r = 64 << 10 if mode == "split_r64k" else 1 << 30
     data = _long_reads(300, 2500, seed=7)
-    out, _ = empanada_b200.run_bytes(data, engine=engine, min_ovlp=40, reduce_mem=r)
+    with engine.tuned(**ROUND_MODES.get(mode, {})):
+        out, _ = empanada_b200.run_bytes(data, engine=engine, min_ovlp=40, reduce_mem=r)
     ref, _ = bind.run(data, 40, r)
     assert out == ref
 

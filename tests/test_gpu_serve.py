@@ -142,16 +142,15 @@ def test_served_mix_equals_alone(engine):
 
 
 @pytest.mark.gpu
-def test_served_failure_and_edge_restart(engine, monkeypatch):
+def test_served_failure_and_edge_restart(engine):
     """A failing job completes with its status; jobs whose edge buffer
     overflows run again alone; the others are unaffected."""
     import cases
 
-    monkeypatch.setenv("EMP_EDGE_CAP", "7")
     bad = engine.job(min_ovlp=20, reduce_mem="16k")
     bad.feed(cases.edge_ooc_hang())
     good = [_job(engine, n) for n in ("tiny", "sub_errors", "read_len_255")]
-    with empanada_b200.Server(engine, rounds_per_launch=4) as srv:
+    with engine.tuned(edge_cap=8), empanada_b200.Server(engine, rounds_per_launch=4) as srv:
         srv.submit(good[0])
         srv.submit(bad)
         srv.step()
