@@ -624,16 +624,22 @@ EMP_COLD void match_smem(uint32_t total, uint32_t S, uint8_t *smem) {
     __syncthreads();
 }
 
-// Cheaper matcher for the usual bucket, where few entries match: a 2-bit
-// Bloom filter of the suffix keys (128K bits) passes a few prefixes; a second
-// filter of those prefixes' keys passes a few suffixes; the two short lists
-// are compared in full.  No entry that matches is filtered out, so the flags
-// equal match_smem's.  Returns false (flags untouched) when the lists would
-// be long; the caller then uses match_smem.
+// Cheaper matcher for the usual bucket, where at most a third of the entries
+// match: a 2-bit Bloom filter of the suffix keys (128K bits) passes the
+// prefixes that may match; a second filter of those prefixes' keys passes
+// the suffixes that may match; the two short lists are then matched through
+// a small hash set of the suffix list's keys.  No entry that matches is
+// filtered out, so the flags equal match_smem's.  Returns false (flags
+// untouched) when a list would be longer than kListMax; the caller then uses
+// match_smem.
 constexpr uint32_t kFilterWords = 4096;  // 128K bits per filter
-constexpr uint32_t kListMax = 1024;
+constexpr uint32_t kListMax = 2048;
+constexpr uint32_t kListHash = 8192;     // slots of the short lists' hash set (power of two)
 constexpr size_t kFBm1 = 0, kFBm2 = kFilterWords * 4, kFPl = 2 * kFilterWords * 4, kFSl = kFPl + kListMax * 2;
-static_assert(kFSl + kListMax * 2 <= kRegion, "filters and lists fit the region");
+constexpr size_t kFHash = kFSl + kListMax * 2;      // u32 [kListHash]: suffix-list index, bit 31 matched
+constexpr size_t kFSlotOf = kFHash + kListHash * 4; // u16 [kListMax]: the slot of each suffix-list entry
+static_assert(kFSlotOf + kListMax * 2 <= kRegion, "filters, lists and their hash set fit the region");
+static_assert(kListMax < kListHash && kListMax <= 65536, "the hash set never fills; u16 list indices");
 
 EMP_DEV void filter_bits(uint64_t key, uint32_t &b1, uint32_t &b2) {
     const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 32);
@@ -707,19 +713,43 @@ EMP_DEV bool match_filter(uint32_t total, uint32_t S, uint8_t *smem, BShared &sh
     __syncthreads();
     const uint32_t ns = sh.tile;
     if (ns > kListMax) return false;
-    for (uint32_t i = threadIdx.x; i < np; i += kT) {  // the two lists in full
-        const uint32_t xp = pl[i];
-        const uint64_t kp = key[xp];
-        bool hit = false;
-        for (uint32_t j = 0; j < ns; ++j) {
-            const uint32_t xs = sl[j];
-            if (key[xs] == kp) {
-                flag[xs] = kMatched;
-                hit = true;
-            }
+    // the two lists: suffix-list keys into a hash set (equal keys share the
+    // slot of the first one in), prefixes probe it, then every suffix of a
+    // slot that a prefix hit is flagged
+    uint32_t *hs = reinterpret_cast<uint32_t *>(reg + kFHash);
+    uint16_t *slot_of = reinterpret_cast<uint16_t *>(reg + kFSlotOf);
+    for (uint32_t i = threadIdx.x; i < kListHash / 4; i += kT)
+        reinterpret_cast<uint4 *>(hs)[i] = make_uint4(kSlotEmpty, kSlotEmpty, kSlotEmpty, kSlotEmpty);
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < ns; j += kT) {
+        const uint64_t k = key[sl[j]];
+        uint32_t sl0 = (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> 32) & (kListHash - 1);
+        for (uint32_t probes = 0; probes < kListHash; ++probes) {
+            const uint32_t old = atomicCAS(hs + sl0, kSlotEmpty, j);
+            if (old == kSlotEmpty || key[sl[old & 0xffffu]] == k) break;
+            sl0 = (sl0 + 1) & (kListHash - 1);
         }
-        if (hit) flag[xp] = kMatched;
+        slot_of[j] = (uint16_t)sl0;
     }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < np; i += kT) {
+        const uint32_t xp = pl[i];
+        const uint64_t k = key[xp];
+        uint32_t sl0 = (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> 32) & (kListHash - 1);
+        for (uint32_t probes = 0; probes < kListHash; ++probes) {
+            const uint32_t w = hs[sl0];
+            if (w == kSlotEmpty) break;
+            if (key[sl[w & 0xffffu]] == k) {
+                flag[xp] = kMatched;
+                if (!(w & kSlotMatched)) atomicOr(hs + sl0, kSlotMatched);
+                break;
+            }
+            sl0 = (sl0 + 1) & (kListHash - 1);
+        }
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < ns; j += kT)
+        if (hs[slot_of[j]] & kSlotMatched) flag[sl[j]] = kMatched;
     __syncthreads();
     return true;
 }
@@ -1442,6 +1472,7 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
 // each round's record, edges from the staging buffer in bucket order (rounds
 // spread over the CTAs, no grid barrier).  Jobs that still have rounds are
 // left as they are for the next launch.
+constexpr uint32_t kPlaceChunk = kT;  // buckets per edge-placing work item (one per thread)
 EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_t *smem) {
     uint64_t *dest = reinterpret_cast<uint64_t *>(smem);  // nb + 1 bucket starts
     uint64_t *roff = dest + kBktMaxBuckets + 1;          // per round of the job: record offset,
@@ -1490,36 +1521,39 @@ EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_
         }
         __syncthreads();
         if (vld(x.overflow)) continue;
-        for (uint32_t q = r0; q < r1; ++q, ++g) {
-            if (g % gridDim.x != blockIdx.x) continue;
-            if (__ldcg(&x.meta[q].n) == __ldcg(&x.meta[q].s)) continue;  // no prefix: no record
+        // one work item per (round, chunk of kPlaceChunk buckets), spread over
+        // the CTAs: a large round's edges are placed by many CTAs at once
+        for (uint32_t q = r0; q < r1; ++q) {
+            const bool rec_q = __ldcg(&x.meta[q].n) != __ldcg(&x.meta[q].s);  // no prefix: no record
             const uint64_t Eq = rE[q - r0];
+            const uint32_t nbq = (uint32_t)rnb[q - r0];
+            const uint32_t items = rec_q ? (Eq ? (nbq + kPlaceChunk - 1) / kPlaceChunk : 1u) : 0u;
             uint8_t *o = x.out + roff[q - r0];
             uint32_t *from = reinterpret_cast<uint32_t *>(o + 12), *to = from + Eq;
-            if (threadIdx.x == 0) {  // u64 n, i32 ovlp_len (write_edges_binary, overlap.cu:148-161)
-                uint32_t *h = reinterpret_cast<uint32_t *>(o);
-                h[0] = (uint32_t)Eq;
-                h[1] = (uint32_t)(Eq >> 32);
-                h[2] = (uint32_t)(x.L - 1 - (int)q);
-            }
-            if (!Eq) continue;
-            const uint32_t nbq = (uint32_t)rnb[q - r0];
             const BktSpan *sp = x.spans + (uint64_t)(q - r0) * x.nb_max;
-            uint64_t run = 0;  // edges of the buckets before the chunk
-            for (uint32_t c0 = 0; c0 < nbq; c0 += kBktMaxBuckets) {  // chunks of buckets: dest fits shared memory
-                const uint32_t cn = nbq - c0 < kBktMaxBuckets ? nbq - c0 : kBktMaxBuckets;
-                uint64_t crun = run;
-                for (uint32_t b0 = 0; b0 < cn; b0 += kT) {
-                    const uint32_t b = b0 + threadIdx.x;
-                    const uint64_t c = b < cn ? __ldcg(&sp[c0 + b].cnt) : 0;
-                    uint64_t tot;
-                    const uint64_t ex = block_exclusive_scan<kT, uint64_t>(c, sh.scan64, &tot);
-                    if (b < cn) dest[b] = crun + ex;
-                    crun += tot;
+            for (uint32_t k = 0; k < items; ++k, ++g) {
+                if (g % gridDim.x != blockIdx.x) continue;
+                if (k == 0 && threadIdx.x == 0) {  // u64 n, i32 ovlp_len (write_edges_binary, overlap.cu:148-161)
+                    uint32_t *h = reinterpret_cast<uint32_t *>(o);
+                    h[0] = (uint32_t)Eq;
+                    h[1] = (uint32_t)(Eq >> 32);
+                    h[2] = (uint32_t)(x.L - 1 - (int)q);
                 }
-                if (threadIdx.x == 0) dest[cn] = crun;
+                if (!Eq) continue;
+                const uint32_t c0 = k * kPlaceChunk;
+                const uint32_t cn = nbq - c0 < kPlaceChunk ? nbq - c0 : kPlaceChunk;
+                uint64_t pre = 0;  // edges of the buckets before the chunk
+                for (uint32_t b = threadIdx.x; b < c0; b += kT) pre += __ldcg(&sp[b].cnt);
+                uint64_t base;
+                block_exclusive_scan<kT, uint64_t>(pre, sh.scan64, &base);
+                const uint32_t b = threadIdx.x;
+                const uint64_t c = b < cn ? __ldcg(&sp[c0 + b].cnt) : 0;
+                uint64_t tot;
+                const uint64_t ex = block_exclusive_scan<kT, uint64_t>(c, sh.scan64, &tot);
+                if (b < cn) dest[b] = base + ex;
+                if (threadIdx.x == 0) dest[cn] = base + tot;
                 __syncthreads();
-                for (uint64_t e = run + threadIdx.x; e < crun; e += kT) {
+                for (uint64_t e = base + threadIdx.x; e < base + tot; e += kT) {
                     uint32_t lo = 0, hi = cn;  // last bucket of the chunk with dest <= e
                     while (hi - lo > 1) {
                         const uint32_t m = (lo + hi) >> 1;
@@ -1531,7 +1565,6 @@ EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_
                     to[e] = __ldcg(x.sto + src);
                 }
                 __syncthreads();
-                run = crun;
             }
         }
         __syncthreads();
