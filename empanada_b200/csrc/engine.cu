@@ -169,7 +169,7 @@ struct emp_job {
     bool fed_last = false;
     double ms_h2d = 0.0;
     // work buffers
-    DevBuf tile_counts, tile_excl, status, misc, seq_start, seq_end, hq, idx, rec_of, keys0, cols, seq2;
+    DevBuf tile_counts, tile_excl, status, misc, seq_start, seq_end, keys0, cols, seq2;
     DevBuf sk0, sv0, sk1, sv1, alive, lk0, lv0, lk1, lv1, used_s, used_p, cnt, offs, efrom, eto, sort_scratch;
     DevBuf akeys, apos, bkeys, parts;  // record splitting
     DevBuf xk0, xv0, xk1, xv1, ring_k, ring_v, cparts;  // sort of a table larger than M
@@ -216,7 +216,7 @@ namespace {
 
 // misc device words (u64 slots)
 enum MiscSlot { kMiscErr = 0, kMiscTotal = 1, kMiscLen = 2, kMiscN = 3, kMiscU = 4, kMiscNout = 5, kMiscSout = 6,
-                kMiscE = 7, kMiscCtr = 8, kMiscParts = 9, kMiscSortN = 10, kMiscSlots = 16 };
+                kMiscE = 7, kMiscCtr = 8, kMiscParts = 9, kMiscSortN = 10, kMiscLen0 = 11, kMiscSlots = 16 };
 
 // internal: the pipeline's edge buffer was too small (never returned by the ABI)
 constexpr emp_status kNeedEdgeRoom = -1000;
@@ -845,7 +845,7 @@ emp_status map_begin(emp_job *j, cudaStream_t s) {
     const uint64_t T = parse_tiles(F);
     EMP_TRY(ensure(j, j->tile_counts, T * 4));
     EMP_TRY(ensure(j, j->tile_excl, T * 8));
-    launch_nl_count(j->fq.as<uint8_t>(), F, j->tile_counts.as<uint32_t>(), s);
+    launch_nl_count(j->fq.as<uint8_t>(), F, j->tile_counts.as<uint32_t>(), j->misc.as<uint64_t>() + kMiscLen0, s);
     EMP_TRY(reset_chain(j, scan_tiles(T), s));
     launch_scan_u32_u64(j->tile_counts.as<uint32_t>(), j->tile_excl.as<uint64_t>(), T, j->status.as<uint64_t>(),
                         chain_ctr(j), j->misc.as<uint64_t>() + kMiscTotal, err_word(j), s);
@@ -866,6 +866,8 @@ void map_finish_empty(emp_job *j, cudaStream_t s) {
     cudaEventRecord(j->map_ev[4], s);
     j->prep.done = true;
 }
+
+emp_status launch_reads(emp_job *j, cudaStream_t s, int wpr);
 
 emp_status map_records(emp_job *j, cudaStream_t s) {
     EMP_TRY(map_check(j));
@@ -890,17 +892,33 @@ emp_status map_records(emp_job *j, cudaStream_t s) {
         EMP_CUDA(cudaMemcpyAsync(j->seq_end.as<uint64_t>() + n_rec - 1, hm + kMiscSlots - 1, 8,
                                  cudaMemcpyHostToDevice, s));
     }
-    // ---- K2a: classify records
-    EMP_TRY(ensure(j, j->hq, n_rec * 4));
-    EMP_TRY(ensure(j, j->idx, n_rec * 4));
+    // ---- K2: every record in one pass: N filter, length, fingerprints of
+    // both read-ends, read-major 2-bit words; kept reads numbered in order.
+    // The words are laid out for the first record's length (the usual case:
+    // every read has it); map_keys runs the pass again when the kept reads'
+    // length needs another layout.
+    const uint64_t len0 = hm[kMiscLen0];
+    const int wpr = len0 >= 1 && len0 <= (uint64_t)kMaxReadLen ? (int)((len0 + 15) / 16) : kMaxReadLen / 16;
+    return launch_reads(j, s, wpr);
+}
+
+// The read pass (K2) with `wpr` read-major words per read.
+emp_status launch_reads(emp_job *j, cudaStream_t s, int wpr) {
+    uint64_t *hm = j->h_misc.as<uint64_t>();
+    uint64_t *dm = j->misc.as<uint64_t>();
+    const uint64_t n_rec = j->prep.n_rec;
+    j->prep.wpr = wpr;
+    EMP_TRY(ensure(j, j->keys0, n_rec * 16));
+    EMP_TRY(ensure(j, j->seq2, n_rec * (uint64_t)wpr * 4));
     const uint32_t mm[2] = {0xffffffffu, 0u};
     std::memcpy(hm + kMiscLen, mm, 8);
     EMP_CUDA(cudaMemcpyAsync(dm + kMiscLen, hm + kMiscLen, 8, cudaMemcpyHostToDevice, s));
-    launch_classify(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->seq_end.as<uint64_t>(), n_rec,
-                    j->hq.as<uint32_t>(), reinterpret_cast<uint32_t *>(dm + kMiscLen), err_word(j), s);
-    EMP_TRY(reset_chain(j, scan_tiles(n_rec), s));
-    launch_scan_u32_u32(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), n_rec, j->status.as<uint64_t>(), chain_ctr(j),
-                        dm + kMiscN, err_word(j), s);
+    EMP_TRY(reset_chain(j, (n_rec + kReadTileRecs - 1) / kReadTileRecs, s));
+    launch_read_hash(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->seq_end.as<uint64_t>(), n_rec,
+                     j->ctx->tables.as<HashTables>(), j->keys0.as<uint64_t>(), j->seq2.as<uint32_t>(), wpr,
+                     j->status.as<uint64_t>(), chain_ctr(j), dm + kMiscN, reinterpret_cast<uint32_t *>(dm + kMiscLen),
+                     err_word(j), s);
+    cudaEventRecord(j->map_ev[1], s);
     return EMP_OK;
 }
 
@@ -941,21 +959,18 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
     if (j->p.min_ovlp < 0) return EMP_E_INVAL;
     const uint64_t n2 = 2 * n;
     if (n2 >= (1ull << 31)) return EMP_E_UNSUPPORTED;
-    const HashTables *tables = j->ctx->tables.as<HashTables>();
-    // ---- K2b: fingerprints + 2-bit column store
+    if (q.wpr != (L + 15) / 16) {  // the kept reads are not as long as the first record: lay the words out again
+        EMP_TRY(launch_reads(j, s, (L + 15) / 16));
+        EMP_TRY(sync_and_check(j, s));
+        if (hm[kMiscErr] & kErrBadBase) return EMP_E_FORMAT;
+    }
+    // ---- column-major 2-bit store, for rounds that run outside the bucket kernel
     q.wpc = (n + 15) / 16;
-    q.wpr = (L + 15) / 16;
-    EMP_TRY(ensure(j, j->rec_of, n * 4));
-    const bool want_cols = columns_needed(j->ctx, n, q.M);
-    if (want_cols) EMP_TRY(ensure(j, j->cols, (uint64_t)L * q.wpc * 4));
-    EMP_TRY(ensure(j, j->seq2, (uint64_t)n * q.wpr * 4));
-    EMP_TRY(ensure(j, j->keys0, n2 * 8));
-    launch_scatter_hq(j->hq.as<uint32_t>(), j->idx.as<uint32_t>(), q.n_rec, j->rec_of.as<uint32_t>(), s);
-    launch_fingerprint_pack(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->rec_of.as<uint32_t>(), n, L, tables,
-                            j->keys0.as<uint64_t>(), want_cols ? j->cols.as<uint32_t>() : nullptr, q.wpc,
-                            j->seq2.as<uint32_t>(), q.wpr, s);
+    if (columns_needed(j->ctx, n, q.M)) {
+        EMP_TRY(ensure(j, j->cols, (uint64_t)L * q.wpc * 4));
+        launch_columns(j->seq2.as<uint32_t>(), n, L, q.wpr, j->cols.as<uint32_t>(), q.wpc, s);
+    }
     j->n_ends = n2;
-    cudaEventRecord(j->map_ev[1], s);
     // ---- fingerprint sort + duplicate removal (overlap.cu:212-225)
     const uint64_t cap = 2 * n2;  // both tables, each at most n2 entries
     EMP_TRY(ensure(j, j->sk0, cap * 8));
@@ -1683,7 +1698,7 @@ emp_status emp_job_destroy(emp_job *job) {
 // every device buffer of the job back to the context (its pool)
 static void release_buffers(emp_job *job) {
     DevBuf *bufs[] = {&job->fq, &job->tile_counts, &job->tile_excl, &job->status, &job->misc, &job->seq_start,
-                      &job->seq_end, &job->hq, &job->idx, &job->rec_of, &job->keys0, &job->cols, &job->seq2, &job->sk0,
+                      &job->seq_end, &job->keys0, &job->cols, &job->seq2, &job->sk0,
                       &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
                       &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
                       &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts, &job->lk_init,
