@@ -1,15 +1,15 @@
-// coop_common.cuh -- pieces shared by the cooperative persistent round
-// kernel (k_bucket.cu): 512-thread CTAs, one per SM, all
-// co-resident (cooperative launch), bounded grid barriers, tile tickets over
-// the tiles of many jobs, chunk-major tile scans.
+// coop_common.cuh -- pieces of the cooperative persistent round kernel
+// (k_bucket.cu): 256-thread CTAs, two per SM, all co-resident (cooperative
+// launch), bounded grid barriers, tile tickets over the tiles of many jobs.
 #pragma once
 
 #include "sort_block.cuh"
 
 namespace emp {
 
-constexpr int kT = kBlkThreads;         // 512
-constexpr int kC = kCoopTile / kT;      // 8 entries per thread per 4096-entry chunk
+constexpr int kT = kBktThreads;         // 256
+constexpr int kC = kBktTile / kT;       // 8 entries per thread per prologue tile
+constexpr int kTW = kT / 32;            // warps of a CTA
 
 // L1 is not coherent across SMs: everything another CTA of this launch may
 // have written (job state, lists, candidates, used marks) is read around L1,
@@ -81,103 +81,25 @@ EMP_DEV bool grid_barrier(CoopCtl *ctl, uint32_t *s_flag, uint32_t *s_gen, uint3
 
 
 
-// Tile scans in chunk-major order (element (c, thread) comes before
-// (c, thread+1) and before (c+1, any)) with two __syncthreads per tile:
-// warp ballots / shuffles per chunk, then one warp scans the 8x16 warp counts.
-EMP_DEV uint32_t tile_flag_scan(const bool (&f)[kC], uint32_t (&ex)[kC], uint32_t *s) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t lt = lanemask_lt_u32();
-    uint32_t inw[kC];
-#pragma unroll
-    for (int c = 0; c < kC; ++c) {
-        const uint32_t b = __ballot_sync(0xffffffffu, f[c]);
-        inw[c] = __popc(b & lt);
-        if (lane == 0) s[c * kBlkWarps + warp] = __popc(b);
-    }
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t a[4], sum = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            a[q] = s[lane * 4 + q];
-            sum += a[q];
-        }
-        uint32_t incl = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        uint32_t run = incl - sum;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            s[lane * 4 + q] = run;
-            run += a[q];
-        }
-        if (lane == 31) s[kC * kBlkWarps] = incl;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < kC; ++c) ex[c] = s[c * kBlkWarps + warp] + inw[c];
-    const uint32_t total = s[kC * kBlkWarps];
-    __syncthreads();  // s is reused by the next call
-    return total;
-}
-
-EMP_DEV uint64_t tile_value_scan(const uint32_t (&v)[kC], uint64_t (&ex)[kC], uint64_t *s) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t inw[kC];
-#pragma unroll
-    for (int c = 0; c < kC; ++c) {
-        uint64_t incl = v[c];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        inw[c] = incl - v[c];
-        if (lane == 31) s[c * kBlkWarps + warp] = incl;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        uint64_t a[4], sum = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            a[q] = s[lane * 4 + q];
-            sum += a[q];
-        }
-        uint64_t incl = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        uint64_t run = incl - sum;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            s[lane * 4 + q] = run;
-            run += a[q];
-        }
-        if (lane == 31) s[kC * kBlkWarps] = incl;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < kC; ++c) ex[c] = s[c * kBlkWarps + warp] + inw[c];
-    const uint64_t total = s[kC * kBlkWarps];
-    __syncthreads();
-    return total;
-}
-
 // prefix of per-job tile counts; count(j) evaluated for every job
 template <class S, class F>
 EMP_DEV uint32_t build_prefix(S &sh, int J, F count) {
-    // each thread takes two consecutive jobs (J <= 1024)
-    const int j0 = 2 * threadIdx.x, j1 = j0 + 1;
-    const uint32_t c0 = j0 < J ? count(j0) : 0u, c1 = j1 < J ? count(j1) : 0u;
+    // each thread takes kPer consecutive jobs (J <= kCoopMaxJobs)
+    constexpr int kPer = (kCoopMaxJobs + kT - 1) / kT;
+    const int j0 = kPer * threadIdx.x;
+    uint32_t c[kPer], run = 0;
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        c[q] = j0 + q < J ? count(j0 + q) : 0u;
+        run += c[q];
+    }
     uint32_t tot;
-    const uint32_t ex = block_exclusive_scan<kT, uint32_t>(c0 + c1, sh.scan32, &tot);
-    if (j0 <= J) sh.pref[j0] = ex;
-    if (j1 <= J) sh.pref[j1] = ex + c0;
+    uint32_t ex = block_exclusive_scan<kT, uint32_t>(run, sh.scan32, &tot);
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        if (j0 + q <= J) sh.pref[j0 + q] = ex;
+        ex += c[q];
+    }
     if (threadIdx.x == 0) sh.pref[J] = tot;
     __syncthreads();
     return tot;

@@ -1501,7 +1501,7 @@ emp_status emp_tuning_default(emp_tuning *t) {
 emp_status emp_ctx_set_tuning(emp_ctx *ctx, const emp_tuning *t) {
     if (!ctx || !t) return EMP_E_INVAL;
     if (t->round_driver < 0 || t->round_driver > 1) return EMP_E_INVAL;
-    if (t->bucket_mean && (t->bucket_mean < kBktMeanMin || t->bucket_mean > 7000)) return EMP_E_INVAL;
+    if (t->bucket_mean && (t->bucket_mean < kBktMeanMin || t->bucket_mean > kBktMeanMax)) return EMP_E_INVAL;
     if (t->region_cap > kBktRegionCap) return EMP_E_INVAL;
     ctx->tune = *t;
     return EMP_OK;

@@ -43,8 +43,8 @@ namespace emp {
 
 namespace {
 
-constexpr uint32_t kBStage = 7168;  // entries of a bucket staged in shared memory
-constexpr uint32_t kBHash = 16384;  // hash slots in shared memory (power of two)
+constexpr uint32_t kBStage = 3200;  // entries of a bucket staged in shared memory
+constexpr uint32_t kBHash = 8192;   // hash slots in shared memory (power of two)
 constexpr uint64_t kEmptySlot = ~0ull;  // never a key: fp1, fp2 < 2^29
 constexpr uint8_t kMatched = 1, kUsed = 2;
 
@@ -73,7 +73,8 @@ static_assert(2 * kBktMaxBuckets <= 65536, "bins fit u16");
 // prologue tile: bin counters, then the staged tile
 constexpr size_t kASmem = 2 * kBktMaxBuckets * 4 + kBktTile * sizeof(BktEntry) + kBktTile * 2;
 // end phase: one round's bucket destinations, the record offsets of a job
-constexpr size_t kESmem = (kBktMaxBuckets + 1 + 3 * kT) * 8;
+constexpr int kMaxJobRounds = 512;  // rounds of one job at most (L - o < kMaxReadLen)
+constexpr size_t kESmem = (kBktMaxBuckets + 1 + 3 * kMaxJobRounds) * 8;
 constexpr size_t kBktSmem = kRSmem > kASmem ? (kRSmem > kESmem ? kRSmem : kESmem) : kASmem;
 
 struct BShared {
@@ -86,7 +87,7 @@ struct BShared {
     const CoopCtl *pctl;  // profiling stamps from inside the steps of a tile
     uint32_t piter;
     HashTables tab;       // powers and inverses (every job of a launch shares them)
-    uint32_t shp_K[kCoopMaxJobs], shp_nb[kCoopMaxJobs], shp_nbn[kCoopMaxJobs];  // this iteration's shapes
+    uint32_t shp_nb[kCoopMaxJobs], shp_nbn[kCoopMaxJobs];  // this iteration's bucket counts
 };
 EMP_DEV void sprobe(const BShared &sh, int p) { probe(sh.pctl, sh.piter, p); }
 
@@ -539,7 +540,7 @@ EMP_COLD uint32_t gather(const BktJob &J, const ListIn li, uint32_t b, BShared &
 // through it).  A tag of all ones is never used, so kSlotEmpty is no slot.
 constexpr uint32_t kSlotEmpty = 0xffffffffu;
 constexpr uint32_t kSlotMatched = 0x80000000u;
-static_assert(kBStage <= 8192 && kBHash == 16384, "13-bit staged indices, 14-bit slot numbers");
+static_assert(kBStage <= 8192 && kBHash <= 16384, "13-bit staged indices, slot bits below the tag's");
 
 EMP_DEV void hash_tag(uint64_t key, uint32_t &slot, uint32_t &tag) {
     const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 32);
@@ -632,9 +633,9 @@ EMP_COLD void match_smem(uint32_t total, uint32_t S, uint8_t *smem) {
 // filtered out, so the flags equal match_smem's.  Returns false (flags
 // untouched) when a list would be longer than kListMax; the caller then uses
 // match_smem.
-constexpr uint32_t kFilterWords = 4096;  // 128K bits per filter
-constexpr uint32_t kListMax = 2048;
-constexpr uint32_t kListHash = 8192;     // slots of the short lists' hash set (power of two)
+constexpr uint32_t kFilterWords = 2048;  // 64K bits per filter
+constexpr uint32_t kListMax = 1024;
+constexpr uint32_t kListHash = 4096;     // slots of the short lists' hash set (power of two)
 constexpr size_t kFBm1 = 0, kFBm2 = kFilterWords * 4, kFPl = 2 * kFilterWords * 4, kFSl = kFPl + kListMax * 2;
 constexpr size_t kFHash = kFSl + kListMax * 2;      // u32 [kListHash]: suffix-list index, bit 31 matched
 constexpr size_t kFSlotOf = kFHash + kListHash * 4; // u16 [kListMax]: the slot of each suffix-list entry
@@ -644,7 +645,7 @@ static_assert(kListMax < kListHash && kListMax <= 65536, "the hash set never fil
 EMP_DEV void filter_bits(uint64_t key, uint32_t &b1, uint32_t &b2) {
     const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 32);
     b1 = h & (kFilterWords * 32 - 1);
-    b2 = (h >> 15) & (kFilterWords * 32 - 1);
+    b2 = (h >> 16) & (kFilterWords * 32 - 1);
 }
 EMP_DEV bool filter_has(const uint32_t *bm, uint32_t b1, uint32_t b2) {
     return ((bm[b1 >> 5] >> (b1 & 31)) & (bm[b2 >> 5] >> (b2 & 31)) & 1u) != 0;
@@ -895,8 +896,8 @@ EMP_DEV uint64_t join_count(const Cands &w, uint32_t c, BShared &sh) {
 // Up to kBCand matched entries of a bucket staged in shared memory are ranked
 // there, 26 bytes each in the region; their keys and values are read from the
 // stage through their staged index.
-constexpr uint32_t kBCand = 2816;
-constexpr uint32_t kFine = 1024;    // fine bins of the ranking
+constexpr uint32_t kBCand = 1408;
+constexpr uint32_t kFine = 512;     // fine bins of the ranking
 constexpr uint32_t kSmallRank = 96; // up to this many: all pairs compared
 constexpr size_t kSCx = 0;                                  // u16 staged index, compaction order
 constexpr size_t kSSk = (kSCx + kBCand * 2 + 7) / 8 * 8;    // u64 sort key
@@ -1476,8 +1477,9 @@ constexpr uint32_t kPlaceChunk = kT;  // buckets per edge-placing work item (one
 EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_t *smem) {
     uint64_t *dest = reinterpret_cast<uint64_t *>(smem);  // nb + 1 bucket starts
     uint64_t *roff = dest + kBktMaxBuckets + 1;          // per round of the job: record offset,
-    uint64_t *rE = roff + kT;                            // edge count,
-    uint64_t *rnb = rE + kT;                             // bucket count
+    uint64_t *rE = roff + kMaxJobRounds;                 // edge count,
+    uint64_t *rnb = rE + kMaxJobRounds;                  // bucket count
+    constexpr int kRPT = kMaxJobRounds / kT;             // rounds per thread
     uint32_t g = 0;
     for (int j = 0; j < J; ++j) {
         BktJob &x = jobs[j];
@@ -1485,35 +1487,54 @@ EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_
         if (blockIdx.x == 0 && threadIdx.x == 0) x.done = 1;
         const uint32_t r0 = (uint32_t)x.r0;
         // the rounds that ran: round r ran iff r < rounds and it had a suffix
-        // (build_graph's loop condition, overlap.cu:258)
-        const uint32_t r = r0 + threadIdx.x;
-        const bool ran = (int)r < x.rounds && __ldcg(&x.meta[r].s) > 0;
-        const uint32_t r1 = r0 + (uint32_t)__syncthreads_count(ran);  // rounds run form a prefix
-        uint64_t S = 0, P = 0, E = 0, C = 0, nb = 0;
-        if (r < r1) {
-            const BktRound &m = x.meta[r];
-            S = __ldcg(&m.s);
-            P = __ldcg(&m.n) - S;
-            E = P ? __ldcg(&m.edges) : 0;
-            C = __ldcg(&m.cands);
-            nb = r == r0 ? bkt_count(x.n_in, x.wave, x.mean) : bkt_count(__ldcg(&x.meta[r - 1].n), x.wave, x.mean);
+        // (build_graph's loop condition, overlap.cu:258); they form a prefix
+        uint32_t nran = 0;
+#pragma unroll
+        for (int q = 0; q < kRPT; ++q) {
+            const uint32_t r = r0 + kRPT * threadIdx.x + q;
+            nran += (int)r < x.rounds && __ldcg(&x.meta[r].s) > 0;
+        }
+        uint32_t ran_all;
+        block_exclusive_scan<kT, uint32_t>(nran, sh.scan32, &ran_all);
+        const uint32_t r1 = r0 + ran_all;
+        uint64_t P[kRPT], E[kRPT], e_my = 0, b_my = 0;
+#pragma unroll
+        for (int q = 0; q < kRPT; ++q) {
+            const uint32_t r = r0 + kRPT * threadIdx.x + q;
+            P[q] = E[q] = 0;
+            if (r < r1) {
+                const BktRound &m = x.meta[r];
+                P[q] = __ldcg(&m.n) - __ldcg(&m.s);
+                E[q] = P[q] ? __ldcg(&m.edges) : 0;
+            }
+            e_my += E[q];
+            b_my += P[q] ? 12 + 8 * E[q] : 0;
         }
         uint64_t e_all, bytes;
-        const uint64_t e0 = block_exclusive_scan<kT, uint64_t>(E, sh.scan64, &e_all);
-        const uint64_t off = block_exclusive_scan<kT, uint64_t>(P ? 12 + 8 * E : 0, sh.scan64, &bytes);
-        if (r < r1) {
-            roff[threadIdx.x] = off;
-            rE[threadIdx.x] = E;
-            rnb[threadIdx.x] = nb;
-            if (blockIdx.x == 0) {
-                RoundRecord &rec = x.records[r];
-                rec.S = S;
-                rec.P = P;
-                rec.E = E;
-                rec.e0 = e0;
-                rec.C = C;
-                rec.nb = nb;
+        uint64_t e0 = block_exclusive_scan<kT, uint64_t>(e_my, sh.scan64, &e_all);
+        uint64_t off = block_exclusive_scan<kT, uint64_t>(b_my, sh.scan64, &bytes);
+#pragma unroll
+        for (int q = 0; q < kRPT; ++q) {
+            const uint32_t r = r0 + kRPT * threadIdx.x + q;
+            if (r < r1) {
+                const BktRound &m = x.meta[r];
+                const uint64_t nb = r == r0 ? bkt_count(x.n_in, x.wave, x.mean)
+                                            : bkt_count(__ldcg(&x.meta[r - 1].n), x.wave, x.mean);
+                roff[r - r0] = off;
+                rE[r - r0] = E[q];
+                rnb[r - r0] = nb;
+                if (blockIdx.x == 0) {
+                    RoundRecord &rec = x.records[r];
+                    rec.S = __ldcg(&m.s);
+                    rec.P = P[q];
+                    rec.E = E[q];
+                    rec.e0 = e0;
+                    rec.C = __ldcg(&m.cands);
+                    rec.nb = nb;
+                }
             }
+            e0 += E[q];
+            off += P[q] ? 12 + 8 * E[q] : 0;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             x.round = r1;
@@ -1571,7 +1592,7 @@ EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_
     }
 }
 
-__global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, CoopCtl *ctl, uint32_t *) {
+__global__ void __launch_bounds__(kT, 2) bucket_rounds_kernel(BktJob *jobs, CoopCtl *ctl, uint32_t *) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ BShared sh;
     const int J = (int)ctl->njobs;
@@ -1596,7 +1617,6 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
         probe(ctl, it, 0);
         total = build_prefix(sh, J, [&](int j) -> uint32_t {
             const RoundShape z = round_shape(jobs[j], jobs[j].iter0 + it);
-            sh.shp_K[j] = z.K;
             sh.shp_nb[j] = z.nb;
             sh.shp_nbn[j] = z.nb_next;
             return z.active ? z.nb : 0u;
@@ -1608,7 +1628,6 @@ __global__ void __launch_bounds__(kT, 1) bucket_rounds_kernel(BktJob *jobs, Coop
             RoundShape z;
             z.active = true;
             z.r = jobs[j].r0 + (int)g;
-            z.K = sh.shp_K[j];
             z.nb = sh.shp_nb[j];
             z.nb_next = sh.shp_nbn[j];
             round_tile(jobs[j], b, g, z, sh, ctl, smem);
@@ -1643,7 +1662,7 @@ static int bucket_grid_size_find(int dev) {
         cudaGetLastError();
         return 0;
     }
-    return occ >= 1 ? sms : 0;  // one CTA per SM
+    return occ >= 2 ? 2 * sms : (occ >= 1 ? sms : 0);  // two CTAs per SM
 }
 
 int bucket_grid_size() {

@@ -155,8 +155,6 @@ struct RoundRecord {
 };
 // ---- cooperative multi-job launches (k_bucket.cu) --------------------------
 constexpr int kCoopMaxJobs = 1024;
-constexpr uint32_t kCoopTile = 4096;  // entries per tile in every phase
-__host__ __device__ inline uint64_t coop_tiles(uint64_t n) { return (n + kCoopTile - 1) / kCoopTile; }
 constexpr uint64_t kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;  // default limit of a grid-barrier wait
 struct CoopCtl {
     uint32_t njobs;
@@ -194,10 +192,12 @@ struct BktEntry {
     uint32_t val;   // rid | table << 31
     uint32_t word;  // cached 16 bases (one seq2 word) of the entry's read
 };
-constexpr uint32_t kBktTile = 4096;               // entries per prologue tile
-constexpr uint32_t kBktMean = 6700;               // entries per bucket aimed at (mean; 5.7 sigma below the staging limit)
-constexpr uint32_t kBktMeanMin = 1024;            // tuning range of the mean
-constexpr uint32_t kBktMaxBuckets = 4096;         // up to this many buckets a CTA bins its entries in shared memory
+constexpr int kBktThreads = 256;                  // threads of a bucket-kernel CTA (two CTAs per SM)
+constexpr uint32_t kBktTile = 2048;               // entries per prologue tile (8 per thread)
+constexpr uint32_t kBktMean = 2900;               // entries per bucket aimed at (mean; 5.5 sigma below the staging limit)
+constexpr uint32_t kBktMeanMin = 512;             // tuning range of the mean
+constexpr uint32_t kBktMeanMax = 3000;
+constexpr uint32_t kBktMaxBuckets = 2048;         // up to this many buckets a CTA bins its entries in shared memory
 constexpr uint32_t kBktHugeBuckets = 1u << 20;    // above kBktMaxBuckets: one global atomic per run of equal bins
 constexpr uint64_t kBktMaxEntries = 320ull << 20; // larger lists run host-synchronised rounds until they fit
 __host__ __device__ inline uint64_t bkt_tiles(uint64_t n) { return (n + kBktTile - 1) / kBktTile; }
@@ -259,7 +259,7 @@ struct BktJob {
     BktRound *meta;          // [rounds + 1], zeroed; round r at meta[r]
 };
 size_t bkt_scratch_bytes(uint64_t n_max);
-constexpr uint32_t kBktRegionCap = 4096;  // entries per (bucket, table) region: 12 sigma above the mean of 3350
+constexpr uint32_t kBktRegionCap = 2048;  // entries per (bucket, table) region: 15 sigma above the mean of 1450
 int bucket_grid_size();                             // 0: no cooperative launch on this device
 cudaError_t launch_bucket_rounds(BktJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
 

@@ -112,8 +112,8 @@ emp_status emp_ctx_destroy(emp_ctx *ctx);
 typedef struct emp_tuning {
     int32_t round_driver;     /* 0: the bucket kernel for every round that cannot split into
                                  several search partitions; 1: host-synchronised rounds only */
-    uint32_t bucket_mean;     /* bucket kernel: entries per key bucket aimed at, 1024..7000 (default 6700) */
-    uint32_t region_cap;      /* bucket kernel: entries per (bucket, table) region, 1..4096 (default 4096);
+    uint32_t bucket_mean;     /* bucket kernel: entries per key bucket aimed at, 512..3000 (default 2900) */
+    uint32_t region_cap;      /* bucket kernel: entries per (bucket, table) region, 1..2048 (default 2048);
                                  a region's overflow goes to a spill area */
     uint32_t reserved0;
     uint64_t edge_cap;        /* first edge-buffer size in edges (default: 4 per read-end, at least 2^20);

@@ -107,7 +107,7 @@ ROUND_MODES = {
     "sync_edge_restart": {"round_driver": 1, "edge_cap": 8},
     "region_spill": {"region_cap": 7},
     "region_spill_some": {"region_cap": 40},
-    "small_buckets": {"bucket_mean": 1024},
+    "small_buckets": {"bucket_mean": 512},
 }
 
 
@@ -128,11 +128,11 @@ def test_round_paths_agree(engine, name, mode):
 
 @pytest.mark.gpu
 def test_many_buckets_direct_binning(engine):
-    """More than 4096 key buckets in a round (the 1.2M x 250 bp workload at
-    1024 entries per bucket): entries take their list positions straight from
+    """More than 2048 key buckets in a round (the 1.2M x 250 bp workload at
+    512 entries per bucket): entries take their list positions straight from
     the bin counters instead of a shared-memory histogram."""
     case = BY_NAME["larger"]
-    with engine.tuned(bucket_mean=1024):
+    with engine.tuned(bucket_mean=512):
         data, out, st = _run(engine, case)
     assert hashlib.sha256(out).hexdigest() == GOLDEN["larger"]["sha256"]
 
