@@ -43,7 +43,7 @@ class Tuning(ctypes.Structure):
         ("round_driver", ctypes.c_int32),
         ("bucket_mean", ctypes.c_uint32),
         ("region_cap", ctypes.c_uint32),
-        ("reserved0", ctypes.c_uint32),
+        ("dedup_driver", ctypes.c_int32),
         ("edge_cap", ctypes.c_uint64),
         ("wait_limit_ns", ctypes.c_uint64),
         ("block_next_wait", ctypes.c_int32),

@@ -35,6 +35,7 @@ enum ErrBits : uint32_t {
     kErrBadBase = 2u,   // a kept read holds a byte outside ACGTacgt
     kErrCapacity = 4u,  // an output would overflow its buffer
     kErrHang = 8u,      // the reference would loop forever on this input
+    kErrDedupFull = 16u,  // a duplicate-removal bucket had too many distinct keys (the sort takes over)
 };
 
 // Powers R^i mod P for i <= kMaxReadLen and the radix inverses (fingerprint.cu:26-34,

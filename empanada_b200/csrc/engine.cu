@@ -169,7 +169,7 @@ struct emp_job {
     bool fed_last = false;
     double ms_h2d = 0.0;
     // work buffers
-    DevBuf tile_counts, tile_excl, status, misc, seq_start, seq_end, keys0, cols, seq2;
+    DevBuf tile_counts, tile_excl, status, misc, seq_start, seq_end, keys0, cols, seq2, dedup_scr;
     DevBuf sk0, sv0, sk1, sv1, alive, lk0, lv0, lk1, lv1, used_s, used_p, cnt, offs, efrom, eto, sort_scratch;
     DevBuf akeys, apos, bkeys, parts;  // record splitting
     DevBuf xk0, xv0, xk1, xv1, ring_k, ring_v, cparts;  // sort of a table larger than M
@@ -868,6 +868,7 @@ void map_finish_empty(emp_job *j, cudaStream_t s) {
 }
 
 emp_status launch_reads(emp_job *j, cudaStream_t s, int wpr);
+emp_status dedup_by_sort(emp_job *j, cudaStream_t s);
 
 emp_status map_records(emp_job *j, cudaStream_t s) {
     EMP_TRY(map_check(j));
@@ -985,6 +986,28 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
     EMP_TRY(ensure(j, j->used_s, n2));
     EMP_TRY(ensure(j, j->used_p, n2));
     EMP_TRY(ensure_sort_scratch(j, cap, s));
+    const uint32_t nbd = n2 <= q.M && j->ctx->tune.dedup_driver == 0 ? dedup_buckets(n2) : 0u;
+    bool hashed = false;
+    if (nbd) {  // in core: the smallest rid of every fingerprint survives, no sort needed
+        EMP_TRY(ensure(j, j->dedup_scr, dedup_scratch_bytes(nbd)));
+        EMP_TRY(reset_chain(j, scan_tiles(nbd), s));
+        hashed = launch_dedup_hash(j->keys0.as<uint64_t>(), n2, nbd, j->dedup_scr.p, j->sk0.as<uint64_t>(),
+                                   j->sv0.as<uint32_t>(), j->alive.as<uint8_t>(), j->status.as<uint64_t>(),
+                                   chain_ctr(j), dm + kMiscSortN, err_word(j), s);
+    }
+    if (!hashed) EMP_TRY(dedup_by_sort(j, s));
+    EMP_TRY(reset_chain(j, upd_tiles(n2), s));
+    launch_init_list(j->keys0.as<uint64_t>(), j->alive.as<uint8_t>(), n, j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(),
+                     j->status.as<uint64_t>(), chain_ctr(j), dm + kMiscU, err_word(j), s);
+    return EMP_OK;
+}
+
+// Duplicate removal through the sort of all (fingerprint, rid) pairs: the
+// reference's chunked sort when 2n > M (its merge tree picks the survivors),
+// else one stable radix sort; the first of every equal-key run survives.
+emp_status dedup_by_sort(emp_job *j, cudaStream_t s) {
+    const JobPrep &q = j->prep;
+    const uint64_t n2 = 2 * q.n;
     EMP_CUDA(cudaMemcpyAsync(j->sk0.p, j->keys0.p, n2 * 8, cudaMemcpyDeviceToDevice, s));
     launch_iota(j->sv0.as<uint32_t>(), n2, s);
     if (n2 > q.M) {  // chunked sort and its duplicate-removal walk (2n > M)
@@ -995,9 +1018,6 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
         timed_sort(j, n2, s);
     }
     launch_dedup_mark(j->sk0.as<uint64_t>(), j->sv0.as<uint32_t>(), n2, j->alive.as<uint8_t>(), s);
-    EMP_TRY(reset_chain(j, upd_tiles(n2), s));
-    launch_init_list(j->keys0.as<uint64_t>(), j->alive.as<uint8_t>(), n, j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(),
-                     j->status.as<uint64_t>(), chain_ctr(j), dm + kMiscU, err_word(j), s);
     return EMP_OK;
 }
 
@@ -1006,6 +1026,16 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
 emp_status map_list(emp_job *j, cudaStream_t s) {
     EMP_TRY(map_check(j));
     JobPrep &q = j->prep;
+    if (j->h_misc.as<uint64_t>()[kMiscErr] & kErrDedupFull) {  // a dedup bucket overflowed: sort instead
+        uint64_t *dm = j->misc.as<uint64_t>();
+        const uint32_t clear = (uint32_t)(j->h_misc.as<uint64_t>()[kMiscErr] & ~(uint64_t)kErrDedupFull);
+        EMP_CUDA(cudaMemcpyAsync(dm + kMiscErr, &clear, 4, cudaMemcpyHostToDevice, s));
+        EMP_TRY(dedup_by_sort(j, s));
+        EMP_TRY(reset_chain(j, upd_tiles(2 * q.n), s));
+        launch_init_list(j->keys0.as<uint64_t>(), j->alive.as<uint8_t>(), q.n, j->lk0.as<uint64_t>(),
+                         j->lv0.as<uint32_t>(), j->status.as<uint64_t>(), chain_ctr(j), dm + kMiscU, err_word(j), s);
+        EMP_TRY(sync_and_check(j, s));
+    }
     if (j->h_misc.as<uint64_t>()[kMiscErr] & kErrHang) return EMP_E_HANG;
     if (j->h_misc.as<uint64_t>()[kMiscErr] & kErrCapacity) return EMP_E_UNSUPPORTED;
     account_sort(j);
@@ -1500,7 +1530,7 @@ emp_status emp_tuning_default(emp_tuning *t) {
 
 emp_status emp_ctx_set_tuning(emp_ctx *ctx, const emp_tuning *t) {
     if (!ctx || !t) return EMP_E_INVAL;
-    if (t->round_driver < 0 || t->round_driver > 1) return EMP_E_INVAL;
+    if (t->round_driver < 0 || t->round_driver > 1 || t->dedup_driver < 0 || t->dedup_driver > 1) return EMP_E_INVAL;
     if (t->bucket_mean && (t->bucket_mean < kBktMeanMin || t->bucket_mean > kBktMeanMax)) return EMP_E_INVAL;
     if (t->region_cap > kBktRegionCap) return EMP_E_INVAL;
     ctx->tune = *t;
@@ -1512,6 +1542,7 @@ emp_status emp_ctx_get_tuning(emp_ctx *ctx, emp_tuning *t) {
     emp_tuning_default(t);
     const emp_tuning &c = ctx->tune;
     t->round_driver = c.round_driver;
+    t->dedup_driver = c.dedup_driver;
     if (c.bucket_mean) t->bucket_mean = c.bucket_mean;
     if (c.region_cap) t->region_cap = c.region_cap;
     t->edge_cap = c.edge_cap;
@@ -1698,7 +1729,7 @@ emp_status emp_job_destroy(emp_job *job) {
 // every device buffer of the job back to the context (its pool)
 static void release_buffers(emp_job *job) {
     DevBuf *bufs[] = {&job->fq, &job->tile_counts, &job->tile_excl, &job->status, &job->misc, &job->seq_start,
-                      &job->seq_end, &job->keys0, &job->cols, &job->seq2, &job->sk0,
+                      &job->seq_end, &job->keys0, &job->dedup_scr, &job->cols, &job->seq2, &job->sk0,
                       &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
                       &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
                       &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts, &job->lk_init,

@@ -45,6 +45,22 @@ constexpr uint64_t kReadTileRecs = 256;
 // cols[c * wpc + i/16] holds base c of read i at bits 2*(i%16)
 void launch_columns(const uint32_t *seq2, uint64_t n, int L, int wpr, uint32_t *cols, uint64_t wpc, cudaStream_t s);
 
+// ---- duplicate removal without a sort (k_dedup.cu) -------------------------
+// alive[e] = 1 iff read-end e has the smallest rid of its fingerprint (the
+// survivor of the reference's in-core sort + unique).  nb key buckets from
+// dedup_buckets(n) (0: use the sort); scratch: dedup_scratch_bytes(nb);
+// pk/pr: n pairs of room; status: scan_tiles(nb) zeroed look-back words,
+// *tile_ctr zeroed.  kErrDedupFull in *err: a bucket overflowed, use the sort.
+// Returns false when the kernels cannot run on this device.
+constexpr uint32_t kDedupMean = 4096;
+constexpr uint32_t kDedupMaxBuckets = 16384;
+constexpr uint64_t kDedupMaxEnds = (uint64_t)kDedupMaxBuckets * 6000;
+uint32_t dedup_buckets(uint64_t n);
+size_t dedup_scratch_bytes(uint32_t nb);
+bool launch_dedup_hash(const uint64_t *keys, uint64_t n, uint32_t nb, void *scratch, uint64_t *pk, uint32_t *pr,
+                       uint8_t *alive, uint64_t *status, uint32_t *tile_ctr, uint64_t *total, uint32_t *err,
+                       cudaStream_t s);
+
 // ---- radix sort (k_sort.cu) ---------------------------------------------
 constexpr int kSortBits = 8;
 constexpr int kSortRadix = 1 << kSortBits;

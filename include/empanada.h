@@ -115,7 +115,9 @@ typedef struct emp_tuning {
     uint32_t bucket_mean;     /* bucket kernel: entries per key bucket aimed at, 512..3000 (default 2900) */
     uint32_t region_cap;      /* bucket kernel: entries per (bucket, table) region, 1..2048 (default 2048);
                                  a region's overflow goes to a spill area */
-    uint32_t reserved0;
+    int32_t dedup_driver;     /* 0: duplicate removal by key buckets and hash sets where 2n <= M (the
+                                 reference's in-core survivor, the smallest rid of each fingerprint);
+                                 1: always by sorting all fingerprints */
     uint64_t edge_cap;        /* first edge-buffer size in edges (default: 4 per read-end, at least 2^20);
                                  a run that needs more reruns its rounds with a larger one */
     uint64_t wait_limit_ns;   /* time limit of every grid-barrier wait of the bucket kernel (default 20 s) */

@@ -108,6 +108,7 @@ ROUND_MODES = {
     "region_spill": {"region_cap": 7},
     "region_spill_some": {"region_cap": 40},
     "small_buckets": {"bucket_mean": 512},
+    "sort_dedup": {"dedup_driver": 1},
 }
 
 
