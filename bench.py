@@ -1,16 +1,20 @@
 #!/usr/bin/env python
 """Throughput of empanada's read-overlap path (fingerprint + sort + overlap) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload NAME]
 
-Workload: the "larger" read set (5 Mbp seeded genome, 1.2M reads x 250 bp,
-0.1 % substitutions, -o 75 -m 8g -r 12g -b 16m -c 64m), generated on the host
-by the seeded C generator.  A step is one complete job over that read set.
+Workload (default): the largest single-GPU configuration, out_of_core_hbm:
+a seeded 100 Mbp genome with 5 % repeat families (1-5 kbp copies, 2-50 each,
+1 % divergence), 33.3M error-free reads x 150 bp at 50x (10.5 GB of FASTQ),
+-o 31 with HBM-sized blocks (-m 160g -r 160g), generated on the host by the
+seeded C generator.  A step is one complete job over that read set.
+--workload larger runs the 1.2M x 250 bp set (-o 75 -m 8g -r 12g -b 16m -c 64m).
 
 impl b200 (default), one process per GPU (torchrun for N > 1; replicas only,
 each rank runs its own job, no data-path collective):
   value     reads/s with the FASTQ already in HBM: device time of emp_job_run
-            (CUDA events on the launching stream), L2 flushed before each step
+            (CUDA events on the launching stream); the FASTQ is larger than L2
+            and a 256 MB buffer is written before each step
   e2e       reads/s through the C ABI with host buffers, wall clock: read
             sets back to back on two jobs, each step issuing the next set's
             emp_job_feed_fastq_async (pinned host -> HBM on the copy engine,
@@ -23,7 +27,8 @@ each rank runs its own job, no data-path collective):
             for the next round, 8 B per edge) / its event-timed duration,
             against the measured HBM copy bandwidth
   cpu_baseline  rank 0 at N=1: the reference's own sources built as a CPU
-            program (oracle/_ref, Thrust on OpenMP) on a bounded sample
+            program (oracle/_ref, Thrust on OpenMP) on a bounded sample at the
+            workload's coverage
 impl reference: that CPU build alone, timed per step on the bounded sample
 (rank 0 only under torchrun).
 """
@@ -80,13 +85,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_summary():
-    """DRAM traffic per algorithmic byte of each profiled kernel, from the
-    committed ncu summary (profiles/traffic.json), if present."""
+def traffic_summary(workload_key: str):
+    """DRAM traffic per algorithmic byte of each kernel profiled on this
+    workload, from the committed ncu summary (profiles/traffic.json)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         try:
-            return {k: float(v["dram_bytes_per_algorithmic_byte"]) for k, v in json.load(open(p)).items()}
+            return {v["kernel"]: float(v["dram_bytes_per_algorithmic_byte"]) for v in json.load(open(p)).values()
+                    if v.get("workload_key") == workload_key}
         except Exception:
             return None
     return None
@@ -167,7 +173,7 @@ def cpu_baseline_block(workload, steps: int = 1):
     from empanada_b200 import synth
     from oracle import bind
 
-    sample = workload.scaled(min(CPU_SAMPLE_READS, workload.n_reads))
+    sample = workload.sampled(min(CPU_SAMPLE_READS, workload.n_reads))
     threads = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as td:
         fq = os.path.join(td, "sample.fq")
@@ -177,12 +183,11 @@ def cpu_baseline_block(workload, steps: int = 1):
             times = [cpu_reference_run(fq, workload.cli_args(), threads, td)[0] for _ in range(steps)]
             kind, cores = "reference", threads
             # the same build on one host thread (OMP_NUM_THREADS=1), a smaller sample
-            one = workload.scaled(min(CPU_SAMPLE_READS_1T, workload.n_reads))
+            one = workload.sampled(min(CPU_SAMPLE_READS_1T, workload.n_reads))
             fq1 = os.path.join(td, "sample1.fq")
             synth.write_fastq(one, fq1)
             t1 = cpu_reference_run(fq1, workload.cli_args(), 1, td)[0]
-            single = {"value": one.n_reads / t1, "unit": "reads/s", "cores": 1,
-                      "sample": f"first {one.n_reads} reads of the workload"}
+            single = {"value": one.n_reads / t1, "unit": "reads/s", "cores": 1, "sample": one.name}
         else:
             data = open(fq, "rb").read()
             times = []
@@ -193,7 +198,7 @@ def cpu_baseline_block(workload, steps: int = 1):
             kind, cores = "port", 1
     v = sample.n_reads / statistics.median(times)
     return {"value": v, "unit": "reads/s", "cores": cores, "kind": kind,
-            "sample": f"first {sample.n_reads} reads of the workload (same genome and error model), "
+            "sample": f"{sample.name}; "
                       f"{'reference sources built with Thrust on OpenMP' if kind == 'reference' else 'oracle C port'}; "
                       f"compute time = wall minus the reference's read_input; median of {len(times)}",
             "single_thread": single}, times
@@ -206,7 +211,7 @@ def run_reference_arm(args, workload):
     from oracle import bind
     from empanada_b200 import synth
 
-    sample = workload.scaled(min(CPU_SAMPLE_READS, workload.n_reads))
+    sample = workload.sampled(min(CPU_SAMPLE_READS, workload.n_reads))
     threads = os.cpu_count() or 1
     times = []
     with tempfile.TemporaryDirectory() as td:
@@ -233,7 +238,7 @@ def run_reference_arm(args, workload):
             "config": {"workload": workload.name, "sample_reads": sample.n_reads, "read_len": workload.read_len,
                        "parallelism": "host threads"},
             "cpu_baseline": {"value": v, "unit": "reads/s", "cores": threads if have_ref else 1, "kind": kind,
-                             "sample": f"first {sample.n_reads} reads of the workload per step"},
+                             "sample": f"{sample.name}, per step"},
             "e2e": {"value": v, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -546,8 +551,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="larger")
+    ap.add_argument("--workload", default="out_of_core_hbm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reads", type=int, default=0,
+                    help="run a sample of the workload at the same coverage (genome shrunk with the read count)")
     ap.add_argument("--kernel", default=None, choices=[None, "sort"],
                     help="microbenchmark one kernel instead of the whole path")
     ap.add_argument("--pairs", type=int, default=1 << 24)
@@ -564,7 +571,9 @@ def main():
                     help="served jobs with a longer first round list run alone (0: the bucket kernel's limit)")
     ap.add_argument("--serve-budget", type=int, default=100, help="admission budget of the server, GiB")
     args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
+    if args.warmup < 3:
+        print(f"bench.py: --warmup {args.warmup} is below the 3 warm-up steps a valid measurement needs",
+              file=sys.stderr)
     if args.impl == "reference" and args.workload in ("served", "batched"):
         if env_rank()[0] == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the reference runs one read set per process and "
@@ -581,6 +590,8 @@ def main():
     from empanada_b200 import synth
 
     workload = synth.WORKLOADS[args.workload]
+    if args.reads:
+        workload = workload.sampled(args.reads)
     if args.kernel == "sort":
         sort_microbench(args)
         return
@@ -666,6 +677,7 @@ def main():
     out_bytes = st["output_bytes"]
     total_ms = reduce_max_over_ranks(total_ms, dist, f"cuda:{device}")
     value = replica_throughput(world, workload.n_reads, args.steps, total_ms / 1000.0)
+    ref_crc = zlib.crc32(job.output())  # every end-to-end step must give these bytes
     job.close()
 
     # ---- e2e: host FASTQ in, output.bin out, through the C ABI
@@ -689,32 +701,44 @@ def main():
                                     reduce_max_over_ranks(sum(e2e_s), dist, f"cuda:{device}"))
     # pipelined: read sets back to back on two jobs; each step issues the
     # asynchronous copy of the next step's read set (the copy engine runs it
-    # beside this step's kernels), runs its own, and copies its output.bin out
+    # beside this step's kernels), runs its own, and copies its output.bin
+    # out.  The K timed steps form one region with no device-wide
+    # synchronisation inside it (that would finish the next set's copy
+    # outside the clock): one barrier before it, one after.
     pair = [eng.job(**params), eng.job(**params)]
     for j in pair:
         j.reserve(F)
-    e2e_p = []
-    for i in range(args.warmup + args.steps):
+
+    def pipelined_step(i):
         cur, nxt = pair[i % 2], pair[(i + 1) % 2]
-        barrier()
-        t0 = time.perf_counter()
         if i == 0:
             cur.reset()
             cur.feed_async(host_np, last=True)
         nxt.reset()
         nxt.feed_async(host_np, last=True)
         cur.run()
-        n_out = cur.output_into(out_host)
-        dt = time.perf_counter() - t0
-        if i >= args.warmup:
-            e2e_p.append(dt)
+        got = cur.output_into(out_host)
+        if got != out_bytes:
+            raise RuntimeError(f"end-to-end step {i}: {got} output bytes, the device-resident run gave {out_bytes}")
+        return got
+
+    for i in range(args.warmup):
+        pipelined_step(i)
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(args.warmup, args.warmup + args.steps):
+        n_out = pipelined_step(i)
+    e2e_elapsed = time.perf_counter() - t0
+    barrier()
+    if zlib.crc32(out_host[:n_out]) != ref_crc:
+        raise RuntimeError("end-to-end: output.bin differs from the device-resident run's")
     for j in pair:
         j.close()
-    e2e_total = reduce_max_over_ranks(sum(e2e_p), dist, f"cuda:{device}")
-    e2e_value = replica_throughput(world, workload.n_reads, len(e2e_p), e2e_total)
+    e2e_total = reduce_max_over_ranks(e2e_elapsed, dist, f"cuda:{device}")
+    e2e_value = replica_throughput(world, workload.n_reads, args.steps, e2e_total)
 
     peak, peak_kind = measured_peaks()
-    traffic = traffic_summary()
+    traffic = traffic_summary(args.workload)
     if rk_ms >= max(sort_ms, upd_ms):  # the all-rounds cooperative kernel dominates
         per_launch = rk_bytes / args.steps
         ms, nl = rk_ms, args.steps

@@ -75,6 +75,17 @@ class Workload:
         """Same genome and error model with fewer reads (a bounded sample)."""
         return dataclasses.replace(self, n_reads=n_reads, name=name or f"{self.name}[:{n_reads}]")
 
+    def sampled(self, n_reads: int) -> "Workload":
+        """A bounded sample at the same coverage: n_reads reads from a genome
+        shrunk by the same factor (same read length, error and repeat model,
+        options and seed), so each read meets as many overlaps as in the full
+        workload."""
+        if n_reads >= self.n_reads:
+            return self
+        g = max(4 * self.read_len, round(self.genome_len * n_reads / self.n_reads))
+        return dataclasses.replace(self, n_reads=n_reads, genome_len=g,
+                                   name=f"{self.name} [sample: {n_reads} reads of a {g} bp genome, same coverage]")
+
 
 SMALL = Workload("small: 1 Mbp genome, 100k x 150 bp error-free reads, -o 31", seed=1,
                  genome_len=1_000_000, n_reads=100_000, read_len=150, min_ovlp=31)
