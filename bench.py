@@ -308,6 +308,12 @@ def batched_bench(args):
     for j, a, b in zip(jobs, offs[:-1], offs[1:]):
         j.reserve(int(b - a))
         j.feed(host_np[a:b], last=True)
+    from empanada_b200 import tune
+
+    tuning = {"source": "defaults", "choice": eng.tuning()}
+    if not args.no_tune and tune.enabled():
+        tuning = tune.tune_batch(eng, jobs, reads, int(np.median([w.read_len for w in sets])))
+        tuning["choice"] = eng.tuning()
 
     def timed(fn, steps, warmup):
         ms = []
@@ -381,7 +387,7 @@ def batched_bench(args):
                     "mode": "every set's FASTQ copied in from pinned host memory with emp_job_feed_fastq_async "
                             "(the first sets' map phase runs beside the later copies), one emp_batch_run, every "
                             "output.bin copied out (wall clock)"},
-            "clocks": clocks, "host_generate_s": gen_s}
+            "clocks": clocks, "host_generate_s": gen_s, "tuning": tuning}
     print(json.dumps(line), flush=True)
 
 
@@ -553,6 +559,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="out_of_core_hbm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the engine's default choices (no autotuning)")
     ap.add_argument("--reads", type=int, default=0,
                     help="run a sample of the workload at the same coverage (genome shrunk with the read count)")
     ap.add_argument("--kernel", default=None, choices=[None, "sort"],
@@ -603,6 +610,7 @@ def main():
     import torch
 
     import empanada_b200
+    from empanada_b200 import tune
 
     rank, local_rank, world = env_rank()
     dist = None
@@ -637,6 +645,10 @@ def main():
     job = eng.job(**params)
     job.reserve(F)
     job.feed(host_np, last=True)
+    tuning = {"source": "defaults", "choice": eng.tuning()}
+    if not args.no_tune and tune.enabled():  # the engine's choices for this workload (empanada_b200/tune.py)
+        tuning = tune.tune_job(eng, job, workload.n_reads, workload.read_len)
+        tuning["choice"] = eng.tuning()
     for _ in range(args.warmup):
         flush.zero_()
         job.run(sptr)
@@ -790,6 +802,7 @@ def main():
                                 "out (wall clock)",
                         "serial_value": e2e_serial},
                 "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+                "tuning": tuning,
                 "job": {k: st[k] for k in ("n_reads", "n_unique", "n_edges", "n_records", "n_rounds", "ms_map",
                                            "ms_dedup", "ms_rounds")},
                 "live_entries": int(sum(st["sfx_live"]) + sum(st["pfx_live"]))}

@@ -47,7 +47,7 @@ class Tuning(ctypes.Structure):
         ("edge_cap", ctypes.c_uint64),
         ("wait_limit_ns", ctypes.c_uint64),
         ("block_next_wait", ctypes.c_int32),
-        ("reserved1", ctypes.c_int32),
+        ("map_streams", ctypes.c_uint32),
     ]
 
     def to_dict(self) -> dict:

@@ -77,7 +77,8 @@ def build_native(verbose: bool = False, ptxas_info: bool = False) -> None:
 def build_oracle(with_reference: bool | None = None) -> None:
     """Checker side: the C restatement, and the reference itself when its sources are present."""
     _run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"])
-    ref = os.environ.get("EMP_REFERENCE_DIR", "/root/reference")
+    # the reference's sources: EMP_REFERENCE_DIR, else a `reference` directory beside the repository
+    ref = os.environ.get("EMP_REFERENCE_DIR") or os.path.join(os.path.dirname(ROOT), "reference")
     if with_reference is None:
         with_reference = os.path.isdir(ref)
     if with_reference and shutil.which("g++"):

@@ -121,7 +121,8 @@ struct HostSlab {
 
 }  // namespace
 
-constexpr int kMapStreams = 8;
+constexpr int kMapStreams = 32;     // streams of a batch's map phase at most
+constexpr int kMapStreamsDefault = 8;
 
 struct emp_ctx {
     int device = 0;
@@ -1182,12 +1183,13 @@ emp_status map_batch(emp_job **jobs, int n, std::vector<emp_status> &rc, cudaStr
     };
     // job i on stream i mod K (K = 1: s itself), every stream after s's work so far
     emp_ctx *ctx = n ? jobs[0]->ctx : nullptr;
-    const int K = n > 1 ? std::min(n, kMapStreams) : 1;
+    const int want = ctx && ctx->tune.map_streams ? (int)ctx->tune.map_streams : kMapStreamsDefault;
+    const int K = n > 1 ? std::min(n, want) : 1;
     std::vector<cudaStream_t> st((size_t)K, s);
     if (K > 1) {
         for (int k = 0; k <= kMapStreams; ++k)
             if (!ctx->map_ev[k]) EMP_CUDA(cudaEventCreateWithFlags(&ctx->map_ev[k], cudaEventDisableTiming));
-        EMP_CUDA(cudaEventRecord(ctx->map_ev[kMapStreams], s));
+        EMP_CUDA(cudaEventRecord(ctx->map_ev[kMapStreams], s));  // the last event: the start of the phase
         for (int k = 0; k < K; ++k) {
             if (!ctx->map_streams[k]) EMP_CUDA(cudaStreamCreateWithFlags(&ctx->map_streams[k], cudaStreamNonBlocking));
             st[k] = ctx->map_streams[k];
@@ -1524,6 +1526,7 @@ emp_status emp_tuning_default(emp_tuning *t) {
     std::memset(t, 0, sizeof *t);
     t->bucket_mean = kBktMean;
     t->region_cap = kBktRegionCap;
+    t->map_streams = kMapStreamsDefault;
     t->wait_limit_ns = kBarrierTimeoutNs;
     return EMP_OK;
 }
@@ -1532,7 +1535,7 @@ emp_status emp_ctx_set_tuning(emp_ctx *ctx, const emp_tuning *t) {
     if (!ctx || !t) return EMP_E_INVAL;
     if (t->round_driver < 0 || t->round_driver > 1 || t->dedup_driver < 0 || t->dedup_driver > 1) return EMP_E_INVAL;
     if (t->bucket_mean && (t->bucket_mean < kBktMeanMin || t->bucket_mean > kBktMeanMax)) return EMP_E_INVAL;
-    if (t->region_cap > kBktRegionCap) return EMP_E_INVAL;
+    if (t->region_cap > kBktRegionCap || t->map_streams > (uint32_t)kMapStreams) return EMP_E_INVAL;
     ctx->tune = *t;
     return EMP_OK;
 }
@@ -1545,6 +1548,7 @@ emp_status emp_ctx_get_tuning(emp_ctx *ctx, emp_tuning *t) {
     t->dedup_driver = c.dedup_driver;
     if (c.bucket_mean) t->bucket_mean = c.bucket_mean;
     if (c.region_cap) t->region_cap = c.region_cap;
+    if (c.map_streams) t->map_streams = c.map_streams;
     t->edge_cap = c.edge_cap;
     if (c.wait_limit_ns) t->wait_limit_ns = c.wait_limit_ns;
     t->block_next_wait = c.block_next_wait;

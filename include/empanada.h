@@ -124,7 +124,8 @@ typedef struct emp_tuning {
     int32_t block_next_wait;  /* testing: the context's next bucket-kernel launch meets a grid barrier
                                  that no arrival completes, so its waits run out after wait_limit_ns and
                                  the run returns EMP_E_TIMEOUT; that launch clears the flag */
-    int32_t reserved1;
+    uint32_t map_streams;     /* streams that the map phase of a batch (or a server step) spreads its
+                                 jobs over, 1..32 (default 8) */
 } emp_tuning;
 emp_status emp_tuning_default(emp_tuning *t);
 /* EMP_E_INVAL for a value outside its range (the context keeps its choices). */

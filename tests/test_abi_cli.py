@@ -53,7 +53,7 @@ def test_tuning_defaults_and_validation_without_a_gpu():
     lib = _native.lib()
     assert lib.emp_tuning_default(ctypes.byref(t)) == 0
     assert t.to_dict() == {"round_driver": 0, "bucket_mean": 2900, "region_cap": 2048, "dedup_driver": 0, "edge_cap": 0,
-                           "wait_limit_ns": 20_000_000_000, "block_next_wait": 0}
+                           "wait_limit_ns": 20_000_000_000, "block_next_wait": 0, "map_streams": 8}
     assert lib.emp_tuning_default(None) == _native.EMP_E_INVAL
     assert lib.emp_ctx_set_tuning(None, ctypes.byref(t)) == _native.EMP_E_INVAL
     assert lib.emp_ctx_get_tuning(None, ctypes.byref(t)) == _native.EMP_E_INVAL
