@@ -560,6 +560,7 @@ def main():
     ap.add_argument("--workload", default="out_of_core_hbm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the engine's default choices (no autotuning)")
+    ap.add_argument("--no-graph", action="store_true", help="skip the unitig layer's measurement")
     ap.add_argument("--reads", type=int, default=0,
                     help="run a sample of the workload at the same coverage (genome shrunk with the read count)")
     ap.add_argument("--kernel", default=None, choices=[None, "sort"],
@@ -689,8 +690,26 @@ def main():
     out_bytes = st["output_bytes"]
     total_ms = reduce_max_over_ranks(total_ms, dist, f"cuda:{device}")
     value = replica_throughput(world, workload.n_reads, args.steps, total_ms / 1000.0)
-    ref_crc = zlib.crc32(job.output())  # every end-to-end step must give these bytes
+    out_bin = job.output()
+    ref_crc = zlib.crc32(out_bin)  # every end-to-end step must give these bytes
     job.close()
+    # ---- the unitig layer over this output.bin (device time), beside its CPU restatement
+    graph = None
+    if not args.no_graph:
+        with empanada_b200.Graph(eng, out_bin, st["n_reads"]) as g:
+            gst = g.stats()
+        graph = {"ms_build": gst["ms_build"], "edges": gst["edges"], "unitigs": gst["unitigs"],
+                 "long_unitigs": gst["long_unitigs"], "cycles": gst["cycles"],
+                 "what": "unitigs (maximal paths of edges u->v with out-degree(u) = in-degree(v) = 1) of the "
+                         "job's output.bin on the device: edge scatter, degrees, pointer jumping, placement"}
+        if rank == 0 and world == 1:
+            from oracle import bind
+
+            t0 = time.perf_counter()
+            bind.unitigs(out_bin, st["n_reads"])
+            graph["cpu_oracle_ms"] = 1000 * (time.perf_counter() - t0)
+            graph["cpu_oracle"] = "oracle/graph_oracle.c, one host thread, serial walk"
+    del out_bin
 
     # ---- e2e: host FASTQ in, output.bin out, through the C ABI
     out_host = torch.empty(out_bytes + 4096, dtype=torch.uint8, pin_memory=True).numpy()
@@ -802,7 +821,7 @@ def main():
                                 "out (wall clock)",
                         "serial_value": e2e_serial},
                 "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
-                "tuning": tuning,
+                "tuning": tuning, "graph": graph,
                 "job": {k: st[k] for k in ("n_reads", "n_unique", "n_edges", "n_records", "n_rounds", "ms_map",
                                            "ms_dedup", "ms_rounds")},
                 "live_entries": int(sum(st["sfx_live"]) + sum(st["pfx_live"]))}

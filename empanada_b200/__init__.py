@@ -28,7 +28,7 @@ import numpy as np
 from . import _native
 from ._native import EmpError, check
 
-__all__ = ["Config", "parse_args", "parse_size", "Engine", "Job", "run_bytes", "run_file", "decode_output",
+__all__ = ["Config", "parse_args", "parse_size", "Engine", "Job", "Graph", "run_bytes", "run_file", "decode_output",
            "EmpError", "UsageExit"]
 
 DEFAULTS = {"o": "31", "m": "1g", "r": "1g", "b": "32m", "c": "64m"}
@@ -343,6 +343,55 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Graph:
+    """Unitigs of the overlap graph in an output.bin (emp_graph_*): read-ends
+    as nodes, the records' edges; a unitig is a maximal path of edges
+    u -> v with out-degree(u) = in-degree(v) = 1."""
+
+    def __init__(self, engine: Engine, output_bin: bytes, n_reads: int):
+        self._lib = engine._lib
+        self.n_reads = int(n_reads)
+        h = ctypes.c_void_p()
+        buf = bytes(output_bin)
+        check(self._lib.emp_graph_build(engine.handle, buf, len(buf), self.n_reads, ctypes.byref(h)),
+              "emp_graph_build")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self._lib.emp_graph_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stats(self) -> dict:
+        st = _native.GraphStats()
+        check(self._lib.emp_graph_get_stats(self.handle, ctypes.byref(st)), "emp_graph_get_stats")
+        return st.to_dict()
+
+    def unitigs(self) -> tuple[np.ndarray, np.ndarray]:
+        """(read-ends in unitig order, each unitig's first position + the end)."""
+        st = self.stats()
+        order = np.zeros(max(1, st["nodes"]), dtype=np.uint32)
+        starts = np.zeros(st["unitigs"] + 1, dtype=np.uint64)
+        check(self._lib.emp_graph_unitigs(self.handle, order.ctypes.data, order.size, starts.ctypes.data,
+                                          starts.size), "emp_graph_unitigs")
+        return order[: st["nodes"]], starts
+
+    def write_gfa(self, path: str, read_len: int) -> None:
+        check(self._lib.emp_graph_write_gfa(self.handle, path.encode(), int(read_len)), "emp_graph_write_gfa")
 
 
 SORT_STATIC_MAX_PAIRS = _native.SORT_STATIC_MAX_PAIRS

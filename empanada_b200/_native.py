@@ -54,6 +54,20 @@ class Tuning(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("reserved")}
 
 
+class GraphStats(ctypes.Structure):
+    _fields_ = [
+        ("nodes", ctypes.c_uint64),
+        ("edges", ctypes.c_uint64),
+        ("unitigs", ctypes.c_uint64),
+        ("long_unitigs", ctypes.c_uint64),
+        ("cycles", ctypes.c_uint64),
+        ("ms_build", ctypes.c_double),
+    ]
+
+    def to_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 # int (*emp_edge_sink)(void *user, int32_t ovlp_len, uint64_t n, const uint32_t *from, const uint32_t *to)
 EDGE_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint64,
                              ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32))
@@ -161,6 +175,11 @@ SIGNATURES = {
     "emp_job_fingerprints": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, _u64p]),
     "emp_run_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Params), ctypes.c_int,
                                     ctypes.POINTER(Stats)]),
+    "emp_graph_build": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(_vp)]),
+    "emp_graph_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(GraphStats)]),
+    "emp_graph_unitigs": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, _vp, ctypes.c_uint64]),
+    "emp_graph_write_gfa": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int32]),
+    "emp_graph_destroy": (ctypes.c_int, [_vp]),
     "emp_sort_pairs": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp]),
     "emp_sort_pairs_static": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, _vp]),
 }

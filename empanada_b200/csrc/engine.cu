@@ -175,8 +175,7 @@ struct emp_job {
     DevBuf akeys, apos, bkeys, parts;  // record splitting
     DevBuf xk0, xv0, xk1, xv1, ring_k, ring_v, cparts;  // sort of a table larger than M
     PinnedBuf h_parts;
-    // the initial list (kept for a rerun with a larger edge buffer), round records
-    DevBuf lk_init, lv_init, records;
+    DevBuf records;  // round records
     PinnedBuf h_records;
     uint64_t ecap_hint = 0;
     uint64_t sorts_since_clear = 0;
@@ -1023,7 +1022,7 @@ emp_status dedup_by_sort(emp_job *j, cudaStream_t s) {
 }
 
 // The initial list (suffixes then prefixes) is ready; the rounds environment
-// follows.  Also keeps the list for a restart with a larger edge buffer.
+// follows.
 emp_status map_list(emp_job *j, cudaStream_t s) {
     EMP_TRY(map_check(j));
     JobPrep &q = j->prep;
@@ -1047,10 +1046,6 @@ emp_status map_list(emp_job *j, cudaStream_t s) {
     cudaEventRecord(j->map_ev[2], s);
     q.rounds = q.L - j->p.min_ovlp;
     if (q.rounds <= 0) return EMP_OK;
-    EMP_TRY(ensure(j, j->lk_init, 2 * U * 8 + 8));
-    EMP_TRY(ensure(j, j->lv_init, 2 * U * 4 + 4));
-    EMP_CUDA(cudaMemcpyAsync(j->lk_init.p, j->lk0.p, 2 * U * 8, cudaMemcpyDeviceToDevice, s));
-    EMP_CUDA(cudaMemcpyAsync(j->lv_init.p, j->lv0.p, 2 * U * 4, cudaMemcpyDeviceToDevice, s));
     const uint64_t ecap0 = j->ctx->tune.edge_cap ? j->ctx->tune.edge_cap : (4 * U > (1u << 20) ? 4 * U : (1u << 20));
     q.ecap = j->ecap_hint ? j->ecap_hint : ecap0;
     return EMP_OK;
@@ -1073,8 +1068,13 @@ emp_status job_rounds(emp_job *j, cudaStream_t s) {
         if (rc != kNeedEdgeRoom || attempt >= 2) return rc == kNeedEdgeRoom ? EMP_E_NOMEM : rc;
         q.ecap = needed + needed / 4 + 1024;
         j->ecap_hint = q.ecap;
-        EMP_CUDA(cudaMemcpyAsync(j->lk0.p, j->lk_init.p, 2 * q.U * 8, cudaMemcpyDeviceToDevice, s));
-        EMP_CUDA(cudaMemcpyAsync(j->lv0.p, j->lv_init.p, 2 * q.U * 4, cudaMemcpyDeviceToDevice, s));
+        // the round drivers overwrite the list buffers: build the initial list again
+        // from the fingerprints and survivor marks, which the rounds leave intact
+        EMP_TRY(reset_chain(j, upd_tiles(2 * q.n), s));
+        launch_init_list(j->keys0.as<uint64_t>(), j->alive.as<uint8_t>(), q.n, j->lk0.as<uint64_t>(),
+                         j->lv0.as<uint32_t>(), j->status.as<uint64_t>(), chain_ctr(j),
+                         j->misc.as<uint64_t>() + kMiscU, err_word(j), s);
+        launch_dup_prefix_half(j->lk0.as<uint64_t>(), j->lv0.as<uint32_t>(), q.U, s);
     }
 }
 
@@ -1200,26 +1200,39 @@ emp_status map_batch(emp_job **jobs, int n, std::vector<emp_status> &rc, cudaStr
         for (cudaStream_t q : st) EMP_CUDA(cudaStreamSynchronize(q));
         return EMP_OK;
     };
+    // largest jobs first, each to the stream with the fewest FASTQ bytes so
+    // far (so that no stream ends a stage long after the others)
+    std::vector<int> order((size_t)n), sid((size_t)n, 0);
+    for (int i = 0; i < n; ++i) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return jobs[a]->F > jobs[b]->F; });
+    {
+        std::vector<uint64_t> load((size_t)K, 0);
+        for (int i : order) {
+            const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            sid[(size_t)i] = k;
+            load[(size_t)k] += jobs[i]->F + 4096;
+        }
+    }
     auto stages = [&]() -> emp_status {
-        for (int i = 0; i < n; ++i) {
-            fail(i, map_begin(jobs[i], st[i % K]));
-            if (rc[i] == EMP_OK) fail(i, map_fetch(jobs[i], st[i % K]));
+        for (int i : order) {
+            fail(i, map_begin(jobs[i], st[sid[i]]));
+            if (rc[i] == EMP_OK) fail(i, map_fetch(jobs[i], st[sid[i]]));
         }
         EMP_TRY(sync_all());
-        for (int i = 0; i < n; ++i) {
+        for (int i : order) {
             if (!live(i)) continue;
-            fail(i, map_records(jobs[i], st[i % K]));
-            if (live(i)) fail(i, map_fetch(jobs[i], st[i % K]));
+            fail(i, map_records(jobs[i], st[sid[i]]));
+            if (live(i)) fail(i, map_fetch(jobs[i], st[sid[i]]));
         }
         EMP_TRY(sync_all());
-        for (int i = 0; i < n; ++i) {
+        for (int i : order) {
             if (!live(i)) continue;
-            fail(i, map_keys(jobs[i], st[i % K]));
-            if (live(i)) fail(i, map_fetch(jobs[i], st[i % K]));
+            fail(i, map_keys(jobs[i], st[sid[i]]));
+            if (live(i)) fail(i, map_fetch(jobs[i], st[sid[i]]));
         }
         EMP_TRY(sync_all());
-        for (int i = 0; i < n; ++i)
-            if (live(i)) fail(i, map_list(jobs[i], st[i % K]));
+        for (int i : order)
+            if (live(i)) fail(i, map_list(jobs[i], st[sid[i]]));
         return EMP_OK;
     };
     const emp_status e = stages();
@@ -1736,8 +1749,7 @@ static void release_buffers(emp_job *job) {
                       &job->seq_end, &job->keys0, &job->dedup_scr, &job->cols, &job->seq2, &job->sk0,
                       &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
                       &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
-                      &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts, &job->lk_init,
-                      &job->lv_init, &job->records, &job->coop_ctl, &job->coop_trace,
+                      &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts, &job->records, &job->coop_ctl, &job->coop_trace,
                       &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_cnt, &job->bk_spill, &job->bk_spans,
                       &job->bk_sfrom, &job->bk_sto, &job->bk_scratch, &job->bk_job, &job->dout,
                       &job->bk_meta, &job->xk0, &job->xv0, &job->xk1, &job->xv1, &job->ring_k, &job->ring_v,
@@ -2183,6 +2195,258 @@ emp_status emp_run_file(const char *input_path, const char *output_path, const e
     emp_job_destroy(job);
     emp_ctx_destroy(ctx);
     return st;
+}
+
+}  // extern "C"
+
+// ---- unitigs of an output.bin ------------------------------------------------
+struct emp_graph {
+    emp_ctx *ctx = nullptr;
+    std::vector<uint8_t> bin;         // the output.bin bytes (the L lines come from them)
+    std::vector<uint64_t> rec_off;    // byte offset of every record
+    uint64_t nodes = 0, edges = 0;
+    std::vector<uint32_t> order;      // read-ends in unitig order
+    std::vector<uint64_t> starts;     // first position of every unitig, then `nodes`
+    emp_graph_stats st{};
+};
+
+extern "C" {
+
+emp_status emp_graph_build(emp_ctx *ctx, const void *output_bin, uint64_t bytes, uint64_t n_reads, emp_graph **out) {
+    if (!ctx || !out || (bytes && !output_bin)) return EMP_E_INVAL;
+    *out = nullptr;
+    if (n_reads == 0 || 2 * n_reads >= (1ull << 31)) return n_reads ? EMP_E_UNSUPPORTED : EMP_E_INVAL;
+    const uint8_t *b = static_cast<const uint8_t *>(output_bin);
+    emp_graph *g = new (std::nothrow) emp_graph();
+    if (!g) return EMP_E_NOMEM;
+    g->ctx = ctx;
+    g->nodes = 2 * n_reads;
+    // the records: u64 n | i32 ovlp_len | u32 from[n] | u32 to[n]
+    std::vector<uint64_t> e0{0};
+    for (uint64_t o = 0; o < bytes;) {
+        uint64_t n = 0;
+        if (o + 12 > bytes) { delete g; return EMP_E_FORMAT; }
+        std::memcpy(&n, b + o, 8);
+        if (n > (bytes - o - 12) / 8) { delete g; return EMP_E_FORMAT; }
+        g->rec_off.push_back(o);
+        e0.push_back(e0.back() + n);
+        o += 12 + 8 * n;
+    }
+    g->edges = e0.back();
+    g->bin.assign(b, b + bytes);
+    cudaSetDevice(ctx->device);
+    const uint32_t V = (uint32_t)g->nodes;
+    const uint64_t E = g->edges, nrec = g->rec_off.size();
+    // one device allocation for everything, in the context's pool
+    const uint64_t scan_t = scan_tiles(V);
+    size_t off = 0;
+    auto take = [&](size_t bytes_) { const size_t o = off; off = (off + bytes_ + 255) / 256 * 256; return o; };
+    const size_t o_bin = take(bytes + 16), o_roff = take(nrec * 8 + 8), o_e0 = take((nrec + 1) * 8);
+    const size_t o_from = take(E * 4 + 4), o_to = take(E * 4 + 4);
+    size_t o_node[15];
+    for (auto &x : o_node) x = take((size_t)V * 4);
+    const size_t o_start = take((size_t)V * 8), o_status = take(scan_t * 8 + 64), o_small = take(64);
+    cudaStream_t s = ctx->stream;
+    void *dev = nullptr;
+    if (cudaMallocFromPoolAsync(&dev, off, ctx->pool, s) != cudaSuccess) {
+        cudaGetLastError();
+        delete g;
+        return EMP_E_NOMEM;
+    }
+    uint8_t *d = static_cast<uint8_t *>(dev);
+    GraphBufs gb{};
+    gb.from = reinterpret_cast<uint32_t *>(d + o_from);
+    gb.to = reinterpret_cast<uint32_t *>(d + o_to);
+    uint32_t **node_arrays[15] = {&gb.dout, &gb.din, &gb.succ, &gb.pred, &gb.hop[0], &gb.hop[1], &gb.dist[0],
+                                  &gb.dist[1], &gb.mn[0], &gb.mn[1], &gb.nx[0], &gb.nx[1], &gb.size, &gb.order,
+                                  nullptr};
+    for (int k = 0; k < 14; ++k) *node_arrays[k] = reinterpret_cast<uint32_t *>(d + o_node[k]);
+    gb.start = reinterpret_cast<uint64_t *>(d + o_start);
+    gb.status = reinterpret_cast<uint64_t *>(d + o_status);
+    uint64_t *small = reinterpret_cast<uint64_t *>(d + o_small);  // tile counter, total, error, cycles
+    gb.tile_ctr = reinterpret_cast<uint32_t *>(small);
+    gb.total = small + 1;
+    gb.err = reinterpret_cast<uint32_t *>(small + 2);
+    gb.cycles = reinterpret_cast<uint32_t *>(small + 3);
+    emp_status rc = EMP_OK;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    PinnedBuf hs;
+    if (!hs.ensure(64)) rc = EMP_E_NOMEM;
+    if (rc == EMP_OK && (cudaEventCreate(&ev[0]) != cudaSuccess || cudaEventCreate(&ev[1]) != cudaSuccess))
+        rc = EMP_E_CUDA;
+    if (rc == EMP_OK) {
+        cudaEventRecord(ev[0], s);
+        if (bytes) cudaMemcpyAsync(d + o_bin, b, bytes, cudaMemcpyHostToDevice, s);
+        if (nrec) cudaMemcpyAsync(d + o_roff, g->rec_off.data(), nrec * 8, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(d + o_e0, e0.data(), (nrec + 1) * 8, cudaMemcpyHostToDevice, s);
+        cudaMemsetAsync(gb.status, 0, scan_t * 8 + 64, s);
+        cudaMemsetAsync(small, 0, 64, s);
+        graph_build(d + o_bin, reinterpret_cast<uint64_t *>(d + o_roff), reinterpret_cast<uint64_t *>(d + o_e0),
+                    (uint32_t)nrec, E, V, gb, s);
+        cudaEventRecord(ev[1], s);
+        g->order.resize(V);
+        std::vector<uint32_t> size(V);
+        cudaMemcpyAsync(g->order.data(), gb.order, (size_t)V * 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(size.data(), gb.size, (size_t)V * 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(hs.p, small, 32, cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = EMP_E_CUDA;
+        const uint64_t *hw = hs.as<uint64_t>();
+        if (rc == EMP_OK && (hw[2] & kErrSpin)) rc = EMP_E_TIMEOUT;
+        if (rc == EMP_OK && (hw[2] & kErrCapacity)) rc = EMP_E_FORMAT;  // an edge beyond the read-ends given
+        if (rc == EMP_OK) {
+            uint64_t pos = 0;
+            for (uint32_t u = 0; u < V; ++u)
+                if (size[u]) {
+                    g->starts.push_back(pos);
+                    pos += size[u];
+                    g->st.long_unitigs += size[u] >= 2;
+                }
+            g->starts.push_back(pos);
+            g->st.nodes = V;
+            g->st.edges = E;
+            g->st.unitigs = g->starts.size() - 1;
+            g->st.cycles = (uint32_t)hw[3];
+            g->st.ms_build = ms_between(ev[0], ev[1]);
+            if (pos != V) rc = EMP_E_CUDA;
+        }
+    }
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    cudaFreeAsync(dev, s);
+    if (rc != EMP_OK) {
+        cudaStreamSynchronize(s);
+        delete g;
+        return rc;
+    }
+    *out = g;
+    return EMP_OK;
+}
+
+emp_status emp_graph_get_stats(emp_graph *g, emp_graph_stats *st) {
+    if (!g || !st) return EMP_E_INVAL;
+    *st = g->st;
+    return EMP_OK;
+}
+
+emp_status emp_graph_unitigs(emp_graph *g, uint32_t *order, uint64_t order_cap, uint64_t *starts, uint64_t starts_cap) {
+    if (!g) return EMP_E_INVAL;
+    if (order) {
+        if (order_cap < g->order.size()) return EMP_E_INVAL;
+        std::memcpy(order, g->order.data(), g->order.size() * 4);
+    }
+    if (starts) {
+        if (starts_cap < g->starts.size()) return EMP_E_INVAL;
+        std::memcpy(starts, g->starts.data(), g->starts.size() * 8);
+    }
+    return EMP_OK;
+}
+
+namespace {
+// decimal digits of v at p; returns the end
+char *put_u64(char *p, uint64_t v) {
+    char t[24];
+    int k = 0;
+    do {
+        t[k++] = (char)('0' + v % 10);
+        v /= 10;
+    } while (v);
+    while (k) *p++ = t[--k];
+    return p;
+}
+}  // namespace
+
+emp_status emp_graph_write_gfa(emp_graph *g, const char *path, int32_t read_len) {
+    if (!g || !path || read_len < 0) return EMP_E_INVAL;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return EMP_E_IO;
+    std::vector<char> buf(1 << 22);
+    size_t used = 0;
+    bool ok = true;
+    auto flush = [&](size_t room) {
+        if (used + room > buf.size()) {
+            ok = ok && std::fwrite(buf.data(), 1, used, f) == used;
+            used = 0;
+        }
+    };
+    auto put = [&](const char *str) {
+        const size_t l = std::strlen(str);
+        flush(l);
+        std::memcpy(buf.data() + used, str, l);
+        used += l;
+    };
+    put("H\tVN:Z:1.0\n");
+    const uint64_t n_reads = g->nodes / 2;
+    for (uint64_t i = 0; i < n_reads; ++i) {  // S <id> * LN:i:<L>
+        flush(64);
+        char *p = buf.data() + used;
+        *p++ = 'S';
+        *p++ = '\t';
+        p = put_u64(p, i);
+        std::memcpy(p, "\t*\tLN:i:", 8);
+        p = put_u64(p + 8, (uint64_t)read_len);
+        *p++ = '\n';
+        used = (size_t)(p - buf.data());
+    }
+    const uint8_t *b = g->bin.data();
+    for (uint64_t o : g->rec_off) {  // L <u> <+|-> <v> <+|-> <len>M, edges in output.bin order
+        uint64_t n = 0;
+        int32_t ovlp = 0;
+        std::memcpy(&n, b + o, 8);
+        std::memcpy(&ovlp, b + o + 8, 4);
+        const uint8_t *fr = b + o + 12, *to = fr + 4 * n;
+        for (uint64_t k = 0; k < n; ++k) {
+            uint32_t u, v;
+            std::memcpy(&u, fr + 4 * k, 4);
+            std::memcpy(&v, to + 4 * k, 4);
+            flush(80);
+            char *p = buf.data() + used;
+            *p++ = 'L';
+            *p++ = '\t';
+            p = put_u64(p, u >> 1);
+            *p++ = '\t';
+            *p++ = (u & 1) ? '-' : '+';
+            *p++ = '\t';
+            p = put_u64(p, v >> 1);
+            *p++ = '\t';
+            *p++ = (v & 1) ? '-' : '+';
+            *p++ = '\t';
+            p = put_u64(p, (uint64_t)(ovlp < 0 ? 0 : ovlp));
+            *p++ = 'M';
+            *p++ = '\n';
+            used = (size_t)(p - buf.data());
+        }
+    }
+    uint64_t k = 0;
+    for (size_t q = 0; q + 1 < g->starts.size(); ++q) {  // P utg<k> <id><+|->,... *
+        const uint64_t a = g->starts[q], z = g->starts[q + 1];
+        if (z - a < 2) continue;
+        flush(32);
+        char *p = buf.data() + used;
+        std::memcpy(p, "P\tutg", 5);
+        p = put_u64(p + 5, k++);
+        *p++ = '\t';
+        used = (size_t)(p - buf.data());
+        for (uint64_t x = a; x < z; ++x) {
+            flush(32);
+            p = buf.data() + used;
+            if (x != a) *p++ = ',';
+            const uint32_t u = g->order[x];
+            p = put_u64(p, u >> 1);
+            *p++ = (u & 1) ? '-' : '+';
+            used = (size_t)(p - buf.data());
+        }
+        put("\t*\n");
+    }
+    flush(buf.size());
+    ok = ok && std::fwrite(buf.data(), 1, used, f) == used;
+    if (std::fclose(f) != 0) ok = false;
+    return ok ? EMP_OK : EMP_E_IO;
+}
+
+emp_status emp_graph_destroy(emp_graph *g) {
+    if (!g) return EMP_E_INVAL;
+    delete g;
+    return EMP_OK;
 }
 
 emp_status emp_sort_pairs(emp_ctx *ctx, uint64_t *d_keys, uint32_t *d_vals, uint64_t n, void *stream) {

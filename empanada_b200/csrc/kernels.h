@@ -61,6 +61,26 @@ bool launch_dedup_hash(const uint64_t *keys, uint64_t n, uint32_t nb, void *scra
                        uint8_t *alive, uint64_t *status, uint32_t *tile_ctr, uint64_t *total, uint32_t *err,
                        cudaStream_t s);
 
+// ---- unitigs of the overlap graph (k_graph.cu) ----------------------------
+// Device arrays of graph_build: per edge from/to (E), per node (nodes = 2n)
+// the degrees, succ/pred, two hop/dist and mn/nx buffers, unitig sizes (at
+// the heads), their starts (u64) and the nodes in unitig order; scan status
+// words (scan_tiles(nodes), zeroed), a tile counter and a total (zeroed),
+// the error word and a cycle counter (zeroed).
+struct GraphBufs {
+    uint32_t *from, *to;
+    uint32_t *dout, *din, *succ, *pred, *hop[2], *dist[2], *mn[2], *nx[2], *size, *order;
+    uint64_t *start;
+    uint64_t *status;
+    uint32_t *tile_ctr;
+    uint64_t *total;
+    uint32_t *err, *cycles;
+};
+// out: output.bin on the device; rec_off[k] its record k's byte offset,
+// rec_e0[k] the record's first edge (rec_e0[nrec] = E).
+void graph_build(const uint8_t *out, const uint64_t *rec_off, const uint64_t *rec_e0, uint32_t nrec, uint64_t E,
+                 uint32_t nodes, const GraphBufs &b, cudaStream_t s);
+
 // ---- radix sort (k_sort.cu) ---------------------------------------------
 constexpr int kSortBits = 8;
 constexpr int kSortRadix = 1 << kSortBits;

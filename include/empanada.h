@@ -245,6 +245,36 @@ emp_status emp_job_fingerprints(emp_job *job, uint64_t *keys, uint64_t cap, uint
 emp_status emp_run_file(const char *input_path, const char *output_path, const emp_params *p, int device,
                         emp_stats *st);
 
+/* Unitigs of the overlap graph in an output.bin: the downstream consumer
+ * that the reference leaves out (its GFA writers, overlap.cu:129-190, are dead
+ * code).  Nodes are read-ends (rid 2i = read i, 2i+1 = its reverse
+ * complement, i < n_reads), edges the records' (from, to) pairs.  Under the
+ * reference's remove_used rule every suffix keeps only its longest overlaps,
+ * so no edge is transitive.  A unitig is a maximal path of edges u -> v with
+ * out-degree(u) = in-degree(v) = 1 (a cycle of them is cut before its
+ * smallest read-end); every read-end is in exactly one unitig.  Built on the
+ * context's device; output_bin is host memory. */
+typedef struct emp_graph emp_graph;
+typedef struct emp_graph_stats {
+    uint64_t nodes;        /* read-ends, 2 n_reads */
+    uint64_t edges;        /* edges of output.bin */
+    uint64_t unitigs;      /* unitigs, singletons included */
+    uint64_t long_unitigs; /* unitigs of two or more read-ends */
+    uint64_t cycles;       /* cycles cut */
+    double ms_build;       /* device time of the build */
+} emp_graph_stats;
+emp_status emp_graph_build(emp_ctx *ctx, const void *output_bin, uint64_t bytes, uint64_t n_reads, emp_graph **out);
+emp_status emp_graph_get_stats(emp_graph *g, emp_graph_stats *st);
+/* The read-ends in unitig order (order[nodes]) and each unitig's first
+ * position (starts[unitigs + 1]); unitigs are ordered by their first
+ * read-end's id.  Either array may be NULL. */
+emp_status emp_graph_unitigs(emp_graph *g, uint32_t *order, uint64_t order_cap, uint64_t *starts, uint64_t starts_cap);
+/* GFA 1.0: a header, one S line per read (length read_len), one L line per
+ * edge in output.bin order (orientation + for rid 2i, - for 2i+1; overlap as
+ * <len>M), one P line per unitig of two or more read-ends. */
+emp_status emp_graph_write_gfa(emp_graph *g, const char *path, int32_t read_len);
+emp_status emp_graph_destroy(emp_graph *g);
+
 /* Stable sort of n (key, value) pairs in device memory by
  * (fp1, fp2, value>>31) -- the key order of thrust::sort_by_key on the
  * reference's fingerprints (cqutils.cuh:195).  Allocates its scratch.

@@ -70,6 +70,12 @@ def lib():
         l.emp_oracle_radix_inv.argtypes = [ctypes.c_int]
         l.emp_oracle_free.restype = None
         l.emp_oracle_free.argtypes = [ctypes.c_void_p]
+        l.emp_oracle_gfa.restype = ctypes.c_int
+        l.emp_oracle_gfa.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int32,
+                                     ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]
+        l.emp_oracle_unitigs.restype = ctypes.c_int
+        l.emp_oracle_unitigs.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_void_p,
+                                         ctypes.c_void_p, u64p]
         _lib = l
     return _lib
 
@@ -116,6 +122,33 @@ def fingerprints(fastq) -> tuple[np.ndarray, int, int]:
     if rc != OK:
         raise OracleError(rc)
     return keys[: 2 * nr.value].copy(), int(nr.value), int(L.value)
+
+
+def gfa(output_bin: bytes, n_reads: int, read_len: int) -> bytes:
+    """The unitig layer's GFA text for an output.bin (the checker of emp_graph_write_gfa)."""
+    keep, ptr, n = _buf(output_bin)
+    text = ctypes.c_void_p()
+    ln = ctypes.c_size_t()
+    rc = lib().emp_oracle_gfa(ptr, n, n_reads, read_len, ctypes.byref(text), ctypes.byref(ln))
+    del keep
+    if rc != 0:
+        raise OracleError(rc)
+    out = ctypes.string_at(text, ln.value)
+    lib().emp_oracle_free(text)
+    return out
+
+
+def unitigs(output_bin: bytes, n_reads: int) -> tuple[np.ndarray, np.ndarray]:
+    """-> (read-ends in unitig order, start of every unitig + the end)."""
+    keep, ptr, n = _buf(output_bin)
+    order = np.zeros(max(1, 2 * n_reads), dtype=np.uint32)
+    starts = np.zeros(2 * n_reads + 1, dtype=np.uint64)
+    nu = ctypes.c_uint64()
+    rc = lib().emp_oracle_unitigs(ptr, n, n_reads, order.ctypes.data, starts.ctypes.data, ctypes.byref(nu))
+    del keep
+    if rc != 0:
+        raise OracleError(rc)
+    return order[: 2 * n_reads].copy(), starts[: nu.value + 1].copy()
 
 
 def hash_of(s: str) -> int:
