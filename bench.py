@@ -701,7 +701,8 @@ def main():
         graph = {"ms_build": gst["ms_build"], "edges": gst["edges"], "unitigs": gst["unitigs"],
                  "long_unitigs": gst["long_unitigs"], "cycles": gst["cycles"],
                  "what": "unitigs (maximal paths of edges u->v with out-degree(u) = in-degree(v) = 1) of the "
-                         "job's output.bin on the device: edge scatter, degrees, pointer jumping, placement"}
+                         "job's output.bin on the device: edge scatter, degrees, one walk per unitig head, cycles "
+                         "cut at their smallest read-end, placement"}
         if rank == 0 and world == 1:
             from oracle import bind
 

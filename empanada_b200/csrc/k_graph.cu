@@ -14,9 +14,12 @@
 //   scatter   the records' edges into (from, to) arrays
 //   degree    in- and out-degree of every node
 //   link      succ / pred along the unitig edges
-//   jump      pointer jumping towards the head (a node without pred), with
-//             the distance to it; nodes that never reach one lie on cycles
-//   cycles    smallest node of every cycle by doubling; the cycle is cut there
+//   walk      one thread per head (a node without pred) follows succ and
+//             gives each node of its path the head and the distance to it;
+//             the nodes no walk reaches lie on cycles
+//   cycles    the smallest node of every cycle by doubling over pred (only
+//             cycle nodes take part); the cycle is cut before it and walked
+//             from it
 //   place     unitig sizes at their heads, starts by a scan, each node at
 //             start(head) + distance
 #include "kernels.h"
@@ -74,40 +77,29 @@ __global__ void graph_link_kernel(const uint32_t *__restrict__ from, const uint3
     }
 }
 
-// One round of pointer jumping towards the head: hop/dist in, hop2/dist2 out.
-// A node whose hop has no pred has reached its head.
-__global__ void graph_jump_kernel(const uint32_t *__restrict__ pred, const uint32_t *__restrict__ hop,
-                                  const uint32_t *__restrict__ dist, uint32_t nodes, uint32_t *__restrict__ hop2,
-                                  uint32_t *__restrict__ dist2) {
-    for (uint32_t u = blockIdx.x * kGT + threadIdx.x; u < nodes; u += gridDim.x * kGT) {
-        const uint32_t h = hop[u];
-        if (pred[h] == kNone) {
-            hop2[u] = h;
-            dist2[u] = dist[u];
-        } else {
-            hop2[u] = hop[h];
-            dist2[u] = dist[u] + dist[h];
-        }
-    }
-}
-
-// hop[u] = pred[u] (or u at a head), dist[u] = 1 (0 at a head)
-__global__ void graph_jump_init_kernel(const uint32_t *__restrict__ pred, uint32_t nodes, uint32_t *__restrict__ hop,
-                                       uint32_t *__restrict__ dist) {
-    for (uint32_t u = blockIdx.x * kGT + threadIdx.x; u < nodes; u += gridDim.x * kGT) {
-        const uint32_t p = pred[u];
-        hop[u] = p == kNone ? u : p;
-        dist[u] = p == kNone ? 0u : 1u;
+// One thread per head h (pred[h] == none, or a cycle's smallest node once
+// `cyc` is set): every node of its path gets hop = h and its distance.
+__global__ void graph_walk_kernel(const uint32_t *__restrict__ pred, const uint32_t *__restrict__ succ,
+                                  const uint32_t *__restrict__ mn, uint32_t nodes, int cyc, uint32_t *__restrict__ hop,
+                                  uint32_t *__restrict__ dist) {
+    for (uint32_t h = blockIdx.x * kGT + threadIdx.x; h < nodes; h += gridDim.x * kGT) {
+        if (cyc ? (hop[h] != kNone || mn[h] != h) : pred[h] != kNone) continue;
+        uint32_t x = h, d = 0;
+        do {
+            hop[x] = h;
+            dist[x] = d++;
+            x = succ[x];
+        } while (x != kNone && x != h && d <= nodes);
     }
 }
 
 // Cycle minimum by doubling over pred: mn/nx in, mn2/nx2 out (nodes whose
 // hop reached a head are not on a cycle and are left alone).
-__global__ void graph_cycle_min_kernel(const uint32_t *__restrict__ pred, const uint32_t *__restrict__ hop,
-                                       const uint32_t *__restrict__ mn, const uint32_t *__restrict__ nx,
-                                       uint32_t nodes, uint32_t *__restrict__ mn2, uint32_t *__restrict__ nx2) {
+__global__ void graph_cycle_min_kernel(const uint32_t *__restrict__ hop, const uint32_t *__restrict__ mn,
+                                       const uint32_t *__restrict__ nx, uint32_t nodes, uint32_t *__restrict__ mn2,
+                                       uint32_t *__restrict__ nx2) {
     for (uint32_t u = blockIdx.x * kGT + threadIdx.x; u < nodes; u += gridDim.x * kGT) {
-        if (pred[hop[u]] == kNone) continue;  // on a path
+        if (hop[u] != kNone) continue;  // on a path
         const uint32_t x = nx[u];
         mn2[u] = min(mn[u], mn[x]);
         nx2[u] = nx[x];
@@ -118,8 +110,8 @@ __global__ void graph_cycle_min_kernel(const uint32_t *__restrict__ pred, const 
 __global__ void graph_cut_kernel(const uint32_t *__restrict__ hop, const uint32_t *__restrict__ mn, uint32_t nodes,
                                  uint32_t *__restrict__ pred, uint32_t *__restrict__ succ, uint32_t *cycles) {
     for (uint32_t u = blockIdx.x * kGT + threadIdx.x; u < nodes; u += gridDim.x * kGT) {
+        if (hop[u] != kNone) continue;  // on a path
         const uint32_t p = pred[u];
-        if (p == kNone || pred[hop[u]] == kNone) continue;  // a head, or on a path
         if (mn[u] == u) {
             succ[p] = kNone;
             pred[u] = kNone;
@@ -161,29 +153,20 @@ void graph_build(const uint8_t *out, const uint64_t *rec_off, const uint64_t *re
     }
     int rounds = 1;
     while ((1ull << rounds) < (uint64_t)nodes + 1) ++rounds;
-    // jump towards the heads; then cut the cycles and jump again
-    for (int pass = 0; pass < 2; ++pass) {
-        graph_jump_init_kernel<<<gn, kGT, 0, s>>>(b.pred, nodes, b.hop[0], b.dist[0]);
-        for (int r = 0; r < rounds; ++r)
-            graph_jump_kernel<<<gn, kGT, 0, s>>>(b.pred, b.hop[r & 1], b.dist[r & 1], nodes, b.hop[(r + 1) & 1],
-                                                  b.dist[(r + 1) & 1]);
-        count_launch(1 + rounds);
-        if (rounds & 1) {  // the result in slot 0
-            cudaMemcpyAsync(b.hop[0], b.hop[1], (size_t)nodes * 4, cudaMemcpyDeviceToDevice, s);
-            cudaMemcpyAsync(b.dist[0], b.dist[1], (size_t)nodes * 4, cudaMemcpyDeviceToDevice, s);
-        }
-        if (pass == 1) break;
-        // cycle minimum: mn = node, nx = pred, doubling (only nodes on cycles move)
-        launch_iota(b.mn[0], nodes, s);
-        cudaMemcpyAsync(b.nx[0], b.pred, (size_t)nodes * 4, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(b.mn[1], b.mn[0], (size_t)nodes * 4, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(b.nx[1], b.nx[0], (size_t)nodes * 4, cudaMemcpyDeviceToDevice, s);
-        for (int r = 0; r < rounds; ++r)
-            graph_cycle_min_kernel<<<gn, kGT, 0, s>>>(b.pred, b.hop[0], b.mn[r & 1], b.nx[r & 1], nodes,
-                                                       b.mn[(r + 1) & 1], b.nx[(r + 1) & 1]);
-        graph_cut_kernel<<<gn, kGT, 0, s>>>(b.hop[0], b.mn[rounds & 1], nodes, b.pred, b.succ, b.cycles);
-        count_launch(rounds + 1);
-    }
+    // the paths from their heads; the nodes left (hop = none) lie on cycles
+    cudaMemsetAsync(b.hop[0], 0xff, (size_t)nodes * 4, s);
+    graph_walk_kernel<<<gn, kGT, 0, s>>>(b.pred, b.succ, nullptr, nodes, 0, b.hop[0], b.dist[0]);
+    // cycle minimum: mn = node, nx = pred, doubling over the cycle nodes only
+    launch_iota(b.mn[0], nodes, s);
+    cudaMemcpyAsync(b.nx[0], b.pred, (size_t)nodes * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(b.mn[1], b.mn[0], (size_t)nodes * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(b.nx[1], b.nx[0], (size_t)nodes * 4, cudaMemcpyDeviceToDevice, s);
+    for (int r = 0; r < rounds; ++r)
+        graph_cycle_min_kernel<<<gn, kGT, 0, s>>>(b.hop[0], b.mn[r & 1], b.nx[r & 1], nodes, b.mn[(r + 1) & 1],
+                                                   b.nx[(r + 1) & 1]);
+    graph_cut_kernel<<<gn, kGT, 0, s>>>(b.hop[0], b.mn[rounds & 1], nodes, b.pred, b.succ, b.cycles);
+    graph_walk_kernel<<<gn, kGT, 0, s>>>(b.pred, b.succ, b.mn[rounds & 1], nodes, 1, b.hop[0], b.dist[0]);
+    count_launch(rounds + 3);
     graph_size_kernel<<<gn, kGT, 0, s>>>(b.hop[0], nodes, b.size);
     launch_scan_u32_u64(b.size, b.start, nodes, b.status, b.tile_ctr, b.total, b.err, s);
     graph_place_kernel<<<gn, kGT, 0, s>>>(b.hop[0], b.dist[0], b.start, nodes, b.order);
