@@ -11,8 +11,10 @@
 //   hist     per-CTA shared-memory histogram of the key buckets (the top
 //            bits of fp1 scaled to nb buckets), added into global counts
 //   (scan)   bucket starts, copied to the bucket cursors
-//   scatter  each (key, rid) to its bucket, one atomic per run of equal
-//            buckets within a warp
+//   scatter  each (key, rid) to its bucket: a CTA ranks a tile of keys per
+//            bucket in shared memory and reserves each bucket's run with one
+//            atomic (up to 2048 buckets), or one atomic per run of equal
+//            buckets within a warp (more buckets, cursors rarely shared)
 //   mark     one CTA per bucket: a shared-memory hash set of the bucket's
 //            distinct keys holding the smallest rid of each (atomicMin),
 //            then alive[rid] = (rid is its key's smallest)
@@ -72,6 +74,48 @@ __global__ void __launch_bounds__(kDT) dedup_scatter_kernel(const uint64_t *__re
         pos = __shfl_sync(peers, pos, leader) + __popc(peers & lanemask_lt_u32());
         pk[pos] = k;
         pr[pos] = (uint32_t)e;
+    }
+}
+
+// The same for few buckets (nb <= kTiledBuckets), where the bucket cursors
+// would be hot: a CTA ranks a tile of kScatterTile keys per bucket in shared
+// memory and reserves each bucket's run with one atomic.
+constexpr uint32_t kTiledBuckets = 2048;
+constexpr int kScatterPer = 16;
+constexpr uint32_t kScatterTile = kDT * kScatterPer;
+
+__global__ void __launch_bounds__(kDT) dedup_scatter_tiled_kernel(const uint64_t *__restrict__ keys, uint64_t n,
+                                                                  uint32_t nb, uint32_t *__restrict__ cursor,
+                                                                  uint64_t *__restrict__ pk,
+                                                                  uint32_t *__restrict__ pr) {
+    __shared__ uint32_t s_cnt[kTiledBuckets];
+    for (uint64_t t0 = (uint64_t)blockIdx.x * kScatterTile; t0 < n; t0 += (uint64_t)gridDim.x * kScatterTile) {
+        for (uint32_t b = threadIdx.x; b < nb; b += kDT) s_cnt[b] = 0;
+        __syncthreads();
+        uint64_t k[kScatterPer];
+        uint32_t bk[kScatterPer], rk[kScatterPer];
+#pragma unroll
+        for (int q = 0; q < kScatterPer; ++q) {
+            const uint64_t e = t0 + (uint64_t)q * kDT + threadIdx.x;
+            k[q] = e < n ? __ldg(keys + e) : 0;
+            bk[q] = e < n ? dedup_bucket(k[q], nb) : 0u;
+            rk[q] = e < n ? atomicAdd(&s_cnt[bk[q]], 1u) : 0u;
+        }
+        __syncthreads();
+        for (uint32_t b = threadIdx.x; b < nb; b += kDT) {
+            const uint32_t c = s_cnt[b];
+            s_cnt[b] = c ? atomicAdd(cursor + b, c) : 0u;  // the run's global start
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kScatterPer; ++q) {
+            const uint64_t e = t0 + (uint64_t)q * kDT + threadIdx.x;
+            if (e >= n) continue;
+            const uint32_t pos = s_cnt[bk[q]] + rk[q];
+            pk[pos] = k[q];
+            pr[pos] = (uint32_t)e;
+        }
+        __syncthreads();
     }
 }
 
@@ -179,8 +223,14 @@ bool launch_dedup_hash(const uint64_t *keys, uint64_t n, uint32_t nb, void *scra
     dedup_hist_kernel<<<g_hist, kDT, nb * 4, s>>>(keys, n, nb, counts);
     launch_scan_u32_u64(counts, start, nb, status, tile_ctr, total, err, s);
     dedup_cursor_kernel<<<(nb + kDT - 1) / kDT, kDT, 0, s>>>(start, nb, cursor);
-    const unsigned g_sc = (unsigned)(per < (uint64_t)sms * 8 ? per : (uint64_t)sms * 8);
-    dedup_scatter_kernel<<<g_sc, kDT, 0, s>>>(keys, n, nb, cursor, pk, pr);
+    if (nb <= kTiledBuckets) {
+        const uint64_t tiles = (n + kScatterTile - 1) / kScatterTile;
+        const unsigned g_t = (unsigned)(tiles < (uint64_t)sms * 8 ? tiles : (uint64_t)sms * 8);
+        dedup_scatter_tiled_kernel<<<g_t, kDT, 0, s>>>(keys, n, nb, cursor, pk, pr);
+    } else {
+        const unsigned g_sc = (unsigned)(per < (uint64_t)sms * 8 ? per : (uint64_t)sms * 8);
+        dedup_scatter_kernel<<<g_sc, kDT, 0, s>>>(keys, n, nb, cursor, pk, pr);
+    }
     const unsigned g_mark = nb < (uint32_t)sms * 2 ? nb : (uint32_t)sms * 2;
     dedup_mark_hash_kernel<<<g_mark, kDT, kMarkSmem, s>>>(pk, pr, start, nb, n, alive, err);
     return true;
