@@ -40,12 +40,16 @@ enum ErrBits : uint32_t {
 
 // Powers R^i mod P for i <= kMaxReadLen and the radix inverses (fingerprint.cu:26-34,
 // overlap.cu:121-122).  Lives in device memory; staged into shared memory by
-// the kernels that need it.
+// the kernels that need it.  chunk[c] holds the weights of read positions
+// 16c .. 16c+15 for the read pass (Rinv = R^-1 mod P):
+//   Rinv1^(16c+7), Rinv1^(16c+15), Rinv2^(16c+7), Rinv2^(16c+15),
+//   R1^(16c), R1^(16c+8), R2^(16c), R2^(16c+8)
 struct HashTables {
     uint32_t pow1[kMaxReadLen + 1];
     uint32_t pow2[kMaxReadLen + 1];
     uint32_t inv1;
     uint32_t inv2;
+    uint32_t chunk[kMaxReadLen / 16][8];
 };
 
 // x mod (2^29 - C) for any 64-bit x: two pseudo-Mersenne folds then one
@@ -103,6 +107,43 @@ EMP_DEV uint64_t prev_pfx(uint64_t key, uint32_t v, uint32_t inv1, uint32_t inv2
 // 59-bit sort key: (fp1, fp2) order-preserving in 58 bits, table bit below.
 EMP_DEV uint64_t sort_key(uint64_t key, uint32_t val) {
     return ((key >> 32) << 30) | ((key & kMask29) << 1) | (val >> 31);
+}
+
+// ---------------------------------------------------------------- bulk copies
+// One-dimensional TMA copies global -> shared completed on an mbarrier (the
+// copy engine moves the bytes; one thread issues them).  Both addresses and
+// the size must be multiples of 16 bytes.
+EMP_DEV uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+EMP_DEV void mbar_init(uint64_t *bar, uint32_t arrivals) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(arrivals) : "memory");
+}
+// generic-proxy accesses of shared memory before this point are ordered
+// before later async-proxy (bulk copy) accesses, and mbarrier inits are seen
+EMP_DEV void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+EMP_DEV void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+// arrive, expecting `bytes` of bulk copies, and start one copy of `bytes`
+EMP_DEV void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// wait for the barrier's phase `parity` to complete; false after `limit` polls
+EMP_DEV bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
 }
 
 // ---------------------------------------------------------------- look-back

@@ -55,6 +55,14 @@ struct DevBuf {
     T *as() const { return reinterpret_cast<T *>(p); }
 };
 
+// exchange two buffers (both from the same pool)
+void swap_buf(DevBuf &a, DevBuf &b) {
+    std::swap(a.p, b.p);
+    std::swap(a.bytes, b.bytes);
+    std::swap(a.pool_stream, b.pool_stream);
+    std::swap(a.pooled, b.pooled);
+}
+
 struct PinnedBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -170,7 +178,7 @@ struct emp_job {
     bool fed_last = false;
     double ms_h2d = 0.0;
     // work buffers
-    DevBuf tile_counts, tile_excl, status, misc, seq_start, seq_end, keys0, cols, seq2, dedup_scr;
+    DevBuf tile_counts, tile_excl, status, misc, keys0, cols, seq2, dedup_scr, keep, keys_tmp, seq2_tmp;
     DevBuf sk0, sv0, sk1, sv1, alive, lk0, lv0, lk1, lv1, used_s, used_p, cnt, offs, efrom, eto, sort_scratch;
     DevBuf akeys, apos, bkeys, parts;  // record splitting
     DevBuf xk0, xv0, xk1, xv1, ring_k, ring_v, cparts;  // sort of a table larger than M
@@ -216,7 +224,8 @@ namespace {
 
 // misc device words (u64 slots)
 enum MiscSlot { kMiscErr = 0, kMiscTotal = 1, kMiscLen = 2, kMiscN = 3, kMiscU = 4, kMiscNout = 5, kMiscSout = 6,
-                kMiscE = 7, kMiscCtr = 8, kMiscParts = 9, kMiscSortN = 10, kMiscLen0 = 11, kMiscSlots = 16 };
+                kMiscE = 7, kMiscCtr = 8, kMiscParts = 9, kMiscSortN = 10, kMiscLen0 = 11, kMiscKept = 12,
+                kMiscSlots = 16 };
 
 // internal: the pipeline's edge buffer was too small (never returned by the ABI)
 constexpr emp_status kNeedEdgeRoom = -1000;
@@ -279,6 +288,17 @@ void host_tables(HashTables &t) {
     }
     t.inv1 = host_modpow(kR1, kP1 - 2, kP1);
     t.inv2 = host_modpow(kR2, kP2 - 2, kP2);
+    for (int c = 0; c < kMaxReadLen / 16; ++c) {
+        const uint64_t t0 = 16ull * c;
+        t.chunk[c][0] = host_modpow(t.inv1, (uint32_t)(t0 + 7), kP1);
+        t.chunk[c][1] = host_modpow(t.inv1, (uint32_t)(t0 + 15), kP1);
+        t.chunk[c][2] = host_modpow(t.inv2, (uint32_t)(t0 + 7), kP2);
+        t.chunk[c][3] = host_modpow(t.inv2, (uint32_t)(t0 + 15), kP2);
+        t.chunk[c][4] = t.pow1[t0];
+        t.chunk[c][5] = t.pow1[t0 + 8];
+        t.chunk[c][6] = t.pow2[t0];
+        t.chunk[c][7] = t.pow2[t0 + 8];
+    }
 }
 
 #define EMP_TRY(x)                         \
@@ -884,15 +904,6 @@ emp_status map_records(emp_job *j, cudaStream_t s) {
     }
     // the map kernels load the FASTQ as aligned 16-byte blocks
     if (reinterpret_cast<uintptr_t>(j->fq.p) & 15u) return EMP_E_CUDA;
-    EMP_TRY(ensure(j, j->seq_start, n_rec * 8));
-    EMP_TRY(ensure(j, j->seq_end, n_rec * 8));
-    launch_nl_locate(j->fq.as<uint8_t>(), F, j->tile_excl.as<uint64_t>(), j->seq_start.as<uint64_t>(),
-                     j->seq_end.as<uint64_t>(), s);
-    if ((total_nl - 1) % 4 == 0) {  // last sequence line ends at end of input
-        hm[kMiscSlots - 1] = F;
-        EMP_CUDA(cudaMemcpyAsync(j->seq_end.as<uint64_t>() + n_rec - 1, hm + kMiscSlots - 1, 8,
-                                 cudaMemcpyHostToDevice, s));
-    }
     // ---- K2: every record in one pass: N filter, length, fingerprints of
     // both read-ends, read-major 2-bit words; kept reads numbered in order.
     // The words are laid out for the first record's length (the usual case:
@@ -911,14 +922,13 @@ emp_status launch_reads(emp_job *j, cudaStream_t s, int wpr) {
     j->prep.wpr = wpr;
     EMP_TRY(ensure(j, j->keys0, n_rec * 16));
     EMP_TRY(ensure(j, j->seq2, n_rec * (uint64_t)wpr * 4));
-    const uint32_t mm[2] = {0xffffffffu, 0u};
-    std::memcpy(hm + kMiscLen, mm, 8);
-    EMP_CUDA(cudaMemcpyAsync(dm + kMiscLen, hm + kMiscLen, 8, cudaMemcpyHostToDevice, s));
-    EMP_TRY(reset_chain(j, (n_rec + kReadTileRecs - 1) / kReadTileRecs, s));
-    launch_read_hash(j->fq.as<uint8_t>(), j->seq_start.as<uint64_t>(), j->seq_end.as<uint64_t>(), n_rec,
-                     j->ctx->tables.as<HashTables>(), j->keys0.as<uint64_t>(), j->seq2.as<uint32_t>(), wpr,
-                     j->status.as<uint64_t>(), chain_ctr(j), dm + kMiscN, reinterpret_cast<uint32_t *>(dm + kMiscLen),
-                     err_word(j), s);
+    EMP_TRY(ensure(j, j->keep, n_rec * 4));
+    const uint32_t mm[4] = {0xffffffffu, 0u, 0u, 0u};  // length extremes, then the kept count
+    std::memcpy(hm + kMiscLen, mm, 16);
+    EMP_CUDA(cudaMemcpyAsync(dm + kMiscLen, hm + kMiscLen, 16, cudaMemcpyHostToDevice, s));
+    launch_read_pass(j->fq.as<uint8_t>(), j->F, j->tile_excl.as<uint64_t>(), j->ctx->tables.as<HashTables>(),
+                     j->keys0.as<uint64_t>(), j->seq2.as<uint32_t>(), wpr, j->keep.as<uint32_t>(), dm + kMiscN,
+                     reinterpret_cast<uint32_t *>(dm + kMiscLen), err_word(j), s);
     cudaEventRecord(j->map_ev[1], s);
     return EMP_OK;
 }
@@ -964,6 +974,17 @@ emp_status map_keys(emp_job *j, cudaStream_t s) {
         EMP_TRY(launch_reads(j, s, (L + 15) / 16));
         EMP_TRY(sync_and_check(j, s));
         if (hm[kMiscErr] & kErrBadBase) return EMP_E_FORMAT;
+    }
+    if (n < q.n_rec) {  // the N filter or an empty line dropped a record: the kept ones to indices 0 .. n-1
+        EMP_TRY(ensure(j, j->keys_tmp, n * 16));
+        EMP_TRY(ensure(j, j->seq2_tmp, n * (uint64_t)q.wpr * 4));
+        EMP_TRY(reset_chain(j, scan_tiles(q.n_rec), s));
+        launch_scan_u32_u32(j->keep.as<uint32_t>(), j->keep.as<uint32_t>(), q.n_rec, j->status.as<uint64_t>(),
+                            chain_ctr(j), dm + kMiscKept, err_word(j), s);
+        launch_compact_reads(j->keep.as<uint32_t>(), q.n_rec, n, j->keys0.as<uint64_t>(), j->seq2.as<uint32_t>(),
+                             q.wpr, j->keys_tmp.as<uint64_t>(), j->seq2_tmp.as<uint32_t>(), s);
+        swap_buf(j->keys0, j->keys_tmp);
+        swap_buf(j->seq2, j->seq2_tmp);
     }
     // ---- column-major 2-bit store, for rounds that run outside the bucket kernel
     q.wpc = (n + 15) / 16;
@@ -1745,9 +1766,8 @@ emp_status emp_job_destroy(emp_job *job) {
 
 // every device buffer of the job back to the context (its pool)
 static void release_buffers(emp_job *job) {
-    DevBuf *bufs[] = {&job->fq, &job->tile_counts, &job->tile_excl, &job->status, &job->misc, &job->seq_start,
-                      &job->seq_end, &job->keys0, &job->dedup_scr, &job->cols, &job->seq2, &job->sk0,
-                      &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
+    DevBuf *bufs[] = {&job->fq, &job->tile_counts, &job->tile_excl, &job->status, &job->misc, &job->keys0,
+                      &job->keep, &job->keys_tmp, &job->seq2_tmp, &job->dedup_scr, &job->cols, &job->seq2, &job->sk0, &job->sv0, &job->sk1, &job->sv1, &job->alive, &job->lk0, &job->lv0, &job->lk1, &job->lv1,
                       &job->used_s, &job->used_p, &job->cnt, &job->offs, &job->efrom, &job->eto,
                       &job->sort_scratch, &job->akeys, &job->apos, &job->bkeys, &job->parts, &job->records, &job->coop_ctl, &job->coop_trace,
                       &job->coop_probe, &job->bk_lst0, &job->bk_lst1, &job->bk_cnt, &job->bk_spill, &job->bk_spans,

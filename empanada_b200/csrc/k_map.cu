@@ -13,13 +13,15 @@
 // Kernels
 //   nl_count      newline count of each 16 KB tile (16-byte vector loads);
 //                 tile 0 also measures the first record's sequence line
-//   nl_locate     global line id of every newline -> start/end of each
-//                 record's sequence line
-//   read_hash     one thread per record: N filter, ACGT check, length, both
-//                 fingerprints and the read-major 2-bit words in one walk
-//                 over the sequence line; kept reads get their index from a
-//                 decoupled look-back over the tiles' kept counts
+//   read_pass     one CTA per tile staged in shared memory: the records'
+//                 sequence lines, N filter, ACGT check, length, both
+//                 fingerprints and the read-major 2-bit words, at each
+//                 record's own index
+//   compact_reads the kept records to consecutive indices (only when the
+//                 N filter or an empty line dropped one)
 //   columns       read-major words -> column-major words (only when needed)
+#include <atomic>
+
 #include "sort_block.cuh"
 
 namespace emp {
@@ -92,224 +94,380 @@ __global__ void __launch_bounds__(256) nl_count_kernel(const uint8_t *__restrict
     if (threadIdx.x == 0) *len0 = (s_nl[0] != 0xffffffffu && s_nl[1] != 0xffffffffu) ? s_nl[1] - s_nl[0] - 1 : 0;
 }
 
-// Newline g ends line g.  Line 4k+1 is record k's sequence: it starts after
-// newline 4k and ends at newline 4k+1.  Thread t of a tile takes its 64
-// consecutive bytes (4 x 16-byte loads): one CTA scan of the per-thread
-// newline counts gives each thread the line id of its first newline.
-__global__ void __launch_bounds__(256) nl_locate_kernel(const uint8_t *__restrict__ fq, uint64_t F,
-                                                        const uint64_t *__restrict__ tile_excl,
-                                                        uint64_t *__restrict__ seq_start,
-                                                        uint64_t *__restrict__ seq_end) {
-    __shared__ uint32_t s_warp[8];
-    const uint64_t base = (uint64_t)blockIdx.x * kParseTile + (uint64_t)threadIdx.x * 64;
-    uint32_t w[16];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint64_t off = base + 16 * k;
-        if (off + 16 <= F) {
-            const uint4 v = __ldg(reinterpret_cast<const uint4 *>(fq + off));
-            w[4 * k] = v.x;
-            w[4 * k + 1] = v.y;
-            w[4 * k + 2] = v.z;
-            w[4 * k + 3] = v.w;
-        } else {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) w[4 * k + q] = 0;
-            for (int bb = 0; bb < 16; ++bb)
-                if (off + bb < F) w[4 * k + (bb >> 2)] |= (uint32_t)fq[off + bb] << (8 * (bb & 3));
-        }
-    }
-    uint32_t cnt = 0;
-#pragma unroll
-    for (int q = 0; q < 16; ++q) cnt += nl_in_word(w[q]);
-    uint32_t tot;
-    uint64_t my = tile_excl[blockIdx.x] + block_exclusive_scan<256, uint32_t>(cnt, s_warp, &tot);
-    if (!cnt) return;
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-        uint32_t m = __vcmpeq4(w[q], 0x0a0a0a0au);  // 0xff in each newline byte
-        while (m) {
-            const int bb = (__ffs(m) - 1) >> 3;
-            m &= ~(0xffu << (8 * bb));
-            const uint64_t pos = base + 4 * q + bb;
-            const uint32_t r = (uint32_t)(my & 3u);
-            if (r == 0) seq_start[my >> 2] = pos + 1;
-            else if (r == 1) seq_end[my >> 2] = pos;
-            ++my;
-        }
-    }
-}
-
 // 0x80 in every byte of t that is zero, 0 elsewhere (no carries between bytes)
 EMP_DEV uint32_t zero_bytes(uint32_t t) { return ~(((t & 0x7f7f7f7fu) + 0x7f7f7f7fu) | t | 0x7f7f7f7fu); }
 
-// N-class bytes (markNs == 9, preprocess.cu:119-121: bits 7-6 = 01 and bit 3
-// set) and bytes outside ACGTacgt among the bytes of x selected by m (0x80
-// per byte)
-EMP_DEV void check4(uint32_t x, uint32_t m, uint32_t &nm, uint32_t &bm) {
-    const uint32_t f = x | 0x20202020u;  // case folded
-    nm |= zero_bytes((x & 0xc8c8c8c8u) ^ 0x48484848u) & m;
-    const uint32_t ok = zero_bytes(f ^ 0x61616161u) | zero_bytes(f ^ 0x63636363u) | zero_bytes(f ^ 0x67676767u) |
-                        zero_bytes(f ^ 0x74747474u);  // a c g t
-    bm |= ~ok & m;
-}
-
 // ---------------------------------------------------------------- reads
-// One thread per FASTQ record, kReadTile records per tile, tiles taken in
-// order from a ticket.  Per record, one walk over its sequence line in
-// aligned 16-byte blocks gives
-//   * the N filter and the ACGT check;
-//   * both fingerprints as sums of per-word terms (the Horner form of
-//     FingerprintMul expanded):
-//         H(read)    = sum_t enc(b_t) R^(L-1-t)         mod P
-//         H(revcomp) = sum_t enc(comp b_t) R^t          mod P
-//     a memory word holding bases t .. t+3 of the read adds
-//         (e0 R^3 + e1 R^2 + e2 R + e3) R^(L-4-t)  and  (e'0 + e'1 R + e'2 R^2 + e'3 R^3) R^t,
-//     each below 2^41, to 64-bit sums (at most 129 words per read: below
-//     2^49) that are reduced once; the words cut by the read's ends go byte
-//     by byte;
-//   * the read-major 2-bit words (16 bases per word, first base in bits 1-0).
-// The kept records of a tile get consecutive read indices after the kept
-// records of all earlier tiles (decoupled look-back on the kept count).
-constexpr int kReadTile = 256;
-constexpr int kSeqWordsMax = kMaxReadLen / 16;
+// One CTA per 16 KB FASTQ tile (the tiles of nl_count), the tile and the
+// 1 KB after it staged in shared memory.  A record belongs to the tile that
+// holds the newline ending its header (line 4k); its sequence line runs from
+// there to newline 4k+1, or to the end of the input.
+//
+//   locate   each thread counts the newlines of 64 tile bytes and 4 halo
+//            bytes; one block scan gives every newline its line id, and the
+//            tile's records their sequence bounds (window offsets)
+//   records  G lanes per record (G from the tile's record count), 16 bases
+//            a lane:
+//            * a byte is one of ACGTacgt iff it equals "ACTG"[(b >> 1) & 3]
+//              up to case (two byte permutes per 4 bytes); only a read that
+//              fails this is searched for N-class bytes (markNs == 9).  The
+//              record is kept when it holds no N-class byte and is not empty;
+//            * the lane's bases give one read-major 2-bit word and, per
+//              fingerprint, two 8-base dot products (dp4a / dp2a) weighted
+//              by the chunk's constants:
+//                H(read)    = R^(L-1) * sum_t enc(b_t) R^-t      mod P
+//                H(revcomp) =           sum_t enc(comp b_t) R^t  mod P
+//              (FingerprintMul's Horner form regrouped: the same residues);
+//              64-bit partial sums meet in a shuffle reduction.
+// Outputs go to the record's own index k (keys[2k], seq2[k * wpr ..]) with
+// keep[k]; the kept count is summed with one atomic per tile.  When a record
+// was dropped, compact_reads moves the kept ones to consecutive indices.  A
+// sequence line that does not end inside the window (over 1 KB: never
+// hashed) is checked by one lane straight from global memory.
+constexpr int kRT = 256;
+constexpr uint32_t kHalo = 528;  // a line of kMaxReadLen bases starting at the tile's end, rounded to 16
+constexpr uint32_t kWin = (uint32_t)kParseTile + kHalo;
+constexpr uint32_t kWinWords = kWin / 4;
+constexpr uint32_t kRecCap = 2048;  // records per batch (a tile owns up to 4096: four newlines each)
+constexpr uint16_t kNoEnd = 0xffffu;
+constexpr int kChunks = kMaxReadLen / 16;
+static_assert(kParseTile == 64 * kRT, "four 16-byte tile chunks per thread");
+static_assert(kHalo % 16 == 0 && kHalo / 16 <= kRT && kHalo >= kMaxReadLen + 1, "one halo chunk per thread at most");
+static_assert(kWin < kNoEnd, "window offsets fit 16 bits");
 static_assert(kMaxReadLen % 16 == 0, "whole read-major words");
 
-__global__ void __launch_bounds__(kReadTile) read_hash_kernel(
-    const uint8_t *__restrict__ fq, const uint64_t *__restrict__ seq_start, const uint64_t *__restrict__ seq_end,
-    uint64_t n_rec, const HashTables *__restrict__ tables, uint64_t *__restrict__ keys, uint32_t *__restrict__ seq2,
-    int wpr, uint64_t *status, uint32_t *tile_ctr, uint64_t *n_kept, uint32_t *len_minmax, uint32_t *err) {
-    __shared__ uint32_t s_pow1[kMaxReadLen + 1], s_pow2[kMaxReadLen + 1];
-    __shared__ uint32_t s_words[kSeqWordsMax][kReadTile + 1];  // [word][thread]
-    __shared__ uint16_t s_who[kReadTile];                      // kept rank -> thread
-    __shared__ uint32_t s_wcnt[kReadTile / 32];
-    __shared__ uint32_t s_tile, s_kept;
-    __shared__ uint64_t s_base;
-    for (int i = threadIdx.x; i <= kMaxReadLen; i += kReadTile) {
-        s_pow1[i] = tables->pow1[i];
-        s_pow2[i] = tables->pow2[i];
+struct __align__(16) ReadSmem {
+    uint32_t win[2][kWinWords + 8];  // two windows (zero past the input), each then zero padding
+    uint32_t chunk[kChunks][8];      // HashTables::chunk
+    uint16_t start[kRecCap];         // sequence line [start, end) of the batch's records (window offsets)
+    uint16_t end[kRecCap];           // kNoEnd: no newline ends it inside the window
+    uint64_t scan[kRT / 32];
+    uint64_t bar[2];  // bulk-copy barriers of the two windows
+};
+
+// newline bytes of a word as 4 bits (byte b -> bit b): the bytes' top bits
+// gathered by one multiply (partial products land on distinct bits)
+EMP_DEV uint32_t nl_bits(uint32_t w) { return ((zero_bytes(w ^ 0x0a0a0a0au) >> 7) * 0x00204081u) >> 21 & 0xfu; }
+
+// 16 window bytes from byte offset off (any alignment): x[q] = bytes off+4q ..
+EMP_DEV void win16(const uint32_t *win, uint32_t off, uint32_t x[4]) {
+    const uint32_t w = off >> 2, sh = (off & 3u) * 8u;
+    uint32_t a = win[w];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const uint32_t b = win[w + q + 1];
+        x[q] = __funnelshift_r(a, b, sh);
+        a = b;
     }
+}
+// 0xff in the first n bytes of a word (n clamped to 0..4)
+EMP_DEV uint32_t lead_bytes(int n) { return n >= 4 ? 0xffffffffu : n <= 0 ? 0u : (1u << (8 * n)) - 1u; }
+// nonzero iff a byte of x selected by vm is not one of ACGTacgt
+EMP_DEV uint32_t not_acgt(uint32_t x, uint32_t vm) {
+    const uint32_t c = (x >> 1) & 0x03030303u;
+    const uint32_t sel = __byte_perm(c | (c >> 4), 0u, 0x4420u);  // the codes as byte selectors
+    const uint32_t want = __byte_perm(0x47544341u, 0u, sel);       // "ACTG"[code]
+    return (x ^ want) & 0xdfdfdfdfu & vm;
+}
+// nonzero iff a byte of x selected by vm is N-class (bits 7-6 = 01, bit 3 set)
+EMP_DEV uint32_t n_class(uint32_t x, uint32_t vm) { return zero_bytes((x & 0xc8c8c8c8u) ^ 0x48484848u) & vm; }
+// 4-base dot products of enc values in bytes (first base first), added to acc
+EMP_DEV uint32_t fw1(uint32_t e, uint32_t acc) { return __dp4a(e, 0x0105197Du, acc); }  // 125 25 5 1
+EMP_DEV uint32_t rc1(uint32_t e, uint32_t acc) { return __dp4a(e, 0x7D190501u, acc); }  // 1 5 25 125
+EMP_DEV uint32_t fw2(uint32_t e, uint32_t acc) {  // 343 49 7 1
+    return __dp2a_lo(0x00310157u, e, __dp2a_hi(0x00010007u, e, acc));
+}
+EMP_DEV uint32_t rc2(uint32_t e, uint32_t acc) {  // 1 7 49 343
+    return __dp2a_lo(0x00070001u, e, __dp2a_hi(0x01570031u, e, acc));
+}
+
+// One lane's 16 bases (x: the chunk's bytes, nv of them in the read; kFull:
+// all 16): the bytes' mismatches against "ACTG"[code] ORed into bad (a
+// mismatch outside bit 5, the case bit, is a byte outside ACGTacgt), the
+// read-major word, and the weighted 8-base sums into the fingerprint
+// accumulators.  Each 8-base sum is below 2^22 and each weight below 2^29; a
+// read adds at most 64 products.
+template <bool kFull>
+EMP_DEV void read_chunk(const uint32_t x[4], int nv, const uint32_t *kc, uint32_t &bad, uint32_t &word, uint64_t &f1,
+                        uint64_t &f2, uint64_t &g1, uint64_t &g2) {
+    uint32_t e[4], ec[4], p[4];
+    const uint32_t s8 = (uint32_t)(nv > 16 ? 16 : nv) * 8u;  // valid bits of the chunk
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const uint32_t vm = kFull ? 0xffffffffu : __funnelshift_lc(0xffffffffu, 0u, s8 > 32u * q ? s8 - 32u * q : 0u);
+        const uint32_t c = (x[q] >> 1) & 0x03030303u;
+        const uint32_t want = __byte_perm(0x47544341u, 0u, __byte_perm(c | (c >> 4), 0u, 0x4420u));  // "ACTG"[code]
+        bad |= kFull ? x[q] ^ want : (x[q] ^ want) & vm;
+        const uint32_t cq = c & vm;  // A0 C1 T2 G3
+        e[q] = kFull ? cq + 0x01010101u : (cq + 0x01010101u) & vm;
+        ec[q] = kFull ? (cq ^ 0x02020202u) + 0x01010101u : ((cq ^ 0x02020202u) + 0x01010101u) & vm;
+        p[q] = cq * 0x01041040u;  // byte 3: the four codes, 2 bits each, first lowest
+    }
+    word = __byte_perm(__byte_perm(p[0], p[1], 0x0073u), __byte_perm(p[2], p[3], 0x0073u), 0x5410u);
+    f1 += (uint64_t)fw1(e[1], fw1(e[0], 0u) * 625u) * kc[0];
+    f1 += (uint64_t)fw1(e[3], fw1(e[2], 0u) * 625u) * kc[1];
+    f2 += (uint64_t)fw2(e[1], fw2(e[0], 0u) * 2401u) * kc[2];
+    f2 += (uint64_t)fw2(e[3], fw2(e[2], 0u) * 2401u) * kc[3];
+    g1 += (uint64_t)rc1(ec[0], rc1(ec[1], 0u) * 625u) * kc[4];
+    g1 += (uint64_t)rc1(ec[2], rc1(ec[3], 0u) * 625u) * kc[5];
+    g2 += (uint64_t)rc2(ec[0], rc2(ec[1], 0u) * 2401u) * kc[6];
+    g2 += (uint64_t)rc2(ec[2], rc2(ec[3], 0u) * 2401u) * kc[7];
+}
+
+// The window of tile `tile` into dst: thread 0 starts one bulk copy of the
+// input's whole 16-byte blocks (completing on bar); the bytes after them up
+// to kWin (the input's last partial block, then zeros) are written by all
+// threads.  Called by every thread of the CTA.
+EMP_DEV void stage_window(const uint8_t *fq, uint64_t F, uint64_t tile, uint32_t *dst, uint64_t *bar) {
+    const uint64_t T0 = tile * kParseTile, avail = F - T0;  // tile < parse_tiles(F): avail >= 1
+    const uint32_t nbulk = (uint32_t)(avail < kWin ? avail : kWin) & ~15u;
+    if (threadIdx.x == 0) {
+        fence_proxy_async();  // the buffer's last reads (generic) before the copy's writes
+        if (nbulk) bulk_load(dst, fq + T0, nbulk, bar);
+        else mbar_arrive(bar);
+    }
+    for (uint32_t w = nbulk / 4 + threadIdx.x; w < kWinWords; w += kRT) {  // only near the input's end
+        uint32_t v = 0;
+        for (uint32_t b = 0; b < 4; ++b)
+            if (4ull * w + b < avail) v |= (uint32_t)fq[T0 + 4ull * w + b] << (8 * b);
+        dst[w] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kRT, 4) read_pass_kernel(const uint8_t *__restrict__ fq, uint64_t F,
+                                                        const uint64_t *__restrict__ tile_excl,
+                                                        const HashTables *__restrict__ tables,
+                                                        uint64_t *__restrict__ keys, uint32_t *__restrict__ seq2,
+                                                        int wpr, uint32_t *__restrict__ keep_out, uint64_t *n_kept,
+                                                        uint32_t *len_minmax, uint32_t *err) {
+    extern __shared__ __align__(16) uint8_t read_smem[];
+    ReadSmem &sm = *reinterpret_cast<ReadSmem *>(read_smem);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint64_t ntiles = (n_rec + kReadTile - 1) / kReadTile;
-    for (;;) {
-        if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
+    for (int i = tid; i < kChunks * 8; i += kRT) sm.chunk[i >> 3][i & 7] = tables->chunk[i >> 3][i & 7];
+    for (int i = tid; i < (int)kRecCap; i += kRT) sm.end[i] = kNoEnd;  // each use resets its slots
+    if (tid < 16) sm.win[tid >> 3][kWinWords + (tid & 7)] = 0;
+    if (tid == 0) {
+        mbar_init(&sm.bar[0], 1);
+        mbar_init(&sm.bar[1], 1);
+        fence_proxy_async();
+    }
+    __syncthreads();
+    const uint64_t ntiles = parse_tiles(F);
+    uint32_t lmin = 0xffffffffu, lmax = 0u, bad_kept = 0u, kept = 0u;
+    if (blockIdx.x < ntiles) stage_window(fq, F, blockIdx.x, sm.win[0], &sm.bar[0]);
+    int buf = 0;
+    uint32_t parity = 0;  // bit b: the phase buffer b's barrier completes next
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, buf ^= 1) {
+        const uint64_t T0 = tile * kParseTile;
+        const bool win_eof = T0 + kWin >= F;  // the window holds the rest of the input
+        const uint64_t E = tile_excl[tile];   // newlines before the tile
+        const bool arrived = mbar_wait(&sm.bar[buf], (parity >> buf) & 1u, kSpinLimit);
+        parity ^= 1u << buf;
+        if (__syncthreads_or(!arrived)) {  // a copy that never lands: report it, give it one more wait
+            if (tid == 0) {
+                atomicOr(err, kErrSpin);
+                mbar_wait(&sm.bar[buf], (parity >> buf) & 1u ^ 1u, kSpinLimit);
+            }
+            return;
+        }
+        if (tile + gridDim.x < ntiles) stage_window(fq, F, tile + gridDim.x, sm.win[buf ^ 1], &sm.bar[buf ^ 1]);
+        const uint32_t *win = sm.win[buf];
+        // ---- locate.  Thread t holds 16-byte chunks t, t+256, t+512, t+768 of
+        // the tile (rows 0-3) and, for t < 33, chunk t of the halo (row 4).  The
+        // rows' newline counts, packed in 13-bit fields (11 for the halo: the
+        // sums never carry), go through one block scan.
+        uint32_t nlm[5];  // newline bytes of each chunk, one bit per byte
+        uint64_t P = 0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (k < 4 || tid < (int)(kHalo / 16)) v = *reinterpret_cast<const uint4 *>(win + 4 * (k * kRT + tid));
+            nlm[k] = nl_bits(v.x) | (nl_bits(v.y) << 4) | (nl_bits(v.z) << 8) | (nl_bits(v.w) << 12);
+            P |= (uint64_t)__popc(nlm[k]) << (13 * k);
+        }
+        uint64_t x = P;  // inclusive warp scan, then the earlier warps' totals
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sm.scan[warp] = x;
         __syncthreads();
-        const uint32_t tile = s_tile;
-        if (tile >= ntiles) break;
-        const uint64_t r = (uint64_t)tile * kReadTile + tid;
-        const bool live = r < n_rec;
-        const uint64_t a = live ? seq_start[r] : 0, b = live ? seq_end[r] : 0;
-        const uint64_t len64 = b > a ? b - a : 0;
-        const int L = len64 > (uint64_t)kMaxReadLen ? kMaxReadLen + 1 : (int)len64;  // > kMaxReadLen: not hashed
-        const bool hash = L <= kMaxReadLen;
-        uint32_t nm = 0, bm = 0;
-        uint64_t f1 = 0, f2 = 0, g1 = 0, g2 = 0;
-        uint64_t pend = 0;  // 2-bit codes of bases 16 jw .. (the words not yet emitted)
-        int jw = 0;
-        for (uint64_t A = a & ~15ull; A < b; A += 16) {
-            const uint4 v = __ldg(reinterpret_cast<const uint4 *>(fq + A));
-            const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+        uint64_t wi = lane < kRT / 32 ? sm.scan[lane] : 0;  // the warps' totals, scanned across lanes
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint64_t W = A + 4 * q;
-                if (W + 4 <= a || W >= b) continue;
-                const uint32_t x = wv[q];
-                const int t = (int)((int64_t)W - (int64_t)a);  // read position of the word's first byte
-                const uint32_t c = (x >> 1) & 0x03030303u;     // base codes A0 C1 T2 G3
-                if (t >= 0 && (uint64_t)W + 4 <= b) {          // the whole word lies inside the read
-                    check4(x, 0x80808080u, nm, bm);
-                    if (hash) {
-                        const uint32_t e = c + 0x01010101u, ec = (c ^ 0x02020202u) + 0x01010101u;
-                        const uint32_t h1 = __dp4a(e, 0x0105197Du, 0u);                       // 125 25 5 1
-                        const uint32_t h2 = __dp4a(e, 0x01073100u, 0u) + (e & 0xffu) * 343u;  // 343 49 7 1
-                        const uint32_t r1 = __dp4a(ec, 0x7D190501u, 0u);                      // 1 5 25 125
-                        const uint32_t r2 = __dp4a(ec, 0x00310701u, 0u) + (ec >> 24) * 343u;  // 1 7 49 343
-                        f1 += (uint64_t)h1 * s_pow1[L - 4 - t];
-                        f2 += (uint64_t)h2 * s_pow2[L - 4 - t];
-                        g1 += (uint64_t)r1 * s_pow1[t];
-                        g2 += (uint64_t)r2 * s_pow2[t];
+        for (int o = 1; o < kRT / 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        const uint64_t tot = __shfl_sync(0xffffffffu, wi, kRT / 32 - 1);
+        const uint64_t ex = x - P + (warp ? __shfl_sync(0xffffffffu, wi, warp - 1) : 0ull);
+        const uint32_t tile_nl = (uint32_t)((tot & 0x1fffu) + ((tot >> 13) & 0x1fffu) + ((tot >> 26) & 0x1fffu) +
+                                            ((tot >> 39) & 0x1fffu));
+        const uint64_t k0 = (E + 3) >> 2, k1 = (E + tile_nl + 3) >> 2;
+        const uint32_t n_own = (uint32_t)(k1 - k0);
+        // Newline j of the window (j = 0, 1, .. from the tile's start) ends line
+        // E + j; with e3 = E & 3 it is newline (e3 + j) & 3 of record
+        // (E >> 2) + ((e3 + j) >> 2), the tile's record ((e3 + j) >> 2) - adj.
+        const uint32_t e3 = (uint32_t)E & 3u, adj = e3 ? 1u : 0u;
+        for (uint32_t b0 = 0; b0 < n_own; b0 += kRecCap) {  // records in batches of kRecCap (one, but for tiny reads)
+            const uint32_t nb = n_own - b0 < kRecCap ? n_own - b0 : kRecCap;
+            uint32_t rowj = e3;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                uint32_t j = rowj + (uint32_t)((ex >> (13 * k)) & 0x1fffu);  // e3 + the chunk's first newline
+                rowj += (uint32_t)((tot >> (13 * k)) & 0x1fffu);
+                uint32_t m = nlm[k];
+                while (m) {
+                    const uint32_t pos = 16u * (k * kRT + tid) + (__ffs(m) - 1);
+                    m &= m - 1;
+                    const uint32_t slot = (j >> 2) - adj - b0, r4 = j & 3u;
+                    if ((j >> 2) >= adj + b0 && slot < nb) {
+                        if (k < 4 && r4 == 0) sm.start[slot] = (uint16_t)(pos + 1);
+                        else if (r4 == 1) sm.end[slot] = (uint16_t)pos;
                     }
-                } else {  // cut by an end of the read: byte by byte
-                    uint32_t m = 0;
+                    ++j;
+                }
+            }
+            __syncthreads();
+            // ---- records: G lanes each
+            const int G = nb > 128 ? 1 : nb > 64 ? 2 : nb > 32 ? 4 : nb > 16 ? 8 : 16;
+            const uint32_t lg = (uint32_t)tid & (G - 1), grp = (uint32_t)tid / G, ngrp = kRT / G;
+            const uint32_t gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~(G - 1));
+            for (uint32_t r0 = 0; r0 < nb; r0 += ngrp) {
+                const uint32_t r = r0 + grp;
+                const bool own = r < nb;
+                uint32_t a = 0, b = 0;
+                bool in_win = false;
+                if (own) {
+                    a = sm.start[r];
+                    b = sm.end[r];
+                    in_win = b != kNoEnd || win_eof;
+                    if (b == kNoEnd && win_eof) b = (uint32_t)(F - T0);
+                }
+                const uint32_t L = in_win ? b - a : 0u;
+                const bool hashed = own && L >= 1 && L <= (uint32_t)kMaxReadLen;
+                const uint64_t k = k0 + b0 + r;
+                const uint32_t nch = (L + 15) / 16;
+                const uint32_t lim = own ? (nch > (uint32_t)wpr ? nch : (uint32_t)wpr) : 0u;  // words up to wpr
+                uint32_t bad = 0;
+                uint64_t f1 = 0, f2 = 0, g1 = 0, g2 = 0;
+                // warp-uniform trips, so that a warp whose chunks are all whole
+                // takes the unmasked path together
+                const uint32_t trips = __reduce_max_sync(0xffffffffu, (lim + G - 1) / G);
+                for (uint32_t it = 0; it < trips; ++it) {
+                    const uint32_t c = lg + it * G;
+                    const bool has = c < nch;
+                    const int nv = (int)(L - 16 * c);
+                    const bool whole = __all_sync(0xffffffffu, !has || !hashed || nv >= 16);
+                    uint32_t word = 0;
+                    if (has) {
+                        uint32_t xw[4];
+                        win16(win, a + 16 * c, xw);
+                        if (!hashed) {
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int tu = t + u;
-                        if (tu < 0 || (uint64_t)(W + u) >= b) continue;
-                        m |= 0x80u << (8 * u);
-                        if (hash) {
-                            const uint32_t cu = (c >> (8 * u)) & 3u, eu = cu + 1u, ecu = (cu ^ 2u) + 1u;
-                            f1 += (uint64_t)eu * s_pow1[L - 1 - tu];
-                            f2 += (uint64_t)eu * s_pow2[L - 1 - tu];
-                            g1 += (uint64_t)ecu * s_pow1[tu];
-                            g2 += (uint64_t)ecu * s_pow2[tu];
+                            for (int q = 0; q < 4; ++q) bad |= not_acgt(xw[q], lead_bytes(nv - 4 * q));
+                        } else if (whole) {
+                            read_chunk<true>(xw, nv, sm.chunk[c], bad, word, f1, f2, g1, g2);
+                        } else {
+                            read_chunk<false>(xw, nv, sm.chunk[c], bad, word, f1, f2, g1, g2);
                         }
                     }
-                    check4(x, m, nm, bm);
+                    if (c < lim && c < (uint32_t)wpr) seq2[k * (uint64_t)wpr + c] = word;
                 }
-                if (hash) {  // the word's bases into the pending 2-bit words
-                    const uint32_t y = (c | (c >> 6)) & 0x000f000fu;
-                    uint64_t c8 = (y & 0xfu) | ((y >> 12) & 0xf0u);  // bases t .. t+3, 2 bits each
-                    if (t + 4 > L) c8 &= (1u << (2 * (L - t))) - 1u;  // past the read's end
-                    if (t < 0) c8 >>= 2 * -t;
-                    pend |= c8 << (2 * (t < 0 ? 0 : t - 16 * jw));
-                    if (t + 4 >= 16 * (jw + 1)) {  // bases up to 16 (jw + 1) - 1 are in
-                        s_words[jw][tid] = (uint32_t)pend;
-                        pend >>= 32;
-                        ++jw;
+                bad &= 0xdfdfdfdfu;
+                const bool gbad = (__ballot_sync(0xffffffffu, bad != 0) & gmask) != 0;
+                uint32_t nm = 0;
+                if (__any_sync(0xffffffffu, gbad) && gbad) {  // rare: are the odd bytes N-class?
+                    for (uint32_t c = lg; c < nch; c += G) {
+                        uint32_t xw[4];
+                        win16(win, a + 16 * c, xw);
+                        const int nv = (int)(L - 16 * c);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) nm |= n_class(xw[q], lead_bytes(nv - 4 * q));
+                    }
+                }
+                const bool gn = (__ballot_sync(0xffffffffu, nm != 0) & gmask) != 0;
+                for (int o = G >> 1; o; o >>= 1) {
+                    f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+                    f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+                    g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+                    g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+                }
+                if (own && lg == 0) {
+                    sm.end[r] = kNoEnd;  // every lane of the group has read it
+                    bool keep, bd;
+                    uint64_t len;
+                    if (in_win) {
+                        keep = !gn && L > 0;
+                        bd = gbad;
+                        len = L;
+                    } else {  // the line runs past the window: one lane walks it in global memory
+                        const uint64_t p0 = T0 + a;
+                        uint64_t p = p0;
+                        bool hn = false;
+                        bd = false;
+                        for (; p < F; ++p) {
+                            const uint32_t c8 = fq[p];
+                            if (c8 == 0x0au) break;
+                            hn |= n_class(c8, 0xffu) != 0;
+                            bd |= not_acgt(c8, 0xffu) != 0;
+                        }
+                        len = p - p0;
+                        keep = !hn && len > 0;
+                    }
+                    keep_out[k] = keep ? 1u : 0u;
+                    if (keep) {
+                        const uint32_t l32 = len > 0xffffffffull ? 0xffffffffu : (uint32_t)len;
+                        lmin = min(lmin, l32);
+                        lmax = max(lmax, l32);
+                        bad_kept |= bd ? 1u : 0u;
+                        ++kept;
+                        if (hashed) {
+                            const uint32_t h1 = mod1((uint64_t)mod1(f1) * __ldg(tables->pow1 + L - 1));
+                            const uint32_t h2 = mod2((uint64_t)mod2(f2) * __ldg(tables->pow2 + L - 1));
+                            ulonglong2 kv;
+                            kv.x = ((uint64_t)h1 << 32) | h2;
+                            kv.y = ((uint64_t)mod1(g1) << 32) | mod2(g2);
+                            *reinterpret_cast<ulonglong2 *>(keys + 2 * k) = kv;
+                        }
                     }
                 }
             }
+            __syncthreads();  // start / end (and, after the last batch, the window) are reused
         }
-        const bool keep = live && !nm && len64 > 0;
-        if (hash && keep && 16 * jw < L) s_words[jw++][tid] = (uint32_t)pend;  // the last, partial word
-        for (int w = hash ? jw : 0; w < wpr; ++w) s_words[w][tid] = 0;
-        // ---- read indices: this tile's kept records after those of earlier tiles
-        const uint32_t bal = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) s_wcnt[warp] = __popc(bal);
-        __syncthreads();
-        if (tid == 0) {
-            uint32_t run = 0;
-            for (int w = 0; w < kReadTile / 32; ++w) {
-                const uint32_t c = s_wcnt[w];
-                s_wcnt[w] = run;
-                run += c;
-            }
-            s_kept = run;
-            s_base = lookback_exclusive(status, tile, run, err);
-            if (tile == ntiles - 1) *n_kept = s_base + run;
-        }
-        __syncthreads();
-        const uint32_t rank = s_wcnt[warp] + __popc(bal & lanemask_lt_u32());
-        const uint64_t i = s_base + rank;
-        if (keep) {
-            s_who[rank] = (uint16_t)tid;
-            ulonglong2 kv;
-            kv.x = ((uint64_t)mod1(f1) << 32) | mod2(f2);
-            kv.y = ((uint64_t)mod1(g1) << 32) | mod2(g2);
-            if (hash) *reinterpret_cast<ulonglong2 *>(keys + 2 * i) = kv;
-            if (bm) atomicOr(err, kErrBadBase);
-        }
-        // length extremes of the kept reads
-        uint32_t lmin = keep ? (len64 > 0xffffffffull ? 0xffffffffu : (uint32_t)len64) : 0xffffffffu;
-        uint32_t lmax = keep ? lmin : 0u;
+    }
+    // kept count, length extremes of the kept reads, the bad-base flag
 #pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            lmin = min(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
-            lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-        }
-        if (lane == 0 && lmax) {
+    for (int o = 16; o; o >>= 1) {
+        kept += __shfl_xor_sync(0xffffffffu, kept, o);
+        lmin = min(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+        lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    }
+    const bool anybad = __any_sync(0xffffffffu, bad_kept != 0);
+    if (lane == 0) {
+        if (kept) atomicAdd(reinterpret_cast<unsigned long long *>(n_kept), (unsigned long long)kept);
+        if (lmax) {
             atomicMin(len_minmax, lmin);
             atomicMax(len_minmax + 1, lmax);
         }
-        __syncthreads();
-        // read-major words of the kept reads: one contiguous run of kept x wpr
-        const uint32_t kept = s_kept;
-        const uint64_t o0 = s_base * (uint64_t)wpr;
-        for (uint32_t q = tid; q < kept * (uint32_t)wpr; q += kReadTile) {
-            const uint32_t rk = q / (uint32_t)wpr, w = q - rk * (uint32_t)wpr;
-            seq2[o0 + q] = s_words[w][s_who[rk]];
-        }
-        __syncthreads();
+        if (anybad) atomicOr(err, kErrBadBase);
+    }
+}
+
+// Kept records to consecutive indices: pos = exclusive scan of keep (a
+// record is kept iff pos[k+1] > pos[k], the last one iff its pos < n_kept).
+__global__ void __launch_bounds__(256) compact_reads_kernel(const uint32_t *__restrict__ pos, uint64_t n_rec,
+                                                            uint64_t n_kept, const uint64_t *__restrict__ keys,
+                                                            const uint32_t *__restrict__ seq2, int wpr,
+                                                            uint64_t *__restrict__ keys_out,
+                                                            uint32_t *__restrict__ seq2_out) {
+    for (uint64_t k = (uint64_t)blockIdx.x * 256 + threadIdx.x; k < n_rec; k += (uint64_t)gridDim.x * 256) {
+        const uint32_t i = pos[k];
+        const uint64_t nxt = k + 1 < n_rec ? pos[k + 1] : n_kept;
+        if (nxt == i) continue;
+        keys_out[2ull * i] = keys[2 * k];
+        keys_out[2ull * i + 1] = keys[2 * k + 1];
+        for (int w = 0; w < wpr; ++w) seq2_out[(uint64_t)i * wpr + w] = seq2[k * wpr + w];
     }
 }
 
@@ -351,32 +509,42 @@ void launch_nl_count(const uint8_t *fq, uint64_t F, uint32_t *tile_counts, uint6
     nl_count_kernel<<<(unsigned)parse_tiles(F), 256, 0, s>>>(fq, F, tile_counts, len0);
 }
 
-void launch_nl_locate(const uint8_t *fq, uint64_t F, const uint64_t *tile_excl, uint64_t *seq_start,
-                      uint64_t *seq_end, cudaStream_t s) {
+void launch_read_pass(const uint8_t *fq, uint64_t F, const uint64_t *tile_excl, const HashTables *tables,
+                      uint64_t *keys, uint32_t *seq2, int wpr, uint32_t *keep, uint64_t *n_kept, uint32_t *len_minmax,
+                      uint32_t *err, cudaStream_t s) {
     if (!F) return;
-    count_launch();
-    nl_locate_kernel<<<(unsigned)parse_tiles(F), 256, 0, s>>>(fq, F, tile_excl, seq_start, seq_end);
-}
-
-void launch_read_hash(const uint8_t *fq, const uint64_t *seq_start, const uint64_t *seq_end, uint64_t n_rec,
-                      const HashTables *tables, uint64_t *keys, uint32_t *seq2, int wpr, uint64_t *status,
-                      uint32_t *tile_ctr, uint64_t *n_kept, uint32_t *len_minmax, uint32_t *err, cudaStream_t s) {
-    if (!n_rec) return;
-    static int grid = 0;  // persistent: SMs x resident CTAs (the same on every B200)
-    if (!grid) {
-        int dev = 0, sms = 148, occ = 1;
-        cudaGetDevice(&dev);
+    // persistent grid (SMs x resident CTAs) and the shared-memory attribute, once per device
+    constexpr int kDevs = 64;
+    static std::atomic<int> grid[kDevs] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) {
+        cudaGetLastError();
+        dev = 0;
+    }
+    int g = grid[dev].load(std::memory_order_acquire);
+    if (!g) {
+        int sms = 148, occ = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, read_hash_kernel, kReadTile, 0) != cudaSuccess ||
+        cudaFuncSetAttribute(read_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ReadSmem));
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, read_pass_kernel, kRT, sizeof(ReadSmem)) !=
+                cudaSuccess ||
             occ < 1)
             occ = 1;
         cudaGetLastError();
-        grid = sms * occ;
+        g = sms * occ;
+        grid[dev].store(g, std::memory_order_release);
     }
-    const uint64_t tiles = (n_rec + kReadTile - 1) / kReadTile;
     count_launch();
-    read_hash_kernel<<<grid_for(tiles, 1, (unsigned)grid), kReadTile, 0, s>>>(
-        fq, seq_start, seq_end, n_rec, tables, keys, seq2, wpr, status, tile_ctr, n_kept, len_minmax, err);
+    read_pass_kernel<<<grid_for(parse_tiles(F), 1, (unsigned)g), kRT, sizeof(ReadSmem), s>>>(
+        fq, F, tile_excl, tables, keys, seq2, wpr, keep, n_kept, len_minmax, err);
+}
+
+void launch_compact_reads(const uint32_t *pos, uint64_t n_rec, uint64_t n_kept, const uint64_t *keys,
+                          const uint32_t *seq2, int wpr, uint64_t *keys_out, uint32_t *seq2_out, cudaStream_t s) {
+    if (!n_rec) return;
+    count_launch();
+    compact_reads_kernel<<<grid_for(n_rec, 256, 148 * 16), 256, 0, s>>>(pos, n_rec, n_kept, keys, seq2, wpr, keys_out,
+                                                                      seq2_out);
 }
 
 void launch_columns(const uint32_t *seq2, uint64_t n, int L, int wpr, uint32_t *cols, uint64_t wpc, cudaStream_t s) {

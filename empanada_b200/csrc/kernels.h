@@ -30,18 +30,20 @@ __host__ __device__ inline uint64_t parse_tiles(uint64_t F) { return (F + kParse
 // tile_counts[t] = newlines in FASTQ tile t; *len0 = length of the first
 // record's sequence line when tile 0 holds its two newlines, else 0
 void launch_nl_count(const uint8_t *fq, uint64_t F, uint32_t *tile_counts, uint64_t *len0, cudaStream_t s);
-void launch_nl_locate(const uint8_t *fq, uint64_t F, const uint64_t *tile_excl, uint64_t *seq_start,
-                      uint64_t *seq_end, cudaStream_t s);
-// Records [0, n_rec) -> kept reads (no N-class byte, non-empty): keys[2i] /
-// keys[2i+1] = fingerprint of kept read i / of its reverse complement,
-// seq2[i * wpr + w] = its bases 16w .. 16w+15 (2 bits each), *n_kept, the
-// kept reads' length extremes in len_minmax, kErrBadBase in *err.  status:
-// (n_rec / 256 + 1) zeroed look-back words, *tile_ctr zeroed.  Reads longer
-// than kMaxReadLen are classified but not hashed.
-void launch_read_hash(const uint8_t *fq, const uint64_t *seq_start, const uint64_t *seq_end, uint64_t n_rec,
-                      const HashTables *tables, uint64_t *keys, uint32_t *seq2, int wpr, uint64_t *status,
-                      uint32_t *tile_ctr, uint64_t *n_kept, uint32_t *len_minmax, uint32_t *err, cudaStream_t s);
-constexpr uint64_t kReadTileRecs = 256;
+// Records k of the FASTQ (tile_excl: newlines before each parse tile):
+// keep[k] = 1 iff the record's sequence line holds no N-class byte and is not
+// empty; keys[2k] / keys[2k+1] = fingerprint of its read / of the reverse
+// complement, seq2[k * wpr + w] = its bases 16w .. 16w+15 (2 bits each, zero
+// past the read); *n_kept += the kept count (start it at 0), the kept reads'
+// length extremes in len_minmax, kErrBadBase in *err.  Reads longer than
+// kMaxReadLen are classified but not hashed.
+void launch_read_pass(const uint8_t *fq, uint64_t F, const uint64_t *tile_excl, const HashTables *tables,
+                      uint64_t *keys, uint32_t *seq2, int wpr, uint32_t *keep, uint64_t *n_kept, uint32_t *len_minmax,
+                      uint32_t *err, cudaStream_t s);
+// The kept records' keys and words to indices 0 .. n_kept-1 in file order;
+// pos = exclusive scan of keep.
+void launch_compact_reads(const uint32_t *pos, uint64_t n_rec, uint64_t n_kept, const uint64_t *keys,
+                          const uint32_t *seq2, int wpr, uint64_t *keys_out, uint32_t *seq2_out, cudaStream_t s);
 // cols[c * wpc + i/16] holds base c of read i at bits 2*(i%16)
 void launch_columns(const uint32_t *seq2, uint64_t n, int L, int wpr, uint32_t *cols, uint64_t wpc, cudaStream_t s);
 
