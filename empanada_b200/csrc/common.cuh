@@ -40,16 +40,19 @@ enum ErrBits : uint32_t {
 
 // Powers R^i mod P for i <= kMaxReadLen and the radix inverses (fingerprint.cu:26-34,
 // overlap.cu:121-122).  Lives in device memory; staged into shared memory by
-// the kernels that need it.  chunk[c] holds the weights of read positions
-// 16c .. 16c+15 for the read pass (Rinv = R^-1 mod P):
-//   Rinv1^(16c+7), Rinv1^(16c+15), Rinv2^(16c+7), Rinv2^(16c+15),
-//   R1^(16c), R1^(16c+8), R2^(16c), R2^(16c+8)
+// the kernels that need it.
 struct HashTables {
     uint32_t pow1[kMaxReadLen + 1];
     uint32_t pow2[kMaxReadLen + 1];
     uint32_t inv1;
     uint32_t inv2;
-    uint32_t chunk[kMaxReadLen / 16][8];
+};
+// Weights of read positions 16c .. 16c+15 for the read pass (Rinv = R^-1 mod
+// P), w[c] = Rinv1^(16c+7), Rinv1^(16c+15), Rinv2^(16c+7), Rinv2^(16c+15),
+// R1^(16c), R1^(16c+8), R2^(16c), R2^(16c+8).  In device memory right after
+// the HashTables.
+struct ChunkWeights {
+    uint32_t w[kMaxReadLen / 16][8];
 };
 
 // x mod (2^29 - C) for any 64-bit x: two pseudo-Mersenne folds then one

@@ -141,7 +141,7 @@ struct emp_ctx {
     // device memory of the jobs' work buffers: a stream-ordered pool that keeps
     // what is freed, so that a job's buffers come and go without cudaMalloc
     cudaMemPool_t pool = nullptr;
-    DevBuf tables;  // HashTables
+    DevBuf tables;  // HashTables, then ChunkWeights
     // emp_sort_pairs working set, kept for the next call
     DevBuf sort_k1, sort_v1, sort_scr, sort_err;
     uint64_t sort_cap = 0;
@@ -280,7 +280,7 @@ uint32_t host_modpow(uint64_t a, uint32_t e, uint32_t p) {
     return (uint32_t)r;
 }
 
-void host_tables(HashTables &t) {
+void host_tables(HashTables &t, ChunkWeights &cw) {
     t.pow1[0] = t.pow2[0] = 1;
     for (int i = 1; i <= kMaxReadLen; ++i) {
         t.pow1[i] = (uint32_t)(((uint64_t)t.pow1[i - 1] * kR1) % kP1);
@@ -290,14 +290,14 @@ void host_tables(HashTables &t) {
     t.inv2 = host_modpow(kR2, kP2 - 2, kP2);
     for (int c = 0; c < kMaxReadLen / 16; ++c) {
         const uint64_t t0 = 16ull * c;
-        t.chunk[c][0] = host_modpow(t.inv1, (uint32_t)(t0 + 7), kP1);
-        t.chunk[c][1] = host_modpow(t.inv1, (uint32_t)(t0 + 15), kP1);
-        t.chunk[c][2] = host_modpow(t.inv2, (uint32_t)(t0 + 7), kP2);
-        t.chunk[c][3] = host_modpow(t.inv2, (uint32_t)(t0 + 15), kP2);
-        t.chunk[c][4] = t.pow1[t0];
-        t.chunk[c][5] = t.pow1[t0 + 8];
-        t.chunk[c][6] = t.pow2[t0];
-        t.chunk[c][7] = t.pow2[t0 + 8];
+        cw.w[c][0] = host_modpow(t.inv1, (uint32_t)(t0 + 7), kP1);
+        cw.w[c][1] = host_modpow(t.inv1, (uint32_t)(t0 + 15), kP1);
+        cw.w[c][2] = host_modpow(t.inv2, (uint32_t)(t0 + 7), kP2);
+        cw.w[c][3] = host_modpow(t.inv2, (uint32_t)(t0 + 15), kP2);
+        cw.w[c][4] = t.pow1[t0];
+        cw.w[c][5] = t.pow1[t0 + 8];
+        cw.w[c][6] = t.pow2[t0];
+        cw.w[c][7] = t.pow2[t0 + 8];
     }
 }
 
@@ -772,10 +772,12 @@ emp_status run_rounds_bucket(emp_job *j, cudaStream_t s, const RoundEnv &env, in
         EMP_CUDA(cudaMemsetAsync(j->coop_probe.p, 0, j->coop_probe.bytes, s));
         hc->probe = j->coop_probe.as<uint64_t>();
     }
+    hj->pre_done = bucket_prologue_apart(*hj) ? 1u : 0u;
     EMP_CUDA(cudaMemcpyAsync(j->bk_job.p, hj, sizeof(BktJob), cudaMemcpyHostToDevice, s));
     EMP_CUDA(cudaMemcpyAsync(j->coop_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
     cudaEvent_t e0 = j->upd_ev[0], e1 = j->upd_ev[1];
     EMP_CUDA(cudaEventRecord(e0, s));
+    if (hj->pre_done) EMP_CUDA(launch_bucket_prologue(j->bk_job.as<BktJob>(), s));
     EMP_CUDA(launch_bucket_rounds(j->bk_job.as<BktJob>(), j->coop_ctl.as<CoopCtl>(), err_word(j), s));
     EMP_CUDA(cudaEventRecord(e1, s));
     EMP_CUDA(cudaMemcpyAsync(hj, j->bk_job.p, sizeof(BktJob), cudaMemcpyDeviceToHost, s));
@@ -927,6 +929,7 @@ emp_status launch_reads(emp_job *j, cudaStream_t s, int wpr) {
     std::memcpy(hm + kMiscLen, mm, 16);
     EMP_CUDA(cudaMemcpyAsync(dm + kMiscLen, hm + kMiscLen, 16, cudaMemcpyHostToDevice, s));
     launch_read_pass(j->fq.as<uint8_t>(), j->F, j->tile_excl.as<uint64_t>(), j->ctx->tables.as<HashTables>(),
+                     reinterpret_cast<const ChunkWeights *>(j->ctx->tables.as<uint8_t>() + sizeof(HashTables)),
                      j->keys0.as<uint64_t>(), j->seq2.as<uint32_t>(), wpr, j->keep.as<uint32_t>(), dm + kMiscN,
                      reinterpret_cast<uint32_t *>(dm + kMiscLen), err_word(j), s);
     cudaEventRecord(j->map_ev[1], s);
@@ -1631,17 +1634,21 @@ emp_status emp_ctx_create(int device, uint64_t hbm_budget_bytes, emp_ctx **out) 
         return EMP_E_CUDA;
     }
     void *p = nullptr;
-    if (cudaMalloc(&p, sizeof(HashTables)) != cudaSuccess) {
+    struct {  // HashTables, then the read pass's ChunkWeights
+        HashTables h;
+        ChunkWeights w;
+    } tabs;
+    static_assert(sizeof(HashTables) % 16 == 0, "the weights start 16-byte aligned");
+    if (cudaMalloc(&p, sizeof tabs) != cudaSuccess) {
         cudaStreamDestroy(c->stream);
         cudaMemPoolDestroy(c->pool);
         delete c;
         return EMP_E_NOMEM;
     }
     c->tables.p = p;
-    c->tables.bytes = sizeof(HashTables);
-    HashTables h;
-    host_tables(h);
-    if (cudaMemcpy(p, &h, sizeof h, cudaMemcpyHostToDevice) != cudaSuccess) {
+    c->tables.bytes = sizeof tabs;
+    host_tables(tabs.h, tabs.w);
+    if (cudaMemcpy(p, &tabs, sizeof tabs, cudaMemcpyHostToDevice) != cudaSuccess) {
         cudaStreamDestroy(c->stream);
         cudaMemPoolDestroy(c->pool);
         delete c;

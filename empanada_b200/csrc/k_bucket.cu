@@ -286,6 +286,21 @@ EMP_DEV void put_direct(const ListOut &o, bool act, uint32_t bin, const uint4 &e
     put_list(o, bin, pos + __popc(peers & lanemask_lt_u32()), e);
 }
 
+// put_direct in two halves, so that several reservations can be in flight:
+// reserve_direct returns the leader's run start (in the leader's lane) and
+// the lanes sharing the bin; position_direct gives each lane its position.
+// Equal keys are common (overlapping reads), so runs of one bin in a warp
+// take one atomic.
+EMP_DEV uint32_t reserve_direct(const ListOut &o, bool act, uint32_t bin, uint32_t &peers) {
+    const uint32_t m = __ballot_sync(0xffffffffu, act);
+    peers = act ? __match_any_sync(m, bin) : 0u;
+    if (act && (threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1)) return atomicAdd(o.cnt + bin, (uint32_t)__popc(peers));
+    return 0u;
+}
+EMP_DEV uint32_t position_direct(uint32_t peers, uint32_t run) {
+    return __shfl_sync(peers, run, __ffs(peers) - 1) + __popc(peers & lanemask_lt_u32());
+}
+
 // Add this CTA's kept entries and suffixes to a round's counts (sh.kept and
 // sh.sfx zeroed, then a __syncthreads, before the per-thread counts came in).
 EMP_DEV void add_counts(BktRound &nx, uint32_t kept, uint32_t sfx, BShared &sh) {
@@ -365,6 +380,7 @@ EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
     }
     __syncthreads();
     const uint64_t base = (uint64_t)k * kBktTile;
+    sprobe(sh, 23);
     uint64_t key[kC];
     uint32_t val[kC], word[kC], rank[kC], bin[kC];
     bool keep[kC];
@@ -375,15 +391,17 @@ EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
         key[c] = keep[c] ? __ldcg(J.lk_in + e) : 0;
         val[c] = keep[c] ? __ldcg(J.lv_in + e) : 0;
     }
+    const bool some_used = J.r0 > 0;  // host-synchronised rounds ran before the launch
 #pragma unroll
     for (int c = 0; c < kC; ++c) {  // used before the launch; the base words
         word[c] = 0;
         if (!keep[c]) continue;
         const uint32_t rid = val[c] & 0x7fffffffu;
-        keep[c] = ((val[c] >> 31) ? J.used_p[rid] : J.used_s[rid]) == 0;
+        if (some_used) keep[c] = ((val[c] >> 31) ? J.used_p[rid] : J.used_s[rid]) == 0;
         if (keep[c]) word[c] = refill_word(a, val[c]);
     }
     if (direct) {  // hash step, bin, position straight from the bin counter
+        sprobe(sh, 24);
         uint32_t kept = 0, sfx = 0;
 #pragma unroll
         for (int c = 0; c < kC; ++c) {
@@ -396,7 +414,9 @@ EMP_COLD void prologue_tile(BktJob &J, uint32_t k, BShared &sh, uint8_t *smem) {
             }
             put_direct(lo, keep[c], bn, make_uint4((uint32_t)key[c], (uint32_t)(key[c] >> 32), val[c], word[c]));
         }
+        sprobe(sh, 25);
         add_counts(I, kept, sfx, sh);
+        sprobe(sh, 26);
         return;
     }
     uint32_t sfx = 0;
@@ -1122,6 +1142,78 @@ EMP_COLD void write_next_direct(const Stage &v, uint32_t total, const StepArgs a
     add_counts(nx, kept, sfx, sh);
 }
 
+// The same for a bucket staged in shared memory, in passes so that the
+// global atomics are not a chain: (1) the hash step of every kept entry in
+// place and its next bin, (2) kU positions per thread reserved back to back,
+// then the stores.
+EMP_COLD void write_next_direct_smem(uint32_t total, const StepArgs a, uint32_t nb, const ListOut lo, BktRound &nx,
+                                     BShared &sh, uint8_t *smem) {
+    uint64_t *key = reinterpret_cast<uint64_t *>(smem + kOffKey);
+    const uint32_t *val = reinterpret_cast<const uint32_t *>(smem + kOffVal);
+    uint32_t *word = reinterpret_cast<uint32_t *>(smem + kOffWord);
+    const uint8_t *flag = smem + kOffFlag;
+    uint32_t *bin = reinterpret_cast<uint32_t *>(smem + kOffReg);  // next bin, or ~0: used
+    if (threadIdx.x == 0) {
+        sh.sfx = 0;
+        sh.kept = 0;
+    }
+    __syncthreads();  // the region's previous users are done
+    uint32_t kept = 0, sfx = 0;
+    constexpr int kA = 4;
+    for (uint32_t x0 = 0; x0 < total; x0 += kA * kT) {
+        uint32_t vl[kA], wd[kA];
+        bool act[kA];
+#pragma unroll
+        for (int u = 0; u < kA; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            act[u] = x < total && !(flag[x] & kUsed);
+            vl[u] = act[u] ? val[x] : 0u;
+            wd[u] = act[u] ? word[x] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kA; ++u)
+            if (act[u] && needs_refill(a, vl[u])) wd[u] = refill_word(a, vl[u]);
+#pragma unroll
+        for (int u = 0; u < kA; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            if (x >= total) continue;
+            uint32_t bn = ~0u;
+            if (act[u]) {
+                const uint64_t ky = step_key(a, key[x], vl[u], wd[u]);
+                bn = 2 * bkt_of(sort_key(ky, vl[u]), nb) + (vl[u] >> 31);
+                key[x] = ky;
+                word[x] = wd[u];
+                ++kept;
+                sfx += (vl[u] >> 31) == 0;
+            }
+            bin[x] = bn;
+        }
+    }
+    __syncthreads();
+    constexpr int kU = 8;
+    for (uint32_t x0 = 0; x0 < total; x0 += kU * kT) {
+        uint32_t bn[kU], pos[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            bn[u] = x < total ? bin[x] : ~0u;
+        }
+        uint32_t peers[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u)  // reservations, independent of one another
+            pos[u] = reserve_direct(lo, bn[u] != ~0u, bn[u], peers[u]);
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if (bn[u] == ~0u) continue;
+            const uint32_t x = x0 + u * kT + threadIdx.x;
+            const uint64_t ky = key[x];
+            put_list(lo, bn[u], position_direct(peers[u], pos[u]),
+                     make_uint4((uint32_t)ky, (uint32_t)(ky >> 32), val[x], word[x]));
+        }
+    }
+    add_counts(nx, kept, sfx, sh);
+}
+
 // Drop the used entries of the staged bucket, apply round a.r's hash step to
 // the rest and write them into the next list's bins (nb buckets).  Counts go
 // to the next round's BktRound.
@@ -1456,7 +1548,9 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
         const uint32_t nb_next = z.nb_next;
         const StepArgs a = step_args(J, sh.tab, z.r + 1, false);
         const ListOut lo = list_out(J, iter + 1);
-        if (nb_next > kBktMaxBuckets) {
+        if (nb_next > kBktMaxBuckets && in_smem) {
+            write_next_direct_smem(total, a, nb_next, lo, N, sh, smem);
+        } else if (nb_next > kBktMaxBuckets) {
             write_next_direct(v, total, a, nb_next, lo, N, sh);
         } else if (in_smem) {
             write_next_smem(total, a, nb_next, lo, N, sh, smem);
@@ -1598,11 +1692,16 @@ __global__ void __launch_bounds__(kT, 2) bucket_rounds_kernel(BktJob *jobs, Coop
     const int J = (int)ctl->njobs;
     for (uint32_t i = threadIdx.x; i < sizeof(HashTables) / 4; i += kT)
         reinterpret_cast<uint32_t *>(&sh.tab)[i] = reinterpret_cast<const uint32_t *>(jobs[0].tables)[i];
-    if (threadIdx.x == 0) sh.gen = 0;
+    if (threadIdx.x == 0) {
+        sh.gen = 0;
+        sh.pctl = ctl;
+        sh.piter = 0;
+    }
     __syncthreads();
+    probe(ctl, 0, 20);  // the launch's phases, stamped with iteration 0's points
     // ---- prologue: the input lists of the jobs this launch starts -> their round r0 lists
     uint32_t total = build_prefix(sh, J, [&](int j) -> uint32_t {
-        return jobs[j].iter0 == 0 ? (uint32_t)bkt_tiles(jobs[j].n_in) : 0u;
+        return jobs[j].iter0 == 0 && !jobs[j].pre_done ? (uint32_t)bkt_tiles(jobs[j].n_in) : 0u;
     });
     tile_loop(sh, &ctl->ticket[0], J, total, [&](int j, uint32_t k) { prologue_tile(jobs[j], k, sh, smem); });
     if (!grid_barrier(ctl, &sh.flag, &sh.gen, 0, 7)) return;
@@ -1637,10 +1736,100 @@ __global__ void __launch_bounds__(kT, 2) bucket_rounds_kernel(BktJob *jobs, Coop
         probe(ctl, it, 10);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = it;
+    probe(ctl, 0, 21);
     place_edges(jobs, J, it, sh, smem);
+    probe(ctl, 0, 22);
+}
+
+// The prologue of a job whose first list is binned directly, as its own
+// launch: no shared memory and a few entries per thread, so that many more
+// warps per SM than the round kernel's hide the latency of the list loads,
+// the base-word loads and the bin counters.  Same entries, same bins.
+constexpr int kPreT = 256, kPreU = 4;
+__global__ void __launch_bounds__(kPreT) bucket_prologue_kernel(const BktJob *job) {
+    const BktJob &J = *job;
+    const uint64_t n_in = J.n_in;
+    const uint32_t nb = bkt_count(n_in, J.wave, J.mean);
+    const StepArgs a = step_args(J, *J.tables, J.r0, true);
+    const ListOut lo = list_out(J, 0);
+    const uint64_t *lk = J.lk_in;
+    const uint32_t *lv = J.lv_in;
+    const uint8_t *used_s = J.used_s, *used_p = J.used_p;
+    const bool some_used = J.r0 > 0;  // host-synchronised rounds ran before the launch
+    uint32_t kept = 0, sfx = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * kPreT * kPreU;
+    for (uint64_t e0 = (uint64_t)blockIdx.x * kPreT * kPreU; e0 < n_in; e0 += stride) {  // uniform per block
+        uint64_t key[kPreU];
+        uint32_t val[kPreU], word[kPreU];
+        bool keep[kPreU];
+#pragma unroll
+        for (int u = 0; u < kPreU; ++u) {
+            const uint64_t e = e0 + u * kPreT + threadIdx.x;
+            keep[u] = e < n_in;
+            key[u] = keep[u] ? __ldcs(lk + e) : 0;
+            val[u] = keep[u] ? __ldcs(lv + e) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kPreU; ++u) {
+            word[u] = 0;
+            if (!keep[u]) continue;
+            const uint32_t rid = val[u] & 0x7fffffffu;
+            if (some_used) keep[u] = ((val[u] >> 31) ? used_p[rid] : used_s[rid]) == 0;
+            if (keep[u]) word[u] = refill_word(a, val[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kPreU; ++u) {
+            uint32_t bn = 0;
+            if (keep[u]) {
+                key[u] = step_key(a, key[u], val[u], word[u]);
+                bn = 2 * bkt_of(sort_key(key[u], val[u]), nb) + (val[u] >> 31);
+                ++kept;
+                sfx += (val[u] >> 31) == 0;
+            }
+            put_direct(lo, keep[u], bn, make_uint4((uint32_t)key[u], (uint32_t)(key[u] >> 32), val[u], word[u]));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        kept += __shfl_xor_sync(0xffffffffu, kept, o);
+        sfx += __shfl_xor_sync(0xffffffffu, sfx, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        BktRound &I = job->meta[J.r0];
+        if (kept) atomicAdd(reinterpret_cast<unsigned long long *>(&I.n), (unsigned long long)kept);
+        if (sfx) atomicAdd(reinterpret_cast<unsigned long long *>(&I.s), (unsigned long long)sfx);
+    }
 }
 
 }  // namespace
+
+bool bucket_prologue_apart(const BktJob &hj) {
+    return hj.iter0 == 0 && hj.n_in > 0 && bkt_count(hj.n_in, hj.wave, hj.mean) > kBktMaxBuckets;
+}
+
+cudaError_t launch_bucket_prologue(BktJob *job, cudaStream_t s) {
+    constexpr int kDevs = 64;
+    static std::atomic<int> grid[kDevs] = {};  // SMs x resident CTAs, per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) {
+        cudaGetLastError();
+        dev = 0;
+    }
+    int g = grid[dev].load(std::memory_order_acquire);
+    if (!g) {
+        int sms = 148, occ = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bucket_prologue_kernel, kPreT, 0) != cudaSuccess ||
+            occ < 1)
+            occ = 1;
+        cudaGetLastError();
+        g = sms * occ;
+        grid[dev].store(g, std::memory_order_release);
+    }
+    count_launch();
+    bucket_prologue_kernel<<<g, kPreT, 0, s>>>(job);
+    return cudaGetLastError();
+}
 
 size_t bkt_scratch_bytes(uint64_t n_max) { return scratch_layout(nullptr, n_max < 1 ? 1 : n_max, nullptr); }
 

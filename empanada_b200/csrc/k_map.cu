@@ -138,7 +138,7 @@ static_assert(kMaxReadLen % 16 == 0, "whole read-major words");
 
 struct __align__(16) ReadSmem {
     uint32_t win[2][kWinWords + 8];  // two windows (zero past the input), each then zero padding
-    uint32_t chunk[kChunks][8];      // HashTables::chunk
+    uint32_t chunk[kChunks][8];      // ChunkWeights::w
     uint16_t start[kRecCap];         // sequence line [start, end) of the batch's records (window offsets)
     uint16_t end[kRecCap];           // kNoEnd: no newline ends it inside the window
     uint64_t scan[kRT / 32];
@@ -237,13 +237,14 @@ EMP_DEV void stage_window(const uint8_t *fq, uint64_t F, uint64_t tile, uint32_t
 __global__ void __launch_bounds__(kRT, 4) read_pass_kernel(const uint8_t *__restrict__ fq, uint64_t F,
                                                         const uint64_t *__restrict__ tile_excl,
                                                         const HashTables *__restrict__ tables,
+                                                        const ChunkWeights *__restrict__ weights,
                                                         uint64_t *__restrict__ keys, uint32_t *__restrict__ seq2,
                                                         int wpr, uint32_t *__restrict__ keep_out, uint64_t *n_kept,
                                                         uint32_t *len_minmax, uint32_t *err) {
     extern __shared__ __align__(16) uint8_t read_smem[];
     ReadSmem &sm = *reinterpret_cast<ReadSmem *>(read_smem);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < kChunks * 8; i += kRT) sm.chunk[i >> 3][i & 7] = tables->chunk[i >> 3][i & 7];
+    for (int i = tid; i < kChunks * 8; i += kRT) sm.chunk[i >> 3][i & 7] = weights->w[i >> 3][i & 7];
     for (int i = tid; i < (int)kRecCap; i += kRT) sm.end[i] = kNoEnd;  // each use resets its slots
     if (tid < 16) sm.win[tid >> 3][kWinWords + (tid & 7)] = 0;
     if (tid == 0) {
@@ -510,7 +511,7 @@ void launch_nl_count(const uint8_t *fq, uint64_t F, uint32_t *tile_counts, uint6
 }
 
 void launch_read_pass(const uint8_t *fq, uint64_t F, const uint64_t *tile_excl, const HashTables *tables,
-                      uint64_t *keys, uint32_t *seq2, int wpr, uint32_t *keep, uint64_t *n_kept, uint32_t *len_minmax,
+                      const ChunkWeights *weights, uint64_t *keys, uint32_t *seq2, int wpr, uint32_t *keep, uint64_t *n_kept, uint32_t *len_minmax,
                       uint32_t *err, cudaStream_t s) {
     if (!F) return;
     // persistent grid (SMs x resident CTAs) and the shared-memory attribute, once per device
@@ -536,7 +537,7 @@ void launch_read_pass(const uint8_t *fq, uint64_t F, const uint64_t *tile_excl, 
     }
     count_launch();
     read_pass_kernel<<<grid_for(parse_tiles(F), 1, (unsigned)g), kRT, sizeof(ReadSmem), s>>>(
-        fq, F, tile_excl, tables, keys, seq2, wpr, keep, n_kept, len_minmax, err);
+        fq, F, tile_excl, tables, weights, keys, seq2, wpr, keep, n_kept, len_minmax, err);
 }
 
 void launch_compact_reads(const uint32_t *pos, uint64_t n_rec, uint64_t n_kept, const uint64_t *keys,

@@ -38,8 +38,8 @@ void launch_nl_count(const uint8_t *fq, uint64_t F, uint32_t *tile_counts, uint6
 // length extremes in len_minmax, kErrBadBase in *err.  Reads longer than
 // kMaxReadLen are classified but not hashed.
 void launch_read_pass(const uint8_t *fq, uint64_t F, const uint64_t *tile_excl, const HashTables *tables,
-                      uint64_t *keys, uint32_t *seq2, int wpr, uint32_t *keep, uint64_t *n_kept, uint32_t *len_minmax,
-                      uint32_t *err, cudaStream_t s);
+                      const ChunkWeights *weights, uint64_t *keys, uint32_t *seq2, int wpr, uint32_t *keep,
+                      uint64_t *n_kept, uint32_t *len_minmax, uint32_t *err, cudaStream_t s);
 // The kept records' keys and words to indices 0 .. n_kept-1 in file order;
 // pos = exclusive scan of keep.
 void launch_compact_reads(const uint32_t *pos, uint64_t n_rec, uint64_t n_kept, const uint64_t *keys,
@@ -291,6 +291,7 @@ struct BktJob {
     uint32_t mean;           // entries per bucket aimed at (bkt_count)
     uint32_t overflow;       // the edge buffer was too small
     uint32_t iter0;          // iterations run by earlier launches (0: the launch starts the job)
+    uint32_t pre_done;       // the prologue ran in its own launch (launch_bucket_prologue)
     uint32_t done;           // set at the end of a launch after which the job has no round left
     uint64_t e_total;        // edges of the finished rounds of this launch
     uint64_t e_stage;        // staging buffer fill
@@ -300,6 +301,11 @@ size_t bkt_scratch_bytes(uint64_t n_max);
 constexpr uint32_t kBktRegionCap = 2048;  // entries per (bucket, table) region: 15 sigma above the mean of 1450
 int bucket_grid_size();                             // 0: no cooperative launch on this device
 cudaError_t launch_bucket_rounds(BktJob *jobs, CoopCtl *ctl, uint32_t *err, cudaStream_t s);
+// Whether a job the round kernel starts (iter0 = 0) bins its first list
+// directly (more than kBktMaxBuckets buckets); such a job's prologue runs
+// faster as its own launch before the round kernel, with pre_done set.
+bool bucket_prologue_apart(const BktJob &host_job);
+cudaError_t launch_bucket_prologue(BktJob *job, cudaStream_t s);
 
 void launch_join_count(const uint64_t *skeys, const uint32_t *svals, uint64_t n, uint32_t *cnt, cudaStream_t s);
 void launch_join_write(const uint64_t *skeys, const uint32_t *svals, uint64_t n, const uint32_t *cnt,
