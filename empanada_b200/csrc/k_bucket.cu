@@ -1190,6 +1190,7 @@ EMP_COLD void write_next_direct_smem(uint32_t total, const StepArgs a, uint32_t 
         }
     }
     __syncthreads();
+    sprobe(sh, 13);
     constexpr int kU = 8;
     for (uint32_t x0 = 0; x0 < total; x0 += kU * kT) {
         uint32_t bn[kU], pos[kU];
@@ -1211,6 +1212,7 @@ EMP_COLD void write_next_direct_smem(uint32_t total, const StepArgs a, uint32_t 
                      make_uint4((uint32_t)ky, (uint32_t)(ky >> 32), val[x], word[x]));
         }
     }
+    sprobe(sh, 15);
     add_counts(nx, kept, sfx, sh);
 }
 
