@@ -22,7 +22,8 @@ each rank runs its own job, no data-path collective):
             output.bin to host; e2e.serial_value: feed, run and copy out one
             after another
   roofline  the dominant kernel (the cooperative kernel that runs every
-            overlap round in one launch): its algorithmic bytes per launch
+            overlap round in one launch, timed with the prologue launch that
+            bins a large job's first list): its algorithmic bytes per launch
             (per round 16 B gathered per entry, 16 B written per entry kept
             for the next round, 8 B per edge) / its event-timed duration,
             against the measured HBM copy bandwidth
@@ -780,8 +781,8 @@ def main():
                     "72 B per candidate, 8 B per edge")
         else:
             kname = "bucket_rounds_kernel"
-            what = ("all rounds in one launch: per round 16 B gathered per entry, 16 B written per entry kept "
-                    "for the next round, 8 B per edge")
+            what = ("all rounds in one launch (with the prologue launch of a directly binned job, timed together): "
+                    "per round 16 B gathered per entry, 16 B written per entry kept for the next round, 8 B per edge")
     elif sort_ms >= upd_ms:  # the radix-sort digit pass dominates
         per_launch = 24.0 * sort_elems / max(sort_passes, 1)
         ms, nl, kname = sort_ms, sort_passes, "onesweep_kernel"
