@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import contextlib
 import ctypes
+import os
 import dataclasses
 import struct
 from typing import Iterable
@@ -238,6 +239,12 @@ class Job:
         self._async_keep = arr
         check(self._lib.emp_job_feed_fastq_async(self.handle, arr.ctypes.data, arr.size, int(last)), "feed_async")
 
+    def feed_files(self, paths) -> None:
+        """Append the FASTQ of files in order (plain, gzip or BGZF) and mark
+        the end of the input (emp_job_feed_files)."""
+        arr = _path_array(paths)
+        check(self._lib.emp_job_feed_files(self.handle, arr, len(arr)), "feed_files")
+
     def feed_device(self, ptr: int, nbytes: int, last: bool = True) -> None:
         check(self._lib.emp_job_feed_fastq_device(self.handle, ptr, nbytes, int(last)), "feed_device")
 
@@ -424,6 +431,39 @@ def run_file(input_path: str, output_path: str, device: int = -1, **params) -> d
     check(_native.lib().emp_run_file(input_path.encode(), output_path.encode(), ctypes.byref(p), device,
                                      ctypes.byref(st)), "emp_run_file")
     return st.to_dict()
+
+
+def _path_array(paths):
+    if isinstance(paths, (str, bytes, os.PathLike)):
+        paths = [paths]
+    enc = [os.fsencode(p) for p in paths]
+    return (ctypes.c_char_p * len(enc))(*enc)
+
+
+def run_files(input_paths, output_path: str, device: int = -1, **params) -> dict:
+    """run_file over the FASTQ of several files in order, each plain, gzip or BGZF."""
+    p = _params(**params)
+    st = _native.Stats()
+    arr = _path_array(input_paths)
+    check(_native.lib().emp_run_files(arr, len(arr), os.fsencode(output_path), ctypes.byref(p), device,
+                                      ctypes.byref(st)), "emp_run_files")
+    return st.to_dict()
+
+
+def load_fastq(paths) -> bytes:
+    """The FASTQ of files as a job reads them (plain, gzip, BGZF; in order,
+    a newline added between files where one is missing), on the host."""
+    arr = _path_array(paths)
+    data = ctypes.c_void_p()
+    n = ctypes.c_uint64()
+    lib = _native.lib()
+    check(lib.emp_fastq_load(arr, len(arr), ctypes.byref(data), ctypes.byref(n)), "emp_fastq_load")
+    if not data.value:
+        return b""
+    try:
+        return ctypes.string_at(data.value, n.value)
+    finally:
+        lib.emp_free(data)
 
 
 def decode_output(data: bytes) -> list[tuple[int, np.ndarray, np.ndarray]]:

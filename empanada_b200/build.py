@@ -26,6 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
 CU_SOURCES = ["k_scan.cu", "k_map.cu", "k_sort.cu", "k_sort_static.cu", "k_round.cu",
               "k_bucket.cu", "k_chunked.cu", "k_dedup.cu", "k_graph.cu", "engine.cu"]
+CXX_SOURCES = ["ingest.cpp"]  # FASTQ files: plain, gzip, BGZF (zlib)
 
 
 def _run(cmd: list[str]) -> str:
@@ -59,12 +60,19 @@ def build_native(verbose: bool = False, ptxas_info: bool = False) -> None:
         if _stale(o, [s] + hdrs) or ptxas_info:
             cmd = [NVCC] + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", s, "-o", o]
             jobs.append(cmd)
+    for src in CXX_SOURCES:  # host-only parts (g++)
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cpp", ".o"))
+        objs.append(o)
+        if _stale(o, [s] + hdrs):
+            jobs.append(["g++", "-O2", "-std=c++17", "-fPIC", "-Wall", "-I", os.path.join(ROOT, "include"), "-c", s,
+                         "-o", o])
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         for out in ex.map(_run, jobs):
             if verbose and out.strip():
                 print(out)
     if _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lz"])
     cli_src = os.path.join(CSRC, "cli.cpp")
     if _stale(CLI, [cli_src, LIB] + hdrs):
         _run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), cli_src, "-o", CLI,

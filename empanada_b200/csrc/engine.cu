@@ -23,6 +23,7 @@
 #include <sys/stat.h>
 
 #include "../../include/empanada.h"
+#include "ingest.h"
 #include "kernels.h"
 
 namespace emp {
@@ -2136,9 +2137,94 @@ emp_status emp_job_fingerprints(emp_job *job, uint64_t *keys, uint64_t cap, uint
     return EMP_OK;
 }
 
-emp_status emp_run_file(const char *input_path, const char *output_path, const emp_params *p, int device,
-                        emp_stats *stats) {
-    if (!input_path || !output_path) return EMP_E_INVAL;
+emp_status emp_job_feed_files(emp_job *job, const char *const *paths, int n_paths) {
+    if (!job) return EMP_E_INVAL;
+    if (job->server) return EMP_E_STATE;
+    if (job->fed_last) return EMP_E_STATE;
+    FastqReader rd;
+    EMP_TRY(rd.open(paths, n_paths));
+    emp_ctx *ctx = job->ctx;
+    cudaSetDevice(ctx->device);
+    if (rd.size_hint()) EMP_TRY(emp_job_reserve(job, job->F + rd.size_hint()));
+    // Two pinned buffers in turn: piece k+1 is read (or inflated) while
+    // piece k copies to the device on the copy stream.
+    const size_t chunk = 128ull << 20;
+    PinnedBuf hb[2];
+    cudaEvent_t copied[2] = {nullptr, nullptr};
+    emp_status st = EMP_OK;
+    if (cudaEventCreateWithFlags(&copied[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&copied[1], cudaEventDisableTiming) != cudaSuccess)
+        st = EMP_E_CUDA;
+    for (int k = 0; st == EMP_OK; ++k) {
+        const int b = k & 1;
+        if (k >= 2 && cudaEventSynchronize(copied[b]) != cudaSuccess) {  // the copy that used this buffer
+            st = EMP_E_CUDA;
+            break;
+        }
+        if (!hb[b].ensure(chunk)) {
+            st = EMP_E_NOMEM;
+            break;
+        }
+        size_t got = 0;
+        st = rd.read(hb[b].p, chunk, &got);
+        if (st != EMP_OK || got == 0) break;
+        st = emp_job_feed_fastq_async(job, hb[b].as<char>(), got, 0);
+        if (st == EMP_OK && cudaEventRecord(copied[b], ctx->copy_stream) != cudaSuccess) st = EMP_E_CUDA;
+    }
+    if (st == EMP_OK) st = emp_job_feed_fastq_async(job, nullptr, 0, 1);
+    // the pinned buffers are released below: their copies must be done
+    if (cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess && st == EMP_OK) st = EMP_E_CUDA;
+    for (cudaEvent_t e : copied)
+        if (e) cudaEventDestroy(e);
+    return st;
+}
+
+emp_status emp_fastq_load(const char *const *paths, int n_paths, void **data, uint64_t *bytes) {
+    if (!data || !bytes) return EMP_E_INVAL;
+    *data = nullptr;
+    *bytes = 0;
+    FastqReader rd;
+    EMP_TRY(rd.open(paths, n_paths));
+    size_t cap = (size_t)rd.size_hint() + FastqReader::kMinChunk;  // the last, empty read fits too
+    uint8_t *buf = static_cast<uint8_t *>(std::malloc(cap));
+    if (!buf) return EMP_E_NOMEM;
+    size_t n = 0;
+    for (;;) {
+        if (cap - n < FastqReader::kMinChunk) {  // room for one more piece
+            const size_t nc = std::max(cap + cap / 2, n + FastqReader::kMinChunk);
+            uint8_t *q = static_cast<uint8_t *>(std::realloc(buf, nc));
+            if (!q) {
+                std::free(buf);
+                return EMP_E_NOMEM;
+            }
+            buf = q;
+            cap = nc;
+        }
+        size_t got = 0;
+        const emp_status st = rd.read(buf + n, cap - n, &got);
+        if (st != EMP_OK) {
+            std::free(buf);
+            return st;
+        }
+        if (got == 0) break;
+        n += got;
+    }
+    if (n == 0) {
+        std::free(buf);
+        return EMP_OK;
+    }
+    *data = buf;
+    *bytes = n;
+    return EMP_OK;
+}
+
+void emp_free(void *p) { std::free(p); }
+
+emp_status emp_run_files(const char *const *input_paths, int n_inputs, const char *output_path, const emp_params *p,
+                         int device, emp_stats *stats) {
+    if (!output_path || n_inputs < 0 || (n_inputs && !input_paths)) return EMP_E_INVAL;
+    for (int i = 0; i < n_inputs; ++i)
+        if (!input_paths[i]) return EMP_E_INVAL;
     emp_ctx *ctx = nullptr;
     EMP_TRY(emp_ctx_create(device, 0, &ctx));
     emp_job *job = nullptr;
@@ -2147,61 +2233,8 @@ emp_status emp_run_file(const char *input_path, const char *output_path, const e
         emp_ctx_destroy(ctx);
         return st;
     }
-    bool ran = false;
-    // Read the input.  A missing file reads as empty, like the reference's
-    // ifstream; a path that exists but is not a readable regular file is an
-    // EMP_E_IO error.  Two pinned buffers alternate: chunk k+1 is read from
-    // the file while chunk k copies to the device on the copy stream.
-    struct stat sb;
-    if (::stat(input_path, &sb) != 0) {
-        if (errno != ENOENT) st = EMP_E_IO;
-    } else if (!S_ISREG(sb.st_mode)) {
-        st = EMP_E_IO;
-    } else if (sb.st_size > 0 && st == EMP_OK) {
-        FILE *f = std::fopen(input_path, "rb");
-        if (!f) st = EMP_E_IO;
-        const uint64_t size = (uint64_t)sb.st_size;
-        const size_t chunk = 128ull << 20;
-        PinnedBuf hb[2];
-        cudaEvent_t copied[2] = {nullptr, nullptr};
-        if (st == EMP_OK && (cudaEventCreateWithFlags(&copied[0], cudaEventDisableTiming) != cudaSuccess ||
-                             cudaEventCreateWithFlags(&copied[1], cudaEventDisableTiming) != cudaSuccess))
-            st = EMP_E_CUDA;
-        if (st == EMP_OK) st = emp_job_reserve(job, size);
-        uint64_t left = size;
-        for (int k = 0; st == EMP_OK && left; ++k) {
-            const int b = k & 1;
-            if (k >= 2 && cudaEventSynchronize(copied[b]) != cudaSuccess) {  // the copy that used this buffer
-                st = EMP_E_CUDA;
-                break;
-            }
-            const size_t want = left < chunk ? (size_t)left : chunk;
-            if (!hb[b].ensure(want)) {
-                st = EMP_E_NOMEM;
-                break;
-            }
-            const size_t got = std::fread(hb[b].p, 1, want, f);
-            if (got != want) {
-                st = EMP_E_IO;
-                break;
-            }
-            left -= got;
-            st = emp_job_feed_fastq_async(job, hb[b].as<char>(), got, left == 0);
-            if (st == EMP_OK && cudaEventRecord(copied[b], ctx->copy_stream) != cudaSuccess) st = EMP_E_CUDA;
-        }
-        if (f) std::fclose(f);
-        if (st == EMP_OK) st = emp_job_run(job, nullptr);  // waits for the last copy
-        cudaStreamSynchronize(ctx->copy_stream);  // the pinned buffers are released below
-        for (cudaEvent_t e : copied)
-            if (e) cudaEventDestroy(e);
-        if (st != EMP_OK) {
-            emp_job_destroy(job);
-            emp_ctx_destroy(ctx);
-            return st;
-        }
-        ran = true;
-    }
-    if (st == EMP_OK && !ran) st = emp_job_run(job, nullptr);
+    st = emp_job_feed_files(job, input_paths, n_inputs);
+    if (st == EMP_OK) st = emp_job_run(job, nullptr);  // waits for the last copy
     if (st == EMP_OK) {
         FILE *g = std::fopen(output_path, "wb");
         if (!g) st = EMP_E_IO;
@@ -2222,6 +2255,12 @@ emp_status emp_run_file(const char *input_path, const char *output_path, const e
     emp_job_destroy(job);
     emp_ctx_destroy(ctx);
     return st;
+}
+
+emp_status emp_run_file(const char *input_path, const char *output_path, const emp_params *p, int device,
+                        emp_stats *stats) {
+    if (!input_path) return EMP_E_INVAL;
+    return emp_run_files(&input_path, 1, output_path, p, device, stats);
 }
 
 }  // extern "C"

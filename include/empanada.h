@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define EMP_ABI_VERSION 5
+#define EMP_ABI_VERSION 6
 
 typedef int emp_status;
 #define EMP_OK 0
@@ -147,6 +147,17 @@ emp_status emp_job_feed_fastq(emp_job *job, const char *bytes, uint64_t n, int l
 emp_status emp_job_feed_fastq_async(emp_job *job, const char *bytes, uint64_t n, int last);
 /* Same for bytes already in device memory on the context's device. */
 emp_status emp_job_feed_fastq_device(emp_job *job, const void *dev_bytes, uint64_t n, int last);
+/* Append the FASTQ of files, in order, and mark the end of the input: each
+ * file plain, gzip (one or more members) or BGZF (blocked gzip, its blocks
+ * inflated in parallel on the host cores); a newline is added after a file
+ * that does not end with one when another non-empty file follows.  A
+ * missing file reads as empty (as the reference's read of its one plain
+ * file, preprocess.cu:195-237); a path that exists but is not a readable
+ * regular file is EMP_E_IO, a damaged gzip stream or BGZF block
+ * EMP_E_FORMAT.  The files are read into two page-locked buffers in turn:
+ * one piece is inflated or read while the previous one copies to the
+ * device (no counterpart in the reference). */
+emp_status emp_job_feed_files(emp_job *job, const char *const *paths, int n_paths);
 /* Reserve device room for `bytes` of FASTQ (optional; avoids regrowth). */
 emp_status emp_job_reserve(emp_job *job, uint64_t bytes);
 /* Forget the fed input and the last result but keep every device buffer, so
@@ -241,9 +252,18 @@ emp_status emp_job_fingerprints(emp_job *job, uint64_t *keys, uint64_t cap, uint
 
 /* The whole reference program (main.cu:9-77): read input_path, write
  * output_path.  A missing input file gives an empty output.bin, as in the
- * reference.  device < 0: current device. */
+ * reference.  device < 0: current device.  The input may also be gzip or
+ * BGZF compressed (emp_job_feed_files). */
 emp_status emp_run_file(const char *input_path, const char *output_path, const emp_params *p, int device,
                         emp_stats *st);
+/* emp_run_file over the FASTQ of several files in order (emp_job_feed_files). */
+emp_status emp_run_files(const char *const *input_paths, int n_inputs, const char *output_path, const emp_params *p,
+                         int device, emp_stats *st);
+/* The FASTQ of files as emp_job_feed_files reads them, into host memory
+ * (malloc'd, freed by emp_free): *data = NULL when it is empty.  No device
+ * is used. */
+emp_status emp_fastq_load(const char *const *paths, int n_paths, void **data, uint64_t *bytes);
+void emp_free(void *p);
 
 /* Unitigs of the overlap graph in an output.bin: the downstream consumer
  * that the reference leaves out (its GFA writers, overlap.cu:129-190, are dead

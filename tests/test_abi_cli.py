@@ -33,7 +33,7 @@ def test_header_declarations_are_exported():
 
 def test_abi_version_and_status_strings():
     lib = _native.lib()
-    assert lib.emp_abi_version() == 5
+    assert lib.emp_abi_version() == 6
     for code in range(0, -10, -1):
         assert lib.emp_status_string(code)
     assert _native.status_string(_native.EMP_E_FORMAT).startswith("reads of unequal length")

@@ -110,3 +110,57 @@ def test_run_file_in_many_chunks(tmp_path):
     assert rc == 0
     data = out.read_bytes()
     assert hashlib.sha256(data).hexdigest() == GOLDEN["larger"]["sha256"]
+
+
+def _records_split(data: bytes, parts: int) -> list[bytes]:
+    """data cut into `parts` pieces at record boundaries (every fourth newline)."""
+    nl = [i for i, c in enumerate(data) if c == 10][3::4]
+    cuts = [nl[len(nl) * k // parts] + 1 for k in range(1, parts)] if len(nl) >= parts else []
+    bounds = [0] + cuts + [len(data)]
+    return [data[a:b] for a, b in zip(bounds, bounds[1:])]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["gzip", "bgzf"])
+def test_cli_reads_compressed_input(tmp_path, kind):
+    """The drop-in command on gzip and BGZF input writes the same output.bin
+    as the reference on the plain file."""
+    import gzip
+
+    from test_ingest import bgzf
+
+    case = BY_NAME["small"]
+    data = case.fastq()
+    fq = tmp_path / "in.fq.gz"
+    fq.write_bytes(gzip.compress(data) if kind == "gzip" else bgzf(data))
+    p = _cli([str(fq), "out.bin"] + list(case.args), cwd=str(tmp_path))
+    assert p.returncode == 0, p.stderr
+    out = (tmp_path / "out.bin").read_bytes()
+    assert hashlib.sha256(out).hexdigest() == GOLDEN["small"]["sha256"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["tiny", "n_reads", "split_r128k"])
+def test_run_files_and_feed_files_match_reference(tmp_path, name):
+    """emp_run_files and emp_job_feed_files over the case's FASTQ cut into a
+    plain, a gzip and a BGZF file (at record boundaries)."""
+    import gzip
+
+    from test_ingest import bgzf
+
+    case = BY_NAME[name]
+    parts = _records_split(case.fastq(), 3)
+    paths = []
+    for k, (piece, enc) in enumerate(zip(parts, (lambda b: b, gzip.compress, bgzf))):
+        q = tmp_path / f"part{k}"
+        q.write_bytes(enc(piece))
+        paths.append(str(q))
+    g = GOLDEN[name]
+    out = tmp_path / "out.bin"
+    params = dict(min_ovlp=case.min_ovlp(), reduce_mem=case.reduce_mem())
+    empanada_b200.run_files(paths, str(out), **params)
+    assert hashlib.sha256(out.read_bytes()).hexdigest() == g["sha256"]
+    with empanada_b200.Engine(0) as eng, eng.job(**params) as job:
+        job.feed_files(paths)
+        job.run()
+        assert hashlib.sha256(job.output()).hexdigest() == g["sha256"]
