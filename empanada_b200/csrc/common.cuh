@@ -135,6 +135,10 @@ EMP_DEV void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+// start pulling `bytes` of global memory into L2 (a hint: no completion)
+EMP_DEV void prefetch_l2(const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
+}
 // wait for the barrier's phase `parity` to complete; false after `limit` polls
 EMP_DEV bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
     for (uint32_t i = 0; i < limit; ++i) {

@@ -134,6 +134,29 @@ EMP_DEV void tile_loop_static(S &sh, uint32_t *ticket, int J, uint32_t total, F 
     }
 }
 
+// tile_loop_static that takes its next tile before it runs the current one,
+// so that the current one can start fetching the next one's data:
+// f(job, local tile, the next tile's global index or ~0u).
+template <class S, class F>
+EMP_DEV void tile_loop_ahead(S &sh, uint32_t *ticket, int J, uint32_t total, F f) {
+    if (blockIdx.x >= total) return;
+    const bool more = total > gridDim.x;
+    uint32_t cur = blockIdx.x;
+    for (;;) {
+        uint32_t nxt = ~0u;
+        if (more) {
+            if (threadIdx.x == 0) sh.tile = gridDim.x + atomicAdd(ticket, 1u);
+            __syncthreads();
+            nxt = sh.tile;
+            __syncthreads();
+            if (nxt >= total) nxt = ~0u;
+        }
+        run_tile(sh, J, cur, [&](int j, uint32_t b) { f(j, b, nxt); });
+        if (nxt == ~0u) return;
+        cur = nxt;
+    }
+}
+
 // take tiles from the ticket until all `total` are gone; f(job, local tile)
 template <class S, class F>
 EMP_DEV void tile_loop(S &sh, uint32_t *ticket, int J, uint32_t total, F f) {

@@ -1475,12 +1475,26 @@ EMP_DEV RoundShape round_shape(const BktJob &J, uint32_t iter) {
     return z;
 }
 
+// The next tile this CTA runs (job, bucket, iteration), whose two regions
+// are pulled into L2 while this one is worked on; job = nullptr: none.
+struct NextTile {
+    const BktJob *job;
+    uint32_t b, iter;
+};
+
 EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &z, BShared &sh, const CoopCtl *ctl,
-                        uint8_t *smem) {
+                        uint8_t *smem, const NextTile &nt) {
     probe(ctl, iter, 2);
     if (threadIdx.x == 0) {
         sh.pctl = ctl;
         sh.piter = iter;
+    }
+    uint32_t ncS = 0, ncP = 0;  // the next tile's region sizes, loaded now and used after the staging
+    ListIn nli;
+    if (threadIdx.x == 0 && nt.job) {
+        nli = list_in(*nt.job, nt.iter);
+        ncS = __ldcg(nli.cnt + 2 * nt.b);
+        ncP = __ldcg(nli.cnt + 2 * nt.b + 1);
     }
     __syncthreads();
     BktRound &I = J.meta[z.r];
@@ -1491,6 +1505,11 @@ EMP_DEV void round_tile(BktJob &J, uint32_t b, uint32_t iter, const RoundShape &
     uint64_t G = 0;
     const uint32_t total = gather(J, li, b, sh, smem, v, S, G);
     const bool in_smem = total <= kBStage;
+    if (threadIdx.x == 0 && nt.job) {
+        const uint32_t s1 = min(ncS, nli.cap), p1 = min(ncP, nli.cap);
+        if (s1) prefetch_l2(nli.lst + (uint64_t)(2 * nt.b) * nli.cap, s1 * 16u);
+        if (p1) prefetch_l2(nli.lst + (uint64_t)(2 * nt.b + 1) * nli.cap, p1 * 16u);
+    }
     probe(ctl, iter, 3);
     // ---- entries whose key is in both tables: flagged, compacted, ranked, joined
     uint32_t c = 0;
@@ -1724,14 +1743,24 @@ __global__ void __launch_bounds__(kT, 2) bucket_rounds_kernel(BktJob *jobs, Coop
         });
         if (total == 0) break;  // no job has a round left
         probe(ctl, it, 1);
-        tile_loop_static(sh, ticket, J, total, [&](int j, uint32_t b) {
+        tile_loop_ahead(sh, ticket, J, total, [&](int j, uint32_t b, uint32_t next) {
             const uint32_t g = jobs[j].iter0 + it;
             RoundShape z;
             z.active = true;
             z.r = jobs[j].r0 + (int)g;
             z.nb = sh.shp_nb[j];
             z.nb_next = sh.shp_nbn[j];
-            round_tile(jobs[j], b, g, z, sh, ctl, smem);
+            NextTile nt{nullptr, 0u, 0u};
+            if (next != ~0u) {
+                int lo = 0, hi = J;
+                while (hi - lo > 1) {
+                    const int m = (lo + hi) >> 1;
+                    if (sh.pref[m] <= next) lo = m;
+                    else hi = m;
+                }
+                nt = NextTile{&jobs[lo], next - sh.pref[lo], jobs[lo].iter0 + it};
+            }
+            round_tile(jobs[j], b, g, z, sh, ctl, smem, nt);
         });
         probe(ctl, it, 9);
         if (!grid_barrier(ctl, &sh.flag, &sh.gen, it, 0)) return;
