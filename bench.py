@@ -453,8 +453,9 @@ def served_bench(args):
         lat = np.zeros(n)
         ok = True
         reads = 0
-        srv = (empanada_b200.Server(eng, rounds_per_launch=args.serve_rounds, hbm_budget_bytes=args.serve_budget << 30,
-                                    batch_max_entries=args.serve_batch_max)
+        srv = (empanada_b200.Server(eng, rounds_per_launch=args.serve_rounds, rounds_per_launch_idle=args.serve_rounds_idle,
+                                    hbm_budget_bytes=args.serve_budget << 30,
+                                    batch_max_entries=args.serve_batch_max, share_min_entries=args.serve_share_min)
                if served else None)
         pending = collections.deque()
         held = {}
@@ -543,8 +544,9 @@ def served_bench(args):
                                    "10-80x, 0.1% substitutions) plus 2% heavy jobs (50 Mbp genome at 30x, 150 or "
                                    "250 bp), -o 31; jobs per rate: rate x "
                                    f"{args.serve_seconds} s within [{args.serve_min_jobs}, {args.serve_max_jobs}]",
-                       "rounds_per_launch": args.serve_rounds, "admission_budget_gib": args.serve_budget,
-                       "batch_max_entries": args.serve_batch_max,
+                       "rounds_per_launch": args.serve_rounds, "rounds_per_launch_idle": args.serve_rounds_idle,
+                       "admission_budget_gib": args.serve_budget,
+                       "batch_max_entries": args.serve_batch_max, "share_min_entries": args.serve_share_min,
                        "rates_per_s": rates},
             "served": served, "plain": plain, "clocks": clocks, "host_generate_s": gen_s,
             "e2e": {"value": served[str(rates[-1])]["reads_per_s"], "unit": "reads/s",
@@ -576,6 +578,11 @@ def main():
     ap.add_argument("--serve-max-jobs", type=int, default=400)
     ap.add_argument("--serve-pool", type=int, default=48)
     ap.add_argument("--serve-rounds", type=int, default=16, help="bucket-kernel rounds per launch")
+    ap.add_argument("--serve-rounds-idle", type=int, default=64,
+                    help="served: rounds per launch while no job waits to join")
+    ap.add_argument("--serve-share-min", type=int, default=8_000_000,
+                    help="served: jobs with a first list at least this long run rounds_per_launch rounds a launch, "
+                         "shorter ones all their rounds (0: every job the launch's rounds)")
     ap.add_argument("--serve-batch-max", type=int, default=0,
                     help="served jobs with a longer first round list run alone (0: the bucket kernel's limit)")
     ap.add_argument("--serve-budget", type=int, default=100, help="admission budget of the server, GiB")

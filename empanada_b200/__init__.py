@@ -306,11 +306,12 @@ class Server:
     from submit() until a step returns it."""
 
     def __init__(self, engine: Engine, rounds_per_launch: int = 16, max_jobs: int = 256,
-                 hbm_budget_bytes: int = 0, rounds_per_launch_idle: int = 64, batch_max_entries: int = 0):
+                 hbm_budget_bytes: int = 0, rounds_per_launch_idle: int = 64, batch_max_entries: int = 0,
+                 share_min_entries: int = 8_000_000):
         self.engine = engine
         self._lib = engine._lib
         p = _native.ServerParams(int(rounds_per_launch), int(max_jobs), int(hbm_budget_bytes),
-                                 int(rounds_per_launch_idle), int(batch_max_entries))
+                                 int(rounds_per_launch_idle), int(batch_max_entries), int(share_min_entries))
         h = ctypes.c_void_p()
         check(self._lib.emp_server_create(engine.handle, ctypes.byref(p), ctypes.byref(h)), "emp_server_create")
         self.handle = h

@@ -80,6 +80,7 @@ class ServerParams(ctypes.Structure):
         ("hbm_budget_bytes", ctypes.c_uint64),
         ("rounds_per_launch_idle", ctypes.c_int32),
         ("batch_max_entries", ctypes.c_uint64),
+        ("share_min_entries", ctypes.c_uint64),
     ]
 
 

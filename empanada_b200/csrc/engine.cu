@@ -1386,11 +1386,21 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
         }
         hj = srv->h_jobs.as<BktJob>();
         hc = reinterpret_cast<CoopCtl *>(hj + nb);
-        for (size_t k = 0; k < nb; ++k) hj[k] = srv->live[k]->bk;
+        // Per-job shares of the launch's iterations: a large job runs a few
+        // rounds (short launches while jobs wait to join, long ones when none
+        // does); a small one all its rounds, which after the large jobs' share
+        // cost a few microseconds each, so it leaves in the launch it joins.
+        const uint32_t share = (uint32_t)(srv->queue.empty() && adm.empty() ? srv->p.rounds_per_launch_idle
+                                                                             : srv->p.rounds_per_launch);
+        bool any_unlimited = false;
+        for (size_t k = 0; k < nb; ++k) {
+            hj[k] = srv->live[k]->bk;
+            const bool large = !srv->p.share_min_entries || 2 * srv->live[k]->prep.U >= srv->p.share_min_entries;
+            hj[k].iter_share = large ? share : 0u;
+            any_unlimited |= !large;
+        }
         coop_ctl_init(ctx, hc, (uint32_t)nb);
-        // short launches while jobs wait to join, long ones when none does
-        hc->iter_cap = (uint32_t)(srv->queue.empty() && adm.empty() ? srv->p.rounds_per_launch_idle
-                                                                     : srv->p.rounds_per_launch);
+        hc->iter_cap = any_unlimited ? 0u : share;
         EMP_CUDA(cudaMemcpyAsync(srv->d_jobs.p, hj, nb * sizeof(BktJob), cudaMemcpyHostToDevice, s));
         EMP_CUDA(cudaMemcpyAsync(srv->d_ctl.p, hc, sizeof(CoopCtl), cudaMemcpyHostToDevice, s));
         EMP_CUDA(cudaEventRecord(srv->ev[0], s));
@@ -1470,7 +1480,8 @@ emp_status server_step(emp_server *srv, cudaStream_t s) {
             done.push_back(j);
             if (!timed_out) EMP_TRY(bucket_fetch(j, job_env(j), s));
         } else {
-            j->bk.iter0 += hc->iters;
+            const uint32_t sh = j->bk.iter_share;
+            j->bk.iter0 += sh && sh < hc->iters ? sh : hc->iters;  // the iterations it ran
             still.push_back(j);
         }
     }
@@ -1959,6 +1970,7 @@ emp_status emp_server_params_default(emp_server_params *p) {
     p->hbm_budget_bytes = 0;
     p->rounds_per_launch_idle = 64;
     p->batch_max_entries = 0;
+    p->share_min_entries = 8000000;
     return EMP_OK;
 }
 

@@ -1598,7 +1598,8 @@ EMP_COLD void place_edges(BktJob *jobs, int J, uint32_t its, BShared &sh, uint8_
     uint32_t g = 0;
     for (int j = 0; j < J; ++j) {
         BktJob &x = jobs[j];
-        if (round_shape(x, x.iter0 + its).active) continue;  // resumes in the next launch
+        const uint32_t ran = x.iter_share && x.iter_share < its ? x.iter_share : its;
+        if (round_shape(x, x.iter0 + ran).active) continue;  // resumes in the next launch
         if (blockIdx.x == 0 && threadIdx.x == 0) x.done = 1;
         const uint32_t r0 = (uint32_t)x.r0;
         // the rounds that ran: round r ran iff r < rounds and it had a suffix
@@ -1736,6 +1737,8 @@ __global__ void __launch_bounds__(kT, 2) bucket_rounds_kernel(BktJob *jobs, Coop
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ticket[1 + ((it + 1) & 1)] = 0;  // last iteration's
         probe(ctl, it, 0);
         total = build_prefix(sh, J, [&](int j) -> uint32_t {
+            const uint32_t share = jobs[j].iter_share;
+            if (share && it >= share) return 0u;  // its share of this launch is used up
             const RoundShape z = round_shape(jobs[j], jobs[j].iter0 + it);
             sh.shp_nb[j] = z.nb;
             sh.shp_nbn[j] = z.nb_next;

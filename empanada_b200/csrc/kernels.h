@@ -292,6 +292,7 @@ struct BktJob {
     uint32_t overflow;       // the edge buffer was too small
     uint32_t iter0;          // iterations run by earlier launches (0: the launch starts the job)
     uint32_t pre_done;       // the prologue ran in its own launch (launch_bucket_prologue)
+    uint32_t iter_share;     // iterations this launch runs for the job at most (0: no limit)
     uint32_t done;           // set at the end of a launch after which the job has no round left
     uint64_t e_total;        // edges of the finished rounds of this launch
     uint64_t e_stage;        // staging buffer fill

@@ -207,6 +207,10 @@ typedef struct emp_server_params {
     uint64_t hbm_budget_bytes; /* admission budget (0: the context's, or none) */
     int32_t rounds_per_launch_idle; /* the same while no job waits to join (default 64) */
     uint64_t batch_max_entries; /* a job whose first round list is longer runs alone (0: the bucket kernel's 16M) */
+    uint64_t share_min_entries; /* a job whose first round list is at least this long runs rounds_per_launch
+                                   (rounds_per_launch_idle while no job waits) rounds of a launch; a shorter
+                                   one runs all its rounds in the launch it joins (default 8M; 0: every job
+                                   the launch's rounds) */
 } emp_server_params;
 emp_status emp_server_params_default(emp_server_params *p);
 emp_status emp_server_create(emp_ctx *ctx, const emp_server_params *p, emp_server **out);

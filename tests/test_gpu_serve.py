@@ -34,14 +34,16 @@ def _drain(srv, limit=100000):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rounds_per_launch", [1, 3, 16, 1000])
-def test_served_golden_cases_staggered(engine, rounds_per_launch):
+@pytest.mark.parametrize("rounds_per_launch,share_min", [(1, 1), (3, 1), (16, 1), (1000, 1), (1, 0), (2, 200_000)])
+def test_served_golden_cases_staggered(engine, rounds_per_launch, share_min):
     """Jobs arrive while others are mid-rounds (a few submitted per step):
-    every output is the reference's."""
+    every output is the reference's.  share_min = 1: every job runs
+    rounds_per_launch rounds a launch; 0: every job the launch's rounds;
+    200k: the larger cases a share, the smaller all their rounds at once."""
     jobs = {n: _job(engine, n) for n in NAMES}
     order = NAMES[::2] + NAMES[1::2]
     with empanada_b200.Server(engine, rounds_per_launch=rounds_per_launch, rounds_per_launch_idle=rounds_per_launch,
-                              max_jobs=8) as srv:
+                              max_jobs=8, share_min_entries=share_min) as srv:
         done = []
         for k in range(0, len(order), 3):
             for n in order[k:k + 3]:
@@ -78,7 +80,7 @@ def test_served_lone_job_in_idle_server_runs_alone(engine):
     (no batched launch); a job admitted while another is in flight joins the
     batch."""
     a, b = _job(engine, "sub_errors"), _job(engine, "odd_len")
-    with empanada_b200.Server(engine, rounds_per_launch=1, rounds_per_launch_idle=1) as srv:
+    with empanada_b200.Server(engine, rounds_per_launch=1, rounds_per_launch_idle=1, share_min_entries=1) as srv:
         srv.submit(a)
         done = srv.step()
         st = srv.stats()
@@ -116,9 +118,11 @@ def test_served_batch_max_entries_sends_jobs_alone(engine):
 
 
 @pytest.mark.gpu
-def test_served_mix_equals_alone(engine):
+@pytest.mark.parametrize("share_min", [1, 8_000_000])
+def test_served_mix_equals_alone(engine, share_min):
     """Mixed read sets (20-300 kbp genomes, 100-300 bp reads) submitted in
-    waves: each output equals the job run alone."""
+    waves: each output equals the job run alone, whether every job runs 8
+    rounds a launch or each all its rounds in the launch it joins."""
     sets = synth.batched_sets(n_sets=40, seed=12, genome_min=20_000, genome_max=300_000, len_max=300)
     data = [synth.fastq_bytes(w) for w in sets]
     alone = []
@@ -126,7 +130,7 @@ def test_served_mix_equals_alone(engine):
         out, _ = empanada_b200.run_bytes(d, engine=engine, min_ovlp=w.min_ovlp)
         alone.append(out)
     jobs = []
-    with empanada_b200.Server(engine, rounds_per_launch=8) as srv:
+    with empanada_b200.Server(engine, rounds_per_launch=8, share_min_entries=share_min) as srv:
         for k, (w, d) in enumerate(zip(sets, data)):
             j = engine.job(min_ovlp=w.min_ovlp)
             j.feed(d)
@@ -150,7 +154,7 @@ def test_served_failure_and_edge_restart(engine):
     bad = engine.job(min_ovlp=20, reduce_mem="16k")
     bad.feed(cases.edge_ooc_hang())
     good = [_job(engine, n) for n in ("tiny", "sub_errors", "read_len_255")]
-    with engine.tuned(edge_cap=8), empanada_b200.Server(engine, rounds_per_launch=4) as srv:
+    with engine.tuned(edge_cap=8), empanada_b200.Server(engine, rounds_per_launch=4, share_min_entries=1) as srv:
         srv.submit(good[0])
         srv.submit(bad)
         srv.step()
@@ -173,7 +177,7 @@ def test_served_admission_budget(engine):
     job, one after another."""
     jobs = [_job(engine, n) for n in ("tiny", "odd_len", "dups_palindromes")]
     budget = max(4 * len(BY_NAME[n].fastq()) for n in ("tiny", "odd_len", "dups_palindromes")) + (64 << 20)
-    with empanada_b200.Server(engine, rounds_per_launch=2, hbm_budget_bytes=budget) as srv:
+    with empanada_b200.Server(engine, rounds_per_launch=2, hbm_budget_bytes=budget, share_min_entries=1) as srv:
         for j in jobs:
             srv.submit(j)
         srv.step()
