@@ -306,20 +306,33 @@ EMP_DEV T block_exclusive_scan(T v, T *smem_warp /* NT/32 */, T *total) {
     }
     if (lane == 31) smem_warp[warp] = x;
     __syncthreads();
-    if (warp == 0) {
-        T w = lane < NT / 32 ? smem_warp[lane] : T(0);
+    if constexpr (NT <= 256) {  // every thread adds up the (at most 8) warp totals itself
+        T before = T(0), all = T(0);
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            T y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
+        for (int w = 0; w < NT / 32; ++w) {
+            const T t = smem_warp[w];
+            all += t;
+            if (w < warp) before += t;
         }
-        if (lane < NT / 32) smem_warp[lane] = w;
+        *total = all;
+        __syncthreads();  // smem_warp is written again by the next scan
+        return before + x - v;
+    } else {
+        if (warp == 0) {
+            T w = lane < NT / 32 ? smem_warp[lane] : T(0);
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                T y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            if (lane < NT / 32) smem_warp[lane] = w;
+        }
+        __syncthreads();
+        T warp_excl = warp ? smem_warp[warp - 1] : T(0);
+        *total = smem_warp[NT / 32 - 1];
+        __syncthreads();
+        return warp_excl + x - v;
     }
-    __syncthreads();
-    T warp_excl = warp ? smem_warp[warp - 1] : T(0);
-    *total = smem_warp[NT / 32 - 1];
-    __syncthreads();
-    return warp_excl + x - v;
 }
 
 }  // namespace emp
