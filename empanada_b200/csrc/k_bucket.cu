@@ -690,8 +690,11 @@ EMP_DEV bool match_filter(uint32_t total, uint32_t S, uint8_t *smem, BShared &sh
     uint32_t *bm2 = reinterpret_cast<uint32_t *>(reg + kFBm2);
     uint16_t *pl = reinterpret_cast<uint16_t *>(reg + kFPl);
     uint16_t *sl = reinterpret_cast<uint16_t *>(reg + kFSl);
+    uint32_t *hs = reinterpret_cast<uint32_t *>(reg + kFHash);
     for (uint32_t i = threadIdx.x; i < 2 * kFilterWords / 4; i += kT)
         reinterpret_cast<uint4 *>(bm1)[i] = make_uint4(0, 0, 0, 0);  // bm1 and bm2
+    for (uint32_t i = threadIdx.x; i < kListHash / 4; i += kT)  // the short lists' hash set, for later
+        reinterpret_cast<uint4 *>(hs)[i] = make_uint4(kSlotEmpty, kSlotEmpty, kSlotEmpty, kSlotEmpty);
     if (threadIdx.x == 0) {
         sh.cnt = 0;
         sh.tile = 0;
@@ -737,11 +740,7 @@ EMP_DEV bool match_filter(uint32_t total, uint32_t S, uint8_t *smem, BShared &sh
     // the two lists: suffix-list keys into a hash set (equal keys share the
     // slot of the first one in), prefixes probe it, then every suffix of a
     // slot that a prefix hit is flagged
-    uint32_t *hs = reinterpret_cast<uint32_t *>(reg + kFHash);
     uint16_t *slot_of = reinterpret_cast<uint16_t *>(reg + kFSlotOf);
-    for (uint32_t i = threadIdx.x; i < kListHash / 4; i += kT)
-        reinterpret_cast<uint4 *>(hs)[i] = make_uint4(kSlotEmpty, kSlotEmpty, kSlotEmpty, kSlotEmpty);
-    __syncthreads();
     for (uint32_t j = threadIdx.x; j < ns; j += kT) {
         const uint64_t k = key[sl[j]];
         uint32_t sl0 = (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> 32) & (kListHash - 1);

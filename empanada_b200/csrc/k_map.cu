@@ -131,7 +131,7 @@ constexpr uint32_t kWinWords = kWin / 4;
 constexpr uint32_t kRecCap = 2048;  // records per batch (a tile owns up to 4096: four newlines each)
 constexpr uint16_t kNoEnd = 0xffffu;
 constexpr int kChunks = kMaxReadLen / 16;
-static_assert(kParseTile == 64 * kRT, "four 16-byte tile chunks per thread");
+static_assert(kParseTile == 64 * kRT, "64 tile bytes per thread");
 static_assert(kHalo % 16 == 0 && kHalo / 16 <= kRT && kHalo >= kMaxReadLen + 1, "one halo chunk per thread at most");
 static_assert(kWin < kNoEnd, "window offsets fit 16 bits");
 static_assert(kMaxReadLen % 16 == 0, "whole read-major words");
@@ -141,13 +141,17 @@ struct __align__(16) ReadSmem {
     uint32_t chunk[kChunks][8];      // ChunkWeights::w
     uint16_t start[kRecCap];         // sequence line [start, end) of the batch's records (window offsets)
     uint16_t end[kRecCap];           // kNoEnd: no newline ends it inside the window
-    uint64_t scan[kRT / 32];
+    uint32_t scan32[kRT / 32];
     uint64_t bar[2];  // bulk-copy barriers of the two windows
 };
 
 // newline bytes of a word as 4 bits (byte b -> bit b): the bytes' top bits
 // gathered by one multiply (partial products land on distinct bits)
 EMP_DEV uint32_t nl_bits(uint32_t w) { return ((zero_bytes(w ^ 0x0a0a0a0au) >> 7) * 0x00204081u) >> 21 & 0xfu; }
+// newline bytes of 16 bytes as 16 bits, byte order
+EMP_DEV uint32_t nl_mask16(const uint4 &v) {
+    return nl_bits(v.x) | (nl_bits(v.y) << 4) | (nl_bits(v.z) << 8) | (nl_bits(v.w) << 12);
+}
 
 // 16 window bytes from byte offset off (any alignment): x[q] = bytes off+4q ..
 EMP_DEV void win16(const uint32_t *win, uint32_t off, uint32_t x[4]) {
@@ -273,37 +277,23 @@ __global__ void __launch_bounds__(kRT, 4) read_pass_kernel(const uint8_t *__rest
         }
         if (tile + gridDim.x < ntiles) stage_window(fq, F, tile + gridDim.x, sm.win[buf ^ 1], &sm.bar[buf ^ 1]);
         const uint32_t *win = sm.win[buf];
-        // ---- locate.  Thread t holds 16-byte chunks t, t+256, t+512, t+768 of
-        // the tile (rows 0-3) and, for t < 33, chunk t of the halo (row 4).  The
-        // rows' newline counts, packed in 13-bit fields (11 for the halo: the
-        // sums never carry), go through one block scan.
-        uint32_t nlm[5];  // newline bytes of each chunk, one bit per byte
-        uint64_t P = 0;
+        // ---- locate.  Thread t holds tile bytes [64t, 64t + 64) (four 16-byte
+        // chunks, read in an order rotated by t so that a quarter-warp's
+        // shared-memory reads spread over the banks) and, for t < 33, halo chunk
+        // t.  Newline masks in byte order (one bit per byte), their counts, one
+        // block scan of (tile count | halo count << 16): no carries (16384, 528).
+        uint64_t m64 = 0;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (k < 4 || tid < (int)(kHalo / 16)) v = *reinterpret_cast<const uint4 *>(win + 4 * (k * kRT + tid));
-            nlm[k] = nl_bits(v.x) | (nl_bits(v.y) << 4) | (nl_bits(v.z) << 8) | (nl_bits(v.w) << 12);
-            P |= (uint64_t)__popc(nlm[k]) << (13 * k);
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t q = (uint32_t)(k + tid) & 3u;
+            m64 |= (uint64_t)nl_mask16(*reinterpret_cast<const uint4 *>(win + 16 * tid + 4 * q)) << (16 * q);
         }
-        uint64_t x = P;  // inclusive warp scan, then the earlier warps' totals
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) sm.scan[warp] = x;
-        __syncthreads();
-        uint64_t wi = lane < kRT / 32 ? sm.scan[lane] : 0;  // the warps' totals, scanned across lanes
-#pragma unroll
-        for (int o = 1; o < kRT / 32; o <<= 1) {
-            const uint64_t y = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += y;
-        }
-        const uint64_t tot = __shfl_sync(0xffffffffu, wi, kRT / 32 - 1);
-        const uint64_t ex = x - P + (warp ? __shfl_sync(0xffffffffu, wi, warp - 1) : 0ull);
-        const uint32_t tile_nl = (uint32_t)((tot & 0x1fffu) + ((tot >> 13) & 0x1fffu) + ((tot >> 26) & 0x1fffu) +
-                                            ((tot >> 39) & 0x1fffu));
+        const uint32_t mh =
+            tid < (int)(kHalo / 16) ? nl_mask16(*reinterpret_cast<const uint4 *>(win + kParseTile / 4 + 4 * tid)) : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan<kRT, uint32_t>((uint32_t)__popcll(m64) | ((uint32_t)__popc(mh) << 16),
+                                                                sm.scan32, &tot);
+        const uint32_t tile_nl = tot & 0xffffu;
         const uint64_t k0 = (E + 3) >> 2, k1 = (E + tile_nl + 3) >> 2;
         const uint32_t n_own = (uint32_t)(k1 - k0);
         // Newline j of the window (j = 0, 1, .. from the tile's start) ends line
@@ -312,22 +302,24 @@ __global__ void __launch_bounds__(kRT, 4) read_pass_kernel(const uint8_t *__rest
         const uint32_t e3 = (uint32_t)E & 3u, adj = e3 ? 1u : 0u;
         for (uint32_t b0 = 0; b0 < n_own; b0 += kRecCap) {  // records in batches of kRecCap (one, but for tiny reads)
             const uint32_t nb = n_own - b0 < kRecCap ? n_own - b0 : kRecCap;
-            uint32_t rowj = e3;
-#pragma unroll
-            for (int k = 0; k < 5; ++k) {
-                uint32_t j = rowj + (uint32_t)((ex >> (13 * k)) & 0x1fffu);  // e3 + the chunk's first newline
-                rowj += (uint32_t)((tot >> (13 * k)) & 0x1fffu);
-                uint32_t m = nlm[k];
-                while (m) {
-                    const uint32_t pos = 16u * (k * kRT + tid) + (__ffs(m) - 1);
-                    m &= m - 1;
-                    const uint32_t slot = (j >> 2) - adj - b0, r4 = j & 3u;
-                    if ((j >> 2) >= adj + b0 && slot < nb) {
-                        if (k < 4 && r4 == 0) sm.start[slot] = (uint16_t)(pos + 1);
-                        else if (r4 == 1) sm.end[slot] = (uint16_t)pos;
-                    }
-                    ++j;
+            uint32_t j = e3 + (ex & 0xffffu);  // e3 + the index of the thread's first newline
+            for (uint64_t m = m64; m;) {
+                const uint32_t pos = 64u * tid + (uint32_t)(__ffsll(m) - 1);
+                m &= m - 1;
+                const uint32_t slot = (j >> 2) - adj - b0, r4 = j & 3u;
+                if ((j >> 2) >= adj + b0 && slot < nb) {
+                    if (r4 == 0) sm.start[slot] = (uint16_t)(pos + 1);
+                    else if (r4 == 1) sm.end[slot] = (uint16_t)pos;
                 }
+                ++j;
+            }
+            j = e3 + tile_nl + (ex >> 16);  // the halo: only sequence ends matter there
+            for (uint32_t m = mh; m;) {
+                const uint32_t pos = (uint32_t)kParseTile + 16u * tid + (uint32_t)(__ffs(m) - 1);
+                m &= m - 1;
+                const uint32_t slot = (j >> 2) - adj - b0;
+                if ((j & 3u) == 1u && (j >> 2) >= adj + b0 && slot < nb) sm.end[slot] = (uint16_t)pos;
+                ++j;
             }
             __syncthreads();
             // ---- records: G lanes each
