@@ -175,6 +175,17 @@ EMP_DEV uint32_t not_acgt(uint32_t x, uint32_t vm) {
 }
 // nonzero iff a byte of x selected by vm is N-class (bits 7-6 = 01, bit 3 set)
 EMP_DEV uint32_t n_class(uint32_t x, uint32_t vm) { return zero_bytes((x & 0xc8c8c8c8u) ^ 0x48484848u) & vm; }
+// x mod P = 2^29 - C for a P chosen at run time (mod1 / mod2 with their
+// constants as arguments, so that the lanes of a group reduce different
+// residues in one instruction stream)
+constexpr uint32_t kP1C = (1u << 29) - kP1, kP2C = (1u << 29) - kP2;
+EMP_DEV uint32_t mod_rt(uint64_t x, uint32_t C, uint32_t P) {
+    uint64_t y = (x & kMask29) + (x >> 29) * C;
+    y = (y & kMask29) + (y >> 29) * C;
+    const uint32_t z = (uint32_t)y;
+    return z >= P ? z - P : z;
+}
+
 // 4-base dot products of enc values in bytes (first base first), added to acc
 EMP_DEV uint32_t fw1(uint32_t e, uint32_t acc) { return __dp4a(e, 0x0105197Du, acc); }  // 125 25 5 1
 EMP_DEV uint32_t rc1(uint32_t e, uint32_t acc) { return __dp4a(e, 0x7D190501u, acc); }  // 1 5 25 125
@@ -415,14 +426,16 @@ __global__ void __launch_bounds__(kRT, 4) read_pass_kernel(const uint8_t *__rest
                         lmax = max(lmax, l32);
                         bad_kept |= bd ? 1u : 0u;
                         ++kept;
-                        if (hashed) {
-                            const uint32_t h1 = mod1((uint64_t)mod1(f1) * __ldg(tables->pow1 + L - 1));
-                            const uint32_t h2 = mod2((uint64_t)mod2(f2) * __ldg(tables->pow2 + L - 1));
-                            ulonglong2 kv;
-                            kv.x = ((uint64_t)h1 << 32) | h2;
-                            kv.y = ((uint64_t)mod1(g1) << 32) | mod2(g2);
-                            *reinterpret_cast<ulonglong2 *>(keys + 2 * k) = kv;
-                        }
+                    }
+                }
+                if (hashed && !gn) {  // kept: its four residues, one lane each (f = lg, lg + G, ..)
+                    uint32_t *kw = reinterpret_cast<uint32_t *>(keys + 2 * k);
+                    for (uint32_t f = lg; f < 4; f += G) {
+                        const bool p2 = (f & 1u) != 0;  // f: 0 fp1, 1 fp2 of the read; 2, 3 of its complement
+                        const uint64_t sum = f == 0 ? f1 : f == 1 ? f2 : f == 2 ? g1 : g2;
+                        const uint32_t C = p2 ? kP2C : kP1C, P = p2 ? kP2 : kP1;
+                        const uint32_t pw = f < 2 ? __ldg((p2 ? tables->pow2 : tables->pow1) + L - 1) : 1u;
+                        kw[f ^ 1u] = mod_rt((uint64_t)mod_rt(sum, C, P) * pw, C, P);  // key = fp1 << 32 | fp2
                     }
                 }
             }
