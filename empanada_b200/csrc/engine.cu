@@ -1,14 +1,18 @@
 // engine.cu -- job orchestration and the C ABI (include/empanada.h).
 //
 // One job runs the reference program's two phases on the device:
-//   map     main.cu:42-58  -> nl_count/scan/nl_locate, classify/scan/scatter,
-//                             fingerprint_pack (k_map.cu)
-//   reduce  overlap.cu:206-293 -> fingerprint sort + dedup_mark + init_list,
-//                             then per round update_compact, sort, join
-//                             (k_round.cu, k_sort.cu)
-// All tables stay in HBM; the only host traffic is the FASTQ in and the
-// edge list out.  output.bin records are assembled on the host exactly as
-// write_edges_binary (overlap.cu:148-161) writes them.
+//   map     main.cu:42-58  -> nl_count + scan, read_pass (and compact_reads
+//                             when a read is dropped) (k_map.cu)
+//   reduce  overlap.cu:206-293 -> duplicate removal by key buckets
+//                             (k_dedup.cu; the sort when 2n > M) +
+//                             init_list, then every round in the bucket
+//                             kernel (k_bucket.cu), or host-synchronised
+//                             rounds while a round's tables reach M/2
+//                             (k_round.cu, k_sort.cu, k_chunked.cu)
+// All tables stay in HBM; the host traffic is the FASTQ in and output.bin
+// out.  output.bin records (write_edges_binary, overlap.cu:148-161) are
+// written on the device by the bucket kernel, on the host for
+// host-synchronised rounds.  Files come in through ingest.cpp.
 #include <algorithm>
 #include <cerrno>
 #include <chrono>
