@@ -86,14 +86,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_summary(workload_key: str):
-    """DRAM traffic per algorithmic byte of each kernel profiled on this
-    workload, from the committed ncu summary (profiles/traffic.json)."""
+def traffic_summary(workload_key: str, field: str = "dram_bytes_per_algorithmic_byte"):
+    """DRAM (or, with field="l2_bytes_per_algorithmic_byte", L2) traffic per
+    algorithmic byte of each kernel profiled on this workload, from the
+    committed ncu summary (profiles/traffic.json)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         try:
-            return {v["kernel"]: float(v["dram_bytes_per_algorithmic_byte"]) for v in json.load(open(p)).values()
-                    if v.get("workload_key") == workload_key}
+            return {v["kernel"]: float(v[field]) for v in json.load(open(p)).values()
+                    if v.get("workload_key") == workload_key and field in v}
         except Exception:
             return None
     return None
@@ -800,11 +801,19 @@ def main():
         what = "round update: 13 B read + 1/4 B of bases per entry in, 12 B written per entry out"
     achieved = per_launch * nl / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
     tb = traffic.get(kname) if traffic else None
+    l2_tb = (traffic_summary(args.workload, "l2_bytes_per_algorithmic_byte") or {}).get(kname)
+    l2 = None
+    if l2_tb and ms > 0:  # the lists stay in L2 here: L2 bytes (ncu) / time against the measured L2 read rate
+        l2_peak = empanada_b200.measure_l2_read(64 << 20, device)
+        l2_ach = l2_tb * per_launch * nl / (ms / 1000.0) / 1e9
+        l2 = {"achieved": l2_ach, "peak": l2_peak, "unit": "GB/s", "frac": l2_ach / l2_peak if l2_peak else None,
+              "traffic": l2_tb * per_launch,
+              "peak_source": "measured live: emp_measure_l2_read, a 64 MiB buffer read 20 times from L2"}
     roofline = {"bound": "hbm", "kernel": kname, "algorithmic": what, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} (HBM copy, burst)",
                 "traffic": (tb * per_launch) if tb else None, "algorithmic_bytes_per_launch": per_launch,
                 "avg_launch_us": 1000.0 * ms / max(nl, 1), "launches": nl,
-                "round_kernel_ms_per_step": rk_ms / args.steps,
+                "l2": l2, "round_kernel_ms_per_step": rk_ms / args.steps,
                 "sort_pass_ms_per_step": sort_ms / args.steps, "update_ms_per_step": upd_ms / args.steps}
 
     cpu = None

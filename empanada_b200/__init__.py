@@ -467,6 +467,13 @@ def load_fastq(paths) -> bytes:
         lib.emp_free(data)
 
 
+def measure_l2_read(nbytes: int = 64 << 20, device: int = -1) -> float:
+    """The device's L2 read bandwidth in GB/s (emp_measure_l2_read)."""
+    g = ctypes.c_double()
+    check(_native.lib().emp_measure_l2_read(device, nbytes, ctypes.byref(g)), "emp_measure_l2_read")
+    return g.value
+
+
 def decode_output(data: bytes) -> list[tuple[int, np.ndarray, np.ndarray]]:
     """output.bin -> [(ovlp_len, from, to), ...] in file order."""
     recs = []

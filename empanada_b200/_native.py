@@ -181,6 +181,7 @@ SIGNATURES = {
     "emp_job_feed_files": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int]),
     "emp_fastq_load": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.POINTER(_vp), _u64p]),
     "emp_free": (None, [_vp]),
+    "emp_measure_l2_read": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]),
     "emp_graph_build": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(_vp)]),
     "emp_graph_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(GraphStats)]),
     "emp_graph_unitigs": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, _vp, ctypes.c_uint64]),

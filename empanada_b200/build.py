@@ -25,7 +25,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
 CU_SOURCES = ["k_scan.cu", "k_map.cu", "k_sort.cu", "k_sort_static.cu", "k_round.cu",
-              "k_bucket.cu", "k_chunked.cu", "k_dedup.cu", "k_graph.cu", "engine.cu"]
+              "k_bucket.cu", "k_chunked.cu", "k_dedup.cu", "k_graph.cu", "k_probe.cu", "engine.cu"]
 CXX_SOURCES = ["ingest.cpp"]  # FASTQ files: plain, gzip, BGZF (zlib)
 
 

@@ -2236,6 +2236,12 @@ emp_status emp_fastq_load(const char *const *paths, int n_paths, void **data, ui
 
 void emp_free(void *p) { std::free(p); }
 
+emp_status emp_measure_l2_read(int device, uint64_t bytes, double *gbs) {
+    if (!gbs || bytes < 16) return EMP_E_INVAL;
+    if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return EMP_E_CUDA;
+    return cuda_status(measure_l2_read(bytes, gbs));
+}
+
 emp_status emp_run_files(const char *const *input_paths, int n_inputs, const char *output_path, const emp_params *p,
                          int device, emp_stats *stats) {
     if (!output_path || n_inputs < 0 || (n_inputs && !input_paths)) return EMP_E_INVAL;

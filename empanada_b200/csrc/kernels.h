@@ -306,6 +306,9 @@ cudaError_t launch_bucket_rounds(BktJob *jobs, CoopCtl *ctl, uint32_t *err, cuda
 // directly (more than kBktMaxBuckets buckets); such a job's prologue runs
 // faster as its own launch before the round kernel, with pre_done set.
 bool bucket_prologue_apart(const BktJob &host_job);
+// The current device's L2 read bandwidth (GB/s) on a buffer of `bytes`
+// (smaller than L2), read 20 times with 16-byte loads (k_probe.cu).
+cudaError_t measure_l2_read(uint64_t bytes, double *gbs);
 cudaError_t launch_bucket_prologue(BktJob *job, cudaStream_t s);
 
 void launch_join_count(const uint64_t *skeys, const uint32_t *svals, uint64_t n, uint32_t *cnt, cudaStream_t s);

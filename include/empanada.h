@@ -269,6 +269,13 @@ emp_status emp_run_files(const char *const *input_paths, int n_inputs, const cha
 emp_status emp_fastq_load(const char *const *paths, int n_paths, void **data, uint64_t *bytes);
 void emp_free(void *p);
 
+/* Measurement aid (no counterpart in the reference): the device's L2 read
+ * bandwidth in GB/s, a buffer of `bytes` (keep it well below the L2's size)
+ * read again and again with 16-byte loads once it is in L2.  The round
+ * kernel's lists stay in L2 on smaller workloads; this is the denominator of
+ * its L2 roofline.  device < 0: current device. */
+emp_status emp_measure_l2_read(int device, uint64_t bytes, double *gbs);
+
 /* Unitigs of the overlap graph in an output.bin: the downstream consumer
  * that the reference leaves out (its GFA writers, overlap.cu:129-190, are dead
  * code).  Nodes are read-ends (rid 2i = read i, 2i+1 = its reverse

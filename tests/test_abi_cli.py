@@ -108,9 +108,17 @@ def test_cli_option_without_value_fails():
     assert p.returncode == 1
 
 
-@pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES") is None and os.path.exists("/dev/nvidia0"),
-                    reason="GPU present: covered by the GPU tests")
+def _gpu_usable() -> bool:
+    ctx = ctypes.c_void_p()
+    if _native.lib().emp_ctx_create(0, 0, ctypes.byref(ctx)) != 0:
+        return False
+    _native.lib().emp_ctx_destroy(ctx)
+    return True
+
+
 def test_cli_without_gpu_fails_cleanly(tmp_path):
+    if _gpu_usable():
+        pytest.skip("GPU present: the CLI runs under the GPU tests")
     fq = tmp_path / "in.fq"
     fq.write_bytes(b"@r0\nACGT\n+\nIIII\n")
     p = _cli([str(fq), str(tmp_path / "out.bin")], cwd=str(tmp_path))
@@ -144,3 +152,10 @@ def test_server_and_batch_arguments_without_a_gpu():
     assert lib.emp_server_destroy(None) == _native.EMP_E_INVAL
     assert lib.emp_batch_run(None, None, 0, None) == _native.EMP_E_INVAL
     assert lib.emp_job_status(None) == _native.EMP_E_INVAL
+
+
+def test_l2_probe_rejects_a_tiny_buffer():
+    """emp_measure_l2_read checks its arguments before touching a device."""
+    g = ctypes.c_double()
+    assert _native.lib().emp_measure_l2_read(-1, 8, ctypes.byref(g)) == -1  # EMP_E_INVAL
+    assert _native.lib().emp_measure_l2_read(-1, 1 << 20, None) == -1
