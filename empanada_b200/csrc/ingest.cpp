@@ -59,7 +59,6 @@ bool inflate_member(const uint8_t *in, size_t in_n, uint8_t *out, size_t out_n) 
 struct FastqReader::File {
     FILE *f = nullptr;
     int kind = 0;  // 0 plain, 1 gzip, 2 BGZF
-    uint64_t size = 0;
     // gzip
     z_stream z{};
     bool z_init = false, z_end = false;
@@ -107,6 +106,7 @@ emp_status FastqReader::open(const char *const *paths, int n, int threads) {
     else if (paths_.size() > 1) size_hint_ += paths_.size() - 1;  // room for the added newlines
     last_byte_ = '\n';
     emitted_ = 0;
+    pending_nl_ = false;
     return EMP_OK;
 }
 
