@@ -57,6 +57,8 @@ def lib():
         l.emp_oracle_run.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_uint64,
                                      ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t),
                                      ctypes.POINTER(OracleStats)]
+        l.emp_oracle_run_var.restype = ctypes.c_int
+        l.emp_oracle_run_var.argtypes = l.emp_oracle_run.argtypes
         l.emp_oracle_fingerprints.restype = ctypes.c_int
         l.emp_oracle_fingerprints.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_uint64,
                                               u64p, ctypes.POINTER(ctypes.c_int32)]
@@ -94,14 +96,15 @@ class OracleError(RuntimeError):
         super().__init__(f"oracle status {code}")
 
 
-def run(fastq, min_ovlp: int = 31, reduce_mem: int = 1 << 30) -> tuple[bytes, dict]:
-    """FASTQ bytes -> (output.bin bytes, stats); raises OracleError on a non-zero status."""
+def run(fastq, min_ovlp: int = 31, reduce_mem: int = 1 << 30, variable: bool = False) -> tuple[bytes, dict]:
+    """FASTQ bytes -> (output.bin bytes, stats); raises OracleError on a non-zero status.
+    variable=True runs the variable-length extension (emp_oracle_run_var)."""
     keep, ptr, n = _buf(fastq)
     out = ctypes.c_void_p()
     out_len = ctypes.c_size_t()
     st = OracleStats()
-    rc = lib().emp_oracle_run(ptr, n, min_ovlp, reduce_mem, ctypes.byref(out), ctypes.byref(out_len),
-                              ctypes.byref(st))
+    fn = lib().emp_oracle_run_var if variable else lib().emp_oracle_run
+    rc = fn(ptr, n, min_ovlp, reduce_mem, ctypes.byref(out), ctypes.byref(out_len), ctypes.byref(st))
     del keep
     if rc != OK:
         raise OracleError(rc)

@@ -32,6 +32,10 @@
  * bases outside ACGTacgt that survive the N filter) return EMP_ORACLE_E_FORMAT;
  * reads longer than 512 return EMP_ORACLE_E_UNSUPPORTED (lengths 256-512 are
  * the reference's undefined range, extended with the same exact hash).
+ * emp_oracle_run_var is the variable-length extension of the same run (the
+ * reference requires equal lengths, fingerprint.cu:134-135): it defines the
+ * result for reads of unequal length and equals emp_oracle_run when every
+ * read has the same length.
  */
 #include "empanada_oracle.h"
 
@@ -138,14 +142,21 @@ void emp_oracle_free(void *p) { free(p); }
  * line (the last may be unterminated); record k's sequence is line 4k+1
  * (extractReads :70-87).  markNs (:119-121) marks each byte; a sequence whose
  * maximum mark is 9 (an N-class byte) is dropped, and '\n' bytes are removed
- * (:146-155); an empty sequence vanishes (:164-167). */
-int emp_oracle_parse(const char *fq, size_t len, char **reads_out, uint64_t *n_out, int32_t *L_out) {
-    size_t cap = 1 << 20, used = 0;
+ * (:146-155); an empty sequence vanishes (:164-167).
+ *
+ * allow_var keeps reads of unequal length (the variable-length extension);
+ * offs_out then receives n + 1 offsets into the concatenated reads (read i is
+ * reads[offs[i], offs[i+1])) and L_out the longest length. */
+static int parse_core(const char *fq, size_t len, int allow_var, char **reads_out, uint64_t **offs_out,
+                      uint64_t *n_out, int32_t *L_out) {
+    size_t cap = 1 << 20, used = 0, ocap = 1024;
     char *reads = (char *)malloc(cap);
-    if (!reads) return EMP_ORACLE_E_NOMEM;
+    uint64_t *offs = allow_var ? (uint64_t *)malloc(ocap * sizeof(uint64_t)) : NULL;
+    if (!reads || (allow_var && !offs)) { free(reads); free(offs); return EMP_ORACLE_E_NOMEM; }
     int32_t L = -1;
     uint64_t n = 0, line = 0;
     size_t pos = 0;
+    int st = EMP_ORACLE_OK;
     while (pos < len) {
         const char *nl = (const char *)memchr(fq + pos, '\n', len - pos);
         size_t e = nl ? (size_t)(nl - fq) : len;
@@ -160,14 +171,27 @@ int emp_oracle_parse(const char *fq, size_t len, char **reads_out, uint64_t *n_o
             size_t sl = e - pos;
             if (maxv != 9 && sl > 0) {
                 for (size_t j = pos; j < e; ++j)
-                    if (!is_acgt(fq[j])) { free(reads); return EMP_ORACLE_E_FORMAT; }
-                if (L < 0) L = (int32_t)(sl > (size_t)INT32_MAX ? INT32_MAX : sl);
-                if ((size_t)L != sl) { free(reads); return EMP_ORACLE_E_FORMAT; }
+                    if (!is_acgt(fq[j])) { st = EMP_ORACLE_E_FORMAT; goto fail; }
+                const int32_t sl32 = (int32_t)(sl > (size_t)INT32_MAX ? INT32_MAX : sl);
+                if (L < 0) L = sl32;
+                if ((size_t)L != sl) {
+                    if (!allow_var) { st = EMP_ORACLE_E_FORMAT; goto fail; }
+                    if (sl32 > L) L = sl32;
+                }
                 if (used + sl > cap) {
                     while (used + sl > cap) cap *= 2;
                     char *nr = (char *)realloc(reads, cap);
-                    if (!nr) { free(reads); return EMP_ORACLE_E_NOMEM; }
+                    if (!nr) { st = EMP_ORACLE_E_NOMEM; goto fail; }
                     reads = nr;
+                }
+                if (allow_var) {
+                    if (n + 2 > ocap) {
+                        ocap *= 2;
+                        uint64_t *no = (uint64_t *)realloc(offs, ocap * sizeof(uint64_t));
+                        if (!no) { st = EMP_ORACLE_E_NOMEM; goto fail; }
+                        offs = no;
+                    }
+                    offs[n] = used;
                 }
                 memcpy(reads + used, fq + pos, sl);
                 used += sl;
@@ -178,19 +202,47 @@ int emp_oracle_parse(const char *fq, size_t len, char **reads_out, uint64_t *n_o
         pos = e + 1;
     }
     /* format errors anywhere in the file take precedence over the length limit */
-    if (n && L > MAX_RD_LEN) { free(reads); return EMP_ORACLE_E_UNSUPPORTED; }
+    if (n && L > MAX_RD_LEN) { st = EMP_ORACLE_E_UNSUPPORTED; goto fail; }
+    if (allow_var) {
+        offs[n] = used;
+        *offs_out = offs;
+    }
     *reads_out = reads;
     *n_out = n;
     *L_out = n ? L : 0;
     return EMP_ORACLE_OK;
+fail:
+    free(reads);
+    free(offs);
+    return st;
+}
+
+int emp_oracle_parse(const char *fq, size_t len, char **reads_out, uint64_t *n_out, int32_t *L_out) {
+    return parse_core(fq, len, 0, reads_out, NULL, n_out, L_out);
+}
+
+/* The kept reads: n reads of L bases back to back, or (off != NULL) read i at
+ * base + off[i] with off[i+1] - off[i] bases. */
+typedef struct {
+    const char *base;
+    const uint64_t *off;
+    int32_t L;
+} readset_t;
+
+static inline const char *rs_read(const readset_t *rs, uint64_t i) {
+    return rs->off ? rs->base + rs->off[i] : rs->base + i * (uint64_t)rs->L;
+}
+static inline int32_t rs_len(const readset_t *rs, uint64_t i) {
+    return rs->off ? (int32_t)(rs->off[i + 1] - rs->off[i]) : rs->L;
 }
 
 /* hash of read i (rid 2i) and of its reverse complement (rid 2i+1);
  * fingerprint.cu:75-115 interleaves forward and RC line ids, so rid = 2i+s. */
-static void fingerprints_of(const char *reads, uint64_t n, int32_t L, uint64_t *keys) {
+static void fingerprints_of(const readset_t *rs, uint64_t n, uint64_t *keys) {
     char rc[MAX_RD_LEN + 1];
     for (uint64_t i = 0; i < n; ++i) {
-        const char *s = reads + i * (uint64_t)L;
+        const char *s = rs_read(rs, i);
+        const int32_t L = rs_len(rs, i);
         for (int32_t j = 0; j < L; ++j) rc[j] = comp(s[L - 1 - j]);
         keys[2 * i] = emp_oracle_hash(s, L);
         keys[2 * i + 1] = emp_oracle_hash(rc, L);
@@ -207,7 +259,8 @@ int emp_oracle_fingerprints(const char *fq, size_t len, uint64_t *keys, uint64_t
     *n_out = n;
     *L_out = L;
     if (2 * n > cap) { free(reads); return EMP_ORACLE_E_INVAL; }
-    fingerprints_of(reads, n, L, keys);
+    const readset_t rs = {reads, NULL, L};
+    fingerprints_of(&rs, n, keys);
     free(reads);
     return EMP_ORACLE_OK;
 }
@@ -423,10 +476,14 @@ static int dedup(table_t *T, size_t M) {
 
 /* regenerate_fingerprints + filter_bases (overlap.cu:605-692).  Sorted by
  * read-end id, then per M-chunk: even ids (forward read-ends) ascending,
- * then odd ids (reverse complements) ascending; even ids take base fcol of
- * read rid/2, odd ids the complement of base rcol. */
-static int regen(table_t *T, const char *reads, int32_t L, int32_t fcol, int32_t rcol, size_t M, int sfx,
-                 int32_t len) {
+ * then odd ids (reverse complements) ascending.  Going from overlap length
+ * ell + 1 to ell, a suffix drops the first base of its read-end (a forward
+ * read-end of length len: base len-1-ell of the read; a reverse complement:
+ * the complement of base ell) and a prefix its last base (forward: base ell;
+ * reverse complement: the complement of base len-1-ell).  With every read of
+ * length L and ell = L-1-round these are the reference's columns: suffix
+ * round, L-1-round; prefix L-1-round, round. */
+static int regen(table_t *T, const readset_t *rs, int32_t ell, size_t M, int sfx) {
     const size_t N = T->n;
     if (radix_sort(T->k, T->v, N, 1)) return -1;
     if (scratch_reserve(N)) return -1;
@@ -436,9 +493,11 @@ static int regen(table_t *T, const char *reads, int32_t L, int32_t fcol, int32_t
             for (size_t i = off; i < off + np; ++i) {
                 uint32_t rid = T->v[i];
                 if ((int)(rid & 1) != parity) continue;
-                const char *rd = reads + (uint64_t)(rid / 2) * (uint64_t)L;
+                const char *rd = rs_read(rs, rid / 2);
+                const int32_t len = rs_len(rs, rid / 2);
+                const int32_t fcol = sfx ? len - 1 - ell : ell, rcol = sfx ? ell : len - 1 - ell;
                 char base = parity ? comp(rd[rcol]) : rd[fcol];
-                g_tk[w] = sfx ? emp_oracle_next_sfx(T->k[i], base, len) : emp_oracle_prev_pfx(T->k[i], base);
+                g_tk[w] = sfx ? emp_oracle_next_sfx(T->k[i], base, ell + 1) : emp_oracle_prev_pfx(T->k[i], base);
                 g_tv[w] = rid;
                 ++w;
             }
@@ -558,9 +617,18 @@ static int emit(table_t *A, table_t *B, size_t M, int32_t ovlp_len, uint8_t *mar
     return rc;
 }
 
-/* build_graph (overlap.cu:206-293) after the map phase (main.cu:42-67). */
-int emp_oracle_run(const char *fq, size_t len, int32_t min_ovlp, uint64_t reduce_mem, uint8_t **out,
-                   size_t *out_len, emp_oracle_stats *stats) {
+/* build_graph (overlap.cu:206-293) after the map phase (main.cu:42-67).
+ *
+ * allow_var runs the variable-length extension (the reference asserts equal
+ * lengths, fingerprint.cu:134-135): the overlap length ell goes from the
+ * longest read's L-1 down to min_ovlp, and a read-end of length len joins both
+ * tables at ell = len-1 (its first proper suffix and prefix), so a table at
+ * ell holds the read-ends longer than ell that have not left it.  Duplicate
+ * removal works on the full-length keys of all read-ends, as in the
+ * reference.  With every read of one length all read-ends join at ell = L-1
+ * and the run is the reference's. */
+static int run_core(const char *fq, size_t len, int32_t min_ovlp, uint64_t reduce_mem, int allow_var, uint8_t **out,
+                    size_t *out_len, emp_oracle_stats *stats) {
     init_tables();
     emp_oracle_stats local;
     if (!stats) stats = &local;
@@ -568,50 +636,88 @@ int emp_oracle_run(const char *fq, size_t len, int32_t min_ovlp, uint64_t reduce
     const size_t M = (size_t)(reduce_mem / 16);
     if (M < 2) return EMP_ORACLE_E_INVAL;
     char *reads = NULL;
+    uint64_t *offs = NULL;
     uint64_t n = 0;
     int32_t L = 0;
-    int st = emp_oracle_parse(fq, len, &reads, &n, &L);
+    int st = parse_core(fq, len, allow_var, &reads, &offs, &n, &L);
     if (st) return st;
     stats->n_reads = n;
     stats->read_len = L;
-    if (L > 0 && min_ovlp < 0) { free(reads); return EMP_ORACLE_E_INVAL; }
+    if (L > 0 && min_ovlp < 0) { free(reads); free(offs); return EMP_ORACLE_E_INVAL; }
+    const readset_t rs = {reads, offs, L};
 
-    table_t S = {0}, P = {0};
+    table_t S = {0}, P = {0}, J = {0};
     bytes_t o = {0};
     uint8_t *mark = NULL;
     int rc = 0;
-    if (tab_reserve(&S, 2 * n)) { rc = EMP_ORACLE_E_NOMEM; goto done; }
-    fingerprints_of(reads, n, L, S.k);
-    for (uint64_t r = 0; r < 2 * n; ++r) S.v[r] = (uint32_t)r;
-    S.n = 2 * n;
+    size_t next = 0;
+    if (tab_reserve(&J, 2 * n)) { rc = EMP_ORACLE_E_NOMEM; goto done; }
+    fingerprints_of(&rs, n, J.k);
+    for (uint64_t r = 0; r < 2 * n; ++r) J.v[r] = (uint32_t)r;
+    J.n = 2 * n;
     /* cq_sort_by_key by read id (overlap.cu:212) leaves the rid order as is */
-    if (fp_sort(&S, M)) { rc = EMP_ORACLE_E_NOMEM; goto done; }          /* overlap.cu:213 */
-    if ((rc = dedup(&S, M)) != 0) goto done;                             /* overlap.cu:222 */
-    stats->n_unique = S.n;
-    if (tab_append(&P, S.k, S.v, S.n)) { rc = EMP_ORACLE_E_NOMEM; goto done; } /* :241-242 */
+    if (fp_sort(&J, M)) { rc = EMP_ORACLE_E_NOMEM; goto done; }          /* overlap.cu:213 */
+    if ((rc = dedup(&J, M)) != 0) goto done;                             /* overlap.cu:222 */
+    stats->n_unique = J.n;
+    if (allow_var) { /* joining order: longest read-ends first (a counting sort by length) */
+        static size_t at[MAX_RD_LEN + 2];
+        memset(at, 0, sizeof at);
+        for (size_t i = 0; i < J.n; ++i) at[MAX_RD_LEN - rs_len(&rs, J.v[i] / 2) + 1]++;
+        for (int c = 1; c <= MAX_RD_LEN + 1; ++c) at[c] += at[c - 1];
+        table_t K = {0};
+        if (tab_reserve(&K, J.n)) { tab_free(&K); rc = EMP_ORACLE_E_NOMEM; goto done; }
+        for (size_t i = 0; i < J.n; ++i) {
+            const size_t d = at[MAX_RD_LEN - rs_len(&rs, J.v[i] / 2)]++;
+            K.k[d] = J.k[i];
+            K.v[d] = J.v[i];
+        }
+        K.n = J.n;
+        tab_free(&J);
+        J = K;
+    }
     mark = (uint8_t *)calloc(2 * n + 1, 1);
     if (!mark) { rc = EMP_ORACLE_E_NOMEM; goto done; }
-    for (int32_t round = 0; round < L - min_ovlp && S.n > 0; ++round) {
+    for (int32_t ell = L - 1, round = 0; ell >= min_ovlp; --ell, ++round) {
+        /* read-ends of length ell+1 join (all of them at ell = L-1 when lengths are equal; :241-242) */
+        size_t end = next;
+        while (end < J.n && (!allow_var || rs_len(&rs, J.v[end] / 2) == ell + 1)) ++end;
+        if (end > next && (tab_append(&S, J.k + next, J.v + next, end - next) ||
+                           tab_append(&P, J.k + next, J.v + next, end - next))) { rc = EMP_ORACLE_E_NOMEM; goto done; }
+        next = end;
+        int more = 0; /* read-ends still to join at some ell' >= min_ovlp */
+        if (next < J.n) more = rs_len(&rs, J.v[next] / 2) - 1 >= min_ovlp;
+        if (S.n == 0 && !more) break;
         if (round < EMP_ORACLE_MAX_ROUNDS) {
             stats->sfx_live[round] = S.n;
             stats->pfx_live[round] = P.n;
         }
         uint64_t e0 = stats->n_edges;
-        if (regen(&S, reads, L, round, L - 1 - round, M, 1, L - round) ||
-            regen(&P, reads, L, L - 1 - round, round, M, 0, 0)) { rc = EMP_ORACLE_E_NOMEM; goto done; }
+        if (regen(&S, &rs, ell, M, 1) || regen(&P, &rs, ell, M, 0)) { rc = EMP_ORACLE_E_NOMEM; goto done; }
         if (fp_sort(&S, M) || fp_sort(&P, M)) { rc = EMP_ORACLE_E_NOMEM; goto done; }
-        rc = emit(&S, &P, M, L - 1 - round, mark, &o, &stats->n_edges, &stats->n_records);
+        rc = emit(&S, &P, M, ell, mark, &o, &stats->n_edges, &stats->n_records);
         if (rc) { if (rc < 0 && rc != EMP_ORACLE_E_HANG) rc = EMP_ORACLE_E_NOMEM; goto done; }
         if (round < EMP_ORACLE_MAX_ROUNDS) stats->edges[round] = stats->n_edges - e0;
         stats->n_rounds = round + 1;
     }
 done:
     free(reads);
+    free(offs);
     free(mark);
     tab_free(&S);
     tab_free(&P);
+    tab_free(&J);
     if (rc) { free(o.p); return rc; }
     *out = o.p;
     *out_len = o.n;
     return EMP_ORACLE_OK;
+}
+
+int emp_oracle_run(const char *fq, size_t len, int32_t min_ovlp, uint64_t reduce_mem, uint8_t **out, size_t *out_len,
+                   emp_oracle_stats *stats) {
+    return run_core(fq, len, min_ovlp, reduce_mem, 0, out, out_len, stats);
+}
+
+int emp_oracle_run_var(const char *fq, size_t len, int32_t min_ovlp, uint64_t reduce_mem, uint8_t **out,
+                       size_t *out_len, emp_oracle_stats *stats) {
+    return run_core(fq, len, min_ovlp, reduce_mem, 1, out, out_len, stats);
 }

@@ -5,7 +5,7 @@
  * package's smoke check and the benchmark's CPU-baseline leg compare the
  * CUDA path against; the product never links, loads or calls it.
  *
- * Parity is pinned: tests/test_oracle_ref.py compares this restatement
+ * Parity is pinned: tests/test_oracle.py compares this restatement
  * byte-for-byte with the reference's own sources built as a CPU program
  * (oracle/Makefile target ref-cpu) on seeded inputs, and against the golden
  * output.bin fixtures in tests/golden/ that the reference build produced.
@@ -47,6 +47,18 @@ typedef struct emp_oracle_stats {
  * (M = reduce_mem / 16 key-value pairs). */
 int emp_oracle_run(const char *fastq, size_t fastq_len, int32_t min_ovlp, uint64_t reduce_mem,
                    uint8_t **out, size_t *out_len, emp_oracle_stats *stats);
+
+/* Variable-length extension of emp_oracle_run (the reference requires equal
+ * read lengths, fingerprint.cu:134-135).  Overlap lengths ell run from the
+ * longest read's L-1 down to min_ovlp; a read-end of length len joins the
+ * suffix and prefix tables at ell = len-1, so the tables at ell hold the
+ * read-ends longer than ell that have not left them, and each round is the
+ * reference's round on those tables (same tie order, partitions, records and
+ * removal).  Duplicates are removed by full-length key, as in the reference.
+ * Equals emp_oracle_run when every kept read has the same length;
+ * stats->read_len is the longest length. */
+int emp_oracle_run_var(const char *fastq, size_t fastq_len, int32_t min_ovlp, uint64_t reduce_mem,
+                       uint8_t **out, size_t *out_len, emp_oracle_stats *stats);
 
 /* FASTQ -> kept reads (n x L ASCII bases, malloc'd) */
 int emp_oracle_parse(const char *fastq, size_t fastq_len, char **reads, uint64_t *n_reads, int32_t *read_len);
