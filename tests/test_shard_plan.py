@@ -33,7 +33,7 @@ from oracle import bind
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 CHILD = r"""
-import struct, sys
+import datetime, struct, sys
 import numpy as np
 import torch
 import torch.distributed as dist
@@ -74,7 +74,7 @@ def prev_pfx(k, e):  # drop the last base of a prefix (wrapping 64-bit arithmeti
 
 def main():
     fq, min_ovlp, out_path = sys.argv[1], int(sys.argv[2]), sys.argv[3]
-    dist.init_process_group("gloo")
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))  # a lost rank ends the others
     rank, W = dist.get_rank(), dist.get_world_size()
     lines = open(fq).read().split("\n")
     reads = [lines[i] for i in range(1, len(lines), 4) if lines[i]]
@@ -170,9 +170,15 @@ def run_sharded(tmp_path, data: bytes, min_ovlp: int, world: int) -> bytes:
                    MASTER_PORT=str(port), OMP_NUM_THREADS="1")
         procs.append(subprocess.Popen([sys.executable, "-c", CHILD, str(fq), str(min_ovlp), str(out)], env=env,
                                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
-    for p in procs:
-        _, err = p.communicate(timeout=300)
-        assert p.returncode == 0, err[-2000:]
+    try:
+        for p in procs:
+            _, err = p.communicate(timeout=300)
+            assert p.returncode == 0, err[-2000:]
+    finally:
+        for p in procs:  # the exact processes started here
+            if p.poll() is None:
+                p.kill()
+                p.wait()
     return out.read_bytes()
 
 
