@@ -44,10 +44,16 @@ def test_two_gloo_ranks_combine_by_the_slowest():
         procs.append(subprocess.Popen([sys.executable, "-c", CHILD.format(root=ROOT)], env=env,
                                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
     outs = []
-    for p in procs:
-        out, err = p.communicate(timeout=120)
-        assert p.returncode == 0, err
-        outs.append(out.strip().splitlines()[-1])
+    try:
+        for p in procs:
+            out, err = p.communicate(timeout=120)
+            assert p.returncode == 0, err
+            outs.append(out.strip().splitlines()[-1])
+    finally:
+        for p in procs:  # the exact processes started here
+            if p.poll() is None:
+                p.kill()
+                p.wait()
     import json
 
     res = [json.loads(o) for o in outs]
