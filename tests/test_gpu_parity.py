@@ -258,3 +258,26 @@ def test_edge_sink_walks_output_records(engine, name):
     assert len(recs) == len(want)
     for (ov, f, t), (ov2, f2, t2) in zip(recs, want):
         assert ov == ov2 and (f == f2).all() and (t == t2).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seqs", [["ACGT", "ACG"], ["ACG", "ACGTACGTACGTACGTACGT"], ["ACGTACGTACGTACGTACGTA", "ACGT"],
+                                  ["ACGR", "ACGT"], ["ACGT", "AC-T"]])
+def test_ragged_or_foreign_reads_are_a_format_error(engine, seqs):
+    """Kept reads of unequal length, or a base outside ACGTacgt that is not
+    N-class: the reference's result is undefined (it asserts equal lengths,
+    fingerprint.cu:134-135), the oracle reports EMP_E_FORMAT, and so does the
+    engine, which then runs the next job correctly."""
+    from cases import fastq
+
+    data = fastq(seqs)
+    with pytest.raises(bind.OracleError) as o:
+        bind.run(data, 1)
+    assert o.value.code == bind.E_FORMAT
+    with engine.job(min_ovlp=1) as job:
+        job.feed(data)
+        with pytest.raises(empanada_b200._native.EmpError) as e:
+            job.run()
+        assert e.value.code == empanada_b200._native.EMP_E_FORMAT
+    data, out, st = _run(engine, BY_NAME["tiny"])
+    assert hashlib.sha256(out).hexdigest() == GOLDEN["tiny"]["sha256"]
