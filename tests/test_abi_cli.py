@@ -159,3 +159,10 @@ def test_l2_probe_rejects_a_tiny_buffer():
     g = ctypes.c_double()
     assert _native.lib().emp_measure_l2_read(-1, 8, ctypes.byref(g)) == -1  # EMP_E_INVAL
     assert _native.lib().emp_measure_l2_read(-1, 1 << 20, None) == -1
+
+
+def test_integration_notes_cover_every_entry_point():
+    """Every function include/empanada.h declares is described in INTEGRATION.md."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = [n for n in declared_functions() if n not in text]
+    assert not missing, missing
