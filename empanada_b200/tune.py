@@ -58,13 +58,18 @@ class Cache:
         self.data: dict = {}
         if os.path.exists(self.path):
             try:
-                self.data = json.load(open(self.path))
+                with open(self.path) as f:
+                    data = json.load(f)
+                self.data = data if isinstance(data, dict) else {}
             except (OSError, ValueError):
                 self.data = {}
 
     def get(self, key: str) -> dict | None:
+        """The cached choice, or None (also for an entry this version cannot read)."""
         e = self.data.get(key)
-        return dict(e["choice"]) if e else None
+        if not isinstance(e, dict) or not isinstance(e.get("choice"), dict):
+            return None
+        return dict(e["choice"])
 
     def put(self, key: str, choice: dict, timings: dict) -> None:
         self.data[key] = {"choice": choice, "timings_ms": timings}

@@ -52,6 +52,19 @@ def test_cache_round_trip_and_shape_keys(tmp_path):
     assert json.load(open(p))[k]["timings_ms"] == {"bucket_mean=2175": 1.0}
 
 
+def test_cache_ignores_what_it_cannot_read(tmp_path):
+    """A damaged or foreign cache file means no cached choice, not an error."""
+    p = tmp_path / "tune.json"
+    k = tune.shape_key("job", 1_200_000, 250)
+    for text in ("{not json", "[1, 2]", json.dumps({k: 3}), json.dumps({k: {"timings_ms": {}}}),
+                 json.dumps({k: {"choice": [2900]}})):
+        p.write_text(text)
+        c = tune.Cache(str(p))
+        assert c.get(k) is None, text
+        c.put(k, {"bucket_mean": 2900}, {})  # and it is rewritten whole
+        assert tune.Cache(str(p)).get(k) == {"bucket_mean": 2900}
+
+
 def test_tune_job_uses_the_cache_without_timing(tmp_path):
     class FakeEngine:
         def __init__(self):
