@@ -30,6 +30,8 @@ import time
 import zlib
 from typing import Callable, Iterable
 
+from . import _native
+
 # the defaults first: they win ties
 JOB_CANDIDATES = {"bucket_mean": [2900, 2175, 1450], "dedup_driver": [0, 1]}
 BATCH_CANDIDATES = {"bucket_mean": [2900, 2175, 1450], "map_streams": [8, 16, 32, 4]}
@@ -125,6 +127,19 @@ def search(space: dict, apply: Callable[[dict], None], run: Callable[[], None], 
     return cands[order.index(lab)], timings
 
 
+def _apply_cached(engine, choice: dict) -> bool:
+    """Apply a cached choice; False (nothing changed) when the engine does not
+    take it: a field this version does not have, or a value it rejects."""
+    before = engine.tuning() if hasattr(engine, "tuning") else None
+    try:
+        engine.set_tuning(**choice)
+        return True
+    except (KeyError, TypeError, ValueError, _native.EmpError):
+        if before is not None:
+            engine.set_tuning(**before)
+        return False
+
+
 def tune_job(engine, job, reads: int, read_len: int, cache: Cache | None = None, space: dict | None = None,
              repeats: int = 2) -> dict:
     """Choose the engine's tuning for runs like `job` (fed, not yet run):
@@ -134,8 +149,7 @@ def tune_job(engine, job, reads: int, read_len: int, cache: Cache | None = None,
     key = shape_key("job", reads, read_len)
     cache = cache if cache is not None else Cache()
     hit = cache.get(key)
-    if hit is not None:
-        engine.set_tuning(**hit)
+    if hit is not None and _apply_cached(engine, hit):
         return {"key": key, "choice": hit, "source": "cache", "timings_ms": None}
 
     best, timings = search(space or JOB_CANDIDATES, lambda c: engine.set_tuning(**c), job.run, job.output, repeats)
@@ -151,8 +165,7 @@ def tune_batch(engine, jobs: Iterable, reads: int, read_len: int, cache: Cache |
     key = shape_key(f"batch{len(jobs)}", reads, read_len)
     cache = cache if cache is not None else Cache()
     hit = cache.get(key)
-    if hit is not None:
-        engine.set_tuning(**hit)
+    if hit is not None and _apply_cached(engine, hit):
         return {"key": key, "choice": hit, "source": "cache", "timings_ms": None}
 
     def outputs() -> bytes:

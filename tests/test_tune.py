@@ -65,6 +65,38 @@ def test_cache_ignores_what_it_cannot_read(tmp_path):
         assert tune.Cache(str(p)).get(k) == {"bucket_mean": 2900}
 
 
+def test_cached_choice_the_engine_does_not_take_is_timed_again(tmp_path):
+    """A cached choice with a field this version lacks (or a value it rejects)
+    is a miss: the candidates are timed and the cache entry replaced."""
+    class FakeEngine:
+        def __init__(self):
+            self.t = {"bucket_mean": 2900, "dedup_driver": 0}
+
+        def tuning(self):
+            return dict(self.t)
+
+        def set_tuning(self, **c):
+            for k in c:
+                if k not in self.t:
+                    raise KeyError(k)
+            self.t.update(c)
+
+    class FakeJob:
+        def run(self):
+            pass
+
+        def output(self):
+            return b"same"
+
+    c = tune.Cache(str(tmp_path / "tune.json"))
+    k = tune.shape_key("job", 1000, 100)
+    c.put(k, {"bucket_mean": 1450, "retired_field": 3}, {})
+    eng = FakeEngine()
+    res = tune.tune_job(eng, FakeJob(), 1000, 100, cache=c, space={"bucket_mean": [2175, 1450]}, repeats=1)
+    assert res["source"] == "timed" and set(res["choice"]) == {"bucket_mean"}
+    assert eng.t["dedup_driver"] == 0 and "retired_field" not in tune.Cache(c.path).get(k)
+
+
 def test_tune_job_uses_the_cache_without_timing(tmp_path):
     class FakeEngine:
         def __init__(self):
