@@ -451,6 +451,12 @@ def run_files(input_paths, output_path: str, device: int = -1, **params) -> dict
     return st.to_dict()
 
 
+def host_bytes(ptr: int, n: int) -> bytes:
+    """A copy of n bytes of host memory at ptr, of any size (ctypes.string_at
+    takes its size as a C int, so it fails from 2 GiB on)."""
+    return (ctypes.c_char * n).from_address(ptr).raw if n else b""
+
+
 def load_fastq(paths) -> bytes:
     """The FASTQ of files as a job reads them (plain, gzip, BGZF; in order,
     a newline added between files where one is missing), on the host."""
@@ -462,7 +468,7 @@ def load_fastq(paths) -> bytes:
     if not data.value:
         return b""
     try:
-        return ctypes.string_at(data.value, n.value)
+        return host_bytes(data.value, n.value)
     finally:
         lib.emp_free(data)
 

@@ -82,6 +82,11 @@ def lib():
     return _lib
 
 
+def _host_bytes(ptr, n: int) -> bytes:
+    """n bytes at ptr, of any size (the ctypes helper for this takes a C int size)."""
+    return (ctypes.c_char * n).from_address(ptr).raw if n else b""
+
+
 def _buf(fastq):
     if isinstance(fastq, np.ndarray):
         a = np.ascontiguousarray(fastq, dtype=np.uint8)
@@ -108,7 +113,7 @@ def run(fastq, min_ovlp: int = 31, reduce_mem: int = 1 << 30, variable: bool = F
     del keep
     if rc != OK:
         raise OracleError(rc)
-    data = ctypes.string_at(out, out_len.value) if out_len.value else b""
+    data = _host_bytes(out.value, out_len.value)
     lib().emp_oracle_free(out)
     return data, st.to_dict()
 
@@ -136,7 +141,7 @@ def gfa(output_bin: bytes, n_reads: int, read_len: int) -> bytes:
     del keep
     if rc != 0:
         raise OracleError(rc)
-    out = ctypes.string_at(text, ln.value)
+    out = _host_bytes(text.value, ln.value)
     lib().emp_oracle_free(text)
     return out
 

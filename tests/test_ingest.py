@@ -114,3 +114,18 @@ def test_bgzf_without_eof_block_and_gzip_with_trailing_garbage(tmp_path):
     g = write(tmp_path / "junk.fq.gz", gzip.compress(data) + b"not gzip")
     with pytest.raises(EmpError):
         empanada_b200.load_fastq(g)
+
+
+def test_host_copies_beyond_2_gib():
+    """load_fastq hands out inputs above 2 GiB (a copy whose size is a C int
+    fails there)."""
+    import psutil
+
+    n = (1 << 31) + 64
+    if psutil.virtual_memory().available < 3 * n:
+        pytest.skip("not enough free host memory for a 2 GiB copy")
+    a = np.zeros(n, dtype=np.uint8)
+    a[[0, (1 << 31) - 1, 1 << 31, n - 1]] = [65, 67, 71, 84]
+    b = empanada_b200.host_bytes(a.ctypes.data, n)
+    assert len(b) == n and b[0] == 65 and b[(1 << 31) - 1] == 67 and b[1 << 31] == 71 and b[-1] == 84
+    assert empanada_b200.host_bytes(a.ctypes.data, 0) == b""
