@@ -1,6 +1,7 @@
 // ingest.cpp -- FASTQ input from files, produced chunk by chunk into the
-// caller's (pinned) buffers: plain files, gzip (one or more members) and
-// BGZF (blocked gzip, the blocks inflated in parallel on the host cores);
+// caller's (pinned) buffers: plain files (slices read by several threads at
+// once), gzip (one or more members) and BGZF (blocked gzip, the blocks
+// inflated in parallel on the host cores);
 // several files are read in order as one FASTQ, with a newline added after a
 // file that does not end with one when another file follows.
 //
@@ -9,6 +10,8 @@
 #include "ingest.h"
 
 #include <sys/stat.h>
+#include <sys/types.h>
+#include <unistd.h>
 #include <zlib.h>
 
 #include <algorithm>
@@ -59,6 +62,8 @@ bool inflate_member(const uint8_t *in, size_t in_n, uint8_t *out, size_t out_n) 
 struct FastqReader::File {
     FILE *f = nullptr;
     int kind = 0;  // 0 plain, 1 gzip, 2 BGZF
+    // plain: the next offset and the size at open (read with pread, in parallel)
+    uint64_t off = 0, size = 0;
     // gzip
     z_stream z{};
     bool z_init = false, z_end = false;
@@ -152,7 +157,11 @@ emp_status FastqReader::open_next() {
     uint8_t h[64];
     const size_t n = std::fread(h, 1, sizeof h, fl->f);
     if (std::fseek(fl->f, 0, SEEK_SET) != 0) return EMP_E_IO;
-    if (n >= 2 && h[0] == 0x1f && h[1] == 0x8b) {
+    if (n < 2 || h[0] != 0x1f || h[1] != 0x8b) {  // plain
+        struct stat sb;
+        if (::fstat(fileno(fl->f), &sb) != 0) return EMP_E_IO;
+        fl->size = (uint64_t)sb.st_size;
+    } else {
         fl->kind = bgzf_block_size(h, n) ? 2 : 1;
         if (fl->kind == 1) {
             if (inflateInit2(&fl->z, 16 + MAX_WBITS) != Z_OK) return EMP_E_NOMEM;
@@ -167,9 +176,47 @@ emp_status FastqReader::open_next() {
 emp_status FastqReader::read_file(uint8_t *dst, size_t cap, size_t *got) {
     File &fl = *cur_;
     *got = 0;
-    if (fl.kind == 0) {
-        *got = std::fread(dst, 1, cap, fl.f);
-        if (*got < cap && std::ferror(fl.f)) return EMP_E_IO;
+    if (fl.kind == 0) {  // slices of at least 16 MiB read by threads side by side (page cache: 4-5x one thread)
+        const uint64_t left = fl.size > fl.off ? fl.size - fl.off : 0;
+        const size_t n = (size_t)std::min<uint64_t>(cap, left);
+        if (!n) return EMP_OK;
+        constexpr size_t kSlice = 16u << 20;
+        const int nt = (int)std::max<size_t>(1, std::min<size_t>((size_t)threads_, n / kSlice));
+        const size_t per = ((n + nt - 1) / nt + 4095) & ~(size_t)4095;
+        const int fd = fileno(fl.f);
+        std::vector<size_t> done(nt, 0);
+        std::atomic<bool> bad{false};
+        auto slice = [&](int t) {
+            const size_t a = std::min(n, (size_t)t * per), b = std::min(n, a + per);
+            size_t p = a;
+            while (p < b) {
+                const ssize_t r = ::pread(fd, dst + p, b - p, (off_t)(fl.off + p));
+                if (r < 0 && errno == EINTR) continue;
+                if (r < 0) {
+                    bad = true;
+                    break;
+                }
+                if (r == 0) break;  // the file got shorter since it was opened
+                p += (size_t)r;
+            }
+            done[t] = p - a;
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(slice, t);
+        slice(0);
+        for (std::thread &t : pool) t.join();
+        if (bad) return EMP_E_IO;
+        size_t total = 0;  // the bytes in one piece from the start
+        for (int t = 0; t < nt; ++t) {
+            total += done[t];
+            const size_t a = std::min(n, (size_t)t * per), b = std::min(n, a + per);
+            if (done[t] < b - a) {
+                fl.size = fl.off + total;  // it ends here
+                break;
+            }
+        }
+        fl.off += total;
+        *got = total;
         return EMP_OK;
     }
     if (fl.kind == 1) {  // a gzip stream: members one after another

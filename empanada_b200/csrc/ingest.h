@@ -26,8 +26,9 @@ class FastqReader {
     FastqReader(const FastqReader &) = delete;
     FastqReader &operator=(const FastqReader &) = delete;
     // The files in order.  A missing file reads as empty; a path that exists
-    // but is not a regular file is EMP_E_IO.  threads: host threads that
-    // inflate BGZF blocks (0: the machine's, at most 32).
+    // but is not a regular file is EMP_E_IO; a plain file is read up to its
+    // size at the time it is opened.  threads: host threads that read slices
+    // of a plain file or inflate BGZF blocks (0: the machine's, at most 32).
     emp_status open(const char *const *paths, int n, int threads = 0);
     // The next bytes of the FASTQ into dst (cap >= kMinChunk): at least cap/2
     // of them unless the input ends; *got = 0 at the end.  EMP_E_FORMAT for a

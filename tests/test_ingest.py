@@ -70,6 +70,16 @@ def test_large_inputs_span_many_pieces(tmp_path):
     assert empanada_b200.load_fastq(bg) == data
 
 
+def test_large_plain_files_read_in_slices(tmp_path):
+    """Plain files above the 16 MiB slice size are read by several threads at
+    once; the pieces land in order, across files too."""
+    a = fastq(300_000, L=150, seed=9)  # about 95 MB: several slices
+    b = fastq(70_001, L=101, seed=10, trailing_newline=False)  # not a multiple of the page size
+    pa, pb = write(tmp_path / "a.fq", a), write(tmp_path / "b.fq", b)
+    assert empanada_b200.load_fastq(pa) == a
+    assert empanada_b200.load_fastq([pb, pa, pb]) == b + b"\n" + a + b
+
+
 def test_files_in_order_with_newlines_between(tmp_path):
     a = fastq(10, seed=5, trailing_newline=False)
     b = fastq(20, seed=6)
