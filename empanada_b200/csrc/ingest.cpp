@@ -43,20 +43,6 @@ size_t bgzf_block_size(const uint8_t *h, size_t n) {
 
 uint32_t le32(const uint8_t *p) { return p[0] | (uint32_t)p[1] << 8 | (uint32_t)p[2] << 16 | (uint32_t)p[3] << 24; }
 
-// One gzip member in memory -> exactly `out_n` bytes at out (its ISIZE).
-bool inflate_member(const uint8_t *in, size_t in_n, uint8_t *out, size_t out_n) {
-    z_stream z{};
-    if (inflateInit2(&z, 16 + MAX_WBITS) != Z_OK) return false;
-    z.next_in = const_cast<Bytef *>(in);
-    z.avail_in = (uInt)in_n;
-    z.next_out = out;
-    z.avail_out = (uInt)out_n;
-    const int rc = inflate(&z, Z_FINISH);
-    const bool ok = rc == Z_STREAM_END && z.total_out == out_n && z.avail_in == 0;
-    inflateEnd(&z);
-    return ok;
-}
-
 }  // namespace
 
 struct FastqReader::File {
@@ -68,8 +54,10 @@ struct FastqReader::File {
     z_stream z{};
     bool z_init = false, z_end = false;
     std::vector<uint8_t> in;
-    // BGZF
-    std::vector<uint8_t> blocks;
+    // BGZF: compressed bytes [lo, hi) of buf not yet inflated; `off` is the
+    // file offset of buf's end
+    std::vector<uint8_t> buf;
+    size_t lo = 0, hi = 0;
     ~File() {
         if (z_init) inflateEnd(&z);
         if (f) std::fclose(f);
@@ -157,11 +145,10 @@ emp_status FastqReader::open_next() {
     uint8_t h[64];
     const size_t n = std::fread(h, 1, sizeof h, fl->f);
     if (std::fseek(fl->f, 0, SEEK_SET) != 0) return EMP_E_IO;
-    if (n < 2 || h[0] != 0x1f || h[1] != 0x8b) {  // plain
-        struct stat sb;
-        if (::fstat(fileno(fl->f), &sb) != 0) return EMP_E_IO;
-        fl->size = (uint64_t)sb.st_size;
-    } else {
+    struct stat sb;
+    if (::fstat(fileno(fl->f), &sb) != 0) return EMP_E_IO;
+    fl->size = (uint64_t)sb.st_size;  // plain and BGZF files are read with pread up to this size
+    if (n >= 2 && h[0] == 0x1f && h[1] == 0x8b) {
         fl->kind = bgzf_block_size(h, n) ? 2 : 1;
         if (fl->kind == 1) {
             if (inflateInit2(&fl->z, 16 + MAX_WBITS) != Z_OK) return EMP_E_NOMEM;
@@ -251,44 +238,73 @@ emp_status FastqReader::read_file(uint8_t *dst, size_t cap, size_t *got) {
         *got = (size_t)(z.next_out - dst);
         return EMP_OK;
     }
-    // BGZF: whole blocks whose inflated sizes fit cap, inflated in parallel
+    // BGZF: whole blocks whose inflated sizes fit cap, inflated in parallel.
+    // Compressed bytes come in by large preads; block bounds are parsed in
+    // memory (a block is at most 64 KiB).
+    constexpr size_t kMaxBlock = 65536, kRefill = 16u << 20, kMaxIn = 256u << 20;
     std::vector<size_t> boff, bsz, ooff;
     size_t total_out = 0;
-    fl.blocks.clear();
+    const int fd = fileno(fl.f);
     for (;;) {
-        uint8_t h[64];
-        const long at = std::ftell(fl.f);
-        const size_t n = std::fread(h, 1, sizeof h, fl.f);
-        if (n == 0) {
-            if (std::ferror(fl.f)) return EMP_E_IO;
-            break;
+        if (fl.hi - fl.lo < kMaxBlock && fl.off < fl.size) {  // room for one whole block, unless the file ends
+            if (boff.empty() && fl.lo) {  // nothing of this call points into buf yet: drop what was inflated
+                std::memmove(fl.buf.data(), fl.buf.data() + fl.lo, fl.hi - fl.lo);
+                fl.hi -= fl.lo;
+                fl.lo = 0;
+            }
+            const size_t want = (size_t)std::min<uint64_t>(kRefill, fl.size - fl.off);
+            if (fl.buf.size() < fl.hi + want) fl.buf.resize(fl.hi + want);
+            size_t p = 0;
+            while (p < want) {
+                const ssize_t r = ::pread(fd, fl.buf.data() + fl.hi + p, want - p, (off_t)(fl.off + p));
+                if (r < 0 && errno == EINTR) continue;
+                if (r < 0) return EMP_E_IO;
+                if (r == 0) break;  // the file got shorter since it was opened
+                p += (size_t)r;
+            }
+            fl.hi += p;
+            fl.off += p;
+            if (p < want) fl.size = fl.off;
         }
-        const size_t bs = bgzf_block_size(h, n);
-        if (!bs) return EMP_E_FORMAT;
-        if (std::fseek(fl.f, at, SEEK_SET) != 0) return EMP_E_IO;
-        const size_t o = fl.blocks.size();
-        fl.blocks.resize(o + bs);
-        if (std::fread(fl.blocks.data() + o, 1, bs, fl.f) != bs) return EMP_E_FORMAT;
-        const uint32_t isize = le32(fl.blocks.data() + o + bs - 4);
-        if (total_out + isize > cap) {  // for the next call
-            fl.blocks.resize(o);
-            if (std::fseek(fl.f, at, SEEK_SET) != 0) return EMP_E_IO;
+        const size_t avail = fl.hi - fl.lo;
+        if (avail == 0) break;  // the end of the file
+        const uint8_t *h = fl.buf.data() + fl.lo;
+        const size_t bs = bgzf_block_size(h, avail);
+        if (!bs || bs < 26 || bs > avail) return EMP_E_FORMAT;  // not a block, or a block cut short
+        const uint32_t isize = le32(h + bs - 4);
+        if (total_out + isize > cap) {
             if (boff.empty()) return EMP_E_FORMAT;  // a block larger than BGZF allows (64 KiB)
-            break;
+            break;                                  // for the next call
         }
-        boff.push_back(o);
+        boff.push_back(fl.lo);
         bsz.push_back(bs);
         ooff.push_back(total_out);
         total_out += isize;
-        if (fl.blocks.size() > (256u << 20)) break;
+        fl.lo += bs;
+        if (fl.lo - boff.front() > kMaxIn) break;
     }
     std::atomic<size_t> next{0};
     std::atomic<bool> bad{false};
-    auto work = [&] {
+    auto work = [&] {  // one zlib stream per thread, reset for each block
+        z_stream z{};
+        if (inflateInit2(&z, 16 + MAX_WBITS) != Z_OK) {
+            bad = true;
+            return;
+        }
         for (size_t b; (b = next.fetch_add(1)) < boff.size();) {
             const size_t isize = (b + 1 < boff.size() ? ooff[b + 1] : total_out) - ooff[b];
-            if (!inflate_member(fl.blocks.data() + boff[b], bsz[b], dst + ooff[b], isize)) bad = true;
+            if (inflateReset(&z) != Z_OK) {
+                bad = true;
+                break;
+            }
+            z.next_in = const_cast<Bytef *>(fl.buf.data() + boff[b]);
+            z.avail_in = (uInt)bsz[b];
+            z.next_out = dst + ooff[b];
+            z.avail_out = (uInt)isize;
+            const int rc = inflate(&z, Z_FINISH);
+            if (rc != Z_STREAM_END || z.avail_out != 0 || z.avail_in != 0) bad = true;
         }
+        inflateEnd(&z);
     };
     const int nt = (int)std::min<size_t>(threads_, (boff.size() + 7) / 8);
     std::vector<std::thread> pool;

@@ -16,13 +16,13 @@ from empanada_b200 import EmpError
 BGZF_EOF = bytes.fromhex("1f8b08040000000000ff0600424302001b0003000000000000000000")
 
 
-def bgzf(data: bytes, block: int = 65280, eof: bool = True) -> bytes:
+def bgzf(data: bytes, block: int = 65280, eof: bool = True, level: int = 6) -> bytes:
     """BGZF (the SAM/BAM blocked gzip): gzip members of at most 64 KiB, each
     with the 'BC' extra subfield giving its size."""
     out = bytearray()
     for o in range(0, len(data), block):
         piece = data[o:o + block]
-        c = zlib.compressobj(6, zlib.DEFLATED, -15)
+        c = zlib.compressobj(level, zlib.DEFLATED, -15)
         body = c.compress(piece) + c.flush()
         bsize = 18 + len(body) + 8
         out += bytes([0x1F, 0x8B, 8, 4, 0, 0, 0, 0, 0, 0xFF]) + struct.pack("<HBBHH", 6, 66, 67, 2, bsize - 1)
@@ -115,6 +115,20 @@ def test_damaged_or_unreadable_input_is_an_error(tmp_path):
     with pytest.raises(EmpError) as e:
         empanada_b200.load_fastq(str(tmp_path / "dir.fq"))
     assert e.value.code == -7  # EMP_E_IO
+
+
+def test_bgzf_blocks_across_reads_of_the_file(tmp_path):
+    """Compressed bytes are read 16 MiB at a time and blocks parsed in memory:
+    blocks that straddle those reads, a file cut inside a block, and bytes
+    after the last block that are not a block."""
+    data = fastq(120_000, L=150, seed=12)  # about 38 MB
+    z = bgzf(data, level=0)  # stored blocks: as large as the data, so several reads
+    p = write(tmp_path / "s.fq.bgz", z)
+    assert empanada_b200.load_fastq(p) == data
+    for bad in (z[: len(z) - 28 - 1000], z + b"not a block"):
+        with pytest.raises(EmpError) as e:
+            empanada_b200.load_fastq(write(tmp_path / "bad.fq.bgz", bad))
+        assert e.value.code == -5  # EMP_E_FORMAT
 
 
 def test_bgzf_without_eof_block_and_gzip_with_trailing_garbage(tmp_path):
