@@ -18,6 +18,8 @@
 #include <atomic>
 #include <cerrno>
 #include <cstring>
+#include <memory>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -55,9 +57,19 @@ struct FastqReader::File {
     bool z_init = false, z_end = false;
     std::vector<uint8_t> in;
     // BGZF: compressed bytes [lo, hi) of buf not yet inflated; `off` is the
-    // file offset of buf's end
-    std::vector<uint8_t> buf;
-    size_t lo = 0, hi = 0;
+    // file offset of buf's end (buf is not zeroed when it grows)
+    std::unique_ptr<uint8_t[]> buf;
+    size_t buf_cap = 0, lo = 0, hi = 0;
+    bool grow(size_t need) {
+        if (need <= buf_cap) return true;
+        const size_t c = std::max(need, 2 * buf_cap);
+        std::unique_ptr<uint8_t[]> nb(new (std::nothrow) uint8_t[c]);
+        if (!nb) return false;
+        if (hi) std::memcpy(nb.get(), buf.get(), hi);
+        buf = std::move(nb);
+        buf_cap = c;
+        return true;
+    }
     ~File() {
         if (z_init) inflateEnd(&z);
         if (f) std::fclose(f);
@@ -245,18 +257,18 @@ emp_status FastqReader::read_file(uint8_t *dst, size_t cap, size_t *got) {
     std::vector<size_t> boff, bsz, ooff;
     size_t total_out = 0;
     const int fd = fileno(fl.f);
+    if (fl.lo) {  // drop what the last call inflated (the rest is under one refill)
+        std::memmove(fl.buf.get(), fl.buf.get() + fl.lo, fl.hi - fl.lo);
+        fl.hi -= fl.lo;
+        fl.lo = 0;
+    }
     for (;;) {
         if (fl.hi - fl.lo < kMaxBlock && fl.off < fl.size) {  // room for one whole block, unless the file ends
-            if (boff.empty() && fl.lo) {  // nothing of this call points into buf yet: drop what was inflated
-                std::memmove(fl.buf.data(), fl.buf.data() + fl.lo, fl.hi - fl.lo);
-                fl.hi -= fl.lo;
-                fl.lo = 0;
-            }
             const size_t want = (size_t)std::min<uint64_t>(kRefill, fl.size - fl.off);
-            if (fl.buf.size() < fl.hi + want) fl.buf.resize(fl.hi + want);
+            if (!fl.grow(fl.hi + want)) return EMP_E_NOMEM;
             size_t p = 0;
             while (p < want) {
-                const ssize_t r = ::pread(fd, fl.buf.data() + fl.hi + p, want - p, (off_t)(fl.off + p));
+                const ssize_t r = ::pread(fd, fl.buf.get() + fl.hi + p, want - p, (off_t)(fl.off + p));
                 if (r < 0 && errno == EINTR) continue;
                 if (r < 0) return EMP_E_IO;
                 if (r == 0) break;  // the file got shorter since it was opened
@@ -268,7 +280,7 @@ emp_status FastqReader::read_file(uint8_t *dst, size_t cap, size_t *got) {
         }
         const size_t avail = fl.hi - fl.lo;
         if (avail == 0) break;  // the end of the file
-        const uint8_t *h = fl.buf.data() + fl.lo;
+        const uint8_t *h = fl.buf.get() + fl.lo;
         const size_t bs = bgzf_block_size(h, avail);
         if (!bs || bs < 26 || bs > avail) return EMP_E_FORMAT;  // not a block, or a block cut short
         const uint32_t isize = le32(h + bs - 4);
@@ -297,7 +309,7 @@ emp_status FastqReader::read_file(uint8_t *dst, size_t cap, size_t *got) {
                 bad = true;
                 break;
             }
-            z.next_in = const_cast<Bytef *>(fl.buf.data() + boff[b]);
+            z.next_in = const_cast<Bytef *>(fl.buf.get() + boff[b]);
             z.avail_in = (uInt)bsz[b];
             z.next_out = dst + ooff[b];
             z.avail_out = (uInt)isize;
