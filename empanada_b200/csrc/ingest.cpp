@@ -45,6 +45,47 @@ size_t bgzf_block_size(const uint8_t *h, size_t n) {
 
 uint32_t le32(const uint8_t *p) { return p[0] | (uint32_t)p[1] << 8 | (uint32_t)p[2] << 16 | (uint32_t)p[3] << 24; }
 
+// n bytes of fd from offset off into dst, in slices of at least min_slice
+// read by up to `threads` threads at once (from the page cache several
+// threads copy 4-5x as fast as one).  *got: the bytes read in one piece from
+// the start; fewer than n only where the file ends sooner.
+emp_status pread_slices(int fd, uint8_t *dst, size_t n, uint64_t off, int threads, size_t min_slice, size_t *got) {
+    *got = 0;
+    if (!n) return EMP_OK;
+    const int nt = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(threads, 1), n / min_slice));
+    const size_t per = ((n + nt - 1) / nt + 4095) & ~(size_t)4095;
+    std::vector<size_t> done(nt, 0);
+    std::atomic<bool> bad{false};
+    auto slice = [&](int t) {
+        const size_t a = std::min(n, (size_t)t * per), b = std::min(n, a + per);
+        size_t p = a;
+        while (p < b) {
+            const ssize_t r = ::pread(fd, dst + p, b - p, (off_t)(off + p));
+            if (r < 0 && errno == EINTR) continue;
+            if (r < 0) {
+                bad = true;
+                break;
+            }
+            if (r == 0) break;  // the file ends here
+            p += (size_t)r;
+        }
+        done[t] = p - a;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(slice, t);
+    slice(0);
+    for (std::thread &t : pool) t.join();
+    if (bad) return EMP_E_IO;
+    size_t total = 0;
+    for (int t = 0; t < nt; ++t) {
+        total += done[t];
+        const size_t a = std::min(n, (size_t)t * per), b = std::min(n, a + per);
+        if (done[t] < b - a) break;
+    }
+    *got = total;
+    return EMP_OK;
+}
+
 }  // namespace
 
 struct FastqReader::File {
@@ -175,45 +216,11 @@ emp_status FastqReader::open_next() {
 emp_status FastqReader::read_file(uint8_t *dst, size_t cap, size_t *got) {
     File &fl = *cur_;
     *got = 0;
-    if (fl.kind == 0) {  // slices of at least 16 MiB read by threads side by side (page cache: 4-5x one thread)
-        const uint64_t left = fl.size > fl.off ? fl.size - fl.off : 0;
-        const size_t n = (size_t)std::min<uint64_t>(cap, left);
-        if (!n) return EMP_OK;
-        constexpr size_t kSlice = 16u << 20;
-        const int nt = (int)std::max<size_t>(1, std::min<size_t>((size_t)threads_, n / kSlice));
-        const size_t per = ((n + nt - 1) / nt + 4095) & ~(size_t)4095;
-        const int fd = fileno(fl.f);
-        std::vector<size_t> done(nt, 0);
-        std::atomic<bool> bad{false};
-        auto slice = [&](int t) {
-            const size_t a = std::min(n, (size_t)t * per), b = std::min(n, a + per);
-            size_t p = a;
-            while (p < b) {
-                const ssize_t r = ::pread(fd, dst + p, b - p, (off_t)(fl.off + p));
-                if (r < 0 && errno == EINTR) continue;
-                if (r < 0) {
-                    bad = true;
-                    break;
-                }
-                if (r == 0) break;  // the file got shorter since it was opened
-                p += (size_t)r;
-            }
-            done[t] = p - a;
-        };
-        std::vector<std::thread> pool;
-        for (int t = 1; t < nt; ++t) pool.emplace_back(slice, t);
-        slice(0);
-        for (std::thread &t : pool) t.join();
-        if (bad) return EMP_E_IO;
-        size_t total = 0;  // the bytes in one piece from the start
-        for (int t = 0; t < nt; ++t) {
-            total += done[t];
-            const size_t a = std::min(n, (size_t)t * per), b = std::min(n, a + per);
-            if (done[t] < b - a) {
-                fl.size = fl.off + total;  // it ends here
-                break;
-            }
-        }
+    if (fl.kind == 0) {  // slices of at least 16 MiB read side by side
+        const size_t n = (size_t)std::min<uint64_t>(cap, fl.size > fl.off ? fl.size - fl.off : 0);
+        size_t total = 0;
+        EMP_TRY_ING(pread_slices(fileno(fl.f), dst, n, fl.off, threads_, 16u << 20, &total));
+        if (total < n) fl.size = fl.off + total;  // the file got shorter since it was opened
         fl.off += total;
         *got = total;
         return EMP_OK;
@@ -251,9 +258,9 @@ emp_status FastqReader::read_file(uint8_t *dst, size_t cap, size_t *got) {
         return EMP_OK;
     }
     // BGZF: whole blocks whose inflated sizes fit cap, inflated in parallel.
-    // Compressed bytes come in by large preads; block bounds are parsed in
-    // memory (a block is at most 64 KiB).
-    constexpr size_t kMaxBlock = 65536, kRefill = 16u << 20, kMaxIn = 256u << 20;
+    // Compressed bytes come in 32 MiB at a time (read in slices side by
+    // side); block bounds are parsed in memory (a block is at most 64 KiB).
+    constexpr size_t kMaxBlock = 65536, kRefill = 32u << 20, kMaxIn = 256u << 20;
     std::vector<size_t> boff, bsz, ooff;
     size_t total_out = 0;
     const int fd = fileno(fl.f);
@@ -267,13 +274,7 @@ emp_status FastqReader::read_file(uint8_t *dst, size_t cap, size_t *got) {
             const size_t want = (size_t)std::min<uint64_t>(kRefill, fl.size - fl.off);
             if (!fl.grow(fl.hi + want)) return EMP_E_NOMEM;
             size_t p = 0;
-            while (p < want) {
-                const ssize_t r = ::pread(fd, fl.buf.get() + fl.hi + p, want - p, (off_t)(fl.off + p));
-                if (r < 0 && errno == EINTR) continue;
-                if (r < 0) return EMP_E_IO;
-                if (r == 0) break;  // the file got shorter since it was opened
-                p += (size_t)r;
-            }
+            EMP_TRY_ING(pread_slices(fd, fl.buf.get() + fl.hi, want, fl.off, threads_, 4u << 20, &p));
             fl.hi += p;
             fl.off += p;
             if (p < want) fl.size = fl.off;
