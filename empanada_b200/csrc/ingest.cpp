@@ -91,7 +91,7 @@ emp_status pread_slices(int fd, uint8_t *dst, size_t n, uint64_t off, int thread
 struct FastqReader::File {
     FILE *f = nullptr;
     int kind = 0;  // 0 plain, 1 gzip, 2 BGZF
-    // plain: the next offset and the size at open (read with pread, in parallel)
+    // plain and BGZF: the next file offset to read and the size at open (pread)
     uint64_t off = 0, size = 0;
     // gzip
     z_stream z{};
